@@ -1,0 +1,195 @@
+"""CPU oracle for the explicit MPM substep -- TEST INFRASTRUCTURE ONLY.
+
+Two checkers live here, used only by tests/, the smoke check and bench.py's
+CPU-baseline leg, never by the product path:
+
+* ``mpm_oracle.c``: a plain-C FP64 restatement of the reference's substep
+  (``PhysBAM Hybrid_Methods MPM_DRIVER``), built to ``oracle/liboracle.so``.
+* ``_ref/ref_scene``: the reference itself (its own sources compiled by
+  ``ref.mk``) driven by ``ref_scene.cpp`` on a scene file.  Present only where
+  the reference sources were available at build time; its dumps are frozen into
+  ``tests/golden/`` by ``tests/golden/make_golden.py``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import shutil
+import subprocess
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+REF_SCENE = os.path.join(REF_DIR, "ref_scene")
+MAXOBJ = 32
+
+
+class _Obj(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("type", ctypes.c_int), ("friction", ctypes.c_double),
+                ("a", ctypes.c_double * 3), ("b", ctypes.c_double * 3)]
+
+
+class _Scene(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("counts", ctypes.c_int * 3), ("dmin", ctypes.c_double * 3),
+                ("dmax", ctypes.c_double * 3), ("model", ctypes.c_int), ("gravity", ctypes.c_double * 3),
+                ("nobj", ctypes.c_int), ("obj", _Obj * MAXOBJ)]
+
+
+def build(force: bool = False) -> str:
+    """Compile the C restatement (gcc, no FMA contraction so it rounds like the reference's x86-64 build)."""
+    src = os.path.join(HERE, "mpm_oracle.c")
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+        subprocess.check_call(["gcc", "-O2", "-std=c99", "-fPIC", "-shared", "-ffp-contract=off",
+                               "-o", LIB, src, "-lm"])
+    return LIB
+
+
+def build_ref(ref_root: str = "/root/reference", jobs: int = os.cpu_count() or 8) -> bool:
+    """Compile the reference's MPM path from its sources (minutes on first run)."""
+    if not os.path.isdir(ref_root):
+        return os.path.exists(REF_SCENE)
+    subprocess.check_call(["make", "-f", os.path.join(HERE, "ref.mk"), "-j%d" % jobs, "REF=" + ref_root,
+                           "OUT=" + REF_DIR], cwd=os.path.dirname(HERE))
+    return True
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(LIB)
+        P = ctypes.POINTER(ctypes.c_double)
+        _lib.oracle_substep.argtypes = [ctypes.POINTER(_Scene), ctypes.c_longlong, P, P, P, P, P, P, P, P,
+                                        ctypes.POINTER(ctypes.c_ubyte), ctypes.c_double, ctypes.c_double,
+                                        P, P, P, P]
+        _lib.oracle_substep.restype = ctypes.c_int
+        _lib.oracle_run.argtypes = [ctypes.POINTER(_Scene), ctypes.c_longlong, P, P, P, P, P, P, P, P,
+                                    ctypes.POINTER(ctypes.c_ubyte), ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        _lib.oracle_run.restype = ctypes.c_int
+        _lib.oracle_pft.argtypes = [ctypes.c_int, ctypes.c_int, P, ctypes.c_double, ctypes.c_double, P]
+        _lib.oracle_svd3.argtypes = [P, P, P, P]
+        _lib.oracle_svd3.restype = ctypes.c_int
+    return _lib
+
+
+def _scene_struct(s) -> _Scene:
+    c = _Scene()
+    c.dim = s.dim
+    for a in range(3):
+        c.counts[a] = s.counts[a] if a < s.dim else 1
+        c.dmin[a] = s.domain_min[a] if a < s.dim else 0.0
+        c.dmax[a] = s.domain_max[a] if a < s.dim else 1.0
+        c.gravity[a] = s.gravity[a] if a < s.dim else 0.0
+    c.model = s.model
+    if len(s.objects) > MAXOBJ:
+        raise ValueError("too many collision objects")
+    c.nobj = len(s.objects)
+    for i, o in enumerate(s.objects):
+        c.obj[i].kind, c.obj[i].type, c.obj[i].friction = o.kind, o.type, o.friction
+        for a in range(s.dim):
+            c.obj[i].a[a], c.obj[i].b[a] = o.a[a], o.b[a]
+    return c
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class State:
+    """Particle state in the reference layout: X,V (n,d); F,B column-major (n,d*d)."""
+
+    def __init__(self, scene):
+        d = scene.dim
+        self.scene = scene
+        self.X = np.ascontiguousarray(scene.X, np.float64).copy()
+        self.V = np.ascontiguousarray(scene.V, np.float64).copy()
+        self.F = np.ascontiguousarray(np.swapaxes(scene.F, 1, 2).reshape(-1, d * d), np.float64)
+        self.B = np.ascontiguousarray(np.swapaxes(scene.B, 1, 2).reshape(-1, d * d), np.float64)
+        self.mass = np.ascontiguousarray(scene.mass, np.float64)
+        self.vol = np.ascontiguousarray(scene.volume, np.float64)
+        self.mu = np.ascontiguousarray(scene.mu, np.float64)
+        self.lam = np.ascontiguousarray(scene.lam, np.float64)
+        self.valid = np.ones(scene.n, np.uint8)
+        self.time = 0.0
+
+    def F_rowmajor(self):
+        d = self.scene.dim
+        return np.swapaxes(self.F.reshape(-1, d, d), 1, 2)
+
+    def B_rowmajor(self):
+        d = self.scene.dim
+        return np.swapaxes(self.B.reshape(-1, d, d), 1, 2)
+
+
+def substep(state: State, want_grid: bool = False):
+    s = state.scene
+    L = lib()
+    sc = _scene_struct(s)
+    gn = int(np.prod([c + 6 for c in s.counts[:s.dim]]))
+    grids = None
+    args = [None] * 4
+    if want_grid:
+        grids = [np.zeros(gn), np.zeros(gn * s.dim), np.zeros(gn * s.dim), np.zeros(gn * s.dim)]
+        args = [_ptr(g) for g in grids]
+    rc = L.oracle_substep(ctypes.byref(sc), s.n, _ptr(state.X), _ptr(state.V), _ptr(state.F), _ptr(state.B),
+                          _ptr(state.mass), _ptr(state.vol), _ptr(state.mu), _ptr(state.lam),
+                          state.valid.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), s.dt, state.time, *args)
+    if rc:
+        raise RuntimeError("oracle_substep failed: %d" % rc)
+    state.time += s.dt
+    if want_grid:
+        shape = tuple(c + 6 for c in s.counts[:s.dim])
+        return {"grid_m": grids[0].reshape(shape), "grid_v0": grids[1].reshape(shape + (s.dim,)),
+                "grid_v": grids[2].reshape(shape + (s.dim,)), "grid_vf": grids[3].reshape(shape + (s.dim,))}
+    return None
+
+
+def run(state: State, nsteps: int):
+    s = state.scene
+    sc = _scene_struct(s)
+    rc = lib().oracle_run(ctypes.byref(sc), s.n, _ptr(state.X), _ptr(state.V), _ptr(state.F), _ptr(state.B),
+                          _ptr(state.mass), _ptr(state.vol), _ptr(state.mu), _ptr(state.lam),
+                          state.valid.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), s.dt, state.time, nsteps)
+    if rc:
+        raise RuntimeError("oracle_run failed: %d" % rc)
+    state.time += nsteps * s.dt
+
+
+def pft(dim, model, F_colmajor, mu, lam):
+    out = np.zeros(dim * dim)
+    Fc = np.ascontiguousarray(F_colmajor, np.float64)
+    lib().oracle_pft(dim, model, _ptr(Fc), mu, lam, _ptr(out))
+    return out
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SCENE)
+
+
+def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timing: bool = False):
+    """Run the reference's own driver on ``scene``; return {step: dump} (and timing JSON if asked)."""
+    from physbam_b200 import scenes as S
+    tmp = tempfile.mkdtemp(prefix="mpmref_")
+    try:
+        sp, dp = os.path.join(tmp, "scene.bin"), os.path.join(tmp, "dump.bin")
+        S.write_scene(sp, scene, dumps)
+        cmd = [REF_SCENE, sp, dp, "-threads", str(threads)]
+        if use_float:
+            cmd.append("-float")
+        if timing:
+            cmd.append("-time")
+        out = subprocess.run(cmd, check=True, capture_output=True, text=True)
+        res = S.read_dump(dp, scene.dim, scene.n, scene.counts) if dumps else {}
+        if timing:
+            import json
+            return res, json.loads(out.stdout.strip().splitlines()[-1])
+        return res
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)

@@ -1,0 +1,258 @@
+// Reference runner: drives the reference's own MPM_DRIVER / MPM_EXAMPLE on a
+// scene file written by physbam_b200/scenes.py, and dumps particle and grid
+// state after chosen substeps.  Test infrastructure only (it pins the CPU
+// restatement in oracle/ and produces the golden fixtures); the product never
+// links or runs it.  Built by oracle/ref.mk against the reference's sources.
+//
+//   ref_scene <scene.bin> <dump.bin> [-threads T] [-float] [-time]
+//
+// The scene is set up through the reference's public API exactly as
+// Projects/mpm/STANDARD_TESTS_BASE.cpp does it: quadratic weights
+// (MPM_EXAMPLE.cpp:197-205), MPM_FINITE_ELEMENTS + COROTATED_FIXED or
+// NEO_HOOKEAN with per-particle Lame arrays (STANDARD_TESTS_BASE.cpp:372-392),
+// MPM_GRAVITY (l.354-358), collision objects through Add_Collision_Object,
+// symplectic Euler, APIC (use_affine), flip=0, fixed dt.
+#include <Core/Log/LOG.h>
+#include <Core/Math_Tools/RANGE.h>
+#include <Core/Matrices/MATRIX.h>
+#include <Core/Vectors/VECTOR.h>
+#include <Geometry/Basic_Geometry/PLANE.h>
+#include <Geometry/Implicit_Objects/ANALYTIC_IMPLICIT_OBJECT.h>
+#include <Deformables/Constitutive_Models/COROTATED_FIXED.h>
+#include <Deformables/Constitutive_Models/NEO_HOOKEAN.h>
+#include <Hybrid_Methods/Examples_And_Drivers/MPM_DRIVER.h>
+#include <Hybrid_Methods/Examples_And_Drivers/MPM_EXAMPLE.h>
+#include <Hybrid_Methods/Examples_And_Drivers/MPM_PARTICLES.h>
+#include <Hybrid_Methods/Forces/MPM_FINITE_ELEMENTS.h>
+#include <Hybrid_Methods/Forces/MPM_GRAVITY.h>
+#include <Hybrid_Methods/Forces/MPM_FORCE_HELPER.h>
+#include <Hybrid_Methods/Iterators/GATHER_SCATTER.h>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#ifdef USE_OPENMP
+#include <omp.h>
+#endif
+using namespace PhysBAM;
+
+namespace {
+struct OBJ { int kind, type; double friction, a[3], b[3]; };
+struct SCENE_FILE
+{
+    int dim, counts[3], model, nsteps, nobj, ndump;
+    double dmin[3], dmax[3], gravity[3], dt, t0;
+    std::vector<int> dumps;
+    std::vector<OBJ> objs;
+    long long n;
+    std::vector<double> X, V, F, B, mass, volume, mu, lambda;
+};
+
+template<class T> void rd(FILE* f, T* p, size_t n)
+{
+    if(fread(p, sizeof(T), n, f) != n) throw std::runtime_error("short scene file");
+}
+
+SCENE_FILE Read_Scene(const char* path)
+{
+    FILE* f = fopen(path, "rb");
+    if(!f) throw std::runtime_error("cannot open scene");
+    char magic[8];
+    rd(f, magic, 8);
+    if(memcmp(magic, "MPMSCN01", 8)) throw std::runtime_error("bad scene magic");
+    SCENE_FILE s;
+    int hdr[9];
+    rd(f, hdr, 9);
+    s.dim = hdr[0]; s.counts[0] = hdr[1]; s.counts[1] = hdr[2]; s.counts[2] = hdr[3];
+    s.model = hdr[4]; s.nsteps = hdr[5]; s.nobj = hdr[6]; s.ndump = hdr[7];
+    double dh[11];
+    rd(f, dh, 11);
+    for(int i = 0; i < 3; i++) { s.dmin[i] = dh[i]; s.dmax[i] = dh[3 + i]; s.gravity[i] = dh[6 + i]; }
+    s.dt = dh[9]; s.t0 = dh[10];
+    s.dumps.resize(s.ndump);
+    if(s.ndump) rd(f, s.dumps.data(), s.ndump);
+    for(int i = 0; i < s.nobj; i++) {
+        OBJ o;
+        rd(f, &o.kind, 1); rd(f, &o.type, 1); rd(f, &o.friction, 1); rd(f, o.a, 3); rd(f, o.b, 3);
+        s.objs.push_back(o);
+    }
+    rd(f, &s.n, 1);
+    size_t n = s.n, d = s.dim;
+    s.X.resize(n * d); s.V.resize(n * d); s.F.resize(n * d * d); s.B.resize(n * d * d);
+    s.mass.resize(n); s.volume.resize(n); s.mu.resize(n); s.lambda.resize(n);
+    rd(f, s.X.data(), n * d); rd(f, s.V.data(), n * d);
+    rd(f, s.F.data(), n * d * d); rd(f, s.B.data(), n * d * d);
+    rd(f, s.mass.data(), n); rd(f, s.volume.data(), n); rd(f, s.mu.data(), n); rd(f, s.lambda.data(), n);
+    fclose(f);
+    return s;
+}
+
+template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
+{
+    typedef typename TV::SCALAR T;
+    typedef VECTOR<int, TV::m> TV_INT;
+    typedef MPM_EXAMPLE<TV> BASE;
+    typedef typename BASE::COLLISION_TYPE COLLISION_TYPE;
+    using BASE::grid; using BASE::particles; using BASE::gather_scatter; using BASE::force_helper;
+    const SCENE_FILE& s;
+
+    FILE_SCENE(const SCENE_FILE& s_, int threads)
+        : BASE(STREAM_TYPE(T())), s(s_)
+    {
+        this->threads = threads;
+        gather_scatter.threads = threads;
+        this->use_symplectic_euler = true;
+        this->use_affine = true;
+        this->flip = 0;
+        this->min_dt = this->max_dt = (T)s.dt;
+        particles.Store_B(true);
+    }
+
+    void Initialize() override
+    {
+        const int d = TV::m;
+        TV_INT counts; TV lo, hi;
+        for(int a = 0; a < d; a++) { counts(a) = s.counts[a]; lo(a) = (T)s.dmin[a]; hi(a) = (T)s.dmax[a]; }
+        grid.Initialize(counts, RANGE<TV>(lo, hi), true);
+        this->Set_Weights(2);
+        particles.Store_Lame(true);
+        particles.Add_Elements((int)s.n);
+        for(int p = 0; p < s.n; p++) {
+            for(int a = 0; a < d; a++) {
+                particles.X(p)(a) = (T)s.X[p * d + a];
+                particles.V(p)(a) = (T)s.V[p * d + a];
+            }
+            for(int k = 0; k < d * d; k++) {
+                particles.F(p).x[k] = (T)s.F[p * d * d + k];
+                particles.B(p).x[k] = (T)s.B[p * d * d + k];
+            }
+            particles.mass(p) = (T)s.mass[p];
+            particles.volume(p) = (T)s.volume[p];
+            particles.mu(p) = (T)s.mu[p];
+            particles.lambda(p) = (T)s.lambda[p];
+            particles.valid(p) = true;
+        }
+        ISOTROPIC_CONSTITUTIVE_MODEL<T, TV::m>* model;
+        if(s.model == 0) model = new COROTATED_FIXED<T, TV::m>((T)1, (T).3);
+        else model = new NEO_HOOKEAN<T, TV::m>((T)1, (T).3);
+        this->Add_Force(*new MPM_FINITE_ELEMENTS<TV>(force_helper, *model, gather_scatter, 0));
+        TV g;
+        for(int a = 0; a < d; a++) g(a) = (T)s.gravity[a];
+        this->Add_Force(*new MPM_GRAVITY<TV>(force_helper, g, gather_scatter, 0));
+        for(const OBJ& o: s.objs) {
+            COLLISION_TYPE type = o.type == 0 ? COLLISION_TYPE::stick : o.type == 1 ? COLLISION_TYPE::slip : COLLISION_TYPE::separate;
+            TV a, b;
+            for(int k = 0; k < d; k++) { a(k) = (T)o.a[k]; b(k) = (T)o.b[k]; }
+            if(o.kind == 0) this->Add_Collision_Object(RANGE<TV>(a, b), type, (T)o.friction);
+            else Add_Plane(a, b, type, (T)o.friction);
+        }
+    }
+
+    void Add_Plane(const VECTOR<T, 3>& n, const VECTOR<T, 3>& x0, COLLISION_TYPE type, T friction)
+    {this->Add_Collision_Object(PLANE<T>(n, x0), type, friction);}
+    void Add_Plane(const VECTOR<T, 2>&, const VECTOR<T, 2>&, COLLISION_TYPE, T)
+    {throw std::runtime_error("plane objects are only wired for 3D in the runner");}
+};
+
+template<class T> void wr(FILE* f, const T* p, size_t n) { fwrite(p, sizeof(T), n, f); }
+
+template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threads, bool report_time)
+{
+    typedef typename TV::SCALAR T;
+    typedef VECTOR<int, TV::m> TV_INT;
+    const int d = TV::m;
+    FILE_SCENE<TV> example(s, threads);
+    char tmpl[] = "/tmp/ref_scene_XXXXXX";
+    std::string outdir = mkdtemp(tmpl);
+    example.viewer_dir.output_directory = outdir;
+    MPM_DRIVER<TV> driver(example);
+    driver.Initialize();
+
+    std::vector<double> gm, gv0, gv, gvf;
+    int current = -1;
+    auto want = [&](int step){for(int x: s.dumps) if(x == step) return true; return false;};
+    auto grab = [&](const ARRAY<TV, TV_INT>& u, std::vector<double>& out)
+    {
+        out.resize((size_t)u.array.m * d);
+        for(int i = 0; i < u.array.m; i++) for(int a = 0; a < d; a++) out[(size_t)i * d + a] = u.array(i)(a);
+    };
+    example.Add_Callbacks(false, "p2g", [&]()
+    {
+        if(!want(current)) return;
+        gm.resize(example.mass.array.m);
+        for(int i = 0; i < example.mass.array.m; i++) gm[i] = example.mass.array(i);
+        grab(example.velocity, gv0);
+    });
+    example.Add_Callbacks(false, "forces", [&]()
+    {
+        if(!want(current)) return;
+        grab(example.velocity, gv);
+        grab(example.velocity_friction_save, gvf);
+    });
+
+    FILE* f = fopen(dump_path, "wb");
+    if(!f) { fprintf(stderr, "cannot open dump\n"); return 1; }
+    double total = 0;
+    for(int step = 0; step < s.nsteps; step++) {
+        current = step;
+        example.dt = (T)s.dt;
+        auto t0 = std::chrono::steady_clock::now();
+        driver.Advance_One_Time_Step();
+        auto t1 = std::chrono::steady_clock::now();
+        total += std::chrono::duration<double>(t1 - t0).count();
+        example.time += example.dt;
+        if(!want(step)) continue;
+        wr(f, &step, 1);
+        std::vector<double> buf;
+        size_t n = s.n;
+        buf.resize(n * d);
+        for(size_t p = 0; p < n; p++) for(int a = 0; a < d; a++) buf[p * d + a] = example.particles.X(p)(a);
+        wr(f, buf.data(), buf.size());
+        for(size_t p = 0; p < n; p++) for(int a = 0; a < d; a++) buf[p * d + a] = example.particles.V(p)(a);
+        wr(f, buf.data(), buf.size());
+        buf.resize(n * d * d);
+        for(size_t p = 0; p < n; p++) for(int k = 0; k < d * d; k++) buf[p * d * d + k] = example.particles.F(p).x[k];
+        wr(f, buf.data(), buf.size());
+        for(size_t p = 0; p < n; p++) for(int k = 0; k < d * d; k++) buf[p * d * d + k] = example.particles.B(p).x[k];
+        wr(f, buf.data(), buf.size());
+        std::vector<unsigned char> valid(n);
+        for(size_t p = 0; p < n; p++) valid[p] = example.particles.valid(p) ? 1 : 0;
+        wr(f, valid.data(), n);
+        wr(f, gm.data(), gm.size());
+        wr(f, gv0.data(), gv0.size());
+        wr(f, gv.data(), gv.size());
+        wr(f, gvf.data(), gvf.size());
+    }
+    fclose(f);
+    if(report_time)
+        printf("{\"substeps\": %d, \"particles\": %lld, \"seconds\": %.9g, \"threads\": %d}\n",
+            s.nsteps, s.n, total, threads);
+    std::string cmd = "rm -rf '" + outdir + "'";
+    if(system(cmd.c_str())) {}
+    return 0;
+}
+}
+
+int main(int argc, char* argv[])
+{
+    if(argc < 3) { fprintf(stderr, "usage: ref_scene scene.bin dump.bin [-threads T] [-float] [-time]\n"); return 2; }
+    int threads = 1;
+    bool use_float = false, report_time = false;
+    for(int i = 3; i < argc; i++) {
+        if(!strcmp(argv[i], "-threads") && i + 1 < argc) threads = atoi(argv[++i]);
+        else if(!strcmp(argv[i], "-float")) use_float = true;
+        else if(!strcmp(argv[i], "-time")) report_time = true;
+    }
+#ifdef USE_OPENMP
+    omp_set_num_threads(threads);
+#endif
+    LOG::Initialize_Logging(true, true, 0, false);
+    SCENE_FILE s = Read_Scene(argv[1]);
+    int rc;
+    if(use_float) rc = s.dim == 2 ? Run<VECTOR<float, 2> >(s, argv[2], threads, report_time) : Run<VECTOR<float, 3> >(s, argv[2], threads, report_time);
+    else rc = s.dim == 2 ? Run<VECTOR<double, 2> >(s, argv[2], threads, report_time) : Run<VECTOR<double, 3> >(s, argv[2], threads, report_time);
+    LOG::Finish_Logging();
+    return rc;
+}

@@ -1,0 +1,374 @@
+"""Seeded synthetic MPM scenes and the binary scene-file format.
+
+The reference has no public dataset for its MPM path: scenes are built in C++
+by `Projects/mpm/STANDARD_TESTS_BASE.cpp` (seeding, Lame parameters l.567-586,
+walls l.487-511).  This module builds the benchmark scenes the same way, from
+one numpy seed, so the CUDA path, the CPU oracle and the reference's own
+driver all start from bit-identical particle arrays:
+
+* particles are seeded ``ppc`` per cell, each uniform in its cell, and kept
+  when inside the body (box or sphere);
+* ``volume = dx^d / ppc``, ``mass = density * volume``, ``F = I``, ``B = 0``;
+* ``mu = E / (2 (1 + nu))``, ``lambda = E nu / ((1 + nu)(1 - 2 nu))`` per
+  particle, as `STANDARD_TESTS_BASE::Set_Lame_On_Particles` computes them;
+* walls are RANGE boxes over the domain thickened by ``dx (2 ghost + 1)``,
+  cut at ``inset`` from one face, as `STANDARD_TESTS_BASE::Add_Walls` builds
+  them.
+
+Layout follows `MPM_PARTICLES` (`Hybrid_Methods/Examples_And_Drivers/
+MPM_PARTICLES.h:18-44`): ``X, V`` are (N, d); ``F, B`` are (N, d, d) stored
+column-major per particle, i.e. ``F[p].T`` in numpy row-major terms (the
+reference's ``MATRIX<T,3>`` keeps ``x[i + d*j]``, `Core/Matrices/MATRIX_3X3.h:115-119`).
+Arrays here are kept as plain (N, d, d) with ``F[p][i, j]`` = row i, col j;
+the writer transposes when it serialises.
+"""
+from __future__ import annotations
+
+import dataclasses
+import struct
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+COROTATED = 0
+NEO_HOOKEAN = 1
+
+STICK = 0
+SLIP = 1
+SEPARATE = 2
+
+BOX = 0
+PLANE = 1
+
+GHOST = 3
+
+
+@dataclasses.dataclass
+class CollisionObject:
+    """A static collision object (`Hybrid_Methods/Collisions/MPM_COLLISION_OBJECT.h:13-37`).
+
+    ``kind`` BOX: ``a`` = min corner, ``b`` = max corner (`Core/Math_Tools/RANGE.cpp:37-63`).
+    ``kind`` PLANE: ``a`` = unit normal, ``b`` = a point on the plane
+    (`Geometry/Basic_Geometry/PLANE.h:52-63`); inside is behind the normal.
+    """
+    kind: int
+    type: int
+    friction: float
+    a: Sequence[float]
+    b: Sequence[float]
+
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    dim: int
+    counts: Sequence[int]
+    domain_min: Sequence[float]
+    domain_max: Sequence[float]
+    model: int
+    gravity: Sequence[float]
+    dt: float
+    nsteps: int
+    objects: List[CollisionObject]
+    X: np.ndarray
+    V: np.ndarray
+    F: np.ndarray
+    B: np.ndarray
+    mass: np.ndarray
+    volume: np.ndarray
+    mu: np.ndarray
+    lam: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return int(self.X.shape[0])
+
+    @property
+    def dx(self) -> float:
+        return float((self.domain_max[0] - self.domain_min[0]) / self.counts[0])
+
+    def copy(self) -> "Scene":
+        return dataclasses.replace(
+            self, X=self.X.copy(), V=self.V.copy(), F=self.F.copy(), B=self.B.copy(),
+            mass=self.mass.copy(), volume=self.volume.copy(), mu=self.mu.copy(), lam=self.lam.copy(),
+            objects=list(self.objects))
+
+    def subset(self, idx) -> "Scene":
+        return dataclasses.replace(
+            self, X=self.X[idx].copy(), V=self.V[idx].copy(), F=self.F[idx].copy(),
+            B=self.B[idx].copy(), mass=self.mass[idx].copy(), volume=self.volume[idx].copy(),
+            mu=self.mu[idx].copy(), lam=self.lam[idx].copy(), objects=list(self.objects))
+
+
+def lame(E, nu):
+    """`STANDARD_TESTS_BASE::Set_Lame_On_Particles` (Projects/mpm/STANDARD_TESTS_BASE.cpp:567-586)."""
+    E = np.asarray(E, dtype=np.float64)
+    nu = np.asarray(nu, dtype=np.float64)
+    mu = E / (2 * (1 + nu))
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    return mu, lam
+
+
+def walls(dim, counts, dmin, dmax, flags, type_, friction, inset):
+    """RANGE walls as `STANDARD_TESTS_BASE::Add_Walls` builds them (STANDARD_TESTS_BASE.cpp:487-511).
+
+    Bit ``2a+s`` of ``flags`` selects one wall; the reference puts bit ``2a+1``
+    on the LOW side of axis ``a`` and bit ``2a`` on the high side.
+    """
+    dx = (np.asarray(dmax, float) - np.asarray(dmin, float)) / np.asarray(counts, float)
+    lo = np.asarray(dmin, float) - dx * (GHOST * 2 + 1)
+    hi = np.asarray(dmax, float) + dx * (GHOST * 2 + 1)
+    out = []
+    for a in range(dim):
+        for s in range(2):
+            if flags & (1 << (a * 2 + s)):
+                wlo, whi = lo.copy(), hi.copy()
+                if s:
+                    whi[a] = dmin[a] + inset
+                else:
+                    wlo[a] = dmax[a] - inset
+                out.append(CollisionObject(BOX, type_, friction, wlo.tolist(), whi.tolist()))
+    return out
+
+
+def _seed_cells(rng, dim, counts, dmin, dx, lo, hi, ppc, inside):
+    """Jitter ``ppc`` particles uniformly in every cell overlapping [lo, hi]; keep those ``inside``."""
+    c0 = np.maximum(np.floor((np.asarray(lo) - dmin) / dx).astype(np.int64), 0)
+    c1 = np.minimum(np.ceil((np.asarray(hi) - dmin) / dx).astype(np.int64), np.asarray(counts))
+    axes = [np.arange(c0[a], c1[a]) for a in range(dim)]
+    cells = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, dim)
+    n = cells.shape[0] * ppc
+    jitter = rng.random((n, dim))
+    X = dmin + (np.repeat(cells, ppc, axis=0) + jitter) * dx
+    return X[inside(X)]
+
+
+def _finish(name, dim, counts, dmin, dmax, model, gravity, dt, nsteps, objects, X, V, E, nu, density, ppc):
+    dx = (dmax[0] - dmin[0]) / counts[0]
+    n = X.shape[0]
+    vol = np.full(n, dx ** dim / ppc)
+    mass = density * vol
+    mu, lam = lame(np.broadcast_to(E, (n,)), np.broadcast_to(nu, (n,)))
+    F = np.broadcast_to(np.eye(dim), (n, dim, dim)).copy()
+    B = np.zeros((n, dim, dim))
+    return Scene(name, dim, list(counts), list(map(float, dmin)), list(map(float, dmax)), model,
+                 list(map(float, gravity)), float(dt), int(nsteps), objects,
+                 np.ascontiguousarray(X, dtype=np.float64), np.ascontiguousarray(V, dtype=np.float64),
+                 F, B, mass, vol, np.ascontiguousarray(mu), np.ascontiguousarray(lam))
+
+
+def block_2d(seed=1234, G=64, ppc=4, E=1e4, nu=0.3, density=1000.0, dt=1e-4, nsteps=100):
+    """2D elastic block: 0.25x0.25 centred (0.5, 0.6), sticky ground at y=0.05 (64^2, 4 ppc)."""
+    rng = np.random.default_rng(seed)
+    dim, counts = 2, [G, G]
+    dmin, dmax = np.zeros(2), np.ones(2)
+    dx = 1.0 / G
+    lo, hi = np.array([0.375, 0.475]), np.array([0.625, 0.725])
+    X = _seed_cells(rng, dim, counts, dmin, dx, lo, hi, ppc,
+                    lambda P: np.all((P >= lo) & (P < hi), axis=1))
+    V = np.zeros_like(X)
+    objects = walls(dim, counts, dmin, dmax, 1 << 3, STICK, 0.0, 0.05)
+    return _finish("block2d", dim, counts, dmin, dmax, COROTATED, [0, -9.8], dt, nsteps, objects,
+                   X, V, E, nu, density, ppc)
+
+
+def spheres_3d(seed=1234, G=128, ppc=8, E=5e4, nu=0.35, density=1000.0, dt=5e-5, nsteps=200,
+               radius=0.12, model=NEO_HOOKEAN):
+    """Two colliding spheres (r=0.12 at x=0.35/0.65, v=+-2 m/s), slip walls, NEO_HOOKEAN (128^3, 8 ppc)."""
+    rng = np.random.default_rng(seed)
+    dim, counts = 3, [G, G, G]
+    dmin, dmax = np.zeros(3), np.ones(3)
+    dx = 1.0 / G
+    Xs, Vs = [], []
+    for c, v in (((0.35, 0.5, 0.5), 2.0), ((0.65, 0.5, 0.5), -2.0)):
+        c = np.asarray(c)
+        X = _seed_cells(rng, dim, counts, dmin, dx, c - radius, c + radius, ppc,
+                        lambda P, c=c: np.sum((P - c) ** 2, axis=1) < radius * radius)
+        Xs.append(X)
+        V = np.zeros_like(X)
+        V[:, 0] = v
+        Vs.append(V)
+    X, V = np.concatenate(Xs), np.concatenate(Vs)
+    objects = walls(dim, counts, dmin, dmax, 63, SLIP, 0.0, 0.05)
+    return _finish("spheres3d", dim, counts, dmin, dmax, model, [0, -9.8, 0], dt, nsteps, objects,
+                   X, V, E, nu, density, ppc)
+
+
+def dam_3d(seed=1234, G=256, ppc=8, E=2e5, nu=0.4, density=1000.0, dt=2e-5, nsteps=100, sigma=0.2):
+    """Dam-break block [0.05,0.45]x[0.05,0.8]x[0.05,0.95], E log-normal (sigma 0.2), sticky floor, slip walls."""
+    rng = np.random.default_rng(seed)
+    dim, counts = 3, [G, G, G]
+    dmin, dmax = np.zeros(3), np.ones(3)
+    dx = 1.0 / G
+    lo, hi = np.array([0.05, 0.05, 0.05]), np.array([0.45, 0.8, 0.95])
+    X = _seed_cells(rng, dim, counts, dmin, dx, lo, hi, ppc,
+                    lambda P: np.all((P >= lo) & (P < hi), axis=1))
+    Ep = E * np.exp(sigma * rng.standard_normal(X.shape[0]))
+    V = np.zeros_like(X)
+    objects = walls(dim, counts, dmin, dmax, 1 << 3, STICK, 0.0, 0.05)
+    objects += walls(dim, counts, dmin, dmax, 63 & ~(1 << 3), SLIP, 0.0, 0.05)
+    return _finish("dam3d", dim, counts, dmin, dmax, COROTATED, [0, -9.8, 0], dt, nsteps, objects,
+                   X, V, Ep, nu, density, ppc)
+
+
+def cube_3d(seed=1234, G=64, ppc=8, side=0.3, nu=0.3, density=1000.0, dt=1e-4, nsteps=64,
+            v0=(1.0, 0.5, 0.0), E_range=(5e3, 5e4), model=COROTATED):
+    """Differentiable cube: side 0.3 centred (0.5,0.5,0.5), E log-uniform, v0 = (1, .5, 0) (64^3, 8 ppc).
+
+    Also returns the seeded target point in [0.3, 0.7]^3 as ``scene.target``.
+    """
+    rng = np.random.default_rng(seed)
+    dim, counts = 3, [G, G, G]
+    dmin, dmax = np.zeros(3), np.ones(3)
+    dx = 1.0 / G
+    c = np.array([0.5, 0.5, 0.5])
+    lo, hi = c - side / 2, c + side / 2
+    X = _seed_cells(rng, dim, counts, dmin, dx, lo, hi, ppc,
+                    lambda P: np.all((P >= lo) & (P < hi), axis=1))
+    Ep = np.exp(rng.uniform(np.log(E_range[0]), np.log(E_range[1]), X.shape[0]))
+    V = np.broadcast_to(np.asarray(v0, float), X.shape).copy()
+    s = _finish("cube3d", dim, counts, dmin, dmax, model, [0, -9.8, 0], dt, nsteps, [],
+                X, V, Ep, nu, density, ppc)
+    s.target = rng.uniform(0.3, 0.7, 3)
+    return s
+
+
+def batch_scenes(seed=1234, count=256, ppc_range=(4, 8), nsteps=100, dt=1e-4):
+    """Independent boxes: grid side from {32,48,64,96}, box side U[0.1,0.4], |v|<=2, per-scene model."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(count):
+        G = int(rng.choice([32, 48, 64, 96]))
+        ppc = int(rng.integers(ppc_range[0], ppc_range[1] + 1))
+        size = rng.uniform(0.1, 0.4, 3)
+        lo = rng.uniform(0.1, 0.9 - size)
+        hi = lo + size
+        v = rng.normal(size=3)
+        v *= rng.uniform(0, 2.0) / max(np.linalg.norm(v), 1e-12)
+        E = float(np.exp(rng.uniform(np.log(1e3), np.log(1e5))))
+        nu = float(rng.uniform(0.2, 0.45))
+        model = int(rng.integers(0, 2))
+        srng = np.random.default_rng([seed, s])
+        dmin = np.zeros(3)
+        X = _seed_cells(srng, 3, [G] * 3, dmin, 1.0 / G, lo, hi, ppc,
+                        lambda P, lo=lo, hi=hi: np.all((P >= lo) & (P < hi), axis=1))
+        V = np.broadcast_to(v, X.shape).copy()
+        out.append(_finish("batch%d" % s, 3, [G] * 3, dmin, np.ones(3), model, [0, -9.8, 0], dt, nsteps,
+                           [], X, V, E, nu, 1000.0, ppc))
+    return out
+
+
+def small_3d(seed=7, G=16, ppc=8, model=COROTATED, nsteps=20, dt=1e-4, E=(2e4, 8e4), nu=0.3,
+             v=(1.5, -0.5, 0.75), with_walls=True, friction=0.0):
+    """A small 3D scene for golden fixtures: a box with a rotating velocity field, walls, per-particle E."""
+    rng = np.random.default_rng(seed)
+    dim, counts = 3, [G, G, G]
+    dmin, dmax = np.zeros(3), np.ones(3)
+    dx = 1.0 / G
+    lo, hi = np.array([0.2, 0.12, 0.3]), np.array([0.6, 0.5, 0.7])
+    X = _seed_cells(rng, dim, counts, dmin, dx, lo, hi, ppc,
+                    lambda P: np.all((P >= lo) & (P < hi), axis=1))
+    Ep = np.exp(rng.uniform(np.log(E[0]), np.log(E[1]), X.shape[0]))
+    c = (lo + hi) / 2
+    V = np.asarray(v, float) + 4.0 * np.cross(np.array([0.3, 1.0, -0.2]), X - c)
+    objects = []
+    if with_walls:
+        objects = walls(dim, counts, dmin, dmax, 1 << 3, STICK, 0.0, 0.15)
+        objects += walls(dim, counts, dmin, dmax, 63 & ~(1 << 3), SLIP, friction, 0.2)
+    s = _finish("small3d", dim, counts, dmin, dmax, model, [0, -9.8, 0], dt, nsteps, objects,
+                X, V, Ep, nu, 1000.0, ppc)
+    # start from a deformed, slightly sheared state so the stress is non-trivial on step 0
+    A = np.eye(3) + 0.08 * rng.standard_normal((3, 3))
+    s.F = np.broadcast_to(A, s.F.shape).copy()
+    s.B = 0.5 * rng.standard_normal(s.B.shape) * dx
+    return s
+
+
+def small_2d(seed=11, G=16, ppc=4, model=COROTATED, nsteps=20, dt=1e-4, friction=0.3):
+    """A small 2D scene for golden fixtures: block falling onto a sticky floor with slip side walls."""
+    rng = np.random.default_rng(seed)
+    dim, counts = 2, [G, G]
+    dmin, dmax = np.zeros(2), np.ones(2)
+    dx = 1.0 / G
+    lo, hi = np.array([0.25, 0.2]), np.array([0.7, 0.55])
+    X = _seed_cells(rng, dim, counts, dmin, dx, lo, hi, ppc,
+                    lambda P: np.all((P >= lo) & (P < hi), axis=1))
+    Ep = np.exp(rng.uniform(np.log(1e4), np.log(5e4), X.shape[0]))
+    V = np.column_stack([np.full(X.shape[0], 1.0), -2.0 + 3.0 * (X[:, 0] - 0.5)])
+    objects = walls(dim, counts, dmin, dmax, 1 << 3, STICK, 0.0, 0.2)
+    objects += walls(dim, counts, dmin, dmax, 3, SLIP, friction, 0.2)
+    s = _finish("small2d", dim, counts, dmin, dmax, model, [0, -9.8], dt, nsteps, objects,
+                X, V, Ep, 0.3, 1000.0, ppc)
+    A = np.eye(2) + 0.1 * rng.standard_normal((2, 2))
+    s.F = np.broadcast_to(A, s.F.shape).copy()
+    s.B = 0.5 * rng.standard_normal(s.B.shape) * dx
+    return s
+
+
+# --------------------------------------------------------------------------------------------
+# Scene file: read by the reference runner (oracle/ref_scene.cpp) and by the C oracle harness.
+# --------------------------------------------------------------------------------------------
+MAGIC = b"MPMSCN01"
+
+
+def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
+    dumps = list(dumps if dumps is not None else [s.nsteps - 1])
+    d = s.dim
+    pad3 = lambda v: list(v) + [0.0] * (3 - len(v))
+    with open(path, "wb") as f:
+        f.write(MAGIC)
+        counts = list(s.counts) + [1] * (3 - d)
+        f.write(struct.pack("<9i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), 0))
+        f.write(struct.pack("<11d", *pad3(s.domain_min), *pad3(s.domain_max), *pad3(s.gravity), s.dt, 0.0))
+        f.write(struct.pack("<%di" % len(dumps), *dumps))
+        for o in s.objects:
+            f.write(struct.pack("<2i7d", o.kind, o.type, o.friction, *pad3(o.a), *pad3(o.b)))
+        f.write(struct.pack("<q", s.n))
+        f.write(np.ascontiguousarray(s.X, np.float64).tobytes())
+        f.write(np.ascontiguousarray(s.V, np.float64).tobytes())
+        # column-major per particle, as MATRIX<T,d> stores it
+        f.write(np.ascontiguousarray(np.swapaxes(s.F, 1, 2), np.float64).tobytes())
+        f.write(np.ascontiguousarray(np.swapaxes(s.B, 1, 2), np.float64).tobytes())
+        for a in (s.mass, s.volume, s.mu, s.lam):
+            f.write(np.ascontiguousarray(a, np.float64).tobytes())
+
+
+def read_dump(path, dim, n, counts):
+    """Read the per-substep dumps written by the reference runner / C oracle.
+
+    Record: int32 step; X (n,d); V (n,d); F (n,d,d col-major); B (same); valid u8[n];
+    grid mass after P2G; grid velocity after P2G (``v = mv/m``, d per node); grid
+    velocity after forces; grid friction velocity after forces.  Grids cover the ghosted domain
+    (G+6)^d, last index fastest (`Core/Math_Tools/RANGE_ITERATOR.h`).
+    """
+    gshape = tuple(c + 2 * GHOST for c in counts[:dim])
+    gn = int(np.prod(gshape))
+    out = {}
+    with open(path, "rb") as f:
+        while True:
+            hdr = f.read(4)
+            if len(hdr) < 4:
+                break
+            step = struct.unpack("<i", hdr)[0]
+            rec = {}
+            rec["X"] = np.frombuffer(f.read(8 * n * dim), np.float64).reshape(n, dim)
+            rec["V"] = np.frombuffer(f.read(8 * n * dim), np.float64).reshape(n, dim)
+            rec["F"] = np.swapaxes(np.frombuffer(f.read(8 * n * dim * dim), np.float64).reshape(n, dim, dim), 1, 2)
+            rec["B"] = np.swapaxes(np.frombuffer(f.read(8 * n * dim * dim), np.float64).reshape(n, dim, dim), 1, 2)
+            rec["valid"] = np.frombuffer(f.read(n), np.uint8).astype(bool)
+            rec["grid_m"] = np.frombuffer(f.read(8 * gn), np.float64).reshape(gshape)
+            rec["grid_v0"] = np.frombuffer(f.read(8 * gn * dim), np.float64).reshape(gshape + (dim,))
+            rec["grid_v"] = np.frombuffer(f.read(8 * gn * dim), np.float64).reshape(gshape + (dim,))
+            rec["grid_vf"] = np.frombuffer(f.read(8 * gn * dim), np.float64).reshape(gshape + (dim,))
+            out[step] = rec
+    return out
+
+
+CONFIGS = {
+    "block2d": block_2d,
+    "spheres3d": spheres_3d,
+    "dam3d": dam_3d,
+    "cube3d": cube_3d,
+    "small3d": small_3d,
+    "small2d": small_2d,
+}

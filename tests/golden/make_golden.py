@@ -1,0 +1,87 @@
+"""Generate the golden fixtures in this folder from the reference itself.
+
+Runs the reference's own MPM_DRIVER (compiled from its sources by
+``oracle/ref.mk``, driven by ``oracle/ref_scene.cpp``) in FP64 on small seeded
+scenes and freezes inputs plus dumps into ``<name>.npz``.  Needs the reference
+tree, so it runs only where that is present; the fixtures are committed so the
+tests never need it.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from physbam_b200 import scenes as S  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+CASES = {
+    # name: (scene factory, dumps, steps whose grids are kept)
+    "small2d_corotated": (lambda: S.small_2d(), [0, 1, 19], [0, 19]),
+    "small2d_neohookean": (lambda: S.small_2d(model=S.NEO_HOOKEAN, seed=5), [0, 19], [0]),
+    "small3d_corotated": (lambda: S.small_3d(), [0, 1, 19], [0, 19]),
+    "small3d_neohookean_friction": (lambda: S.small_3d(model=S.NEO_HOOKEAN, seed=9, friction=0.4), [0, 19], [0]),
+    # BASELINE 2D case, exactly: 64^2, block 0.25^2 at (0.5,0.6), 4 ppc, corotated, sticky ground, 100 substeps
+    "block2d_cfg": (lambda: S.block_2d(), [0, 9, 99], [0, 99]),
+}
+
+
+def main():
+    oracle.build()
+    if not oracle.ref_available():
+        oracle.build_ref()
+    for name, (make, dumps, grid_steps) in CASES.items():
+        scene = make()
+        ref = oracle.run_reference(scene, dumps, threads=1)
+        arrays = dict(
+            dim=scene.dim, counts=np.array(scene.counts), dmin=np.array(scene.domain_min),
+            dmax=np.array(scene.domain_max), model=scene.model, gravity=np.array(scene.gravity),
+            dt=scene.dt, nsteps=scene.nsteps,
+            obj_kind=np.array([o.kind for o in scene.objects], np.int32),
+            obj_type=np.array([o.type for o in scene.objects], np.int32),
+            obj_friction=np.array([o.friction for o in scene.objects]),
+            obj_a=np.array([o.a for o in scene.objects]).reshape(-1, scene.dim),
+            obj_b=np.array([o.b for o in scene.objects]).reshape(-1, scene.dim),
+            X=scene.X, V=scene.V, F=scene.F, B=scene.B, mass=scene.mass, volume=scene.volume,
+            mu=scene.mu, lam=scene.lam, dumps=np.array(dumps))
+        for step in dumps:
+            r = ref[step]
+            for k in ("X", "V", "F", "B", "valid"):
+                arrays["s%d_%s" % (step, k)] = r[k]
+            if step in grid_steps:
+                for k in ("grid_m", "grid_v0", "grid_v", "grid_vf"):
+                    arrays["s%d_%s" % (step, k)] = r[k]
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+        print(name, scene.n, "particles", os.path.getsize(os.path.join(OUT, name + ".npz")), "bytes")
+
+
+def load(name):
+    """Load a fixture back into a Scene plus its reference dumps {step: {key: array}}."""
+    z = np.load(os.path.join(OUT, name + ".npz"))
+    dim = int(z["dim"])
+    objs = [S.CollisionObject(int(k), int(t), float(f), list(a), list(b))
+            for k, t, f, a, b in zip(z["obj_kind"], z["obj_type"], z["obj_friction"], z["obj_a"], z["obj_b"])]
+    scene = S.Scene(name, dim, [int(c) for c in z["counts"]], list(z["dmin"]), list(z["dmax"]), int(z["model"]),
+                    list(z["gravity"]), float(z["dt"]), int(z["nsteps"]), objs,
+                    z["X"].copy(), z["V"].copy(), z["F"].copy(), z["B"].copy(), z["mass"].copy(),
+                    z["volume"].copy(), z["mu"].copy(), z["lam"].copy())
+    dumps = {}
+    for step in z["dumps"]:
+        step = int(step)
+        rec = {}
+        for k in ("X", "V", "F", "B", "valid", "grid_m", "grid_v0", "grid_v", "grid_vf"):
+            key = "s%d_%s" % (step, k)
+            if key in z:
+                rec[k] = z[key]
+        dumps[step] = rec
+    return scene, dumps
+
+
+if __name__ == "__main__":
+    main()
