@@ -1,0 +1,342 @@
+"""Benchmark of the explicit MPM substep on B200 (particle-substeps/s).
+
+Workload: the BASELINE 3D case -- two NEO_HOOKEAN spheres (r = 0.12, +-2 m/s)
+on a 128^3 grid, 8 particles per cell (242,664 particles), slip walls,
+gravity, dt = 5e-5.  One step = one substep over the whole scene.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Timing: W untimed substeps, then K substeps each timed with CUDA events on the
+library's stream, the L2 flushed (a 512 MB write) before every timed substep;
+value = particles * K / (sum of substep times), max over ranks.  `e2e` goes
+through the public C ABI with host buffers: per step, upload of the scene from
+pinned host memory, the scene's full run of substeps (CUDA-graph replay),
+download of the particle state.  `--impl reference` times the reference's own
+CPU driver (compiled from its sources into oracle/_ref) on the host cores.
+Multi-GPU: independent replicas, one per rank (the substep does not shard).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-substeps/s"
+WORKLOAD = "spheres3d-128^3-neohookean-8ppc-fp32"
+ALG_BYTES = {"p2g": 112, "g2p": 144, "substep": 256}    # bytes per particle (FP32, 3D)
+GRID_BYTES_PER_NODE = 48                                # grid update: read 16, write 32
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            if len(s) >= 9:
+                for nm, v in zip(names, s[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_arm(args):
+    """Time the reference's own CPU driver (oracle/_ref, all host threads) on the workload."""
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    import oracle
+    from physbam_b200 import scenes as S
+    scene = S.spheres_3d()
+    cores = os.cpu_count() or 1
+    nsteps = args.warmup + args.steps
+    if oracle.ref_available():
+        s = scene.copy()
+        s.nsteps = nsteps
+        _, t = oracle.run_reference(s, [], threads=cores, timing=True)
+        secs = t["step_seconds"][args.warmup:]
+        kind = "reference"
+        sample = "full scene (%d particles), %d timed substeps after %d warm-up, PhysBAM MPM_DRIVER FP64, %d OpenMP threads" % (
+            scene.n, args.steps, args.warmup, cores)
+    else:
+        st = oracle.State(scene)
+        oracle.run(st, args.warmup)
+        t0 = time.perf_counter()
+        oracle.run(st, args.steps)
+        secs = [(time.perf_counter() - t0) / args.steps] * args.steps
+        kind, cores = "port", 1
+        sample = "full scene (%d particles), %d substeps, C restatement FP64, 1 thread" % (scene.n, args.steps)
+    total = float(sum(secs))
+    value = scene.n * args.steps / total
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded jittered-in-cell seeding, numpy PCG64 seed 1234)",
+            "config": {"workload": WORKLOAD, "particles": scene.n, "grid": "128^3", "dt": scene.dt},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_sample(scene, seconds_budget=20.0):
+    """Bounded CPU sample of the same workload (rank 0, N=1 only)."""
+    import oracle
+    cores = os.cpu_count() or 1
+    if oracle.ref_available():
+        s = scene.copy()
+        s.nsteps = 12
+        _, t = oracle.run_reference(s, [], threads=cores, timing=True)
+        secs = t["step_seconds"][2:]
+        return {"value": scene.n * len(secs) / sum(secs), "unit": METRIC, "cores": cores, "kind": "reference",
+                "sample": "full scene (%d particles), 10 substeps after 2 warm-up, PhysBAM MPM_DRIVER FP64, %d OpenMP threads"
+                          % (scene.n, cores)}
+    st = oracle.State(scene)
+    t0 = time.perf_counter()
+    oracle.run(st, 2)
+    dt = (time.perf_counter() - t0) / 2
+    return {"value": scene.n / dt, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": "full scene (%d particles), 2 substeps, C restatement FP64, 1 thread" % scene.n}
+
+
+def kernels_per_substep(scene):
+    """Our kernels launched per fast-path substep: 5 per radix digit pass
+    (histogram, 3-kernel scan, scatter) + ranges, tail, p2g, grid, g2p."""
+    blocks = 1
+    for c in scene.counts:
+        blocks *= (c + 4 + 3) // 4
+    bits = 6
+    while (1 << bits) <= blocks * 64:
+        bits += 1
+    return 5 * ((bits + 7) // 8) + 5
+
+
+def read_traffic(kernel):
+    """Per-launch DRAM traffic of `kernel` on this workload from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 4 and parts[0] == kernel and parts[1] == WORKLOAD:
+                return float(parts[2])
+    return None
+
+
+def our_arm(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from physbam_b200 import driver as D
+    from physbam_b200 import scenes as S
+
+    scene = S.spheres_3d()
+    n = scene.n
+    drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+    stream = torch.cuda.Stream()
+    drv.set_stream(stream.cuda_stream)
+    drv.set_scene_particles(scene)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # warm-up (also captures the two substep graphs)
+    drv.advance(max(args.warmup, 3))
+    drv.synchronize()
+
+    # per-kernel shares from an eager, event-timed pass (separate from the headline)
+    drv.set_timing(True)
+    for _ in range(4):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        drv.Advance_One_Time_Step()
+    drv.synchronize()
+    ktimes = drv.get_timing()
+    drv.set_timing(False)
+
+    # headline: K substeps, each a graph replay on the library stream, L2 flushed before each
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+                evs[k][0].record(stream)
+            drv.advance(1)
+            with torch.cuda.stream(stream):
+                evs[k][1].record(stream)
+        torch.cuda.synchronize()
+    drv.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    value = world * n * args.steps / (ms_max / 1e3)
+
+    # e2e through the public API with pinned host buffers
+    d = 3
+    pin = lambda shape: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+    hX, hV, hF, hB = pin((n, d)), pin((n, d)), pin((n, d, d)), pin((n, d, d))
+    hm, hvol, hmu, hla = pin(n), pin(n), pin(n), pin(n)
+    hX[:], hV[:], hF[:], hB[:] = scene.X, scene.V, scene.F, scene.B
+    hm[:], hvol[:], hmu[:], hla[:] = scene.mass, scene.volume, scene.mu, scene.lam
+    e2e_steps = max(1, min(args.steps, 3))
+    frame = scene.nsteps
+    h2d = n * 4 * (3 + 3 + 9 + 9 + 4)
+    d2h = n * (4 * (3 + 3 + 9 + 9) + 1)
+    e2e_drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+    e2e_drv.set_particles(hX, hV, hF, hB, hm, hvol, hmu, hla, dtype=np.float32)
+    e2e_drv.advance(2)
+    e2e_drv.get_particles(dtype=np.float32)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_drv.set_particles(hX, hV, hF, hB, hm, hvol, hmu, hla, dtype=np.float32)
+        e2e_drv.advance(frame)
+        out = e2e_drv.get_particles(dtype=np.float32)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * frame * e2e_steps / float(te.item())
+    e2e_drv.close()
+    assert out["valid"].sum() > 0
+
+    # roofline: the kernel with the largest share of device time
+    peak, peak_kind = measured_peaks()
+    shares = {k: v[0] for k, v in ktimes.items()}
+    total_k = sum(shares.values())
+    top = max(shares, key=shares.get)
+    per_launch_ms = ktimes[top][0] / max(ktimes[top][1], 1)
+    alg = {"fast_p2g": ALG_BYTES["p2g"] * n, "fast_g2p": ALG_BYTES["g2p"] * n}.get(top)
+    roof = None
+    if alg:
+        achieved = alg / (per_launch_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "kernel": top, "traffic": read_traffic(top),
+                "alg_bytes_per_launch": alg}
+    substep_ms = ms_max / args.steps
+    launches_per_step = kernels_per_substep(scene)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(scene)
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": substep_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded jittered-in-cell seeding, numpy PCG64 seed 1234)",
+            "config": {"workload": WORKLOAD, "particles": n, "grid": "128^3", "dt": scene.dt,
+                       "l2": "flushed before every timed substep (512 MB write)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "step": "upload + %d substeps (CUDA graph) + download, pinned host buffers" % frame},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": roof,
+            "substep_roofline": {"achieved": ALG_BYTES["substep"] * n / (substep_ms / 1e3) / 1e9, "peak": peak,
+                                 "unit": "GB/s", "frac": ALG_BYTES["substep"] * n / (substep_ms / 1e3) / 1e9 / peak,
+                                 "alg_bytes_per_particle": ALG_BYTES["substep"]},
+            "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()},
+            "kernel_share": {k: v / total_k for k, v in shares.items()},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary()}
+    drv.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,210 @@
+/*
+ * mpm_capi.h -- C ABI of the B200 explicit MPM substep (libphysbam_mpm.so).
+ *
+ * Drop-in for the explicit (symplectic Euler) APIC substep of PhysBAM's
+ * Hybrid_Methods MPM driver.  Every entry point is extern "C", takes plain
+ * pointers and sizes, returns an int status (0 = MPM_OK) and never throws.
+ * One handle owns one simulation on one CUDA device and one stream; a handle
+ * is not re-entrant (the reference driver is called from one host thread too,
+ * Projects/mpm/STANDARD_TESTS_BASE.cpp:171-183).
+ *
+ * Particle arrays use the reference's MPM_PARTICLES layout
+ * (Hybrid_Methods/Examples_And_Drivers/MPM_PARTICLES.h:18-44):
+ *   X, V      n * d scalars, one d-vector per particle (ARRAY_VIEW<TV>)
+ *   F, B      n * d * d scalars, column-major per particle (MATRIX<T,d>,
+ *             Core/Matrices/MATRIX_3X3.h:115-119)
+ *   mass, volume, mu, lambda   n scalars
+ *   valid     n bytes (ARRAY_VIEW<bool>)
+ * with scalar type float or double (the reference's T).
+ *
+ * Grid arrays returned by mpm_get_grid cover the ghosted domain
+ * GRID::Domain_Indices(3) = [-3, G+3)^d with the last index fastest, the
+ * layout of ARRAY<T,TV_INT> (MPM_DRIVER.cpp:102-108).
+ */
+#ifndef MPM_CAPI_H
+#define MPM_CAPI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; PHYSBAM_FATAL_ERROR / PHYSBAM_ASSERT throw std::runtime_error in
+ * the reference (Core/Log/DEBUG_UTILITIES.cpp:95-103); here they become codes. */
+enum mpm_status {
+    MPM_OK = 0,
+    MPM_ERR_ARG = 1,        /* bad argument, size or layout */
+    MPM_ERR_CUDA = 2,       /* a CUDA call failed; see mpm_last_error */
+    MPM_ERR_NAN = 3,        /* a non-finite value appeared in the particle state */
+    MPM_ERR_DOMAIN = 4,     /* a particle stencil left the ghosted grid */
+    MPM_ERR_TIMEOUT = 5,    /* a bounded device-side wait gave up */
+    MPM_ERR_NOMEM = 6,      /* device allocation failed */
+    MPM_ERR_STATE = 7,      /* call out of order (e.g. substep before particles) */
+    MPM_ERR_NOT_CONVERGED = 8 /* a bounded SVD iteration did not converge */
+};
+
+enum mpm_precision { MPM_FP32 = 0, MPM_FP64 = 1 };
+
+/* COROTATED_FIXED (Deformables/Constitutive_Models/COROTATED_FIXED.cpp:59-65),
+ * NEO_HOOKEAN with failure threshold .25 (NEO_HOOKEAN.cpp:42-82). */
+enum mpm_model { MPM_COROTATED_FIXED = 0, MPM_NEO_HOOKEAN = 1 };
+
+/* MPM_COLLISION_OBJECT::COLLISION_TYPE (Hybrid_Methods/Collisions/MPM_COLLISION_OBJECT.h:21) */
+enum mpm_collision_type { MPM_STICK = 0, MPM_SLIP = 1, MPM_SEPARATE = 2 };
+
+/* implicit object behind a collision object: RANGE box or PLANE half-space */
+enum mpm_object_kind { MPM_BOX = 0, MPM_PLANE = 1 };
+
+/* which kernels run the substep */
+enum mpm_path {
+    MPM_PATH_FAST = 0,   /* cell-sorted particles, shared-memory tiles, fused stress (FP32) */
+    MPM_PATH_PLAIN = 1   /* one thread per particle, global atomics, reference data layout */
+};
+
+#define MPM_MAX_OBJECTS 8
+
+typedef struct mpm_handle mpm_handle;
+
+/* GRID<TV> (Grid_Tools/Grids/GRID.h) as MPM_EXAMPLE uses it: a MAC grid of
+ * counts[a] cells over [domain_min, domain_max], ghost = 3 (MPM_EXAMPLE.h:86). */
+typedef struct {
+    int dim;                 /* 2 or 3 */
+    int counts[3];
+    double domain_min[3];
+    double domain_max[3];
+    int ghost;               /* must be 3 */
+} mpm_grid_desc;
+
+/* The forces of MPM_EXAMPLE::forces for the explicit path: one
+ * MPM_FINITE_ELEMENTS force (per-particle Lame arrays) and MPM_GRAVITY. */
+typedef struct {
+    int model;               /* mpm_model */
+    int precision;           /* mpm_precision: arithmetic of the device path */
+    int path;                /* mpm_path */
+    double gravity[3];
+} mpm_model_desc;
+
+/* MPM_EXAMPLE::Add_Collision_Object(io, type, friction) for a static object.
+ * MPM_BOX:   a = min corner, b = max corner (RANGE<TV>).
+ * MPM_PLANE: a = unit normal, b = a point on the plane (PLANE<T>). */
+typedef struct {
+    int kind;
+    int type;
+    double friction;
+    double a[3];
+    double b[3];
+} mpm_collision_object;
+
+/* A view of MPM_PARTICLES attribute arrays.  dtype is the element type of
+ * every floating-point array (mpm_precision).  on_device = 1 means the
+ * pointers are CUDA device pointers on the handle's device. */
+typedef struct {
+    int64_t n;
+    int dtype;
+    int on_device;
+    void* X;
+    void* V;
+    void* F;
+    void* B;
+    void* mass;
+    void* volume;
+    void* mu;
+    void* lambda;
+    uint8_t* valid;
+} mpm_particles_view;
+
+/* ---- lifetime ----------------------------------------------------------- */
+
+/* Replaces MPM_DRIVER<TV>::MPM_DRIVER(example) + MPM_DRIVER::Initialize's grid
+ * set-up (Hybrid_Methods/Examples_And_Drivers/MPM_DRIVER.cpp:47-55,81-137).
+ * Binds the handle to the current CUDA device. */
+int mpm_create(const mpm_grid_desc* grid, const mpm_model_desc* model, mpm_handle** out);
+
+/* Replaces MPM_DRIVER::~MPM_DRIVER (MPM_DRIVER.cpp:59-67). */
+int mpm_destroy(mpm_handle* h);
+
+/* Run on this CUDA stream (cudaStream_t) instead of the handle's own. */
+int mpm_set_stream(mpm_handle* h, void* stream);
+
+/* ---- scene --------------------------------------------------------------- */
+
+/* Replaces MPM_EXAMPLE::Add_Collision_Object for the whole list
+ * (Hybrid_Methods/Examples_And_Drivers/MPM_EXAMPLE.cpp:331-338).  At most
+ * MPM_MAX_OBJECTS objects. */
+int mpm_set_collision_objects(mpm_handle* h, const mpm_collision_object* objs, int count);
+
+/* Copies the particles in (the caller keeps ownership).  Replaces filling
+ * MPM_EXAMPLE::particles in a scene's Initialize (MPM_PARTICLES.cpp:10-22,76-88). */
+int mpm_set_particles(mpm_handle* h, const mpm_particles_view* view);
+
+/* Copies X, V, F, B and valid out in the caller's particle order (mass,
+ * volume, mu, lambda are read-only and left untouched). */
+int mpm_get_particles(mpm_handle* h, mpm_particles_view* view);
+
+/* ---- the substep ------------------------------------------------------- */
+
+/* One explicit substep: MPM_DRIVER::Advance_One_Time_Step (MPM_DRIVER.cpp:141-157)
+ * with use_symplectic_euler, use_affine, flip = 0 and quadratic weights:
+ * Update_Simulated_Particles, Update_Particle_Weights, Particle_To_Grid,
+ * Apply_Forces (incl. MPM_OBJECTIVE::Adjust_For_Collision and Apply_Friction),
+ * Grid_To_Particle.  Asynchronous on the handle's stream. */
+int mpm_substep(mpm_handle* h, double dt, double time);
+
+/* nsteps substeps at fixed dt (the fixed-dt frame loop of
+ * MPM_DRIVER::Simulate_To_Frame with min_dt = max_dt, MPM_DRIVER.cpp:161-201),
+ * replayed from a captured CUDA graph. */
+int mpm_advance(mpm_handle* h, double dt, double time, int nsteps);
+
+/* The three phases of the substep, for callers that hook between them like
+ * the reference's named Step callbacks "p2g", "forces", "g2p"
+ * (MPM_DRIVER.cpp:1380-1393).  On the fast path the stress scatter of
+ * Apply_Forces is fused into the P2G kernel; mpm_apply_forces then runs the
+ * grid update alone. */
+int mpm_particle_to_grid(mpm_handle* h, double dt, double time);  /* MPM_DRIVER::Particle_To_Grid, l.245-306 */
+int mpm_apply_forces(mpm_handle* h, double dt, double time);      /* MPM_DRIVER::Apply_Forces, l.959-1060 */
+int mpm_grid_to_particle(mpm_handle* h, double dt, double time);  /* MPM_DRIVER::Grid_To_Particle, l.450-515 */
+
+/* Waits for the handle's stream and reports device-side error flags
+ * (NaN, domain, non-convergence). */
+int mpm_synchronize(mpm_handle* h);
+
+/* ---- inspection ---------------------------------------------------------- */
+
+/* Grids of the last substep as doubles on the host, each (G+6)^d nodes (times
+ * d for vectors): mass after P2G (MPM_EXAMPLE::mass), velocity after P2G
+ * (velocity_save; NULL-able, FP64/plain path only), velocity after the forces
+ * (MPM_EXAMPLE::velocity) and friction velocity (velocity_friction_save).
+ * Any pointer may be NULL. */
+int mpm_get_grid(mpm_handle* h, double* mass, double* v0, double* v, double* vfric);
+
+/* Number of valid particles (MPM_EXAMPLE::simulated_particles.m). */
+int mpm_count_valid(mpm_handle* h, int64_t* count);
+
+/* Per-kernel device time: enable (1) / disable (0) CUDA-event timing, then read
+ * totals.  names gets a comma-separated list, ms and launches one entry each. */
+int mpm_set_timing(mpm_handle* h, int enable);
+int mpm_get_timing(mpm_handle* h, char* names, int names_len, double* ms, int64_t* launches, int max_entries, int* count);
+
+/* ---- sorting ------------------------------------------------------------- */
+
+/* Stable LSD radix sort of n 32-bit keys by their low `bits` bits (1..32) on
+ * the current device, host arrays in and out: the kernels the fast path sorts
+ * particle cell keys with, which replace the reference's x-slab binning
+ * GATHER_SCATTER::Prepare_Scatter (Hybrid_Methods/Iterators/GATHER_SCATTER.cpp:33-87).
+ * perm[i] = index of the i-th smallest key (ties keep input order). */
+int mpm_radix_sort_u32(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm);
+
+/* Fast path only: cell keys of the current particle slots, and the sorted keys
+ * and slot permutation of the last sort (host arrays of n entries, NULL-able).
+ * Key = (particle block << 6) | cell in block; 0xffffffff = invalid particle. */
+int mpm_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm);
+
+/* Human-readable text of the last error on this handle / of a status code. */
+int mpm_last_error(mpm_handle* h, char* buf, int len);
+const char* mpm_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -195,13 +195,15 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
     FILE* f = fopen(dump_path, "wb");
     if(!f) { fprintf(stderr, "cannot open dump\n"); return 1; }
     double total = 0;
+    std::vector<double> step_seconds;
     for(int step = 0; step < s.nsteps; step++) {
         current = step;
         example.dt = (T)s.dt;
         auto t0 = std::chrono::steady_clock::now();
         driver.Advance_One_Time_Step();
         auto t1 = std::chrono::steady_clock::now();
-        total += std::chrono::duration<double>(t1 - t0).count();
+        step_seconds.push_back(std::chrono::duration<double>(t1 - t0).count());
+        total += step_seconds.back();
         example.time += example.dt;
         if(!want(step)) continue;
         wr(f, &step, 1);
@@ -226,9 +228,12 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
         wr(f, gvf.data(), gvf.size());
     }
     fclose(f);
-    if(report_time)
-        printf("{\"substeps\": %d, \"particles\": %lld, \"seconds\": %.9g, \"threads\": %d}\n",
+    if(report_time) {
+        printf("{\"substeps\": %d, \"particles\": %lld, \"seconds\": %.9g, \"threads\": %d, \"step_seconds\": [",
             s.nsteps, s.n, total, threads);
+        for(size_t i = 0; i < step_seconds.size(); i++) printf("%s%.9g", i ? ", " : "", step_seconds[i]);
+        printf("]}\n");
+    }
     std::string cmd = "rm -rf '" + outdir + "'";
     if(system(cmd.c_str())) {}
     return 0;

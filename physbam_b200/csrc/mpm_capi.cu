@@ -1,0 +1,375 @@
+// C ABI entry points (include/mpm_capi.h).  No exception crosses this file's
+// boundary; every entry point returns an mpm_status.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "mpm_internal.h"
+
+int set_error(mpm_handle* h, int code, const std::string& msg)
+{
+    if(h) h->last_error = msg;
+    return code;
+}
+
+int check_cuda(mpm_handle* h, cudaError_t e, const char* what)
+{
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    if(e == cudaErrorMemoryAllocation) return set_error(h, MPM_ERR_NOMEM, msg);
+    return set_error(h, MPM_ERR_CUDA, msg);
+}
+
+int timer_begin(mpm_handle* h, const char* name)
+{
+    if(!h->timing) return -1;
+    int slot = -1;
+    for(size_t i = 0; i < h->timers.size(); i++)
+        if(h->timers[i].name == name) slot = (int)i;
+    if(slot < 0) {
+        KernelTimer t;
+        t.name = name;
+        h->timers.push_back(t);
+        slot = (int)h->timers.size() - 1;
+    }
+    PendingEvent p;
+    p.timer = slot;
+    for(int k = 0; k < 2; k++) {
+        cudaEvent_t ev;
+        if(!h->event_pool.empty()) { ev = h->event_pool.back(); h->event_pool.pop_back(); }
+        else cudaEventCreate(&ev);
+        (k ? p.stop : p.start) = ev;
+    }
+    cudaEventRecord(p.start, h->stream);
+    h->pending.push_back(p);
+    return (int)h->pending.size() - 1;
+}
+
+void timer_end(mpm_handle* h, int slot)
+{
+    if(slot < 0 || !h->timing) return;
+    cudaEventRecord(h->pending[slot].stop, h->stream);
+}
+
+static void drain_timers(mpm_handle* h)
+{
+    for(PendingEvent& p: h->pending) {
+        float ms = 0;
+        cudaEventSynchronize(p.stop);
+        if(cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
+            h->timers[p.timer].ms += ms;
+            h->timers[p.timer].launches++;
+        }
+        h->event_pool.push_back(p.start);
+        h->event_pool.push_back(p.stop);
+    }
+    h->pending.clear();
+}
+
+static bool fast(const mpm_handle* h) { return h->model.path == MPM_PATH_FAST; }
+
+static int read_flags(mpm_handle* h)
+{
+    unsigned f = 0;
+    MPM_CUDA(h, cudaMemcpyAsync(&f, h->d_flags, sizeof(f), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    if(!f) return MPM_OK;
+    MPM_CUDA(h, cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream));
+    if(f & MPM_FLAG_NAN) return set_error(h, MPM_ERR_NAN, "non-finite particle state");
+    if(f & MPM_FLAG_DOMAIN) return set_error(h, MPM_ERR_DOMAIN, "particle stencil outside the ghosted grid");
+    if(f & MPM_FLAG_TIMEOUT) return set_error(h, MPM_ERR_TIMEOUT, "device wait gave up");
+    if(f & MPM_FLAG_NOT_CONVERGED) return set_error(h, MPM_ERR_NOT_CONVERGED, "SVD did not converge");
+    return MPM_OK;
+}
+
+static int release_graph(mpm_handle* h)
+{
+    for(int k = 0; k < 2; k++) {
+        if(h->graphs[k]) cudaGraphExecDestroy(h->graphs[k]);
+        h->graphs[k] = nullptr;
+    }
+    h->graph_dt = 0;
+    return MPM_OK;
+}
+
+extern "C" {
+
+const char* mpm_status_string(int s)
+{
+    switch(s) {
+        case MPM_OK: return "ok";
+        case MPM_ERR_ARG: return "bad argument";
+        case MPM_ERR_CUDA: return "CUDA error";
+        case MPM_ERR_NAN: return "non-finite value";
+        case MPM_ERR_DOMAIN: return "particle outside the grid";
+        case MPM_ERR_TIMEOUT: return "device wait timed out";
+        case MPM_ERR_NOMEM: return "out of device memory";
+        case MPM_ERR_STATE: return "call out of order";
+        case MPM_ERR_NOT_CONVERGED: return "SVD did not converge";
+    }
+    return "unknown status";
+}
+
+int mpm_last_error(mpm_handle* h, char* buf, int len)
+{
+    if(!h || !buf || len <= 0) return MPM_ERR_ARG;
+    snprintf(buf, (size_t)len, "%s", h->last_error.c_str());
+    return MPM_OK;
+}
+
+int mpm_create(const mpm_grid_desc* g, const mpm_model_desc* m, mpm_handle** out)
+{
+    if(!g || !m || !out) return MPM_ERR_ARG;
+    *out = nullptr;
+    if(g->dim != 2 && g->dim != 3) return MPM_ERR_ARG;
+    if(g->ghost != MPM_GHOST) return MPM_ERR_ARG;
+    if(m->model != MPM_COROTATED_FIXED && m->model != MPM_NEO_HOOKEAN) return MPM_ERR_ARG;
+    if(m->precision != MPM_FP32 && m->precision != MPM_FP64) return MPM_ERR_ARG;
+    if(m->path != MPM_PATH_FAST && m->path != MPM_PATH_PLAIN) return MPM_ERR_ARG;
+    if(m->path == MPM_PATH_FAST && (g->dim != 3 || m->precision != MPM_FP32)) return MPM_ERR_ARG;
+    for(int k = 0; k < g->dim; k++) {
+        if(g->counts[k] < 1 || g->counts[k] > 4096) return MPM_ERR_ARG;
+        if(!(g->domain_max[k] > g->domain_min[k])) return MPM_ERR_ARG;
+    }
+    mpm_handle* h = new(std::nothrow) mpm_handle();
+    if(!h) return MPM_ERR_NOMEM;
+    if(cudaGetDevice(&h->device) != cudaSuccess) { delete h; return MPM_ERR_CUDA; }
+    if(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device) != cudaSuccess) { delete h; return MPM_ERR_CUDA; }
+    if(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { delete h; return MPM_ERR_CUDA; }
+    h->own_stream = true;
+    h->grid = *g;
+    h->model = *m;
+    SceneParams& sp = h->sp;
+    memset(&sp, 0, sizeof(sp));
+    sp.dim = g->dim;
+    for(int k = 0; k < 3; k++) {
+        bool on = k < g->dim;
+        sp.counts[k] = on ? g->counts[k] : 1;
+        sp.dmin[k] = on ? g->domain_min[k] : 0;
+        sp.dmax[k] = on ? g->domain_max[k] : 1;
+        sp.dx[k] = (sp.dmax[k] - sp.dmin[k]) / sp.counts[k];   // GRID::Initialize, GRID.cpp:23-24
+        sp.inv_dx[k] = 1 / sp.dx[k];
+        sp.gravity[k] = on ? m->gravity[k] : 0;
+    }
+    sp.model = m->model;
+    if(cudaMalloc(&h->d_flags, sizeof(unsigned)) != cudaSuccess ||
+       cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned), h->stream) != cudaSuccess) {
+        cudaStreamDestroy(h->stream);
+        delete h;
+        return MPM_ERR_CUDA;
+    }
+    *out = h;
+    return MPM_OK;
+}
+
+int mpm_destroy(mpm_handle* h)
+{
+    if(!h) return MPM_ERR_ARG;
+    cudaStreamSynchronize(h->stream);
+    release_graph(h);
+    drain_timers(h);
+    for(cudaEvent_t e: h->event_pool) cudaEventDestroy(e);
+    plain_free(h);
+    fast_free(h);
+    cudaFree(h->d_flags);
+    if(h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MPM_OK;
+}
+
+int mpm_set_stream(mpm_handle* h, void* stream)
+{
+    if(!h) return MPM_ERR_ARG;
+    cudaStreamSynchronize(h->stream);
+    release_graph(h);
+    if(h->own_stream) cudaStreamDestroy(h->stream);
+    h->stream = (cudaStream_t)stream;
+    h->own_stream = false;
+    return MPM_OK;
+}
+
+int mpm_set_collision_objects(mpm_handle* h, const mpm_collision_object* objs, int count)
+{
+    if(!h || count < 0 || count > MPM_MAX_OBJECTS || (count && !objs)) return MPM_ERR_ARG;
+    for(int i = 0; i < count; i++) {
+        const mpm_collision_object& o = objs[i];
+        if(o.kind != MPM_BOX && o.kind != MPM_PLANE) return set_error(h, MPM_ERR_ARG, "unknown object kind");
+        if(o.type < MPM_STICK || o.type > MPM_SEPARATE) return set_error(h, MPM_ERR_ARG, "unknown collision type");
+        if(o.kind == MPM_BOX)
+            for(int k = 0; k < h->sp.dim; k++)
+                if(!(o.b[k] > o.a[k])) return set_error(h, MPM_ERR_ARG, "box with an empty side (RANGE::Signed_Distance)");
+    }
+    release_graph(h);
+    h->sp.nobj = count;
+    for(int i = 0; i < count; i++) {
+        mpm::DevObject& d = h->sp.objs[i];
+        d.kind = objs[i].kind;
+        d.type = objs[i].type;
+        d.friction = objs[i].friction;
+        for(int k = 0; k < 3; k++) { d.a[k] = objs[i].a[k]; d.b[k] = objs[i].b[k]; }
+    }
+    return MPM_OK;
+}
+
+int mpm_set_particles(mpm_handle* h, const mpm_particles_view* v)
+{
+    if(!h || !v || v->n < 0) return MPM_ERR_ARG;
+    if(v->dtype != MPM_FP32 && v->dtype != MPM_FP64) return set_error(h, MPM_ERR_ARG, "dtype");
+    release_graph(h);
+    int rc = fast(h) ? fast_set_particles(h, v) : plain_set_particles(h, v);
+    if(rc) return rc;
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->n = v->n;
+    h->have_particles = true;
+    return read_flags(h);
+}
+
+int mpm_get_particles(mpm_handle* h, mpm_particles_view* v)
+{
+    if(!h || !v) return MPM_ERR_ARG;
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    if(v->dtype != MPM_FP32 && v->dtype != MPM_FP64) return set_error(h, MPM_ERR_ARG, "dtype");
+    return fast(h) ? fast_get_particles(h, v) : plain_get_particles(h, v);
+}
+
+static int check_dt(mpm_handle* h, double dt)
+{
+    if(!h) return MPM_ERR_ARG;
+    if(!(dt > 0) || !std::isfinite(dt)) return set_error(h, MPM_ERR_ARG, "dt must be positive");
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    return MPM_OK;
+}
+
+int mpm_particle_to_grid(mpm_handle* h, double dt, double time)
+{
+    int rc = check_dt(h, dt);
+    if(rc) return rc;
+    return fast(h) ? fast_p2g(h, dt, time) : plain_p2g(h, dt, time);
+}
+
+int mpm_apply_forces(mpm_handle* h, double dt, double time)
+{
+    int rc = check_dt(h, dt);
+    if(rc) return rc;
+    return fast(h) ? fast_forces(h, dt, time) : plain_forces(h, dt, time);
+}
+
+int mpm_grid_to_particle(mpm_handle* h, double dt, double time)
+{
+    int rc = check_dt(h, dt);
+    if(rc) return rc;
+    return fast(h) ? fast_g2p(h, dt, time) : plain_g2p(h, dt, time);
+}
+
+int mpm_substep(mpm_handle* h, double dt, double time)
+{
+    int rc = check_dt(h, dt);
+    if(rc) return rc;
+    if((rc = mpm_particle_to_grid(h, dt, time))) return rc;
+    if((rc = mpm_apply_forces(h, dt, time))) return rc;
+    return mpm_grid_to_particle(h, dt, time);
+}
+
+int mpm_advance(mpm_handle* h, double dt, double time, int nsteps)
+{
+    int rc = check_dt(h, dt);
+    if(rc) return rc;
+    if(nsteps < 0) return set_error(h, MPM_ERR_ARG, "nsteps < 0");
+    if(h->timing) {   // per-kernel events cannot live inside a graph: run eagerly
+        for(int s = 0; s < nsteps; s++)
+            if((rc = mpm_substep(h, dt, time + s * dt))) return rc;
+        return MPM_OK;
+    }
+    // One captured graph per substep; the fast path alternates its particle
+    // buffers, so it keeps one graph per buffer parity.
+    if(h->graph_dt != dt) release_graph(h);
+    for(int s = 0; s < nsteps; s++) {
+        int par = fast(h) ? h->fast.cur : 0;
+        if(!h->graphs[par]) {
+            cudaGraph_t g;
+            MPM_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            int crc = mpm_substep(h, dt, time);
+            cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+            if(fast(h)) h->fast.cur = par;     // capture executed nothing
+            if(crc) { if(e == cudaSuccess) cudaGraphDestroy(g); return crc; }
+            if(e != cudaSuccess) return check_cuda(h, e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&h->graphs[par], g, 0);
+            cudaGraphDestroy(g);
+            if(e != cudaSuccess) { h->graphs[par] = nullptr; return check_cuda(h, e, "cudaGraphInstantiate"); }
+            h->graph_dt = dt;
+        }
+        MPM_CUDA(h, cudaGraphLaunch(h->graphs[par], h->stream));
+        if(fast(h)) h->fast.cur = 1 - par;
+    }
+    return MPM_OK;
+}
+
+int mpm_synchronize(mpm_handle* h)
+{
+    if(!h) return MPM_ERR_ARG;
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    MPM_CUDA(h, cudaGetLastError());
+    return read_flags(h);
+}
+
+int mpm_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf)
+{
+    if(!h) return MPM_ERR_ARG;
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    return fast(h) ? fast_get_grid(h, m, v0, v, vf) : plain_get_grid(h, m, v0, v, vf);
+}
+
+int mpm_count_valid(mpm_handle* h, int64_t* count)
+{
+    if(!h || !count) return MPM_ERR_ARG;
+    if(!h->have_particles) { *count = 0; return MPM_OK; }
+    return fast(h) ? fast_count_valid(h, count) : plain_count_valid(h, count);
+}
+
+int mpm_radix_sort_u32(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm)
+{
+    return radix_sort_host(keys, n, bits, sorted_keys, perm);
+}
+
+int mpm_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm)
+{
+    if(!h) return MPM_ERR_ARG;
+    if(!fast(h)) return set_error(h, MPM_ERR_ARG, "sort state exists on the fast path only");
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    return fast_debug_sort_state(h, slot_keys, sorted_keys, perm);
+}
+
+int mpm_set_timing(mpm_handle* h, int enable)
+{
+    if(!h) return MPM_ERR_ARG;
+    cudaStreamSynchronize(h->stream);
+    drain_timers(h);
+    h->timing = enable != 0;
+    for(KernelTimer& t: h->timers) { t.ms = 0; t.launches = 0; }
+    return MPM_OK;
+}
+
+int mpm_get_timing(mpm_handle* h, char* names, int names_len, double* ms, int64_t* launches, int max_entries, int* count)
+{
+    if(!h || !count) return MPM_ERR_ARG;
+    drain_timers(h);
+    std::string all;
+    int c = 0;
+    for(const KernelTimer& t: h->timers) {
+        if(c < max_entries) {
+            if(ms) ms[c] = t.ms;
+            if(launches) launches[c] = t.launches;
+            if(c) all += ",";
+            all += t.name;
+        }
+        c++;
+    }
+    *count = c < max_entries ? c : max_entries;
+    if(names && names_len > 0) snprintf(names, (size_t)names_len, "%s", all.c_str());
+    return MPM_OK;
+}
+
+}  // extern "C"

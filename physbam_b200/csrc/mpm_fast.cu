@@ -1,0 +1,866 @@
+// Fast path: the explicit MPM substep in FP32 with cell-sorted particles.
+//
+// Per substep (MPM_DRIVER::Advance_One_Time_Step, MPM_DRIVER.cpp:141-157):
+//   sort     particle keys (block of 4^3 cells, cell in block) are radix-sorted;
+//            the previous G2P wrote them, so the particles are already nearly in
+//            order and the permutation is local.
+//   ranges   sorted keys -> [start, end) per particle block, list of active
+//            blocks, number of valid particles (invalid ones carry the
+//            sentinel key and sort to the tail).
+//   p2g      one CTA per active block: B-spline weights, the stress
+//            P(F) F^T (fused; MPM_FINITE_ELEMENTS::Precompute, .cpp:47-67) and
+//            APIC momentum plus dt * force accumulate into a 6^3-node shared
+//            tile, flushed with one float4 atomic per touched node
+//            (Particle_To_Grid l.245-306 and MPM_FINITE_ELEMENTS::Add_Forces,
+//            MPM_GRAVITY::Add_Forces folded in).  The CTA marks the node blocks
+//            its tile covers.
+//   grid     one CTA per marked node block: v = (mv + dt f)/m + dt g, the
+//            collision projection and friction (Apply_Forces l.959-1060),
+//            zeroes the accumulator for the next substep.
+//   g2p      one CTA per active block: stage the tile of (v, v_fric), gather,
+//            update F, X, V and the APIC B (Grid_To_Particle l.450-515),
+//            write the particle to its sorted slot in the other buffer and
+//            its next key.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "mpm_internal.h"
+#include "mpm_sort.cuh"
+
+namespace {
+
+using namespace mpm;
+
+constexpr int BS = 4;                      // cells per particle-block edge
+constexpr int TE = BS + 2;                 // tile edge in nodes
+constexpr int TN = TE * TE * TE;           // 216 nodes per tile
+constexpr uint32_t SENTINEL = 0xffffffffu;
+constexpr int NCOMP = 24;                  // x3 v3 F9 B9 floats per particle
+constexpr int C_X = 0, C_V = 3, C_F = 6, C_B = 15;
+
+struct FastArgs {
+    SceneParams sp;
+    int64_t n, npad;
+    const float* src;
+    const float4* src_attr;
+    const int* src_pid;
+    float* dst;
+    float4* dst_attr;
+    int* dst_pid;
+    const uint32_t* perm;
+    const uint32_t* sorted_keys;
+    uint32_t* keys_next;
+    uint32_t *bstart, *bend, *active, *nb_flag, *nb_list, *counters;
+    float4* acc;
+    float4* vel;
+    int GA[3], NB[3], NN[3];
+    float dt;
+    float dmin[3], dmax[3], dx[3], inv[3];
+    float gravity[3];
+    unsigned* flags;
+};
+
+__device__ __forceinline__ int64_t node_index(const FastArgs& a, int qx, int qy, int qz)
+{
+    return ((int64_t)qx * a.GA[1] + qy) * a.GA[2] + qz;
+}
+
+// Cell key of a position: the block and in-block cell of the first stencil
+// node (base + 3 in ghosted node coordinates).  SENTINEL when the stencil
+// would leave the ghosted grid.
+__device__ __forceinline__ uint32_t cell_key(const FastArgs& a, const float* X)
+{
+    int cc[3];
+#pragma unroll
+    for(int k = 0; k < 3; k++) {
+        float y = X[k] - a.dx[k];
+        int base = (int)floorf((y - a.dmin[k]) * a.inv[k]);
+        cc[k] = base + MPM_GHOST;
+        if(cc[k] < 0 || cc[k] > a.sp.counts[k] + MPM_GHOST) return SENTINEL;
+    }
+    uint32_t b = ((uint32_t)(cc[0] >> 2) * a.NB[1] + (uint32_t)(cc[1] >> 2)) * a.NB[2] + (uint32_t)(cc[2] >> 2);
+    return (b << 6) | ((cc[0] & 3) << 4) | ((cc[1] & 3) << 2) | (cc[2] & 3);
+}
+
+__device__ __forceinline__ void block_coords(const FastArgs& a, uint32_t b, int& bx, int& by, int& bz)
+{
+    bz = b % a.NB[2];
+    uint32_t r = b / a.NB[2];
+    by = r % a.NB[1];
+    bx = r / a.NB[1];
+}
+
+// ---------------------------------------------------------------------------
+// Stress P(F) F^T in FP32 without an SVD where that is exact in exact
+// arithmetic and well conditioned; otherwise (inverted or nearly degenerate
+// F, or the neo-Hookean clamp region) the caller falls back to the FP64 SVD.
+//   NEO_HOOKEAN, J >= .25:  P F^T = mu (F F^T - I) + lambda ln J I
+//   COROTATED_FIXED, J > 0: P F^T = 2 mu (b - sqrt(b)) + lambda J (J-1) I,
+//     b = F F^T; sqrt(b) = R F^T is the left stretch, from the eigenvalues of
+//     b and the closed form of Hoger & Carlson (1984):
+//     sqrt(b) = (-b^2 + (I1^2 - I2) b + I1 I3 I) / (I1 I2 - I3)
+//     with I1, I2, I3 the invariants of sqrt(b).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool stress_fast(int model, const float* F, float mu, float la, float* PFT)
+{
+    float b00 = F[0] * F[0] + F[3] * F[3] + F[6] * F[6];
+    float b11 = F[1] * F[1] + F[4] * F[4] + F[7] * F[7];
+    float b22 = F[2] * F[2] + F[5] * F[5] + F[8] * F[8];
+    float b01 = F[0] * F[1] + F[3] * F[4] + F[6] * F[7];
+    float b02 = F[0] * F[2] + F[3] * F[5] + F[6] * F[8];
+    float b12 = F[1] * F[2] + F[4] * F[5] + F[7] * F[8];
+    float J = F[0] * (F[4] * F[8] - F[7] * F[5]) - F[3] * (F[1] * F[8] - F[7] * F[2]) + F[6] * (F[1] * F[5] - F[4] * F[2]);
+    if(model == MPM_NEO_HOOKEAN) {
+        if(!(J >= (float)kNeoHookeanThreshold)) return false;
+        float d = la * logf(J) - mu;
+        PFT[0] = mu * b00 + d; PFT[4] = mu * b11 + d; PFT[8] = mu * b22 + d;
+        PFT[1] = PFT[3] = mu * b01;
+        PFT[2] = PFT[6] = mu * b02;
+        PFT[5] = PFT[7] = mu * b12;
+        return true;
+    }
+    if(!(J > 0.f)) return false;
+    // eigenvalues of b (trigonometric form); only symmetric functions of their
+    // square roots are used, which stay accurate for repeated eigenvalues
+    float q = (b00 + b11 + b22) * (1.f / 3.f);
+    float c00 = b00 - q, c11 = b11 - q, c22 = b22 - q;
+    float off = b01 * b01 + b02 * b02 + b12 * b12;
+    float p2 = (c00 * c00 + c11 * c11 + c22 * c22 + 2.f * off) * (1.f / 6.f);
+    float l1, l2, l3;
+    if(p2 <= 1e-14f * q * q) {
+        l1 = l2 = l3 = q;
+    } else {
+        float p = sqrtf(p2), ip = 1.f / p;
+        float e00 = c00 * ip, e11 = c11 * ip, e22 = c22 * ip, e01 = b01 * ip, e02 = b02 * ip, e12 = b12 * ip;
+        float det = e00 * (e11 * e22 - e12 * e12) - e01 * (e01 * e22 - e12 * e02) + e02 * (e01 * e12 - e11 * e02);
+        float r = fminf(fmaxf(0.5f * det, -1.f), 1.f);
+        float phi = acosf(r) * (1.f / 3.f);
+        l1 = q + 2.f * p * cosf(phi);
+        l3 = q + 2.f * p * cosf(phi + 2.0943951023931953f);
+        l2 = 3.f * q - l1 - l3;
+    }
+    if(!(l3 > 1e-4f * l1)) return false;     // sigma_min / sigma_max < 1e-2: FP64 SVD
+    float m1 = sqrtf(l1), m2 = sqrtf(fmaxf(l2, 0.f)), m3 = sqrtf(l3);
+    float I1 = m1 + m2 + m3, I2 = m1 * m2 + m2 * m3 + m3 * m1, I3 = J;
+    float den = I1 * I2 - I3;
+    if(!(den > 0.f)) return false;
+    float ca = I1 * I1 - I2, cb = I1 * I3, id = 1.f / den;
+    // b^2 (symmetric)
+    float s00 = b00 * b00 + b01 * b01 + b02 * b02;
+    float s11 = b01 * b01 + b11 * b11 + b12 * b12;
+    float s22 = b02 * b02 + b12 * b12 + b22 * b22;
+    float s01 = b00 * b01 + b01 * b11 + b02 * b12;
+    float s02 = b00 * b02 + b01 * b12 + b02 * b22;
+    float s12 = b01 * b02 + b11 * b12 + b12 * b22;
+    float u00 = (-s00 + ca * b00 + cb) * id, u11 = (-s11 + ca * b11 + cb) * id, u22 = (-s22 + ca * b22 + cb) * id;
+    float u01 = (-s01 + ca * b01) * id, u02 = (-s02 + ca * b02) * id, u12 = (-s12 + ca * b12) * id;
+    float mu2 = 2.f * mu, pr = la * J * (J - 1.f);
+    PFT[0] = mu2 * (b00 - u00) + pr; PFT[4] = mu2 * (b11 - u11) + pr; PFT[8] = mu2 * (b22 - u22) + pr;
+    PFT[1] = PFT[3] = mu2 * (b01 - u01);
+    PFT[2] = PFT[6] = mu2 * (b02 - u02);
+    PFT[5] = PFT[7] = mu2 * (b12 - u12);
+    return true;
+}
+
+// FP64 fallback: the reference's signed SVD route, out of line so its
+// registers do not weigh on the common path.
+__device__ __noinline__ bool stress_fp64(int model, const float* Ff, float mu, float la, float* PFT)
+{
+    double F[9], P[9];
+#pragma unroll
+    for(int e = 0; e < 9; e++) F[e] = Ff[e];
+    bool ok = pft_svd<double, 3>(model, F, (double)mu, (double)la, P);
+#pragma unroll
+    for(int e = 0; e < 9; e++) PFT[e] = (float)P[e];
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_init_keys(FastArgs a, const uint8_t* valid_by_slot)
+{
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        float X[3] = {a.src[(C_X + 0) * a.npad + i], a.src[(C_X + 1) * a.npad + i], a.src[(C_X + 2) * a.npad + i]};
+        uint32_t k = valid_by_slot[i] ? cell_key(a, X) : SENTINEL;
+        if(valid_by_slot[i] && k == SENTINEL) atomicOr(a.flags, MPM_FLAG_DOMAIN);
+        a.keys_next[i] = k;
+    }
+}
+
+__global__ void k_ranges(FastArgs a)
+{
+    for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < a.n; j += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t k = a.sorted_keys[j];
+        uint32_t kp = j ? a.sorted_keys[j - 1] : SENTINEL;
+        if(k == SENTINEL) {
+            if(j == 0 || kp != SENTINEL) a.counters[CNT_ACTIVE_PARTICLES] = (uint32_t)j;
+            continue;
+        }
+        uint32_t b = k >> 6;
+        if(j == 0 || (kp >> 6) != b) {
+            a.bstart[b] = (uint32_t)j;
+            a.active[atomicAdd(&a.counters[CNT_ACTIVE_BLOCKS], 1u)] = b;
+        }
+        uint32_t kn = j + 1 < a.n ? a.sorted_keys[j + 1] : SENTINEL;
+        if(kn == SENTINEL || (kn >> 6) != b) a.bend[b] = (uint32_t)(j + 1);
+        if(j + 1 == a.n) a.counters[CNT_ACTIVE_PARTICLES] = (uint32_t)a.n;
+    }
+}
+
+// Invalid particles keep their last state; move them to their sorted slot.
+__global__ void k_tail(FastArgs a)
+{
+    int64_t n_act = a.counters[CNT_ACTIVE_PARTICLES];
+    for(int64_t j = n_act + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < a.n; j += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t i = a.perm[j];
+#pragma unroll 4
+        for(int c = 0; c < NCOMP; c++) a.dst[c * a.npad + j] = a.src[c * a.npad + i];
+        a.dst_attr[j] = a.src_attr[i];
+        a.dst_pid[j] = a.src_pid[i];
+        a.keys_next[j] = SENTINEL;
+    }
+}
+
+__device__ __forceinline__ int next_work(uint32_t* ctr, int* s_work)
+{
+    __syncthreads();
+    if(threadIdx.x == 0) *s_work = (int)atomicAdd(ctr, 1u);
+    __syncthreads();
+    return *s_work;
+}
+
+template<int THREADS> __global__ void __launch_bounds__(THREADS) k_p2g(FastArgs a)
+{
+    __shared__ float tm[TN], tx[TN], ty[TN], tz[TN];
+    __shared__ int s_work;
+    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
+    const float Dx = 4.f * a.inv[0] * a.inv[0], Dy = 4.f * a.inv[1] * a.inv[1], Dz = 4.f * a.inv[2] * a.inv[2];
+    for(int w = next_work(&a.counters[CNT_P2G_WORK], &s_work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &s_work)) {
+        uint32_t b = a.active[w];
+        int bx, by, bz;
+        block_coords(a, b, bx, by, bz);
+        const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;   // tile origin, ghosted node coords
+        for(int t = threadIdx.x; t < TN; t += THREADS) { tm[t] = 0; tx[t] = 0; ty[t] = 0; tz[t] = 0; }
+        __syncthreads();
+        const uint32_t s = a.bstart[b], e = a.bend[b];
+        for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
+            const uint32_t i = a.perm[j];
+            float X[3], V[3], F[9], Bm[9];
+#pragma unroll
+            for(int k = 0; k < 3; k++) { X[k] = a.src[(C_X + k) * a.npad + i]; V[k] = a.src[(C_V + k) * a.npad + i]; }
+#pragma unroll
+            for(int k = 0; k < 9; k++) { F[k] = a.src[(C_F + k) * a.npad + i]; Bm[k] = a.src[(C_B + k) * a.npad + i]; }
+            const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
+            float PFT[9];
+            if(!stress_fast(a.sp.model, F, at.z, at.w, PFT)) {
+                atomicAdd(&a.counters[CNT_FALLBACK], 1u);
+                if(!stress_fp64(a.sp.model, F, at.z, at.w, PFT)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
+            }
+            Axis<float> ax[3];
+#pragma unroll
+            for(int k = 0; k < 3; k++) ax[k] = spline_axis<float>(X[k], a.dmin[k], a.dx[k], a.inv[k]);
+            const int lx = ax[0].base + MPM_GHOST - ox, ly = ax[1].base + MPM_GHOST - oy, lz = ax[2].base + MPM_GHOST - oz;
+            // stress term: dt * volume * PFT ; affine term: mass * B * Dp^-1 applied per axis offset
+            const float sv = a.dt * at.y;
+            float S[9];
+#pragma unroll
+            for(int k = 0; k < 9; k++) S[k] = sv * PFT[k];
+            const float m = at.x;
+            float mv[3] = {m * V[0], m * V[1], m * V[2]};
+            float ux[3][3], uy[3][3], uz[3][3];   // [offset][component] = m B[:,axis] D (Z_axis - X_axis)
+#pragma unroll
+            for(int o = 0; o < 3; o++) {
+                float dxo = (a.dmin[0] + ((float)(ax[0].base + o) + 0.5f) * a.dx[0] - X[0]) * Dx * m;
+                float dyo = (a.dmin[1] + ((float)(ax[1].base + o) + 0.5f) * a.dx[1] - X[1]) * Dy * m;
+                float dzo = (a.dmin[2] + ((float)(ax[2].base + o) + 0.5f) * a.dx[2] - X[2]) * Dz * m;
+#pragma unroll
+                for(int r = 0; r < 3; r++) {
+                    ux[o][r] = Bm[r + 0] * dxo;
+                    uy[o][r] = Bm[r + 3] * dyo;
+                    uz[o][r] = Bm[r + 6] * dzo;
+                }
+            }
+#pragma unroll
+            for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+                for(int jj = 0; jj < 3; jj++) {
+                    const float wxy = ax[0].w[ii] * ax[1].w[jj];
+                    const float gx0 = ax[0].dw[ii] * ax[1].w[jj], gy0 = ax[0].w[ii] * ax[1].dw[jj];
+#pragma unroll
+                    for(int kk = 0; kk < 3; kk++) {
+                        const float w = wxy * ax[2].w[kk];
+                        const float g0 = gx0 * ax[2].w[kk], g1 = gy0 * ax[2].w[kk], g2 = wxy * ax[2].dw[kk];
+                        const int t = ((lx + ii) * TE + (ly + jj)) * TE + (lz + kk);
+                        float px = w * (mv[0] + ux[ii][0] + uy[jj][0] + uz[kk][0]) - (S[0] * g0 + S[3] * g1 + S[6] * g2);
+                        float py = w * (mv[1] + ux[ii][1] + uy[jj][1] + uz[kk][1]) - (S[1] * g0 + S[4] * g1 + S[7] * g2);
+                        float pz = w * (mv[2] + ux[ii][2] + uy[jj][2] + uz[kk][2]) - (S[2] * g0 + S[5] * g1 + S[8] * g2);
+                        atomicAdd(&tm[t], w * m);
+                        atomicAdd(&tx[t], px);
+                        atomicAdd(&ty[t], py);
+                        atomicAdd(&tz[t], pz);
+                    }
+                }
+        }
+        __syncthreads();
+        for(int t = threadIdx.x; t < TN; t += THREADS) {
+            float mm = tm[t];
+            if(mm != 0.f) {
+                int qx = ox + t / (TE * TE), qy = oy + (t / TE) % TE, qz = oz + t % TE;
+                atomicAdd(&a.acc[node_index(a, qx, qy, qz)], make_float4(tx[t], ty[t], tz[t], mm));
+            }
+        }
+        if(threadIdx.x < 8) {
+            int nx = bx + (threadIdx.x >> 2), ny = by + ((threadIdx.x >> 1) & 1), nz = bz + (threadIdx.x & 1);
+            uint32_t nb = ((uint32_t)nx * a.NN[1] + ny) * a.NN[2] + nz;
+            if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.counters[CNT_NODE_BLOCKS], 1u)] = nb;
+        }
+    }
+}
+
+// One node block (4^3 nodes) per 64 threads.
+__global__ void __launch_bounds__(64) k_grid(FastArgs a)
+{
+    __shared__ int s_work;
+    const uint32_t nnb = a.counters[CNT_NODE_BLOCKS];
+    for(int w = next_work(&a.counters[CNT_GRID_WORK], &s_work); w < (int)nnb; w = next_work(&a.counters[CNT_GRID_WORK], &s_work)) {
+        uint32_t nb = a.nb_list[w];
+        int nz = nb % a.NN[2], r = nb / a.NN[2], ny = r % a.NN[1], nx = r / a.NN[1];
+        int t = threadIdx.x;
+        int qx = 4 * nx + (t >> 4), qy = 4 * ny + ((t >> 2) & 3), qz = 4 * nz + (t & 3);
+        int64_t q = node_index(a, qx, qy, qz);
+        float4 c = a.acc[q];
+        float4 o0 = make_float4(0, 0, 0, 0), o1 = make_float4(0, 0, 0, 0);
+        if(c.w != 0.f) {
+            float im = 1.f / c.w;
+            float V[3] = {c.x * im + a.dt * a.gravity[0], c.y * im + a.dt * a.gravity[1], c.z * im + a.dt * a.gravity[2]};
+            float vn[3], vf[3];
+            if(a.sp.nobj) {
+                float X0[3] = {a.dmin[0] + ((float)(qx - MPM_GHOST) + 0.5f) * a.dx[0],
+                               a.dmin[1] + ((float)(qy - MPM_GHOST) + 0.5f) * a.dx[1],
+                               a.dmin[2] + ((float)(qz - MPM_GHOST) + 0.5f) * a.dx[2]};
+                float zero[3] = {0.f, 0.f, 0.f};
+                collide_node<float, 3>(a.sp.objs, a.sp.nobj, X0, zero, V, a.dt, vn, vf);
+            } else {
+#pragma unroll
+                for(int k = 0; k < 3; k++) vn[k] = vf[k] = V[k];
+            }
+            o0 = make_float4(vn[0], vn[1], vn[2], vf[0]);
+            o1 = make_float4(vf[1], vf[2], c.w, 0.f);
+            a.acc[q] = make_float4(0, 0, 0, 0);
+        }
+        a.vel[2 * q] = o0;
+        a.vel[2 * q + 1] = o1;
+        if(t == 0) a.nb_flag[nb] = 0u;
+    }
+}
+
+template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
+{
+    __shared__ float4 tv[2 * TN];
+    __shared__ int s_work;
+    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
+    const float dt = a.dt;
+    for(int w = next_work(&a.counters[CNT_G2P_WORK], &s_work); w < (int)nblocks; w = next_work(&a.counters[CNT_G2P_WORK], &s_work)) {
+        uint32_t b = a.active[w];
+        int bx, by, bz;
+        block_coords(a, b, bx, by, bz);
+        const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;
+        for(int t = threadIdx.x; t < 2 * TN; t += THREADS) {
+            int nd = t >> 1;
+            int qx = ox + nd / (TE * TE), qy = oy + (nd / TE) % TE, qz = oz + nd % TE;
+            tv[t] = a.vel[2 * node_index(a, qx, qy, qz) + (t & 1)];
+        }
+        __syncthreads();
+        const uint32_t s = a.bstart[b], e = a.bend[b];
+        for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
+            const uint32_t i = a.perm[j];
+            float X[3], F[9];
+#pragma unroll
+            for(int k = 0; k < 3; k++) X[k] = a.src[(C_X + k) * a.npad + i];
+#pragma unroll
+            for(int k = 0; k < 9; k++) F[k] = a.src[(C_F + k) * a.npad + i];
+            Axis<float> ax[3];
+#pragma unroll
+            for(int k = 0; k < 3; k++) ax[k] = spline_axis<float>(X[k], a.dmin[k], a.dx[k], a.inv[k]);
+            const int lx = ax[0].base + MPM_GHOST - ox, ly = ax[1].base + MPM_GHOST - oy, lz = ax[2].base + MPM_GHOST - oz;
+            float dX[3][3];   // [axis][offset]: Z - X
+#pragma unroll
+            for(int o = 0; o < 3; o++)
+#pragma unroll
+                for(int k = 0; k < 3; k++) dX[k][o] = a.dmin[k] + ((float)(ax[k].base + o) + 0.5f) * a.dx[k] - X[k];
+            float Vp[3] = {0, 0, 0}, Vf[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Bv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            float K01 = 0, K02 = 0, K12 = 0;
+#pragma unroll
+            for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+                for(int jj = 0; jj < 3; jj++) {
+                    const float wxy = ax[0].w[ii] * ax[1].w[jj];
+                    const float gx0 = ax[0].dw[ii] * ax[1].w[jj], gy0 = ax[0].w[ii] * ax[1].dw[jj];
+#pragma unroll
+                    for(int kk = 0; kk < 3; kk++) {
+                        const float wt = wxy * ax[2].w[kk];
+                        const float g0 = gx0 * ax[2].w[kk], g1 = gy0 * ax[2].w[kk], g2 = wxy * ax[2].dw[kk];
+                        const int t = ((lx + ii) * TE + (ly + jj)) * TE + (lz + kk);
+                        const float4 p0 = tv[2 * t], p1 = tv[2 * t + 1];
+                        const float vn[3] = {p0.x, p0.y, p0.z}, vf[3] = {p0.w, p1.x, p1.y};
+                        const float wf[3] = {wt * vf[0], wt * vf[1], wt * vf[2]};
+#pragma unroll
+                        for(int r = 0; r < 3; r++) {
+                            Vp[r] += wt * vn[r];
+                            Vf[r] += wf[r];
+                            G[r] += vn[r] * g0; G[r + 3] += vn[r] * g1; G[r + 6] += vn[r] * g2;
+                            Bv[r] += wf[r] * dX[0][ii]; Bv[r + 3] += wf[r] * dX[1][jj]; Bv[r + 6] += wf[r] * dX[2][kk];
+                        }
+                        K01 += wf[0] * vn[1] - wf[1] * vn[0];
+                        K02 += wf[0] * vn[2] - wf[2] * vn[0];
+                        K12 += wf[1] * vn[2] - wf[2] * vn[1];
+                    }
+                }
+            // F <- (I + dt grad v) F
+            float Fn[9];
+#pragma unroll
+            for(int c = 0; c < 3; c++)
+#pragma unroll
+                for(int r = 0; r < 3; r++)
+                    Fn[r + 3 * c] = F[r + 3 * c] + dt * (G[r] * F[3 * c] + G[r + 3] * F[3 * c + 1] + G[r + 6] * F[3 * c + 2]);
+            float xn[3];
+#pragma unroll
+            for(int k = 0; k < 3; k++) xn[k] = X[k] + dt * Vp[k];
+            // APIC B in the reference's xi_new form, rewritten with the partition of
+            // unity: B = sum w vf (Z - X) + dt/2 [sum w (vf vn^T - vn vf^T) - (Vf Vp^T - Vp Vf^T)]
+            const float h = 0.5f * dt;
+            const float A01 = h * (K01 - (Vf[0] * Vp[1] - Vp[0] * Vf[1]));
+            const float A02 = h * (K02 - (Vf[0] * Vp[2] - Vp[0] * Vf[2]));
+            const float A12 = h * (K12 - (Vf[1] * Vp[2] - Vp[1] * Vf[2]));
+            float Bn[9] = {Bv[0], Bv[1] - A01, Bv[2] - A02,
+                           Bv[3] + A01, Bv[4], Bv[5] - A12,
+                           Bv[6] + A02, Bv[7] + A12, Bv[8]};
+            bool ok = true;
+            for(int k = 0; k < 3; k++) {
+                float eps = FLT_EPSILON * 4.f * (a.dmax[k] - a.dmin[k]);
+                if(!(xn[k] >= a.dmin[k] + eps && xn[k] <= a.dmax[k] - eps)) ok = false;
+            }
+            bool finite = true;
+#pragma unroll
+            for(int k = 0; k < 9; k++) finite = finite && isfinite(Fn[k]);
+            finite = finite && isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]);
+            if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); ok = false; }
+            uint32_t key = ok ? cell_key(a, xn) : SENTINEL;
+#pragma unroll
+            for(int k = 0; k < 3; k++) { a.dst[(C_X + k) * a.npad + j] = xn[k]; a.dst[(C_V + k) * a.npad + j] = Vf[k]; }
+#pragma unroll
+            for(int k = 0; k < 9; k++) { a.dst[(C_F + k) * a.npad + j] = Fn[k]; a.dst[(C_B + k) * a.npad + j] = Bn[k]; }
+            a.dst_attr[j] = a.src_attr[i];
+            a.dst_pid[j] = a.src_pid[i];
+            a.keys_next[j] = key;
+        }
+        __syncthreads();
+    }
+}
+
+// Reference layout <-> sorted SoA
+template<class T> __global__ void k_scatter_in(FastArgs a, const T* X, const T* V, const T* F, const T* B, const T* m,
+    const T* vol, const T* mu, const T* la, const uint8_t* valid, uint8_t* valid_slot)
+{
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+        float* d = a.dst;
+        for(int k = 0; k < 3; k++) { d[(C_X + k) * a.npad + p] = (float)X[p * 3 + k]; d[(C_V + k) * a.npad + p] = (float)V[p * 3 + k]; }
+        for(int k = 0; k < 9; k++) { d[(C_F + k) * a.npad + p] = (float)F[p * 9 + k]; d[(C_B + k) * a.npad + p] = (float)B[p * 9 + k]; }
+        a.dst_attr[p] = make_float4((float)m[p], (float)vol[p], (float)mu[p], (float)la[p]);
+        a.dst_pid[p] = (int)p;
+        valid_slot[p] = valid ? valid[p] : 1;
+    }
+}
+
+template<class T> __global__ void k_gather_out(FastArgs a, const uint32_t* keys, T* X, T* V, T* F, T* B, uint8_t* valid)
+{
+    for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < a.n; j += (int64_t)gridDim.x * blockDim.x) {
+        int p = a.src_pid[j];
+        const float* s = a.src;
+        for(int k = 0; k < 3; k++) {
+            if(X) X[(int64_t)p * 3 + k] = (T)s[(C_X + k) * a.npad + j];
+            if(V) V[(int64_t)p * 3 + k] = (T)s[(C_V + k) * a.npad + j];
+        }
+        for(int k = 0; k < 9; k++) {
+            if(F) F[(int64_t)p * 9 + k] = (T)s[(C_F + k) * a.npad + j];
+            if(B) B[(int64_t)p * 9 + k] = (T)s[(C_B + k) * a.npad + j];
+        }
+        if(valid) valid[p] = keys[j] != SENTINEL;
+    }
+}
+
+__global__ void k_grid_out(FastArgs a, const uint32_t* list, uint32_t count, double* m, double* v, double* vf, int G0, int G1, int G2)
+{
+    // one node block per CTA of 64 threads
+    for(uint32_t w = blockIdx.x; w < count; w += gridDim.x) {
+        uint32_t nb = list[w];
+        int nz = nb % a.NN[2], r = nb / a.NN[2], ny = r % a.NN[1], nx = r / a.NN[1];
+        int t = threadIdx.x;
+        int qx = 4 * nx + (t >> 4), qy = 4 * ny + ((t >> 2) & 3), qz = 4 * nz + (t & 3);
+        if(qx >= G0 || qy >= G1 || qz >= G2) continue;
+        int64_t q = node_index(a, qx, qy, qz);
+        int64_t o = ((int64_t)qx * G1 + qy) * G2 + qz;
+        float4 p0 = a.vel[2 * q], p1 = a.vel[2 * q + 1];
+        if(m) m[o] = p1.z;
+        if(v) { v[3 * o] = p0.x; v[3 * o + 1] = p0.y; v[3 * o + 2] = p0.z; }
+        if(vf) { vf[3 * o] = p0.w; vf[3 * o + 1] = p1.x; vf[3 * o + 2] = p1.y; }
+    }
+}
+
+__global__ void k_count_keys(const uint32_t* keys, int64_t n, unsigned long long* out)
+{
+    unsigned long long c = 0;
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) c += keys[i] != SENTINEL;
+    atomicAdd(out, c);
+}
+
+FastArgs make_args(mpm_handle* h, double dt)
+{
+    FastArgs a;
+    FastState& f = h->fast;
+    a.sp = h->sp;
+    a.n = f.n;
+    a.npad = f.npad;
+    int c = f.cur, o = 1 - f.cur;
+    a.src = f.soa[c]; a.src_attr = f.attr[c]; a.src_pid = f.pid[c];
+    a.dst = f.soa[o]; a.dst_attr = f.attr[o]; a.dst_pid = f.pid[o];
+    a.perm = f.perm;
+    a.sorted_keys = f.sorted_keys;
+    a.keys_next = f.keys;
+    a.bstart = f.bstart; a.bend = f.bend; a.active = f.active;
+    a.nb_flag = f.nb_flag; a.nb_list = f.nb_list; a.counters = f.counters;
+    a.acc = f.acc; a.vel = f.vel;
+    for(int k = 0; k < 3; k++) {
+        a.GA[k] = 4 * f.NN[k];
+        a.NB[k] = f.NB[k];
+        a.NN[k] = f.NN[k];
+        a.dmin[k] = (float)h->sp.dmin[k];
+        a.dmax[k] = (float)h->sp.dmax[k];
+        a.dx[k] = (float)h->sp.dx[k];
+        a.inv[k] = (float)h->sp.inv_dx[k];
+        a.gravity[k] = (float)h->sp.gravity[k];
+    }
+    a.dt = (float)dt;
+    a.flags = h->d_flags;
+    return a;
+}
+
+int grid_stride_blocks(mpm_handle* h, int64_t n, int t)
+{
+    int64_t b = (n + t - 1) / t, cap = (int64_t)h->sm_count * 16;
+    if(b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+constexpr int P2G_THREADS = 128;
+constexpr int G2P_THREADS = 128;
+
+}  // namespace
+
+int fast_alloc(mpm_handle* h, int64_t n)
+{
+    FastState& f = h->fast;
+    if(h->sp.dim != 3) return set_error(h, MPM_ERR_ARG, "the fast path is 3D; use MPM_PATH_PLAIN for 2D");
+    if(n > 0x7fffffffLL) return set_error(h, MPM_ERR_ARG, "more than 2^31-1 particles");
+    if(!f.acc) {
+        int64_t nodes = 1, blocks = 1, nblocks = 1;
+        for(int k = 0; k < 3; k++) {
+            f.NB[k] = (h->sp.counts[k] + 4 + 3) / 4;
+            f.NN[k] = f.NB[k] + 1;
+            f.GP[k] = 4 * f.NB[k] + 2;
+            nodes *= 4 * f.NN[k];
+            blocks *= f.NB[k];
+            nblocks *= f.NN[k];
+        }
+        int bits = 6;
+        while((1LL << bits) <= blocks * 64) bits++;
+        if(bits > 32) return set_error(h, MPM_ERR_ARG, "grid too large for 32-bit cell keys");
+        f.key_bits = bits;
+        MPM_CUDA(h, cudaMalloc(&f.acc, nodes * sizeof(float4)));
+        MPM_CUDA(h, cudaMalloc(&f.vel, nodes * 2 * sizeof(float4)));
+        MPM_CUDA(h, cudaMemsetAsync(f.acc, 0, nodes * sizeof(float4), h->stream));
+        MPM_CUDA(h, cudaMemsetAsync(f.vel, 0, nodes * 2 * sizeof(float4), h->stream));
+        MPM_CUDA(h, cudaMalloc(&f.bstart, blocks * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.bend, blocks * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.active, blocks * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.nb_flag, nblocks * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.nb_list, nblocks * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMemsetAsync(f.nb_flag, 0, nblocks * sizeof(uint32_t), h->stream));
+        MPM_CUDA(h, cudaMalloc(&f.counters, CNT_COUNT * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_p2g<P2G_THREADS>, P2G_THREADS, 0);
+        f.p2g_ctas = h->sm_count * (occ > 0 ? occ : 1);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_g2p<G2P_THREADS>, G2P_THREADS, 0);
+        f.g2p_ctas = h->sm_count * (occ > 0 ? occ : 1);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_grid, 64, 0);
+        f.grid_ctas = h->sm_count * (occ > 0 ? occ : 1);
+    }
+    if(f.n != n || !f.soa[0]) {
+        for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); }
+        uint32_t* ps[] = {f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, f.sort_hist, f.sort_part};
+        for(uint32_t* p: ps) cudaFree(p);
+        int64_t np = ((n ? n : 1) + 31) / 32 * 32;
+        f.npad = np;
+        for(int b = 0; b < 2; b++) {
+            MPM_CUDA(h, cudaMalloc(&f.soa[b], NCOMP * np * sizeof(float)));
+            MPM_CUDA(h, cudaMalloc(&f.attr[b], np * sizeof(float4)));
+            MPM_CUDA(h, cudaMalloc(&f.pid[b], np * sizeof(int)));
+        }
+        MPM_CUDA(h, cudaMalloc(&f.keys, np * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.sorted_keys, np * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.perm, np * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.sort_keys_alt, np * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.sort_vals_alt, np * sizeof(uint32_t)));
+        f.sort_tiles = mpm_sort::tiles_for(np);
+        MPM_CUDA(h, cudaMalloc(&f.sort_hist, mpm_sort::hist_words(np) * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.sort_part, mpm_sort::part_words(np) * sizeof(uint32_t)));
+        f.n = n;
+    }
+    return MPM_OK;
+}
+
+void fast_free(mpm_handle* h)
+{
+    FastState& f = h->fast;
+    for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); }
+    void* ps[] = {f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, f.sort_hist, f.sort_part,
+                  f.bstart, f.bend, f.active, f.nb_flag, f.nb_list, f.counters, f.acc, f.vel};
+    for(void* p: ps) cudaFree(p);
+    f = FastState();
+}
+
+int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
+{
+    int rc = fast_alloc(h, v->n);
+    if(rc) return rc;
+    FastState& f = h->fast;
+    int64_t n = v->n;
+    f.cur = 0;
+    f.keys_ready = false;
+    if(!n) return MPM_OK;
+    // stage caller arrays on the device if needed
+    bool dev = v->on_device != 0;
+    size_t e = v->dtype == MPM_FP64 ? 8 : 4;
+    const void* src[8] = {v->X, v->V, v->F, v->B, v->mass, v->volume, v->mu, v->lambda};
+    int64_t cnt[8] = {3 * n, 3 * n, 9 * n, 9 * n, n, n, n, n};
+    void* dptr[8] = {};
+    void* owned[8] = {};
+    for(int i = 0; i < 8; i++) {
+        if(!src[i]) return set_error(h, MPM_ERR_ARG, "null particle array");
+        if(dev) dptr[i] = const_cast<void*>(src[i]);
+        else {
+            MPM_CUDA(h, cudaMallocAsync(&owned[i], cnt[i] * e, h->stream));
+            MPM_CUDA(h, cudaMemcpyAsync(owned[i], src[i], cnt[i] * e, cudaMemcpyHostToDevice, h->stream));
+            dptr[i] = owned[i];
+        }
+    }
+    uint8_t *dvalid = nullptr, *valid_slot = nullptr;
+    if(v->valid) {
+        if(dev) dvalid = v->valid;
+        else {
+            MPM_CUDA(h, cudaMallocAsync((void**)&dvalid, n, h->stream));
+            MPM_CUDA(h, cudaMemcpyAsync(dvalid, v->valid, n, cudaMemcpyHostToDevice, h->stream));
+        }
+    }
+    MPM_CUDA(h, cudaMallocAsync((void**)&valid_slot, n, h->stream));
+    FastArgs a = make_args(h, 0.0);
+    a.dst = f.soa[0]; a.dst_attr = f.attr[0]; a.dst_pid = f.pid[0];
+    int blocks = grid_stride_blocks(h, n, 256);
+    if(e == 8)
+        k_scatter_in<double><<<blocks, 256, 0, h->stream>>>(a, (const double*)dptr[0], (const double*)dptr[1], (const double*)dptr[2],
+            (const double*)dptr[3], (const double*)dptr[4], (const double*)dptr[5], (const double*)dptr[6], (const double*)dptr[7], dvalid, valid_slot);
+    else
+        k_scatter_in<float><<<blocks, 256, 0, h->stream>>>(a, (const float*)dptr[0], (const float*)dptr[1], (const float*)dptr[2],
+            (const float*)dptr[3], (const float*)dptr[4], (const float*)dptr[5], (const float*)dptr[6], (const float*)dptr[7], dvalid, valid_slot);
+    MPM_LAUNCHED(h, "k_scatter_in");
+    a = make_args(h, 0.0);
+    k_init_keys<<<blocks, 256, 0, h->stream>>>(a, valid_slot);
+    MPM_LAUNCHED(h, "k_init_keys");
+    for(int i = 0; i < 8; i++) if(owned[i]) MPM_CUDA(h, cudaFreeAsync(owned[i], h->stream));
+    if(v->valid && !dev) MPM_CUDA(h, cudaFreeAsync(dvalid, h->stream));
+    MPM_CUDA(h, cudaFreeAsync(valid_slot, h->stream));
+    f.keys_ready = true;
+    return MPM_OK;
+}
+
+int fast_get_particles(mpm_handle* h, mpm_particles_view* v)
+{
+    FastState& f = h->fast;
+    if(v->n != f.n) return set_error(h, MPM_ERR_ARG, "particle count differs from mpm_set_particles");
+    int64_t n = v->n;
+    if(!n) return MPM_OK;
+    bool dev = v->on_device != 0;
+    size_t e = v->dtype == MPM_FP64 ? 8 : 4;
+    void* dst[4] = {v->X, v->V, v->F, v->B};
+    int64_t cnt[4] = {3 * n, 3 * n, 9 * n, 9 * n};
+    void* dptr[4] = {};
+    for(int i = 0; i < 4; i++) {
+        if(!dst[i]) continue;
+        if(dev) dptr[i] = dst[i];
+        else MPM_CUDA(h, cudaMallocAsync(&dptr[i], cnt[i] * e, h->stream));
+    }
+    uint8_t* dvalid = nullptr;
+    if(v->valid) {
+        if(dev) dvalid = v->valid;
+        else MPM_CUDA(h, cudaMallocAsync((void**)&dvalid, n, h->stream));
+    }
+    FastArgs a = make_args(h, 0.0);
+    int blocks = grid_stride_blocks(h, n, 256);
+    if(e == 8) k_gather_out<double><<<blocks, 256, 0, h->stream>>>(a, f.keys, (double*)dptr[0], (double*)dptr[1], (double*)dptr[2], (double*)dptr[3], dvalid);
+    else k_gather_out<float><<<blocks, 256, 0, h->stream>>>(a, f.keys, (float*)dptr[0], (float*)dptr[1], (float*)dptr[2], (float*)dptr[3], dvalid);
+    MPM_LAUNCHED(h, "k_gather_out");
+    if(!dev) {
+        for(int i = 0; i < 4; i++) {
+            if(!dst[i]) continue;
+            MPM_CUDA(h, cudaMemcpyAsync(dst[i], dptr[i], cnt[i] * e, cudaMemcpyDeviceToHost, h->stream));
+            MPM_CUDA(h, cudaFreeAsync(dptr[i], h->stream));
+        }
+        if(dvalid) {
+            MPM_CUDA(h, cudaMemcpyAsync(v->valid, dvalid, n, cudaMemcpyDeviceToHost, h->stream));
+            MPM_CUDA(h, cudaFreeAsync(dvalid, h->stream));
+        }
+    }
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+// sort + ranges + tail copy + P2G (with fused stress and gravity)
+int fast_p2g(mpm_handle* h, double dt, double)
+{
+    FastState& f = h->fast;
+    if(!f.keys_ready) return set_error(h, MPM_ERR_STATE, "particles not set");
+    int64_t n = f.n;
+    if(!n) return MPM_OK;
+    uint32_t *ko = nullptr, *vo = nullptr;
+    int slot = timer_begin(h, "fast_sort");
+    // sort keys (in f.keys, left intact for get_particles) into sorted_keys / perm
+    MPM_CUDA(h, cudaMemcpyAsync(f.sorted_keys, f.keys, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    cudaError_t e = mpm_sort::radix_sort(f.sorted_keys, f.sort_keys_alt, f.perm, f.sort_vals_alt, n, f.key_bits,
+                                         f.sort_hist, f.sort_part, h->stream, &ko, &vo);
+    if(e != cudaSuccess) return check_cuda(h, e, "radix_sort");
+    if(ko != f.sorted_keys) MPM_CUDA(h, cudaMemcpyAsync(f.sorted_keys, ko, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    if(vo != f.perm) MPM_CUDA(h, cudaMemcpyAsync(f.perm, vo, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    timer_end(h, slot);
+    FastArgs a = make_args(h, dt);
+    slot = timer_begin(h, "fast_ranges");
+    MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
+    k_ranges<<<grid_stride_blocks(h, n, 256), 256, 0, h->stream>>>(a);
+    MPM_LAUNCHED(h, "k_ranges");
+    k_tail<<<h->sm_count * 2, 256, 0, h->stream>>>(a);
+    MPM_LAUNCHED(h, "k_tail");
+    timer_end(h, slot);
+    slot = timer_begin(h, "fast_p2g");
+    k_p2g<P2G_THREADS><<<f.p2g_ctas, P2G_THREADS, 0, h->stream>>>(a);
+    timer_end(h, slot);
+    MPM_LAUNCHED(h, "k_p2g");
+    return MPM_OK;
+}
+
+int fast_forces(mpm_handle* h, double dt, double)
+{
+    FastState& f = h->fast;
+    if(!f.n) return MPM_OK;
+    FastArgs a = make_args(h, dt);
+    int slot = timer_begin(h, "fast_grid");
+    k_grid<<<f.grid_ctas, 64, 0, h->stream>>>(a);
+    timer_end(h, slot);
+    MPM_LAUNCHED(h, "k_grid");
+    return MPM_OK;
+}
+
+int fast_g2p(mpm_handle* h, double dt, double)
+{
+    FastState& f = h->fast;
+    if(!f.n) return MPM_OK;
+    FastArgs a = make_args(h, dt);
+    int slot = timer_begin(h, "fast_g2p");
+    k_g2p<G2P_THREADS><<<f.g2p_ctas, G2P_THREADS, 0, h->stream>>>(a);
+    timer_end(h, slot);
+    MPM_LAUNCHED(h, "k_g2p");
+    f.cur = 1 - f.cur;
+    return MPM_OK;
+}
+
+int fast_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf)
+{
+    FastState& f = h->fast;
+    if(v0) return set_error(h, MPM_ERR_ARG, "velocity after P2G is not kept on the fast path");
+    int G[3];
+    int64_t gn = 1;
+    for(int k = 0; k < 3; k++) { G[k] = h->sp.counts[k] + 2 * MPM_GHOST; gn *= G[k]; }
+    uint32_t count = 0;
+    MPM_CUDA(h, cudaMemcpyAsync(&count, f.counters + CNT_NODE_BLOCKS, sizeof(count), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    double *dm = nullptr, *dv = nullptr, *dvf = nullptr;
+    if(m) { MPM_CUDA(h, cudaMallocAsync((void**)&dm, gn * 8, h->stream)); MPM_CUDA(h, cudaMemsetAsync(dm, 0, gn * 8, h->stream)); }
+    if(v) { MPM_CUDA(h, cudaMallocAsync((void**)&dv, gn * 24, h->stream)); MPM_CUDA(h, cudaMemsetAsync(dv, 0, gn * 24, h->stream)); }
+    if(vf) { MPM_CUDA(h, cudaMallocAsync((void**)&dvf, gn * 24, h->stream)); MPM_CUDA(h, cudaMemsetAsync(dvf, 0, gn * 24, h->stream)); }
+    FastArgs a = make_args(h, 0.0);
+    if(count) {
+        k_grid_out<<<count < 65535u ? count : 65535u, 64, 0, h->stream>>>(a, f.nb_list, count, dm, dv, dvf, G[0], G[1], G[2]);
+        MPM_LAUNCHED(h, "k_grid_out");
+    }
+    if(m) { MPM_CUDA(h, cudaMemcpyAsync(m, dm, gn * 8, cudaMemcpyDeviceToHost, h->stream)); MPM_CUDA(h, cudaFreeAsync(dm, h->stream)); }
+    if(v) { MPM_CUDA(h, cudaMemcpyAsync(v, dv, gn * 24, cudaMemcpyDeviceToHost, h->stream)); MPM_CUDA(h, cudaFreeAsync(dv, h->stream)); }
+    if(vf) { MPM_CUDA(h, cudaMemcpyAsync(vf, dvf, gn * 24, cudaMemcpyDeviceToHost, h->stream)); MPM_CUDA(h, cudaFreeAsync(dvf, h->stream)); }
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+int fast_count_valid(mpm_handle* h, int64_t* c)
+{
+    FastState& f = h->fast;
+    unsigned long long* d = nullptr;
+    MPM_CUDA(h, cudaMallocAsync(&d, sizeof(*d), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(d, 0, sizeof(*d), h->stream));
+    if(f.n) {
+        k_count_keys<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(f.keys, f.n, d);
+        MPM_LAUNCHED(h, "k_count_keys");
+    }
+    unsigned long long r = 0;
+    MPM_CUDA(h, cudaMemcpyAsync(&r, d, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaFreeAsync(d, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    *c = (int64_t)r;
+    return MPM_OK;
+}
+
+int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm)
+{
+    FastState& f = h->fast;
+    size_t bytes = f.n * sizeof(uint32_t);
+    if(slot_keys) MPM_CUDA(h, cudaMemcpyAsync(slot_keys, f.keys, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if(sorted_keys) MPM_CUDA(h, cudaMemcpyAsync(sorted_keys, f.sorted_keys, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if(perm) MPM_CUDA(h, cudaMemcpyAsync(perm, f.perm, bytes, cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm)
+{
+    if(n < 0 || bits < 1 || bits > 32 || (n && (!keys || !sorted_keys || !perm))) return MPM_ERR_ARG;
+    if(n > 0x7fffffffLL) return MPM_ERR_ARG;
+    if(!n) return MPM_OK;
+    cudaStream_t st;
+    if(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return MPM_ERR_CUDA;
+    uint32_t *k = nullptr, *ka = nullptr, *v = nullptr, *va = nullptr, *hist = nullptr, *part = nullptr;
+    int rc = MPM_OK;
+    size_t b = n * sizeof(uint32_t);
+    if(cudaMalloc(&k, b) || cudaMalloc(&ka, b) || cudaMalloc(&v, b) || cudaMalloc(&va, b) ||
+       cudaMalloc(&hist, mpm_sort::hist_words(n) * 4) || cudaMalloc(&part, mpm_sort::part_words(n) * 4)) rc = MPM_ERR_NOMEM;
+    if(!rc) {
+        uint32_t *ko, *vo;
+        cudaMemcpyAsync(k, keys, b, cudaMemcpyHostToDevice, st);
+        if(mpm_sort::radix_sort(k, ka, v, va, n, bits, hist, part, st, &ko, &vo) != cudaSuccess) rc = MPM_ERR_CUDA;
+        else {
+            cudaMemcpyAsync(sorted_keys, ko, b, cudaMemcpyDeviceToHost, st);
+            cudaMemcpyAsync(perm, vo, b, cudaMemcpyDeviceToHost, st);
+            if(cudaStreamSynchronize(st) != cudaSuccess) rc = MPM_ERR_CUDA;
+        }
+    }
+    cudaFree(k); cudaFree(ka); cudaFree(v); cudaFree(va); cudaFree(hist); cudaFree(part);
+    cudaStreamDestroy(st);
+    return rc;
+}

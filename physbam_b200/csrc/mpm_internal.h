@@ -1,0 +1,149 @@
+// Handle layout and internal interfaces of libphysbam_mpm.so (not public).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "mpm_math.cuh"
+#include "mpm_types.h"
+
+// Everything a kernel needs about the scene, passed by value.
+struct SceneParams {
+    int dim;
+    int counts[3];
+    double dmin[3], dmax[3], dx[3], inv_dx[3];
+    int model;
+    double gravity[3];
+    int nobj;
+    mpm::DevObject objs[MPM_MAX_OBJECTS];
+};
+
+// Reference-layout device arrays for the plain path (one thread per particle).
+struct PlainState {
+    int64_t n = 0, gn = 0;
+    void *X = nullptr, *V = nullptr, *F = nullptr, *B = nullptr;
+    void *mass = nullptr, *vol = nullptr, *mu = nullptr, *lam = nullptr, *pft = nullptr;
+    uint8_t* valid = nullptr;
+    void *gm = nullptr, *gmv = nullptr, *gv0 = nullptr, *gf = nullptr, *gv = nullptr, *gvf = nullptr;
+};
+
+// Fast path: cell-sorted SoA particles (double-buffered), block-sparse grid.
+struct FastState {
+    int64_t n = 0, npad = 0;
+    int GP[3] = {0, 0, 0};   // node extent of the internal grid (>= G+6, = 4*NB+2)
+    int NB[3] = {0, 0, 0};   // particle blocks (4^3 cells) per axis
+    int NN[3] = {0, 0, 0};   // node blocks (4^3 nodes) per axis
+    int key_bits = 0;
+    int cur = 0;
+    float* soa[2] = {nullptr, nullptr};       // 24 * npad floats: x y z, vx vy vz, F0..8, B0..8
+    float4* attr[2] = {nullptr, nullptr};     // mass, volume, mu, lambda
+    int* pid[2] = {nullptr, nullptr};         // caller's particle index
+    uint32_t* keys = nullptr;                 // keys of the current buffer's slots
+    uint32_t* sorted_keys = nullptr;
+    uint32_t* perm = nullptr;                 // sorted position -> slot in the current buffer
+    uint32_t* sort_keys_alt = nullptr;
+    uint32_t* sort_vals_alt = nullptr;
+    uint32_t* sort_hist = nullptr;            // 4 passes * 256 * tiles
+    uint32_t* sort_part = nullptr;            // scan partials
+    int64_t sort_tiles = 0;
+    uint32_t* bstart = nullptr;               // per particle block
+    uint32_t* bend = nullptr;
+    uint32_t* active = nullptr;               // active particle blocks
+    uint32_t* nb_flag = nullptr;              // node-block touched this substep
+    uint32_t* nb_list = nullptr;              // touched node blocks
+    uint32_t* counters = nullptr;             // see FastCounter
+    float4* acc = nullptr;                    // P2G accumulator: momentum+dt*force (xyz), mass (w)
+    float4* vel = nullptr;                    // per node 2 x float4: vnew.xyz, vfric.x | vfric.yz, mass, 0
+    bool keys_ready = false;
+    int p2g_ctas = 0, g2p_ctas = 0, grid_ctas = 0;
+};
+
+enum FastCounter {
+    CNT_ACTIVE_BLOCKS = 0,
+    CNT_ACTIVE_PARTICLES = 1,
+    CNT_P2G_WORK = 2,
+    CNT_G2P_WORK = 3,
+    CNT_NODE_BLOCKS = 4,
+    CNT_GRID_WORK = 5,
+    CNT_FALLBACK = 6,
+    CNT_COUNT = 8
+};
+
+struct KernelTimer {
+    std::string name;
+    double ms = 0;
+    int64_t launches = 0;
+};
+
+struct PendingEvent {
+    int timer;
+    cudaEvent_t start, stop;
+};
+
+struct mpm_handle {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    mpm_grid_desc grid{};
+    mpm_model_desc model{};
+    SceneParams sp{};
+    int64_t n = 0;
+    bool have_particles = false;
+    unsigned* d_flags = nullptr;
+    PlainState plain;
+    FastState fast;
+    // timing
+    bool timing = false;
+    std::vector<KernelTimer> timers;
+    std::vector<PendingEvent> pending;
+    std::vector<cudaEvent_t> event_pool;
+    // one captured substep per particle-buffer parity (the fast path swaps buffers)
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    double graph_dt = 0;
+    std::string last_error;
+};
+
+// timing helpers (mpm_capi.cu)
+int timer_begin(mpm_handle* h, const char* name);
+void timer_end(mpm_handle* h, int slot);
+
+// plain path (mpm_plain.cu)
+int plain_alloc(mpm_handle* h, int64_t n);
+void plain_free(mpm_handle* h);
+int plain_set_particles(mpm_handle* h, const mpm_particles_view* v);
+int plain_get_particles(mpm_handle* h, mpm_particles_view* v);
+int plain_p2g(mpm_handle* h, double dt, double time);
+int plain_forces(mpm_handle* h, double dt, double time);
+int plain_g2p(mpm_handle* h, double dt, double time);
+int plain_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf);
+int plain_count_valid(mpm_handle* h, int64_t* c);
+
+// fast path (mpm_fast.cu)
+int fast_alloc(mpm_handle* h, int64_t n);
+void fast_free(mpm_handle* h);
+int fast_set_particles(mpm_handle* h, const mpm_particles_view* v);
+int fast_get_particles(mpm_handle* h, mpm_particles_view* v);
+int fast_p2g(mpm_handle* h, double dt, double time);
+int fast_forces(mpm_handle* h, double dt, double time);
+int fast_g2p(mpm_handle* h, double dt, double time);
+int fast_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf);
+int fast_count_valid(mpm_handle* h, int64_t* c);
+int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm);
+int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm);
+
+// helpers
+int set_error(mpm_handle* h, int code, const std::string& msg);
+int check_cuda(mpm_handle* h, cudaError_t e, const char* what);
+#define MPM_CUDA(h, call)                                   \
+    do {                                                    \
+        cudaError_t e__ = (call);                           \
+        if(e__ != cudaSuccess) return check_cuda(h, e__, #call); \
+    } while(0)
+#define MPM_LAUNCHED(h, what)                               \
+    do {                                                    \
+        cudaError_t e__ = cudaGetLastError();               \
+        if(e__ != cudaSuccess) return check_cuda(h, e__, what); \
+    } while(0)

@@ -1,0 +1,525 @@
+// Device math for the explicit MPM substep: quadratic B-spline weights, the
+// 3x3 / 2x2 signed SVD, the two constitutive models, and the static collision
+// objects.  Templated on the scalar type so the FP64 path and the FP64
+// fallbacks inside the FP32 path share one implementation.
+//
+// Matrices are column-major, a[i + d*j], the layout of PhysBAM's MATRIX<T,d>
+// (Core/Matrices/MATRIX_3X3.h:115-119).
+#pragma once
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mpm_types.h"
+
+namespace mpm {
+
+template<class T> struct Lim;
+template<> struct Lim<double> { static constexpr double eps = DBL_EPSILON; };
+template<> struct Lim<float> { static constexpr float eps = FLT_EPSILON; };
+
+template<class T> __host__ __device__ __forceinline__ T sqr(T x) { return x * x; }
+
+// ---------------------------------------------------------------------------
+// Quadratic B-spline weights.
+// PARTICLE_GRID_WEIGHTS_SPLINE<TV,2>::Compute_Precompute_Data / Compute_Weights
+// (Hybrid_Methods/Iterators/PARTICLE_GRID_WEIGHTS_SPLINE.cpp:93-105,133-139):
+// base = Cell(X - dX), x = (X - Center(base)) / dX, and per axis
+//   w0 = .5 (x-1.5)^2, w1 = .75 - (x-1)^2, w2 = .5 (x-2.5)^2  with derivatives / dX.
+// ---------------------------------------------------------------------------
+template<class T> struct Axis {
+    int base;
+    T w[3], dw[3];
+};
+
+template<class T> __device__ __forceinline__ Axis<T> spline_axis(T X, T dmin, T dx, T inv)
+{
+    Axis<T> a;
+    T y = X - dx;
+    a.base = (int)floor((y - dmin) * inv);
+    T c = dmin + ((T)a.base + (T).5) * dx;
+    T x = (X - c) * inv;
+    a.w[0] = (T).5 * sqr(x - (T)1.5);
+    a.dw[0] = (x - (T)1.5) * inv;
+    x -= (T)1;
+    a.w[1] = -x * x + (T).75;
+    a.dw[1] = (T)-2 * x * inv;
+    x -= (T)1;
+    a.w[2] = (T).5 * sqr(x + (T)1.5);
+    a.dw[2] = (x + (T)1.5) * inv;
+    return a;
+}
+
+// ---------------------------------------------------------------------------
+// Signed SVD, U and V rotations, the smallest singular value possibly
+// negative.  3x3: implicit-shift QR of Gast, Fu, Jiang & Teran (2016,
+// "Implicit-shifted Symmetric QR Singular Value Decomposition of 3x3
+// Matrices", UCLA tech report), the method the reference uses
+// (Core/Matrices/MATRIX_3X3.cpp:202-236).  2x2: indefinite polar
+// decomposition then a symmetric eigenproblem (MATRIX_2X2.h:313-322,
+// SYMMETRIC_MATRIX_2X2.h:364-375).
+// ---------------------------------------------------------------------------
+#define M3(A, i, j) (A)[(i) + 3 * (j)]
+
+template<class T> __device__ __forceinline__ void givens(T a, T b, T g[2])
+{
+    T m = sqrt(a * a + b * b);
+    if(m != 0) { T s = (T)1 / m; g[0] = a * s; g[1] = -b * s; }
+    else { g[0] = 1; g[1] = 0; }
+}
+template<class T> __device__ __forceinline__ void apply_l(T* A, const T g[2], int i, int j)
+{
+#pragma unroll
+    for(int c = 0; c < 3; c++) {
+        T v = M3(A, i, c), w = M3(A, j, c);
+        M3(A, i, c) = g[0] * v + g[1] * w;
+        M3(A, j, c) = g[0] * w - g[1] * v;
+    }
+}
+template<class T> __device__ __forceinline__ void apply_r(T* A, const T g[2], int i, int j)
+{
+#pragma unroll
+    for(int r = 0; r < 3; r++) {
+        T v = M3(A, r, i), w = M3(A, r, j);
+        M3(A, r, i) = g[0] * v + g[1] * w;
+        M3(A, r, j) = g[0] * w - g[1] * v;
+    }
+}
+template<class T> __device__ void zero_l(T* U, T* A, int r0, int r1, int c)
+{
+    T g[2];
+    givens(M3(A, r0, c), M3(A, r1, c), g);
+    apply_l(A, g, r1, r0);
+    apply_r(U, g, r1, r0);
+    M3(A, r1, c) = 0;
+}
+template<class T> __device__ void zero_r(T* V, T* A, int c0, int c1, int r)
+{
+    T g[2];
+    givens(M3(A, r, c0), M3(A, r, c1), g);
+    apply_r(A, g, c1, c0);
+    apply_r(V, g, c1, c0);
+    M3(A, r, c1) = 0;
+}
+template<class T> __device__ void zero_chasing(T* U, T* A, T* V)
+{
+    zero_l(U, A, 0, 1, 0);
+    zero_r(V, A, 1, 2, 0);
+    zero_l(U, A, 1, 2, 1);
+}
+template<class T> __device__ void swap_col(T* U, int i, int j)
+{
+#pragma unroll
+    for(int r = 0; r < 3; r++) { T u = M3(U, r, i), v = M3(U, r, j); M3(U, r, i) = v; M3(U, r, j) = -u; }
+}
+template<class T> __device__ void swap_row(T* U, int i, int j)
+{
+#pragma unroll
+    for(int c = 0; c < 3; c++) { T u = M3(U, i, c), v = M3(U, j, c); M3(U, i, c) = v; M3(U, j, c) = -u; }
+}
+template<class T> __device__ void sv_swap(T* U, T* D, T* V, int i, int j)
+{
+    swap_col(U, i, j);
+    swap_col(V, i, j);
+    T t = D[i]; D[i] = D[j]; D[j] = t;
+}
+template<class T> __device__ void flip_sign(T* U, T* D, int i, int j)
+{
+    D[i] = -D[i]; D[j] = -D[j];
+#pragma unroll
+    for(int r = 0; r < 3; r++) { M3(U, r, i) = -M3(U, r, i); M3(U, r, j) = -M3(U, r, j); }
+}
+template<class T> __device__ __forceinline__ int argmax3(T a, T b, T c)
+{
+    return a >= c ? (a >= b ? 0 : 1) : (b >= c ? 1 : 2);
+}
+template<class T> __device__ void sort_sv(T* U, T* D, T* V)
+{
+    int i = argmax3(fabs(D[0]), fabs(D[1]), fabs(D[2]));
+    if(i > 0) sv_swap(U, D, V, 0, i);
+    if(fabs(D[1]) < fabs(D[2])) sv_swap(U, D, V, 1, 2);
+    if(D[0] < 0) flip_sign(U, D, 0, D[1] < 0 ? 1 : 2);
+    else if(D[1] < 0) flip_sign(U, D, 1, 2);
+}
+template<class T> __device__ void sym2_eigen(T x00, T x10, T x11, T l[2], T V[4])
+{
+    T a = (T).5 * (x00 + x11), b = (T).5 * (x00 - x11), c = x10;
+    T c2 = sqr(c), m = sqrt(sqr(b) + c2), k = x00 * x11 - c2;
+    if(a >= 0) { l[0] = a + m; l[1] = l[0] != 0 ? k / l[0] : 0; }
+    else { l[1] = a - m; l[0] = l[1] != 0 ? k / l[1] : 0; }
+    if(l[1] > l[0]) { T t = l[0]; l[0] = l[1]; l[1] = t; }
+    T v0, v1;
+    if(b >= 0) { v0 = m + b; v1 = c; } else { v0 = -c; v1 = b - m; }
+    T n = sqrt(v0 * v0 + v1 * v1);
+    if(n != 0) { T s = (T)1 / n; v0 *= s; v1 *= s; } else { v0 = 1; v1 = 0; }
+    V[0] = v0; V[1] = v1; V[2] = -v1; V[3] = v0;
+}
+template<class T> __device__ void svd2(const T* x, T* U, T* s, T* V)
+{
+    T x03 = x[0] + x[3], cs, sn;
+    if(x03 == 0) { cs = 0; sn = 1; }
+    else { T t = (x[1] - x[2]) / x03; cs = (T)1 / sqrt(1 + t * t); sn = t * cs; }
+    T Q[4] = {cs, sn, -sn, cs};
+    T S00 = Q[0] * x[0] + Q[1] * x[1], S10 = Q[0] * x[2] + Q[1] * x[3], S11 = Q[2] * x[2] + Q[3] * x[3];
+    sym2_eigen(S00, S10, S11, s, V);
+    if(s[1] < 0 && fabs(s[1]) >= fabs(s[0])) {
+        T a = -s[1], b = -s[0];
+        s[0] = a; s[1] = b;
+#pragma unroll
+        for(int i = 0; i < 4; i++) Q[i] = -Q[i];
+        T W0 = V[2], W1 = V[3], W2 = -V[0], W3 = -V[1];
+        V[0] = W0; V[1] = W1; V[2] = W2; V[3] = W3;
+    }
+    U[0] = Q[0] * V[0] + Q[2] * V[1]; U[1] = Q[1] * V[0] + Q[3] * V[1];
+    U[2] = Q[0] * V[2] + Q[2] * V[3]; U[3] = Q[1] * V[2] + Q[3] * V[3];
+}
+template<class T> __device__ void top_block(T* U, T* B, T* V, T* D)
+{
+    T a[4] = {M3(B, 0, 0), M3(B, 1, 0), M3(B, 0, 1), M3(B, 1, 1)}, u[4], d[2], v[4];
+    svd2(a, u, d, v);
+    apply_r(U, u, 0, 1);
+    apply_r(V, v, 0, 1);
+    D[0] = d[0]; D[1] = d[1]; D[2] = M3(B, 2, 2);
+    sort_sv(U, D, V);
+}
+template<class T> __device__ void bot_block(T* U, T* B, T* V, T* D)
+{
+    T a[4] = {M3(B, 1, 1), M3(B, 2, 1), M3(B, 1, 2), M3(B, 2, 2)}, u[4], d[2], v[4];
+    svd2(a, u, d, v);
+    apply_r(U, u, 1, 2);
+    apply_r(V, v, 1, 2);
+    D[0] = M3(B, 0, 0); D[1] = d[0]; D[2] = d[1];
+    sort_sv(U, D, V);
+}
+template<class T> __device__ bool check_tolerances(T* B, T* U, T* D, T* V, T tau)
+{
+    if(fabs(M3(B, 1, 2)) <= tau) { top_block(U, B, V, D); return true; }
+    if(fabs(M3(B, 0, 1)) <= tau) { bot_block(U, B, V, D); return true; }
+    if(fabs(M3(B, 1, 1)) <= tau) {
+        T g[2], o[2];
+        givens(M3(B, 1, 2), M3(B, 2, 2), g);
+        o[0] = -g[1]; o[1] = g[0];
+        apply_l(B, o, 2, 1);
+        apply_r(U, o, 2, 1);
+        top_block(U, B, V, D);
+        return true;
+    }
+    if(fabs(M3(B, 2, 2)) <= tau) {
+        zero_r(V, B, 1, 2, 1);
+        zero_r(V, B, 0, 2, 0);
+        top_block(U, B, V, D);
+        return true;
+    }
+    if(fabs(M3(B, 0, 0)) <= tau) {
+        zero_l(U, B, 1, 0, 1);
+        zero_l(U, B, 2, 0, 2);
+        bot_block(U, B, V, D);
+        return true;
+    }
+    return false;
+}
+template<class T> __device__ bool lazy_sort(T* U, T* B, T* V, int i, int j)
+{
+    if(fabs(M3(B, i, i)) * 100 >= fabs(M3(B, j, j))) return false;
+    swap_row(B, i, j); swap_col(U, i, j); swap_col(B, i, j); swap_col(V, i, j);
+    return true;
+}
+
+// Returns false when the iteration did not converge within max_it sweeps
+// (the reference iterates without bound; a bounded loop keeps the GPU safe).
+template<class T> __device__ bool svd3(const T* F, T* U, T* D, T* V, int max_it = 64)
+{
+    T B[9];
+#pragma unroll
+    for(int i = 0; i < 9; i++) { B[i] = F[i]; U[i] = V[i] = (i % 4 == 0) ? (T)1 : (T)0; }
+    zero_l(U, B, 1, 2, 0);
+    zero_chasing(U, B, V);
+    T fro = 0;
+#pragma unroll
+    for(int i = 0; i < 9; i++) fro += B[i] * B[i];
+    T tau = (T)16 * Lim<T>::eps * fmax((T).5 * sqrt(fro), (T)1);
+    for(int it = 0; it < max_it; it++) {
+        if(check_tolerances(B, U, D, V, tau)) return true;
+        bool ls = lazy_sort(U, B, V, 0, 1);
+        ls |= lazy_sort(U, B, V, 0, 2);
+        ls |= lazy_sort(U, B, V, 1, 2);
+        if(ls) {
+            zero_l(U, B, 1, 2, 0);
+            zero_chasing(U, B, V);
+            if(check_tolerances(B, U, D, V, tau)) return true;
+        }
+        T al0 = M3(B, 0, 0), al1 = M3(B, 1, 1), al2 = M3(B, 2, 2);
+        T be0 = M3(B, 0, 1), be1 = M3(B, 1, 2);
+        T ga0 = al0 * be0, ga1 = al1 * be1;
+        T a0 = al1 * al1 + be0 * be0;
+        T a1 = al2 * al2 + be1 * be1;
+        T b0 = ga1;
+        T d = (T).5 * (a0 - a1);
+        T mu = a1 - b0 * b0 / (d + (d >= 0 ? (T)1 : (T)-1) * sqrt(d * d + b0 * b0));
+        T g[2];
+        givens(al0 * al0 - mu, ga0, g);
+        apply_r(B, g, 1, 0);
+        apply_r(V, g, 1, 0);
+        zero_chasing(U, B, V);
+    }
+    D[0] = M3(B, 0, 0); D[1] = M3(B, 1, 1); D[2] = M3(B, 2, 2);
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Constitutive models on singular values.
+// COROTATED_FIXED::P_From_Strain (Deformables/Constitutive_Models/COROTATED_FIXED.cpp:59-65):
+//   Phat = 2 mu (S - I) + lambda (J - 1) cof(S)
+// NEO_HOOKEAN::P_From_Strain with Clamp_To_Hyperbola (NEO_HOOKEAN.cpp:42-82),
+// failure threshold .25 (the header default the reference's scenes use).
+// ---------------------------------------------------------------------------
+constexpr double kNeoHookeanThreshold = 0.25;
+
+template<class T, int d> __device__ void phat(int model, const T* s, T mu, T la, T* P)
+{
+    T J = d == 2 ? s[0] * s[1] : s[0] * s[1] * s[2];
+    if(model == MPM_COROTATED_FIXED) {
+        T cof[3];
+        if(d == 2) { cof[0] = s[1]; cof[1] = s[0]; }
+        else { cof[0] = s[1] * s[2]; cof[1] = s[0] * s[2]; cof[2] = s[0] * s[1]; }
+        T k = la * (J - 1);
+#pragma unroll
+        for(int a = 0; a < d; a++) P[a] = 2 * mu * (s[a] - 1) + k * cof[a];
+        return;
+    }
+    const T ft = (T)kNeoHookeanThreshold;
+    if(J >= ft) {
+        T c = mu - la * log(J);
+#pragma unroll
+        for(int a = 0; a < d; a++) P[a] = mu * s[a] - c * ((T)1 / s[a]);
+        return;
+    }
+    T Fc[3];
+    if(d == 2) {
+        if(sqr(s[0]) > ft) { Fc[0] = s[0]; Fc[1] = ft / s[0]; }
+        else { Fc[0] = Fc[1] = sqrt(ft); }
+    } else {
+        if(s[0] * s[1] * s[1] > ft) { Fc[0] = s[0]; Fc[1] = s[1]; Fc[2] = ft / (s[0] * s[1]); }
+        else if(s[0] * s[0] * s[0] > ft) { T c = sqrt(ft / s[0]); Fc[0] = s[0]; Fc[1] = Fc[2] = c; }
+        else { Fc[0] = Fc[1] = Fc[2] = cbrt(ft); }
+    }
+    T Fi[3], dF[3], inner = 0;
+#pragma unroll
+    for(int a = 0; a < d; a++) { Fi[a] = (T)1 / Fc[a]; dF[a] = s[a] - Fc[a]; inner += Fi[a] * dF[a]; }
+    T c = mu - la * log(ft);
+#pragma unroll
+    for(int a = 0; a < d; a++) P[a] = mu * s[a] + c * (sqr(Fi[a]) * dF[a] - Fi[a]) + la * inner * Fi[a];
+}
+
+// MPM_FINITE_ELEMENTS::Precompute (Hybrid_Methods/Forces/MPM_FINITE_ELEMENTS.cpp:47-67):
+// PFT = U Phat(S) (F V)^T, i.e. P(F) F^T.  Returns false if the SVD did not converge.
+template<class T, int d> __device__ bool pft_svd(int model, const T* F, T mu, T la, T* PFT)
+{
+    T U[9], V[9], s[3], P[3];
+    bool ok = true;
+    if(d == 2) {
+        svd2(F, U, s, V);
+        phat<T, 2>(model, s, mu, la, P);
+        T FV[4];
+        FV[0] = F[0] * V[0] + F[2] * V[1]; FV[1] = F[1] * V[0] + F[3] * V[1];
+        FV[2] = F[0] * V[2] + F[2] * V[3]; FV[3] = F[1] * V[2] + F[3] * V[3];
+        T PT[4] = {P[0] * FV[0], P[1] * FV[2], P[0] * FV[1], P[1] * FV[3]};
+        PFT[0] = U[0] * PT[0] + U[2] * PT[1]; PFT[1] = U[1] * PT[0] + U[3] * PT[1];
+        PFT[2] = U[0] * PT[2] + U[2] * PT[3]; PFT[3] = U[1] * PT[2] + U[3] * PT[3];
+        return true;
+    }
+    ok = svd3(F, U, s, V);
+    phat<T, 3>(model, s, mu, la, P);
+    T FV[9], PT[9];
+#pragma unroll
+    for(int j = 0; j < 3; j++)
+#pragma unroll
+        for(int i = 0; i < 3; i++)
+            FV[i + 3 * j] = F[i] * V[3 * j] + F[i + 3] * V[3 * j + 1] + F[i + 6] * V[3 * j + 2];
+#pragma unroll
+    for(int i = 0; i < 3; i++)
+#pragma unroll
+        for(int j = 0; j < 3; j++) PT[i + 3 * j] = P[i] * FV[j + 3 * i];
+#pragma unroll
+    for(int j = 0; j < 3; j++)
+#pragma unroll
+        for(int i = 0; i < 3; i++)
+            PFT[i + 3 * j] = U[i] * PT[3 * j] + U[i + 3] * PT[3 * j + 1] + U[i + 6] * PT[3 * j + 2];
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+// Static collision objects (MPM_COLLISION_OBJECT, Hybrid_Methods/Collisions/
+// MPM_COLLISION_OBJECT.cpp:27-48, with ANALYTIC_IMPLICIT_OBJECT forwarding to
+// RANGE::Signed_Distance / RANGE::Normal, Core/Math_Tools/RANGE.cpp:37-63, or
+// PLANE, Geometry/Basic_Geometry/PLANE.h:52-63).
+// ---------------------------------------------------------------------------
+struct DevObject {
+    int kind, type;
+    double friction;
+    double a[3], b[3];
+};
+
+template<class T, int d> __device__ T object_phi(const DevObject& o, const T* X)
+{
+    if(o.kind == MPM_PLANE) {
+        T s = 0;
+#pragma unroll
+        for(int a = 0; a < d; a++) s += (T)o.a[a] * (X[a] - (T)o.b[a]);
+        return s;
+    }
+    T phi[3], mx = -(T)INFINITY, out = 0;
+    bool all_le = true;
+#pragma unroll
+    for(int a = 0; a < d; a++) {
+        T lo = (T)o.a[a], hi = (T)o.b[a];
+        T len = hi - lo, c = (lo + hi) * (T).5;
+        phi[a] = fabs(X[a] - c) - (T).5 * len;
+        if(!(phi[a] <= 0)) all_le = false;
+        mx = phi[a] > mx ? phi[a] : mx;
+    }
+    if(!all_le) {
+#pragma unroll
+        for(int a = 0; a < d; a++) { T p = phi[a] > 0 ? phi[a] : 0; out += p * p; }
+        return sqrt(out);
+    }
+    return mx;
+}
+
+template<class T, int d> __device__ void object_normal(const DevObject& o, const T* X, T* n)
+{
+    if(o.kind == MPM_PLANE) {
+#pragma unroll
+        for(int a = 0; a < d; a++) n[a] = (T)o.a[a];
+        return;
+    }
+    bool inside = true;
+    T pmax[3], pmin[3];
+#pragma unroll
+    for(int a = 0; a < d; a++) {
+        T lo = (T)o.a[a], hi = (T)o.b[a];
+        if(!(X[a] >= lo && X[a] <= hi)) inside = false;
+        pmax[a] = X[a] - hi;
+        pmin[a] = lo - X[a];
+    }
+    if(inside) {
+        T m[3];
+#pragma unroll
+        for(int a = 0; a < d; a++) m[a] = pmin[a] > pmax[a] ? pmin[a] : pmax[a];
+        int ax = d == 2 ? (m[0] >= m[1] ? 0 : 1) : argmax3(m[0], m[1], m[2]);
+#pragma unroll
+        for(int a = 0; a < d; a++) n[a] = 0;
+        n[ax] = pmax[ax] > pmin[ax] ? (T)1 : (T)-1;
+        return;
+    }
+    T mag = 0;
+#pragma unroll
+    for(int a = 0; a < d; a++) {
+        T p = pmin[a] > pmax[a] ? pmin[a] : pmax[a];
+        n[a] = p > 0 ? (pmax[a] > pmin[a] ? p : -p) : 0;
+        mag += n[a] * n[a];
+    }
+    mag = sqrt(mag);
+    if(mag != 0) {
+        T s = (T)1 / mag;
+#pragma unroll
+        for(int a = 0; a < d; a++) n[a] *= s;
+    } else {
+#pragma unroll
+        for(int a = 0; a < d; a++) n[a] = a == 0 ? (T)1 : (T)0;
+    }
+}
+
+// Grid-node collision projection and Coulomb friction for one node.
+// MPM_OBJECTIVE::Test_Add_Collision / Adjust_For_Collision
+// (Hybrid_Methods/System/MPM_OBJECTIVE.cpp:150-225), MPM_DRIVER::Apply_Friction
+// (Hybrid_Methods/Examples_And_Drivers/MPM_DRIVER.cpp:1064-1094) and the final
+// assembly of Apply_Forces (l.1050-1056), for static objects (velocity 0).
+//
+// In: v0 (grid velocity after P2G), dv (dt/m f), node centre X0.
+// Out: vnew (velocity), vfric (velocity_friction_save).
+template<class T, int d> __device__ void collide_node(const DevObject* objs, int nobj, const T* X0,
+    const T* v0, T* dv, T dt, T* vnew, T* vfric)
+{
+    T dvb[3], nrm[MPM_MAX_OBJECTS][3];
+    int cobj[MPM_MAX_OBJECTS];
+    int ncol = 0;
+    bool stuck = false;
+#pragma unroll
+    for(int a = 0; a < d; a++) dvb[a] = dv[a];
+    for(int j = 0; j < nobj; j++) {
+        const DevObject& o = objs[j];
+        T Vn[3], Xn[3];
+#pragma unroll
+        for(int a = 0; a < d; a++) { Vn[a] = v0[a] + dv[a]; Xn[a] = X0[a] + dt * Vn[a]; }
+        T phi0 = object_phi<T, d>(o, X0);
+        T phi = object_phi<T, d>(o, Xn) - fmin(phi0, (T)0);
+        if(o.type == MPM_STICK && phi0 > 0) continue;
+        if(o.type == MPM_SLIP && phi0 > 0) continue;
+        if(o.type == MPM_SEPARATE && phi > (T)1e-15) continue;
+        if(o.type != MPM_STICK && phi > (T)FLT_MAX) continue;
+        T n[3];
+        object_normal<T, d>(o, Xn, n);
+#pragma unroll
+        for(int a = 0; a < d; a++) nrm[ncol][a] = n[a];
+        cobj[ncol] = j;
+        ncol++;
+#pragma unroll
+        for(int a = 0; a < d; a++) Xn[a] -= phi * n[a];
+#pragma unroll
+        for(int a = 0; a < d; a++) Vn[a] = (Xn[a] - X0[a]) / dt;
+        if(o.type == MPM_STICK) {
+#pragma unroll
+            for(int a = 0; a < d; a++) Vn[a] = 0;
+            stuck = true;
+        }
+#pragma unroll
+        for(int a = 0; a < d; a++) dv[a] = Vn[a] - v0[a];
+    }
+    T gvf[3], v[3];
+#pragma unroll
+    for(int a = 0; a < d; a++) gvf[a] = dv[a];
+    if(nobj) {
+#pragma unroll
+        for(int a = 0; a < d; a++) v[a] = stuck ? (T)0 : v0[a] + dv[a];
+        for(int c = 0; c < ncol; c++) {
+            const T* n = nrm[c];
+            T nf = 0, vn = 0, t[3], tm = 0;
+#pragma unroll
+            for(int a = 0; a < d; a++) nf += n[a] * (dv[a] - dvb[a]);
+#pragma unroll
+            for(int a = 0; a < d; a++) vn += v[a] * n[a];
+#pragma unroll
+            for(int a = 0; a < d; a++) { t[a] = v[a] - vn * n[a]; tm += t[a] * t[a]; }
+            tm = sqrt(tm);
+            if(tm != 0) {
+                T s = (T)1 / tm;
+#pragma unroll
+                for(int a = 0; a < d; a++) t[a] *= s;
+            } else {
+#pragma unroll
+                for(int a = 0; a < d; a++) t[a] = a == 0 ? (T)1 : (T)0;
+            }
+            T kf = (T)objs[cobj[c]].friction * nf;
+            if(tm <= kf) {
+                T vv = 0;
+#pragma unroll
+                for(int a = 0; a < d; a++) vv += v[a] * n[a];
+#pragma unroll
+                for(int a = 0; a < d; a++) v[a] = vv * n[a];
+            } else {
+#pragma unroll
+                for(int a = 0; a < d; a++) v[a] -= kf * t[a];
+            }
+#pragma unroll
+            for(int a = 0; a < d; a++) gvf[a] = v[a] - v0[a];
+        }
+    }
+#pragma unroll
+    for(int a = 0; a < d; a++) {
+        vnew[a] = dv[a] + v0[a];
+        vfric[a] = stuck ? (T)0 : gvf[a] + v0[a];
+    }
+}
+
+}  // namespace mpm

@@ -1,0 +1,556 @@
+// Plain path: a direct GPU port of the reference's explicit substep, one thread
+// per particle (or grid node), global atomics for every scatter, particles in
+// the reference's MPM_PARTICLES layout and arrival order.  Templated on the
+// scalar type; in FP64 it is the baseline the FP32 fast path is measured
+// against, and the path whose grids are checked node-for-node against the
+// reference (it keeps velocity_save and separate force arrays like the
+// reference does).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "mpm_internal.h"
+
+namespace {
+
+using namespace mpm;
+
+template<class T> struct PlainArgs {
+    SceneParams sp;
+    int64_t n, gn;
+    int gs[3];
+    T *X, *V, *F, *B;
+    const T *mass, *vol, *mu, *lam;
+    T* pft;
+    uint8_t* valid;
+    T *gm, *gmv, *gv0, *gf, *gv, *gvf;
+    T dt;
+    unsigned* flags;
+};
+
+template<class T, int d> struct Stencil {
+    Axis<T> ax[3];
+    int base[3];
+};
+
+// Weights of one particle; returns false if the 3^d stencil leaves the ghosted grid.
+template<class T, int d> __device__ bool make_stencil(const PlainArgs<T>& a, const T* X, Stencil<T, d>& s)
+{
+    bool ok = true;
+#pragma unroll
+    for(int k = 0; k < d; k++) {
+        s.ax[k] = spline_axis<T>(X[k], (T)a.sp.dmin[k], (T)a.sp.dx[k], (T)a.sp.inv_dx[k]);
+        s.base[k] = s.ax[k].base;
+        int lo = s.base[k] + MPM_GHOST, hi = lo + 2;
+        if(lo < 0 || hi >= a.gs[k]) ok = false;
+    }
+    return ok;
+}
+
+// Tensor-product node q (RANGE_ITERATOR order, last axis fastest):
+// PARTICLE_GRID_WEIGHTS_SPLINE::Compute (PARTICLE_GRID_WEIGHTS_SPLINE.cpp:33-56).
+template<class T, int d> __device__ __forceinline__ void node(const PlainArgs<T>& a, const Stencil<T, d>& s, int q,
+    int64_t& flat, T& w, T* g, T* Z)
+{
+    int off[3];
+    if(d == 3) { off[0] = q / 9; off[1] = (q / 3) % 3; off[2] = q % 3; }
+    else { off[0] = q / 3; off[1] = q % 3; off[2] = 0; }
+    T aw[3];
+#pragma unroll
+    for(int k = 0; k < d; k++) aw[k] = s.ax[k].w[off[k]];
+    w = aw[0] * aw[1];
+    if(d == 3) w *= aw[2];
+#pragma unroll
+    for(int k = 0; k < d; k++) g[k] = 1;
+#pragma unroll
+    for(int j = 0; j < d; j++) {
+        T dj = s.ax[j].dw[off[j]];
+#pragma unroll
+        for(int i = 0; i < d; i++) g[i] *= i == j ? dj : aw[j];
+    }
+    flat = 0;
+#pragma unroll
+    for(int k = 0; k < d; k++) {
+        int idx = s.base[k] + off[k];
+        flat = flat * a.gs[k] + (idx + MPM_GHOST);
+        Z[k] = (T)a.sp.dmin[k] + ((T)idx + (T).5) * (T)a.sp.dx[k];
+    }
+}
+
+template<class T> __global__ void k_clear(PlainArgs<T> a)
+{
+    const int d = a.sp.dim;
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.gn; i += (int64_t)gridDim.x * blockDim.x) {
+        a.gm[i] = 0;
+        for(int k = 0; k < d; k++) {
+            a.gmv[i * d + k] = 0; a.gf[i * d + k] = 0; a.gv0[i * d + k] = 0;
+            a.gv[i * d + k] = 0; a.gvf[i * d + k] = 0;
+        }
+    }
+}
+
+// MPM_DRIVER::Particle_To_Grid scatter (MPM_DRIVER.cpp:259-271).
+template<class T, int d> __global__ void k_p2g(PlainArgs<T> a)
+{
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if(p >= a.n || !a.valid[p]) return;
+    const T* X = a.X + p * d;
+    Stencil<T, d> s;
+    if(!make_stencil<T, d>(a, X, s)) { atomicOr(a.flags, MPM_FLAG_DOMAIN); return; }
+    T Dp_inv[3];
+#pragma unroll
+    for(int k = 0; k < d; k++) Dp_inv[k] = 4 * (T)a.sp.inv_dx[k] * (T)a.sp.inv_dx[k];
+    const T* Bp = a.B + p * d * d;
+    T mp = a.mass[p];
+    const int nq = d == 3 ? 27 : 9;
+    for(int q = 0; q < nq; q++) {
+        int64_t i;
+        T w, g[3], Z[3];
+        node<T, d>(a, s, q, i, w, g, Z);
+        atomicAdd(a.gm + i, w * mp);
+        T Vn[3], Y[3];
+#pragma unroll
+        for(int k = 0; k < d; k++) { Vn[k] = w * a.V[p * d + k]; Y[k] = (Z[k] - X[k]) * Dp_inv[k]; }
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T sum = 0;
+#pragma unroll
+            for(int c = 0; c < d; c++) sum += Bp[r + d * c] * Y[c];
+            Vn[r] += sum * w;
+        }
+#pragma unroll
+        for(int k = 0; k < d; k++) atomicAdd(a.gmv + i * d + k, mp * Vn[k]);
+    }
+}
+
+// v = mv / m on nodes with mass (MPM_DRIVER.cpp:282-305).
+template<class T> __global__ void k_normalize(PlainArgs<T> a)
+{
+    const int d = a.sp.dim;
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.gn; i += (int64_t)gridDim.x * blockDim.x) {
+        T m = a.gm[i];
+        for(int k = 0; k < d; k++) a.gv0[i * d + k] = m != 0 ? a.gmv[i * d + k] / m : (T)0;
+    }
+}
+
+// MPM_FINITE_ELEMENTS::Precompute (MPM_FINITE_ELEMENTS.cpp:47-67).
+template<class T, int d> __global__ void k_stress(PlainArgs<T> a)
+{
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if(p >= a.n || !a.valid[p]) return;
+    T F[9], PFT[9];
+#pragma unroll
+    for(int e = 0; e < d * d; e++) F[e] = a.F[p * d * d + e];
+    if(!pft_svd<T, d>(a.sp.model, F, a.mu[p], a.lam[p], PFT)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
+#pragma unroll
+    for(int e = 0; e < d * d; e++) a.pft[p * d * d + e] = PFT[e];
+}
+
+// MPM_FINITE_ELEMENTS::Add_Forces (MPM_FINITE_ELEMENTS.cpp:84-99) and
+// MPM_GRAVITY::Add_Forces (MPM_GRAVITY.cpp:62-68) in one pass.
+template<class T, int d> __global__ void k_forces(PlainArgs<T> a)
+{
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if(p >= a.n || !a.valid[p]) return;
+    Stencil<T, d> s;
+    if(!make_stencil<T, d>(a, a.X + p * d, s)) return;
+    T A[9];
+#pragma unroll
+    for(int e = 0; e < d * d; e++) A[e] = a.pft[p * d * d + e] * a.vol[p];
+    T mp = a.mass[p];
+    const int nq = d == 3 ? 27 : 9;
+    for(int q = 0; q < nq; q++) {
+        int64_t i;
+        T w, g[3], Z[3];
+        node<T, d>(a, s, q, i, w, g, Z);
+        T wm = w * mp;
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T sum = 0;
+#pragma unroll
+            for(int c = 0; c < d; c++) sum += A[r + d * c] * g[c];
+            atomicAdd(a.gf + i * d + r, -sum + wm * (T)a.sp.gravity[r]);
+        }
+    }
+}
+
+// Apply_Forces grid update: dv = dt/m f, collision projection, friction,
+// assembly (MPM_DRIVER.cpp:989-1056, MPM_OBJECTIVE.cpp:150-225).
+template<class T, int d> __global__ void k_grid_update(PlainArgs<T> a)
+{
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.gn; i += (int64_t)gridDim.x * blockDim.x) {
+        T m = a.gm[i];
+        if(m == 0) continue;
+        T dv[3], v0[3], X0[3], vn[3], vf[3];
+        T s = a.dt / m;
+        int64_t r = i;
+        int idx[3];
+        for(int k = d - 1; k >= 0; k--) { idx[k] = (int)(r % a.gs[k]) - MPM_GHOST; r /= a.gs[k]; }
+#pragma unroll
+        for(int k = 0; k < d; k++) {
+            dv[k] = s * a.gf[i * d + k];
+            v0[k] = a.gv0[i * d + k];
+            X0[k] = (T)a.sp.dmin[k] + ((T)idx[k] + (T).5) * (T)a.sp.dx[k];
+        }
+        collide_node<T, d>(a.sp.objs, a.sp.nobj, X0, v0, dv, a.dt, vn, vf);
+#pragma unroll
+        for(int k = 0; k < d; k++) { a.gv[i * d + k] = vn[k]; a.gvf[i * d + k] = vf[k]; }
+    }
+}
+
+// MPM_DRIVER::Grid_To_Particle (MPM_DRIVER.cpp:450-515) and
+// Reflect_Or_Invalidate_Particle (l.1219-1239, all sides free).
+template<class T, int d> __global__ void k_g2p(PlainArgs<T> a)
+{
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if(p >= a.n || !a.valid[p]) return;
+    T* X = a.X + p * d;
+    Stencil<T, d> s;
+    if(!make_stencil<T, d>(a, X, s)) return;
+    T Vpic[3] = {0, 0, 0}, Vpf[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Bh[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int nq = d == 3 ? 27 : 9;
+    for(int q = 0; q < nq; q++) {
+        int64_t i;
+        T w, g[3], Z[3];
+        node<T, d>(a, s, q, i, w, g, Z);
+        T vn[3], vf[3], Zp[3], Zm[3];
+#pragma unroll
+        for(int k = 0; k < d; k++) {
+            vn[k] = a.gv[i * d + k];
+            vf[k] = a.gvf[i * d + k];
+            Vpic[k] += w * vn[k];
+            Vpf[k] += w * vf[k];
+            T xi = Z[k] + a.dt * vn[k];
+            Zp[k] = Z[k] + xi;
+            Zm[k] = Z[k] - xi;
+        }
+#pragma unroll
+        for(int c = 0; c < d; c++)
+#pragma unroll
+            for(int r = 0; r < d; r++) G[r + d * c] += vn[r] * g[c];
+        T hw = w / 2;
+#pragma unroll
+        for(int c = 0; c < d; c++)
+#pragma unroll
+            for(int r = 0; r < d; r++) Bh[r + d * c] += hw * (vf[r] * Zp[c] + Zm[r] * vf[c]);
+    }
+    T* Fp = a.F + p * d * d;
+    T A[9], Fn[9];
+#pragma unroll
+    for(int e = 0; e < d * d; e++) A[e] = a.dt * G[e];
+#pragma unroll
+    for(int k = 0; k < d; k++) A[k + d * k] += 1;
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T sum = 0;
+#pragma unroll
+            for(int e = 0; e < d; e++) sum += A[r + d * e] * Fp[e + d * c];
+            Fn[r + d * c] = sum;
+        }
+    T xn[3];
+    bool finite = true;
+#pragma unroll
+    for(int k = 0; k < d; k++) xn[k] = X[k] + a.dt * Vpic[k];
+    T* Bp = a.B + p * d * d;
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++)
+            Bp[r + d * c] = Bh[r + d * c] - (T).5 * (Vpf[r] * (X[c] + xn[c]) + (X[r] - xn[r]) * Vpf[c]);
+#pragma unroll
+    for(int e = 0; e < d * d; e++) { Fp[e] = Fn[e]; finite = finite && isfinite(Fn[e]); }
+    bool keep = true;
+#pragma unroll
+    for(int k = 0; k < d; k++) {
+        X[k] = xn[k];
+        a.V[p * d + k] = Vpf[k];
+        finite = finite && isfinite(xn[k]) && isfinite(Vpf[k]);
+        T eps = Lim<T>::eps * 4 * ((T)a.sp.dmax[k] - (T)a.sp.dmin[k]);
+        if(xn[k] < (T)a.sp.dmin[k] + eps) keep = false;
+        else if(xn[k] > (T)a.sp.dmax[k] - eps) keep = false;
+    }
+    if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); keep = false; }
+    if(!keep) a.valid[p] = 0;
+}
+
+template<class T> __global__ void k_count_valid(const uint8_t* valid, int64_t n, unsigned long long* out)
+{
+    unsigned long long c = 0;
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) c += valid[i] ? 1 : 0;
+    atomicAdd(out, c);
+}
+
+template<class T> PlainArgs<T> args(mpm_handle* h, double dt)
+{
+    PlainArgs<T> a;
+    PlainState& s = h->plain;
+    a.sp = h->sp;
+    a.n = s.n;
+    a.gn = s.gn;
+    for(int k = 0; k < 3; k++) a.gs[k] = k < h->sp.dim ? h->sp.counts[k] + 2 * MPM_GHOST : 1;
+    a.X = (T*)s.X; a.V = (T*)s.V; a.F = (T*)s.F; a.B = (T*)s.B;
+    a.mass = (const T*)s.mass; a.vol = (const T*)s.vol; a.mu = (const T*)s.mu; a.lam = (const T*)s.lam;
+    a.pft = (T*)s.pft; a.valid = s.valid;
+    a.gm = (T*)s.gm; a.gmv = (T*)s.gmv; a.gv0 = (T*)s.gv0; a.gf = (T*)s.gf; a.gv = (T*)s.gv; a.gvf = (T*)s.gvf;
+    a.dt = (T)dt;
+    a.flags = h->d_flags;
+    return a;
+}
+
+int pblocks(int64_t n, int t) { int64_t b = (n + t - 1) / t; return (int)(b < 1 ? 1 : b); }
+int gblocks(mpm_handle* h, int64_t n, int t)
+{
+    int64_t b = (n + t - 1) / t, cap = (int64_t)h->sm_count * 8;
+    if(b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+size_t esize(mpm_handle* h) { return h->model.precision == MPM_FP64 ? 8 : 4; }
+
+template<class T> int p2g_t(mpm_handle* h, double dt)
+{
+    PlainArgs<T> a = args<T>(h, dt);
+    const int t = 128;
+    int slot = timer_begin(h, "plain_clear");
+    k_clear<T><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a);
+    timer_end(h, slot);
+    MPM_LAUNCHED(h, "k_clear");
+    if(a.n) {
+        slot = timer_begin(h, "plain_p2g");
+        if(h->sp.dim == 3) k_p2g<T, 3><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
+        else k_p2g<T, 2><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
+        timer_end(h, slot);
+        MPM_LAUNCHED(h, "k_p2g");
+    }
+    slot = timer_begin(h, "plain_normalize");
+    k_normalize<T><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a);
+    timer_end(h, slot);
+    MPM_LAUNCHED(h, "k_normalize");
+    return MPM_OK;
+}
+
+template<class T> int forces_t(mpm_handle* h, double dt)
+{
+    PlainArgs<T> a = args<T>(h, dt);
+    const int t = 128;
+    if(a.n) {
+        int slot = timer_begin(h, "plain_stress");
+        if(h->sp.dim == 3) k_stress<T, 3><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
+        else k_stress<T, 2><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
+        timer_end(h, slot);
+        MPM_LAUNCHED(h, "k_stress");
+        slot = timer_begin(h, "plain_forces");
+        if(h->sp.dim == 3) k_forces<T, 3><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
+        else k_forces<T, 2><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
+        timer_end(h, slot);
+        MPM_LAUNCHED(h, "k_forces");
+    }
+    int slot = timer_begin(h, "plain_grid_update");
+    if(h->sp.dim == 3) k_grid_update<T, 3><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a);
+    else k_grid_update<T, 2><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a);
+    timer_end(h, slot);
+    MPM_LAUNCHED(h, "k_grid_update");
+    return MPM_OK;
+}
+
+template<class T> int g2p_t(mpm_handle* h, double dt)
+{
+    PlainArgs<T> a = args<T>(h, dt);
+    if(!a.n) return MPM_OK;
+    const int t = 128;
+    int slot = timer_begin(h, "plain_g2p");
+    if(h->sp.dim == 3) k_g2p<T, 3><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
+    else k_g2p<T, 2><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
+    timer_end(h, slot);
+    MPM_LAUNCHED(h, "k_g2p");
+    return MPM_OK;
+}
+
+template<class Tin, class Tout> __global__ void k_convert(const Tin* in, Tout* out, int64_t n)
+{
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) out[i] = (Tout)in[i];
+}
+
+}  // namespace
+
+int plain_alloc(mpm_handle* h, int64_t n)
+{
+    PlainState& s = h->plain;
+    const int d = h->sp.dim;
+    size_t e = esize(h);
+    int64_t gn = 1;
+    for(int k = 0; k < d; k++) gn *= h->sp.counts[k] + 2 * MPM_GHOST;
+    if(s.gn != gn) {
+        void** g[] = {&s.gm, &s.gmv, &s.gv0, &s.gf, &s.gv, &s.gvf};
+        for(void** p: g) { cudaFree(*p); *p = nullptr; }
+        MPM_CUDA(h, cudaMalloc(&s.gm, gn * e));
+        for(int i = 1; i < 6; i++) MPM_CUDA(h, cudaMalloc(g[i], gn * d * e));
+        s.gn = gn;
+        for(void** p: g) MPM_CUDA(h, cudaMemsetAsync(*p, 0, (p == &s.gm ? gn : gn * d) * e, h->stream));
+    }
+    if(s.n != n) {
+        void** pa[] = {&s.X, &s.V, &s.F, &s.B, &s.mass, &s.vol, &s.mu, &s.lam, &s.pft};
+        for(void** p: pa) { cudaFree(*p); *p = nullptr; }
+        cudaFree(s.valid); s.valid = nullptr;
+        int64_t m = n ? n : 1;
+        MPM_CUDA(h, cudaMalloc(&s.X, m * d * e));
+        MPM_CUDA(h, cudaMalloc(&s.V, m * d * e));
+        MPM_CUDA(h, cudaMalloc(&s.F, m * d * d * e));
+        MPM_CUDA(h, cudaMalloc(&s.B, m * d * d * e));
+        MPM_CUDA(h, cudaMalloc(&s.pft, m * d * d * e));
+        MPM_CUDA(h, cudaMalloc(&s.mass, m * e));
+        MPM_CUDA(h, cudaMalloc(&s.vol, m * e));
+        MPM_CUDA(h, cudaMalloc(&s.mu, m * e));
+        MPM_CUDA(h, cudaMalloc(&s.lam, m * e));
+        MPM_CUDA(h, cudaMalloc(&s.valid, m));
+        s.n = n;
+    }
+    return MPM_OK;
+}
+
+void plain_free(mpm_handle* h)
+{
+    PlainState& s = h->plain;
+    void* ps[] = {s.X, s.V, s.F, s.B, s.mass, s.vol, s.mu, s.lam, s.pft, s.valid, s.gm, s.gmv, s.gv0, s.gf, s.gv, s.gvf};
+    for(void* p: ps) cudaFree(p);
+    s = PlainState();
+}
+
+// Copy one array in, converting between the caller's and the path's scalar type.
+static int copy_in(mpm_handle* h, void* dst, const void* src, int64_t count, int src_dtype, bool src_dev)
+{
+    size_t e = esize(h), se = src_dtype == MPM_FP64 ? 8 : 4;
+    if(!src) return set_error(h, MPM_ERR_ARG, "null particle array");
+    if(se == e) {
+        MPM_CUDA(h, cudaMemcpyAsync(dst, src, count * e, src_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
+        return MPM_OK;
+    }
+    void* tmp = const_cast<void*>(src);
+    void* owned = nullptr;
+    if(!src_dev) {
+        MPM_CUDA(h, cudaMallocAsync(&owned, count * se, h->stream));
+        MPM_CUDA(h, cudaMemcpyAsync(owned, src, count * se, cudaMemcpyHostToDevice, h->stream));
+        tmp = owned;
+    }
+    int b = (int)((count + 255) / 256);
+    if(b > 4096) b = 4096;
+    if(b < 1) b = 1;
+    if(se == 8) k_convert<double, float><<<b, 256, 0, h->stream>>>((const double*)tmp, (float*)dst, count);
+    else k_convert<float, double><<<b, 256, 0, h->stream>>>((const float*)tmp, (double*)dst, count);
+    MPM_LAUNCHED(h, "k_convert");
+    if(owned) MPM_CUDA(h, cudaFreeAsync(owned, h->stream));
+    return MPM_OK;
+}
+
+static int copy_out(mpm_handle* h, void* dst, const void* src, int64_t count, int dst_dtype, bool dst_dev)
+{
+    size_t e = esize(h), de = dst_dtype == MPM_FP64 ? 8 : 4;
+    if(!dst) return MPM_OK;
+    if(de == e) {
+        MPM_CUDA(h, cudaMemcpyAsync(dst, src, count * e, dst_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+        return MPM_OK;
+    }
+    void* tmp = dst;
+    void* owned = nullptr;
+    if(!dst_dev) {
+        MPM_CUDA(h, cudaMallocAsync(&owned, count * de, h->stream));
+        tmp = owned;
+    }
+    int b = (int)((count + 255) / 256);
+    if(b > 4096) b = 4096;
+    if(b < 1) b = 1;
+    if(e == 8) k_convert<double, float><<<b, 256, 0, h->stream>>>((const double*)src, (float*)tmp, count);
+    else k_convert<float, double><<<b, 256, 0, h->stream>>>((const float*)src, (double*)tmp, count);
+    MPM_LAUNCHED(h, "k_convert");
+    if(owned) {
+        MPM_CUDA(h, cudaMemcpyAsync(dst, owned, count * de, cudaMemcpyDeviceToHost, h->stream));
+        MPM_CUDA(h, cudaFreeAsync(owned, h->stream));
+    }
+    return MPM_OK;
+}
+
+int plain_set_particles(mpm_handle* h, const mpm_particles_view* v)
+{
+    int rc = plain_alloc(h, v->n);
+    if(rc) return rc;
+    PlainState& s = h->plain;
+    const int d = h->sp.dim;
+    bool dev = v->on_device != 0;
+    int64_t n = v->n;
+    if(!n) return MPM_OK;
+    if((rc = copy_in(h, s.X, v->X, n * d, v->dtype, dev))) return rc;
+    if((rc = copy_in(h, s.V, v->V, n * d, v->dtype, dev))) return rc;
+    if((rc = copy_in(h, s.F, v->F, n * d * d, v->dtype, dev))) return rc;
+    if((rc = copy_in(h, s.B, v->B, n * d * d, v->dtype, dev))) return rc;
+    if((rc = copy_in(h, s.mass, v->mass, n, v->dtype, dev))) return rc;
+    if((rc = copy_in(h, s.vol, v->volume, n, v->dtype, dev))) return rc;
+    if((rc = copy_in(h, s.mu, v->mu, n, v->dtype, dev))) return rc;
+    if((rc = copy_in(h, s.lam, v->lambda, n, v->dtype, dev))) return rc;
+    if(v->valid) MPM_CUDA(h, cudaMemcpyAsync(s.valid, v->valid, n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
+    else MPM_CUDA(h, cudaMemsetAsync(s.valid, 1, n, h->stream));
+    return MPM_OK;
+}
+
+int plain_get_particles(mpm_handle* h, mpm_particles_view* v)
+{
+    PlainState& s = h->plain;
+    const int d = h->sp.dim;
+    if(v->n != s.n) return set_error(h, MPM_ERR_ARG, "particle count differs from mpm_set_particles");
+    bool dev = v->on_device != 0;
+    int64_t n = v->n;
+    if(!n) return MPM_OK;
+    int rc;
+    if((rc = copy_out(h, v->X, s.X, n * d, v->dtype, dev))) return rc;
+    if((rc = copy_out(h, v->V, s.V, n * d, v->dtype, dev))) return rc;
+    if((rc = copy_out(h, v->F, s.F, n * d * d, v->dtype, dev))) return rc;
+    if((rc = copy_out(h, v->B, s.B, n * d * d, v->dtype, dev))) return rc;
+    if(v->valid) MPM_CUDA(h, cudaMemcpyAsync(v->valid, s.valid, n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+int plain_p2g(mpm_handle* h, double dt, double)
+{
+    return h->model.precision == MPM_FP64 ? p2g_t<double>(h, dt) : p2g_t<float>(h, dt);
+}
+int plain_forces(mpm_handle* h, double dt, double)
+{
+    return h->model.precision == MPM_FP64 ? forces_t<double>(h, dt) : forces_t<float>(h, dt);
+}
+int plain_g2p(mpm_handle* h, double dt, double)
+{
+    return h->model.precision == MPM_FP64 ? g2p_t<double>(h, dt) : g2p_t<float>(h, dt);
+}
+
+int plain_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf)
+{
+    PlainState& s = h->plain;
+    const int d = h->sp.dim;
+    int rc;
+    if(m && (rc = copy_out(h, m, s.gm, s.gn, MPM_FP64, false))) return rc;
+    if(v0 && (rc = copy_out(h, v0, s.gv0, s.gn * d, MPM_FP64, false))) return rc;
+    if(v && (rc = copy_out(h, v, s.gv, s.gn * d, MPM_FP64, false))) return rc;
+    if(vf && (rc = copy_out(h, vf, s.gvf, s.gn * d, MPM_FP64, false))) return rc;
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+int plain_count_valid(mpm_handle* h, int64_t* c)
+{
+    unsigned long long* d = nullptr;
+    MPM_CUDA(h, cudaMallocAsync(&d, sizeof(*d), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(d, 0, sizeof(*d), h->stream));
+    if(h->plain.n) {
+        k_count_valid<float><<<gblocks(h, h->plain.n, 256), 256, 0, h->stream>>>(h->plain.valid, h->plain.n, d);
+        MPM_LAUNCHED(h, "k_count_valid");
+    }
+    unsigned long long r = 0;
+    MPM_CUDA(h, cudaMemcpyAsync(&r, d, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaFreeAsync(d, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    *c = (int64_t)r;
+    return MPM_OK;
+}

@@ -1,0 +1,281 @@
+"""Host-side mirror of the reference's explicit MPM driver over the C ABI.
+
+`MPM_DRIVER` here plays the part of PhysBAM's ``MPM_DRIVER<TV>``
+(``Hybrid_Methods/Examples_And_Drivers/MPM_DRIVER.h:22-80``) for the explicit
+path: the same step names, one handle per simulation, state kept on the GPU
+between calls.  Every call goes through ``libphysbam_mpm.so``; there is no
+CPU fallback, and importing this module on a machine without the library
+raises.  Errors come back as `MPMError`, the way PHYSBAM_FATAL_ERROR surfaces
+as ``std::runtime_error`` in the reference (``Core/Log/DEBUG_UTILITIES.cpp:95-103``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import scenes as S
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libphysbam_mpm.so")
+
+MPM_OK = 0
+FP32, FP64 = 0, 1
+PATH_FAST, PATH_PLAIN = 0, 1
+MAX_OBJECTS = 8
+STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "non-finite value", 4: "particle outside the grid",
+          5: "device wait timed out", 6: "out of device memory", 7: "call out of order", 8: "SVD did not converge"}
+
+
+class MPMError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (STATUS.get(code, "?"), code, msg))
+        self.code = code
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("counts", ctypes.c_int * 3), ("domain_min", ctypes.c_double * 3),
+                ("domain_max", ctypes.c_double * 3), ("ghost", ctypes.c_int)]
+
+
+class ModelDesc(ctypes.Structure):
+    _fields_ = [("model", ctypes.c_int), ("precision", ctypes.c_int), ("path", ctypes.c_int),
+                ("gravity", ctypes.c_double * 3)]
+
+
+class CollisionObject(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("type", ctypes.c_int), ("friction", ctypes.c_double),
+                ("a", ctypes.c_double * 3), ("b", ctypes.c_double * 3)]
+
+
+class ParticlesView(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("dtype", ctypes.c_int), ("on_device", ctypes.c_int),
+                ("X", ctypes.c_void_p), ("V", ctypes.c_void_p), ("F", ctypes.c_void_p), ("B", ctypes.c_void_p),
+                ("mass", ctypes.c_void_p), ("volume", ctypes.c_void_p), ("mu", ctypes.c_void_p),
+                ("lambda_", ctypes.c_void_p), ("valid", ctypes.c_void_p)]
+
+
+EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_objects", "mpm_set_particles",
+           "mpm_get_particles", "mpm_substep", "mpm_advance", "mpm_particle_to_grid", "mpm_apply_forces",
+           "mpm_grid_to_particle", "mpm_synchronize", "mpm_get_grid", "mpm_count_valid", "mpm_set_timing",
+           "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state"]
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libphysbam_mpm.so.  Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("libphysbam_mpm.so is not built (run __graft_entry__.build()); "
+                           "the MPM path has no CPU fallback")
+    L = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    L.mpm_create.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(ModelDesc), ctypes.POINTER(P)]
+    L.mpm_destroy.argtypes = [P]
+    L.mpm_set_stream.argtypes = [P, P]
+    L.mpm_set_collision_objects.argtypes = [P, ctypes.POINTER(CollisionObject), ctypes.c_int]
+    L.mpm_set_particles.argtypes = [P, ctypes.POINTER(ParticlesView)]
+    L.mpm_get_particles.argtypes = [P, ctypes.POINTER(ParticlesView)]
+    for f in ("mpm_substep", "mpm_particle_to_grid", "mpm_apply_forces", "mpm_grid_to_particle"):
+        getattr(L, f).argtypes = [P, ctypes.c_double, ctypes.c_double]
+    L.mpm_advance.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    L.mpm_synchronize.argtypes = [P]
+    L.mpm_get_grid.argtypes = [P, P, P, P, P]
+    L.mpm_count_valid.argtypes = [P, ctypes.POINTER(ctypes.c_int64)]
+    L.mpm_set_timing.argtypes = [P, ctypes.c_int]
+    L.mpm_get_timing.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.mpm_last_error.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
+    L.mpm_radix_sort_u32.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P]
+    L.mpm_debug_sort_state.argtypes = [P, P, P, P]
+    L.mpm_status_string.argtypes = [ctypes.c_int]
+    L.mpm_status_string.restype = ctypes.c_char_p
+    for f in EXPORTS:
+        if f != "mpm_status_string":
+            getattr(L, f).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class MPM_DRIVER:
+    """Explicit MPM substep on one GPU, keyed to a `scenes.Scene` (grid, model, gravity, objects)."""
+
+    def __init__(self, scene: S.Scene, precision: int = FP32, path: int = PATH_FAST):
+        self.L = load_library()
+        self.scene = scene
+        self.dim = scene.dim
+        self.precision = precision
+        self.path = path
+        g = GridDesc()
+        g.dim = scene.dim
+        for a in range(3):
+            g.counts[a] = scene.counts[a] if a < scene.dim else 1
+            g.domain_min[a] = scene.domain_min[a] if a < scene.dim else 0.0
+            g.domain_max[a] = scene.domain_max[a] if a < scene.dim else 1.0
+        g.ghost = S.GHOST
+        m = ModelDesc()
+        m.model, m.precision, m.path = scene.model, precision, path
+        for a in range(scene.dim):
+            m.gravity[a] = scene.gravity[a]
+        self.h = ctypes.c_void_p()
+        self._check(self.L.mpm_create(ctypes.byref(g), ctypes.byref(m), ctypes.byref(self.h)), "mpm_create")
+        self.set_collision_objects(scene.objects)
+        self.time = 0.0
+        self.n = 0
+
+    # -- errors ---------------------------------------------------------------
+    def _check(self, rc, what):
+        if rc != MPM_OK:
+            buf = ctypes.create_string_buffer(512)
+            if self.__dict__.get("h"):
+                self.L.mpm_last_error(self.h, buf, 512)
+            raise MPMError(rc, "%s: %s" % (what, buf.value.decode(errors="replace")))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mpm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- scene ----------------------------------------------------------------
+    def set_collision_objects(self, objects: Sequence[S.CollisionObject]):
+        arr = (CollisionObject * max(len(objects), 1))()
+        for i, o in enumerate(objects):
+            arr[i].kind, arr[i].type, arr[i].friction = o.kind, o.type, o.friction
+            for a in range(self.dim):
+                arr[i].a[a], arr[i].b[a] = o.a[a], o.b[a]
+        self._check(self.L.mpm_set_collision_objects(self.h, arr, len(objects)), "mpm_set_collision_objects")
+
+    def set_particles(self, X, V, F, B, mass, volume, mu, lam, valid=None, dtype=np.float64):
+        """Arrays in the reference layout: X,V (n,d); F,B (n,d,d) row/col as numpy matrices."""
+        d = self.dim
+        n = X.shape[0]
+        self._keep = [np.ascontiguousarray(X, dtype), np.ascontiguousarray(V, dtype),
+                      np.ascontiguousarray(np.swapaxes(F, 1, 2).reshape(n, d * d), dtype),
+                      np.ascontiguousarray(np.swapaxes(B, 1, 2).reshape(n, d * d), dtype),
+                      np.ascontiguousarray(mass, dtype), np.ascontiguousarray(volume, dtype),
+                      np.ascontiguousarray(mu, dtype), np.ascontiguousarray(lam, dtype)]
+        v = ParticlesView()
+        v.n, v.dtype, v.on_device = n, FP64 if dtype == np.float64 else FP32, 0
+        v.X, v.V, v.F, v.B, v.mass, v.volume, v.mu, v.lambda_ = [a.ctypes.data for a in self._keep]
+        vv = None
+        if valid is not None:
+            vv = np.ascontiguousarray(valid, np.uint8)
+            v.valid = vv.ctypes.data
+        self._check(self.L.mpm_set_particles(self.h, ctypes.byref(v)), "mpm_set_particles")
+        self._keep = None
+        self.n = n
+
+    def set_scene_particles(self, scene: Optional[S.Scene] = None, dtype=np.float64):
+        s = scene or self.scene
+        self.set_particles(s.X, s.V, s.F, s.B, s.mass, s.volume, s.mu, s.lam, dtype=dtype)
+
+    def get_particles(self, dtype=np.float64):
+        d, n = self.dim, self.n
+        X = np.empty((n, d), dtype)
+        V = np.empty((n, d), dtype)
+        F = np.empty((n, d * d), dtype)
+        B = np.empty((n, d * d), dtype)
+        valid = np.empty(n, np.uint8)
+        v = ParticlesView()
+        v.n, v.dtype, v.on_device = n, FP64 if dtype == np.float64 else FP32, 0
+        v.X, v.V, v.F, v.B = X.ctypes.data, V.ctypes.data, F.ctypes.data, B.ctypes.data
+        v.valid = valid.ctypes.data
+        self._check(self.L.mpm_get_particles(self.h, ctypes.byref(v)), "mpm_get_particles")
+        F = np.swapaxes(F.reshape(n, d, d), 1, 2)
+        B = np.swapaxes(B.reshape(n, d, d), 1, 2)
+        return {"X": X, "V": V, "F": F, "B": B, "valid": valid.astype(bool)}
+
+    # -- the substep (MPM_DRIVER.cpp:141-157) --------------------------------
+    def Advance_One_Time_Step(self, dt: Optional[float] = None):
+        dt = self.scene.dt if dt is None else dt
+        self._check(self.L.mpm_substep(self.h, dt, self.time), "mpm_substep")
+        self.time += dt
+
+    def Particle_To_Grid(self, dt=None):
+        self._check(self.L.mpm_particle_to_grid(self.h, self.scene.dt if dt is None else dt, self.time), "p2g")
+
+    def Apply_Forces(self, dt=None):
+        self._check(self.L.mpm_apply_forces(self.h, self.scene.dt if dt is None else dt, self.time), "forces")
+
+    def Grid_To_Particle(self, dt=None):
+        dt = self.scene.dt if dt is None else dt
+        self._check(self.L.mpm_grid_to_particle(self.h, dt, self.time), "g2p")
+        self.time += dt
+
+    def advance(self, nsteps: int, dt: Optional[float] = None):
+        """Fixed-dt substep loop (Simulate_To_Frame with min_dt = max_dt), CUDA-graph replay."""
+        dt = self.scene.dt if dt is None else dt
+        self._check(self.L.mpm_advance(self.h, dt, self.time, nsteps), "mpm_advance")
+        self.time += nsteps * dt
+
+    def synchronize(self):
+        self._check(self.L.mpm_synchronize(self.h), "mpm_synchronize")
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self.L.mpm_set_stream(self.h, ctypes.c_void_p(stream_ptr)), "mpm_set_stream")
+
+    # -- inspection -----------------------------------------------------------
+    def get_grid(self, want_v0=False):
+        shape = tuple(c + 2 * S.GHOST for c in self.scene.counts[:self.dim])
+        gn = int(np.prod(shape))
+        m = np.zeros(gn)
+        v0 = np.zeros(gn * self.dim) if want_v0 else None
+        v = np.zeros(gn * self.dim)
+        vf = np.zeros(gn * self.dim)
+        self._check(self.L.mpm_get_grid(self.h, _ptr(m), _ptr(v0), _ptr(v), _ptr(vf)), "mpm_get_grid")
+        out = {"grid_m": m.reshape(shape), "grid_v": v.reshape(shape + (self.dim,)),
+               "grid_vf": vf.reshape(shape + (self.dim,))}
+        if want_v0:
+            out["grid_v0"] = v0.reshape(shape + (self.dim,))
+        return out
+
+    def sort_state(self):
+        n = self.n
+        keys, sk, perm = (np.empty(n, np.uint32) for _ in range(3))
+        self._check(self.L.mpm_debug_sort_state(self.h, _ptr(keys), _ptr(sk), _ptr(perm)), "mpm_debug_sort_state")
+        return keys, sk, perm
+
+    def count_valid(self) -> int:
+        c = ctypes.c_int64()
+        self._check(self.L.mpm_count_valid(self.h, ctypes.byref(c)), "mpm_count_valid")
+        return int(c.value)
+
+    def set_timing(self, on: bool):
+        self._check(self.L.mpm_set_timing(self.h, 1 if on else 0), "mpm_set_timing")
+
+    def get_timing(self):
+        names = ctypes.create_string_buffer(4096)
+        ms = (ctypes.c_double * 64)()
+        launches = (ctypes.c_int64 * 64)()
+        count = ctypes.c_int()
+        self._check(self.L.mpm_get_timing(self.h, names, 4096, ctypes.cast(ms, ctypes.c_void_p),
+                                          ctypes.cast(launches, ctypes.c_void_p), 64, ctypes.byref(count)),
+                    "mpm_get_timing")
+        keys = names.value.decode().split(",") if count.value else []
+        return {k: (ms[i], launches[i]) for i, k in enumerate(keys)}
+
+
+def radix_sort_u32(keys: np.ndarray, bits: int = 32):
+    """Sort uint32 keys by their low `bits` bits on the GPU; returns (sorted_keys, perm)."""
+    L = load_library()
+    k = np.ascontiguousarray(keys, np.uint32)
+    out = np.empty_like(k)
+    perm = np.empty_like(k)
+    rc = L.mpm_radix_sort_u32(_ptr(k), k.size, bits, _ptr(out), _ptr(perm))
+    if rc != MPM_OK:
+        raise MPMError(rc, "mpm_radix_sort_u32")
+    return out, perm
