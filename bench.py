@@ -34,6 +34,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "particle-substeps/s"
 WORKLOAD = "spheres3d-128^3-neohookean-8ppc-fp32"
+LARGE_WORKLOAD = "dam3d-256^3-corotated-8ppc-fp32"
 ALG_BYTES = {"p2g": 112, "g2p": 144, "substep": 256}    # bytes per particle (FP32, 3D)
 GRID_BYTES_PER_NODE = 48                                # grid update: read 16, write 32
 
@@ -176,17 +177,69 @@ def kernels_per_substep(scene):
     return 5 * ((bits + 7) // 8) + 5
 
 
-def read_traffic(kernel):
-    """Per-launch DRAM traffic of `kernel` on this workload from the committed ncu summary, if any."""
+def read_traffic(kernel, workload=WORKLOAD):
+    """Per-launch DRAM traffic of `kernel` on `workload` from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         for line in f:
             parts = line.split()
-            if len(parts) >= 4 and parts[0] == kernel and parts[1] == WORKLOAD:
+            if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload:
                 return float(parts[2])
     return None
+
+
+def measure_substeps(drv, stream, flush, steps, warmup, dist=None, clock_index=None):
+    """Warm up, take per-kernel shares from an eager event-timed pass, then time
+    `steps` graph-replayed substeps, each bracketed by CUDA events on the
+    library's stream with the L2 flushed before it.  Returns (ms_total, kernel
+    times, clock summary)."""
+    import torch
+    drv.advance(max(warmup, 3))
+    drv.synchronize()
+    drv.set_timing(True)
+    for _ in range(4):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        drv.Advance_One_Time_Step()
+    drv.synchronize()
+    ktimes = drv.get_timing()
+    drv.set_timing(False)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(clock_index) if clock_index is not None else None
+    if clk:
+        clk.__enter__()
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+            evs[k][0].record(stream)
+        drv.advance(1)
+        with torch.cuda.stream(stream):
+            evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__(None, None, None)
+    drv.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    return ms, ktimes, (clk.summary() if clk else None)
+
+
+def roofline_of(ktimes, n, peak, peak_kind, workload):
+    shares = {k: v[0] for k, v in ktimes.items()}
+    top = max(shares, key=shares.get)
+    per_launch_ms = ktimes[top][0] / max(ktimes[top][1], 1)
+    alg = {"fast_p2g": ALG_BYTES["p2g"] * n, "fast_g2p": ALG_BYTES["g2p"] * n}.get(top)
+    if not alg:
+        return {"bound": "hbm", "kernel": top, "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                "traffic": None, "note": "dominant kernel has no algorithmic byte count"}
+    achieved = alg / (per_launch_ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": peak_kind, "kernel": top, "traffic": read_traffic(top, workload),
+            "alg_bytes_per_launch": alg, "ms_per_launch": per_launch_ms}
 
 
 def our_arm(args):
@@ -201,6 +254,7 @@ def our_arm(args):
     from physbam_b200 import driver as D
     from physbam_b200 import scenes as S
 
+    peak, peak_kind = measured_peaks()
     scene = S.spheres_3d()
     n = scene.n
     drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
@@ -209,42 +263,14 @@ def our_arm(args):
     drv.set_scene_particles(scene)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    # warm-up (also captures the two substep graphs)
-    drv.advance(max(args.warmup, 3))
-    drv.synchronize()
-
-    # per-kernel shares from an eager, event-timed pass (separate from the headline)
-    drv.set_timing(True)
-    for _ in range(4):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-        drv.Advance_One_Time_Step()
-    drv.synchronize()
-    ktimes = drv.get_timing()
-    drv.set_timing(False)
-
-    # headline: K substeps, each a graph replay on the library stream, L2 flushed before each
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(float(k))
-                evs[k][0].record(stream)
-            drv.advance(1)
-            with torch.cuda.stream(stream):
-                evs[k][1].record(stream)
-        torch.cuda.synchronize()
-    drv.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in evs)
+    ms, ktimes, clocks = measure_substeps(drv, stream, flush, args.steps, args.warmup, dist, local)
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
     ms_max = float(t.item())
     value = world * n * args.steps / (ms_max / 1e3)
+    drv.close()
 
     # e2e through the public API with pinned host buffers
     d = 3
@@ -277,21 +303,13 @@ def our_arm(args):
     e2e_drv.close()
     assert out["valid"].sum() > 0
 
-    # roofline: the kernel with the largest share of device time
-    peak, peak_kind = measured_peaks()
-    shares = {k: v[0] for k, v in ktimes.items()}
-    total_k = sum(shares.values())
-    top = max(shares, key=shares.get)
-    per_launch_ms = ktimes[top][0] / max(ktimes[top][1], 1)
-    alg = {"fast_p2g": ALG_BYTES["p2g"] * n, "fast_g2p": ALG_BYTES["g2p"] * n}.get(top)
-    roof = None
-    if alg:
-        achieved = alg / (per_launch_ms / 1e3) / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_kind": peak_kind, "kernel": top, "traffic": read_traffic(top),
-                "alg_bytes_per_launch": alg}
     substep_ms = ms_max / args.steps
-    launches_per_step = kernels_per_substep(scene)
+    roof = roofline_of(ktimes, n, peak, peak_kind, WORKLOAD)
+    total_k = sum(v[0] for v in ktimes.values())
+
+    large = None
+    if world == 1 and not args.no_large:
+        large = measure_large(args, D, S, stream, flush, peak, peak_kind)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -305,22 +323,44 @@ def our_arm(args):
                        "parallelism": "replicas" if world > 1 else "single"},
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "step": "upload + %d substeps (CUDA graph) + download, pinned host buffers" % frame},
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": kernels_per_substep(scene) * args.steps,
             "roofline": roof,
             "substep_roofline": {"achieved": ALG_BYTES["substep"] * n / (substep_ms / 1e3) / 1e9, "peak": peak,
                                  "unit": "GB/s", "frac": ALG_BYTES["substep"] * n / (substep_ms / 1e3) / 1e9 / peak,
                                  "alg_bytes_per_particle": ALG_BYTES["substep"]},
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()},
-            "kernel_share": {k: v / total_k for k, v in shares.items()},
+            "kernel_share": {k: v[0] / total_k for k, v in ktimes.items()},
+            "large_config": large,
             "cpu_baseline": cpu,
-            "clocks": clk.summary()}
-    drv.close()
+            "clocks": clocks}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def measure_large(args, D, S, stream, flush, peak, peak_kind):
+    """The 256^3 dam-break scene (36M particles): the HBM-bound regime of the same kernels."""
+    scene = S.dam_3d()
+    n = scene.n
+    drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+    drv.set_stream(stream.cuda_stream)
+    drv.set_scene_particles(scene, dtype=np.float32)
+    del scene.F, scene.B
+    steps = max(5, min(args.steps, 20))
+    ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
+    drv.close()
+    sub = ms / steps
+    total_k = sum(v[0] for v in ktimes.values())
+    return {"workload": LARGE_WORKLOAD, "particles": n, "steps": steps, "ms_per_step": sub,
+            "value": n * steps / (ms / 1e3), "unit": METRIC,
+            "substep_roofline": {"achieved": ALG_BYTES["substep"] * n / (sub / 1e3) / 1e9, "peak": peak,
+                                 "unit": "GB/s", "frac": ALG_BYTES["substep"] * n / (sub / 1e3) / 1e9 / peak},
+            "roofline": roofline_of(ktimes, n, peak, peak_kind, LARGE_WORKLOAD),
+            "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()},
+            "kernel_share": {k: v[0] / total_k for k, v in ktimes.items()}}
 
 
 def main():
@@ -330,6 +370,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-large", action="store_true", help="skip the 256^3 dam-break measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

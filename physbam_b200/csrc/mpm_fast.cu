@@ -233,6 +233,8 @@ __device__ __forceinline__ int next_work(uint32_t* ctr, int* s_work)
 template<int THREADS> __global__ void __launch_bounds__(THREADS) k_p2g(FastArgs a)
 {
     __shared__ float tm[TN], tx[TN], ty[TN], tz[TN];
+    __shared__ uint32_t ccount[64], cstart[64];
+    __shared__ uint32_t s_maxc;
     __shared__ int s_work;
     const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
     const float Dx = 4.f * a.inv[0] * a.inv[0], Dy = 4.f * a.inv[1] * a.inv[1], Dz = 4.f * a.inv[2] * a.inv[2];
@@ -242,10 +244,33 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_p2g(FastArgs 
         block_coords(a, b, bx, by, bz);
         const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;   // tile origin, ghosted node coords
         for(int t = threadIdx.x; t < TN; t += THREADS) { tm[t] = 0; tx[t] = 0; ty[t] = 0; tz[t] = 0; }
+        if(threadIdx.x < 64) ccount[threadIdx.x] = 0;
         __syncthreads();
         const uint32_t s = a.bstart[b], e = a.bend[b];
-        for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
-            const uint32_t i = a.perm[j];
+        // particles of a block arrive sorted by cell; count them per cell so the
+        // loop below can hand each lane of a warp a particle of a different cell:
+        // then no two lanes of one shared-memory atomic hit the same node.
+        for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) atomicAdd(&ccount[a.sorted_keys[j] & 63u], 1u);
+        __syncthreads();
+        if(threadIdx.x < 32) {
+            uint32_t c0 = ccount[2 * threadIdx.x], c1 = ccount[2 * threadIdx.x + 1];
+            uint32_t sum = c0 + c1, x = sum, mx = c0 > c1 ? c0 : c1;
+#pragma unroll
+            for(int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if((int)threadIdx.x >= o) x += y;
+                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            }
+            cstart[2 * threadIdx.x] = x - sum;
+            cstart[2 * threadIdx.x + 1] = x - sum + c0;
+            if(threadIdx.x == 0) s_maxc = mx;
+        }
+        __syncthreads();
+        const uint32_t slots = s_maxc * 64u;
+        for(uint32_t q = threadIdx.x; q < slots; q += THREADS) {
+            const uint32_t c = q & 63u, r = q >> 6;
+            if(r >= ccount[c]) continue;
+            const uint32_t i = a.perm[s + cstart[c] + r];
             float X[3], V[3], F[9], Bm[9];
 #pragma unroll
             for(int k = 0; k < 3; k++) { X[k] = a.src[(C_X + k) * a.npad + i]; V[k] = a.src[(C_V + k) * a.npad + i]; }
@@ -599,8 +624,9 @@ int fast_alloc(mpm_handle* h, int64_t n)
     }
     if(f.n != n || !f.soa[0]) {
         for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); }
-        uint32_t* ps[] = {f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, f.sort_hist, f.sort_part};
+        uint32_t* ps[] = {f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, f.sort_scratch};
         for(uint32_t* p: ps) cudaFree(p);
+        if(n >= (1LL << 30)) return set_error(h, MPM_ERR_ARG, "more than 2^30 - 1 particles");
         int64_t np = ((n ? n : 1) + 31) / 32 * 32;
         f.npad = np;
         for(int b = 0; b < 2; b++) {
@@ -613,9 +639,9 @@ int fast_alloc(mpm_handle* h, int64_t n)
         MPM_CUDA(h, cudaMalloc(&f.perm, np * sizeof(uint32_t)));
         MPM_CUDA(h, cudaMalloc(&f.sort_keys_alt, np * sizeof(uint32_t)));
         MPM_CUDA(h, cudaMalloc(&f.sort_vals_alt, np * sizeof(uint32_t)));
-        f.sort_tiles = mpm_sort::tiles_for(np);
-        MPM_CUDA(h, cudaMalloc(&f.sort_hist, mpm_sort::hist_words(np) * sizeof(uint32_t)));
-        MPM_CUDA(h, cudaMalloc(&f.sort_part, mpm_sort::part_words(np) * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.sort_scratch, mpm_sort::scratch_words(np) * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMemsetAsync(f.sort_scratch, 0, mpm_sort::scratch_words(np) * sizeof(uint32_t), h->stream));
+        MPM_CUDA(h, mpm_sort::prepare());
         f.n = n;
     }
     return MPM_OK;
@@ -625,7 +651,7 @@ void fast_free(mpm_handle* h)
 {
     FastState& f = h->fast;
     for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); }
-    void* ps[] = {f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, f.sort_hist, f.sort_part,
+    void* ps[] = {f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, f.sort_scratch,
                   f.bstart, f.bend, f.active, f.nb_flag, f.nb_list, f.counters, f.acc, f.vel};
     for(void* p: ps) cudaFree(p);
     f = FastState();
@@ -638,7 +664,7 @@ int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
     FastState& f = h->fast;
     int64_t n = v->n;
     f.cur = 0;
-    f.keys_ready = false;
+    f.keys_ready = n == 0;
     if(!n) return MPM_OK;
     // stage caller arrays on the device if needed
     bool dev = v->on_device != 0;
@@ -733,15 +759,11 @@ int fast_p2g(mpm_handle* h, double dt, double)
     if(!f.keys_ready) return set_error(h, MPM_ERR_STATE, "particles not set");
     int64_t n = f.n;
     if(!n) return MPM_OK;
-    uint32_t *ko = nullptr, *vo = nullptr;
     int slot = timer_begin(h, "fast_sort");
-    // sort keys (in f.keys, left intact for get_particles) into sorted_keys / perm
-    MPM_CUDA(h, cudaMemcpyAsync(f.sorted_keys, f.keys, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
-    cudaError_t e = mpm_sort::radix_sort(f.sorted_keys, f.sort_keys_alt, f.perm, f.sort_vals_alt, n, f.key_bits,
-                                         f.sort_hist, f.sort_part, h->stream, &ko, &vo);
+    // sort the slot keys (f.keys, left intact for get_particles) into sorted_keys / perm
+    cudaError_t e = mpm_sort::radix_sort(f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, n, f.key_bits,
+                                         f.sort_scratch, h->d_flags, MPM_FLAG_TIMEOUT, h->sm_count * 4, h->stream);
     if(e != cudaSuccess) return check_cuda(h, e, "radix_sort");
-    if(ko != f.sorted_keys) MPM_CUDA(h, cudaMemcpyAsync(f.sorted_keys, ko, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
-    if(vo != f.perm) MPM_CUDA(h, cudaMemcpyAsync(f.perm, vo, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
     timer_end(h, slot);
     FastArgs a = make_args(h, dt);
     slot = timer_begin(h, "fast_ranges");
@@ -841,26 +863,36 @@ int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_k
 int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm)
 {
     if(n < 0 || bits < 1 || bits > 32 || (n && (!keys || !sorted_keys || !perm))) return MPM_ERR_ARG;
-    if(n > 0x7fffffffLL) return MPM_ERR_ARG;
+    if(n >= (1LL << 30)) return MPM_ERR_ARG;
     if(!n) return MPM_OK;
+    int dev = 0, sms = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaStream_t st;
     if(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return MPM_ERR_CUDA;
-    uint32_t *k = nullptr, *ka = nullptr, *v = nullptr, *va = nullptr, *hist = nullptr, *part = nullptr;
+    uint32_t *k = nullptr, *ko = nullptr, *vo = nullptr, *ka = nullptr, *va = nullptr, *scratch = nullptr;
+    unsigned* flags = nullptr;
     int rc = MPM_OK;
     size_t b = n * sizeof(uint32_t);
-    if(cudaMalloc(&k, b) || cudaMalloc(&ka, b) || cudaMalloc(&v, b) || cudaMalloc(&va, b) ||
-       cudaMalloc(&hist, mpm_sort::hist_words(n) * 4) || cudaMalloc(&part, mpm_sort::part_words(n) * 4)) rc = MPM_ERR_NOMEM;
+    size_t sw = mpm_sort::scratch_words(n) * sizeof(uint32_t);
+    if(cudaMalloc(&k, b) || cudaMalloc(&ko, b) || cudaMalloc(&vo, b) || cudaMalloc(&ka, b) || cudaMalloc(&va, b) ||
+       cudaMalloc(&scratch, sw) || cudaMalloc(&flags, sizeof(unsigned))) rc = MPM_ERR_NOMEM;
+    if(!rc && (cudaMemsetAsync(scratch, 0, sw, st) || cudaMemsetAsync(flags, 0, sizeof(unsigned), st) ||
+               mpm_sort::prepare())) rc = MPM_ERR_CUDA;
     if(!rc) {
-        uint32_t *ko, *vo;
         cudaMemcpyAsync(k, keys, b, cudaMemcpyHostToDevice, st);
-        if(mpm_sort::radix_sort(k, ka, v, va, n, bits, hist, part, st, &ko, &vo) != cudaSuccess) rc = MPM_ERR_CUDA;
+        if(mpm_sort::radix_sort(k, ko, vo, ka, va, n, bits, scratch, flags, MPM_FLAG_TIMEOUT, sms * 4, st) != cudaSuccess)
+            rc = MPM_ERR_CUDA;
         else {
+            unsigned f = 0;
             cudaMemcpyAsync(sorted_keys, ko, b, cudaMemcpyDeviceToHost, st);
             cudaMemcpyAsync(perm, vo, b, cudaMemcpyDeviceToHost, st);
+            cudaMemcpyAsync(&f, flags, sizeof(f), cudaMemcpyDeviceToHost, st);
             if(cudaStreamSynchronize(st) != cudaSuccess) rc = MPM_ERR_CUDA;
+            else if(f & MPM_FLAG_TIMEOUT) rc = MPM_ERR_TIMEOUT;
         }
     }
-    cudaFree(k); cudaFree(ka); cudaFree(v); cudaFree(va); cudaFree(hist); cudaFree(part);
+    cudaFree(k); cudaFree(ko); cudaFree(vo); cudaFree(ka); cudaFree(va); cudaFree(scratch); cudaFree(flags);
     cudaStreamDestroy(st);
     return rc;
 }

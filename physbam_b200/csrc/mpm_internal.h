@@ -45,9 +45,7 @@ struct FastState {
     uint32_t* perm = nullptr;                 // sorted position -> slot in the current buffer
     uint32_t* sort_keys_alt = nullptr;
     uint32_t* sort_vals_alt = nullptr;
-    uint32_t* sort_hist = nullptr;            // 4 passes * 256 * tiles
-    uint32_t* sort_part = nullptr;            // scan partials
-    int64_t sort_tiles = 0;
+    uint32_t* sort_scratch = nullptr;         // histograms, tickets, epoch, look-back status words
     uint32_t* bstart = nullptr;               // per particle block
     uint32_t* bend = nullptr;
     uint32_t* active = nullptr;               // active particle blocks

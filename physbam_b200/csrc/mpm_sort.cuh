@@ -3,15 +3,27 @@
 // The reference bins particles into x-slabs for its OpenMP scatter
 // (GATHER_SCATTER::Prepare_Scatter, Hybrid_Methods/Iterators/GATHER_SCATTER.cpp:
 // 33-87); here particles are sorted by (block, cell) key every substep so a
-// CTA can own a block of cells.  Only the low `bits` bits take part, in 8-bit
-// digits.  Per digit place:
-//   1. every tile counts its digits (digit-major table [digit][tile]);
-//   2. the table is exclusive-scanned (3 kernels);
-//   3. each tile ranks its keys stably (warp __match_any_sync + popc, warp
-//      by warp in index order), stages them in shared memory in digit order
-//      and writes runs of equal digits to consecutive global addresses.
+// CTA can own a block of cells.  Only the low `bits` bits take part, in
+// digits of up to 8 bits.
+//
+// One kernel counts every digit place's global histogram up front; then one
+// kernel per digit place does the whole pass (the single-pass "onesweep"
+// scheme of Adinets & Merrill, 2022):
+//   * tiles are numbered in the order CTAs start (atomic ticket), so a tile
+//     only ever waits on tiles that are already running;
+//   * each tile ranks its keys stably (warp __match_any_sync + popc, warp by
+//     warp in index order), publishes its per-digit counts, and looks back
+//     over earlier tiles' published counts / inclusive prefixes (decoupled
+//     look-back) to find where its keys go;
+//   * keys are staged in shared memory in digit order and runs of equal
+//     digits are written to consecutive global addresses.
+// Status words carry an epoch (bumped on the device by the histogram kernel),
+// so nothing needs clearing between sorts and the sort replays inside a CUDA
+// graph.  Every spin-wait is bounded: past the limit the kernel sets an error
+// flag and moves on instead of hanging.
 // The result is bit-identical to a CPU stable sort on the same keys.
 #pragma once
+#include <cuda/atomic>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -19,32 +31,60 @@
 namespace mpm_sort {
 
 constexpr int kThreads = 256;
-constexpr int kItems = 8;
-constexpr int kTile = kThreads * kItems;   // 2048 keys per tile
+constexpr int kItems = 16;
+constexpr int kTile = kThreads * kItems;   // 4096 keys per tile
 constexpr int kRadix = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxPasses = 4;
-constexpr int kScanChunk = 4096;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+constexpr uint64_t kFlagAggregate = 1;
+constexpr uint64_t kFlagInclusive = 2;
+
+// global scratch layout (in 32-bit words)
+//   [0, 1024)                   digit histograms, kMaxPasses x 256
+//   [1024, 1028)                tile tickets per pass
+//   [1028]                      epoch
+//   then (8-byte aligned)       status words, kMaxPasses x tiles x 256 (uint64)
+constexpr int kHistWords = kMaxPasses * kRadix;
+constexpr int kTicketOff = kHistWords;
+constexpr int kEpochOff = kTicketOff + kMaxPasses;
+constexpr int kStatusOff = kEpochOff + 4;     // keep 16-byte alignment
 
 __host__ __device__ inline int64_t tiles_for(int64_t n) { return (n + kTile - 1) / kTile; }
+inline int64_t scratch_words(int64_t n) { return kStatusOff + 2 * (int64_t)kMaxPasses * tiles_for(n > 0 ? n : 1) * kRadix; }
 
-// hist[digit][tile] for one digit place, on the keys in their current order.
-__global__ void __launch_bounds__(kThreads) k_hist(const uint32_t* __restrict__ keys, int64_t n, int shift,
-    int64_t tiles, uint32_t* __restrict__ hist)
+__device__ __forceinline__ int passes_for(int bits) { return (bits + 7) / 8; }
+__device__ __forceinline__ uint32_t digit_mask(int bits, int pass)
 {
-    __shared__ uint32_t cnt[kRadix];
-    for(int i = threadIdx.x; i < kRadix; i += kThreads) cnt[i] = 0;
-    __syncthreads();
-    int64_t base = (int64_t)blockIdx.x * kTile;
-    for(int k = 0; k < kItems; k++) {
-        int64_t idx = base + k * kThreads + threadIdx.x;
-        if(idx < n) atomicAdd(&cnt[(keys[idx] >> shift) & 255u], 1u);
-    }
-    __syncthreads();
-    for(int i = threadIdx.x; i < kRadix; i += kThreads) hist[(int64_t)i * tiles + blockIdx.x] = cnt[i];
+    int w = bits - 8 * pass;
+    return w >= 8 ? 255u : ((1u << w) - 1u);
 }
 
-// --- exclusive scan of a uint32 array (per-chunk reduce, scan of partials, downsweep)
+// Global histograms of every digit place; also resets the tile tickets and
+// bumps the epoch (block 0, thread 0).  `scratch` histograms must be zero.
+__global__ void __launch_bounds__(kThreads) k_upfront_hist(const uint32_t* __restrict__ keys, int64_t n, int bits,
+    uint32_t* __restrict__ scratch)
+{
+    __shared__ uint32_t cnt[kMaxPasses][kRadix];
+    const int passes = passes_for(bits);
+    for(int i = threadIdx.x; i < kMaxPasses * kRadix; i += kThreads) (&cnt[0][0])[i] = 0;
+    __syncthreads();
+    for(int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        uint32_t k = keys[i];
+        for(int p = 0; p < passes; p++) atomicAdd(&cnt[p][(k >> (8 * p)) & digit_mask(bits, p)], 1u);
+    }
+    __syncthreads();
+    for(int i = threadIdx.x; i < passes * kRadix; i += kThreads) {
+        uint32_t c = (&cnt[0][0])[i];
+        if(c) atomicAdd(&scratch[i], c);
+    }
+    if(blockIdx.x == 0 && threadIdx.x == 0) {
+        for(int p = 0; p < kMaxPasses; p++) scratch[kTicketOff + p] = 0;
+        scratch[kEpochOff] += 1;
+    }
+}
+
 __device__ inline uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem, uint32_t& total)
 {
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -72,159 +112,148 @@ __device__ inline uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem, uint
     return warp_prefix + x - v;
 }
 
-__global__ void __launch_bounds__(kThreads) k_scan_reduce(const uint32_t* __restrict__ in, int64_t len, uint32_t* __restrict__ part)
-{
-    __shared__ uint32_t red[kWarps];
-    int64_t base = (int64_t)blockIdx.x * kScanChunk;
-    uint32_t s = 0;
-    for(int i = threadIdx.x; i < kScanChunk; i += kThreads) {
-        int64_t j = base + i;
-        if(j < len) s += in[j];
-    }
-#pragma unroll
-    for(int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if(threadIdx.x == 0) {
-        uint32_t t = 0;
-        for(int w = 0; w < kWarps; w++) t += red[w];
-        part[blockIdx.x] = t;
-    }
-}
+struct PassSmem {
+    uint32_t wcnt[kWarps][kRadix];
+    uint32_t dstart[kRadix];
+    uint32_t gbase[kRadix];
+    uint32_t skey[kTile];
+    uint32_t sval[kTile];
+    uint32_t scan_tmp[32];
+    uint32_t tile;
+};
 
-__global__ void __launch_bounds__(kThreads) k_scan_partials(uint32_t* part, int64_t nparts)
+// One digit place.  vals_in == nullptr means payload = index.
+__global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int bits, int pass, int64_t tiles,
+    uint32_t* __restrict__ scratch, unsigned* __restrict__ err_flags, unsigned timeout_flag)
 {
-    __shared__ uint32_t smem[32];
-    uint32_t carry = 0;
-    for(int64_t base = 0; base < nparts; base += kThreads) {
-        int64_t j = base + threadIdx.x;
-        uint32_t v = j < nparts ? part[j] : 0, total;
-        uint32_t ex = block_exclusive_scan(v, smem, total);
-        if(j < nparts) part[j] = carry + ex;
-        carry += total;
-    }
-}
-
-__global__ void __launch_bounds__(kThreads) k_scan_down(uint32_t* __restrict__ data, int64_t len, const uint32_t* __restrict__ part)
-{
-    __shared__ uint32_t smem[32];
-    int64_t base = (int64_t)blockIdx.x * kScanChunk;
-    uint32_t carry = part[blockIdx.x];
-    constexpr int per = kScanChunk / kThreads;   // 16 consecutive items per thread
-    uint32_t v[per], s = 0;
-    int64_t j0 = base + (int64_t)threadIdx.x * per;
-#pragma unroll
-    for(int i = 0; i < per; i++) { v[i] = j0 + i < len ? data[j0 + i] : 0; s += v[i]; }
-    uint32_t total;
-    uint32_t ex = block_exclusive_scan(s, smem, total);
-    uint32_t run = carry + ex;
-#pragma unroll
-    for(int i = 0; i < per; i++) {
-        if(j0 + i < len) data[j0 + i] = run;
-        run += v[i];
-    }
-}
-
-// One digit place: stable rank + scatter.  vals_in == nullptr means payload = index.
-__global__ void __launch_bounds__(kThreads) k_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int shift, int64_t tiles,
-    const uint32_t* __restrict__ offsets)
-{
-    __shared__ uint32_t wcnt[kWarps][kRadix];
-    __shared__ uint32_t dstart[kRadix];
-    __shared__ uint32_t skey[kTile];
-    __shared__ uint32_t sval[kTile];
-    __shared__ uint32_t scan_tmp[32];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PassSmem& S = *reinterpret_cast<PassSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for(int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&wcnt[0][0])[i] = 0;
+    const int shift = 8 * pass;
+    const uint32_t mask = digit_mask(bits, pass);
+    for(int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&S.wcnt[0][0])[i] = 0;
+    if(threadIdx.x == 0) S.tile = atomicAdd(&scratch[kTicketOff + pass], 1u);
     __syncthreads();
+    const uint32_t tile = S.tile;
+    const uint64_t epoch = scratch[kEpochOff];
+    uint64_t* status = reinterpret_cast<uint64_t*>(scratch + kStatusOff) + (int64_t)pass * tiles * kRadix;
 
-    const int64_t base = (int64_t)blockIdx.x * kTile;
+    const int64_t base = (int64_t)tile * kTile;
     uint32_t key[kItems], val[kItems], rank[kItems];
     const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
     for(int k = 0; k < kItems; k++) {
         int64_t idx = base + warp * (32 * kItems) + k * 32 + lane;
         bool ok = idx < n;
-        key[k] = ok ? keys_in[idx] : 0xffffffffu;
+        key[k] = ok ? keys_in[idx] : 0u;
         val[k] = ok ? (vals_in ? vals_in[idx] : (uint32_t)idx) : 0u;
-        uint32_t dg = ok ? (key[k] >> shift) & 255u : 256u;
+        uint32_t dg = ok ? (key[k] >> shift) & mask : 256u;
         uint32_t peers = __match_any_sync(0xffffffffu, dg);
         uint32_t r = 0;
-        if(ok) r = wcnt[warp][dg] + __popc(peers & lt);
+        if(ok) r = S.wcnt[warp][dg] + __popc(peers & lt);
         __syncwarp();
-        if(ok && (31 - __clz(peers)) == lane) wcnt[warp][dg] += __popc(peers);
+        if(ok && (31 - __clz(peers)) == lane) S.wcnt[warp][dg] += __popc(peers);
         __syncwarp();
         rank[k] = r;
     }
     __syncthreads();
-    // per digit: exclusive over warps, tile total; then exclusive over digits
+    // thread d owns digit d: exclusive over warps, tile total
+    const int d = threadIdx.x;
     uint32_t tot = 0;
-    for(int dg = threadIdx.x; dg < kRadix; dg += kThreads) {
+    {
         uint32_t off = 0;
-        for(int w = 0; w < kWarps; w++) { uint32_t c = wcnt[w][dg]; wcnt[w][dg] = off; off += c; }
+        for(int w = 0; w < kWarps; w++) { uint32_t c = S.wcnt[w][d]; S.wcnt[w][d] = off; off += c; }
         tot = off;
     }
+    // publish and look back (decoupled look-back, one digit per thread)
+    cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(status[(int64_t)tile * kRadix + d]);
+    uint32_t excl = 0;
+    if(tile == 0) {
+        mine.store((epoch << 34) | (kFlagInclusive << 32) | tot, cuda::memory_order_relaxed);
+    } else {
+        mine.store((epoch << 34) | (kFlagAggregate << 32) | tot, cuda::memory_order_relaxed);
+        int64_t j = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while(j >= 0) {
+            cuda::atomic_ref<uint64_t, cuda::thread_scope_device> other(status[j * kRadix + d]);
+            uint64_t w = other.load(cuda::memory_order_relaxed);
+            uint64_t flag = (w >> 34) == epoch ? (w >> 32) & 3u : 0u;
+            if(flag == 0) {
+                if(++spins > kSpinLimit) { atomicOr(err_flags, timeout_flag); break; }
+                continue;
+            }
+            excl += (uint32_t)w;
+            if(flag == kFlagInclusive) break;
+            j--;
+        }
+        mine.store((epoch << 34) | (kFlagInclusive << 32) | (excl + tot), cuda::memory_order_relaxed);
+    }
+    // global start of digit d: exclusive scan of the upfront histogram
+    uint32_t gtotal;
+    uint32_t gex = block_exclusive_scan(scratch[pass * kRadix + d], S.scan_tmp, gtotal);
+    S.gbase[d] = gex + excl;
     uint32_t total;
-    uint32_t ex = block_exclusive_scan(tot, scan_tmp, total);
-    if(threadIdx.x < kRadix) dstart[threadIdx.x] = ex;
+    uint32_t ex = block_exclusive_scan(tot, S.scan_tmp, total);
+    S.dstart[d] = ex;
     __syncthreads();
 #pragma unroll
     for(int k = 0; k < kItems; k++) {
         int64_t idx = base + warp * (32 * kItems) + k * 32 + lane;
         if(idx < n) {
-            uint32_t dg = (key[k] >> shift) & 255u;
-            uint32_t pos = dstart[dg] + wcnt[warp][dg] + rank[k];
-            skey[pos] = key[k];
-            sval[pos] = val[k];
+            uint32_t dg = (key[k] >> shift) & mask;
+            uint32_t pos = S.dstart[dg] + S.wcnt[warp][dg] + rank[k];
+            S.skey[pos] = key[k];
+            S.sval[pos] = val[k];
         }
     }
     __syncthreads();
-    int64_t tile_n = n - base < kTile ? n - base : kTile;
+    const int64_t tile_n = n - base < kTile ? n - base : kTile;
     for(int i = threadIdx.x; i < tile_n; i += kThreads) {
-        uint32_t k0 = skey[i];
-        uint32_t dg = (k0 >> shift) & 255u;
-        int64_t pos = (int64_t)offsets[(int64_t)dg * tiles + blockIdx.x] + (i - dstart[dg]);
+        uint32_t k0 = S.skey[i];
+        uint32_t dg = (k0 >> shift) & mask;
+        int64_t pos = (int64_t)S.gbase[dg] + (i - S.dstart[dg]);
         keys_out[pos] = k0;
-        vals_out[pos] = sval[i];
+        vals_out[pos] = S.sval[i];
     }
 }
 
-// Scratch: hist = 256*tiles words, part = ceil(256*tiles/chunk) words.
-inline int64_t hist_words(int64_t n) { return (int64_t)kRadix * tiles_for(n); }
-inline int64_t part_words(int64_t n) { return (kRadix * tiles_for(n) + kScanChunk - 1) / kScanChunk + 1; }
+inline size_t pass_smem() { return sizeof(PassSmem); }
 
-// Sorts keys[0..n) by their low `bits` bits.  On return *keys_out / *vals_out
-// point at whichever buffers hold the result (keys/keys_alt, vals/vals_alt).
-inline cudaError_t radix_sort(uint32_t* keys, uint32_t* keys_alt, uint32_t* vals, uint32_t* vals_alt,
-    int64_t n, int bits, uint32_t* hist, uint32_t* part, cudaStream_t st,
-    uint32_t** keys_out, uint32_t** vals_out)
+inline cudaError_t prepare()
 {
-    int passes = (bits + 7) / 8;
-    if(passes > kMaxPasses) passes = kMaxPasses;
-    if(passes < 1) passes = 1;
-    int64_t tiles = tiles_for(n);
-    *keys_out = keys;
-    *vals_out = nullptr;
+    return cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem());
+}
+
+// Sorts keys[0..n) by their low `bits` bits (1..32).  keys is read only;
+// the result lands in (keys_out, vals_out), which must not alias keys;
+// (keys_alt, vals_alt) are ping-pong buffers.  scratch = scratch_words(n)
+// words whose epoch region persists between sorts.  n < 2^30.
+inline cudaError_t radix_sort(const uint32_t* keys, uint32_t* keys_out, uint32_t* vals_out, uint32_t* keys_alt,
+    uint32_t* vals_alt, int64_t n, int bits, uint32_t* scratch, unsigned* err_flags, unsigned timeout_flag,
+    int hist_blocks, cudaStream_t st)
+{
     if(n == 0) return cudaSuccess;
-    int64_t len = (int64_t)kRadix * tiles;
-    int64_t chunks = (len + kScanChunk - 1) / kScanChunk;
-    uint32_t *kin = keys, *vin = nullptr, *kout = keys_alt, *vout = vals_alt;
+    int passes = (bits + 7) / 8;
+    int64_t tiles = tiles_for(n);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, kHistWords * sizeof(uint32_t), st);
+    if(e != cudaSuccess) return e;
+    int hb = (int)((n + kThreads * 16 - 1) / (kThreads * 16));
+    if(hb > hist_blocks) hb = hist_blocks;
+    if(hb < 1) hb = 1;
+    k_upfront_hist<<<hb, kThreads, 0, st>>>(keys, n, bits, scratch);
+    // ping-pong so that the last pass writes (keys_out, vals_out)
+    const uint32_t* kin = keys;
+    const uint32_t* vin = nullptr;
     for(int p = 0; p < passes; p++) {
-        uint32_t* h = hist;
-        k_hist<<<(unsigned)tiles, kThreads, 0, st>>>(kin, n, 8 * p, tiles, h);
-        k_scan_reduce<<<(unsigned)chunks, kThreads, 0, st>>>(h, len, part);
-        k_scan_partials<<<1, kThreads, 0, st>>>(part, chunks);
-        k_scan_down<<<(unsigned)chunks, kThreads, 0, st>>>(h, len, part);
-        k_scatter<<<(unsigned)tiles, kThreads, 0, st>>>(kin, vin, kout, vout, n, 8 * p, tiles, h);
-        // ping-pong: keys <-> keys_alt, vals_alt <-> vals
-        kin = kout;
-        vin = vout;
-        kout = (kout == keys_alt) ? keys : keys_alt;
-        vout = (vout == vals_alt) ? vals : vals_alt;
+        bool last_to_out = ((passes - 1 - p) % 2) == 0;
+        uint32_t* ko = last_to_out ? keys_out : keys_alt;
+        uint32_t* vo = last_to_out ? vals_out : vals_alt;
+        k_onesweep<<<(unsigned)tiles, kThreads, pass_smem(), st>>>(kin, vin, ko, vo, n, bits, p, tiles, scratch,
+                                                                    err_flags, timeout_flag);
+        kin = ko;
+        vin = vo;
     }
-    *keys_out = kin;
-    *vals_out = vin;
     return cudaGetLastError();
 }
 
