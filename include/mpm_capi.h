@@ -186,6 +186,27 @@ int mpm_count_valid(mpm_handle* h, int64_t* count);
 int mpm_set_timing(mpm_handle* h, int enable);
 int mpm_get_timing(mpm_handle* h, char* names, int names_len, double* ms, int64_t* launches, int max_entries, int* count);
 
+/* ---- differentiation ------------------------------------------------------ */
+
+/* Records a differentiable rollout: nsteps explicit substeps from the current
+ * particles, keeping the particle state every checkpoint_every substeps.
+ * MPM_PATH_PLAIN, 3D, no collision objects.  The reference has no reverse
+ * mode; this is the forward whose transposed linearisation mpm_diff_backward
+ * applies (the reference's linearisations of the same maps are
+ * MPM_FINITE_ELEMENTS::Add_Hessian_Times, Hybrid_Methods/Forces/
+ * MPM_FINITE_ELEMENTS.cpp:103-132, and MPM_OBJECTIVE::Update_F,
+ * Hybrid_Methods/System/MPM_OBJECTIVE.cpp:95-134).  The handle ends at the
+ * final state. */
+int mpm_diff_forward(mpm_handle* h, double dt, int nsteps, int checkpoint_every);
+
+/* Reverse pass of the last mpm_diff_forward: given dL/d(final X, V, F, B) in
+ * grad_final, writes dL/d(initial X, V, F, B) to grad_initial and dL/dmu,
+ * dL/dlambda (n each) to grad_mu / grad_lambda.  Segments between checkpoints
+ * are recomputed.  Views carry only X, V, F, B; dtype must equal the path's
+ * precision; on_device selects device or host pointers. */
+int mpm_diff_backward(mpm_handle* h, const mpm_particles_view* grad_final, mpm_particles_view* grad_initial,
+                      void* grad_mu, void* grad_lambda);
+
 /* ---- sorting ------------------------------------------------------------- */
 
 /* Stable LSD radix sort of n 32-bit keys by their low `bits` bits (1..32) on

@@ -172,6 +172,7 @@ int mpm_destroy(mpm_handle* h)
     release_graph(h);
     drain_timers(h);
     for(cudaEvent_t e: h->event_pool) cudaEventDestroy(e);
+    diff_free(h);
     plain_free(h);
     fast_free(h);
     cudaFree(h->d_flags);
@@ -219,6 +220,7 @@ int mpm_set_particles(mpm_handle* h, const mpm_particles_view* v)
     if(!h || !v || v->n < 0) return MPM_ERR_ARG;
     if(v->dtype != MPM_FP32 && v->dtype != MPM_FP64) return set_error(h, MPM_ERR_ARG, "dtype");
     release_graph(h);
+    diff_free(h);
     int rc = fast(h) ? fast_set_particles(h, v) : plain_set_particles(h, v);
     if(rc) return rc;
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -327,6 +329,24 @@ int mpm_count_valid(mpm_handle* h, int64_t* count)
     if(!h || !count) return MPM_ERR_ARG;
     if(!h->have_particles) { *count = 0; return MPM_OK; }
     return fast(h) ? fast_count_valid(h, count) : plain_count_valid(h, count);
+}
+
+int mpm_diff_forward(mpm_handle* h, double dt, int nsteps, int checkpoint_every)
+{
+    int rc = check_dt(h, dt);
+    if(rc) return rc;
+    release_graph(h);
+    if((rc = diff_forward(h, dt, nsteps, checkpoint_every))) return rc;
+    return mpm_synchronize(h);
+}
+
+int mpm_diff_backward(mpm_handle* h, const mpm_particles_view* grad_final, mpm_particles_view* grad_initial,
+    void* grad_mu, void* grad_lambda)
+{
+    if(!h || !grad_final || !grad_initial) return MPM_ERR_ARG;
+    int rc = diff_backward(h, grad_final, grad_initial, grad_mu, grad_lambda);
+    if(rc) return rc;
+    return read_flags(h);
 }
 
 int mpm_radix_sort_u32(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm)

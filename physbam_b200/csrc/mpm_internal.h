@@ -101,6 +101,8 @@ struct mpm_handle {
     // one captured substep per particle-buffer parity (the fast path swaps buffers)
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};
     double graph_dt = 0;
+    // checkpoints of the last mpm_diff_forward (mpm_adjoint.cu)
+    void* diff = nullptr;
     std::string last_error;
 };
 
@@ -131,6 +133,11 @@ int fast_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf);
 int fast_count_valid(mpm_handle* h, int64_t* c);
 int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm);
 int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm);
+
+// adjoint (mpm_adjoint.cu)
+int diff_forward(mpm_handle* h, double dt, int nsteps, int every);
+int diff_backward(mpm_handle* h, const mpm_particles_view* gout, mpm_particles_view* gin, void* gmu, void* glam);
+void diff_free(mpm_handle* h);
 
 // helpers
 int set_error(mpm_handle* h, int code, const std::string& msg);

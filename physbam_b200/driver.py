@@ -60,7 +60,8 @@ class ParticlesView(ctypes.Structure):
 EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_objects", "mpm_set_particles",
            "mpm_get_particles", "mpm_substep", "mpm_advance", "mpm_particle_to_grid", "mpm_apply_forces",
            "mpm_grid_to_particle", "mpm_synchronize", "mpm_get_grid", "mpm_count_valid", "mpm_set_timing",
-           "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state"]
+           "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state",
+           "mpm_diff_forward", "mpm_diff_backward"]
 
 _lib = None
 
@@ -90,6 +91,8 @@ def load_library(path: str = LIB_PATH):
     L.mpm_set_timing.argtypes = [P, ctypes.c_int]
     L.mpm_get_timing.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.mpm_last_error.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
+    L.mpm_diff_forward.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    L.mpm_diff_backward.argtypes = [P, ctypes.POINTER(ParticlesView), ctypes.POINTER(ParticlesView), P, P]
     L.mpm_radix_sort_u32.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P]
     L.mpm_debug_sort_state.argtypes = [P, P, P, P]
     L.mpm_status_string.argtypes = [ctypes.c_int]
@@ -198,6 +201,66 @@ class MPM_DRIVER:
         F = np.swapaxes(F.reshape(n, d, d), 1, 2)
         B = np.swapaxes(B.reshape(n, d, d), 1, 2)
         return {"X": X, "V": V, "F": F, "B": B, "valid": valid.astype(bool)}
+
+    # -- device-resident arrays (torch tensors on the handle's device) ------------
+    def _dev_view(self, X, V, Fc, Bc, mass=None, volume=None, mu=None, lam=None, valid=None):
+        import torch
+        ts = [X, V, Fc, Bc, mass, volume, mu, lam]
+        dt = X.dtype
+        for t in ts:
+            if t is not None:
+                assert t.is_cuda and t.is_contiguous() and t.dtype == dt, "contiguous CUDA tensors of one dtype"
+        v = ParticlesView()
+        v.n, v.on_device = X.shape[0], 1
+        v.dtype = FP64 if dt == torch.float64 else FP32
+        v.X, v.V, v.F, v.B = X.data_ptr(), V.data_ptr(), Fc.data_ptr(), Bc.data_ptr()
+        if mass is not None:
+            v.mass, v.volume, v.mu, v.lambda_ = mass.data_ptr(), volume.data_ptr(), mu.data_ptr(), lam.data_ptr()
+        if valid is not None:
+            v.valid = valid.data_ptr()
+        return v
+
+    def set_particles_device(self, X, V, Fc, Bc, mass, volume, mu, lam):
+        """Device tensors; F and B column-major per particle (i.e. F[p].T flattened)."""
+        import torch
+        torch.cuda.current_stream().synchronize()
+        v = self._dev_view(X, V, Fc, Bc, mass, volume, mu, lam)
+        self._check(self.L.mpm_set_particles(self.h, ctypes.byref(v)), "mpm_set_particles")
+        self.n = X.shape[0]
+
+    def get_particles_device(self, dtype):
+        import torch
+        n, d = self.n, self.dim
+        X = torch.empty((n, d), dtype=dtype, device="cuda")
+        V = torch.empty_like(X)
+        Fc = torch.empty((n, d * d), dtype=dtype, device="cuda")
+        Bc = torch.empty_like(Fc)
+        valid = torch.empty(n, dtype=torch.uint8, device="cuda")
+        torch.cuda.current_stream().synchronize()
+        v = self._dev_view(X, V, Fc, Bc, valid=valid)
+        self._check(self.L.mpm_get_particles(self.h, ctypes.byref(v)), "mpm_get_particles")
+        return X, V, Fc, Bc, valid
+
+    # -- differentiation -------------------------------------------------------
+    def diff_forward(self, nsteps, checkpoint_every=8, dt=None):
+        dt = self.scene.dt if dt is None else dt
+        self._check(self.L.mpm_diff_forward(self.h, dt, nsteps, checkpoint_every), "mpm_diff_forward")
+        self.time += nsteps * dt
+
+    def diff_backward(self, gX, gV, gFc, gBc):
+        """Device tensors of dL/d(final X, V, F col-major, B col-major); returns the initial-state grads + mu, lambda."""
+        import torch
+        n = self.n
+        out = [torch.empty_like(gX), torch.empty_like(gV), torch.empty_like(gFc), torch.empty_like(gBc)]
+        gmu = torch.empty(n, dtype=gX.dtype, device="cuda")
+        glam = torch.empty_like(gmu)
+        torch.cuda.current_stream().synchronize()
+        vin = self._dev_view(gX.contiguous(), gV.contiguous(), gFc.contiguous(), gBc.contiguous())
+        vout = self._dev_view(*out)
+        self._check(self.L.mpm_diff_backward(self.h, ctypes.byref(vin), ctypes.byref(vout),
+                                             ctypes.c_void_p(gmu.data_ptr()), ctypes.c_void_p(glam.data_ptr())),
+                    "mpm_diff_backward")
+        return (*out, gmu, glam)
 
     # -- the substep (MPM_DRIVER.cpp:141-157) --------------------------------
     def Advance_One_Time_Step(self, dt: Optional[float] = None):
