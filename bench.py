@@ -255,6 +255,8 @@ def our_arm(args):
     from physbam_b200 import scenes as S
 
     peak, peak_kind = measured_peaks()
+    if args.scene:
+        return profile_case(args, D, S)
     scene = S.spheres_3d()
     n = scene.n
     drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
@@ -341,6 +343,27 @@ def our_arm(args):
     return 0
 
 
+def profile_case(args, D, S):
+    """Small single-scene run for profilers: `--scene NAME --grid G` (no e2e, no CPU, no flush).
+    Prints one JSON line with the per-kernel times; used to make the ncu summaries."""
+    import torch
+    make = {"spheres3d": S.spheres_3d, "dam3d": S.dam_3d, "cube3d": S.cube_3d}[args.scene]
+    scene = make(G=args.grid) if args.grid else make()
+    drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+    drv.set_scene_particles(scene, dtype=np.float32)
+    drv.advance(args.warmup)
+    drv.synchronize()
+    drv.set_timing(True)
+    for _ in range(args.steps):
+        drv.Advance_One_Time_Step()
+    drv.synchronize()
+    kt = drv.get_timing()
+    drv.close()
+    print(json.dumps({"scene": args.scene, "grid": args.grid, "particles": scene.n, "steps": args.steps,
+                      "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in kt.items()}}), flush=True)
+    return 0
+
+
 def measure_large(args, D, S, stream, flush, peak, peak_kind):
     """The 256^3 dam-break scene (36M particles): the HBM-bound regime of the same kernels."""
     scene = S.dam_3d()
@@ -371,6 +394,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-large", action="store_true", help="skip the 256^3 dam-break measurement")
+    ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d"], help="profiling run of one scene only")
+    ap.add_argument("--grid", type=int, default=0, help="grid cells per side for --scene")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

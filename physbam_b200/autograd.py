@@ -56,6 +56,17 @@ def rollout(drv, X, V, F, B, mu, lam, mass, volume, nsteps, checkpoint_every=8):
 
 
 def com_loss(X, mass, target):
-    """Squared distance of the final mass-weighted centre of mass to `target`."""
+    """Squared distance of the final mass-weighted centre of mass to `target`.
+
+    Internal forces conserve momentum, so without collision objects this loss
+    depends on v0 and gravity only; its gradient w.r.t. E is zero."""
     com = (mass[:, None] * X).sum(0) / mass.sum()
+    return ((com - target) ** 2).sum()
+
+
+def part_com_loss(X, mass, part, target):
+    """Same loss for the centre of mass of a subset `part` (bool mask) of the
+    particles; it moves with the body's deformation, so it depends on E."""
+    m = mass * part
+    com = (m[:, None] * X).sum(0) / m.sum()
     return ((com - target) ** 2).sum()

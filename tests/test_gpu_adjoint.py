@@ -1,6 +1,9 @@
 """GPU tests of the hand-written adjoint (mpm_diff_forward / mpm_diff_backward).
 
-Loss: squared distance of the final centre of mass to a seeded target; the
+Loss: squared distance of the final centre of mass to a seeded target (the
+BASELINE loss; the v0 checks use it) and the same for the half of the body
+that starts at x > 0.5 (it moves with the deformation, so the E checks use
+it -- the whole-body centre of mass does not depend on E at all).  The
 parameters are the initial velocity v0 (shared by all particles) and the
 per-particle Young's modulus E.  Gradients are checked against central finite
 differences of the FP64 forward (step scanned, best kept), in FP64 and FP32,
@@ -24,7 +27,7 @@ def setup(scene, prec):
     return drv, dtype, t
 
 
-def loss_fn(drv, scene, t, dtype, v0, E, nsteps, every, want_grad):
+def loss_fn(drv, scene, t, dtype, v0, E, nsteps, every, want_grad, part=False):
     import torch
     from physbam_b200 import autograd as A
     nu = 0.3
@@ -40,7 +43,10 @@ def loss_fn(drv, scene, t, dtype, v0, E, nsteps, every, want_grad):
     lam = Et * nu / ((1 + nu) * (1 - 2 * nu))
     V = v0t.expand(n, 3).contiguous()
     X1, V1, F1, B1, valid = A.rollout(drv, X, V, F, B, mu, lam, mass, vol, nsteps, every)
-    L = A.com_loss(X1, mass, target)
+    if part:
+        L = A.part_com_loss(X1, mass, t(scene.X[:, 0] > 0.5), target)
+    else:
+        L = A.com_loss(X1, mass, target)
     if not want_grad:
         return float(L)
     L.backward()
@@ -62,14 +68,16 @@ def check_case(scene, nsteps, every, tol=1e-3, E_dir_seed=0):
     E = scene.mu * 2 * (1 + 0.3)
     drv64, dt64, t64 = setup(scene, D.FP64)
     f_v = lambda v: loss_fn(drv64, scene, t64, dt64, v, E, nsteps, every, False)
-    f_E = lambda e: loss_fn(drv64, scene, t64, dt64, v0, e, nsteps, every, False)
-    L64, gv64, gE64 = loss_fn(drv64, scene, t64, dt64, v0, E, nsteps, every, True)
+    f_E = lambda e: loss_fn(drv64, scene, t64, dt64, v0, e, nsteps, every, False, part=True)
+    L64, gv64, _ = loss_fn(drv64, scene, t64, dt64, v0, E, nsteps, every, True)
+    _, _, gE64 = loss_fn(drv64, scene, t64, dt64, v0, E, nsteps, every, True, part=True)
     rng = np.random.default_rng(E_dir_seed)
     dirE = rng.standard_normal(scene.n) * E * 0.1
     ests_v = [fd(f_v, v0, np.eye(3)[k]) for k in range(3)]
     est_E = fd(lambda s: f_E(E + s * dirE), 0.0, 1.0, hs=(1e-2, 3e-3, 1e-3, 3e-4))
     drv32, dt32, t32 = setup(scene, D.FP32)
-    L32, gv32, gE32 = loss_fn(drv32, scene, t32, dt32, v0, E, nsteps, every, True)
+    L32, gv32, _ = loss_fn(drv32, scene, t32, dt32, v0, E, nsteps, every, True)
+    _, _, gE32 = loss_fn(drv32, scene, t32, dt32, v0, E, nsteps, every, True, part=True)
     scale_v = np.linalg.norm(gv64)
     out = {}
     for name, gv, gE in (("fp64", gv64, gE64), ("fp32", gv32, gE32)):
@@ -103,7 +111,7 @@ def test_checkpoint_interval_does_not_change_gradients(cuda_device):
     res = []
     for every in (1, 5, 12):
         drv, dt, t = setup(scene, D.FP64)
-        res.append(loss_fn(drv, scene, t, dt, v0, E, 12, every, True))
+        res.append(loss_fn(drv, scene, t, dt, v0, E, 12, every, True, part=True))
         drv.close()
     for r in res[1:]:
         np.testing.assert_allclose(r[1], res[0][1], rtol=1e-12)
