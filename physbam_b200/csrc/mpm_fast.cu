@@ -230,113 +230,132 @@ __device__ __forceinline__ int next_work(uint32_t* ctr, int* s_work)
     return *s_work;
 }
 
-template<int THREADS> __global__ void __launch_bounds__(THREADS) k_p2g(FastArgs a)
+// P2G, one thread per cell of the block.  A thread walks the particles of its
+// cell (they share the 27 nodes) and accumulates mass and momentum plus dt*force
+// for those nodes in registers, then adds them to the block's shared tile: one
+// shared atomic per node value per cell instead of per particle, and the 64
+// lanes of a block hit 64 different node addresses for any given offset.
+//   p_i += w m (V + B D (Z_i - X)) - dt vol S g,   m_i += w m
+// is evaluated separably: per (x, y) offset pair the terms that do not depend
+// on z are formed once, leaving three FMAs per node component.
+__global__ void __launch_bounds__(64) k_p2g(FastArgs a)
 {
     __shared__ float tm[TN], tx[TN], ty[TN], tz[TN];
     __shared__ uint32_t ccount[64], cstart[64];
-    __shared__ uint32_t s_maxc;
     __shared__ int s_work;
     const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
     const float Dx = 4.f * a.inv[0] * a.inv[0], Dy = 4.f * a.inv[1] * a.inv[1], Dz = 4.f * a.inv[2] * a.inv[2];
+    const int c = threadIdx.x;   // cell in block: (lx << 4) | (ly << 2) | lz
+    const int lx = c >> 4, ly = (c >> 2) & 3, lz = c & 3;
     for(int w = next_work(&a.counters[CNT_P2G_WORK], &s_work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &s_work)) {
         uint32_t b = a.active[w];
         int bx, by, bz;
         block_coords(a, b, bx, by, bz);
         const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;   // tile origin, ghosted node coords
-        for(int t = threadIdx.x; t < TN; t += THREADS) { tm[t] = 0; tx[t] = 0; ty[t] = 0; tz[t] = 0; }
-        if(threadIdx.x < 64) ccount[threadIdx.x] = 0;
+        for(int t = c; t < TN; t += 64) { tm[t] = 0; tx[t] = 0; ty[t] = 0; tz[t] = 0; }
+        ccount[c] = 0;
         __syncthreads();
         const uint32_t s = a.bstart[b], e = a.bend[b];
-        // particles of a block arrive sorted by cell; count them per cell so the
-        // loop below can hand each lane of a warp a particle of a different cell:
-        // then no two lanes of one shared-memory atomic hit the same node.
-        for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) atomicAdd(&ccount[a.sorted_keys[j] & 63u], 1u);
+        for(uint32_t j = s + c; j < e; j += 64) atomicAdd(&ccount[a.sorted_keys[j] & 63u], 1u);
         __syncthreads();
-        if(threadIdx.x < 32) {
-            uint32_t c0 = ccount[2 * threadIdx.x], c1 = ccount[2 * threadIdx.x + 1];
-            uint32_t sum = c0 + c1, x = sum, mx = c0 > c1 ? c0 : c1;
+        if(c < 32) {
+            uint32_t c0 = ccount[2 * c], c1 = ccount[2 * c + 1];
+            uint32_t sum = c0 + c1, x = sum;
 #pragma unroll
             for(int o = 1; o < 32; o <<= 1) {
                 uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                if((int)threadIdx.x >= o) x += y;
-                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                if(c >= o) x += y;
             }
-            cstart[2 * threadIdx.x] = x - sum;
-            cstart[2 * threadIdx.x + 1] = x - sum + c0;
-            if(threadIdx.x == 0) s_maxc = mx;
+            cstart[2 * c] = x - sum;
+            cstart[2 * c + 1] = x - sum + c0;
         }
         __syncthreads();
-        const uint32_t slots = s_maxc * 64u;
-        for(uint32_t q = threadIdx.x; q < slots; q += THREADS) {
-            const uint32_t c = q & 63u, r = q >> 6;
-            if(r >= ccount[c]) continue;
-            const uint32_t i = a.perm[s + cstart[c] + r];
-            float X[3], V[3], F[9], Bm[9];
+        const uint32_t cnt = ccount[c], beg = s + cstart[c];
+        if(cnt) {
+            float am[27], ax[27], ay[27], az[27];
 #pragma unroll
-            for(int k = 0; k < 3; k++) { X[k] = a.src[(C_X + k) * a.npad + i]; V[k] = a.src[(C_V + k) * a.npad + i]; }
+            for(int q = 0; q < 27; q++) { am[q] = 0; ax[q] = 0; ay[q] = 0; az[q] = 0; }
+            for(uint32_t k = 0; k < cnt; k++) {
+                const uint32_t i = a.perm[beg + k];
+                float X[3], V[3], F[9], Bm[9];
 #pragma unroll
-            for(int k = 0; k < 9; k++) { F[k] = a.src[(C_F + k) * a.npad + i]; Bm[k] = a.src[(C_B + k) * a.npad + i]; }
-            const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
-            float PFT[9];
-            if(!stress_fast(a.sp.model, F, at.z, at.w, PFT)) {
-                atomicAdd(&a.counters[CNT_FALLBACK], 1u);
-                if(!stress_fp64(a.sp.model, F, at.z, at.w, PFT)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
-            }
-            Axis<float> ax[3];
+                for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
 #pragma unroll
-            for(int k = 0; k < 3; k++) ax[k] = spline_axis<float>(X[k], a.dmin[k], a.dx[k], a.inv[k]);
-            const int lx = ax[0].base + MPM_GHOST - ox, ly = ax[1].base + MPM_GHOST - oy, lz = ax[2].base + MPM_GHOST - oz;
-            // stress term: dt * volume * PFT ; affine term: mass * B * Dp^-1 applied per axis offset
-            const float sv = a.dt * at.y;
-            float S[9];
-#pragma unroll
-            for(int k = 0; k < 9; k++) S[k] = sv * PFT[k];
-            const float m = at.x;
-            float mv[3] = {m * V[0], m * V[1], m * V[2]};
-            float ux[3][3], uy[3][3], uz[3][3];   // [offset][component] = m B[:,axis] D (Z_axis - X_axis)
-#pragma unroll
-            for(int o = 0; o < 3; o++) {
-                float dxo = (a.dmin[0] + ((float)(ax[0].base + o) + 0.5f) * a.dx[0] - X[0]) * Dx * m;
-                float dyo = (a.dmin[1] + ((float)(ax[1].base + o) + 0.5f) * a.dx[1] - X[1]) * Dy * m;
-                float dzo = (a.dmin[2] + ((float)(ax[2].base + o) + 0.5f) * a.dx[2] - X[2]) * Dz * m;
-#pragma unroll
-                for(int r = 0; r < 3; r++) {
-                    ux[o][r] = Bm[r + 0] * dxo;
-                    uy[o][r] = Bm[r + 3] * dyo;
-                    uz[o][r] = Bm[r + 6] * dzo;
+                for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; Bm[r] = a.src[(C_B + r) * a.npad + i]; }
+                const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
+                float S[9];
+                if(!stress_fast(a.sp.model, F, at.z, at.w, S)) {
+                    atomicAdd(&a.counters[CNT_FALLBACK], 1u);
+                    if(!stress_fp64(a.sp.model, F, at.z, at.w, S)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
                 }
+                const float sv = a.dt * at.y, m = at.x;
+#pragma unroll
+                for(int r = 0; r < 9; r++) S[r] *= sv;
+                Axis<float> wx = spline_axis<float>(X[0], a.dmin[0], a.dx[0], a.inv[0]);
+                Axis<float> wy = spline_axis<float>(X[1], a.dmin[1], a.dx[1], a.inv[1]);
+                Axis<float> wz = spline_axis<float>(X[2], a.dmin[2], a.dx[2], a.inv[2]);
+                // affine term m B D (Z - X), separable per axis offset
+                float ux[3][3], uy[3][3], uz[3][3];
+#pragma unroll
+                for(int o = 0; o < 3; o++) {
+                    float dxo = (a.dmin[0] + ((float)(wx.base + o) + 0.5f) * a.dx[0] - X[0]) * Dx * m;
+                    float dyo = (a.dmin[1] + ((float)(wy.base + o) + 0.5f) * a.dx[1] - X[1]) * Dy * m;
+                    float dzo = (a.dmin[2] + ((float)(wz.base + o) + 0.5f) * a.dx[2] - X[2]) * Dz * m;
+#pragma unroll
+                    for(int r = 0; r < 3; r++) {
+                        ux[o][r] = Bm[r] * dxo + m * V[r];   // the x factor also carries m V
+                        uy[o][r] = Bm[r + 3] * dyo;
+                        uz[o][r] = Bm[r + 6] * dzo;
+                    }
+                }
+#pragma unroll
+                for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+                    for(int jj = 0; jj < 3; jj++) {
+                        const float wxy = wx.w[ii] * wy.w[jj];
+                        const float gx0 = wx.dw[ii] * wy.w[jj], gy0 = wx.w[ii] * wy.dw[jj];
+                        const float mxy = m * wxy;
+                        float P[3], Cc[3];
+#pragma unroll
+                        for(int r = 0; r < 3; r++) {
+                            P[r] = wxy * (ux[ii][r] + uy[jj][r]) - (S[r] * gx0 + S[r + 3] * gy0);
+                            Cc[r] = S[r + 6] * wxy;
+                        }
+#pragma unroll
+                        for(int kk = 0; kk < 3; kk++) {
+                            const int q = (ii * 3 + jj) * 3 + kk;
+                            const float wzk = wz.w[kk], dwz = wz.dw[kk], wq = wxy * wzk;
+                            am[q] += mxy * wzk;
+                            ax[q] += wzk * P[0] + wq * uz[kk][0] - Cc[0] * dwz;
+                            ay[q] += wzk * P[1] + wq * uz[kk][1] - Cc[1] * dwz;
+                            az[q] += wzk * P[2] + wq * uz[kk][2] - Cc[2] * dwz;
+                        }
+                    }
             }
+            const int t0 = (lx * TE + ly) * TE + lz;
 #pragma unroll
             for(int ii = 0; ii < 3; ii++)
 #pragma unroll
-                for(int jj = 0; jj < 3; jj++) {
-                    const float wxy = ax[0].w[ii] * ax[1].w[jj];
-                    const float gx0 = ax[0].dw[ii] * ax[1].w[jj], gy0 = ax[0].w[ii] * ax[1].dw[jj];
+                for(int jj = 0; jj < 3; jj++)
 #pragma unroll
                     for(int kk = 0; kk < 3; kk++) {
-                        const float w = wxy * ax[2].w[kk];
-                        const float g0 = gx0 * ax[2].w[kk], g1 = gy0 * ax[2].w[kk], g2 = wxy * ax[2].dw[kk];
-                        const int t = ((lx + ii) * TE + (ly + jj)) * TE + (lz + kk);
-                        float px = w * (mv[0] + ux[ii][0] + uy[jj][0] + uz[kk][0]) - (S[0] * g0 + S[3] * g1 + S[6] * g2);
-                        float py = w * (mv[1] + ux[ii][1] + uy[jj][1] + uz[kk][1]) - (S[1] * g0 + S[4] * g1 + S[7] * g2);
-                        float pz = w * (mv[2] + ux[ii][2] + uy[jj][2] + uz[kk][2]) - (S[2] * g0 + S[5] * g1 + S[8] * g2);
-                        atomicAdd(&tm[t], w * m);
-                        atomicAdd(&tx[t], px);
-                        atomicAdd(&ty[t], py);
-                        atomicAdd(&tz[t], pz);
+                        const int q = (ii * 3 + jj) * 3 + kk, t = t0 + (ii * TE + jj) * TE + kk;
+                        atomicAdd(&tm[t], am[q]);
+                        atomicAdd(&tx[t], ax[q]);
+                        atomicAdd(&ty[t], ay[q]);
+                        atomicAdd(&tz[t], az[q]);
                     }
-                }
         }
         __syncthreads();
-        for(int t = threadIdx.x; t < TN; t += THREADS) {
+        for(int t = c; t < TN; t += 64) {
             float mm = tm[t];
             if(mm != 0.f) {
                 int qx = ox + t / (TE * TE), qy = oy + (t / TE) % TE, qz = oz + t % TE;
                 atomicAdd(&a.acc[node_index(a, qx, qy, qz)], make_float4(tx[t], ty[t], tz[t], mm));
             }
         }
-        if(threadIdx.x < 8) {
-            int nx = bx + (threadIdx.x >> 2), ny = by + ((threadIdx.x >> 1) & 1), nz = bz + (threadIdx.x & 1);
+        if(c < 8) {
+            int nx = bx + (c >> 2), ny = by + ((c >> 1) & 1), nz = bz + (c & 1);
             uint32_t nb = ((uint32_t)nx * a.NN[1] + ny) * a.NN[2] + nz;
             if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.counters[CNT_NODE_BLOCKS], 1u)] = nb;
         }
@@ -380,6 +399,16 @@ __global__ void __launch_bounds__(64) k_grid(FastArgs a)
     }
 }
 
+// G2P, one thread per particle in sorted order (coalesced).  The tile of
+// (v_new, v_fric) is staged in shared memory; the sums over the 27 nodes are
+// taken separably (z first, then y, then x), so each node costs two 16-byte
+// shared loads and twelve FMAs:
+//   V' = sum w vn,  G = sum vn g^T,  Vf = sum w vf,  Bv = sum w vf (Z - X)^T.
+// The antisymmetric part of the reference's B (MPM_DRIVER.cpp:482-485,503-508),
+//   dt/2 [sum w (vf vn^T - vn vf^T) - (Vf V'^T - V' Vf^T)],
+// is non-zero only where the grid update changed v_fric against v_new (nodes
+// that met a collision object), so it is summed only for tiles holding such
+// nodes.
 template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
 {
     __shared__ float4 tv[2 * TN];
@@ -391,12 +420,16 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
         int bx, by, bz;
         block_coords(a, b, bx, by, bz);
         const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;
-        for(int t = threadIdx.x; t < 2 * TN; t += THREADS) {
-            int nd = t >> 1;
-            int qx = ox + nd / (TE * TE), qy = oy + (nd / TE) % TE, qz = oz + nd % TE;
-            tv[t] = a.vel[2 * node_index(a, qx, qy, qz) + (t & 1)];
+        int differs = 0;
+        for(int t = threadIdx.x; t < TN; t += THREADS) {
+            int qx = ox + t / (TE * TE), qy = oy + (t / TE) % TE, qz = oz + t % TE;
+            int64_t q = node_index(a, qx, qy, qz);
+            float4 p0 = a.vel[2 * q], p1 = a.vel[2 * q + 1];
+            tv[2 * t] = p0;
+            tv[2 * t + 1] = p1;
+            differs |= (p0.w != p0.x) | (p1.x != p0.y) | (p1.y != p0.z);
         }
-        __syncthreads();
+        const bool anti = __syncthreads_or(differs) != 0;
         const uint32_t s = a.bstart[b], e = a.bend[b];
         for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
             const uint32_t i = a.perm[j];
@@ -405,41 +438,60 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
             for(int k = 0; k < 3; k++) X[k] = a.src[(C_X + k) * a.npad + i];
 #pragma unroll
             for(int k = 0; k < 9; k++) F[k] = a.src[(C_F + k) * a.npad + i];
-            Axis<float> ax[3];
+            const float4 at = a.src_attr[i];
+            const int pid = a.src_pid[i];
+            Axis<float> wx = spline_axis<float>(X[0], a.dmin[0], a.dx[0], a.inv[0]);
+            Axis<float> wy = spline_axis<float>(X[1], a.dmin[1], a.dx[1], a.inv[1]);
+            Axis<float> wz = spline_axis<float>(X[2], a.dmin[2], a.dx[2], a.inv[2]);
+            const int t0 = ((wx.base + MPM_GHOST - ox) * TE + (wy.base + MPM_GHOST - oy)) * TE + (wz.base + MPM_GHOST - oz);
+            float dX[3], dY[3], wzd[3];
 #pragma unroll
-            for(int k = 0; k < 3; k++) ax[k] = spline_axis<float>(X[k], a.dmin[k], a.dx[k], a.inv[k]);
-            const int lx = ax[0].base + MPM_GHOST - ox, ly = ax[1].base + MPM_GHOST - oy, lz = ax[2].base + MPM_GHOST - oz;
-            float dX[3][3];   // [axis][offset]: Z - X
-#pragma unroll
-            for(int o = 0; o < 3; o++)
-#pragma unroll
-                for(int k = 0; k < 3; k++) dX[k][o] = a.dmin[k] + ((float)(ax[k].base + o) + 0.5f) * a.dx[k] - X[k];
+            for(int o = 0; o < 3; o++) {
+                dX[o] = a.dmin[0] + ((float)(wx.base + o) + 0.5f) * a.dx[0] - X[0];
+                dY[o] = a.dmin[1] + ((float)(wy.base + o) + 0.5f) * a.dx[1] - X[1];
+                wzd[o] = wz.w[o] * (a.dmin[2] + ((float)(wz.base + o) + 0.5f) * a.dx[2] - X[2]);
+            }
             float Vp[3] = {0, 0, 0}, Vf[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Bv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             float K01 = 0, K02 = 0, K12 = 0;
 #pragma unroll
             for(int ii = 0; ii < 3; ii++)
 #pragma unroll
                 for(int jj = 0; jj < 3; jj++) {
-                    const float wxy = ax[0].w[ii] * ax[1].w[jj];
-                    const float gx0 = ax[0].dw[ii] * ax[1].w[jj], gy0 = ax[0].w[ii] * ax[1].dw[jj];
+                    float Sw[3] = {0, 0, 0}, Sd[3] = {0, 0, 0}, Tw[3] = {0, 0, 0}, Td[3] = {0, 0, 0};
+                    float k01 = 0, k02 = 0, k12 = 0;
 #pragma unroll
                     for(int kk = 0; kk < 3; kk++) {
-                        const float wt = wxy * ax[2].w[kk];
-                        const float g0 = gx0 * ax[2].w[kk], g1 = gy0 * ax[2].w[kk], g2 = wxy * ax[2].dw[kk];
-                        const int t = ((lx + ii) * TE + (ly + jj)) * TE + (lz + kk);
+                        const int t = t0 + (ii * TE + jj) * TE + kk;
                         const float4 p0 = tv[2 * t], p1 = tv[2 * t + 1];
                         const float vn[3] = {p0.x, p0.y, p0.z}, vf[3] = {p0.w, p1.x, p1.y};
-                        const float wf[3] = {wt * vf[0], wt * vf[1], wt * vf[2]};
 #pragma unroll
                         for(int r = 0; r < 3; r++) {
-                            Vp[r] += wt * vn[r];
-                            Vf[r] += wf[r];
-                            G[r] += vn[r] * g0; G[r + 3] += vn[r] * g1; G[r + 6] += vn[r] * g2;
-                            Bv[r] += wf[r] * dX[0][ii]; Bv[r + 3] += wf[r] * dX[1][jj]; Bv[r + 6] += wf[r] * dX[2][kk];
+                            Sw[r] += vn[r] * wz.w[kk];
+                            Sd[r] += vn[r] * wz.dw[kk];
+                            Tw[r] += vf[r] * wz.w[kk];
+                            Td[r] += vf[r] * wzd[kk];
                         }
-                        K01 += wf[0] * vn[1] - wf[1] * vn[0];
-                        K02 += wf[0] * vn[2] - wf[2] * vn[0];
-                        K12 += wf[1] * vn[2] - wf[2] * vn[1];
+                        if(anti) {
+                            k01 += wz.w[kk] * (vf[0] * vn[1] - vf[1] * vn[0]);
+                            k02 += wz.w[kk] * (vf[0] * vn[2] - vf[2] * vn[0]);
+                            k12 += wz.w[kk] * (vf[1] * vn[2] - vf[2] * vn[1]);
+                        }
+                    }
+                    const float wxy = wx.w[ii] * wy.w[jj], gx0 = wx.dw[ii] * wy.w[jj], gy0 = wx.w[ii] * wy.dw[jj];
+                    K01 += wxy * k01;
+                    K02 += wxy * k02;
+                    K12 += wxy * k12;
+                    const float wxX = wxy * dX[ii], wxY = wxy * dY[jj];
+#pragma unroll
+                    for(int r = 0; r < 3; r++) {
+                        Vp[r] += wxy * Sw[r];
+                        G[r] += gx0 * Sw[r];
+                        G[r + 3] += gy0 * Sw[r];
+                        G[r + 6] += wxy * Sd[r];
+                        Vf[r] += wxy * Tw[r];
+                        Bv[r] += wxX * Tw[r];
+                        Bv[r + 3] += wxY * Tw[r];
+                        Bv[r + 6] += wxy * Td[r];
                     }
                 }
             // F <- (I + dt grad v) F
@@ -452,16 +504,15 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
             float xn[3];
 #pragma unroll
             for(int k = 0; k < 3; k++) xn[k] = X[k] + dt * Vp[k];
-            // APIC B in the reference's xi_new form, rewritten with the partition of
-            // unity: B = sum w vf (Z - X) + dt/2 [sum w (vf vn^T - vn vf^T) - (Vf Vp^T - Vp Vf^T)]
             const float h = 0.5f * dt;
             const float A01 = h * (K01 - (Vf[0] * Vp[1] - Vp[0] * Vf[1]));
             const float A02 = h * (K02 - (Vf[0] * Vp[2] - Vp[0] * Vf[2]));
             const float A12 = h * (K12 - (Vf[1] * Vp[2] - Vp[1] * Vf[2]));
-            float Bn[9] = {Bv[0], Bv[1] - A01, Bv[2] - A02,
-                           Bv[3] + A01, Bv[4], Bv[5] - A12,
-                           Bv[6] + A02, Bv[7] + A12, Bv[8]};
+            const float Bn[9] = {Bv[0], Bv[1] - A01, Bv[2] - A02,
+                                 Bv[3] + A01, Bv[4], Bv[5] - A12,
+                                 Bv[6] + A02, Bv[7] + A12, Bv[8]};
             bool ok = true;
+#pragma unroll
             for(int k = 0; k < 3; k++) {
                 float eps = FLT_EPSILON * 4.f * (a.dmax[k] - a.dmin[k]);
                 if(!(xn[k] >= a.dmin[k] + eps && xn[k] <= a.dmax[k] - eps)) ok = false;
@@ -471,16 +522,15 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
             for(int k = 0; k < 9; k++) finite = finite && isfinite(Fn[k]);
             finite = finite && isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]);
             if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); ok = false; }
-            uint32_t key = ok ? cell_key(a, xn) : SENTINEL;
+            const uint32_t key = ok ? cell_key(a, xn) : SENTINEL;
 #pragma unroll
             for(int k = 0; k < 3; k++) { a.dst[(C_X + k) * a.npad + j] = xn[k]; a.dst[(C_V + k) * a.npad + j] = Vf[k]; }
 #pragma unroll
             for(int k = 0; k < 9; k++) { a.dst[(C_F + k) * a.npad + j] = Fn[k]; a.dst[(C_B + k) * a.npad + j] = Bn[k]; }
-            a.dst_attr[j] = a.src_attr[i];
-            a.dst_pid[j] = a.src_pid[i];
+            a.dst_attr[j] = at;
+            a.dst_pid[j] = pid;
             a.keys_next[j] = key;
         }
-        __syncthreads();
     }
 }
 
@@ -578,7 +628,7 @@ int grid_stride_blocks(mpm_handle* h, int64_t n, int t)
     return (int)(b < 1 ? 1 : b);
 }
 
-constexpr int P2G_THREADS = 128;
+constexpr int P2G_THREADS = 64;   // one thread per cell of a 4^3 block
 constexpr int G2P_THREADS = 128;
 
 }  // namespace
@@ -615,7 +665,7 @@ int fast_alloc(mpm_handle* h, int64_t n)
         MPM_CUDA(h, cudaMalloc(&f.counters, CNT_COUNT * sizeof(uint32_t)));
         MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
         int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_p2g<P2G_THREADS>, P2G_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_p2g, P2G_THREADS, 0);
         f.p2g_ctas = h->sm_count * (occ > 0 ? occ : 1);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_g2p<G2P_THREADS>, G2P_THREADS, 0);
         f.g2p_ctas = h->sm_count * (occ > 0 ? occ : 1);
@@ -774,7 +824,7 @@ int fast_p2g(mpm_handle* h, double dt, double)
     MPM_LAUNCHED(h, "k_tail");
     timer_end(h, slot);
     slot = timer_begin(h, "fast_p2g");
-    k_p2g<P2G_THREADS><<<f.p2g_ctas, P2G_THREADS, 0, h->stream>>>(a);
+    k_p2g<<<f.p2g_ctas, P2G_THREADS, 0, h->stream>>>(a);
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_p2g");
     return MPM_OK;

@@ -140,14 +140,18 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
     uint64_t* status = reinterpret_cast<uint64_t*>(scratch + kStatusOff) + (int64_t)pass * tiles * kRadix;
 
     const int64_t base = (int64_t)tile * kTile;
-    uint32_t key[kItems], val[kItems], rank[kItems];
+    uint32_t key[kItems], rank[kItems];
     const uint32_t lt = (1u << lane) - 1u;
+    const int64_t wbase = base + warp * (32 * kItems) + lane;
+    // all loads first, so the 16 keys of a thread are in flight together
 #pragma unroll
     for(int k = 0; k < kItems; k++) {
-        int64_t idx = base + warp * (32 * kItems) + k * 32 + lane;
-        bool ok = idx < n;
-        key[k] = ok ? keys_in[idx] : 0u;
-        val[k] = ok ? (vals_in ? vals_in[idx] : (uint32_t)idx) : 0u;
+        int64_t idx = wbase + k * 32;
+        key[k] = idx < n ? keys_in[idx] : 0u;
+    }
+#pragma unroll
+    for(int k = 0; k < kItems; k++) {
+        bool ok = wbase + k * 32 < n;
         uint32_t dg = ok ? (key[k] >> shift) & mask : 256u;
         uint32_t peers = __match_any_sync(0xffffffffu, dg);
         uint32_t r = 0;
@@ -199,12 +203,11 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
     __syncthreads();
 #pragma unroll
     for(int k = 0; k < kItems; k++) {
-        int64_t idx = base + warp * (32 * kItems) + k * 32 + lane;
-        if(idx < n) {
+        if(wbase + k * 32 < n) {
             uint32_t dg = (key[k] >> shift) & mask;
             uint32_t pos = S.dstart[dg] + S.wcnt[warp][dg] + rank[k];
             S.skey[pos] = key[k];
-            S.sval[pos] = val[k];
+            S.sval[pos] = (uint32_t)(warp * (32 * kItems) + k * 32 + lane);   // tile-local index
         }
     }
     __syncthreads();
@@ -213,8 +216,9 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
         uint32_t k0 = S.skey[i];
         uint32_t dg = (k0 >> shift) & mask;
         int64_t pos = (int64_t)S.gbase[dg] + (i - S.dstart[dg]);
+        int64_t src = base + S.sval[i];
         keys_out[pos] = k0;
-        vals_out[pos] = S.sval[i];
+        vals_out[pos] = vals_in ? vals_in[src] : (uint32_t)src;
     }
 }
 
