@@ -216,6 +216,25 @@ int mpm_diff_backward(mpm_handle* h, const mpm_particles_view* grad_final, mpm_p
  * perm[i] = index of the i-th smallest key (ties keep input order). */
 int mpm_radix_sort_u32(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm);
 
+/* The same sort for callers that cannot allocate device memory at the time
+ * they sort: work recorded into a CUDA graph by stream capture, hosts that
+ * give the library a fixed memory budget up front, and loops that cannot
+ * absorb cudaMalloc/cudaFree and the device synchronisation they bring.
+ * There is no counterpart in the reference (it sorts on the CPU).
+ * keys, sorted_keys and perm are DEVICE arrays of n entries on the current
+ * device (keys must not alias an output); the work runs on `stream`
+ * (cudaStream_t, NULL = legacy default stream) and the call returns when it
+ * is done.  It allocates nothing: its temporaries live in one fixed array
+ * compiled into the library (about 2.6 MB, held on every device that loads
+ * the library until exit), so n is limited to MPM_NOALLOC_MAX_KEYS; larger n
+ * returns MPM_ERR_ARG (use mpm_radix_sort_u32).  The first call on a device
+ * looks up that array's address and zeroes it (a synchronous cudaMemset):
+ * make that first call before any stream capture.  All calls on a device
+ * share the array, so calls that overlap on the GPU race; serialise them. */
+#define MPM_NOALLOC_MAX_KEYS 262144
+int mpm_radix_sort_u32_noalloc(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm,
+                               void* stream);
+
 /* Fast path only: cell keys of the current particle slots, and the sorted keys
  * and slot permutation of the last sort (host arrays of n entries, NULL-able).
  * Key = (particle block << 6) | cell in block; 0xffffffff = invalid particle. */

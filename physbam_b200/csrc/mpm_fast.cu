@@ -25,6 +25,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "mpm_internal.h"
 #include "mpm_sort.cuh"
@@ -945,4 +946,81 @@ int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_
     cudaFree(k); cudaFree(ko); cudaFree(vo); cudaFree(ka); cudaFree(va); cudaFree(scratch); cudaFree(flags);
     cudaStreamDestroy(st);
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Radix sort without any allocation.
+//
+// Some callers cannot allocate device memory when they need to sort: code
+// recorded into a CUDA graph by stream capture (an allocation would either be
+// illegal there or become part of the graph), hosts that give this library a
+// fixed memory budget up front and forbid growth afterwards, and loops with
+// latency limits that cannot absorb cudaMalloc / cudaFree and the device-wide
+// synchronisation cudaFree implies.  mpm_radix_sort_u32_noalloc serves them:
+// the caller passes device arrays for the keys and both outputs, and every
+// temporary the sort needs lives in one fixed array compiled into this file.
+//
+// The array is a file-scope __device__ variable, so every GPU that loads the
+// library holds it (about 2.6 MB) until the process exits, whether or not the
+// entry point is used.  It is shared by all calls on a device and keeps the
+// previous call's contents; each call clears what must start at zero.  Calls
+// that overlap on the GPU (two streams, or two host threads) race on it.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int64_t kNoAllocMaxKeys = MPM_NOALLOC_MAX_KEYS;
+constexpr int64_t kNoAllocSortWords =
+    mpm_sort::kStatusOff + 2LL * mpm_sort::kMaxPasses * ((kNoAllocMaxKeys + mpm_sort::kTile - 1) / mpm_sort::kTile) * mpm_sort::kRadix;
+constexpr int64_t kNoAllocKeysAlt = kNoAllocSortWords;                 // ping-pong keys
+constexpr int64_t kNoAllocValsAlt = kNoAllocKeysAlt + kNoAllocMaxKeys;  // ping-pong payloads
+constexpr int64_t kNoAllocFlag = kNoAllocValsAlt + kNoAllocMaxKeys;     // timeout flag word
+constexpr int64_t kNoAllocWords = kNoAllocFlag + 64;
+
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+// The host-side name g_noalloc_scratch is only a stand-in for the device
+// variable; kernels get its device address, looked up once per device.
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint32_t* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Once per device, with that device current: find the array's device address
+// and zero it (the look-back status words must start with epoch 0).
+int noalloc_setup(int dev, uint32_t** out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if(!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if(cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MPM_ERR_CUDA;
+        if(cudaMemset(p, 0, sizeof(uint32_t) * kNoAllocWords) != cudaSuccess) return MPM_ERR_CUDA;
+        if(mpm_sort::prepare() != cudaSuccess) return MPM_ERR_CUDA;
+        g_noalloc_ptr[dev] = (uint32_t*)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return MPM_OK;
+}
+}  // namespace
+
+extern "C" int mpm_radix_sort_u32_noalloc(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys,
+    uint32_t* perm, void* stream)
+{
+    if(n < 0 || bits < 1 || bits > 32) return MPM_ERR_ARG;
+    if(n > kNoAllocMaxKeys) return MPM_ERR_ARG;     // beyond the fixed scratch: use mpm_radix_sort_u32
+    if(n == 0) return MPM_OK;
+    if(!keys || !sorted_keys || !perm || keys == sorted_keys || keys == perm) return MPM_ERR_ARG;
+    int dev = 0;
+    if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return MPM_ERR_CUDA;
+    uint32_t* base = nullptr;
+    int rc = noalloc_setup(dev, &base);
+    if(rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned* flag = (unsigned*)(base + kNoAllocFlag);
+    if(cudaMemsetAsync(flag, 0, sizeof(unsigned), st) != cudaSuccess) return MPM_ERR_CUDA;
+    int sms = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if(mpm_sort::radix_sort(keys, sorted_keys, perm, base + kNoAllocKeysAlt, base + kNoAllocValsAlt, n, bits, base,
+                            flag, MPM_FLAG_TIMEOUT, sms * 4, st) != cudaSuccess) return MPM_ERR_CUDA;
+    unsigned f = 0;
+    if(cudaMemcpyAsync(&f, flag, sizeof(f), cudaMemcpyDeviceToHost, st) != cudaSuccess) return MPM_ERR_CUDA;
+    if(cudaStreamSynchronize(st) != cudaSuccess) return MPM_ERR_CUDA;
+    return (f & MPM_FLAG_TIMEOUT) ? MPM_ERR_TIMEOUT : MPM_OK;
 }
