@@ -166,15 +166,15 @@ def cpu_baseline_sample(scene, seconds_budget=20.0):
 
 
 def kernels_per_substep(scene):
-    """Our kernels launched per fast-path substep: 5 per radix digit pass
-    (histogram, 3-kernel scan, scatter) + ranges, tail, p2g, grid, g2p."""
+    """Our kernels launched per fast-path substep: the digit histograms, one
+    single-pass kernel per radix digit, ranges, tail, p2g, grid, g2p."""
     blocks = 1
     for c in scene.counts:
         blocks *= (c + 4 + 3) // 4
     bits = 6
     while (1 << bits) <= blocks * 64:
         bits += 1
-    return 5 * ((bits + 7) // 8) + 5
+    return (bits + 7) // 8 + 6
 
 
 def read_traffic(kernel, workload=WORKLOAD):
@@ -309,9 +309,13 @@ def our_arm(args):
     roof = roofline_of(ktimes, n, peak, peak_kind, WORKLOAD)
     total_k = sum(v[0] for v in ktimes.values())
 
-    large = None
+    large = batch = adjoint = None
     if world == 1 and not args.no_large:
         large = measure_large(args, D, S, stream, flush, peak, peak_kind)
+    if world == 1 and not args.no_batch:
+        batch = measure_batch(args, D, S, stream, flush, peak)
+    if world == 1 and not args.no_adjoint:
+        adjoint = measure_adjoint(D, S)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -333,6 +337,8 @@ def our_arm(args):
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()},
             "kernel_share": {k: v[0] / total_k for k, v in ktimes.items()},
             "large_config": large,
+            "batch_config": batch,
+            "adjoint": adjoint,
             "cpu_baseline": cpu,
             "clocks": clocks}
     if dist:
@@ -341,6 +347,60 @@ def our_arm(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def measure_batch(args, D, S, stream, flush, peak):
+    """256 independent scenes (grid side from {32,48,64,96}, boxes of
+    seeded size, 4-8 ppc, both models) in one handle; launch shapes from the autotuner."""
+    import torch
+    scenes = S.batch_scenes(seed=1234, count=256)
+    n = sum(s.n for s in scenes)
+    drv = D.MPM_BATCH(scenes)
+    drv.set_stream(stream.cuda_stream)
+    drv.set_scene_particles(dtype=np.float32)
+    report = drv.autotune(substeps=3)
+    steps = max(5, min(args.steps, 20))
+    ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
+    drv.close()
+    sub = ms / steps
+    return {"workload": "batch256-3d-grids{32,48,64,96}-fp32", "scenes": len(scenes), "particles": n,
+            "steps": steps, "ms_per_step": sub, "value": n * steps / (ms / 1e3), "unit": METRIC,
+            "substep_roofline": {"achieved": ALG_BYTES["substep"] * n / (sub / 1e3) / 1e9, "peak": peak,
+                                 "unit": "GB/s", "frac": ALG_BYTES["substep"] * n / (sub / 1e3) / 1e9 / peak},
+            "autotune": report,
+            "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
+
+
+def measure_adjoint(D, S):
+    """64^3 cube, 64 substeps, checkpoint every 8; FP32 forward and
+    backward through the C ABI (device arrays), timed with CUDA events."""
+    import torch
+    scene = S.cube_3d()
+    n = scene.n
+    drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_PLAIN)
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device="cuda")
+    X, V = t(scene.X), t(scene.V)
+    Fc = t(np.swapaxes(scene.F, 1, 2).reshape(n, 9))
+    Bc = t(np.swapaxes(scene.B, 1, 2).reshape(n, 9))
+    m, vol, mu, lam = t(scene.mass), t(scene.volume), t(scene.mu), t(scene.lam)
+    g = [torch.ones_like(X) * 1e-3, torch.zeros_like(V), torch.zeros_like(Fc), torch.zeros_like(Bc)]
+    fwd, bwd = [], []
+    for it in range(4):
+        drv.set_particles_device(X, V, Fc, Bc, m, vol, mu, lam)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        drv.diff_forward(64, 8)
+        t1 = time.perf_counter()
+        drv.diff_backward(*g)
+        t2 = time.perf_counter()
+        if it:
+            fwd.append(t1 - t0)
+            bwd.append(t2 - t1)
+    drv.close()
+    f, b = min(fwd), min(bwd)
+    return {"workload": "cube3d-64^3-corotated-8ppc, 64 substeps, checkpoint every 8, fp32", "particles": n,
+            "fwd_ms": f * 1e3, "bwd_ms": b * 1e3, "bwd_over_fwd": b / f,
+            "timing": "host wall clock around synchronous C-ABI calls, best of 3"}
 
 
 def profile_case(args, D, S):
@@ -394,6 +454,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-large", action="store_true", help="skip the 256^3 dam-break measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 256-scene batched measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the forward/backward timing")
     ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d"], help="profiling run of one scene only")
     ap.add_argument("--grid", type=int, default=0, help="grid cells per side for --scene")
     args = ap.parse_args()

@@ -186,6 +186,35 @@ int mpm_count_valid(mpm_handle* h, int64_t* count);
 int mpm_set_timing(mpm_handle* h, int enable);
 int mpm_get_timing(mpm_handle* h, char* names, int names_len, double* ms, int64_t* launches, int max_entries, int* count);
 
+/* ---- many independent scenes in one handle --------------------------------- */
+
+/* One scene of a batch.  Its particles are particle_count consecutive entries
+ * of the arrays given to mpm_set_particles, scenes in order; its collision
+ * objects are objects[first_object, first_object + object_count) of
+ * mpm_batch_create. */
+typedef struct {
+    mpm_grid_desc grid;      /* dim must be 3, ghost 3 */
+    int model;               /* mpm_model */
+    double gravity[3];
+    int64_t particle_count;
+    int first_object;
+    int object_count;        /* <= MPM_MAX_OBJECTS */
+} mpm_scene_desc;
+
+/* A handle that advances `count` independent scenes (different grid sizes,
+ * domains, models, objects) together: every phase of the substep is one
+ * persistent launch over the blocks of all scenes, and mpm_advance replays it
+ * from a CUDA graph.  FP32 fast path.  The reference runs one MPM_EXAMPLE per
+ * process; there is no counterpart call. */
+int mpm_batch_create(const mpm_scene_desc* scenes, int count, const mpm_collision_object* objects, int object_count,
+                     mpm_handle** out);
+
+/* Time the fast path's launch shapes (P2G work split, G2P block size, number of
+ * persistent CTAs) for `substeps` substeps each on the handle's own particles
+ * and keep the fastest; the particle state is left unchanged.  `report` (may be
+ * NULL) receives the timings. */
+int mpm_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len);
+
 /* ---- differentiation ------------------------------------------------------ */
 
 /* Records a differentiable rollout: nsteps explicit substeps from the current

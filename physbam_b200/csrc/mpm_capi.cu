@@ -203,6 +203,7 @@ int mpm_set_collision_objects(mpm_handle* h, const mpm_collision_object* objs, i
             for(int k = 0; k < h->sp.dim; k++)
                 if(!(o.b[k] > o.a[k])) return set_error(h, MPM_ERR_ARG, "box with an empty side (RANGE::Signed_Distance)");
     }
+    if(fast(h) && h->fast.batch) return set_error(h, MPM_ERR_ARG, "a batch takes its objects at mpm_batch_create");
     release_graph(h);
     h->sp.nobj = count;
     for(int i = 0; i < count; i++) {
@@ -211,6 +212,18 @@ int mpm_set_collision_objects(mpm_handle* h, const mpm_collision_object* objs, i
         d.type = objs[i].type;
         d.friction = objs[i].friction;
         for(int k = 0; k < 3; k++) { d.a[k] = objs[i].a[k]; d.b[k] = objs[i].b[k]; }
+    }
+    if(fast(h) && h->fast.scenes) {   // particles already set: refresh the device tables of scene 0
+        FastState& f = h->fast;
+        f.objs_h.assign(count > 0 ? count : 1, mpm::DevObject{});
+        for(int i = 0; i < count; i++) f.objs_h[i] = h->sp.objs[i];
+        f.scenes_h[0].obj_begin = 0;
+        f.scenes_h[0].nobj = count;
+        cudaFree(f.objs);
+        f.objs = nullptr;
+        MPM_CUDA(h, cudaMalloc(&f.objs, f.objs_h.size() * sizeof(mpm::DevObject)));
+        MPM_CUDA(h, cudaMemcpy(f.objs, f.objs_h.data(), f.objs_h.size() * sizeof(mpm::DevObject), cudaMemcpyHostToDevice));
+        MPM_CUDA(h, cudaMemcpy(f.scenes, f.scenes_h.data(), sizeof(SceneDev), cudaMemcpyHostToDevice));
     }
     return MPM_OK;
 }
@@ -329,6 +342,38 @@ int mpm_count_valid(mpm_handle* h, int64_t* count)
     if(!h || !count) return MPM_ERR_ARG;
     if(!h->have_particles) { *count = 0; return MPM_OK; }
     return fast(h) ? fast_count_valid(h, count) : plain_count_valid(h, count);
+}
+
+int mpm_batch_create(const mpm_scene_desc* scenes, int count, const mpm_collision_object* objects, int object_count,
+    mpm_handle** out)
+{
+    if(!scenes || !out || count < 1 || object_count < 0 || (object_count && !objects)) return MPM_ERR_ARG;
+    *out = nullptr;
+    mpm_model_desc m;
+    memset(&m, 0, sizeof(m));
+    m.model = scenes[0].model;
+    m.precision = MPM_FP32;
+    m.path = MPM_PATH_FAST;
+    mpm_handle* h = nullptr;
+    int rc = mpm_create(&scenes[0].grid, &m, &h);
+    if(rc) return rc;
+    h->fast.batch = true;
+    if((rc = fast_setup_scenes(h, scenes, count, objects, object_count))) {
+        mpm_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return MPM_OK;
+}
+
+int mpm_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len)
+{
+    int rc = check_dt(h, dt);
+    if(rc) return rc;
+    if(!fast(h)) return set_error(h, MPM_ERR_ARG, "the autotuner tunes the fast path");
+    release_graph(h);
+    if((rc = fast_autotune(h, dt, substeps, report, report_len))) return rc;
+    return read_flags(h);
 }
 
 int mpm_diff_forward(mpm_handle* h, double dt, int nsteps, int checkpoint_every)

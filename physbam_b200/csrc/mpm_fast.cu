@@ -1,26 +1,29 @@
-// Fast path: the explicit MPM substep in FP32 with cell-sorted particles.
+// Fast path: the explicit MPM substep in FP32 with cell-sorted particles, for
+// one scene or a batch of independent scenes (a single scene is a batch of one).
 //
-// Per substep (MPM_DRIVER::Advance_One_Time_Step, MPM_DRIVER.cpp:141-157):
-//   sort     particle keys (block of 4^3 cells, cell in block) are radix-sorted;
-//            the previous G2P wrote them, so the particles are already nearly in
-//            order and the permutation is local.
+// Per substep (MPM_DRIVER::Advance_One_Time_Step, MPM_DRIVER.cpp:141-157), each
+// phase is ONE persistent launch over the blocks of all scenes:
+//   sort     particle keys (global block of 4^3 cells, cell in block) are
+//            radix-sorted; the previous G2P wrote them, so particles are already
+//            nearly in order and the permutation is local.
 //   ranges   sorted keys -> [start, end) per particle block, list of active
 //            blocks, number of valid particles (invalid ones carry the
 //            sentinel key and sort to the tail).
-//   p2g      one CTA per active block: B-spline weights, the stress
-//            P(F) F^T (fused; MPM_FINITE_ELEMENTS::Precompute, .cpp:47-67) and
-//            APIC momentum plus dt * force accumulate into a 6^3-node shared
-//            tile, flushed with one float4 atomic per touched node
-//            (Particle_To_Grid l.245-306 and MPM_FINITE_ELEMENTS::Add_Forces,
-//            MPM_GRAVITY::Add_Forces folded in).  The CTA marks the node blocks
-//            its tile covers.
-//   grid     one CTA per marked node block: v = (mv + dt f)/m + dt g, the
-//            collision projection and friction (Apply_Forces l.959-1060),
-//            zeroes the accumulator for the next substep.
+//   p2g      one CTA per active block: B-spline weights, the stress P(F) F^T
+//            (fused; MPM_FINITE_ELEMENTS::Precompute, .cpp:47-67), APIC momentum
+//            plus dt * force into a 6^3-node shared tile, flushed with one
+//            float4 atomic per touched node (Particle_To_Grid l.245-306 with
+//            MPM_FINITE_ELEMENTS::Add_Forces and MPM_GRAVITY::Add_Forces folded
+//            in).  The CTA marks the node blocks its tile covers.
+//   grid     one CTA per marked node block: v = (mv + dt f)/m + dt g, collision
+//            projection and friction (Apply_Forces l.959-1060); clears the
+//            accumulator for the next substep.
 //   g2p      one CTA per active block: stage the tile of (v, v_fric), gather,
-//            update F, X, V and the APIC B (Grid_To_Particle l.450-515),
-//            write the particle to its sorted slot in the other buffer and
-//            its next key.
+//            update F, X, V and the APIC B (Grid_To_Particle l.450-515), write
+//            the particle to its sorted slot in the other buffer with its next key.
+// Scenes differ in grid size, domain, model and collision objects; blocks and
+// node blocks of all scenes share one numbering, and a CTA looks up the scene
+// of the block it works on.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -42,7 +45,6 @@ constexpr int NCOMP = 24;                  // x3 v3 F9 B9 floats per particle
 constexpr int C_X = 0, C_V = 3, C_F = 6, C_B = 15;
 
 struct FastArgs {
-    SceneParams sp;
     int64_t n, npad;
     const float* src;
     const float4* src_attr;
@@ -56,41 +58,51 @@ struct FastArgs {
     uint32_t *bstart, *bend, *active, *nb_flag, *nb_list, *counters;
     float4* acc;
     float4* vel;
-    int GA[3], NB[3], NN[3];
+    const SceneDev* scenes;
+    const uint16_t* block_scene;
+    const uint16_t* nb_scene;
+    const int64_t* pbase;
+    const DevObject* objs;
+    int nscenes;
     float dt;
-    float dmin[3], dmax[3], dx[3], inv[3];
-    float gravity[3];
     unsigned* flags;
 };
 
-__device__ __forceinline__ int64_t node_index(const FastArgs& a, int qx, int qy, int qz)
+__device__ __forceinline__ int64_t node_index(const SceneDev& sc, int qx, int qy, int qz)
 {
-    return ((int64_t)qx * a.GA[1] + qy) * a.GA[2] + qz;
+    return sc.node_base + ((int64_t)qx * sc.GA[1] + qy) * sc.GA[2] + qz;
 }
 
-// Cell key of a position: the block and in-block cell of the first stencil
-// node (base + 3 in ghosted node coordinates).  SENTINEL when the stencil
-// would leave the ghosted grid.
-__device__ __forceinline__ uint32_t cell_key(const FastArgs& a, const float* X)
+// Cell key of a position in scene sc: its global block and in-block cell of the
+// first stencil node (base + 3 in ghosted node coordinates).  SENTINEL when the
+// stencil would leave the ghosted grid.
+__device__ __forceinline__ uint32_t cell_key(const SceneDev& sc, const float* X)
 {
     int cc[3];
 #pragma unroll
     for(int k = 0; k < 3; k++) {
-        float y = X[k] - a.dx[k];
-        int base = (int)floorf((y - a.dmin[k]) * a.inv[k]);
+        float y = X[k] - sc.dx[k];
+        int base = (int)floorf((y - sc.dmin[k]) * sc.inv[k]);
         cc[k] = base + MPM_GHOST;
-        if(cc[k] < 0 || cc[k] > a.sp.counts[k] + MPM_GHOST) return SENTINEL;
+        if(cc[k] < 0 || cc[k] > sc.counts[k] + MPM_GHOST) return SENTINEL;
     }
-    uint32_t b = ((uint32_t)(cc[0] >> 2) * a.NB[1] + (uint32_t)(cc[1] >> 2)) * a.NB[2] + (uint32_t)(cc[2] >> 2);
-    return (b << 6) | ((cc[0] & 3) << 4) | ((cc[1] & 3) << 2) | (cc[2] & 3);
+    uint32_t b = ((uint32_t)(cc[0] >> 2) * sc.NB[1] + (uint32_t)(cc[1] >> 2)) * sc.NB[2] + (uint32_t)(cc[2] >> 2);
+    return ((sc.block_base + b) << 6) | ((cc[0] & 3) << 4) | ((cc[1] & 3) << 2) | (cc[2] & 3);
 }
 
-__device__ __forceinline__ void block_coords(const FastArgs& a, uint32_t b, int& bx, int& by, int& bz)
+__device__ __forceinline__ void block_coords(const SceneDev& sc, uint32_t lb, int& bx, int& by, int& bz)
 {
-    bz = b % a.NB[2];
-    uint32_t r = b / a.NB[2];
-    by = r % a.NB[1];
-    bx = r / a.NB[1];
+    bz = lb % sc.NB[2];
+    uint32_t r = lb / sc.NB[2];
+    by = r % sc.NB[1];
+    bx = r / sc.NB[1];
+}
+
+// Copy scene s into shared memory (the caller synchronises before use).
+__device__ __forceinline__ void stage_scene(const FastArgs& a, int s, SceneDev* out)
+{
+    constexpr int words = (int)(sizeof(SceneDev) / 4);
+    if(threadIdx.x < words) ((uint32_t*)out)[threadIdx.x] = ((const uint32_t*)(a.scenes + s))[threadIdx.x];
 }
 
 // ---------------------------------------------------------------------------
@@ -148,7 +160,6 @@ __device__ __forceinline__ bool stress_fast(int model, const float* F, float mu,
     float den = I1 * I2 - I3;
     if(!(den > 0.f)) return false;
     float ca = I1 * I1 - I2, cb = I1 * I3, id = 1.f / den;
-    // b^2 (symmetric)
     float s00 = b00 * b00 + b01 * b01 + b02 * b02;
     float s11 = b01 * b01 + b11 * b11 + b12 * b12;
     float s22 = b02 * b02 + b12 * b12 + b22 * b22;
@@ -182,8 +193,14 @@ __device__ __noinline__ bool stress_fp64(int model, const float* Ff, float mu, f
 __global__ void k_init_keys(FastArgs a, const uint8_t* valid_by_slot)
 {
     for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        // scene of particle i: pbase[s] <= i < pbase[s + 1] (particles arrive in scene order)
+        int lo = 0, hi = a.nscenes - 1;
+        while(lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if(a.pbase[mid] <= i) lo = mid; else hi = mid - 1;
+        }
         float X[3] = {a.src[(C_X + 0) * a.npad + i], a.src[(C_X + 1) * a.npad + i], a.src[(C_X + 2) * a.npad + i]};
-        uint32_t k = valid_by_slot[i] ? cell_key(a, X) : SENTINEL;
+        uint32_t k = valid_by_slot[i] ? cell_key(a.scenes[lo], X) : SENTINEL;
         if(valid_by_slot[i] && k == SENTINEL) atomicOr(a.flags, MPM_FLAG_DOMAIN);
         a.keys_next[i] = k;
     }
@@ -231,107 +248,165 @@ __device__ __forceinline__ int next_work(uint32_t* ctr, int* s_work)
     return *s_work;
 }
 
-// P2G, one thread per cell of the block.  A thread walks the particles of its
-// cell (they share the 27 nodes) and accumulates mass and momentum plus dt*force
-// for those nodes in registers, then adds them to the block's shared tile: one
-// shared atomic per node value per cell instead of per particle, and the 64
-// lanes of a block hit 64 different node addresses for any given offset.
-//   p_i += w m (V + B D (Z_i - X)) - dt vol S g,   m_i += w m
-// is evaluated separably: per (x, y) offset pair the terms that do not depend
-// on z are formed once, leaving three FMAs per node component.
-__global__ void __launch_bounds__(64) k_p2g(FastArgs a)
+// Per-particle P2G coefficients.  For node (ii, jj, kk) the contribution is
+//   mass += mxy[ii][jj] wz[kk]
+//   p_r  += wz[kk] P_r(ii,jj) + w uz[kk][r] - Cc_r(ii,jj) dwz[kk],   w = wxy wz[kk]
+// where p_i = w m (V + B D (Z_i - X)) - dt vol S g collects momentum and dt * force.
+struct P2GParticle {
+    Axis<float> wx, wy, wz;
+    float m;
+    float ux[3][3], uy[3][3], uz[3][3];
+    float S[9];
+};
+
+__device__ __forceinline__ void p2g_particle(const FastArgs& a, const SceneDev& sc, uint32_t i, P2GParticle& P)
 {
-    __shared__ float tm[TN], tx[TN], ty[TN], tz[TN];
-    __shared__ uint32_t ccount[64], cstart[64];
-    __shared__ int s_work;
+    float X[3], V[3], F[9], Bm[9];
+#pragma unroll
+    for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
+#pragma unroll
+    for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; Bm[r] = a.src[(C_B + r) * a.npad + i]; }
+    const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
+    if(!stress_fast(sc.model, F, at.z, at.w, P.S)) {
+        // only this rare branch needs an addressable array for the out-of-line call
+        float T[9];
+        atomicAdd(&a.counters[CNT_FALLBACK], 1u);
+        if(!stress_fp64(sc.model, F, at.z, at.w, T)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
+#pragma unroll
+        for(int r = 0; r < 9; r++) P.S[r] = T[r];
+    }
+    const float sv = a.dt * at.y, m = at.x;
+    P.m = m;
+#pragma unroll
+    for(int r = 0; r < 9; r++) P.S[r] *= sv;
+    P.wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
+    P.wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
+    P.wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
+    const float Dx = 4.f * sc.inv[0] * sc.inv[0] * m, Dy = 4.f * sc.inv[1] * sc.inv[1] * m, Dz = 4.f * sc.inv[2] * sc.inv[2] * m;
+#pragma unroll
+    for(int o = 0; o < 3; o++) {
+        float dxo = (sc.dmin[0] + ((float)(P.wx.base + o) + 0.5f) * sc.dx[0] - X[0]) * Dx;
+        float dyo = (sc.dmin[1] + ((float)(P.wy.base + o) + 0.5f) * sc.dx[1] - X[1]) * Dy;
+        float dzo = (sc.dmin[2] + ((float)(P.wz.base + o) + 0.5f) * sc.dx[2] - X[2]) * Dz;
+#pragma unroll
+        for(int r = 0; r < 3; r++) {
+            P.ux[o][r] = Bm[r] * dxo + m * V[r];   // the x factor also carries m V
+            P.uy[o][r] = Bm[r + 3] * dyo;
+            P.uz[o][r] = Bm[r + 6] * dzo;
+        }
+    }
+}
+
+// Visit the 27 node contributions of one particle: f(q, mass, px, py, pz).
+template<class FN> __device__ __forceinline__ void p2g_nodes(const P2GParticle& P, FN&& f)
+{
+#pragma unroll
+    for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+        for(int jj = 0; jj < 3; jj++) {
+            const float wxy = P.wx.w[ii] * P.wy.w[jj];
+            const float gx0 = P.wx.dw[ii] * P.wy.w[jj], gy0 = P.wx.w[ii] * P.wy.dw[jj];
+            const float mxy = P.m * wxy;
+            float Pr[3], Cc[3];
+#pragma unroll
+            for(int r = 0; r < 3; r++) {
+                Pr[r] = wxy * (P.ux[ii][r] + P.uy[jj][r]) - (P.S[r] * gx0 + P.S[r + 3] * gy0);
+                Cc[r] = P.S[r + 6] * wxy;
+            }
+#pragma unroll
+            for(int kk = 0; kk < 3; kk++) {
+                const float wzk = P.wz.w[kk], dwz = P.wz.dw[kk], wq = wxy * wzk;
+                f((ii * 3 + jj) * 3 + kk, mxy * wzk,
+                  wzk * Pr[0] + wq * P.uz[kk][0] - Cc[0] * dwz,
+                  wzk * Pr[1] + wq * P.uz[kk][1] - Cc[1] * dwz,
+                  wzk * Pr[2] + wq * P.uz[kk][2] - Cc[2] * dwz);
+            }
+        }
+}
+
+struct P2GTile {
+    float m[TN], x[TN], y[TN], z[TN];
+    uint32_t ccount[64], cstart[64];
+    uint32_t maxc;
+    SceneDev sc;
+    int work;
+};
+
+// Block set-up shared by both P2G variants: stage the scene, zero the tile,
+// count the block's particles per cell (they arrive sorted by cell) and scan.
+__device__ __forceinline__ void p2g_begin(const FastArgs& a, P2GTile& T, uint32_t b)
+{
+    stage_scene(a, a.block_scene[b], &T.sc);
+    for(int t = threadIdx.x; t < TN; t += blockDim.x) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+    if(threadIdx.x < 64) T.ccount[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t s = a.bstart[b], e = a.bend[b];
+    for(uint32_t j = s + threadIdx.x; j < e; j += blockDim.x) atomicAdd(&T.ccount[a.sorted_keys[j] & 63u], 1u);
+    __syncthreads();
+    if(threadIdx.x < 32) {
+        const int c = threadIdx.x;
+        uint32_t c0 = T.ccount[2 * c], c1 = T.ccount[2 * c + 1];
+        uint32_t sum = c0 + c1, x = sum, mx = c0 > c1 ? c0 : c1;
+#pragma unroll
+        for(int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if(c >= o) x += y;
+            mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        T.cstart[2 * c] = x - sum;
+        T.cstart[2 * c + 1] = x - sum + c0;
+        if(c == 0) T.maxc = mx;
+    }
+    __syncthreads();
+}
+
+// Flush the tile with one float4 atomic per touched node and mark the 8 node
+// blocks the tile covers for the grid update.
+__device__ __forceinline__ void p2g_end(const FastArgs& a, P2GTile& T, uint32_t lb)
+{
+    __syncthreads();
+    const SceneDev& sc = T.sc;
+    int bx, by, bz;
+    block_coords(sc, lb, bx, by, bz);
+    for(int t = threadIdx.x; t < TN; t += blockDim.x) {
+        float mm = T.m[t];
+        if(mm != 0.f) {
+            int qx = 4 * bx + t / (TE * TE), qy = 4 * by + (t / TE) % TE, qz = 4 * bz + t % TE;
+            atomicAdd(&a.acc[node_index(sc, qx, qy, qz)], make_float4(T.x[t], T.y[t], T.z[t], mm));
+        }
+    }
+    if(threadIdx.x < 8) {
+        int nx = bx + (threadIdx.x >> 2), ny = by + ((threadIdx.x >> 1) & 1), nz = bz + (threadIdx.x & 1);
+        uint32_t nb = sc.nb_base + ((uint32_t)nx * sc.NN[1] + ny) * sc.NN[2] + nz;
+        if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.counters[CNT_NODE_BLOCKS], 1u)] = nb;
+    }
+}
+
+// P2G variant 0: one thread per cell of the block.  A thread walks the
+// particles of its cell (they share the 27 nodes), accumulates the node values
+// in registers, and adds them to the shared tile once per cell: 8x fewer
+// shared atomics than one per particle, and the 64 lanes of a block hit 64
+// different node addresses for any given node offset.
+__global__ void __launch_bounds__(64) k_p2g_cells(FastArgs a)
+{
+    __shared__ P2GTile T;
     const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    const float Dx = 4.f * a.inv[0] * a.inv[0], Dy = 4.f * a.inv[1] * a.inv[1], Dz = 4.f * a.inv[2] * a.inv[2];
     const int c = threadIdx.x;   // cell in block: (lx << 4) | (ly << 2) | lz
     const int lx = c >> 4, ly = (c >> 2) & 3, lz = c & 3;
-    for(int w = next_work(&a.counters[CNT_P2G_WORK], &s_work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &s_work)) {
-        uint32_t b = a.active[w];
-        int bx, by, bz;
-        block_coords(a, b, bx, by, bz);
-        const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;   // tile origin, ghosted node coords
-        for(int t = c; t < TN; t += 64) { tm[t] = 0; tx[t] = 0; ty[t] = 0; tz[t] = 0; }
-        ccount[c] = 0;
-        __syncthreads();
-        const uint32_t s = a.bstart[b], e = a.bend[b];
-        for(uint32_t j = s + c; j < e; j += 64) atomicAdd(&ccount[a.sorted_keys[j] & 63u], 1u);
-        __syncthreads();
-        if(c < 32) {
-            uint32_t c0 = ccount[2 * c], c1 = ccount[2 * c + 1];
-            uint32_t sum = c0 + c1, x = sum;
-#pragma unroll
-            for(int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                if(c >= o) x += y;
-            }
-            cstart[2 * c] = x - sum;
-            cstart[2 * c + 1] = x - sum + c0;
-        }
-        __syncthreads();
-        const uint32_t cnt = ccount[c], beg = s + cstart[c];
+    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
+        const uint32_t b = a.active[w];
+        p2g_begin(a, T, b);
+        const uint32_t cnt = T.ccount[c], beg = a.bstart[b] + T.cstart[c];
         if(cnt) {
             float am[27], ax[27], ay[27], az[27];
 #pragma unroll
             for(int q = 0; q < 27; q++) { am[q] = 0; ax[q] = 0; ay[q] = 0; az[q] = 0; }
             for(uint32_t k = 0; k < cnt; k++) {
-                const uint32_t i = a.perm[beg + k];
-                float X[3], V[3], F[9], Bm[9];
-#pragma unroll
-                for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
-#pragma unroll
-                for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; Bm[r] = a.src[(C_B + r) * a.npad + i]; }
-                const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
-                float S[9];
-                if(!stress_fast(a.sp.model, F, at.z, at.w, S)) {
-                    atomicAdd(&a.counters[CNT_FALLBACK], 1u);
-                    if(!stress_fp64(a.sp.model, F, at.z, at.w, S)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
-                }
-                const float sv = a.dt * at.y, m = at.x;
-#pragma unroll
-                for(int r = 0; r < 9; r++) S[r] *= sv;
-                Axis<float> wx = spline_axis<float>(X[0], a.dmin[0], a.dx[0], a.inv[0]);
-                Axis<float> wy = spline_axis<float>(X[1], a.dmin[1], a.dx[1], a.inv[1]);
-                Axis<float> wz = spline_axis<float>(X[2], a.dmin[2], a.dx[2], a.inv[2]);
-                // affine term m B D (Z - X), separable per axis offset
-                float ux[3][3], uy[3][3], uz[3][3];
-#pragma unroll
-                for(int o = 0; o < 3; o++) {
-                    float dxo = (a.dmin[0] + ((float)(wx.base + o) + 0.5f) * a.dx[0] - X[0]) * Dx * m;
-                    float dyo = (a.dmin[1] + ((float)(wy.base + o) + 0.5f) * a.dx[1] - X[1]) * Dy * m;
-                    float dzo = (a.dmin[2] + ((float)(wz.base + o) + 0.5f) * a.dx[2] - X[2]) * Dz * m;
-#pragma unroll
-                    for(int r = 0; r < 3; r++) {
-                        ux[o][r] = Bm[r] * dxo + m * V[r];   // the x factor also carries m V
-                        uy[o][r] = Bm[r + 3] * dyo;
-                        uz[o][r] = Bm[r + 6] * dzo;
-                    }
-                }
-#pragma unroll
-                for(int ii = 0; ii < 3; ii++)
-#pragma unroll
-                    for(int jj = 0; jj < 3; jj++) {
-                        const float wxy = wx.w[ii] * wy.w[jj];
-                        const float gx0 = wx.dw[ii] * wy.w[jj], gy0 = wx.w[ii] * wy.dw[jj];
-                        const float mxy = m * wxy;
-                        float P[3], Cc[3];
-#pragma unroll
-                        for(int r = 0; r < 3; r++) {
-                            P[r] = wxy * (ux[ii][r] + uy[jj][r]) - (S[r] * gx0 + S[r + 3] * gy0);
-                            Cc[r] = S[r + 6] * wxy;
-                        }
-#pragma unroll
-                        for(int kk = 0; kk < 3; kk++) {
-                            const int q = (ii * 3 + jj) * 3 + kk;
-                            const float wzk = wz.w[kk], dwz = wz.dw[kk], wq = wxy * wzk;
-                            am[q] += mxy * wzk;
-                            ax[q] += wzk * P[0] + wq * uz[kk][0] - Cc[0] * dwz;
-                            ay[q] += wzk * P[1] + wq * uz[kk][1] - Cc[1] * dwz;
-                            az[q] += wzk * P[2] + wq * uz[kk][2] - Cc[2] * dwz;
-                        }
-                    }
+                P2GParticle P;
+                p2g_particle(a, T.sc, a.perm[beg + k], P);
+                p2g_nodes(P, [&](int q, float m, float px, float py, float pz) {
+                    am[q] += m; ax[q] += px; ay[q] += py; az[q] += pz;
+                });
             }
             const int t0 = (lx * TE + ly) * TE + lz;
 #pragma unroll
@@ -341,25 +416,44 @@ __global__ void __launch_bounds__(64) k_p2g(FastArgs a)
 #pragma unroll
                     for(int kk = 0; kk < 3; kk++) {
                         const int q = (ii * 3 + jj) * 3 + kk, t = t0 + (ii * TE + jj) * TE + kk;
-                        atomicAdd(&tm[t], am[q]);
-                        atomicAdd(&tx[t], ax[q]);
-                        atomicAdd(&ty[t], ay[q]);
-                        atomicAdd(&tz[t], az[q]);
+                        atomicAdd(&T.m[t], am[q]);
+                        atomicAdd(&T.x[t], ax[q]);
+                        atomicAdd(&T.y[t], ay[q]);
+                        atomicAdd(&T.z[t], az[q]);
                     }
         }
-        __syncthreads();
-        for(int t = c; t < TN; t += 64) {
-            float mm = tm[t];
-            if(mm != 0.f) {
-                int qx = ox + t / (TE * TE), qy = oy + (t / TE) % TE, qz = oz + t % TE;
-                atomicAdd(&a.acc[node_index(a, qx, qy, qz)], make_float4(tx[t], ty[t], tz[t], mm));
-            }
+        p2g_end(a, T, b - T.sc.block_base);
+    }
+}
+
+// P2G variant 1: one thread per particle, handed out round-robin over the
+// cells of the block (lane c of a round takes that cell's next particle), so
+// the lanes of one shared atomic hit different nodes.  Fewer registers than
+// variant 0, one shared atomic per node value per particle.
+template<int THREADS> __global__ void __launch_bounds__(THREADS) k_p2g_interleaved(FastArgs a)
+{
+    __shared__ P2GTile T;
+    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
+    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
+        const uint32_t b = a.active[w];
+        p2g_begin(a, T, b);
+        const uint32_t s = a.bstart[b], slots = T.maxc * 64u;
+        for(uint32_t q = threadIdx.x; q < slots; q += THREADS) {
+            const uint32_t c = q & 63u, r = q >> 6;
+            if(r >= T.ccount[c]) continue;
+            P2GParticle P;
+            p2g_particle(a, T.sc, a.perm[s + T.cstart[c] + r], P);
+            const int t0 = (((c >> 4)) * TE + ((c >> 2) & 3)) * TE + (c & 3);
+            p2g_nodes(P, [&](int qn, float m, float px, float py, float pz) {
+                const int ii = qn / 9, jj = (qn / 3) % 3, kk = qn % 3;
+                const int t = t0 + (ii * TE + jj) * TE + kk;
+                atomicAdd(&T.m[t], m);
+                atomicAdd(&T.x[t], px);
+                atomicAdd(&T.y[t], py);
+                atomicAdd(&T.z[t], pz);
+            });
         }
-        if(c < 8) {
-            int nx = bx + (c >> 2), ny = by + ((c >> 1) & 1), nz = bz + (c & 1);
-            uint32_t nb = ((uint32_t)nx * a.NN[1] + ny) * a.NN[2] + nz;
-            if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.counters[CNT_NODE_BLOCKS], 1u)] = nb;
-        }
+        p2g_end(a, T, b - T.sc.block_base);
     }
 }
 
@@ -367,25 +461,30 @@ __global__ void __launch_bounds__(64) k_p2g(FastArgs a)
 __global__ void __launch_bounds__(64) k_grid(FastArgs a)
 {
     __shared__ int s_work;
+    __shared__ SceneDev s_sc;
     const uint32_t nnb = a.counters[CNT_NODE_BLOCKS];
     for(int w = next_work(&a.counters[CNT_GRID_WORK], &s_work); w < (int)nnb; w = next_work(&a.counters[CNT_GRID_WORK], &s_work)) {
-        uint32_t nb = a.nb_list[w];
-        int nz = nb % a.NN[2], r = nb / a.NN[2], ny = r % a.NN[1], nx = r / a.NN[1];
+        const uint32_t nb = a.nb_list[w];
+        stage_scene(a, a.nb_scene[nb], &s_sc);
+        __syncthreads();
+        const SceneDev& sc = s_sc;
+        const uint32_t lnb = nb - sc.nb_base;
+        int nz = lnb % sc.NN[2], r = lnb / sc.NN[2], ny = r % sc.NN[1], nx = r / sc.NN[1];
         int t = threadIdx.x;
         int qx = 4 * nx + (t >> 4), qy = 4 * ny + ((t >> 2) & 3), qz = 4 * nz + (t & 3);
-        int64_t q = node_index(a, qx, qy, qz);
+        int64_t q = node_index(sc, qx, qy, qz);
         float4 c = a.acc[q];
         float4 o0 = make_float4(0, 0, 0, 0), o1 = make_float4(0, 0, 0, 0);
         if(c.w != 0.f) {
             float im = 1.f / c.w;
-            float V[3] = {c.x * im + a.dt * a.gravity[0], c.y * im + a.dt * a.gravity[1], c.z * im + a.dt * a.gravity[2]};
+            float V[3] = {c.x * im + a.dt * sc.gravity[0], c.y * im + a.dt * sc.gravity[1], c.z * im + a.dt * sc.gravity[2]};
             float vn[3], vf[3];
-            if(a.sp.nobj) {
-                float X0[3] = {a.dmin[0] + ((float)(qx - MPM_GHOST) + 0.5f) * a.dx[0],
-                               a.dmin[1] + ((float)(qy - MPM_GHOST) + 0.5f) * a.dx[1],
-                               a.dmin[2] + ((float)(qz - MPM_GHOST) + 0.5f) * a.dx[2]};
+            if(sc.nobj) {
+                float X0[3] = {sc.dmin[0] + ((float)(qx - MPM_GHOST) + 0.5f) * sc.dx[0],
+                               sc.dmin[1] + ((float)(qy - MPM_GHOST) + 0.5f) * sc.dx[1],
+                               sc.dmin[2] + ((float)(qz - MPM_GHOST) + 0.5f) * sc.dx[2]};
                 float zero[3] = {0.f, 0.f, 0.f};
-                collide_node<float, 3>(a.sp.objs, a.sp.nobj, X0, zero, V, a.dt, vn, vf);
+                collide_node<float, 3>(a.objs + sc.obj_begin, sc.nobj, X0, zero, V, a.dt, vn, vf);
             } else {
 #pragma unroll
                 for(int k = 0; k < 3; k++) vn[k] = vf[k] = V[k];
@@ -414,17 +513,21 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
 {
     __shared__ float4 tv[2 * TN];
     __shared__ int s_work;
+    __shared__ SceneDev s_sc;
     const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
     const float dt = a.dt;
     for(int w = next_work(&a.counters[CNT_G2P_WORK], &s_work); w < (int)nblocks; w = next_work(&a.counters[CNT_G2P_WORK], &s_work)) {
-        uint32_t b = a.active[w];
+        const uint32_t b = a.active[w];
+        stage_scene(a, a.block_scene[b], &s_sc);
+        __syncthreads();
+        const SceneDev& sc = s_sc;
         int bx, by, bz;
-        block_coords(a, b, bx, by, bz);
+        block_coords(sc, b - sc.block_base, bx, by, bz);
         const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;
         int differs = 0;
         for(int t = threadIdx.x; t < TN; t += THREADS) {
             int qx = ox + t / (TE * TE), qy = oy + (t / TE) % TE, qz = oz + t % TE;
-            int64_t q = node_index(a, qx, qy, qz);
+            int64_t q = node_index(sc, qx, qy, qz);
             float4 p0 = a.vel[2 * q], p1 = a.vel[2 * q + 1];
             tv[2 * t] = p0;
             tv[2 * t + 1] = p1;
@@ -441,16 +544,16 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
             for(int k = 0; k < 9; k++) F[k] = a.src[(C_F + k) * a.npad + i];
             const float4 at = a.src_attr[i];
             const int pid = a.src_pid[i];
-            Axis<float> wx = spline_axis<float>(X[0], a.dmin[0], a.dx[0], a.inv[0]);
-            Axis<float> wy = spline_axis<float>(X[1], a.dmin[1], a.dx[1], a.inv[1]);
-            Axis<float> wz = spline_axis<float>(X[2], a.dmin[2], a.dx[2], a.inv[2]);
+            Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
+            Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
+            Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
             const int t0 = ((wx.base + MPM_GHOST - ox) * TE + (wy.base + MPM_GHOST - oy)) * TE + (wz.base + MPM_GHOST - oz);
             float dX[3], dY[3], wzd[3];
 #pragma unroll
             for(int o = 0; o < 3; o++) {
-                dX[o] = a.dmin[0] + ((float)(wx.base + o) + 0.5f) * a.dx[0] - X[0];
-                dY[o] = a.dmin[1] + ((float)(wy.base + o) + 0.5f) * a.dx[1] - X[1];
-                wzd[o] = wz.w[o] * (a.dmin[2] + ((float)(wz.base + o) + 0.5f) * a.dx[2] - X[2]);
+                dX[o] = sc.dmin[0] + ((float)(wx.base + o) + 0.5f) * sc.dx[0] - X[0];
+                dY[o] = sc.dmin[1] + ((float)(wy.base + o) + 0.5f) * sc.dx[1] - X[1];
+                wzd[o] = wz.w[o] * (sc.dmin[2] + ((float)(wz.base + o) + 0.5f) * sc.dx[2] - X[2]);
             }
             float Vp[3] = {0, 0, 0}, Vf[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Bv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
             float K01 = 0, K02 = 0, K12 = 0;
@@ -515,15 +618,15 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
             bool ok = true;
 #pragma unroll
             for(int k = 0; k < 3; k++) {
-                float eps = FLT_EPSILON * 4.f * (a.dmax[k] - a.dmin[k]);
-                if(!(xn[k] >= a.dmin[k] + eps && xn[k] <= a.dmax[k] - eps)) ok = false;
+                float eps = FLT_EPSILON * 4.f * (sc.dmax[k] - sc.dmin[k]);
+                if(!(xn[k] >= sc.dmin[k] + eps && xn[k] <= sc.dmax[k] - eps)) ok = false;
             }
             bool finite = true;
 #pragma unroll
             for(int k = 0; k < 9; k++) finite = finite && isfinite(Fn[k]);
             finite = finite && isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]);
             if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); ok = false; }
-            const uint32_t key = ok ? cell_key(a, xn) : SENTINEL;
+            const uint32_t key = ok ? cell_key(sc, xn) : SENTINEL;
 #pragma unroll
             for(int k = 0; k < 3; k++) { a.dst[(C_X + k) * a.npad + j] = xn[k]; a.dst[(C_V + k) * a.npad + j] = Vf[k]; }
 #pragma unroll
@@ -566,16 +669,17 @@ template<class T> __global__ void k_gather_out(FastArgs a, const uint32_t* keys,
     }
 }
 
+// Grids of scene 0 in the reference's ghosted layout (single-scene handles).
 __global__ void k_grid_out(FastArgs a, const uint32_t* list, uint32_t count, double* m, double* v, double* vf, int G0, int G1, int G2)
 {
-    // one node block per CTA of 64 threads
+    const SceneDev& sc = a.scenes[0];
     for(uint32_t w = blockIdx.x; w < count; w += gridDim.x) {
-        uint32_t nb = list[w];
-        int nz = nb % a.NN[2], r = nb / a.NN[2], ny = r % a.NN[1], nx = r / a.NN[1];
+        uint32_t nb = list[w] - sc.nb_base;
+        int nz = nb % sc.NN[2], r = nb / sc.NN[2], ny = r % sc.NN[1], nx = r / sc.NN[1];
         int t = threadIdx.x;
         int qx = 4 * nx + (t >> 4), qy = 4 * ny + ((t >> 2) & 3), qz = 4 * nz + (t & 3);
         if(qx >= G0 || qy >= G1 || qz >= G2) continue;
-        int64_t q = node_index(a, qx, qy, qz);
+        int64_t q = node_index(sc, qx, qy, qz);
         int64_t o = ((int64_t)qx * G1 + qy) * G2 + qz;
         float4 p0 = a.vel[2 * q], p1 = a.vel[2 * q + 1];
         if(m) m[o] = p1.z;
@@ -595,7 +699,6 @@ FastArgs make_args(mpm_handle* h, double dt)
 {
     FastArgs a;
     FastState& f = h->fast;
-    a.sp = h->sp;
     a.n = f.n;
     a.npad = f.npad;
     int c = f.cur, o = 1 - f.cur;
@@ -607,16 +710,9 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.bstart = f.bstart; a.bend = f.bend; a.active = f.active;
     a.nb_flag = f.nb_flag; a.nb_list = f.nb_list; a.counters = f.counters;
     a.acc = f.acc; a.vel = f.vel;
-    for(int k = 0; k < 3; k++) {
-        a.GA[k] = 4 * f.NN[k];
-        a.NB[k] = f.NB[k];
-        a.NN[k] = f.NN[k];
-        a.dmin[k] = (float)h->sp.dmin[k];
-        a.dmax[k] = (float)h->sp.dmax[k];
-        a.dx[k] = (float)h->sp.dx[k];
-        a.inv[k] = (float)h->sp.inv_dx[k];
-        a.gravity[k] = (float)h->sp.gravity[k];
-    }
+    a.scenes = f.scenes; a.block_scene = f.block_scene; a.nb_scene = f.nb_scene; a.pbase = f.pbase;
+    a.objs = f.objs;
+    a.nscenes = f.nscenes;
     a.dt = (float)dt;
     a.flags = h->d_flags;
     return a;
@@ -629,55 +725,157 @@ int grid_stride_blocks(mpm_handle* h, int64_t n, int t)
     return (int)(b < 1 ? 1 : b);
 }
 
-constexpr int P2G_THREADS = 64;   // one thread per cell of a 4^3 block
-constexpr int G2P_THREADS = 128;
+// Launch shapes the autotuner chooses among.
+const int kG2PThreads[] = {64, 128, 256};
+
+int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult)
+{
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, 0);
+    return h->sm_count * (occ > 0 ? occ : 1) * mult;
+}
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Scenes: block / node-block / grid numbering of the whole batch.
+// ---------------------------------------------------------------------------
+int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, const mpm_collision_object* objs, int nobjs)
+{
+    FastState& f = h->fast;
+    if(count < 1 || count > 65535) return set_error(h, MPM_ERR_ARG, "between 1 and 65535 scenes");
+    std::vector<SceneDev> sc(count);
+    std::vector<int64_t> pb(count + 1, 0);
+    int64_t blocks = 0, nblocks = 0, nodes = 0;
+    for(int s = 0; s < count; s++) {
+        const mpm_scene_desc& d = descs[s];
+        if(d.grid.dim != 3 || d.grid.ghost != MPM_GHOST) return set_error(h, MPM_ERR_ARG, "batched scenes are 3D with ghost 3");
+        if(d.model != MPM_COROTATED_FIXED && d.model != MPM_NEO_HOOKEAN) return set_error(h, MPM_ERR_ARG, "model");
+        if(d.particle_count < 0) return set_error(h, MPM_ERR_ARG, "particle_count");
+        if(d.object_count < 0 || d.object_count > MPM_MAX_OBJECTS || d.first_object < 0 || d.first_object + d.object_count > nobjs)
+            return set_error(h, MPM_ERR_ARG, "scene collision-object range");
+        SceneDev& c = sc[s];
+        memset(&c, 0, sizeof(c));
+        int64_t snodes = 1, sblocks = 1, snb = 1;
+        for(int k = 0; k < 3; k++) {
+            if(d.grid.counts[k] < 1 || d.grid.counts[k] > 4096 || !(d.grid.domain_max[k] > d.grid.domain_min[k]))
+                return set_error(h, MPM_ERR_ARG, "scene grid");
+            double dx = (d.grid.domain_max[k] - d.grid.domain_min[k]) / d.grid.counts[k];   // GRID.cpp:23-24
+            c.dmin[k] = (float)d.grid.domain_min[k];
+            c.dmax[k] = (float)d.grid.domain_max[k];
+            c.dx[k] = (float)dx;
+            c.inv[k] = (float)(1 / dx);
+            c.gravity[k] = (float)d.gravity[k];
+            c.counts[k] = d.grid.counts[k];
+            c.NB[k] = (d.grid.counts[k] + 4 + 3) / 4;
+            c.NN[k] = c.NB[k] + 1;
+            c.GA[k] = 4 * c.NN[k];
+            snodes *= c.GA[k];
+            sblocks *= c.NB[k];
+            snb *= c.NN[k];
+        }
+        c.block_base = (uint32_t)blocks;
+        c.nb_base = (uint32_t)nblocks;
+        c.node_base = nodes;
+        c.model = d.model;
+        c.obj_begin = d.first_object;
+        c.nobj = d.object_count;
+        blocks += sblocks;
+        nblocks += snb;
+        nodes += snodes;
+        pb[s + 1] = pb[s] + d.particle_count;
+    }
+    int bits = 6;
+    while((1LL << bits) <= blocks * 64) bits++;
+    if(bits > 32) return set_error(h, MPM_ERR_ARG, "batch too large for 32-bit cell keys");
+    fast_free(h);
+    f.nscenes = count;
+    f.scenes_h = sc;
+    f.pbase_h = pb;
+    f.key_bits = bits;
+    f.total_blocks = blocks;
+    f.total_nblocks = nblocks;
+    f.total_nodes = nodes;
+    std::vector<uint16_t> bs(blocks), ns(nblocks);
+    for(int s = 0; s < count; s++) {
+        int64_t b1 = s + 1 < count ? sc[s + 1].block_base : blocks;
+        int64_t n1 = s + 1 < count ? sc[s + 1].nb_base : nblocks;
+        for(int64_t b = sc[s].block_base; b < b1; b++) bs[b] = (uint16_t)s;
+        for(int64_t b = sc[s].nb_base; b < n1; b++) ns[b] = (uint16_t)s;
+    }
+    MPM_CUDA(h, cudaMalloc(&f.scenes, count * sizeof(SceneDev)));
+    MPM_CUDA(h, cudaMemcpy(f.scenes, sc.data(), count * sizeof(SceneDev), cudaMemcpyHostToDevice));
+    MPM_CUDA(h, cudaMalloc(&f.pbase, (count + 1) * sizeof(int64_t)));
+    MPM_CUDA(h, cudaMemcpy(f.pbase, pb.data(), (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+    MPM_CUDA(h, cudaMalloc(&f.block_scene, blocks * sizeof(uint16_t)));
+    MPM_CUDA(h, cudaMemcpy(f.block_scene, bs.data(), blocks * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    MPM_CUDA(h, cudaMalloc(&f.nb_scene, nblocks * sizeof(uint16_t)));
+    MPM_CUDA(h, cudaMemcpy(f.nb_scene, ns.data(), nblocks * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    f.objs_h.assign(nobjs > 0 ? nobjs : 1, DevObject{});
+    for(int i = 0; i < nobjs; i++) {
+        DevObject& o = f.objs_h[i];
+        o.kind = objs[i].kind;
+        o.type = objs[i].type;
+        o.friction = objs[i].friction;
+        for(int k = 0; k < 3; k++) { o.a[k] = objs[i].a[k]; o.b[k] = objs[i].b[k]; }
+    }
+    MPM_CUDA(h, cudaMalloc(&f.objs, f.objs_h.size() * sizeof(DevObject)));
+    MPM_CUDA(h, cudaMemcpy(f.objs, f.objs_h.data(), f.objs_h.size() * sizeof(DevObject), cudaMemcpyHostToDevice));
+    MPM_CUDA(h, cudaMalloc(&f.acc, nodes * sizeof(float4)));
+    MPM_CUDA(h, cudaMalloc(&f.vel, nodes * 2 * sizeof(float4)));
+    MPM_CUDA(h, cudaMemset(f.acc, 0, nodes * sizeof(float4)));
+    MPM_CUDA(h, cudaMemset(f.vel, 0, nodes * 2 * sizeof(float4)));
+    MPM_CUDA(h, cudaMalloc(&f.bstart, blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.bend, blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.active, blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.nb_flag, nblocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.nb_list, nblocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMemset(f.nb_flag, 0, nblocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.counters, CNT_COUNT * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMemset(f.counters, 0, CNT_COUNT * sizeof(uint32_t)));
+    return MPM_OK;
+}
+
+// Single-scene handles: scene 0 from the handle's grid, model and objects.
+int fast_single_scene(mpm_handle* h)
+{
+    mpm_scene_desc d;
+    memset(&d, 0, sizeof(d));
+    d.grid = h->grid;
+    d.model = h->model.model;
+    for(int k = 0; k < 3; k++) d.gravity[k] = h->model.gravity[k];
+    d.particle_count = h->fast.n;
+    d.first_object = 0;
+    d.object_count = h->sp.nobj;
+    mpm_collision_object objs[MPM_MAX_OBJECTS];
+    for(int i = 0; i < h->sp.nobj; i++) {
+        objs[i].kind = h->sp.objs[i].kind;
+        objs[i].type = h->sp.objs[i].type;
+        objs[i].friction = h->sp.objs[i].friction;
+        for(int k = 0; k < 3; k++) { objs[i].a[k] = h->sp.objs[i].a[k]; objs[i].b[k] = h->sp.objs[i].b[k]; }
+    }
+    int64_t n = h->fast.n;
+    int rc = fast_setup_scenes(h, &d, 1, objs, h->sp.nobj);
+    h->fast.n = n;
+    return rc;
+}
 
 int fast_alloc(mpm_handle* h, int64_t n)
 {
     FastState& f = h->fast;
     if(h->sp.dim != 3) return set_error(h, MPM_ERR_ARG, "the fast path is 3D; use MPM_PATH_PLAIN for 2D");
-    if(n > 0x7fffffffLL) return set_error(h, MPM_ERR_ARG, "more than 2^31-1 particles");
-    if(!f.acc) {
-        int64_t nodes = 1, blocks = 1, nblocks = 1;
-        for(int k = 0; k < 3; k++) {
-            f.NB[k] = (h->sp.counts[k] + 4 + 3) / 4;
-            f.NN[k] = f.NB[k] + 1;
-            f.GP[k] = 4 * f.NB[k] + 2;
-            nodes *= 4 * f.NN[k];
-            blocks *= f.NB[k];
-            nblocks *= f.NN[k];
-        }
-        int bits = 6;
-        while((1LL << bits) <= blocks * 64) bits++;
-        if(bits > 32) return set_error(h, MPM_ERR_ARG, "grid too large for 32-bit cell keys");
-        f.key_bits = bits;
-        MPM_CUDA(h, cudaMalloc(&f.acc, nodes * sizeof(float4)));
-        MPM_CUDA(h, cudaMalloc(&f.vel, nodes * 2 * sizeof(float4)));
-        MPM_CUDA(h, cudaMemsetAsync(f.acc, 0, nodes * sizeof(float4), h->stream));
-        MPM_CUDA(h, cudaMemsetAsync(f.vel, 0, nodes * 2 * sizeof(float4), h->stream));
-        MPM_CUDA(h, cudaMalloc(&f.bstart, blocks * sizeof(uint32_t)));
-        MPM_CUDA(h, cudaMalloc(&f.bend, blocks * sizeof(uint32_t)));
-        MPM_CUDA(h, cudaMalloc(&f.active, blocks * sizeof(uint32_t)));
-        MPM_CUDA(h, cudaMalloc(&f.nb_flag, nblocks * sizeof(uint32_t)));
-        MPM_CUDA(h, cudaMalloc(&f.nb_list, nblocks * sizeof(uint32_t)));
-        MPM_CUDA(h, cudaMemsetAsync(f.nb_flag, 0, nblocks * sizeof(uint32_t), h->stream));
-        MPM_CUDA(h, cudaMalloc(&f.counters, CNT_COUNT * sizeof(uint32_t)));
-        MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
-        int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_p2g, P2G_THREADS, 0);
-        f.p2g_ctas = h->sm_count * (occ > 0 ? occ : 1);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_g2p<G2P_THREADS>, G2P_THREADS, 0);
-        f.g2p_ctas = h->sm_count * (occ > 0 ? occ : 1);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_grid, 64, 0);
-        f.grid_ctas = h->sm_count * (occ > 0 ? occ : 1);
+    if(n >= (1LL << 30)) return set_error(h, MPM_ERR_ARG, "more than 2^30 - 1 particles");
+    if(f.batch) {
+        if(n != f.pbase_h.back()) return set_error(h, MPM_ERR_ARG, "particle count differs from the scenes' total");
+    } else {
+        int rc;
+        f.n = n;
+        if((rc = fast_single_scene(h))) return rc;
     }
     if(f.n != n || !f.soa[0]) {
-        for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); }
-        uint32_t* ps[] = {f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, f.sort_scratch};
-        for(uint32_t* p: ps) cudaFree(p);
-        if(n >= (1LL << 30)) return set_error(h, MPM_ERR_ARG, "more than 2^30 - 1 particles");
+        for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; }
+        uint32_t** ps[] = {&f.keys, &f.sorted_keys, &f.perm, &f.sort_keys_alt, &f.sort_vals_alt, &f.sort_scratch};
+        for(uint32_t** p: ps) { cudaFree(*p); *p = nullptr; }
         int64_t np = ((n ? n : 1) + 31) / 32 * 32;
         f.npad = np;
         for(int b = 0; b < 2; b++) {
@@ -701,11 +899,15 @@ int fast_alloc(mpm_handle* h, int64_t n)
 void fast_free(mpm_handle* h)
 {
     FastState& f = h->fast;
-    for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); }
-    void* ps[] = {f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, f.sort_scratch,
-                  f.bstart, f.bend, f.active, f.nb_flag, f.nb_list, f.counters, f.acc, f.vel};
-    for(void* p: ps) cudaFree(p);
-    f = FastState();
+    for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; }
+    void** ps[] = {(void**)&f.keys, (void**)&f.sorted_keys, (void**)&f.perm, (void**)&f.sort_keys_alt, (void**)&f.sort_vals_alt,
+                   (void**)&f.sort_scratch, (void**)&f.bstart, (void**)&f.bend, (void**)&f.active, (void**)&f.nb_flag,
+                   (void**)&f.nb_list, (void**)&f.counters, (void**)&f.acc, (void**)&f.vel, (void**)&f.scenes,
+                   (void**)&f.block_scene, (void**)&f.nb_scene, (void**)&f.pbase, (void**)&f.objs};
+    for(void** p: ps) { cudaFree(*p); *p = nullptr; }
+    f.n = 0;
+    f.npad = 0;
+    f.keys_ready = false;
 }
 
 int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
@@ -825,7 +1027,8 @@ int fast_p2g(mpm_handle* h, double dt, double)
     MPM_LAUNCHED(h, "k_tail");
     timer_end(h, slot);
     slot = timer_begin(h, "fast_p2g");
-    k_p2g<<<f.p2g_ctas, P2G_THREADS, 0, h->stream>>>(a);
+    if(f.p2g_variant == 0) k_p2g_cells<<<occupancy_ctas(h, (const void*)k_p2g_cells, 64, f.cta_mult), 64, 0, h->stream>>>(a);
+    else k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_p2g");
     return MPM_OK;
@@ -837,7 +1040,7 @@ int fast_forces(mpm_handle* h, double dt, double)
     if(!f.n) return MPM_OK;
     FastArgs a = make_args(h, dt);
     int slot = timer_begin(h, "fast_grid");
-    k_grid<<<f.grid_ctas, 64, 0, h->stream>>>(a);
+    k_grid<<<occupancy_ctas(h, (const void*)k_grid, 64, 1), 64, 0, h->stream>>>(a);
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_grid");
     return MPM_OK;
@@ -849,7 +1052,11 @@ int fast_g2p(mpm_handle* h, double dt, double)
     if(!f.n) return MPM_OK;
     FastArgs a = make_args(h, dt);
     int slot = timer_begin(h, "fast_g2p");
-    k_g2p<G2P_THREADS><<<f.g2p_ctas, G2P_THREADS, 0, h->stream>>>(a);
+    switch(f.g2p_threads) {
+        case 64: k_g2p<64><<<occupancy_ctas(h, (const void*)k_g2p<64>, 64, f.cta_mult), 64, 0, h->stream>>>(a); break;
+        case 256: k_g2p<256><<<occupancy_ctas(h, (const void*)k_g2p<256>, 256, f.cta_mult), 256, 0, h->stream>>>(a); break;
+        default: k_g2p<128><<<occupancy_ctas(h, (const void*)k_g2p<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a); break;
+    }
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_g2p");
     f.cur = 1 - f.cur;
@@ -860,6 +1067,7 @@ int fast_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf)
 {
     FastState& f = h->fast;
     if(v0) return set_error(h, MPM_ERR_ARG, "velocity after P2G is not kept on the fast path");
+    if(f.nscenes != 1) return set_error(h, MPM_ERR_ARG, "grids are returned for single-scene handles");
     int G[3];
     int64_t gn = 1;
     for(int k = 0; k < 3; k++) { G[k] = h->sp.counts[k] + 2 * MPM_GHOST; gn *= G[k]; }
@@ -911,6 +1119,87 @@ int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_k
     return MPM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Autotuner: times every (P2G variant, G2P block size, persistent-CTA multiple)
+// on the handle's own particles for a few substeps and keeps the fastest.  The
+// particle state is restored afterwards (the trials run on a copy).
+// ---------------------------------------------------------------------------
+int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len)
+{
+    FastState& f = h->fast;
+    if(!f.keys_ready || !f.n) return set_error(h, MPM_ERR_STATE, "particles not set");
+    if(substeps < 1) substeps = 1;
+    // keep the current state: both buffers + keys
+    const int64_t np = f.npad;
+    float* save_soa = nullptr;
+    float4* save_attr = nullptr;
+    int* save_pid = nullptr;
+    uint32_t* save_keys = nullptr;
+    MPM_CUDA(h, cudaMalloc(&save_soa, NCOMP * np * sizeof(float)));
+    MPM_CUDA(h, cudaMalloc(&save_attr, np * sizeof(float4)));
+    MPM_CUDA(h, cudaMalloc(&save_pid, np * sizeof(int)));
+    MPM_CUDA(h, cudaMalloc(&save_keys, np * sizeof(uint32_t)));
+    const int cur0 = f.cur;
+    MPM_CUDA(h, cudaMemcpyAsync(save_soa, f.soa[cur0], NCOMP * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(save_attr, f.attr[cur0], np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(save_pid, f.pid[cur0], np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(save_keys, f.keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::string rep;
+    float best = 1e30f;
+    int best_v = f.p2g_variant, best_t = f.g2p_threads, best_m = f.cta_mult;
+    const bool timing = h->timing;
+    h->timing = false;
+    int rc = MPM_OK;
+    for(int variant = 0; variant < 2 && !rc; variant++)
+        for(int ti = 0; ti < 3 && !rc; ti++)
+            for(int mult = 1; mult <= 2 && !rc; mult++) {
+                f.p2g_variant = variant;
+                f.g2p_threads = kG2PThreads[ti];
+                f.cta_mult = mult;
+                // restore, warm up one substep, then time
+                f.cur = cur0;
+                cudaMemcpyAsync(f.soa[cur0], save_soa, NCOMP * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
+                cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
+                cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
+                cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
+                if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_g2p(h, dt, 0))) break;
+                cudaEventRecord(e0, h->stream);
+                for(int s = 0; s < substeps && !rc; s++)
+                    if(!(rc = fast_p2g(h, dt, 0)) && !(rc = fast_forces(h, dt, 0))) rc = fast_g2p(h, dt, 0);
+                cudaEventRecord(e1, h->stream);
+                if(cudaEventSynchronize(e1) != cudaSuccess) { rc = check_cuda(h, cudaGetLastError(), "autotune"); break; }
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms /= substeps;
+                char line[128];
+                snprintf(line, sizeof line, "%sp2g=%s g2p=%d ctas=x%d: %.4f ms", rep.empty() ? "" : "; ",
+                         variant ? "interleaved" : "cells", kG2PThreads[ti], mult, ms);
+                rep += line;
+                if(ms < best) { best = ms; best_v = variant; best_t = kG2PThreads[ti]; best_m = mult; }
+            }
+    h->timing = timing;
+    f.p2g_variant = best_v;
+    f.g2p_threads = best_t;
+    f.cta_mult = best_m;
+    f.cur = cur0;
+    cudaMemcpyAsync(f.soa[cur0], save_soa, NCOMP * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(save_soa); cudaFree(save_attr); cudaFree(save_pid); cudaFree(save_keys);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    char tail[128];
+    snprintf(tail, sizeof tail, " | chosen p2g=%s g2p=%d ctas=x%d (%.4f ms/substep)", best_v ? "interleaved" : "cells", best_t, best_m, best);
+    rep += tail;
+    if(report && report_len > 0) snprintf(report, (size_t)report_len, "%s", rep.c_str());
+    return rc;
+}
+
 int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm)
 {
     if(n < 0 || bits < 1 || bits > 32 || (n && (!keys || !sorted_keys || !perm))) return MPM_ERR_ARG;
@@ -935,12 +1224,12 @@ int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_
         if(mpm_sort::radix_sort(k, ko, vo, ka, va, n, bits, scratch, flags, MPM_FLAG_TIMEOUT, sms * 4, st) != cudaSuccess)
             rc = MPM_ERR_CUDA;
         else {
-            unsigned f = 0;
+            unsigned fl = 0;
             cudaMemcpyAsync(sorted_keys, ko, b, cudaMemcpyDeviceToHost, st);
             cudaMemcpyAsync(perm, vo, b, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(&f, flags, sizeof(f), cudaMemcpyDeviceToHost, st);
+            cudaMemcpyAsync(&fl, flags, sizeof(fl), cudaMemcpyDeviceToHost, st);
             if(cudaStreamSynchronize(st) != cudaSuccess) rc = MPM_ERR_CUDA;
-            else if(f & MPM_FLAG_TIMEOUT) rc = MPM_ERR_TIMEOUT;
+            else if(fl & MPM_FLAG_TIMEOUT) rc = MPM_ERR_TIMEOUT;
         }
     }
     cudaFree(k); cudaFree(ko); cudaFree(vo); cudaFree(ka); cudaFree(va); cudaFree(scratch); cudaFree(flags);

@@ -29,14 +29,38 @@ struct PlainState {
     void *gm = nullptr, *gmv = nullptr, *gv0 = nullptr, *gf = nullptr, *gv = nullptr, *gvf = nullptr;
 };
 
-// Fast path: cell-sorted SoA particles (double-buffered), block-sparse grid.
+// One scene of a batch, as the fast-path kernels see it.
+struct SceneDev {
+    float dmin[3], dmax[3], dx[3], inv[3], gravity[3];
+    int counts[3];
+    int NB[3];              // particle blocks (4^3 cells) per axis
+    int NN[3];              // node blocks (4^3 nodes) per axis
+    int GA[3];              // grid node extent per axis (4 NN >= G + 6)
+    uint32_t block_base;    // first global particle-block id of the scene
+    uint32_t nb_base;       // first global node-block id of the scene
+    int64_t node_base;      // first node of the scene's grid in the pooled grid
+    int model;
+    int obj_begin, nobj;    // collision objects [obj_begin, obj_begin + nobj)
+    int pad;
+};
+
+// Fast path: cell-sorted SoA particles (double-buffered), block-sparse grids of
+// one or more scenes.
 struct FastState {
     int64_t n = 0, npad = 0;
-    int GP[3] = {0, 0, 0};   // node extent of the internal grid (>= G+6, = 4*NB+2)
-    int NB[3] = {0, 0, 0};   // particle blocks (4^3 cells) per axis
-    int NN[3] = {0, 0, 0};   // node blocks (4^3 nodes) per axis
     int key_bits = 0;
     int cur = 0;
+    bool batch = false;                       // created by mpm_batch_create
+    int nscenes = 0;
+    std::vector<SceneDev> scenes_h;
+    std::vector<int64_t> pbase_h;             // particle offset of each scene, nscenes + 1
+    std::vector<mpm::DevObject> objs_h;
+    int64_t total_blocks = 0, total_nblocks = 0, total_nodes = 0;
+    SceneDev* scenes = nullptr;
+    uint16_t* block_scene = nullptr;          // global particle block -> scene
+    uint16_t* nb_scene = nullptr;             // global node block -> scene
+    int64_t* pbase = nullptr;
+    mpm::DevObject* objs = nullptr;
     float* soa[2] = {nullptr, nullptr};       // 24 * npad floats: x y z, vx vy vz, F0..8, B0..8
     float4* attr[2] = {nullptr, nullptr};     // mass, volume, mu, lambda
     int* pid[2] = {nullptr, nullptr};         // caller's particle index
@@ -55,7 +79,10 @@ struct FastState {
     float4* acc = nullptr;                    // P2G accumulator: momentum+dt*force (xyz), mass (w)
     float4* vel = nullptr;                    // per node 2 x float4: vnew.xyz, vfric.x | vfric.yz, mass, 0
     bool keys_ready = false;
-    int p2g_ctas = 0, g2p_ctas = 0, grid_ctas = 0;
+    // launch shapes (mpm_autotune)
+    int p2g_variant = 0;                      // 0: thread per cell, 1: thread per particle, cells interleaved
+    int g2p_threads = 128;
+    int cta_mult = 1;
 };
 
 enum FastCounter {
@@ -132,6 +159,8 @@ int fast_g2p(mpm_handle* h, double dt, double time);
 int fast_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf);
 int fast_count_valid(mpm_handle* h, int64_t* c);
 int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm);
+int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, const mpm_collision_object* objs, int nobjs);
+int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len);
 int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm);
 
 // adjoint (mpm_adjoint.cu)

@@ -61,7 +61,7 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_get_particles", "mpm_substep", "mpm_advance", "mpm_particle_to_grid", "mpm_apply_forces",
            "mpm_grid_to_particle", "mpm_synchronize", "mpm_get_grid", "mpm_count_valid", "mpm_set_timing",
            "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state",
-           "mpm_diff_forward", "mpm_diff_backward"]
+           "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune"]
 
 _lib = None
 
@@ -342,3 +342,65 @@ def radix_sort_u32(keys: np.ndarray, bits: int = 32):
     if rc != MPM_OK:
         raise MPMError(rc, "mpm_radix_sort_u32")
     return out, perm
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [("grid", GridDesc), ("model", ctypes.c_int), ("gravity", ctypes.c_double * 3),
+                ("particle_count", ctypes.c_int64), ("first_object", ctypes.c_int), ("object_count", ctypes.c_int)]
+
+
+class MPM_BATCH(MPM_DRIVER):
+    """Many independent 3D scenes advanced together (mpm_batch_create): every phase
+    of the substep is one persistent launch over all scenes.  FP32 fast path."""
+
+    def __init__(self, scenes_list):
+        self.L = load_library()
+        L = self.L
+        L.mpm_batch_create.argtypes = [ctypes.POINTER(SceneDesc), ctypes.c_int, ctypes.POINTER(CollisionObject),
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.mpm_batch_create.restype = ctypes.c_int
+        L.mpm_autotune.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        L.mpm_autotune.restype = ctypes.c_int
+        self.scenes = list(scenes_list)
+        self.scene = self.scenes[0]
+        self.dim = 3
+        self.precision, self.path = FP32, PATH_FAST
+        descs = (SceneDesc * len(self.scenes))()
+        objs = []
+        for i, s in enumerate(self.scenes):
+            if s.dim != 3:
+                raise ValueError("batched scenes are 3D")
+            d = descs[i]
+            d.grid.dim, d.grid.ghost = 3, S.GHOST
+            for a in range(3):
+                d.grid.counts[a] = s.counts[a]
+                d.grid.domain_min[a], d.grid.domain_max[a] = s.domain_min[a], s.domain_max[a]
+                d.gravity[a] = s.gravity[a]
+            d.model = s.model
+            d.particle_count = s.n
+            d.first_object, d.object_count = len(objs), len(s.objects)
+            objs += list(s.objects)
+        arr = (CollisionObject * max(len(objs), 1))()
+        for i, o in enumerate(objs):
+            arr[i].kind, arr[i].type, arr[i].friction = o.kind, o.type, o.friction
+            for a in range(3):
+                arr[i].a[a], arr[i].b[a] = o.a[a], o.b[a]
+        self.h = ctypes.c_void_p()
+        self._check(L.mpm_batch_create(descs, len(self.scenes), arr, len(objs), ctypes.byref(self.h)), "mpm_batch_create")
+        self.time = 0.0
+        self.n = 0
+        self.offsets = np.cumsum([0] + [s.n for s in self.scenes])
+
+    def set_scene_particles(self, scene=None, dtype=np.float64):
+        cat = lambda name: np.concatenate([getattr(s, name) for s in self.scenes])
+        self.set_particles(cat("X"), cat("V"), cat("F"), cat("B"), cat("mass"), cat("volume"), cat("mu"), cat("lam"),
+                           dtype=dtype)
+
+    def split(self, arrays):
+        return [{k: v[self.offsets[i]:self.offsets[i + 1]] for k, v in arrays.items()} for i in range(len(self.scenes))]
+
+    def autotune(self, substeps=3, dt=None):
+        dt = self.scene.dt if dt is None else dt
+        buf = ctypes.create_string_buffer(4096)
+        self._check(self.L.mpm_autotune(self.h, dt, substeps, buf, 4096), "mpm_autotune")
+        return buf.value.decode()
