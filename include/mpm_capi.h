@@ -181,6 +181,32 @@ int mpm_get_grid(mpm_handle* h, double* mass, double* v0, double* v, double* vfr
 /* Number of valid particles (MPM_EXAMPLE::simulated_particles.m). */
 int mpm_count_valid(mpm_handle* h, int64_t* count);
 
+/* Conservation and CFL diagnostics, reduced on the GPU in FP64. */
+typedef struct {
+    double mass;
+    double momentum[3];
+    double angular_momentum[3];   /* 2D: the one component is [0] */
+    double kinetic_energy;
+    double max_speed;             /* particles only */
+    double max_affine_speed;      /* particles only: |V| + |B|_F 6 sqrt(d) / dx */
+    int64_t count;                /* valid particles / grid nodes with mass */
+} mpm_totals;
+
+/* Over the valid particles: MPM_EXAMPLE::Total_Particle_Linear_Momentum,
+ * Total_Particle_Angular_Momentum (incl. the APIC B term) and
+ * Total_Particle_Kinetic_Energy (MPM_EXAMPLE.cpp:209-327), with
+ * MPM_DRIVER::Max_Particle_Speed and Grid_V_Upper_Bound (MPM_DRIVER.cpp:1112-1138). */
+int mpm_particle_totals(mpm_handle* h, mpm_totals* out);
+
+/* Over the grid of the last substep, velocity after the forces:
+ * Total_Grid_Linear_Momentum / Angular_Momentum / Kinetic_Energy. */
+int mpm_grid_totals(mpm_handle* h, mpm_totals* out);
+
+/* MPM_DRIVER::Compute_Dt (MPM_DRIVER.cpp:1098-1105) with the affine CFL bound
+ * (use_affine_cfl): cfl * dx_min / v, or max_dt when v is below
+ * cfl * dx_min / max_dt. */
+int mpm_compute_dt(mpm_handle* h, double cfl, double max_dt, double* dt);
+
 /* Per-kernel device time: enable (1) / disable (0) CUDA-event timing, then read
  * totals.  names gets a comma-separated list, ms and launches one entry each. */
 int mpm_set_timing(mpm_handle* h, int enable);

@@ -173,8 +173,12 @@ def ref_available() -> bool:
     return os.path.exists(REF_SCENE)
 
 
-def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timing: bool = False):
-    """Run the reference's own driver on ``scene``; return {step: dump} (and timing JSON if asked)."""
+def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timing: bool = False, totals=None):
+    """Run the reference's own driver on ``scene``; return {step: dump} (and timing JSON if asked).
+
+    ``totals=(cfl, max_dt)`` returns instead ``(dumps, diagnostics)``: the
+    reference's Total_Particle_* momenta and energy, Max_Particle_Speed,
+    Grid_V_Upper_Bound and Compute_Dt on the final state."""
     from physbam_b200 import scenes as S
     tmp = tempfile.mkdtemp(prefix="mpmref_")
     try:
@@ -185,11 +189,53 @@ def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timin
             cmd.append("-float")
         if timing:
             cmd.append("-time")
+        if totals is not None:
+            cmd += ["-totals", repr(float(totals[0])), repr(float(totals[1]))]
         out = subprocess.run(cmd, check=True, capture_output=True, text=True)
         res = S.read_dump(dp, scene.dim, scene.n, scene.counts) if dumps else {}
+        if totals is not None:
+            import json
+            lines = [ln for ln in out.stdout.splitlines() if ln.startswith('{"mass"')]
+            return res, json.loads(lines[-1])
         if timing:
             import json
             return res, json.loads(out.stdout.strip().splitlines()[-1])
         return res
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+def particle_totals(X, V, B, mass, valid, dx):
+    """FP64 particle diagnostics in the reference's form.
+
+    MPM_EXAMPLE::Total_Particle_Linear_Momentum / Angular_Momentum /
+    Kinetic_Energy (Hybrid_Methods/Examples_And_Drivers/MPM_EXAMPLE.cpp:209-327)
+    and MPM_DRIVER::Max_Particle_Speed / Grid_V_Upper_Bound
+    (Hybrid_Methods/Examples_And_Drivers/MPM_DRIVER.cpp:1107-1138).  ``B`` is
+    (n, d, d) with B[p, r, c]; ``dx`` the cell size per axis.
+    """
+    ok = np.asarray(valid, bool)
+    X, V, B, m = (np.asarray(a, np.float64)[ok] for a in (X, V, B, mass))
+    d = X.shape[1]
+    dx = np.broadcast_to(np.asarray(dx, np.float64), (d,))
+    if d == 3:
+        eps = np.stack([B[:, 1, 2] - B[:, 2, 1], B[:, 2, 0] - B[:, 0, 2], B[:, 0, 1] - B[:, 1, 0]], 1)
+        L = (m[:, None] * (np.cross(X, V) - eps)).sum(0)
+    else:
+        L = np.array([(m * (X[:, 0] * V[:, 1] - X[:, 1] * V[:, 0] - (B[:, 0, 1] - B[:, 1, 0]))).sum(), 0.0, 0.0])
+    Dp_inv = 4.0 / dx ** 2                       # quadratic B-spline Dp^-1, one entry per axis
+    ke = 0.5 * (m * (V ** 2).sum(1)).sum() + 0.5 * (m * (B ** 2 * Dp_inv[None, None, :]).sum((1, 2))).sum()
+    speed = np.sqrt((V ** 2).sum(1))
+    xi = 6.0 * np.sqrt(d) / dx.max()
+    affine = speed + np.sqrt((B ** 2).sum((1, 2))) * xi
+    mom = np.zeros(3)
+    mom[:d] = (m[:, None] * V).sum(0)
+    return {"mass": m.sum(), "momentum": mom, "angular_momentum": L, "kinetic_energy": ke,
+            "max_speed": speed.max(initial=0.0), "max_affine_speed": affine.max(initial=0.0), "count": int(ok.sum())}
+
+
+def compute_dt(max_affine_speed, dx_min, cfl, max_dt):
+    """MPM_DRIVER::Compute_Dt (Hybrid_Methods/Examples_And_Drivers/MPM_DRIVER.cpp:1098-1105)."""
+    critical = cfl * dx_min / max_dt
+    v = max_affine_speed
+    return cfl * dx_min / v if v > critical else max_dt

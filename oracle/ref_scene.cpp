@@ -4,7 +4,7 @@
 // restatement in oracle/ and produces the golden fixtures); the product never
 // links or runs it.  Built by oracle/ref.mk against the reference's sources.
 //
-//   ref_scene <scene.bin> <dump.bin> [-threads T] [-float] [-time]
+//   ref_scene <scene.bin> <dump.bin> [-threads T] [-float] [-time] [-totals CFL MAX_DT]
 //
 // The scene is set up through the reference's public API exactly as
 // Projects/mpm/STANDARD_TESTS_BASE.cpp does it: quadratic weights
@@ -158,7 +158,10 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
 
 template<class T> void wr(FILE* f, const T* p, size_t n) { fwrite(p, sizeof(T), n, f); }
 
-template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threads, bool report_time)
+struct TOTALS_REQUEST { bool on = false; double cfl = 1, max_dt = 1; };
+
+template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threads, bool report_time,
+    const TOTALS_REQUEST& totals)
 {
     typedef typename TV::SCALAR T;
     typedef VECTOR<int, TV::m> TV_INT;
@@ -228,6 +231,22 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
         wr(f, gvf.data(), gvf.size());
     }
     fclose(f);
+    if(totals.on) {
+        // the reference's own diagnostics on the final particle state
+        auto lin = example.Total_Particle_Linear_Momentum();
+        auto ang = example.Total_Particle_Angular_Momentum();
+        double mass = 0;
+        for(int k = 0; k < example.simulated_particles.m; k++) mass += example.particles.mass(example.simulated_particles(k));
+        example.cfl = (T)totals.cfl;
+        example.max_dt = (T)totals.max_dt;
+        printf("{\"mass\": %.17g, \"count\": %d, \"momentum\": [", mass, example.simulated_particles.m);
+        for(int a = 0; a < d; a++) printf("%s%.17g", a ? ", " : "", (double)lin(a));
+        printf("], \"angular_momentum\": [");
+        for(int a = 0; a < ang.m; a++) printf("%s%.17g", a ? ", " : "", (double)ang(a));
+        printf("], \"kinetic_energy\": %.17g, \"max_speed\": %.17g, \"max_affine_speed\": %.17g, \"dt\": %.17g}\n",
+            (double)example.Total_Particle_Kinetic_Energy(), (double)driver.Max_Particle_Speed(),
+            (double)driver.Grid_V_Upper_Bound(), (double)driver.Compute_Dt());
+    }
     if(report_time) {
         printf("{\"substeps\": %d, \"particles\": %lld, \"seconds\": %.9g, \"threads\": %d, \"step_seconds\": [",
             s.nsteps, s.n, total, threads);
@@ -242,13 +261,19 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
 
 int main(int argc, char* argv[])
 {
-    if(argc < 3) { fprintf(stderr, "usage: ref_scene scene.bin dump.bin [-threads T] [-float] [-time]\n"); return 2; }
+    if(argc < 3) { fprintf(stderr, "usage: ref_scene scene.bin dump.bin [-threads T] [-float] [-time] [-totals CFL MAX_DT]\n"); return 2; }
     int threads = 1;
     bool use_float = false, report_time = false;
+    TOTALS_REQUEST totals;
     for(int i = 3; i < argc; i++) {
         if(!strcmp(argv[i], "-threads") && i + 1 < argc) threads = atoi(argv[++i]);
         else if(!strcmp(argv[i], "-float")) use_float = true;
         else if(!strcmp(argv[i], "-time")) report_time = true;
+        else if(!strcmp(argv[i], "-totals") && i + 2 < argc) {
+            totals.on = true;
+            totals.cfl = atof(argv[++i]);
+            totals.max_dt = atof(argv[++i]);
+        }
     }
 #ifdef USE_OPENMP
     omp_set_num_threads(threads);
@@ -256,8 +281,8 @@ int main(int argc, char* argv[])
     LOG::Initialize_Logging(true, true, 0, false);
     SCENE_FILE s = Read_Scene(argv[1]);
     int rc;
-    if(use_float) rc = s.dim == 2 ? Run<VECTOR<float, 2> >(s, argv[2], threads, report_time) : Run<VECTOR<float, 3> >(s, argv[2], threads, report_time);
-    else rc = s.dim == 2 ? Run<VECTOR<double, 2> >(s, argv[2], threads, report_time) : Run<VECTOR<double, 3> >(s, argv[2], threads, report_time);
+    if(use_float) rc = s.dim == 2 ? Run<VECTOR<float, 2> >(s, argv[2], threads, report_time, totals) : Run<VECTOR<float, 3> >(s, argv[2], threads, report_time, totals);
+    else rc = s.dim == 2 ? Run<VECTOR<double, 2> >(s, argv[2], threads, report_time, totals) : Run<VECTOR<double, 3> >(s, argv[2], threads, report_time, totals);
     LOG::Finish_Logging();
     return rc;
 }

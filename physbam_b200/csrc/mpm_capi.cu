@@ -2,6 +2,7 @@
 // boundary; every entry point returns an mpm_status.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -405,6 +406,38 @@ int mpm_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_ke
     if(!fast(h)) return set_error(h, MPM_ERR_ARG, "sort state exists on the fast path only");
     if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
     return fast_debug_sort_state(h, slot_keys, sorted_keys, perm);
+}
+
+int mpm_particle_totals(mpm_handle* h, mpm_totals* out)
+{
+    if(!h || !out) return MPM_ERR_ARG;
+    memset(out, 0, sizeof(*out));
+    if(!h->have_particles) return MPM_OK;
+    return fast(h) ? fast_particle_totals(h, out) : plain_particle_totals(h, out);
+}
+
+int mpm_grid_totals(mpm_handle* h, mpm_totals* out)
+{
+    if(!h || !out) return MPM_ERR_ARG;
+    memset(out, 0, sizeof(*out));
+    if(!h->have_particles) return MPM_OK;
+    return fast(h) ? fast_grid_totals(h, out) : plain_grid_totals(h, out);
+}
+
+int mpm_compute_dt(mpm_handle* h, double cfl, double max_dt, double* dt)
+{
+    if(!h || !dt || !(cfl > 0) || !(max_dt > 0)) return MPM_ERR_ARG;
+    mpm_totals t;
+    int rc = mpm_particle_totals(h, &t);
+    if(rc) return rc;
+    double dx_min = h->sp.dx[0];
+    for(int k = 1; k < h->sp.dim; k++) dx_min = std::min(dx_min, h->sp.dx[k]);
+    if(fast(h) && h->fast.batch)   // smallest cell of any scene
+        for(const SceneDev& s: h->fast.scenes_h)
+            for(int k = 0; k < 3; k++) dx_min = std::min(dx_min, (double)s.dx[k]);
+    double critical = cfl * dx_min / max_dt, v = t.max_affine_speed;
+    *dt = v > critical ? cfl * dx_min / v : max_dt;
+    return MPM_OK;
 }
 
 int mpm_set_timing(mpm_handle* h, int enable)

@@ -1313,3 +1313,144 @@ extern "C" int mpm_radix_sort_u32_noalloc(const uint32_t* keys, int64_t n, int b
     if(cudaStreamSynchronize(st) != cudaSuccess) return MPM_ERR_CUDA;
     return (f & MPM_FLAG_TIMEOUT) ? MPM_ERR_TIMEOUT : MPM_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Diagnostics in FP64 (MPM_EXAMPLE::Total_Particle_* / Total_Grid_*,
+// MPM_EXAMPLE.cpp:209-327; MPM_DRIVER::Max_Particle_Speed / Grid_V_Upper_Bound,
+// MPM_DRIVER.cpp:1112-1138).  acc: mass, momentum[3], angular[3], kinetic,
+// count; mx: max speed, max affine speed (as ordered bits of non-negative doubles).
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ void warp_add(double* acc, double v)
+{
+#pragma unroll
+    for(int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if((threadIdx.x & 31) == 0 && v != 0) atomicAdd(acc, v);
+}
+__device__ __forceinline__ void warp_max(unsigned long long* mx, double v)
+{
+#pragma unroll
+    for(int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if((threadIdx.x & 31) == 0) atomicMax(mx, (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void k_particle_totals(FastArgs a, double* acc, unsigned long long* mx)
+{
+    double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, vmax = 0, amax = 0;
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t key = a.keys_next[i];
+        if(key == SENTINEL) continue;
+        const SceneDev& sc = a.scenes[a.block_scene[key >> 6]];
+        double X[3], V[3], B[9];
+        for(int k = 0; k < 3; k++) { X[k] = a.src[(C_X + k) * a.npad + i]; V[k] = a.src[(C_V + k) * a.npad + i]; }
+        for(int k = 0; k < 9; k++) B[k] = a.src[(C_B + k) * a.npad + i];
+        double m = a.src_attr[i].x;
+        s[0] += m;
+        for(int k = 0; k < 3; k++) s[1 + k] += m * V[k];
+        // m X x V - m B:epsilon  (Contract_Permutation_Tensor = (B12-B21, B20-B02, B01-B10))
+        s[4] += m * (X[1] * V[2] - X[2] * V[1]) - m * (B[7] - B[5]);
+        s[5] += m * (X[2] * V[0] - X[0] * V[2]) - m * (B[2] - B[6]);
+        s[6] += m * (X[0] * V[1] - X[1] * V[0]) - m * (B[3] - B[1]);
+        double v2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2], bd = 0, bf = 0;
+        for(int c = 0; c < 3; c++)
+            for(int r = 0; r < 3; r++) {
+                double b2 = B[r + 3 * c] * B[r + 3 * c];
+                bd += b2 * 4.0 * (double)sc.inv[c] * (double)sc.inv[c];
+                bf += b2;
+            }
+        s[7] += 0.5 * m * v2 + 0.5 * m * bd;
+        s[8] += 1;
+        double inv_min = fmin((double)sc.inv[0], fmin((double)sc.inv[1], (double)sc.inv[2]));
+        double sp = sqrt(v2);
+        vmax = fmax(vmax, sp);
+        amax = fmax(amax, sp + sqrt(bf) * 6.0 * sqrt(3.0) * inv_min);
+    }
+    for(int k = 0; k < 9; k++) warp_add(acc + k, s[k]);
+    warp_max(mx, vmax);
+    warp_max(mx + 1, amax);
+}
+
+// one node block per CTA of 64 threads, over the node blocks of the last substep
+__global__ void k_grid_totals(FastArgs a, uint32_t count, double* acc)
+{
+    double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for(uint32_t w = blockIdx.x; w < count; w += gridDim.x) {
+        const uint32_t nb = a.nb_list[w];
+        const SceneDev& sc = a.scenes[a.nb_scene[nb]];
+        const uint32_t lnb = nb - sc.nb_base;
+        int nz = lnb % sc.NN[2], r = lnb / sc.NN[2], ny = r % sc.NN[1], nx = r / sc.NN[1];
+        int t = threadIdx.x;
+        int qx = 4 * nx + (t >> 4), qy = 4 * ny + ((t >> 2) & 3), qz = 4 * nz + (t & 3);
+        int64_t q = node_index(sc, qx, qy, qz);
+        float4 p0 = a.vel[2 * q], p1 = a.vel[2 * q + 1];
+        double m = p1.z;
+        if(m == 0) continue;
+        double v[3] = {p0.x, p0.y, p0.z};
+        double X[3] = {sc.dmin[0] + ((double)(qx - MPM_GHOST) + 0.5) * sc.dx[0], sc.dmin[1] + ((double)(qy - MPM_GHOST) + 0.5) * sc.dx[1],
+                       sc.dmin[2] + ((double)(qz - MPM_GHOST) + 0.5) * sc.dx[2]};
+        s[0] += m;
+        for(int k = 0; k < 3; k++) s[1 + k] += m * v[k];
+        s[4] += m * (X[1] * v[2] - X[2] * v[1]);
+        s[5] += m * (X[2] * v[0] - X[0] * v[2]);
+        s[6] += m * (X[0] * v[1] - X[1] * v[0]);
+        s[7] += 0.5 * m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        s[8] += 1;
+    }
+    for(int k = 0; k < 9; k++) warp_add(acc + k, s[k]);
+}
+}  // namespace
+
+static int totals_out(mpm_handle* h, double* dacc, unsigned long long* dmx, mpm_totals* out)
+{
+    double acc[9];
+    unsigned long long mx[2] = {0, 0};
+    MPM_CUDA(h, cudaMemcpyAsync(acc, dacc, sizeof acc, cudaMemcpyDeviceToHost, h->stream));
+    if(dmx) MPM_CUDA(h, cudaMemcpyAsync(mx, dmx, sizeof mx, cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    out->mass = acc[0];
+    for(int k = 0; k < 3; k++) { out->momentum[k] = acc[1 + k]; out->angular_momentum[k] = acc[4 + k]; }
+    out->kinetic_energy = acc[7];
+    out->count = (int64_t)acc[8];
+    double v0, v1;
+    memcpy(&v0, &mx[0], 8);
+    memcpy(&v1, &mx[1], 8);
+    out->max_speed = v0;
+    out->max_affine_speed = v1;
+    return MPM_OK;
+}
+
+int fast_particle_totals(mpm_handle* h, mpm_totals* out)
+{
+    FastState& f = h->fast;
+    double* d = nullptr;
+    MPM_CUDA(h, cudaMallocAsync((void**)&d, 16 * sizeof(double), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(d, 0, 16 * sizeof(double), h->stream));
+    if(f.n) {
+        FastArgs a = make_args(h, 0.0);
+        k_particle_totals<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(a, d, (unsigned long long*)(d + 12));
+        MPM_LAUNCHED(h, "k_particle_totals");
+    }
+    int rc = totals_out(h, d, (unsigned long long*)(d + 12), out);
+    cudaFreeAsync(d, h->stream);
+    return rc;
+}
+
+int fast_grid_totals(mpm_handle* h, mpm_totals* out)
+{
+    FastState& f = h->fast;
+    uint32_t count = 0;
+    MPM_CUDA(h, cudaMemcpyAsync(&count, f.counters + CNT_NODE_BLOCKS, sizeof(count), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    double* d = nullptr;
+    MPM_CUDA(h, cudaMallocAsync((void**)&d, 16 * sizeof(double), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(d, 0, 16 * sizeof(double), h->stream));
+    if(count) {
+        FastArgs a = make_args(h, 0.0);
+        k_grid_totals<<<count < 65535u ? count : 65535u, 64, 0, h->stream>>>(a, count, d);
+        MPM_LAUNCHED(h, "k_grid_totals");
+    }
+    int rc = totals_out(h, d, nullptr, out);
+    out->max_speed = out->max_affine_speed = 0;
+    cudaFreeAsync(d, h->stream);
+    return rc;
+}

@@ -554,3 +554,128 @@ int plain_count_valid(mpm_handle* h, int64_t* c)
     *c = (int64_t)r;
     return MPM_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Diagnostics in FP64 (MPM_EXAMPLE::Total_Particle_* / Total_Grid_*,
+// MPM_EXAMPLE.cpp:209-327; MPM_DRIVER::Max_Particle_Speed / Grid_V_Upper_Bound,
+// MPM_DRIVER.cpp:1112-1138).  2D angular momentum goes to component 0.
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ void pwarp_add(double* acc, double v)
+{
+#pragma unroll
+    for(int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if((threadIdx.x & 31) == 0 && v != 0) atomicAdd(acc, v);
+}
+__device__ __forceinline__ void pwarp_max(unsigned long long* mx, double v)
+{
+#pragma unroll
+    for(int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if((threadIdx.x & 31) == 0) atomicMax(mx, (unsigned long long)__double_as_longlong(v));
+}
+
+template<class T> __global__ void k_plain_particle_totals(PlainArgs<T> a, double* acc, unsigned long long* mx)
+{
+    const int d = a.sp.dim;
+    double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, vmax = 0, amax = 0;
+    double inv_min = a.sp.inv_dx[0];
+    for(int k = 1; k < d; k++) inv_min = fmin(inv_min, a.sp.inv_dx[k]);
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+        if(!a.valid[p]) continue;
+        double X[3] = {0, 0, 0}, V[3] = {0, 0, 0}, B[9];
+        for(int k = 0; k < d; k++) { X[k] = a.X[p * d + k]; V[k] = a.V[p * d + k]; }
+        for(int k = 0; k < d * d; k++) B[k] = a.B[p * d * d + k];
+        double m = a.mass[p];
+        s[0] += m;
+        for(int k = 0; k < d; k++) s[1 + k] += m * V[k];
+        if(d == 3) {
+            s[4] += m * (X[1] * V[2] - X[2] * V[1]) - m * (B[7] - B[5]);
+            s[5] += m * (X[2] * V[0] - X[0] * V[2]) - m * (B[2] - B[6]);
+            s[6] += m * (X[0] * V[1] - X[1] * V[0]) - m * (B[3] - B[1]);
+        } else {
+            s[4] += m * (X[0] * V[1] - X[1] * V[0]) - m * (B[2] - B[1]);
+        }
+        double v2 = 0, bd = 0, bf = 0;
+        for(int k = 0; k < d; k++) v2 += V[k] * V[k];
+        for(int c = 0; c < d; c++)
+            for(int r = 0; r < d; r++) {
+                double b2 = B[r + d * c] * B[r + d * c];
+                bd += b2 * 4.0 * a.sp.inv_dx[c] * a.sp.inv_dx[c];
+                bf += b2;
+            }
+        s[7] += 0.5 * m * v2 + 0.5 * m * bd;
+        s[8] += 1;
+        double sp = sqrt(v2);
+        vmax = fmax(vmax, sp);
+        amax = fmax(amax, sp + sqrt(bf) * 6.0 * sqrt((double)d) * inv_min);
+    }
+    for(int k = 0; k < 9; k++) pwarp_add(acc + k, s[k]);
+    pwarp_max(mx, vmax);
+    pwarp_max(mx + 1, amax);
+}
+
+template<class T> __global__ void k_plain_grid_totals(PlainArgs<T> a, double* acc)
+{
+    const int d = a.sp.dim;
+    double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.gn; i += (int64_t)gridDim.x * blockDim.x) {
+        double m = a.gm[i];
+        if(m == 0) continue;
+        int64_t r = i;
+        int idx[3] = {0, 0, 0};
+        for(int k = d - 1; k >= 0; k--) { idx[k] = (int)(r % a.gs[k]) - MPM_GHOST; r /= a.gs[k]; }
+        double X[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+        for(int k = 0; k < d; k++) {
+            X[k] = a.sp.dmin[k] + ((double)idx[k] + 0.5) * a.sp.dx[k];
+            v[k] = a.gv[i * d + k];
+        }
+        s[0] += m;
+        for(int k = 0; k < d; k++) s[1 + k] += m * v[k];
+        if(d == 3) {
+            s[4] += m * (X[1] * v[2] - X[2] * v[1]);
+            s[5] += m * (X[2] * v[0] - X[0] * v[2]);
+            s[6] += m * (X[0] * v[1] - X[1] * v[0]);
+        } else {
+            s[4] += m * (X[0] * v[1] - X[1] * v[0]);
+        }
+        s[7] += 0.5 * m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        s[8] += 1;
+    }
+    for(int k = 0; k < 9; k++) pwarp_add(acc + k, s[k]);
+}
+}  // namespace
+
+static int plain_totals(mpm_handle* h, bool grid, mpm_totals* out)
+{
+    double* d = nullptr;
+    MPM_CUDA(h, cudaMallocAsync((void**)&d, 16 * sizeof(double), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(d, 0, 16 * sizeof(double), h->stream));
+    const int t = 256;
+    if(h->model.precision == MPM_FP64) {
+        PlainArgs<double> a = args<double>(h, 0.0);
+        if(grid) k_plain_grid_totals<double><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a, d);
+        else if(a.n) k_plain_particle_totals<double><<<gblocks(h, a.n, t), t, 0, h->stream>>>(a, d, (unsigned long long*)(d + 12));
+    } else {
+        PlainArgs<float> a = args<float>(h, 0.0);
+        if(grid) k_plain_grid_totals<float><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a, d);
+        else if(a.n) k_plain_particle_totals<float><<<gblocks(h, a.n, t), t, 0, h->stream>>>(a, d, (unsigned long long*)(d + 12));
+    }
+    MPM_LAUNCHED(h, "k_plain_totals");
+    double acc[9];
+    unsigned long long mx[2];
+    MPM_CUDA(h, cudaMemcpyAsync(acc, d, sizeof acc, cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(mx, d + 12, sizeof mx, cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    cudaFreeAsync(d, h->stream);
+    out->mass = acc[0];
+    for(int k = 0; k < 3; k++) { out->momentum[k] = acc[1 + k]; out->angular_momentum[k] = acc[4 + k]; }
+    out->kinetic_energy = acc[7];
+    out->count = (int64_t)acc[8];
+    memcpy(&out->max_speed, &mx[0], 8);
+    memcpy(&out->max_affine_speed, &mx[1], 8);
+    if(grid) out->max_speed = out->max_affine_speed = 0;
+    return MPM_OK;
+}
+
+int plain_particle_totals(mpm_handle* h, mpm_totals* out) { return plain_totals(h, false, out); }
+int plain_grid_totals(mpm_handle* h, mpm_totals* out) { return plain_totals(h, true, out); }

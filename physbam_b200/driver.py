@@ -50,6 +50,17 @@ class CollisionObject(ctypes.Structure):
                 ("a", ctypes.c_double * 3), ("b", ctypes.c_double * 3)]
 
 
+class Totals(ctypes.Structure):
+    _fields_ = [("mass", ctypes.c_double), ("momentum", ctypes.c_double * 3), ("angular_momentum", ctypes.c_double * 3),
+                ("kinetic_energy", ctypes.c_double), ("max_speed", ctypes.c_double),
+                ("max_affine_speed", ctypes.c_double), ("count", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {"mass": self.mass, "momentum": np.array(self.momentum[:]),
+                "angular_momentum": np.array(self.angular_momentum[:]), "kinetic_energy": self.kinetic_energy,
+                "max_speed": self.max_speed, "max_affine_speed": self.max_affine_speed, "count": self.count}
+
+
 class ParticlesView(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("dtype", ctypes.c_int), ("on_device", ctypes.c_int),
                 ("X", ctypes.c_void_p), ("V", ctypes.c_void_p), ("F", ctypes.c_void_p), ("B", ctypes.c_void_p),
@@ -61,7 +72,8 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_get_particles", "mpm_substep", "mpm_advance", "mpm_particle_to_grid", "mpm_apply_forces",
            "mpm_grid_to_particle", "mpm_synchronize", "mpm_get_grid", "mpm_count_valid", "mpm_set_timing",
            "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state",
-           "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune"]
+           "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune", "mpm_particle_totals",
+           "mpm_grid_totals", "mpm_compute_dt"]
 
 _lib = None
 
@@ -94,6 +106,9 @@ def load_library(path: str = LIB_PATH):
     L.mpm_diff_forward.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_int]
     L.mpm_diff_backward.argtypes = [P, ctypes.POINTER(ParticlesView), ctypes.POINTER(ParticlesView), P, P]
     L.mpm_radix_sort_u32.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P]
+    L.mpm_particle_totals.argtypes = [P, ctypes.POINTER(Totals)]
+    L.mpm_grid_totals.argtypes = [P, ctypes.POINTER(Totals)]
+    L.mpm_compute_dt.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
     L.mpm_debug_sort_state.argtypes = [P, P, P, P]
     L.mpm_status_string.argtypes = [ctypes.c_int]
     L.mpm_status_string.restype = ctypes.c_char_p
@@ -311,6 +326,22 @@ class MPM_DRIVER:
         keys, sk, perm = (np.empty(n, np.uint32) for _ in range(3))
         self._check(self.L.mpm_debug_sort_state(self.h, _ptr(keys), _ptr(sk), _ptr(perm)), "mpm_debug_sort_state")
         return keys, sk, perm
+
+    def particle_totals(self):
+        t = Totals()
+        self._check(self.L.mpm_particle_totals(self.h, ctypes.byref(t)), "mpm_particle_totals")
+        return t.as_dict()
+
+    def grid_totals(self):
+        t = Totals()
+        self._check(self.L.mpm_grid_totals(self.h, ctypes.byref(t)), "mpm_grid_totals")
+        return t.as_dict()
+
+    def compute_dt(self, cfl=1.0, max_dt=None):
+        out = ctypes.c_double()
+        max_dt = self.scene.dt if max_dt is None else max_dt
+        self._check(self.L.mpm_compute_dt(self.h, cfl, max_dt, ctypes.byref(out)), "mpm_compute_dt")
+        return out.value
 
     def count_valid(self) -> int:
         c = ctypes.c_int64()

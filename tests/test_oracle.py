@@ -9,6 +9,7 @@ import pytest
 
 import oracle
 from make_golden import CASES, load
+from physbam_b200 import scenes as S
 
 # The restatement follows the reference's operation order, so it agrees to a
 # few ulps per step; B carries a cancellation (sum w vf Z - Vpf X) that
@@ -100,3 +101,27 @@ def test_pft_matches_closed_forms():
         got_n = oracle.pft(3, 1, Fc, mu, la).reshape(3, 3).T
         np.testing.assert_allclose(got_c, coro, rtol=1e-9, atol=1e-9 * np.abs(coro).max())
         np.testing.assert_allclose(got_n, nh, rtol=1e-9, atol=1e-9 * np.abs(nh).max())
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference runner not built (no reference sources)")
+@pytest.mark.parametrize("dim", [2, 3])
+def test_totals_match_reference(dim):
+    """oracle.particle_totals / compute_dt against the reference's own
+    Total_Particle_*, Grid_V_Upper_Bound and Compute_Dt on the same final state."""
+    scene = S.small_3d(nsteps=4) if dim == 3 else S.small_2d(nsteps=4)
+    # a CFL small enough that the affine speed bound decides the step
+    cfl, max_dt = 1e-3, 1e-2
+    dumps, ref = oracle.run_reference(scene, [scene.nsteps - 1], threads=2, totals=(cfl, max_dt))
+    last = dumps[scene.nsteps - 1]
+    got = oracle.particle_totals(last["X"], last["V"], last["B"], scene.mass, last["valid"], scene.dx)
+    assert got["count"] == ref["count"]
+    assert got["mass"] == pytest.approx(ref["mass"], rel=1e-13)
+    np.testing.assert_allclose(got["momentum"][:dim], ref["momentum"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(got["angular_momentum"][:len(ref["angular_momentum"])], ref["angular_momentum"],
+                               rtol=1e-12, atol=1e-14)
+    assert got["kinetic_energy"] == pytest.approx(ref["kinetic_energy"], rel=1e-12)
+    assert got["max_speed"] == pytest.approx(ref["max_speed"], rel=1e-13)
+    assert got["max_affine_speed"] == pytest.approx(ref["max_affine_speed"], rel=1e-13)
+    dt = oracle.compute_dt(got["max_affine_speed"], scene.dx, cfl, max_dt)
+    assert dt < max_dt
+    assert dt == pytest.approx(ref["dt"], rel=1e-13)
