@@ -100,10 +100,8 @@ class ClockSampler:
 
 
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from physbam_b200 import replicas
+    return replicas.rank_env()
 
 
 def reference_arm(args):
@@ -246,11 +244,8 @@ def our_arm(args):
     import torch
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from physbam_b200 import replicas
+    dist = replicas.init("nccl", timeout_s=120)
     from physbam_b200 import driver as D
     from physbam_b200 import scenes as S
 
@@ -263,14 +258,13 @@ def our_arm(args):
     stream = torch.cuda.Stream()
     drv.set_stream(stream.cuda_stream)
     drv.set_scene_particles(scene)
+    tuned = drv.autotune(substeps=3)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     ms, ktimes, clocks = measure_substeps(drv, stream, flush, args.steps, args.warmup, dist, local)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    ms_max = replicas.max_over_ranks(ms, dist, "cuda")
     if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    ms_max = float(t.item())
     value = world * n * args.steps / (ms_max / 1e3)
     drv.close()
 
@@ -298,10 +292,7 @@ def our_arm(args):
         e2e_drv.advance(frame)
         out = e2e_drv.get_particles(dtype=np.float32)
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * frame * e2e_steps / float(te.item())
+    e2e_value = world * n * frame * e2e_steps / replicas.max_over_ranks(e2e_s, dist, "cuda")
     e2e_drv.close()
     assert out["valid"].sum() > 0
 
@@ -309,11 +300,13 @@ def our_arm(args):
     roof = roofline_of(ktimes, n, peak, peak_kind, WORKLOAD)
     total_k = sum(v[0] for v in ktimes.values())
 
-    large = batch = adjoint = None
+    large = batch = adjoint = plain = None
+    if world == 1 and not args.no_plain:
+        plain = measure_plain_fp64(args, D, S, stream, flush, substep_ms)
     if world == 1 and not args.no_large:
         large = measure_large(args, D, S, stream, flush, peak, peak_kind)
-    if world == 1 and not args.no_batch:
-        batch = measure_batch(args, D, S, stream, flush, peak)
+    if not args.no_batch:
+        batch = measure_batch(args, D, S, stream, flush, peak, dist)
     if world == 1 and not args.no_adjoint:
         adjoint = measure_adjoint(D, S)
 
@@ -330,12 +323,14 @@ def our_arm(args):
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "step": "upload + %d substeps (CUDA graph) + download, pinned host buffers" % frame},
             "gpu_launches": kernels_per_substep(scene) * args.steps,
+            "autotune": tuned,
             "roofline": roof,
             "substep_roofline": {"achieved": ALG_BYTES["substep"] * n / (substep_ms / 1e3) / 1e9, "peak": peak,
                                  "unit": "GB/s", "frac": ALG_BYTES["substep"] * n / (substep_ms / 1e3) / 1e9 / peak,
                                  "alg_bytes_per_particle": ALG_BYTES["substep"]},
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()},
             "kernel_share": {k: v[0] / total_k for k, v in ktimes.items()},
+            "plain_fp64": plain,
             "large_config": large,
             "batch_config": batch,
             "adjoint": adjoint,
@@ -349,25 +344,51 @@ def our_arm(args):
     return 0
 
 
-def measure_batch(args, D, S, stream, flush, peak):
-    """256 independent scenes (grid side from {32,48,64,96}, boxes of
-    seeded size, 4-8 ppc, both models) in one handle; launch shapes from the autotuner."""
-    import torch
-    scenes = S.batch_scenes(seed=1234, count=256)
-    n = sum(s.n for s in scenes)
+def measure_batch(args, D, S, stream, flush, peak, dist=None):
+    """256 independent scenes (grid side from {32,48,64,96}, boxes of seeded size,
+    4-8 ppc, both models) in one handle; launch shapes from the autotuner.  With
+    N ranks the scenes are split into N partitions of similar particle totals
+    (no collective on the data path); the whole job's rate is all particles over
+    the slowest rank's time."""
+    from physbam_b200 import replicas
+    world, rank, _ = replicas.rank_env()
+    every = S.batch_scenes(seed=1234, count=256)
+    mine = replicas.partition_scenes([s.n for s in every], world)[rank]
+    scenes = [every[i] for i in mine]
+    n_all = sum(s.n for s in every)
     drv = D.MPM_BATCH(scenes)
     drv.set_stream(stream.cuda_stream)
     drv.set_scene_particles(dtype=np.float32)
     report = drv.autotune(substeps=3)
     steps = max(5, min(args.steps, 20))
-    ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
+    ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3, dist)
     drv.close()
+    ms = replicas.max_over_ranks(ms, dist, "cuda")
     sub = ms / steps
-    return {"workload": "batch256-3d-grids{32,48,64,96}-fp32", "scenes": len(scenes), "particles": n,
+    n = n_all
+    return {"workload": "batch256-3d-grids{32,48,64,96}-fp32", "scenes": len(every), "particles": n,
+            "partition": "%d ranks, %d scenes on rank 0" % (world, len(mine)) if world > 1 else "single",
+            "scaling": "strong",
             "steps": steps, "ms_per_step": sub, "value": n * steps / (ms / 1e3), "unit": METRIC,
             "substep_roofline": {"achieved": ALG_BYTES["substep"] * n / (sub / 1e3) / 1e9, "peak": peak,
                                  "unit": "GB/s", "frac": ALG_BYTES["substep"] * n / (sub / 1e3) / 1e9 / peak},
             "autotune": report,
+            "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
+
+
+def measure_plain_fp64(args, D, S, stream, flush, fast_ms):
+    """The same workload on the plain FP64 path (reference layout, one thread per
+    particle, global atomics): the FP32 fast path's speed-up over it."""
+    scene = S.spheres_3d()
+    drv = D.MPM_DRIVER(scene, precision=D.FP64, path=D.PATH_PLAIN)
+    drv.set_stream(stream.cuda_stream)
+    drv.set_scene_particles(scene)
+    steps = max(5, min(args.steps, 20))
+    ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
+    drv.close()
+    sub = ms / steps
+    return {"workload": WORKLOAD.replace("fp32", "fp64-plain"), "steps": steps, "ms_per_step": sub,
+            "value": scene.n * steps / (ms / 1e3), "unit": METRIC, "fast_fp32_speedup": sub / fast_ms,
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
 
 
@@ -432,6 +453,7 @@ def measure_large(args, D, S, stream, flush, peak, peak_kind):
     drv.set_stream(stream.cuda_stream)
     drv.set_scene_particles(scene, dtype=np.float32)
     del scene.F, scene.B
+    tuned = drv.autotune(substeps=2)
     steps = max(5, min(args.steps, 20))
     ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
     drv.close()
@@ -442,6 +464,7 @@ def measure_large(args, D, S, stream, flush, peak, peak_kind):
             "substep_roofline": {"achieved": ALG_BYTES["substep"] * n / (sub / 1e3) / 1e9, "peak": peak,
                                  "unit": "GB/s", "frac": ALG_BYTES["substep"] * n / (sub / 1e3) / 1e9 / peak},
             "roofline": roofline_of(ktimes, n, peak, peak_kind, LARGE_WORKLOAD),
+            "autotune": tuned,
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()},
             "kernel_share": {k: v[0] / total_k for k, v in ktimes.items()}}
 
@@ -456,6 +479,7 @@ def main():
     ap.add_argument("--no-large", action="store_true", help="skip the 256^3 dam-break measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-scene batched measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward/backward timing")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 path on the same workload")
     ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d"], help="profiling run of one scene only")
     ap.add_argument("--grid", type=int, default=0, help="grid cells per side for --scene")
     args = ap.parse_args()

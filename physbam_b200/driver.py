@@ -106,6 +106,7 @@ def load_library(path: str = LIB_PATH):
     L.mpm_diff_forward.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_int]
     L.mpm_diff_backward.argtypes = [P, ctypes.POINTER(ParticlesView), ctypes.POINTER(ParticlesView), P, P]
     L.mpm_radix_sort_u32.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P]
+    L.mpm_autotune.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
     L.mpm_particle_totals.argtypes = [P, ctypes.POINTER(Totals)]
     L.mpm_grid_totals.argtypes = [P, ctypes.POINTER(Totals)]
     L.mpm_compute_dt.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
@@ -327,6 +328,14 @@ class MPM_DRIVER:
         self._check(self.L.mpm_debug_sort_state(self.h, _ptr(keys), _ptr(sk), _ptr(perm)), "mpm_debug_sort_state")
         return keys, sk, perm
 
+    def autotune(self, substeps=3, dt=None):
+        """Time every launch-shape choice of the fast path on the current state
+        (restored after each trial) and keep the fastest; returns the report."""
+        dt = self.scene.dt if dt is None else dt
+        buf = ctypes.create_string_buffer(4096)
+        self._check(self.L.mpm_autotune(self.h, dt, substeps, buf, 4096), "mpm_autotune")
+        return buf.value.decode()
+
     def particle_totals(self):
         t = Totals()
         self._check(self.L.mpm_particle_totals(self.h, ctypes.byref(t)), "mpm_particle_totals")
@@ -390,8 +399,6 @@ class MPM_BATCH(MPM_DRIVER):
         L.mpm_batch_create.argtypes = [ctypes.POINTER(SceneDesc), ctypes.c_int, ctypes.POINTER(CollisionObject),
                                        ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
         L.mpm_batch_create.restype = ctypes.c_int
-        L.mpm_autotune.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
-        L.mpm_autotune.restype = ctypes.c_int
         self.scenes = list(scenes_list)
         self.scene = self.scenes[0]
         self.dim = 3
@@ -430,8 +437,4 @@ class MPM_BATCH(MPM_DRIVER):
     def split(self, arrays):
         return [{k: v[self.offsets[i]:self.offsets[i + 1]] for k, v in arrays.items()} for i in range(len(self.scenes))]
 
-    def autotune(self, substeps=3, dt=None):
-        dt = self.scene.dt if dt is None else dt
-        buf = ctypes.create_string_buffer(4096)
-        self._check(self.L.mpm_autotune(self.h, dt, substeps, buf, 4096), "mpm_autotune")
-        return buf.value.decode()
+

@@ -50,7 +50,7 @@ def loss_fn(drv, scene, t, dtype, v0, E, nsteps, every, want_grad, part=False):
     if not want_grad:
         return float(L)
     L.backward()
-    return float(L), v0t.grad.detach().cpu().numpy().astype(np.float64), Et.grad.detach().cpu().numpy().astype(np.float64)
+    return float(L.detach()), v0t.grad.detach().cpu().numpy().astype(np.float64), Et.grad.detach().cpu().numpy().astype(np.float64)
 
 
 def fd(f, x0, direction, hs=(1e-3, 3e-4, 1e-4, 3e-5)):
