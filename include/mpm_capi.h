@@ -204,7 +204,8 @@ int mpm_grid_totals(mpm_handle* h, mpm_totals* out);
 
 /* MPM_DRIVER::Compute_Dt (MPM_DRIVER.cpp:1098-1105) with the affine CFL bound
  * (use_affine_cfl): cfl * dx_min / v, or max_dt when v is below
- * cfl * dx_min / max_dt. */
+ * cfl * dx_min / max_dt.  For a batch, dx_min is the smallest cell of any
+ * scene and v the largest bound of any scene: a step every scene can take. */
 int mpm_compute_dt(mpm_handle* h, double cfl, double max_dt, double* dt);
 
 /* Per-kernel device time: enable (1) / disable (0) CUDA-event timing, then read
