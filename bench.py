@@ -163,16 +163,17 @@ def cpu_baseline_sample(scene, seconds_budget=20.0):
             "sample": "full scene (%d particles), 2 substeps, C restatement FP64, 1 thread" % scene.n}
 
 
-def kernels_per_substep(scene):
+def kernels_per_substep(scene, p2g_variant=0):
     """Our kernels launched per fast-path substep: the digit histograms, one
-    single-pass kernel per radix digit, ranges, tail, p2g, grid, g2p."""
+    single-pass kernel per radix digit, ranges, tail, p2g (+ its FP64-stress
+    kernel for the two-lanes-per-range variant), grid, g2p."""
     blocks = 1
     for c in scene.counts:
         blocks *= (c + 4 + 3) // 4
     bits = 6
     while (1 << bits) <= blocks * 64:
         bits += 1
-    return (bits + 7) // 8 + 6
+    return (bits + 7) // 8 + 6 + (1 if p2g_variant == 2 else 0)
 
 
 def read_traffic(kernel, workload=WORKLOAD):
@@ -259,6 +260,7 @@ def our_arm(args):
     drv.set_stream(stream.cuda_stream)
     drv.set_scene_particles(scene)
     tuned = drv.autotune(substeps=3)
+    shape = drv.get_launch_shape()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     ms, ktimes, clocks = measure_substeps(drv, stream, flush, args.steps, args.warmup, dist, local)
@@ -322,7 +324,7 @@ def our_arm(args):
                        "parallelism": "replicas" if world > 1 else "single"},
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "step": "upload + %d substeps (CUDA graph) + download, pinned host buffers" % frame},
-            "gpu_launches": kernels_per_substep(scene) * args.steps,
+            "gpu_launches": kernels_per_substep(scene, shape[0]) * args.steps,
             "autotune": tuned,
             "roofline": roof,
             "substep_roofline": {"achieved": ALG_BYTES["substep"] * n / (substep_ms / 1e3) / 1e9, "peak": peak,

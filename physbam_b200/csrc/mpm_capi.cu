@@ -377,6 +377,30 @@ int mpm_autotune(mpm_handle* h, double dt, int substeps, char* report, int repor
     return read_flags(h);
 }
 
+int mpm_set_launch_shape(mpm_handle* h, int p2g_variant, int g2p_threads, int cta_mult)
+{
+    if(!h) return MPM_ERR_ARG;
+    if(!fast(h)) return set_error(h, MPM_ERR_ARG, "launch shapes belong to the fast path");
+    if(p2g_variant < MPM_P2G_CELLS || p2g_variant > MPM_P2G_PAIRS) return set_error(h, MPM_ERR_ARG, "unknown P2G variant");
+    if(g2p_threads != 64 && g2p_threads != 128 && g2p_threads != 256) return set_error(h, MPM_ERR_ARG, "G2P threads: 64, 128 or 256");
+    if(cta_mult != 1 && cta_mult != 2) return set_error(h, MPM_ERR_ARG, "CTA multiplier: 1 or 2");
+    release_graph(h);
+    h->fast.p2g_variant = p2g_variant;
+    h->fast.g2p_threads = g2p_threads;
+    h->fast.cta_mult = cta_mult;
+    return MPM_OK;
+}
+
+int mpm_get_launch_shape(mpm_handle* h, int* p2g_variant, int* g2p_threads, int* cta_mult)
+{
+    if(!h || !p2g_variant || !g2p_threads || !cta_mult) return MPM_ERR_ARG;
+    if(!fast(h)) return set_error(h, MPM_ERR_ARG, "launch shapes belong to the fast path");
+    *p2g_variant = h->fast.p2g_variant;
+    *g2p_threads = h->fast.g2p_threads;
+    *cta_mult = h->fast.cta_mult;
+    return MPM_OK;
+}
+
 int mpm_diff_forward(mpm_handle* h, double dt, int nsteps, int checkpoint_every)
 {
     int rc = check_dt(h, dt);

@@ -56,6 +56,7 @@ struct FastArgs {
     const uint32_t* sorted_keys;
     uint32_t* keys_next;
     uint32_t *bstart, *bend, *active, *nb_flag, *nb_list, *counters;
+    uint32_t* fallback;   // sorted positions whose stress takes the FP64 route (P2G variant 2)
     float4* acc;
     float4* vel;
     const SceneDev* scenes;
@@ -457,6 +458,186 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_p2g_interleav
     }
 }
 
+// P2G variant 2: two lanes per contiguous range of the block's sorted
+// particles.  The ranges split the block evenly (no lane idles on a sparse
+// cell), and the two lanes of a pair split the four node quantities: the even
+// lane accumulates mass and x momentum, the odd lane y and z momentum, so each
+// holds 54 accumulators instead of 108 and twice as many warps fit on an SM.
+// Accumulators go to the shared tile whenever the range moves to a new cell.
+//
+// Every quantity has the separable form (w = wx wy wz at node (i, j, k))
+//   q_node = Hx[i] wy[j] wz[k] + wx[i] Hy[j] wz[k] + wx[i] wy[j] Hz[k]
+// with, for momentum component r and axis a,
+//   Ha[o] = wa[o] m B(r,a) Dinv_a (x_a(o) - X_a) - dt vol PF^T(r,a) wa'(o)
+//           (+ wa[o] m V_r on the x axis),
+// i.e. w m (V + B Dinv (x - X)) - dt vol PF^T grad w; mass is the same form
+// with V_r = 1, B = 0 and PF^T = 0 (MPM_DRIVER::Particle_To_Grid,
+// MPM_DRIVER.cpp:245-306, with MPM_FINITE_ELEMENTS::Add_Forces,
+// MPM_FINITE_ELEMENTS.cpp:84-99, folded in as dt f).
+struct PairSlot {
+    float Hx[3], Hy[3], Hz[3];
+};
+
+__device__ __forceinline__ void pair_slot(const Axis<float>& wx, const Axis<float>& wy, const Axis<float>& wz,
+    const float dX[3][3], float mV, const float mBD[3], const float S[3], PairSlot& q)
+{
+#pragma unroll
+    for(int o = 0; o < 3; o++) {
+        q.Hx[o] = wx.w[o] * fmaf(mBD[0], dX[0][o], mV) - S[0] * wx.dw[o];
+        q.Hy[o] = wy.w[o] * (mBD[1] * dX[1][o]) - S[1] * wy.dw[o];
+        q.Hz[o] = wz.w[o] * (mBD[2] * dX[2][o]) - S[2] * wz.dw[o];
+    }
+}
+
+template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_p2g_pairs(FastArgs a)
+{
+    __shared__ P2GTile T;
+    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
+    const bool odd = threadIdx.x & 1;
+    const int pair = threadIdx.x >> 1;
+    constexpr int kPairs = THREADS / 2;
+    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
+        const uint32_t b = a.active[w];
+        stage_scene(a, a.block_scene[b], &T.sc);
+        for(int t = threadIdx.x; t < TN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+        __syncthreads();
+        const SceneDev& sc = T.sc;
+        const uint32_t s = a.bstart[b], e = a.bend[b];
+        const uint32_t per = (e - s + kPairs - 1) / kPairs;
+        const uint32_t j0 = s + pair * per, j1 = min(j0 + per, e);
+        float* const out0 = odd ? T.y : T.m;
+        float* const out1 = odd ? T.z : T.x;
+        float acc0[27], acc1[27];
+#pragma unroll
+        for(int q = 0; q < 27; q++) { acc0[q] = 0.f; acc1[q] = 0.f; }
+        int cell = -1;
+        for(uint32_t j = j0; j < j1; j++) {
+            const int c = (int)(a.sorted_keys[j] & 63u);
+            if(c != cell) {
+                if(cell >= 0) {
+                    const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+#pragma unroll
+                    for(int q = 0; q < 27; q++) {
+                        const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+                        atomicAdd(&out0[t], acc0[q]);
+                        atomicAdd(&out1[t], acc1[q]);
+                        acc0[q] = 0.f;
+                        acc1[q] = 0.f;
+                    }
+                }
+                cell = c;
+            }
+            const uint32_t i = a.perm[j];
+            float X[3], F[9];
+#pragma unroll
+            for(int r = 0; r < 3; r++) X[r] = a.src[(C_X + r) * a.npad + i];
+#pragma unroll
+            for(int r = 0; r < 9; r++) F[r] = a.src[(C_F + r) * a.npad + i];
+            const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
+            // this lane's two components: even lane (mass, x), odd lane (y, z)
+            const int r0 = odd ? 1 : 0, r1 = odd ? 2 : 0;
+            float V0 = a.src[(C_V + r0) * a.npad + i], V1 = a.src[(C_V + r1) * a.npad + i];
+            float B0[3], B1[3];
+#pragma unroll
+            for(int c2 = 0; c2 < 3; c2++) {
+                B0[c2] = a.src[(C_B + r0 + 3 * c2) * a.npad + i];
+                B1[c2] = a.src[(C_B + r1 + 3 * c2) * a.npad + i];
+            }
+            float S[9];
+            if(!stress_fast(sc.model, F, at.z, at.w, S)) {
+                // the FP64 SVD route runs in k_p2g_fallback, which adds this
+                // particle's force; here it contributes mass and momentum only
+                if(!odd) a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
+#pragma unroll
+                for(int r = 0; r < 9; r++) S[r] = 0.f;
+            }
+            const float sv = a.dt * at.y, m = at.x;
+            const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
+            const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
+            const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
+            float dX[3][3];
+#pragma unroll
+            for(int o = 0; o < 3; o++) {
+                dX[0][o] = sc.dmin[0] + ((float)(wx.base + o) + 0.5f) * sc.dx[0] - X[0];
+                dX[1][o] = sc.dmin[1] + ((float)(wy.base + o) + 0.5f) * sc.dx[1] - X[1];
+                dX[2][o] = sc.dmin[2] + ((float)(wz.base + o) + 0.5f) * sc.dx[2] - X[2];
+            }
+            const float Dm[3] = {4.f * sc.inv[0] * sc.inv[0] * m, 4.f * sc.inv[1] * sc.inv[1] * m,
+                                 4.f * sc.inv[2] * sc.inv[2] * m};
+            float mBD0[3], mBD1[3], S0[3], S1[3];
+#pragma unroll
+            for(int c2 = 0; c2 < 3; c2++) {
+                // slot 0 of the even lane is the mass: V = 1, B = 0, PF^T = 0
+                mBD0[c2] = odd ? B0[c2] * Dm[c2] : 0.f;
+                mBD1[c2] = B1[c2] * Dm[c2];
+                S0[c2] = odd ? S[1 + 3 * c2] * sv : 0.f;
+                S1[c2] = (odd ? S[2 + 3 * c2] : S[3 * c2]) * sv;
+            }
+            PairSlot q0, q1;
+            pair_slot(wx, wy, wz, dX, odd ? m * V0 : m, mBD0, S0, q0);
+            pair_slot(wx, wy, wz, dX, m * V1, mBD1, S1, q1);
+#pragma unroll
+            for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+                for(int jj = 0; jj < 3; jj++) {
+                    const float wxy = wx.w[ii] * wy.w[jj];
+                    const float A0 = fmaf(q0.Hx[ii], wy.w[jj], wx.w[ii] * q0.Hy[jj]);
+                    const float A1 = fmaf(q1.Hx[ii], wy.w[jj], wx.w[ii] * q1.Hy[jj]);
+#pragma unroll
+                    for(int kk = 0; kk < 3; kk++) {
+                        const int q = (ii * 3 + jj) * 3 + kk;
+                        acc0[q] = fmaf(A0, wz.w[kk], fmaf(wxy, q0.Hz[kk], acc0[q]));
+                        acc1[q] = fmaf(A1, wz.w[kk], fmaf(wxy, q1.Hz[kk], acc1[q]));
+                    }
+                }
+        }
+        if(cell >= 0) {
+            const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+#pragma unroll
+            for(int q = 0; q < 27; q++) {
+                const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+                atomicAdd(&out0[t], acc0[q]);
+                atomicAdd(&out1[t], acc1[q]);
+            }
+        }
+        p2g_end(a, T, b - sc.block_base);
+    }
+}
+
+// The elastic force of the particles k_p2g_pairs listed for the FP64 stress
+// route: -dt vol PF^T grad w added to the momentum of their 27 nodes.  Their
+// nodes lie in their block's tile, whose node blocks P2G already marked.
+__global__ void k_p2g_fallback(FastArgs a)
+{
+    const uint32_t count = a.counters[CNT_FALLBACK];
+    for(uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t j = a.fallback[k], i = a.perm[j];
+        const SceneDev& sc = a.scenes[a.block_scene[a.sorted_keys[j] >> 6]];
+        float X[3], F[9], S[9];
+#pragma unroll
+        for(int r = 0; r < 3; r++) X[r] = a.src[(C_X + r) * a.npad + i];
+#pragma unroll
+        for(int r = 0; r < 9; r++) F[r] = a.src[(C_F + r) * a.npad + i];
+        const float4 at = a.src_attr[i];
+        if(!stress_fp64(sc.model, F, at.z, at.w, S)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
+        const float sv = a.dt * at.y;
+        const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
+        const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
+        const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
+        for(int ii = 0; ii < 3; ii++)
+            for(int jj = 0; jj < 3; jj++)
+                for(int kk = 0; kk < 3; kk++) {
+                    const float g0 = wx.dw[ii] * wy.w[jj] * wz.w[kk], g1 = wx.w[ii] * wy.dw[jj] * wz.w[kk],
+                                g2 = wx.w[ii] * wy.w[jj] * wz.dw[kk];
+                    float f[3];
+#pragma unroll
+                    for(int r = 0; r < 3; r++) f[r] = -sv * (S[r] * g0 + S[r + 3] * g1 + S[r + 6] * g2);
+                    const int64_t q = node_index(sc, wx.base + MPM_GHOST + ii, wy.base + MPM_GHOST + jj, wz.base + MPM_GHOST + kk);
+                    atomicAdd(&a.acc[q], make_float4(f[0], f[1], f[2], 0.f));
+                }
+    }
+}
+
 // One node block (4^3 nodes) per 64 threads.
 __global__ void __launch_bounds__(64) k_grid(FastArgs a)
 {
@@ -710,6 +891,7 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.bstart = f.bstart; a.bend = f.bend; a.active = f.active;
     a.nb_flag = f.nb_flag; a.nb_list = f.nb_list; a.counters = f.counters;
     a.acc = f.acc; a.vel = f.vel;
+    a.fallback = f.sort_keys_alt;   // the sort's ping-pong buffer is free until the next sort
     a.scenes = f.scenes; a.block_scene = f.block_scene; a.nb_scene = f.nb_scene; a.pbase = f.pbase;
     a.objs = f.objs;
     a.nscenes = f.nscenes;
@@ -727,6 +909,7 @@ int grid_stride_blocks(mpm_handle* h, int64_t n, int t)
 
 // Launch shapes the autotuner chooses among.
 const int kG2PThreads[] = {64, 128, 256};
+const char* const kP2GNames[] = {"cells", "interleaved", "pairs"};
 
 int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult)
 {
@@ -1028,7 +1211,13 @@ int fast_p2g(mpm_handle* h, double dt, double)
     timer_end(h, slot);
     slot = timer_begin(h, "fast_p2g");
     if(f.p2g_variant == 0) k_p2g_cells<<<occupancy_ctas(h, (const void*)k_p2g_cells, 64, f.cta_mult), 64, 0, h->stream>>>(a);
-    else k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
+    else if(f.p2g_variant == 1)
+        k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
+    else {
+        k_p2g_pairs<128><<<occupancy_ctas(h, (const void*)k_p2g_pairs<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
+        MPM_LAUNCHED(h, "k_p2g_pairs");
+        k_p2g_fallback<<<h->sm_count, 128, 0, h->stream>>>(a);
+    }
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_p2g");
     return MPM_OK;
@@ -1153,7 +1342,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
     const bool timing = h->timing;
     h->timing = false;
     int rc = MPM_OK;
-    for(int variant = 0; variant < 2 && !rc; variant++)
+    for(int variant = 0; variant < 3 && !rc; variant++)
         for(int ti = 0; ti < 3 && !rc; ti++)
             for(int mult = 1; mult <= 2 && !rc; mult++) {
                 f.p2g_variant = variant;
@@ -1176,7 +1365,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
                 ms /= substeps;
                 char line[128];
                 snprintf(line, sizeof line, "%sp2g=%s g2p=%d ctas=x%d: %.4f ms", rep.empty() ? "" : "; ",
-                         variant ? "interleaved" : "cells", kG2PThreads[ti], mult, ms);
+                         kP2GNames[variant], kG2PThreads[ti], mult, ms);
                 rep += line;
                 if(ms < best) { best = ms; best_v = variant; best_t = kG2PThreads[ti]; best_m = mult; }
             }
@@ -1194,7 +1383,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     char tail[128];
-    snprintf(tail, sizeof tail, " | chosen p2g=%s g2p=%d ctas=x%d (%.4f ms/substep)", best_v ? "interleaved" : "cells", best_t, best_m, best);
+    snprintf(tail, sizeof tail, " | chosen p2g=%s g2p=%d ctas=x%d (%.4f ms/substep)", kP2GNames[best_v], best_t, best_m, best);
     rep += tail;
     if(report && report_len > 0) snprintf(report, (size_t)report_len, "%s", rep.c_str());
     return rc;
@@ -1306,8 +1495,9 @@ extern "C" int mpm_radix_sort_u32_noalloc(const uint32_t* keys, int64_t n, int b
     if(cudaMemsetAsync(flag, 0, sizeof(unsigned), st) != cudaSuccess) return MPM_ERR_CUDA;
     int sms = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // 4096-key tiles always: the fixed scratch holds the look-back words for those
     if(mpm_sort::radix_sort(keys, sorted_keys, perm, base + kNoAllocKeysAlt, base + kNoAllocValsAlt, n, bits, base,
-                            flag, MPM_FLAG_TIMEOUT, sms * 4, st) != cudaSuccess) return MPM_ERR_CUDA;
+                            flag, MPM_FLAG_TIMEOUT, sms * 4, st, false) != cudaSuccess) return MPM_ERR_CUDA;
     unsigned f = 0;
     if(cudaMemcpyAsync(&f, flag, sizeof(f), cudaMemcpyDeviceToHost, st) != cudaSuccess) return MPM_ERR_CUDA;
     if(cudaStreamSynchronize(st) != cudaSuccess) return MPM_ERR_CUDA;

@@ -33,6 +33,11 @@ namespace mpm_sort {
 constexpr int kThreads = 256;
 constexpr int kItems = 16;
 constexpr int kTile = kThreads * kItems;   // 4096 keys per tile
+// Small sorts (up to kSmallSortMax keys) use 1024-key tiles: four times the
+// CTAs, so a sort of a few hundred thousand keys still spreads over the SMs.
+constexpr int kSmallItems = 4;
+constexpr int kSmallTile = kThreads * kSmallItems;
+constexpr int64_t kSmallSortMax = 1 << 21;
 constexpr int kRadix = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxPasses = 4;
@@ -51,8 +56,14 @@ constexpr int kTicketOff = kHistWords;
 constexpr int kEpochOff = kTicketOff + kMaxPasses;
 constexpr int kStatusOff = kEpochOff + 4;     // keep 16-byte alignment
 
-__host__ __device__ inline int64_t tiles_for(int64_t n) { return (n + kTile - 1) / kTile; }
-inline int64_t scratch_words(int64_t n) { return kStatusOff + 2 * (int64_t)kMaxPasses * tiles_for(n > 0 ? n : 1) * kRadix; }
+__host__ __device__ constexpr int64_t tiles_for(int64_t n, int tile = kTile) { return (n + tile - 1) / tile; }
+// Scratch for any sort of up to n keys, whichever tile size it picks.
+inline int64_t scratch_words(int64_t n)
+{
+    int64_t t = tiles_for(n > 0 ? n : 1);
+    int64_t small = tiles_for(n < kSmallSortMax ? (n > 0 ? n : 1) : kSmallSortMax, kSmallTile);
+    return kStatusOff + 2 * (int64_t)kMaxPasses * (t > small ? t : small) * kRadix;
+}
 
 __device__ __forceinline__ int passes_for(int bits) { return (bits + 7) / 8; }
 __device__ __forceinline__ uint32_t digit_mask(int bits, int pass)
@@ -112,23 +123,26 @@ __device__ inline uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem, uint
     return warp_prefix + x - v;
 }
 
-struct PassSmem {
+template<int ITEMS> struct PassSmem {
     uint32_t wcnt[kWarps][kRadix];
     uint32_t dstart[kRadix];
     uint32_t gbase[kRadix];
-    uint32_t skey[kTile];
-    uint32_t sval[kTile];
+    uint32_t skey[kThreads * ITEMS];
+    uint32_t sval[kThreads * ITEMS];
     uint32_t scan_tmp[32];
     uint32_t tile;
 };
 
-// One digit place.  vals_in == nullptr means payload = index.
+// One digit place over tiles of kThreads * ITEMS keys.  vals_in == nullptr
+// means payload = index.
+template<int ITEMS>
 __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int bits, int pass, int64_t tiles,
     uint32_t* __restrict__ scratch, unsigned* __restrict__ err_flags, unsigned timeout_flag)
 {
+    constexpr int kItems = ITEMS, kTile = kThreads * ITEMS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    PassSmem& S = *reinterpret_cast<PassSmem*>(smem_raw);
+    PassSmem<ITEMS>& S = *reinterpret_cast<PassSmem<ITEMS>*>(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int shift = 8 * pass;
     const uint32_t mask = digit_mask(bits, pass);
@@ -222,24 +236,29 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
     }
 }
 
-inline size_t pass_smem() { return sizeof(PassSmem); }
+template<int ITEMS> inline size_t pass_smem() { return sizeof(PassSmem<ITEMS>); }
 
 inline cudaError_t prepare()
 {
-    return cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem());
+    cudaError_t e = cudaFuncSetAttribute(k_onesweep<kItems>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pass_smem<kItems>());
+    if(e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_onesweep<kSmallItems>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)pass_smem<kSmallItems>());
 }
 
 // Sorts keys[0..n) by their low `bits` bits (1..32).  keys is read only;
 // the result lands in (keys_out, vals_out), which must not alias keys;
 // (keys_alt, vals_alt) are ping-pong buffers.  scratch = scratch_words(n)
 // words whose epoch region persists between sorts.  n < 2^30.
+// `small_tiles` allows 1024-key tiles for n <= kSmallSortMax.
 inline cudaError_t radix_sort(const uint32_t* keys, uint32_t* keys_out, uint32_t* vals_out, uint32_t* keys_alt,
     uint32_t* vals_alt, int64_t n, int bits, uint32_t* scratch, unsigned* err_flags, unsigned timeout_flag,
-    int hist_blocks, cudaStream_t st)
+    int hist_blocks, cudaStream_t st, bool small_tiles = true)
 {
     if(n == 0) return cudaSuccess;
     int passes = (bits + 7) / 8;
-    int64_t tiles = tiles_for(n);
+    const bool small = small_tiles && n <= kSmallSortMax;
+    int64_t tiles = small ? tiles_for(n, kSmallTile) : tiles_for(n);
     cudaError_t e = cudaMemsetAsync(scratch, 0, kHistWords * sizeof(uint32_t), st);
     if(e != cudaSuccess) return e;
     int hb = (int)((n + kThreads * 16 - 1) / (kThreads * 16));
@@ -253,8 +272,12 @@ inline cudaError_t radix_sort(const uint32_t* keys, uint32_t* keys_out, uint32_t
         bool last_to_out = ((passes - 1 - p) % 2) == 0;
         uint32_t* ko = last_to_out ? keys_out : keys_alt;
         uint32_t* vo = last_to_out ? vals_out : vals_alt;
-        k_onesweep<<<(unsigned)tiles, kThreads, pass_smem(), st>>>(kin, vin, ko, vo, n, bits, p, tiles, scratch,
-                                                                    err_flags, timeout_flag);
+        if(small)
+            k_onesweep<kSmallItems><<<(unsigned)tiles, kThreads, pass_smem<kSmallItems>(), st>>>(
+                kin, vin, ko, vo, n, bits, p, tiles, scratch, err_flags, timeout_flag);
+        else
+            k_onesweep<kItems><<<(unsigned)tiles, kThreads, pass_smem<kItems>(), st>>>(
+                kin, vin, ko, vo, n, bits, p, tiles, scratch, err_flags, timeout_flag);
         kin = ko;
         vin = vo;
     }

@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(HERE, "libphysbam_mpm.so")
 
 MPM_OK = 0
 FP32, FP64 = 0, 1
+P2G_CELLS, P2G_INTERLEAVED, P2G_PAIRS = 0, 1, 2
 PATH_FAST, PATH_PLAIN = 0, 1
 MAX_OBJECTS = 8
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "non-finite value", 4: "particle outside the grid",
@@ -73,7 +74,7 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_grid_to_particle", "mpm_synchronize", "mpm_get_grid", "mpm_count_valid", "mpm_set_timing",
            "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state",
            "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune", "mpm_particle_totals",
-           "mpm_grid_totals", "mpm_compute_dt"]
+           "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape"]
 
 _lib = None
 
@@ -107,6 +108,8 @@ def load_library(path: str = LIB_PATH):
     L.mpm_diff_backward.argtypes = [P, ctypes.POINTER(ParticlesView), ctypes.POINTER(ParticlesView), P, P]
     L.mpm_radix_sort_u32.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P]
     L.mpm_autotune.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+    L.mpm_set_launch_shape.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.mpm_get_launch_shape.argtypes = [P] + [ctypes.POINTER(ctypes.c_int)] * 3
     L.mpm_particle_totals.argtypes = [P, ctypes.POINTER(Totals)]
     L.mpm_grid_totals.argtypes = [P, ctypes.POINTER(Totals)]
     L.mpm_compute_dt.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
@@ -335,6 +338,14 @@ class MPM_DRIVER:
         buf = ctypes.create_string_buffer(4096)
         self._check(self.L.mpm_autotune(self.h, dt, substeps, buf, 4096), "mpm_autotune")
         return buf.value.decode()
+
+    def set_launch_shape(self, p2g_variant, g2p_threads=128, cta_mult=1):
+        self._check(self.L.mpm_set_launch_shape(self.h, p2g_variant, g2p_threads, cta_mult), "mpm_set_launch_shape")
+
+    def get_launch_shape(self):
+        v = [ctypes.c_int() for _ in range(3)]
+        self._check(self.L.mpm_get_launch_shape(self.h, *[ctypes.byref(x) for x in v]), "mpm_get_launch_shape")
+        return tuple(x.value for x in v)
 
     def particle_totals(self):
         t = Totals()

@@ -42,9 +42,11 @@ TOL_FP64 = {"X": 1e-12, "V": 1e-9, "F": 1e-10, "B": 1e-8, "grid_m": 1e-12, "grid
 TOL_FP32 = {"X": 2e-6, "V": 2e-3, "F": 1e-4, "B": 2e-3, "grid_m": 1e-5, "grid_v": 1e-3, "grid_vf": 1e-3}
 
 
-def run_case(name, precision, path, tol):
+def run_case(name, precision, path, tol, shape=None):
     scene, dumps = load(name)
     drv = D().MPM_DRIVER(scene, precision=precision, path=path)
+    if shape is not None:
+        drv.set_launch_shape(*shape)
     drv.set_scene_particles(scene)
     worst = {}
     for step in range(max(dumps) + 1):
@@ -77,13 +79,62 @@ def test_plain_fp64_matches_reference(cuda_device, name):
     run_case(name, D().FP64, D().PATH_PLAIN, TOL_FP64)
 
 
+# launch shapes: (P2G variant, G2P threads per CTA, CTA multiplier)
+SHAPES = [(0, 128, 1), (1, 64, 2), (2, 256, 1), (2, 128, 2)]
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "p2g%d-g2p%d-x%d" % s)
 @pytest.mark.parametrize("name", sorted(n for n in CASES if n.startswith("small3d")))
-def test_fast_fp32_matches_reference(cuda_device, name):
-    run_case(name, D().FP32, D().PATH_FAST, TOL_FP32)
+def test_fast_fp32_matches_reference(cuda_device, name, shape):
+    run_case(name, D().FP32, D().PATH_FAST, TOL_FP32, shape)
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "p2g%d-g2p%d-x%d" % s)
+@pytest.mark.parametrize("model", [S.COROTATED, S.NEO_HOOKEAN])
+def test_fast_stress_fallback_matches_plain_fp64(cuda_device, model, shape):
+    """Inverted and nearly flat F take the FP64 SVD route on the fast path
+    (the P2G kernel defers their force to a second kernel for variant 2)."""
+    scene = S.small_3d(model=model, nsteps=3)
+    rng = np.random.default_rng(5)
+    n = scene.n
+    F = scene.F.copy()
+    inv = rng.random(n) < 0.3
+    F[inv, :, 0] *= -1.0                                  # det < 0
+    flat = (~inv) & (rng.random(n) < 0.15)
+    F[flat, :, 2] *= 5e-3                                 # sigma_min / sigma_max < 1e-2
+    scene.F = F
+    got = {}
+    for prec, path, sh in ((D().FP64, D().PATH_PLAIN, None), (D().FP32, D().PATH_FAST, shape)):
+        drv = D().MPM_DRIVER(scene, precision=prec, path=path)
+        if sh is not None:
+            drv.set_launch_shape(*sh)
+        drv.set_scene_particles(scene)
+        for _ in range(scene.nsteps):
+            drv.Advance_One_Time_Step()
+        got[path] = drv.get_particles()
+        drv.close()
+    ref, fast = got[D().PATH_PLAIN], got[D().PATH_FAST]
+    np.testing.assert_array_equal(fast["valid"], ref["valid"])
+    vmax = float(np.abs(ref["V"]).max())
+    assert rel(fast["X"], ref["X"], 1.0) < 2e-6
+    assert rel(fast["V"], ref["V"], vmax) < 2e-3
+    assert rel(fast["F"], ref["F"], 1.0) < 1e-4
+
+
+def test_launch_shape_round_trip(cuda_device):
+    scene = S.small_3d(nsteps=1)
+    drv = D().MPM_DRIVER(scene)
+    drv.set_launch_shape(2, 64, 2)
+    assert drv.get_launch_shape() == (2, 64, 2)
+    for bad in [(3, 128, 1), (0, 96, 1), (0, 128, 3)]:
+        with pytest.raises(D().MPMError):
+            drv.set_launch_shape(*bad)
+    assert drv.get_launch_shape() == (2, 64, 2)
+    drv.close()
 
 
 @pytest.mark.parametrize("n,bits", [(0, 8), (1, 8), (2047, 11), (2048, 16), (2049, 17), (100_003, 25),
-                                    (1_000_000, 32), (300_000, 6)])
+                                    (1_000_000, 32), (300_000, 6), (3_000_001, 30)])
 def test_radix_sort_bit_exact(cuda_device, n, bits):
     rng = np.random.default_rng(n + bits)
     keys = rng.integers(0, 2 ** 32, n, dtype=np.uint64).astype(np.uint32)
