@@ -165,15 +165,15 @@ def cpu_baseline_sample(scene, seconds_budget=20.0):
 
 def kernels_per_substep(scene, p2g_variant=0):
     """Our kernels launched per fast-path substep: the digit histograms, one
-    single-pass kernel per radix digit, ranges, tail, p2g (+ its FP64-stress
-    kernel for the two-lanes-per-range variant), grid, g2p."""
+    single-pass kernel per radix digit, ranges (+ invalid tail), p2g (+ its
+    FP64-stress kernel for the two-lanes-per-range variant), grid, g2p."""
     blocks = 1
     for c in scene.counts:
         blocks *= (c + 4 + 3) // 4
     bits = 6
     while (1 << bits) <= blocks * 64:
         bits += 1
-    return (bits + 7) // 8 + 6 + (1 if p2g_variant == 2 else 0)
+    return (bits + 7) // 8 + 5 + (1 if p2g_variant == 2 else 0)
 
 
 def read_traffic(kernel, workload=WORKLOAD):
@@ -433,6 +433,8 @@ def profile_case(args, D, S):
     make = {"spheres3d": S.spheres_3d, "dam3d": S.dam_3d, "cube3d": S.cube_3d}[args.scene]
     scene = make(G=args.grid) if args.grid else make()
     drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+    if args.shape:
+        drv.set_launch_shape(*[int(x) for x in args.shape.split(",")])
     drv.set_scene_particles(scene, dtype=np.float32)
     drv.advance(args.warmup)
     drv.synchronize()
@@ -484,6 +486,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 path on the same workload")
     ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d"], help="profiling run of one scene only")
     ap.add_argument("--grid", type=int, default=0, help="grid cells per side for --scene")
+    ap.add_argument("--shape", default="", help="launch shape for --scene: P2G variant,G2P threads,CTA multiplier")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -207,6 +207,9 @@ __global__ void k_init_keys(FastArgs a, const uint8_t* valid_by_slot)
     }
 }
 
+// Block ranges of the sorted keys and the list of active blocks.  Invalid
+// particles (sentinel keys, sorted last) keep their last state: they are
+// copied to their sorted slot here, as G2P does for the valid ones.
 __global__ void k_ranges(FastArgs a)
 {
     for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < a.n; j += (int64_t)gridDim.x * blockDim.x) {
@@ -214,6 +217,12 @@ __global__ void k_ranges(FastArgs a)
         uint32_t kp = j ? a.sorted_keys[j - 1] : SENTINEL;
         if(k == SENTINEL) {
             if(j == 0 || kp != SENTINEL) a.counters[CNT_ACTIVE_PARTICLES] = (uint32_t)j;
+            const uint32_t i = a.perm[j];
+#pragma unroll 4
+            for(int c = 0; c < NCOMP; c++) a.dst[c * a.npad + j] = a.src[c * a.npad + i];
+            a.dst_attr[j] = a.src_attr[i];
+            a.dst_pid[j] = a.src_pid[i];
+            a.keys_next[j] = SENTINEL;
             continue;
         }
         uint32_t b = k >> 6;
@@ -227,19 +236,6 @@ __global__ void k_ranges(FastArgs a)
     }
 }
 
-// Invalid particles keep their last state; move them to their sorted slot.
-__global__ void k_tail(FastArgs a)
-{
-    int64_t n_act = a.counters[CNT_ACTIVE_PARTICLES];
-    for(int64_t j = n_act + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < a.n; j += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t i = a.perm[j];
-#pragma unroll 4
-        for(int c = 0; c < NCOMP; c++) a.dst[c * a.npad + j] = a.src[c * a.npad + i];
-        a.dst_attr[j] = a.src_attr[i];
-        a.dst_pid[j] = a.src_pid[i];
-        a.keys_next[j] = SENTINEL;
-    }
-}
 
 __device__ __forceinline__ int next_work(uint32_t* ctr, int* s_work)
 {
@@ -638,20 +634,18 @@ __global__ void k_p2g_fallback(FastArgs a)
     }
 }
 
-// One node block (4^3 nodes) per 64 threads.
-__global__ void __launch_bounds__(64) k_grid(FastArgs a)
+// One thread per node of the listed node blocks (4^3 nodes each, 64
+// consecutive threads), grid-stride: no barrier, no work counter.  A warp's
+// 32 nodes share a node block and so a scene record, read through L1.
+__global__ void __launch_bounds__(256) k_grid(FastArgs a)
 {
-    __shared__ int s_work;
-    __shared__ SceneDev s_sc;
-    const uint32_t nnb = a.counters[CNT_NODE_BLOCKS];
-    for(int w = next_work(&a.counters[CNT_GRID_WORK], &s_work); w < (int)nnb; w = next_work(&a.counters[CNT_GRID_WORK], &s_work)) {
-        const uint32_t nb = a.nb_list[w];
-        stage_scene(a, a.nb_scene[nb], &s_sc);
-        __syncthreads();
-        const SceneDev& sc = s_sc;
+    const uint64_t total = (uint64_t)a.counters[CNT_NODE_BLOCKS] * 64u;
+    for(uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total; g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t nb = a.nb_list[g >> 6];
+        const SceneDev& sc = a.scenes[a.nb_scene[nb]];
         const uint32_t lnb = nb - sc.nb_base;
         int nz = lnb % sc.NN[2], r = lnb / sc.NN[2], ny = r % sc.NN[1], nx = r / sc.NN[1];
-        int t = threadIdx.x;
+        int t = (int)(g & 63u);
         int qx = 4 * nx + (t >> 4), qy = 4 * ny + ((t >> 2) & 3), qz = 4 * nz + (t & 3);
         int64_t q = node_index(sc, qx, qy, qz);
         float4 c = a.acc[q];
@@ -1206,8 +1200,6 @@ int fast_p2g(mpm_handle* h, double dt, double)
     MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
     k_ranges<<<grid_stride_blocks(h, n, 256), 256, 0, h->stream>>>(a);
     MPM_LAUNCHED(h, "k_ranges");
-    k_tail<<<h->sm_count * 2, 256, 0, h->stream>>>(a);
-    MPM_LAUNCHED(h, "k_tail");
     timer_end(h, slot);
     slot = timer_begin(h, "fast_p2g");
     if(f.p2g_variant == 0) k_p2g_cells<<<occupancy_ctas(h, (const void*)k_p2g_cells, 64, f.cta_mult), 64, 0, h->stream>>>(a);
@@ -1229,7 +1221,7 @@ int fast_forces(mpm_handle* h, double dt, double)
     if(!f.n) return MPM_OK;
     FastArgs a = make_args(h, dt);
     int slot = timer_begin(h, "fast_grid");
-    k_grid<<<occupancy_ctas(h, (const void*)k_grid, 64, 1), 64, 0, h->stream>>>(a);
+    k_grid<<<h->sm_count * 8, 256, 0, h->stream>>>(a);
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_grid");
     return MPM_OK;

@@ -81,9 +81,19 @@ __global__ void __launch_bounds__(kThreads) k_upfront_hist(const uint32_t* __res
     const int passes = passes_for(bits);
     for(int i = threadIdx.x; i < kMaxPasses * kRadix; i += kThreads) (&cnt[0][0])[i] = 0;
     __syncthreads();
-    for(int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
-        uint32_t k = keys[i];
-        for(int p = 0; p < passes; p++) atomicAdd(&cnt[p][(k >> (8 * p)) & digit_mask(bits, p)], 1u);
+    // keys arrive nearly sorted (last substep's order), so the lanes of a warp
+    // mostly share their high digits: one atomic per distinct digit per warp
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * kThreads;
+    const int64_t end = (n + 31) & ~(int64_t)31;   // whole warps stay in the loop
+    for(int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < end; i += stride) {
+        const bool ok = i < n;
+        const uint32_t k = ok ? keys[i] : 0u;
+        for(int p = 0; p < passes; p++) {
+            const uint32_t dg = ok ? (k >> (8 * p)) & digit_mask(bits, p) : 256u;
+            const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+            if(ok && (__ffs(peers) - 1) == lane) atomicAdd(&cnt[p][dg], (uint32_t)__popc(peers));
+        }
     }
     __syncthreads();
     for(int i = threadIdx.x; i < passes * kRadix; i += kThreads) {
@@ -261,7 +271,7 @@ inline cudaError_t radix_sort(const uint32_t* keys, uint32_t* keys_out, uint32_t
     int64_t tiles = small ? tiles_for(n, kSmallTile) : tiles_for(n);
     cudaError_t e = cudaMemsetAsync(scratch, 0, kHistWords * sizeof(uint32_t), st);
     if(e != cudaSuccess) return e;
-    int hb = (int)((n + kThreads * 16 - 1) / (kThreads * 16));
+    int hb = (int)((n + kThreads * 4 - 1) / (kThreads * 4));
     if(hb > hist_blocks) hb = hist_blocks;
     if(hb < 1) hb = 1;
     k_upfront_hist<<<hb, kThreads, 0, st>>>(keys, n, bits, scratch);
