@@ -173,7 +173,7 @@ def kernels_per_substep(scene, p2g_variant=0):
     bits = 6
     while (1 << bits) <= blocks * 64:
         bits += 1
-    return (bits + 7) // 8 + 5 + (1 if p2g_variant == 2 else 0)
+    return (bits + 7) // 8 + 5 + (1 if p2g_variant >= 2 else 0)
 
 
 def read_traffic(kernel, workload=WORKLOAD):

@@ -600,6 +600,203 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
     }
 }
 
+// P2G variant 3: as variant 2 (two lanes per range, the even lane holding
+// mass and x momentum, the odd lane y and z), but the lanes share the
+// per-particle work: the even lane prepares particle j, the odd lane particle
+// j + 1 (stress, weights and the separable factors of all four quantities),
+// and each sends its partner the weights and the factors of the partner's two
+// quantities through a shuffle.
+struct PairPrep {
+    float w[9];            // wx[3], wy[3], wz[3]
+    PairSlot keep0, keep1, send0, send1;
+    int cell;
+};
+
+__device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc, uint32_t j, bool odd, PairPrep& P)
+{
+    const uint32_t i = a.perm[j];
+    P.cell = (int)(a.sorted_keys[j] & 63u);
+    float X[3], V[3], F[9], B[9];
+#pragma unroll
+    for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
+#pragma unroll
+    for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; B[r] = a.src[(C_B + r) * a.npad + i]; }
+    const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
+    float S[9];
+    if(!stress_fast(sc.model, F, at.z, at.w, S)) {
+        // the FP64 SVD route runs in k_p2g_fallback, which adds the force
+        a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
+#pragma unroll
+        for(int r = 0; r < 9; r++) S[r] = 0.f;
+    }
+    const float sv = a.dt * at.y, m = at.x;
+    const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
+    const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
+    const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
+    float dX[3][3];
+    const float bx = (float)wx.base + 0.5f, by = (float)wy.base + 0.5f, bz = (float)wz.base + 0.5f;
+#pragma unroll
+    for(int o = 0; o < 3; o++) {
+        dX[0][o] = sc.dmin[0] + (bx + (float)o) * sc.dx[0] - X[0];
+        dX[1][o] = sc.dmin[1] + (by + (float)o) * sc.dx[1] - X[1];
+        dX[2][o] = sc.dmin[2] + (bz + (float)o) * sc.dx[2] - X[2];
+    }
+    const float Dm[3] = {4.f * sc.inv[0] * sc.inv[0] * m, 4.f * sc.inv[1] * sc.inv[1] * m, 4.f * sc.inv[2] * sc.inv[2] * m};
+    PairSlot q[3], qm;
+#pragma unroll
+    for(int r = 0; r < 3; r++) {
+        const float mBD[3] = {B[r] * Dm[0], B[r + 3] * Dm[1], B[r + 6] * Dm[2]};
+        const float Sr[3] = {S[r] * sv, S[r + 3] * sv, S[r + 6] * sv};
+        pair_slot(wx, wy, wz, dX, m * V[r], mBD, Sr, q[r]);
+    }
+#pragma unroll
+    for(int o = 0; o < 3; o++) { qm.Hx[o] = m * wx.w[o]; qm.Hy[o] = 0.f; qm.Hz[o] = 0.f; }
+#pragma unroll
+    for(int o = 0; o < 3; o++) { P.w[o] = wx.w[o]; P.w[3 + o] = wy.w[o]; P.w[6 + o] = wz.w[o]; }
+    // even lane keeps (mass, x) and sends (y, z); odd lane the other way round
+#pragma unroll
+    for(int o = 0; o < 3; o++) {
+        P.keep0.Hx[o] = odd ? q[1].Hx[o] : qm.Hx[o]; P.send0.Hx[o] = odd ? qm.Hx[o] : q[1].Hx[o];
+        P.keep0.Hy[o] = odd ? q[1].Hy[o] : 0.f;      P.send0.Hy[o] = odd ? 0.f : q[1].Hy[o];
+        P.keep0.Hz[o] = odd ? q[1].Hz[o] : 0.f;      P.send0.Hz[o] = odd ? 0.f : q[1].Hz[o];
+        P.keep1.Hx[o] = odd ? q[2].Hx[o] : q[0].Hx[o]; P.send1.Hx[o] = odd ? q[0].Hx[o] : q[2].Hx[o];
+        P.keep1.Hy[o] = odd ? q[2].Hy[o] : q[0].Hy[o]; P.send1.Hy[o] = odd ? q[0].Hy[o] : q[2].Hy[o];
+        P.keep1.Hz[o] = odd ? q[2].Hz[o] : q[0].Hz[o]; P.send1.Hz[o] = odd ? q[0].Hz[o] : q[2].Hz[o];
+    }
+}
+
+__device__ __forceinline__ void pair_accumulate(const float* w, const PairSlot& q0, const PairSlot& q1, float* acc0, float* acc1)
+{
+#pragma unroll
+    for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+        for(int jj = 0; jj < 3; jj++) {
+            const float wxy = w[ii] * w[3 + jj];
+            const float A0 = fmaf(q0.Hx[ii], w[3 + jj], w[ii] * q0.Hy[jj]);
+            const float A1 = fmaf(q1.Hx[ii], w[3 + jj], w[ii] * q1.Hy[jj]);
+#pragma unroll
+            for(int kk = 0; kk < 3; kk++) {
+                const int q = (ii * 3 + jj) * 3 + kk;
+                acc0[q] = fmaf(A0, w[6 + kk], fmaf(wxy, q0.Hz[kk], acc0[q]));
+                acc1[q] = fmaf(A1, w[6 + kk], fmaf(wxy, q1.Hz[kk], acc1[q]));
+            }
+        }
+}
+
+__device__ __forceinline__ void pair_flush(int cell, float* out0, float* out1, float* acc0, float* acc1)
+{
+    const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+#pragma unroll
+    for(int q = 0; q < 27; q++) {
+        const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+        atomicAdd(&out0[t], acc0[q]);
+        atomicAdd(&out1[t], acc1[q]);
+        acc0[q] = 0.f;
+        acc1[q] = 0.f;
+    }
+}
+
+// Swap with the other lane of the pair.  Only the pair takes part: pairs of
+// one warp may run different trip counts.
+__device__ __forceinline__ unsigned pair_mask() { return 3u << ((threadIdx.x & 31) & ~1u); }
+__device__ __forceinline__ float shfl1(float v) { return __shfl_xor_sync(pair_mask(), v, 1); }
+
+template<int THREADS> __global__ void __launch_bounds__(THREADS, 384 / THREADS) k_p2g_pairx(FastArgs a)
+{
+    __shared__ P2GTile T;
+    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
+    const bool odd = threadIdx.x & 1;
+    const int pair = threadIdx.x >> 1;
+    constexpr int kPairs = THREADS / 2;
+    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
+        const uint32_t b = a.active[w];
+        stage_scene(a, a.block_scene[b], &T.sc);
+        for(int t = threadIdx.x; t < TN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+        __syncthreads();
+        const SceneDev& sc = T.sc;
+        const uint32_t s = a.bstart[b], e = a.bend[b];
+        // ranges of an even length, so both lanes of a pair always have a particle but the last
+        const uint32_t per = ((e - s + kPairs - 1) / kPairs + 1) & ~1u;
+        const uint32_t j0 = s + pair * per, j1 = min(j0 + per, e);
+        float* const out0 = odd ? T.y : T.m;
+        float* const out1 = odd ? T.z : T.x;
+        float acc0[27], acc1[27];
+#pragma unroll
+        for(int q = 0; q < 27; q++) { acc0[q] = 0.f; acc1[q] = 0.f; }
+        int cell = -1;
+        // the pair's lanes run the same trip count: j0 and j1 are shared
+        for(uint32_t j = j0; j < j1; j += 2) {
+            const bool have1 = j + 1 < j1;
+            PairPrep P;
+            const bool mine = !odd || have1;
+            if(mine) pair_prep(a, sc, j + (odd ? 1u : 0u), odd, P);
+            else {
+#pragma unroll
+                for(int k = 0; k < 9; k++) P.w[k] = 0.f;
+                P.cell = -1;
+            }
+            // swap: partner's cell, weights and the factors of my quantities
+            PairPrep R;
+            R.cell = __shfl_xor_sync(pair_mask(), P.cell, 1);
+#pragma unroll
+            for(int k = 0; k < 9; k++) R.w[k] = shfl1(P.w[k]);
+#pragma unroll
+            for(int o = 0; o < 3; o++) {
+                R.keep0.Hx[o] = shfl1(P.send0.Hx[o]); R.keep0.Hy[o] = shfl1(P.send0.Hy[o]); R.keep0.Hz[o] = shfl1(P.send0.Hz[o]);
+                R.keep1.Hx[o] = shfl1(P.send1.Hx[o]); R.keep1.Hy[o] = shfl1(P.send1.Hy[o]); R.keep1.Hz[o] = shfl1(P.send1.Hz[o]);
+            }
+            // particle j first (the even lane's), then j + 1 (the odd lane's)
+            const int c_first = odd ? R.cell : P.cell, c_second = odd ? P.cell : R.cell;
+            {
+                if(c_first != cell) {
+                    if(cell >= 0) pair_flush(cell, out0, out1, acc0, acc1);
+                    cell = c_first;
+                }
+                float wf[9];
+#pragma unroll
+                for(int k = 0; k < 9; k++) wf[k] = odd ? R.w[k] : P.w[k];
+                PairSlot f0, f1;
+#pragma unroll
+                for(int o = 0; o < 3; o++) {
+                    f0.Hx[o] = odd ? R.keep0.Hx[o] : P.keep0.Hx[o]; f0.Hy[o] = odd ? R.keep0.Hy[o] : P.keep0.Hy[o];
+                    f0.Hz[o] = odd ? R.keep0.Hz[o] : P.keep0.Hz[o];
+                    f1.Hx[o] = odd ? R.keep1.Hx[o] : P.keep1.Hx[o]; f1.Hy[o] = odd ? R.keep1.Hy[o] : P.keep1.Hy[o];
+                    f1.Hz[o] = odd ? R.keep1.Hz[o] : P.keep1.Hz[o];
+                }
+                pair_accumulate(wf, f0, f1, acc0, acc1);
+            }
+            if(have1) {
+                if(c_second != cell) {
+                    pair_flush(cell, out0, out1, acc0, acc1);
+                    cell = c_second;
+                }
+                float ws[9];
+#pragma unroll
+                for(int k = 0; k < 9; k++) ws[k] = odd ? P.w[k] : R.w[k];
+                PairSlot g0, g1;
+#pragma unroll
+                for(int o = 0; o < 3; o++) {
+                    g0.Hx[o] = odd ? P.keep0.Hx[o] : R.keep0.Hx[o]; g0.Hy[o] = odd ? P.keep0.Hy[o] : R.keep0.Hy[o];
+                    g0.Hz[o] = odd ? P.keep0.Hz[o] : R.keep0.Hz[o];
+                    g1.Hx[o] = odd ? P.keep1.Hx[o] : R.keep1.Hx[o]; g1.Hy[o] = odd ? P.keep1.Hy[o] : R.keep1.Hy[o];
+                    g1.Hz[o] = odd ? P.keep1.Hz[o] : R.keep1.Hz[o];
+                }
+                pair_accumulate(ws, g0, g1, acc0, acc1);
+            }
+        }
+        if(cell >= 0) {
+            const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+#pragma unroll
+            for(int q = 0; q < 27; q++) {
+                const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+                atomicAdd(&out0[t], acc0[q]);
+                atomicAdd(&out1[t], acc1[q]);
+            }
+        }
+        p2g_end(a, T, b - sc.block_base);
+    }
+}
+
 // The elastic force of the particles k_p2g_pairs listed for the FP64 stress
 // route: -dt vol PF^T grad w added to the momentum of their 27 nodes.  Their
 // nodes lie in their block's tile, whose node blocks P2G already marked.
@@ -903,7 +1100,7 @@ int grid_stride_blocks(mpm_handle* h, int64_t n, int t)
 
 // Launch shapes the autotuner chooses among.
 const int kG2PThreads[] = {64, 128, 256};
-const char* const kP2GNames[] = {"cells", "interleaved", "pairs"};
+const char* const kP2GNames[] = {"cells", "interleaved", "pairs", "pairx"};
 
 int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult)
 {
@@ -1206,7 +1403,10 @@ int fast_p2g(mpm_handle* h, double dt, double)
     else if(f.p2g_variant == 1)
         k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
     else {
-        k_p2g_pairs<128><<<occupancy_ctas(h, (const void*)k_p2g_pairs<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
+        if(f.p2g_variant == 2)
+            k_p2g_pairs<128><<<occupancy_ctas(h, (const void*)k_p2g_pairs<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
+        else
+            k_p2g_pairx<128><<<occupancy_ctas(h, (const void*)k_p2g_pairx<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
         MPM_LAUNCHED(h, "k_p2g_pairs");
         k_p2g_fallback<<<h->sm_count, 128, 0, h->stream>>>(a);
     }
@@ -1334,7 +1534,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
     const bool timing = h->timing;
     h->timing = false;
     int rc = MPM_OK;
-    for(int variant = 0; variant < 3 && !rc; variant++)
+    for(int variant = 0; variant < 4 && !rc; variant++)
         for(int ti = 0; ti < 3 && !rc; ti++)
             for(int mult = 1; mult <= 2 && !rc; mult++) {
                 f.p2g_variant = variant;

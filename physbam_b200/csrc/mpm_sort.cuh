@@ -201,19 +201,38 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
         mine.store((epoch << 34) | (kFlagInclusive << 32) | tot, cuda::memory_order_relaxed);
     } else {
         mine.store((epoch << 34) | (kFlagAggregate << 32) | tot, cuda::memory_order_relaxed);
+        // Read kWindow predecessors at once: when every tile starts together,
+        // tile k walks about k/2 tiles back before it meets an inclusive
+        // prefix, so the walk's latency, not its work, is what costs.  Tile 0
+        // is always inclusive, so the walk stops at j = 0 at the latest.
+        constexpr int kWindow = 8;
         int64_t j = (int64_t)tile - 1;
         uint32_t spins = 0;
-        while(j >= 0) {
-            cuda::atomic_ref<uint64_t, cuda::thread_scope_device> other(status[j * kRadix + d]);
-            uint64_t w = other.load(cuda::memory_order_relaxed);
-            uint64_t flag = (w >> 34) == epoch ? (w >> 32) & 3u : 0u;
-            if(flag == 0) {
-                if(++spins > kSpinLimit) { atomicOr(err_flags, timeout_flag); break; }
-                continue;
+        bool done = false;
+        while(!done) {
+            uint64_t w[kWindow];
+#pragma unroll
+            for(int u = 0; u < kWindow; u++) {
+                w[u] = 0;
+                if(j - u >= 0) {
+                    cuda::atomic_ref<uint64_t, cuda::thread_scope_device> other(status[(j - u) * kRadix + d]);
+                    w[u] = other.load(cuda::memory_order_relaxed);
+                }
             }
-            excl += (uint32_t)w;
-            if(flag == kFlagInclusive) break;
-            j--;
+            int adv = 0;
+            bool stop = false;
+#pragma unroll
+            for(int u = 0; u < kWindow; u++) {
+                if(stop || j - u < 0) break;
+                const uint64_t flag = (w[u] >> 34) == epoch ? (w[u] >> 32) & 3u : 0u;
+                if(flag == 0) { stop = true; break; }     // not published yet: poll again from here
+                excl += (uint32_t)w[u];
+                adv++;
+                if(flag == kFlagInclusive) { done = true; stop = true; }
+            }
+            if(done) break;
+            if(adv == 0 && ++spins > kSpinLimit) { atomicOr(err_flags, timeout_flag); break; }
+            j -= adv;
         }
         mine.store((epoch << 34) | (kFlagInclusive << 32) | (excl + tot), cuda::memory_order_relaxed);
     }
