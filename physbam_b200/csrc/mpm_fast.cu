@@ -423,37 +423,6 @@ __global__ void __launch_bounds__(64) k_p2g_cells(FastArgs a)
     }
 }
 
-// P2G variant 1: one thread per particle, handed out round-robin over the
-// cells of the block (lane c of a round takes that cell's next particle), so
-// the lanes of one shared atomic hit different nodes.  Fewer registers than
-// variant 0, one shared atomic per node value per particle.
-template<int THREADS> __global__ void __launch_bounds__(THREADS) k_p2g_interleaved(FastArgs a)
-{
-    __shared__ P2GTile T;
-    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
-        const uint32_t b = a.active[w];
-        p2g_begin(a, T, b);
-        const uint32_t s = a.bstart[b], slots = T.maxc * 64u;
-        for(uint32_t q = threadIdx.x; q < slots; q += THREADS) {
-            const uint32_t c = q & 63u, r = q >> 6;
-            if(r >= T.ccount[c]) continue;
-            P2GParticle P;
-            p2g_particle(a, T.sc, a.perm[s + T.cstart[c] + r], P);
-            const int t0 = (((c >> 4)) * TE + ((c >> 2) & 3)) * TE + (c & 3);
-            p2g_nodes(P, [&](int qn, float m, float px, float py, float pz) {
-                const int ii = qn / 9, jj = (qn / 3) % 3, kk = qn % 3;
-                const int t = t0 + (ii * TE + jj) * TE + kk;
-                atomicAdd(&T.m[t], m);
-                atomicAdd(&T.x[t], px);
-                atomicAdd(&T.y[t], py);
-                atomicAdd(&T.z[t], pz);
-            });
-        }
-        p2g_end(a, T, b - T.sc.block_base);
-    }
-}
-
 // P2G variant 2: two lanes per contiguous range of the block's sorted
 // particles.  The ranges split the block evenly (no lane idles on a sparse
 // cell), and the two lanes of a pair split the four node quantities: the even
@@ -612,10 +581,19 @@ struct PairPrep {
     int cell;
 };
 
-__device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc, uint32_t j, bool odd, PairPrep& P)
+// Weights and separable factors of all four node quantities of the particle
+// at sorted position j (mass: Hx = m wx, Hy = Hz = 0).  A particle whose
+// stress needs the FP64 route is listed for k_p2g_fallback and contributes
+// mass and momentum here.
+struct P2GFactors {
+    float w[9];            // wx[3], wy[3], wz[3]
+    float mwx[3];          // mass factor m wx
+    PairSlot q[3];         // momentum components x, y, z
+};
+
+__device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneDev& sc, uint32_t j, P2GFactors& P)
 {
     const uint32_t i = a.perm[j];
-    P.cell = (int)(a.sorted_keys[j] & 63u);
     float X[3], V[3], F[9], B[9];
 #pragma unroll
     for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
@@ -624,7 +602,6 @@ __device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc,
     const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
     float S[9];
     if(!stress_fast(sc.model, F, at.z, at.w, S)) {
-        // the FP64 SVD route runs in k_p2g_fallback, which adds the force
         a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
 #pragma unroll
         for(int r = 0; r < 9; r++) S[r] = 0.f;
@@ -642,17 +619,30 @@ __device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc,
         dX[2][o] = sc.dmin[2] + (bz + (float)o) * sc.dx[2] - X[2];
     }
     const float Dm[3] = {4.f * sc.inv[0] * sc.inv[0] * m, 4.f * sc.inv[1] * sc.inv[1] * m, 4.f * sc.inv[2] * sc.inv[2] * m};
-    PairSlot q[3], qm;
 #pragma unroll
     for(int r = 0; r < 3; r++) {
         const float mBD[3] = {B[r] * Dm[0], B[r + 3] * Dm[1], B[r + 6] * Dm[2]};
         const float Sr[3] = {S[r] * sv, S[r + 3] * sv, S[r + 6] * sv};
-        pair_slot(wx, wy, wz, dX, m * V[r], mBD, Sr, q[r]);
+        pair_slot(wx, wy, wz, dX, m * V[r], mBD, Sr, P.q[r]);
     }
 #pragma unroll
-    for(int o = 0; o < 3; o++) { qm.Hx[o] = m * wx.w[o]; qm.Hy[o] = 0.f; qm.Hz[o] = 0.f; }
+    for(int o = 0; o < 3; o++) {
+        P.mwx[o] = m * wx.w[o];
+        P.w[o] = wx.w[o]; P.w[3 + o] = wy.w[o]; P.w[6 + o] = wz.w[o];
+    }
+}
+
+__device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc, uint32_t j, bool odd, PairPrep& P)
+{
+    P.cell = (int)(a.sorted_keys[j] & 63u);
+    P2GFactors G;
+    particle_factors(a, sc, j, G);
 #pragma unroll
-    for(int o = 0; o < 3; o++) { P.w[o] = wx.w[o]; P.w[3 + o] = wy.w[o]; P.w[6 + o] = wz.w[o]; }
+    for(int k = 0; k < 9; k++) P.w[k] = G.w[k];
+    PairSlot qm;
+#pragma unroll
+    for(int o = 0; o < 3; o++) { qm.Hx[o] = G.mwx[o]; qm.Hy[o] = 0.f; qm.Hz[o] = 0.f; }
+    const PairSlot* q = G.q;
     // even lane keeps (mass, x) and sends (y, z); odd lane the other way round
 #pragma unroll
     for(int o = 0; o < 3; o++) {
@@ -664,6 +654,7 @@ __device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc,
         P.keep1.Hz[o] = odd ? q[2].Hz[o] : q[0].Hz[o]; P.send1.Hz[o] = odd ? q[0].Hz[o] : q[2].Hz[o];
     }
 }
+
 
 __device__ __forceinline__ void pair_accumulate(const float* w, const PairSlot& q0, const PairSlot& q1, float* acc0, float* acc1)
 {
@@ -693,6 +684,49 @@ __device__ __forceinline__ void pair_flush(int cell, float* out0, float* out1, f
         atomicAdd(&out1[t], acc1[q]);
         acc0[q] = 0.f;
         acc1[q] = 0.f;
+    }
+}
+
+// P2G variant 1: one thread per particle, handed out round-robin over the
+// cells of the block (lane c of a round takes that cell's next particle), so
+// the lanes of one shared atomic hit different nodes.  No accumulators: the
+// 27 node values of all four quantities go straight to the shared tile, so
+// the kernel needs few registers and keeps many warps in flight, at the price
+// of four shared atomics per node.
+template<int THREADS> __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_p2g_interleaved(FastArgs a)
+{
+    __shared__ P2GTile T;
+    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
+    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
+        const uint32_t b = a.active[w];
+        p2g_begin(a, T, b);
+        const uint32_t s = a.bstart[b], slots = T.maxc * 64u;
+        for(uint32_t q = threadIdx.x; q < slots; q += THREADS) {
+            const uint32_t c = q & 63u, r = q >> 6;
+            if(r >= T.ccount[c]) continue;
+            P2GFactors P;
+            particle_factors(a, T.sc, s + T.cstart[c] + r, P);
+            const int t0 = ((c >> 4) * TE + ((c >> 2) & 3)) * TE + (c & 3);
+#pragma unroll
+            for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+                for(int jj = 0; jj < 3; jj++) {
+                    const float wxy = P.w[ii] * P.w[3 + jj], mxy = P.mwx[ii] * P.w[3 + jj];
+                    float A[3];
+#pragma unroll
+                    for(int r2 = 0; r2 < 3; r2++) A[r2] = fmaf(P.q[r2].Hx[ii], P.w[3 + jj], P.w[ii] * P.q[r2].Hy[jj]);
+#pragma unroll
+                    for(int kk = 0; kk < 3; kk++) {
+                        const int t = t0 + (ii * TE + jj) * TE + kk;
+                        const float wz = P.w[6 + kk];
+                        atomicAdd(&T.m[t], mxy * wz);
+                        atomicAdd(&T.x[t], fmaf(A[0], wz, wxy * P.q[0].Hz[kk]));
+                        atomicAdd(&T.y[t], fmaf(A[1], wz, wxy * P.q[1].Hz[kk]));
+                        atomicAdd(&T.z[t], fmaf(A[2], wz, wxy * P.q[2].Hz[kk]));
+                    }
+                }
+        }
+        p2g_end(a, T, b - T.sc.block_base);
     }
 }
 
@@ -1400,10 +1434,10 @@ int fast_p2g(mpm_handle* h, double dt, double)
     timer_end(h, slot);
     slot = timer_begin(h, "fast_p2g");
     if(f.p2g_variant == 0) k_p2g_cells<<<occupancy_ctas(h, (const void*)k_p2g_cells, 64, f.cta_mult), 64, 0, h->stream>>>(a);
-    else if(f.p2g_variant == 1)
-        k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
     else {
-        if(f.p2g_variant == 2)
+        if(f.p2g_variant == 1)
+            k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
+        else if(f.p2g_variant == 2)
             k_p2g_pairs<128><<<occupancy_ctas(h, (const void*)k_p2g_pairs<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
         else
             k_p2g_pairx<128><<<occupancy_ctas(h, (const void*)k_p2g_pairx<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
