@@ -56,7 +56,7 @@ struct FastArgs {
     const uint32_t* sorted_keys;
     uint32_t* keys_next;
     uint32_t *bstart, *bend, *active, *nb_flag, *nb_list, *counters;
-    uint32_t* fallback;   // sorted positions whose stress takes the FP64 route (P2G variants 1-3)
+    uint32_t* fallback;   // sorted positions whose stress takes the FP64 route (P2G variant 2)
     float4* acc;
     float4* vel;
     const SceneDev* scenes;
@@ -324,7 +324,6 @@ template<class FN> __device__ __forceinline__ void p2g_nodes(const P2GParticle& 
 struct P2GTile {
     float m[TN], x[TN], y[TN], z[TN];
     uint32_t ccount[64], cstart[64];
-    uint32_t ustart[65];   // work units (up to kUnit particles of one cell) before each cell
     uint32_t maxc;
     SceneDev sc;
     int work;
@@ -424,12 +423,12 @@ __global__ void __launch_bounds__(64) k_p2g_cells(FastArgs a)
     }
 }
 
-// P2G variant 2: two lanes per work unit (up to kUnit particles of one cell).
-// Units split the block finely (a sparse cell keeps few lanes busy for long),
-// and the two lanes of a pair split the four node quantities: the even lane
-// accumulates mass and x momentum, the odd lane y and z momentum, so each
+// P2G variant 2: two lanes per contiguous range of the block's sorted
+// particles.  The ranges split the block evenly (no lane idles on a sparse
+// cell), and the two lanes of a pair split the four node quantities: the even
+// lane accumulates mass and x momentum, the odd lane y and z momentum, so each
 // holds 54 accumulators instead of 108 and twice as many warps fit on an SM.
-// Accumulators go to the shared tile once per unit.
+// Accumulators go to the shared tile whenever the range moves to a new cell.
 //
 // Every quantity has the separable form (w = wx wy wz at node (i, j, k))
 //   q_node = Hx[i] wy[j] wz[k] + wx[i] Hy[j] wz[k] + wx[i] wy[j] Hz[k]
@@ -455,55 +454,6 @@ __device__ __forceinline__ void pair_slot(const Axis<float>& wx, const Axis<floa
     }
 }
 
-// Work units of the pair variants: each cell's particles in runs of up to
-// kUnit, so a unit never spans two cells and every lane flushes its
-// accumulators once per unit, at the same point of the code as the other lanes.
-constexpr int kUnit = 4;
-
-__device__ __forceinline__ void p2g_units(P2GTile& T)
-{
-    if(threadIdx.x < 32) {
-        const int c = threadIdx.x;
-        const uint32_t u0 = (T.ccount[2 * c] + kUnit - 1) / kUnit, u1 = (T.ccount[2 * c + 1] + kUnit - 1) / kUnit;
-        uint32_t x = u0 + u1;
-#pragma unroll
-        for(int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if(c >= o) x += y;
-        }
-        T.ustart[2 * c] = x - u0 - u1;
-        T.ustart[2 * c + 1] = x - u1;
-        if(c == 31) T.ustart[64] = x;
-    }
-    __syncthreads();
-}
-
-// The cell of unit u: the last cell whose first unit is at or before u (empty
-// cells own no units, so that cell is never empty).
-__device__ __forceinline__ int unit_cell(const P2GTile& T, uint32_t u)
-{
-    int lo = 0, hi = 63;
-#pragma unroll
-    for(int k = 0; k < 6; k++) {
-        const int mid = (lo + hi + 1) >> 1;
-        if(T.ustart[mid] <= u) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ void pair_flush(int cell, float* out0, float* out1, float* acc0, float* acc1)
-{
-    const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
-#pragma unroll
-    for(int q = 0; q < 27; q++) {
-        const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
-        atomicAdd(&out0[t], acc0[q]);
-        atomicAdd(&out1[t], acc1[q]);
-        acc0[q] = 0.f;
-        acc1[q] = 0.f;
-    }
-}
-
 template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_p2g_pairs(FastArgs a)
 {
     __shared__ P2GTile T;
@@ -513,20 +463,35 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
     constexpr int kPairs = THREADS / 2;
     for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
         const uint32_t b = a.active[w];
-        p2g_begin(a, T, b);
-        p2g_units(T);
+        stage_scene(a, a.block_scene[b], &T.sc);
+        for(int t = threadIdx.x; t < TN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+        __syncthreads();
         const SceneDev& sc = T.sc;
-        const uint32_t s = a.bstart[b], units = T.ustart[64];
+        const uint32_t s = a.bstart[b], e = a.bend[b];
+        const uint32_t per = (e - s + kPairs - 1) / kPairs;
+        const uint32_t j0 = s + pair * per, j1 = min(j0 + per, e);
         float* const out0 = odd ? T.y : T.m;
         float* const out1 = odd ? T.z : T.x;
         float acc0[27], acc1[27];
 #pragma unroll
         for(int q = 0; q < 27; q++) { acc0[q] = 0.f; acc1[q] = 0.f; }
-        for(uint32_t u = pair; u < units; u += kPairs) {
-            const int cell = unit_cell(T, u);
-            const uint32_t k0 = (u - T.ustart[cell]) * kUnit;
-            const uint32_t j0 = s + T.cstart[cell] + k0, j1 = j0 + min((uint32_t)kUnit, T.ccount[cell] - k0);
-            for(uint32_t j = j0; j < j1; j++) {
+        int cell = -1;
+        for(uint32_t j = j0; j < j1; j++) {
+            const int c = (int)(a.sorted_keys[j] & 63u);
+            if(c != cell) {
+                if(cell >= 0) {
+                    const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+#pragma unroll
+                    for(int q = 0; q < 27; q++) {
+                        const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+                        atomicAdd(&out0[t], acc0[q]);
+                        atomicAdd(&out1[t], acc1[q]);
+                        acc0[q] = 0.f;
+                        acc1[q] = 0.f;
+                    }
+                }
+                cell = c;
+            }
             const uint32_t i = a.perm[j];
             float X[3], F[9];
 #pragma unroll
@@ -590,14 +555,21 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
                         acc1[q] = fmaf(A1, wz.w[kk], fmaf(wxy, q1.Hz[kk], acc1[q]));
                     }
                 }
+        }
+        if(cell >= 0) {
+            const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+#pragma unroll
+            for(int q = 0; q < 27; q++) {
+                const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+                atomicAdd(&out0[t], acc0[q]);
+                atomicAdd(&out1[t], acc1[q]);
             }
-            pair_flush(cell, out0, out1, acc0, acc1);
         }
         p2g_end(a, T, b - sc.block_base);
     }
 }
 
-// P2G variant 3: as variant 2 (two lanes per work unit, the even lane holding
+// P2G variant 3: as variant 2 (two lanes per range, the even lane holding
 // mass and x momentum, the odd lane y and z), but the lanes share the
 // per-particle work: the even lane prepares particle j, the odd lane particle
 // j + 1 (stress, weights and the separable factors of all four quantities),
@@ -606,6 +578,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
 struct PairPrep {
     float w[9];            // wx[3], wy[3], wz[3]
     PairSlot keep0, keep1, send0, send1;
+    int cell;
 };
 
 // Weights and separable factors of all four node quantities of the particle
@@ -661,6 +634,7 @@ __device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneD
 
 __device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc, uint32_t j, bool odd, PairPrep& P)
 {
+    P.cell = (int)(a.sorted_keys[j] & 63u);
     P2GFactors G;
     particle_factors(a, sc, j, G);
 #pragma unroll
@@ -700,6 +674,18 @@ __device__ __forceinline__ void pair_accumulate(const float* w, const PairSlot& 
         }
 }
 
+__device__ __forceinline__ void pair_flush(int cell, float* out0, float* out1, float* acc0, float* acc1)
+{
+    const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+#pragma unroll
+    for(int q = 0; q < 27; q++) {
+        const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+        atomicAdd(&out0[t], acc0[q]);
+        atomicAdd(&out1[t], acc1[q]);
+        acc0[q] = 0.f;
+        acc1[q] = 0.f;
+    }
+}
 
 // P2G variant 1: one thread per particle, handed out round-robin over the
 // cells of the block (lane c of a round takes that cell's next particle), so
@@ -758,57 +744,88 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 384 / THREADS) 
     constexpr int kPairs = THREADS / 2;
     for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
         const uint32_t b = a.active[w];
-        p2g_begin(a, T, b);
-        p2g_units(T);
+        stage_scene(a, a.block_scene[b], &T.sc);
+        for(int t = threadIdx.x; t < TN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+        __syncthreads();
         const SceneDev& sc = T.sc;
-        const uint32_t s = a.bstart[b], units = T.ustart[64];
+        const uint32_t s = a.bstart[b], e = a.bend[b];
+        // ranges of an even length, so both lanes of a pair always have a particle but the last
+        const uint32_t per = ((e - s + kPairs - 1) / kPairs + 1) & ~1u;
+        const uint32_t j0 = s + pair * per, j1 = min(j0 + per, e);
         float* const out0 = odd ? T.y : T.m;
         float* const out1 = odd ? T.z : T.x;
         float acc0[27], acc1[27];
 #pragma unroll
         for(int q = 0; q < 27; q++) { acc0[q] = 0.f; acc1[q] = 0.f; }
-        for(uint32_t u = pair; u < units; u += kPairs) {
-            const int cell = unit_cell(T, u);
-            const uint32_t k0 = (u - T.ustart[cell]) * kUnit;
-            const uint32_t j0 = s + T.cstart[cell] + k0, j1 = j0 + min((uint32_t)kUnit, T.ccount[cell] - k0);
-            // both lanes of a pair run the same trip count
-            for(uint32_t j = j0; j < j1; j += 2) {
-                const bool have1 = j + 1 < j1;
-                PairPrep P;
-                if(!odd || have1) pair_prep(a, sc, j + (odd ? 1u : 0u), odd, P);
-                else {
+        int cell = -1;
+        // the pair's lanes run the same trip count: j0 and j1 are shared
+        for(uint32_t j = j0; j < j1; j += 2) {
+            const bool have1 = j + 1 < j1;
+            PairPrep P;
+            const bool mine = !odd || have1;
+            if(mine) pair_prep(a, sc, j + (odd ? 1u : 0u), odd, P);
+            else {
 #pragma unroll
-                    for(int k = 0; k < 9; k++) P.w[k] = 0.f;
+                for(int k = 0; k < 9; k++) P.w[k] = 0.f;
+                P.cell = -1;
+            }
+            // swap: partner's cell, weights and the factors of my quantities
+            PairPrep R;
+            R.cell = __shfl_xor_sync(pair_mask(), P.cell, 1);
+#pragma unroll
+            for(int k = 0; k < 9; k++) R.w[k] = shfl1(P.w[k]);
+#pragma unroll
+            for(int o = 0; o < 3; o++) {
+                R.keep0.Hx[o] = shfl1(P.send0.Hx[o]); R.keep0.Hy[o] = shfl1(P.send0.Hy[o]); R.keep0.Hz[o] = shfl1(P.send0.Hz[o]);
+                R.keep1.Hx[o] = shfl1(P.send1.Hx[o]); R.keep1.Hy[o] = shfl1(P.send1.Hy[o]); R.keep1.Hz[o] = shfl1(P.send1.Hz[o]);
+            }
+            // particle j first (the even lane's), then j + 1 (the odd lane's)
+            const int c_first = odd ? R.cell : P.cell, c_second = odd ? P.cell : R.cell;
+            {
+                if(c_first != cell) {
+                    if(cell >= 0) pair_flush(cell, out0, out1, acc0, acc1);
+                    cell = c_first;
                 }
-                // swap: partner's weights and the factors of my quantities
-                PairPrep R;
+                float wf[9];
 #pragma unroll
-                for(int k = 0; k < 9; k++) R.w[k] = shfl1(P.w[k]);
+                for(int k = 0; k < 9; k++) wf[k] = odd ? R.w[k] : P.w[k];
+                PairSlot f0, f1;
 #pragma unroll
                 for(int o = 0; o < 3; o++) {
-                    R.keep0.Hx[o] = shfl1(P.send0.Hx[o]); R.keep0.Hy[o] = shfl1(P.send0.Hy[o]); R.keep0.Hz[o] = shfl1(P.send0.Hz[o]);
-                    R.keep1.Hx[o] = shfl1(P.send1.Hx[o]); R.keep1.Hy[o] = shfl1(P.send1.Hy[o]); R.keep1.Hz[o] = shfl1(P.send1.Hz[o]);
+                    f0.Hx[o] = odd ? R.keep0.Hx[o] : P.keep0.Hx[o]; f0.Hy[o] = odd ? R.keep0.Hy[o] : P.keep0.Hy[o];
+                    f0.Hz[o] = odd ? R.keep0.Hz[o] : P.keep0.Hz[o];
+                    f1.Hx[o] = odd ? R.keep1.Hx[o] : P.keep1.Hx[o]; f1.Hy[o] = odd ? R.keep1.Hy[o] : P.keep1.Hy[o];
+                    f1.Hz[o] = odd ? R.keep1.Hz[o] : P.keep1.Hz[o];
                 }
-                if(have1) {
-                    pair_accumulate(P.w, P.keep0, P.keep1, acc0, acc1);
-                    pair_accumulate(R.w, R.keep0, R.keep1, acc0, acc1);
-                } else {
-                    // one particle left (the even lane's): the odd lane takes it from R
-                    float w1[9];
-                    PairSlot h0, h1;
-#pragma unroll
-                    for(int k = 0; k < 9; k++) w1[k] = odd ? R.w[k] : P.w[k];
-#pragma unroll
-                    for(int o = 0; o < 3; o++) {
-                        h0.Hx[o] = odd ? R.keep0.Hx[o] : P.keep0.Hx[o]; h0.Hy[o] = odd ? R.keep0.Hy[o] : P.keep0.Hy[o];
-                        h0.Hz[o] = odd ? R.keep0.Hz[o] : P.keep0.Hz[o];
-                        h1.Hx[o] = odd ? R.keep1.Hx[o] : P.keep1.Hx[o]; h1.Hy[o] = odd ? R.keep1.Hy[o] : P.keep1.Hy[o];
-                        h1.Hz[o] = odd ? R.keep1.Hz[o] : P.keep1.Hz[o];
-                    }
-                    pair_accumulate(w1, h0, h1, acc0, acc1);
-                }
+                pair_accumulate(wf, f0, f1, acc0, acc1);
             }
-            pair_flush(cell, out0, out1, acc0, acc1);
+            if(have1) {
+                if(c_second != cell) {
+                    pair_flush(cell, out0, out1, acc0, acc1);
+                    cell = c_second;
+                }
+                float ws[9];
+#pragma unroll
+                for(int k = 0; k < 9; k++) ws[k] = odd ? P.w[k] : R.w[k];
+                PairSlot g0, g1;
+#pragma unroll
+                for(int o = 0; o < 3; o++) {
+                    g0.Hx[o] = odd ? P.keep0.Hx[o] : R.keep0.Hx[o]; g0.Hy[o] = odd ? P.keep0.Hy[o] : R.keep0.Hy[o];
+                    g0.Hz[o] = odd ? P.keep0.Hz[o] : R.keep0.Hz[o];
+                    g1.Hx[o] = odd ? P.keep1.Hx[o] : R.keep1.Hx[o]; g1.Hy[o] = odd ? P.keep1.Hy[o] : R.keep1.Hy[o];
+                    g1.Hz[o] = odd ? P.keep1.Hz[o] : R.keep1.Hz[o];
+                }
+                pair_accumulate(ws, g0, g1, acc0, acc1);
+            }
+        }
+        if(cell >= 0) {
+            const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+#pragma unroll
+            for(int q = 0; q < 27; q++) {
+                const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+                atomicAdd(&out0[t], acc0[q]);
+                atomicAdd(&out1[t], acc1[q]);
+            }
         }
         p2g_end(a, T, b - sc.block_base);
     }
@@ -1406,7 +1423,7 @@ int fast_p2g(mpm_handle* h, double dt, double)
     int slot = timer_begin(h, "fast_sort");
     // sort the slot keys (f.keys, left intact for get_particles) into sorted_keys / perm
     cudaError_t e = mpm_sort::radix_sort(f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, n, f.key_bits,
-                                         f.sort_scratch, h->d_flags, MPM_FLAG_TIMEOUT, h->sm_count, h->stream);
+                                         f.sort_scratch, h->d_flags, MPM_FLAG_TIMEOUT, h->sm_count * 4, h->stream);
     if(e != cudaSuccess) return check_cuda(h, e, "radix_sort");
     timer_end(h, slot);
     FastArgs a = make_args(h, dt);
@@ -1619,7 +1636,7 @@ int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_
                mpm_sort::prepare())) rc = MPM_ERR_CUDA;
     if(!rc) {
         cudaMemcpyAsync(k, keys, b, cudaMemcpyHostToDevice, st);
-        if(mpm_sort::radix_sort(k, ko, vo, ka, va, n, bits, scratch, flags, MPM_FLAG_TIMEOUT, sms, st) != cudaSuccess)
+        if(mpm_sort::radix_sort(k, ko, vo, ka, va, n, bits, scratch, flags, MPM_FLAG_TIMEOUT, sms * 4, st) != cudaSuccess)
             rc = MPM_ERR_CUDA;
         else {
             unsigned fl = 0;

@@ -290,8 +290,7 @@ inline cudaError_t radix_sort(const uint32_t* keys, uint32_t* keys_out, uint32_t
     int64_t tiles = small ? tiles_for(n, kSmallTile) : tiles_for(n);
     cudaError_t e = cudaMemsetAsync(scratch, 0, kHistWords * sizeof(uint32_t), st);
     if(e != cudaSuccess) return e;
-    // few CTAs: each adds its histograms to the same few global words at the end
-    int hb = (int)((n + 8191) / 8192);
+    int hb = (int)((n + kThreads * 4 - 1) / (kThreads * 4));
     if(hb > hist_blocks) hb = hist_blocks;
     if(hb < 1) hb = 1;
     k_upfront_hist<<<hb, kThreads, 0, st>>>(keys, n, bits, scratch);
