@@ -165,15 +165,14 @@ def cpu_baseline_sample(scene, seconds_budget=20.0):
 
 def kernels_per_substep(scene, p2g_variant=0):
     """Our kernels launched per fast-path substep: the digit histograms, one
-    single-pass kernel per radix digit, ranges (+ invalid tail), p2g (+ its
-    FP64-stress kernel for the two-lanes-per-range variant), grid, g2p."""
+    single-pass kernel per radix digit, ranges (+ invalid tail), p2g, grid, g2p."""
     blocks = 1
     for c in scene.counts:
         blocks *= (c + 4 + 3) // 4
     bits = 6
     while (1 << bits) <= blocks * 64:
         bits += 1
-    return (bits + 7) // 8 + 5 + (1 if p2g_variant >= 2 else 0)
+    return (bits + 7) // 8 + 5
 
 
 def read_traffic(kernel, workload=WORKLOAD):

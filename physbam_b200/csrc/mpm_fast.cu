@@ -379,6 +379,53 @@ __device__ __forceinline__ void p2g_end(const FastArgs& a, P2GTile& T, uint32_t 
     }
 }
 
+// The elastic force of the particles the P2G variants 1-3 listed for the FP64
+// stress route: -dt vol PF^T grad w added to the momentum of their 27 nodes.
+// Their nodes lie in their block's tile, whose node blocks P2G already
+// marked.  The CTA of the P2G launch that finishes last does this, once every
+// other CTA has listed its particles.
+__device__ __noinline__ void p2g_fallback_force(const FastArgs& a, uint32_t k)
+{
+    const uint32_t j = a.fallback[k], i = a.perm[j];
+    const SceneDev& sc = a.scenes[a.block_scene[a.sorted_keys[j] >> 6]];
+    float X[3], F[9], S[9];
+#pragma unroll
+    for(int r = 0; r < 3; r++) X[r] = a.src[(C_X + r) * a.npad + i];
+#pragma unroll
+    for(int r = 0; r < 9; r++) F[r] = a.src[(C_F + r) * a.npad + i];
+    const float4 at = a.src_attr[i];
+    if(!stress_fp64(sc.model, F, at.z, at.w, S)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
+    const float sv = a.dt * at.y;
+    const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
+    const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
+    const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
+    for(int ii = 0; ii < 3; ii++)
+        for(int jj = 0; jj < 3; jj++)
+            for(int kk = 0; kk < 3; kk++) {
+                const float g0 = wx.dw[ii] * wy.w[jj] * wz.w[kk], g1 = wx.w[ii] * wy.dw[jj] * wz.w[kk],
+                            g2 = wx.w[ii] * wy.w[jj] * wz.dw[kk];
+                float f[3];
+#pragma unroll
+                for(int r = 0; r < 3; r++) f[r] = -sv * (S[r] * g0 + S[r + 3] * g1 + S[r + 6] * g2);
+                const int64_t q = node_index(sc, wx.base + MPM_GHOST + ii, wy.base + MPM_GHOST + jj, wz.base + MPM_GHOST + kk);
+                atomicAdd(&a.acc[q], make_float4(f[0], f[1], f[2], 0.f));
+            }
+}
+
+__device__ __forceinline__ void p2g_finish(const FastArgs& a, int* s_last)
+{
+    __syncthreads();
+    if(threadIdx.x == 0) {
+        __threadfence();
+        *s_last = atomicAdd(&a.counters[CNT_P2G_DONE], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if(!*s_last) return;
+    __threadfence();
+    const uint32_t count = *(volatile uint32_t*)&a.counters[CNT_FALLBACK];
+    for(uint32_t k = threadIdx.x; k < count; k += blockDim.x) p2g_fallback_force(a, k);
+}
+
 // P2G variant 0: one thread per cell of the block.  A thread walks the
 // particles of its cell (they share the 27 nodes), accumulates the node values
 // in registers, and adds them to the shared tile once per cell: 8x fewer
@@ -510,7 +557,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
             }
             float S[9];
             if(!stress_fast(sc.model, F, at.z, at.w, S)) {
-                // the FP64 SVD route runs in k_p2g_fallback, which adds this
+                // the FP64 SVD route runs in p2g_finish, which adds this
                 // particle's force; here it contributes mass and momentum only
                 if(!odd) a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
 #pragma unroll
@@ -567,6 +614,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
         }
         p2g_end(a, T, b - sc.block_base);
     }
+    p2g_finish(a, &T.work);
 }
 
 // P2G variant 3: as variant 2 (two lanes per range, the even lane holding
@@ -583,7 +631,7 @@ struct PairPrep {
 
 // Weights and separable factors of all four node quantities of the particle
 // at sorted position j (mass: Hx = m wx, Hy = Hz = 0).  A particle whose
-// stress needs the FP64 route is listed for k_p2g_fallback and contributes
+// stress needs the FP64 route is listed for p2g_finish and contributes
 // mass and momentum here.
 struct P2GFactors {
     float w[9];            // wx[3], wy[3], wz[3]
@@ -728,6 +776,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
         }
         p2g_end(a, T, b - T.sc.block_base);
     }
+    p2g_finish(a, &T.work);
 }
 
 // Swap with the other lane of the pair.  Only the pair takes part: pairs of
@@ -829,79 +878,78 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 384 / THREADS) 
         }
         p2g_end(a, T, b - sc.block_base);
     }
-}
-
-// The elastic force of the particles k_p2g_pairs listed for the FP64 stress
-// route: -dt vol PF^T grad w added to the momentum of their 27 nodes.  Their
-// nodes lie in their block's tile, whose node blocks P2G already marked.
-__global__ void k_p2g_fallback(FastArgs a)
-{
-    const uint32_t count = a.counters[CNT_FALLBACK];
-    for(uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-        const uint32_t j = a.fallback[k], i = a.perm[j];
-        const SceneDev& sc = a.scenes[a.block_scene[a.sorted_keys[j] >> 6]];
-        float X[3], F[9], S[9];
-#pragma unroll
-        for(int r = 0; r < 3; r++) X[r] = a.src[(C_X + r) * a.npad + i];
-#pragma unroll
-        for(int r = 0; r < 9; r++) F[r] = a.src[(C_F + r) * a.npad + i];
-        const float4 at = a.src_attr[i];
-        if(!stress_fp64(sc.model, F, at.z, at.w, S)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
-        const float sv = a.dt * at.y;
-        const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
-        const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
-        const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
-        for(int ii = 0; ii < 3; ii++)
-            for(int jj = 0; jj < 3; jj++)
-                for(int kk = 0; kk < 3; kk++) {
-                    const float g0 = wx.dw[ii] * wy.w[jj] * wz.w[kk], g1 = wx.w[ii] * wy.dw[jj] * wz.w[kk],
-                                g2 = wx.w[ii] * wy.w[jj] * wz.dw[kk];
-                    float f[3];
-#pragma unroll
-                    for(int r = 0; r < 3; r++) f[r] = -sv * (S[r] * g0 + S[r + 3] * g1 + S[r + 6] * g2);
-                    const int64_t q = node_index(sc, wx.base + MPM_GHOST + ii, wy.base + MPM_GHOST + jj, wz.base + MPM_GHOST + kk);
-                    atomicAdd(&a.acc[q], make_float4(f[0], f[1], f[2], 0.f));
-                }
-    }
+    p2g_finish(a, &T.work);
 }
 
 // One thread per node of the listed node blocks (4^3 nodes each, 64
-// consecutive threads), grid-stride: no barrier, no work counter.  A warp's
-// 32 nodes share a node block and so a scene record, read through L1.
+// consecutive threads), grid-stride with CTA-uniform trip counts.  Each group
+// of 64 threads (one node block) copies its scene record and collision
+// objects, rounded to float, into shared memory before use; a one-scene
+// handle does that once per CTA.
 __global__ void __launch_bounds__(256) k_grid(FastArgs a)
 {
+    constexpr int kGroups = 4;   // node blocks per CTA pass
+    __shared__ SceneDev s_sc[kGroups];
+    __shared__ DevObjectF s_obj[kGroups][MPM_MAX_OBJECTS];
+    __shared__ int s_scene[kGroups];
+    const int grp = threadIdx.x >> 6, t = threadIdx.x & 63;
     const uint64_t total = (uint64_t)a.counters[CNT_NODE_BLOCKS] * 64u;
-    for(uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total; g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t nb = a.nb_list[g >> 6];
-        const SceneDev& sc = a.scenes[a.nb_scene[nb]];
-        const uint32_t lnb = nb - sc.nb_base;
-        int nz = lnb % sc.NN[2], r = lnb / sc.NN[2], ny = r % sc.NN[1], nx = r / sc.NN[1];
-        int t = (int)(g & 63u);
-        int qx = 4 * nx + (t >> 4), qy = 4 * ny + ((t >> 2) & 3), qz = 4 * nz + (t & 3);
-        int64_t q = node_index(sc, qx, qy, qz);
-        float4 c = a.acc[q];
-        float4 o0 = make_float4(0, 0, 0, 0), o1 = make_float4(0, 0, 0, 0);
-        if(c.w != 0.f) {
-            float im = 1.f / c.w;
-            float V[3] = {c.x * im + a.dt * sc.gravity[0], c.y * im + a.dt * sc.gravity[1], c.z * im + a.dt * sc.gravity[2]};
-            float vn[3], vf[3];
-            if(sc.nobj) {
-                float X0[3] = {sc.dmin[0] + ((float)(qx - MPM_GHOST) + 0.5f) * sc.dx[0],
-                               sc.dmin[1] + ((float)(qy - MPM_GHOST) + 0.5f) * sc.dx[1],
-                               sc.dmin[2] + ((float)(qz - MPM_GHOST) + 0.5f) * sc.dx[2]};
-                float zero[3] = {0.f, 0.f, 0.f};
-                collide_node<float, 3>(a.objs + sc.obj_begin, sc.nobj, X0, zero, V, a.dt, vn, vf);
-            } else {
+    const uint64_t stride = (uint64_t)gridDim.x * 256u;
+    if(threadIdx.x < kGroups) s_scene[threadIdx.x] = -1;
+    __syncthreads();
+    for(uint64_t g0 = blockIdx.x * 256ull; g0 < total; g0 += stride) {
+        const uint64_t g = g0 + threadIdx.x;
+        const bool live = g < total;
+        const uint32_t nb = live ? a.nb_list[g >> 6] : 0u;
+        const int scene = live ? (int)a.nb_scene[nb] : s_scene[grp];
+        // restage when this group's scene changed (all 64 threads agree)
+        if(scene != s_scene[grp] && scene >= 0) {
+            constexpr int words = (int)(sizeof(SceneDev) / 4);
+            if(t < words) ((uint32_t*)&s_sc[grp])[t] = ((const uint32_t*)(a.scenes + scene))[t];
+            const SceneDev& gs = a.scenes[scene];
+            if(t < gs.nobj) {
+                const DevObject& o = a.objs[gs.obj_begin + t];
+                DevObjectF& f = s_obj[grp][t];
+                f.kind = o.kind;
+                f.type = o.type;
+                f.friction = (float)o.friction;
 #pragma unroll
-                for(int k = 0; k < 3; k++) vn[k] = vf[k] = V[k];
+                for(int k = 0; k < 3; k++) { f.a[k] = (float)o.a[k]; f.b[k] = (float)o.b[k]; }
             }
-            o0 = make_float4(vn[0], vn[1], vn[2], vf[0]);
-            o1 = make_float4(vf[1], vf[2], c.w, 0.f);
-            a.acc[q] = make_float4(0, 0, 0, 0);
         }
-        a.vel[2 * q] = o0;
-        a.vel[2 * q + 1] = o1;
-        if(t == 0) a.nb_flag[nb] = 0u;
+        __syncthreads();
+        if(t == 0 && live) s_scene[grp] = scene;
+        if(live) {
+            const SceneDev& sc = s_sc[grp];
+            const uint32_t lnb = nb - sc.nb_base;
+            int nz = lnb % sc.NN[2], r = lnb / sc.NN[2], ny = r % sc.NN[1], nx = r / sc.NN[1];
+            int qx = 4 * nx + (t >> 4), qy = 4 * ny + ((t >> 2) & 3), qz = 4 * nz + (t & 3);
+            int64_t q = node_index(sc, qx, qy, qz);
+            float4 c = a.acc[q];
+            float4 o0 = make_float4(0, 0, 0, 0), o1 = make_float4(0, 0, 0, 0);
+            if(c.w != 0.f) {
+                float im = 1.f / c.w;
+                float V[3] = {c.x * im + a.dt * sc.gravity[0], c.y * im + a.dt * sc.gravity[1], c.z * im + a.dt * sc.gravity[2]};
+                float vn[3], vf[3];
+                if(sc.nobj) {
+                    float X0[3] = {sc.dmin[0] + ((float)(qx - MPM_GHOST) + 0.5f) * sc.dx[0],
+                                   sc.dmin[1] + ((float)(qy - MPM_GHOST) + 0.5f) * sc.dx[1],
+                                   sc.dmin[2] + ((float)(qz - MPM_GHOST) + 0.5f) * sc.dx[2]};
+                    float zero[3] = {0.f, 0.f, 0.f};
+                    collide_node<float, 3>(s_obj[grp], sc.nobj, X0, zero, V, a.dt, vn, vf);
+                } else {
+#pragma unroll
+                    for(int k = 0; k < 3; k++) vn[k] = vf[k] = V[k];
+                }
+                o0 = make_float4(vn[0], vn[1], vn[2], vf[0]);
+                o1 = make_float4(vf[1], vf[2], c.w, 0.f);
+                a.acc[q] = make_float4(0, 0, 0, 0);
+            }
+            a.vel[2 * q] = o0;
+            a.vel[2 * q + 1] = o1;
+            if(t == 0) a.nb_flag[nb] = 0u;
+        }
+        __syncthreads();
     }
 }
 
@@ -1442,7 +1490,6 @@ int fast_p2g(mpm_handle* h, double dt, double)
         else
             k_p2g_pairx<128><<<occupancy_ctas(h, (const void*)k_p2g_pairx<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
         MPM_LAUNCHED(h, "k_p2g_pairs");
-        k_p2g_fallback<<<h->sm_count, 128, 0, h->stream>>>(a);
     }
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_p2g");

@@ -93,6 +93,7 @@ enum FastCounter {
     CNT_NODE_BLOCKS = 4,
     CNT_GRID_WORK = 5,
     CNT_FALLBACK = 6,
+    CNT_P2G_DONE = 7,
     CNT_COUNT = 8
 };
 

@@ -360,7 +360,15 @@ struct DevObject {
     double a[3], b[3];
 };
 
-template<class T, int d> __device__ T object_phi(const DevObject& o, const T* X)
+// The same object with its numbers rounded to float once (the FP32 path
+// rounds each of them to float where it uses them, so results are the same).
+struct DevObjectF {
+    int kind, type;
+    float friction;
+    float a[3], b[3];
+};
+
+template<class T, int d, class O> __device__ T object_phi(const O& o, const T* X)
 {
     if(o.kind == MPM_PLANE) {
         T s = 0;
@@ -386,7 +394,7 @@ template<class T, int d> __device__ T object_phi(const DevObject& o, const T* X)
     return mx;
 }
 
-template<class T, int d> __device__ void object_normal(const DevObject& o, const T* X, T* n)
+template<class T, int d, class O> __device__ void object_normal(const O& o, const T* X, T* n)
 {
     if(o.kind == MPM_PLANE) {
 #pragma unroll
@@ -438,7 +446,7 @@ template<class T, int d> __device__ void object_normal(const DevObject& o, const
 //
 // In: v0 (grid velocity after P2G), dv (dt/m f), node centre X0.
 // Out: vnew (velocity), vfric (velocity_friction_save).
-template<class T, int d> __device__ void collide_node(const DevObject* objs, int nobj, const T* X0,
+template<class T, int d, class O> __device__ void collide_node(const O* objs, int nobj, const T* X0,
     const T* v0, T* dv, T dt, T* vnew, T* vfric)
 {
     T dvb[3], nrm[MPM_MAX_OBJECTS][3];
@@ -448,14 +456,14 @@ template<class T, int d> __device__ void collide_node(const DevObject* objs, int
 #pragma unroll
     for(int a = 0; a < d; a++) dvb[a] = dv[a];
     for(int j = 0; j < nobj; j++) {
-        const DevObject& o = objs[j];
+        const O& o = objs[j];
+        const T phi0 = object_phi<T, d>(o, X0);
+        // stick and slip test only nodes that start inside the object
+        if((o.type == MPM_STICK || o.type == MPM_SLIP) && phi0 > 0) continue;
         T Vn[3], Xn[3];
 #pragma unroll
         for(int a = 0; a < d; a++) { Vn[a] = v0[a] + dv[a]; Xn[a] = X0[a] + dt * Vn[a]; }
-        T phi0 = object_phi<T, d>(o, X0);
         T phi = object_phi<T, d>(o, Xn) - fmin(phi0, (T)0);
-        if(o.type == MPM_STICK && phi0 > 0) continue;
-        if(o.type == MPM_SLIP && phi0 > 0) continue;
         if(o.type == MPM_SEPARATE && phi > (T)1e-15) continue;
         if(o.type != MPM_STICK && phi > (T)FLT_MAX) continue;
         T n[3];
