@@ -26,6 +26,7 @@
 // of the block it works on.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
