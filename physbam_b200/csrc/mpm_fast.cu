@@ -1478,7 +1478,7 @@ int fast_p2g(mpm_handle* h, double dt, double)
     FastArgs a = make_args(h, dt);
     slot = timer_begin(h, "fast_ranges");
     MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
-    k_ranges<<<std::min(grid_stride_blocks(h, n, 256), h->sm_count * 2), 256, 0, h->stream>>>(a);
+    k_ranges<<<grid_stride_blocks(h, n, 256), 256, 0, h->stream>>>(a);
     MPM_LAUNCHED(h, "k_ranges");
     timer_end(h, slot);
     slot = timer_begin(h, "fast_p2g");
