@@ -201,6 +201,46 @@ class MPM_DRIVER:
         self._keep = None
         self.n = n
 
+    def _native(self, arrays, n, what):
+        dtype = arrays[0].dtype
+        if dtype not in (np.float32, np.float64):
+            raise ValueError("%s: float32 or float64 arrays" % what)
+        d = self.dim
+        shapes = [(n, d), (n, d), (n, d * d), (n, d * d)] + [(n,)] * (len(arrays) - 4)
+        for arr, shp in zip(arrays, shapes):
+            if arr.dtype != dtype or arr.shape != shp or not arr.flags.c_contiguous:
+                raise ValueError("%s: arrays must be C-contiguous %s of shapes %s" % (what, dtype, shapes))
+        return FP64 if dtype == np.float64 else FP32
+
+    def set_particles_native(self, X, V, Fc, Bc, mass, volume, mu, lam, valid=None):
+        """Arrays already in the C-ABI (PhysBAM) layout, passed by pointer with no
+        host-side copy: X, V (n, d); Fc, Bc (n, d*d) with F[i + d*j] = F(i, j);
+        mass, volume, mu, lambda (n,); all one float dtype, C-contiguous.  With
+        page-locked (pinned) arrays the upload is a plain DMA."""
+        n = X.shape[0]
+        v = ParticlesView()
+        v.n, v.dtype, v.on_device = n, self._native([X, V, Fc, Bc, mass, volume, mu, lam], n, "set_particles_native"), 0
+        v.X, v.V, v.F, v.B, v.mass, v.volume, v.mu, v.lambda_ = [a.ctypes.data for a in (X, V, Fc, Bc, mass, volume, mu, lam)]
+        if valid is not None:
+            if valid.dtype != np.uint8 or valid.shape != (n,) or not valid.flags.c_contiguous:
+                raise ValueError("set_particles_native: valid must be a contiguous uint8 array of n")
+            v.valid = valid.ctypes.data
+        self._check(self.L.mpm_set_particles(self.h, ctypes.byref(v)), "mpm_set_particles")
+        self.n = n
+
+    def get_particles_native(self, X, V, Fc, Bc, valid=None):
+        """Fill caller arrays in the C-ABI layout (as set_particles_native) with
+        the particle state, in the caller's particle order, no host-side copy."""
+        n = self.n
+        v = ParticlesView()
+        v.n, v.dtype, v.on_device = n, self._native([X, V, Fc, Bc], n, "get_particles_native"), 0
+        v.X, v.V, v.F, v.B = X.ctypes.data, V.ctypes.data, Fc.ctypes.data, Bc.ctypes.data
+        if valid is not None:
+            if valid.dtype != np.uint8 or valid.shape != (n,) or not valid.flags.c_contiguous:
+                raise ValueError("get_particles_native: valid must be a contiguous uint8 array of n")
+            v.valid = valid.ctypes.data
+        self._check(self.L.mpm_get_particles(self.h, ctypes.byref(v)), "mpm_get_particles")
+
     def set_scene_particles(self, scene: Optional[S.Scene] = None, dtype=np.float64):
         s = scene or self.scene
         self.set_particles(s.X, s.V, s.F, s.B, s.mass, s.volume, s.mu, s.lam, dtype=dtype)

@@ -283,3 +283,32 @@ def test_grid_mass_conservation_full_size(cuda_device):
     total = float(np.sum(g["grid_m"]))
     assert abs(total - scene.mass.sum()) / scene.mass.sum() < 1e-5
     drv.close()
+
+
+def test_native_layout_round_trip(cuda_device):
+    """set_particles_native / get_particles_native (C-ABI layout, no host copies)
+    give the same state as the numpy-matrix calls."""
+    scene = S.small_3d(nsteps=3)
+    n = scene.n
+    col = lambda M: np.ascontiguousarray(np.swapaxes(M, 1, 2).reshape(n, 9), np.float32)
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    a = D().MPM_DRIVER(scene)
+    a.set_particles_native(f32(scene.X), f32(scene.V), col(scene.F), col(scene.B), f32(scene.mass),
+                           f32(scene.volume), f32(scene.mu), f32(scene.lam))
+    b = D().MPM_DRIVER(scene)
+    b.set_scene_particles(scene, dtype=np.float32)
+    for drv in (a, b):
+        drv.advance(scene.nsteps)
+    X, V = np.empty((n, 3), np.float32), np.empty((n, 3), np.float32)
+    Fc, Bc, valid = np.empty((n, 9), np.float32), np.empty((n, 9), np.float32), np.empty(n, np.uint8)
+    a.get_particles_native(X, V, Fc, Bc, valid)
+    ref = b.get_particles(dtype=np.float32)
+    np.testing.assert_array_equal(X, ref["X"])
+    np.testing.assert_array_equal(V, ref["V"])
+    np.testing.assert_array_equal(Fc.reshape(n, 3, 3).transpose(0, 2, 1), ref["F"])
+    np.testing.assert_array_equal(Bc.reshape(n, 3, 3).transpose(0, 2, 1), ref["B"])
+    np.testing.assert_array_equal(valid.astype(bool), ref["valid"])
+    with pytest.raises(ValueError):
+        a.get_particles_native(X, V, Fc.reshape(n, 3, 3), Bc, valid)
+    a.close()
+    b.close()
