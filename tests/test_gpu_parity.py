@@ -303,10 +303,12 @@ def test_native_layout_round_trip(cuda_device):
     Fc, Bc, valid = np.empty((n, 9), np.float32), np.empty((n, 9), np.float32), np.empty(n, np.uint8)
     a.get_particles_native(X, V, Fc, Bc, valid)
     ref = b.get_particles(dtype=np.float32)
-    np.testing.assert_array_equal(X, ref["X"])
-    np.testing.assert_array_equal(V, ref["V"])
-    np.testing.assert_array_equal(Fc.reshape(n, 3, 3).transpose(0, 2, 1), ref["F"])
-    np.testing.assert_array_equal(Bc.reshape(n, 3, 3).transpose(0, 2, 1), ref["B"])
+    # the two runs differ only in the order of float atomics
+    vmax = float(np.abs(ref["V"]).max())
+    assert rel(X, ref["X"], 1.0) < 1e-6
+    assert rel(V, ref["V"], vmax) < 1e-4
+    assert rel(Fc.reshape(n, 3, 3).transpose(0, 2, 1), ref["F"], 1.0) < 1e-5
+    assert rel(Bc.reshape(n, 3, 3).transpose(0, 2, 1), ref["B"], vmax / scene.dx) < 1e-4
     np.testing.assert_array_equal(valid.astype(bool), ref["valid"])
     with pytest.raises(ValueError):
         a.get_particles_native(X, V, Fc.reshape(n, 3, 3), Bc, valid)
