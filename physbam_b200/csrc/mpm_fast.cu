@@ -385,16 +385,19 @@ __device__ __forceinline__ void p2g_end(const FastArgs& a, P2GTile& T, uint32_t 
 // Their nodes lie in their block's tile, whose node blocks P2G already
 // marked.  The CTA of the P2G launch that finishes last does this, once every
 // other CTA has listed its particles.
-__device__ __noinline__ void p2g_fallback_force(const FastArgs& a, uint32_t k)
+// from_dst: the particle's state is its new one in slot j of the other
+// buffer (G2P fused with P2G), else the current one at perm[j].
+__device__ __noinline__ void p2g_fallback_force(const FastArgs& a, uint32_t k, bool from_dst)
 {
-    const uint32_t j = a.fallback[k], i = a.perm[j];
+    const uint32_t j = a.fallback[k], i = from_dst ? j : a.perm[j];
+    const float* const state = from_dst ? a.dst : a.src;
     const SceneDev& sc = a.scenes[a.block_scene[a.sorted_keys[j] >> 6]];
     float X[3], F[9], S[9];
 #pragma unroll
-    for(int r = 0; r < 3; r++) X[r] = a.src[(C_X + r) * a.npad + i];
+    for(int r = 0; r < 3; r++) X[r] = state[(C_X + r) * a.npad + i];
 #pragma unroll
-    for(int r = 0; r < 9; r++) F[r] = a.src[(C_F + r) * a.npad + i];
-    const float4 at = a.src_attr[i];
+    for(int r = 0; r < 9; r++) F[r] = state[(C_F + r) * a.npad + i];
+    const float4 at = from_dst ? a.dst_attr[j] : a.src_attr[i];
     if(!stress_fp64(sc.model, F, at.z, at.w, S)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
     const float sv = a.dt * at.y;
     const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
@@ -408,12 +411,17 @@ __device__ __noinline__ void p2g_fallback_force(const FastArgs& a, uint32_t k)
                 float f[3];
 #pragma unroll
                 for(int r = 0; r < 3; r++) f[r] = -sv * (S[r] * g0 + S[r + 3] * g1 + S[r + 6] * g2);
-                const int64_t q = node_index(sc, wx.base + MPM_GHOST + ii, wy.base + MPM_GHOST + jj, wz.base + MPM_GHOST + kk);
-                atomicAdd(&a.acc[q], make_float4(f[0], f[1], f[2], 0.f));
+                const int qx = wx.base + MPM_GHOST + ii, qy = wy.base + MPM_GHOST + jj, qz = wz.base + MPM_GHOST + kk;
+                atomicAdd(&a.acc[node_index(sc, qx, qy, qz)], make_float4(f[0], f[1], f[2], 0.f));
+                // after G2P the particle may sit outside the tile its block marked
+                if(from_dst) {
+                    const uint32_t nb = sc.nb_base + ((uint32_t)(qx >> 2) * sc.NN[1] + (qy >> 2)) * sc.NN[2] + (qz >> 2);
+                    if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.counters[CNT_NODE_BLOCKS], 1u)] = nb;
+                }
             }
 }
 
-__device__ __forceinline__ void p2g_finish(const FastArgs& a, int* s_last)
+__device__ __forceinline__ void p2g_finish(const FastArgs& a, int* s_last, bool from_dst = false)
 {
     __syncthreads();
     if(threadIdx.x == 0) {
@@ -424,7 +432,7 @@ __device__ __forceinline__ void p2g_finish(const FastArgs& a, int* s_last)
     if(!*s_last) return;
     __threadfence();
     const uint32_t count = *(volatile uint32_t*)&a.counters[CNT_FALLBACK];
-    for(uint32_t k = threadIdx.x; k < count; k += blockDim.x) p2g_fallback_force(a, k);
+    for(uint32_t k = threadIdx.x; k < count; k += blockDim.x) p2g_fallback_force(a, k, from_dst);
 }
 
 // P2G variant 0: one thread per cell of the block.  A thread walks the
@@ -638,17 +646,14 @@ struct P2GFactors {
     float w[9];            // wx[3], wy[3], wz[3]
     float mwx[3];          // mass factor m wx
     PairSlot q[3];         // momentum components x, y, z
+    int base[3];           // first stencil node - ghost, per axis
 };
 
-__device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneDev& sc, uint32_t j, P2GFactors& P)
+// Factors from a particle state held in registers (X, V, F, B, attributes);
+// `j` is the sorted position recorded if the stress needs the FP64 route.
+__device__ __forceinline__ void factors_from(const FastArgs& a, const SceneDev& sc, const float* X, const float* V,
+    const float* F, const float* B, const float4 at, uint32_t j, P2GFactors& P)
 {
-    const uint32_t i = a.perm[j];
-    float X[3], V[3], F[9], B[9];
-#pragma unroll
-    for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
-#pragma unroll
-    for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; B[r] = a.src[(C_B + r) * a.npad + i]; }
-    const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
     float S[9];
     if(!stress_fast(sc.model, F, at.z, at.w, S)) {
         a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
@@ -659,6 +664,7 @@ __device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneD
     const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
     const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
     const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
+    P.base[0] = wx.base; P.base[1] = wy.base; P.base[2] = wz.base;
     float dX[3][3];
     const float bx = (float)wx.base + 0.5f, by = (float)wy.base + 0.5f, bz = (float)wz.base + 0.5f;
 #pragma unroll
@@ -679,6 +685,37 @@ __device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneD
         P.mwx[o] = m * wx.w[o];
         P.w[o] = wx.w[o]; P.w[3 + o] = wy.w[o]; P.w[6 + o] = wz.w[o];
     }
+}
+
+__device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneDev& sc, uint32_t j, P2GFactors& P)
+{
+    const uint32_t i = a.perm[j];
+    float X[3], V[3], F[9], B[9];
+#pragma unroll
+    for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
+#pragma unroll
+    for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; B[r] = a.src[(C_B + r) * a.npad + i]; }
+    factors_from(a, sc, X, V, F, B, a.src_attr[i], j, P);   // attributes: mass, volume, mu, lambda
+}
+
+// The 27 node values of one particle: f(ii, jj, kk, mass, px, py, pz).
+template<class FN> __device__ __forceinline__ void factor_nodes(const P2GFactors& P, FN&& f)
+{
+#pragma unroll
+    for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+        for(int jj = 0; jj < 3; jj++) {
+            const float wxy = P.w[ii] * P.w[3 + jj], mxy = P.mwx[ii] * P.w[3 + jj];
+            float A[3];
+#pragma unroll
+            for(int r2 = 0; r2 < 3; r2++) A[r2] = fmaf(P.q[r2].Hx[ii], P.w[3 + jj], P.w[ii] * P.q[r2].Hy[jj]);
+#pragma unroll
+            for(int kk = 0; kk < 3; kk++) {
+                const float wz = P.w[6 + kk];
+                f(ii, jj, kk, mxy * wz, fmaf(A[0], wz, wxy * P.q[0].Hz[kk]), fmaf(A[1], wz, wxy * P.q[1].Hz[kk]),
+                  fmaf(A[2], wz, wxy * P.q[2].Hz[kk]));
+            }
+        }
 }
 
 __device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc, uint32_t j, bool odd, PairPrep& P)
@@ -756,24 +793,13 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
             P2GFactors P;
             particle_factors(a, T.sc, s + T.cstart[c] + r, P);
             const int t0 = ((c >> 4) * TE + ((c >> 2) & 3)) * TE + (c & 3);
-#pragma unroll
-            for(int ii = 0; ii < 3; ii++)
-#pragma unroll
-                for(int jj = 0; jj < 3; jj++) {
-                    const float wxy = P.w[ii] * P.w[3 + jj], mxy = P.mwx[ii] * P.w[3 + jj];
-                    float A[3];
-#pragma unroll
-                    for(int r2 = 0; r2 < 3; r2++) A[r2] = fmaf(P.q[r2].Hx[ii], P.w[3 + jj], P.w[ii] * P.q[r2].Hy[jj]);
-#pragma unroll
-                    for(int kk = 0; kk < 3; kk++) {
-                        const int t = t0 + (ii * TE + jj) * TE + kk;
-                        const float wz = P.w[6 + kk];
-                        atomicAdd(&T.m[t], mxy * wz);
-                        atomicAdd(&T.x[t], fmaf(A[0], wz, wxy * P.q[0].Hz[kk]));
-                        atomicAdd(&T.y[t], fmaf(A[1], wz, wxy * P.q[1].Hz[kk]));
-                        atomicAdd(&T.z[t], fmaf(A[2], wz, wxy * P.q[2].Hz[kk]));
-                    }
-                }
+            factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
+                const int t = t0 + (ii * TE + jj) * TE + kk;
+                atomicAdd(&T.m[t], m);
+                atomicAdd(&T.x[t], px);
+                atomicAdd(&T.y[t], py);
+                atomicAdd(&T.z[t], pz);
+            });
         }
         p2g_end(a, T, b - T.sc.block_base);
     }
@@ -964,13 +990,147 @@ __global__ void __launch_bounds__(256) k_grid(FastArgs a)
 // is non-zero only where the grid update changed v_fric against v_new (nodes
 // that met a collision object), so it is summed only for tiles holding such
 // nodes.
+// Stage the 6^3 tile of (v_new, v_fric, mass) of a particle block; true when
+// some node's friction velocity differs from its velocity (collided nodes).
+__device__ __forceinline__ bool g2p_stage(const FastArgs& a, const SceneDev& sc, float4* tv, int ox, int oy, int oz, int threads)
+{
+    int differs = 0;
+    for(int t = threadIdx.x; t < TN; t += threads) {
+        int qx = ox + t / (TE * TE), qy = oy + (t / TE) % TE, qz = oz + t % TE;
+        int64_t q = node_index(sc, qx, qy, qz);
+        float4 p0 = a.vel[2 * q], p1 = a.vel[2 * q + 1];
+        tv[2 * t] = p0;
+        tv[2 * t + 1] = p1;
+        differs |= (p0.w != p0.x) | (p1.x != p0.y) | (p1.y != p0.z);
+    }
+    return __syncthreads_or(differs) != 0;
+}
+
+// G2P of the particle at sorted position j against the staged tile `tv`
+// (origin node (ox, oy, oz)): writes its new state to slot j of the other
+// buffer and its next key; returns it in `o` for a fused P2G.
+struct G2PState {
+    float xn[3], Vf[3], Fn[9], Bn[9];
+    float4 at;
+    bool ok;
+};
+
+__device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& sc, const float4* tv, bool anti,
+    int ox, int oy, int oz, uint32_t j, G2PState& out)
+{
+    const float dt = a.dt;
+    const uint32_t i = a.perm[j];
+    float X[3], F[9];
+#pragma unroll
+    for(int k = 0; k < 3; k++) X[k] = a.src[(C_X + k) * a.npad + i];
+#pragma unroll
+    for(int k = 0; k < 9; k++) F[k] = a.src[(C_F + k) * a.npad + i];
+    const float4 at = a.src_attr[i];
+    const int pid = a.src_pid[i];
+    Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
+    Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
+    Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
+    const int t0 = ((wx.base + MPM_GHOST - ox) * TE + (wy.base + MPM_GHOST - oy)) * TE + (wz.base + MPM_GHOST - oz);
+    float dX[3], dY[3], wzd[3];
+#pragma unroll
+    for(int o = 0; o < 3; o++) {
+        dX[o] = sc.dmin[0] + ((float)(wx.base + o) + 0.5f) * sc.dx[0] - X[0];
+        dY[o] = sc.dmin[1] + ((float)(wy.base + o) + 0.5f) * sc.dx[1] - X[1];
+        wzd[o] = wz.w[o] * (sc.dmin[2] + ((float)(wz.base + o) + 0.5f) * sc.dx[2] - X[2]);
+    }
+    float* const Vf = out.Vf;
+    Vf[0] = Vf[1] = Vf[2] = 0.f;
+    float Vp[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Bv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    float K01 = 0, K02 = 0, K12 = 0;
+#pragma unroll
+    for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+        for(int jj = 0; jj < 3; jj++) {
+            float Sw[3] = {0, 0, 0}, Sd[3] = {0, 0, 0}, Tw[3] = {0, 0, 0}, Td[3] = {0, 0, 0};
+            float k01 = 0, k02 = 0, k12 = 0;
+#pragma unroll
+            for(int kk = 0; kk < 3; kk++) {
+                const int t = t0 + (ii * TE + jj) * TE + kk;
+                const float4 p0 = tv[2 * t], p1 = tv[2 * t + 1];
+                const float vn[3] = {p0.x, p0.y, p0.z}, vf[3] = {p0.w, p1.x, p1.y};
+#pragma unroll
+                for(int r = 0; r < 3; r++) {
+                    Sw[r] += vn[r] * wz.w[kk];
+                    Sd[r] += vn[r] * wz.dw[kk];
+                    Tw[r] += vf[r] * wz.w[kk];
+                    Td[r] += vf[r] * wzd[kk];
+                }
+                if(anti) {
+                    k01 += wz.w[kk] * (vf[0] * vn[1] - vf[1] * vn[0]);
+                    k02 += wz.w[kk] * (vf[0] * vn[2] - vf[2] * vn[0]);
+                    k12 += wz.w[kk] * (vf[1] * vn[2] - vf[2] * vn[1]);
+                }
+            }
+            const float wxy = wx.w[ii] * wy.w[jj], gx0 = wx.dw[ii] * wy.w[jj], gy0 = wx.w[ii] * wy.dw[jj];
+            K01 += wxy * k01;
+            K02 += wxy * k02;
+            K12 += wxy * k12;
+            const float wxX = wxy * dX[ii], wxY = wxy * dY[jj];
+#pragma unroll
+            for(int r = 0; r < 3; r++) {
+                Vp[r] += wxy * Sw[r];
+                G[r] += gx0 * Sw[r];
+                G[r + 3] += gy0 * Sw[r];
+                G[r + 6] += wxy * Sd[r];
+                Vf[r] += wxy * Tw[r];
+                Bv[r] += wxX * Tw[r];
+                Bv[r + 3] += wxY * Tw[r];
+                Bv[r + 6] += wxy * Td[r];
+            }
+        }
+    // F <- (I + dt grad v) F
+    float* const Fn = out.Fn;
+#pragma unroll
+    for(int c = 0; c < 3; c++)
+#pragma unroll
+        for(int r = 0; r < 3; r++)
+            Fn[r + 3 * c] = F[r + 3 * c] + dt * (G[r] * F[3 * c] + G[r + 3] * F[3 * c + 1] + G[r + 6] * F[3 * c + 2]);
+    float* const xn = out.xn;
+#pragma unroll
+    for(int k = 0; k < 3; k++) xn[k] = X[k] + dt * Vp[k];
+    const float h = 0.5f * dt;
+    const float A01 = h * (K01 - (Vf[0] * Vp[1] - Vp[0] * Vf[1]));
+    const float A02 = h * (K02 - (Vf[0] * Vp[2] - Vp[0] * Vf[2]));
+    const float A12 = h * (K12 - (Vf[1] * Vp[2] - Vp[1] * Vf[2]));
+    const float Bn[9] = {Bv[0], Bv[1] - A01, Bv[2] - A02,
+                         Bv[3] + A01, Bv[4], Bv[5] - A12,
+                         Bv[6] + A02, Bv[7] + A12, Bv[8]};
+    bool ok = true;
+#pragma unroll
+    for(int k = 0; k < 3; k++) {
+        float eps = FLT_EPSILON * 4.f * (sc.dmax[k] - sc.dmin[k]);
+        if(!(xn[k] >= sc.dmin[k] + eps && xn[k] <= sc.dmax[k] - eps)) ok = false;
+    }
+    bool finite = true;
+#pragma unroll
+    for(int k = 0; k < 9; k++) finite = finite && isfinite(Fn[k]);
+    finite = finite && isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]);
+    if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); ok = false; }
+    const uint32_t key = ok ? cell_key(sc, xn) : SENTINEL;
+#pragma unroll
+    for(int k = 0; k < 3; k++) { a.dst[(C_X + k) * a.npad + j] = xn[k]; a.dst[(C_V + k) * a.npad + j] = Vf[k]; }
+#pragma unroll
+    for(int k = 0; k < 9; k++) { a.dst[(C_F + k) * a.npad + j] = Fn[k]; a.dst[(C_B + k) * a.npad + j] = Bn[k]; }
+    a.dst_attr[j] = at;
+    a.dst_pid[j] = pid;
+    a.keys_next[j] = key;
+#pragma unroll
+    for(int k = 0; k < 9; k++) out.Bn[k] = Bn[k];
+    out.at = at;
+    out.ok = ok;
+}
+
 template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
 {
     __shared__ float4 tv[2 * TN];
     __shared__ int s_work;
     __shared__ SceneDev s_sc;
     const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    const float dt = a.dt;
     for(int w = next_work(&a.counters[CNT_G2P_WORK], &s_work); w < (int)nblocks; w = next_work(&a.counters[CNT_G2P_WORK], &s_work)) {
         const uint32_t b = a.active[w];
         stage_scene(a, a.block_scene[b], &s_sc);
@@ -979,118 +1139,126 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
         int bx, by, bz;
         block_coords(sc, b - sc.block_base, bx, by, bz);
         const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;
-        int differs = 0;
-        for(int t = threadIdx.x; t < TN; t += THREADS) {
-            int qx = ox + t / (TE * TE), qy = oy + (t / TE) % TE, qz = oz + t % TE;
-            int64_t q = node_index(sc, qx, qy, qz);
-            float4 p0 = a.vel[2 * q], p1 = a.vel[2 * q + 1];
-            tv[2 * t] = p0;
-            tv[2 * t + 1] = p1;
-            differs |= (p0.w != p0.x) | (p1.x != p0.y) | (p1.y != p0.z);
-        }
-        const bool anti = __syncthreads_or(differs) != 0;
+        const bool anti = g2p_stage(a, sc, tv, ox, oy, oz, THREADS);
         const uint32_t s = a.bstart[b], e = a.bend[b];
         for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
-            const uint32_t i = a.perm[j];
-            float X[3], F[9];
-#pragma unroll
-            for(int k = 0; k < 3; k++) X[k] = a.src[(C_X + k) * a.npad + i];
-#pragma unroll
-            for(int k = 0; k < 9; k++) F[k] = a.src[(C_F + k) * a.npad + i];
-            const float4 at = a.src_attr[i];
-            const int pid = a.src_pid[i];
-            Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
-            Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
-            Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
-            const int t0 = ((wx.base + MPM_GHOST - ox) * TE + (wy.base + MPM_GHOST - oy)) * TE + (wz.base + MPM_GHOST - oz);
-            float dX[3], dY[3], wzd[3];
-#pragma unroll
-            for(int o = 0; o < 3; o++) {
-                dX[o] = sc.dmin[0] + ((float)(wx.base + o) + 0.5f) * sc.dx[0] - X[0];
-                dY[o] = sc.dmin[1] + ((float)(wy.base + o) + 0.5f) * sc.dx[1] - X[1];
-                wzd[o] = wz.w[o] * (sc.dmin[2] + ((float)(wz.base + o) + 0.5f) * sc.dx[2] - X[2]);
-            }
-            float Vp[3] = {0, 0, 0}, Vf[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Bv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            float K01 = 0, K02 = 0, K12 = 0;
-#pragma unroll
-            for(int ii = 0; ii < 3; ii++)
-#pragma unroll
-                for(int jj = 0; jj < 3; jj++) {
-                    float Sw[3] = {0, 0, 0}, Sd[3] = {0, 0, 0}, Tw[3] = {0, 0, 0}, Td[3] = {0, 0, 0};
-                    float k01 = 0, k02 = 0, k12 = 0;
-#pragma unroll
-                    for(int kk = 0; kk < 3; kk++) {
-                        const int t = t0 + (ii * TE + jj) * TE + kk;
-                        const float4 p0 = tv[2 * t], p1 = tv[2 * t + 1];
-                        const float vn[3] = {p0.x, p0.y, p0.z}, vf[3] = {p0.w, p1.x, p1.y};
-#pragma unroll
-                        for(int r = 0; r < 3; r++) {
-                            Sw[r] += vn[r] * wz.w[kk];
-                            Sd[r] += vn[r] * wz.dw[kk];
-                            Tw[r] += vf[r] * wz.w[kk];
-                            Td[r] += vf[r] * wzd[kk];
-                        }
-                        if(anti) {
-                            k01 += wz.w[kk] * (vf[0] * vn[1] - vf[1] * vn[0]);
-                            k02 += wz.w[kk] * (vf[0] * vn[2] - vf[2] * vn[0]);
-                            k12 += wz.w[kk] * (vf[1] * vn[2] - vf[2] * vn[1]);
-                        }
-                    }
-                    const float wxy = wx.w[ii] * wy.w[jj], gx0 = wx.dw[ii] * wy.w[jj], gy0 = wx.w[ii] * wy.dw[jj];
-                    K01 += wxy * k01;
-                    K02 += wxy * k02;
-                    K12 += wxy * k12;
-                    const float wxX = wxy * dX[ii], wxY = wxy * dY[jj];
-#pragma unroll
-                    for(int r = 0; r < 3; r++) {
-                        Vp[r] += wxy * Sw[r];
-                        G[r] += gx0 * Sw[r];
-                        G[r + 3] += gy0 * Sw[r];
-                        G[r + 6] += wxy * Sd[r];
-                        Vf[r] += wxy * Tw[r];
-                        Bv[r] += wxX * Tw[r];
-                        Bv[r + 3] += wxY * Tw[r];
-                        Bv[r + 6] += wxy * Td[r];
-                    }
-                }
-            // F <- (I + dt grad v) F
-            float Fn[9];
-#pragma unroll
-            for(int c = 0; c < 3; c++)
-#pragma unroll
-                for(int r = 0; r < 3; r++)
-                    Fn[r + 3 * c] = F[r + 3 * c] + dt * (G[r] * F[3 * c] + G[r + 3] * F[3 * c + 1] + G[r + 6] * F[3 * c + 2]);
-            float xn[3];
-#pragma unroll
-            for(int k = 0; k < 3; k++) xn[k] = X[k] + dt * Vp[k];
-            const float h = 0.5f * dt;
-            const float A01 = h * (K01 - (Vf[0] * Vp[1] - Vp[0] * Vf[1]));
-            const float A02 = h * (K02 - (Vf[0] * Vp[2] - Vp[0] * Vf[2]));
-            const float A12 = h * (K12 - (Vf[1] * Vp[2] - Vp[1] * Vf[2]));
-            const float Bn[9] = {Bv[0], Bv[1] - A01, Bv[2] - A02,
-                                 Bv[3] + A01, Bv[4], Bv[5] - A12,
-                                 Bv[6] + A02, Bv[7] + A12, Bv[8]};
-            bool ok = true;
-#pragma unroll
-            for(int k = 0; k < 3; k++) {
-                float eps = FLT_EPSILON * 4.f * (sc.dmax[k] - sc.dmin[k]);
-                if(!(xn[k] >= sc.dmin[k] + eps && xn[k] <= sc.dmax[k] - eps)) ok = false;
-            }
-            bool finite = true;
-#pragma unroll
-            for(int k = 0; k < 9; k++) finite = finite && isfinite(Fn[k]);
-            finite = finite && isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]);
-            if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); ok = false; }
-            const uint32_t key = ok ? cell_key(sc, xn) : SENTINEL;
-#pragma unroll
-            for(int k = 0; k < 3; k++) { a.dst[(C_X + k) * a.npad + j] = xn[k]; a.dst[(C_V + k) * a.npad + j] = Vf[k]; }
-#pragma unroll
-            for(int k = 0; k < 9; k++) { a.dst[(C_F + k) * a.npad + j] = Fn[k]; a.dst[(C_B + k) * a.npad + j] = Bn[k]; }
-            a.dst_attr[j] = at;
-            a.dst_pid[j] = pid;
-            a.keys_next[j] = key;
+            G2PState o;
+            g2p_particle(a, sc, tv, anti, ox, oy, oz, j, o);
         }
     }
+}
+
+// G2P of substep n fused with P2G of substep n + 1 (used by mpm_advance when
+// substeps run back to back): a thread finishes a particle's G2P, keeps the new
+// state in registers and scatters it at once into the accumulator of the next
+// grid, so the particle state is read once per substep instead of twice and
+// the separate P2G launch goes away.  The scatter goes to an 8^3 shared tile
+// around the particle block (its 6^3 stencil tile grown by one node on each
+// side): a particle that moved at most one cell stays inside it (the CFL
+// condition keeps |v| dt below a cell); one that moved further adds its 27 node
+// values straight to the global accumulator.  Particles are handed out
+// round-robin over the block's cells, as in the interleaved P2G, so the lanes
+// of one shared atomic hit different nodes.
+constexpr int TE2 = BS + 4;                 // grown tile edge in nodes
+constexpr int TN2 = TE2 * TE2 * TE2;        // 512 nodes
+
+struct FusedTile {
+    float4 tv[2 * TN];                      // G2P: (v_new, v_fric, mass) of the 6^3 tile
+    float m[TN2], x[TN2], y[TN2], z[TN2];   // P2G of the next substep, 8^3 tile
+    uint32_t ccount[64], cstart[64];
+    uint32_t maxc;
+    uint32_t nbmark[27];                    // node blocks around the particle block that got mass
+    SceneDev sc;
+    int work;
+};
+
+__device__ __forceinline__ void mark_node_block(const FastArgs& a, const SceneDev& sc, int nx, int ny, int nz)
+{
+    const uint32_t nb = sc.nb_base + ((uint32_t)nx * sc.NN[1] + ny) * sc.NN[2] + nz;
+    if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.counters[CNT_NODE_BLOCKS], 1u)] = nb;
+}
+
+template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p2g(FastArgs a)
+{
+    __shared__ FusedTile T;
+    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
+    for(int w = next_work(&a.counters[CNT_G2P_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_G2P_WORK], &T.work)) {
+        const uint32_t b = a.active[w];
+        stage_scene(a, a.block_scene[b], &T.sc);
+        for(int t = threadIdx.x; t < TN2; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+        if(threadIdx.x < 64) T.ccount[threadIdx.x] = 0;
+        if(threadIdx.x < 27) T.nbmark[threadIdx.x] = 0;
+        __syncthreads();
+        const SceneDev& sc = T.sc;
+        int bx, by, bz;
+        block_coords(sc, b - sc.block_base, bx, by, bz);
+        const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;
+        const uint32_t s = a.bstart[b], e = a.bend[b];
+        for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) atomicAdd(&T.ccount[a.sorted_keys[j] & 63u], 1u);
+        const bool anti = g2p_stage(a, sc, T.tv, ox, oy, oz, THREADS);   // synchronises
+        if(threadIdx.x < 32) {
+            const int c = threadIdx.x;
+            uint32_t c0 = T.ccount[2 * c], c1 = T.ccount[2 * c + 1];
+            uint32_t sum = c0 + c1, x = sum, mx = c0 > c1 ? c0 : c1;
+#pragma unroll
+            for(int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if(c >= o) x += y;
+                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            }
+            T.cstart[2 * c] = x - sum;
+            T.cstart[2 * c + 1] = x - sum + c0;
+            if(c == 0) T.maxc = mx;
+        }
+        __syncthreads();
+        const uint32_t slots = T.maxc * 64u;
+        for(uint32_t q = threadIdx.x; q < slots; q += THREADS) {
+            const uint32_t c = q & 63u, r = q >> 6;
+            if(r >= T.ccount[c]) continue;
+            const uint32_t j = s + T.cstart[c] + r;
+            G2PState g;
+            g2p_particle(a, sc, T.tv, anti, ox, oy, oz, j, g);
+            if(!g.ok) continue;
+            P2GFactors P;
+            factors_from(a, sc, g.xn, g.Vf, g.Fn, g.Bn, g.at, j, P);
+            // first stencil node relative to the grown tile's origin (ox - 1, oy - 1, oz - 1)
+            const int sx = P.base[0] + MPM_GHOST - ox + 1, sy = P.base[1] + MPM_GHOST - oy + 1, sz = P.base[2] + MPM_GHOST - oz + 1;
+            if(sx >= 0 && sx <= TE2 - 3 && sy >= 0 && sy <= TE2 - 3 && sz >= 0 && sz <= TE2 - 3) {
+                const int t0 = (sx * TE2 + sy) * TE2 + sz;
+                factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
+                    const int t = t0 + (ii * TE2 + jj) * TE2 + kk;
+                    atomicAdd(&T.m[t], m);
+                    atomicAdd(&T.x[t], px);
+                    atomicAdd(&T.y[t], py);
+                    atomicAdd(&T.z[t], pz);
+                });
+            } else {
+                const int qx0 = P.base[0] + MPM_GHOST, qy0 = P.base[1] + MPM_GHOST, qz0 = P.base[2] + MPM_GHOST;
+                factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
+                    const int qx = qx0 + ii, qy = qy0 + jj, qz = qz0 + kk;
+                    atomicAdd(&a.acc[node_index(sc, qx, qy, qz)], make_float4(px, py, pz, m));
+                    mark_node_block(a, sc, qx >> 2, qy >> 2, qz >> 2);
+                });
+            }
+        }
+        __syncthreads();
+        // flush the grown tile; nodes with mass mark their node block
+        for(int t = threadIdx.x; t < TN2; t += THREADS) {
+            const float mm = T.m[t];
+            if(mm != 0.f) {
+                const int tx = t / (TE2 * TE2), ty = (t / TE2) % TE2, tz = t % TE2;
+                const int qx = ox - 1 + tx, qy = oy - 1 + ty, qz = oz - 1 + tz;
+                atomicAdd(&a.acc[node_index(sc, qx, qy, qz)], make_float4(T.x[t], T.y[t], T.z[t], mm));
+                T.nbmark[((qx >> 2) - bx + 1) * 9 + ((qy >> 2) - by + 1) * 3 + ((qz >> 2) - bz + 1)] = 1u;
+            }
+        }
+        __syncthreads();
+        if(threadIdx.x < 27 && T.nbmark[threadIdx.x]) {
+            const int k = threadIdx.x;
+            mark_node_block(a, sc, bx - 1 + k / 9, by - 1 + (k / 3) % 3, bz - 1 + k % 3);
+        }
+    }
+    p2g_finish(a, &T.work, true);
 }
 
 // Reference layout <-> sorted SoA
@@ -1183,7 +1351,7 @@ int grid_stride_blocks(mpm_handle* h, int64_t n, int t)
 
 // Launch shapes the autotuner chooses among.
 const int kG2PThreads[] = {64, 128, 256};
-const char* const kP2GNames[] = {"cells", "interleaved", "pairs", "pairx"};
+const char* const kP2GNames[] = {"cells", "interleaved", "pairs", "pairx", "fused"};
 
 int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult)
 {
@@ -1463,12 +1631,13 @@ int fast_get_particles(mpm_handle* h, mpm_particles_view* v)
 }
 
 // sort + ranges + tail copy + P2G (with fused stress and gravity)
-int fast_p2g(mpm_handle* h, double dt, double)
+// Sort the keys, then block ranges and the active list.  `counters` words
+// [0, first_kept) are cleared first (the whole set for a standalone P2G; the
+// fused loop keeps the node-block count its grid update and mpm_get_grid read).
+static int fast_sort_ranges(mpm_handle* h, double dt, int cleared)
 {
     FastState& f = h->fast;
-    if(!f.keys_ready) return set_error(h, MPM_ERR_STATE, "particles not set");
-    int64_t n = f.n;
-    if(!n) return MPM_OK;
+    const int64_t n = f.n;
     int slot = timer_begin(h, "fast_sort");
     // sort the slot keys (f.keys, left intact for get_particles) into sorted_keys / perm
     cudaError_t e = mpm_sort::radix_sort(f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, n, f.key_bits,
@@ -1477,14 +1646,26 @@ int fast_p2g(mpm_handle* h, double dt, double)
     timer_end(h, slot);
     FastArgs a = make_args(h, dt);
     slot = timer_begin(h, "fast_ranges");
-    MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, cleared * sizeof(uint32_t), h->stream));
     k_ranges<<<grid_stride_blocks(h, n, 256), 256, 0, h->stream>>>(a);
     MPM_LAUNCHED(h, "k_ranges");
     timer_end(h, slot);
-    slot = timer_begin(h, "fast_p2g");
+    return MPM_OK;
+}
+
+int fast_p2g(mpm_handle* h, double dt, double)
+{
+    FastState& f = h->fast;
+    if(!f.keys_ready) return set_error(h, MPM_ERR_STATE, "particles not set");
+    if(!f.n) return MPM_OK;
+    int rc = fast_sort_ranges(h, dt, CNT_COUNT);
+    if(rc) return rc;
+    FastArgs a = make_args(h, dt);
+    int slot = timer_begin(h, "fast_p2g");
     if(f.p2g_variant == 0) k_p2g_cells<<<occupancy_ctas(h, (const void*)k_p2g_cells, 64, f.cta_mult), 64, 0, h->stream>>>(a);
     else {
-        if(f.p2g_variant == 1)
+        // the fused mode's first P2G of an mpm_advance call is the interleaved one
+        if(f.p2g_variant == 1 || f.p2g_variant == MPM_P2G_FUSED)
             k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
         else if(f.p2g_variant == 2)
             k_p2g_pairs<128><<<occupancy_ctas(h, (const void*)k_p2g_pairs<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
@@ -1495,6 +1676,34 @@ int fast_p2g(mpm_handle* h, double dt, double)
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_p2g");
     return MPM_OK;
+}
+
+// Fused loop segment: G2P of this substep with P2G of the next (k_g2p2g), then
+// the next substep's sort and ranges.  Its grid update (fast_forces) runs
+// between the two.
+int fast_g2p2g(mpm_handle* h, double dt)
+{
+    FastState& f = h->fast;
+    if(!f.n) return MPM_OK;
+    FastArgs a = make_args(h, dt);
+    int slot = timer_begin(h, "fast_g2p2g");
+    // node-block count, fallback list and finish counter of the next P2G
+    MPM_CUDA(h, cudaMemsetAsync(f.counters + CNT_NODE_BLOCKS, 0, (CNT_COUNT - CNT_NODE_BLOCKS) * sizeof(uint32_t), h->stream));
+    switch(f.g2p_threads) {
+        case 64: k_g2p2g<64><<<occupancy_ctas(h, (const void*)k_g2p2g<64>, 64, f.cta_mult), 64, 0, h->stream>>>(a); break;
+        case 256: k_g2p2g<256><<<occupancy_ctas(h, (const void*)k_g2p2g<256>, 256, f.cta_mult), 256, 0, h->stream>>>(a); break;
+        default: k_g2p2g<128><<<occupancy_ctas(h, (const void*)k_g2p2g<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a); break;
+    }
+    timer_end(h, slot);
+    MPM_LAUNCHED(h, "k_g2p2g");
+    f.cur = 1 - f.cur;
+    return MPM_OK;
+}
+
+int fast_resort(mpm_handle* h, double dt)
+{
+    if(!h->fast.n) return MPM_OK;
+    return fast_sort_ranges(h, dt, CNT_NODE_BLOCKS);
 }
 
 int fast_forces(mpm_handle* h, double dt, double)
@@ -1616,7 +1825,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
     const bool timing = h->timing;
     h->timing = false;
     int rc = MPM_OK;
-    for(int variant = 0; variant < 4 && !rc; variant++)
+    for(int variant = 0; variant <= MPM_P2G_FUSED && !rc; variant++)
         for(int ti = 0; ti < 3 && !rc; ti++)
             for(int mult = 1; mult <= 2 && !rc; mult++) {
                 f.p2g_variant = variant;
@@ -1628,11 +1837,22 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
                 cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
-                if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_g2p(h, dt, 0))) break;
-                cudaEventRecord(e0, h->stream);
-                for(int s = 0; s < substeps && !rc; s++)
-                    if(!(rc = fast_p2g(h, dt, 0)) && !(rc = fast_forces(h, dt, 0))) rc = fast_g2p(h, dt, 0);
-                cudaEventRecord(e1, h->stream);
+                if(variant == MPM_P2G_FUSED) {
+                    // the fused loop: one P2G, then G2P2G + grid + sort per substep
+                    if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0))) break;
+                    if((rc = fast_g2p2g(h, dt)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_resort(h, dt))) break;
+                    cudaEventRecord(e0, h->stream);
+                    for(int s = 0; s < substeps && !rc; s++)
+                        if(!(rc = fast_g2p2g(h, dt)) && !(rc = fast_forces(h, dt, 0))) rc = fast_resort(h, dt);
+                    cudaEventRecord(e1, h->stream);
+                    if(!rc) rc = fast_g2p(h, dt, 0);   // leaves the grid accumulator empty
+                } else {
+                    if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_g2p(h, dt, 0))) break;
+                    cudaEventRecord(e0, h->stream);
+                    for(int s = 0; s < substeps && !rc; s++)
+                        if(!(rc = fast_p2g(h, dt, 0)) && !(rc = fast_forces(h, dt, 0))) rc = fast_g2p(h, dt, 0);
+                    cudaEventRecord(e1, h->stream);
+                }
                 if(cudaEventSynchronize(e1) != cudaSuccess) { rc = check_cuda(h, cudaGetLastError(), "autotune"); break; }
                 float ms = 0;
                 cudaEventElapsedTime(&ms, e0, e1);
