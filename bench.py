@@ -443,11 +443,8 @@ def profile_case(args, D, S):
     drv.advance(args.warmup)
     drv.synchronize()
     drv.set_timing(True)
-    if drv.get_launch_shape()[0] == D.P2G_FUSED:
-        drv.advance(args.steps)          # the fused loop runs inside mpm_advance only
-    else:
-        for _ in range(args.steps):
-            drv.Advance_One_Time_Step()
+    for _ in range(args.steps):
+        drv.Advance_One_Time_Step()
     drv.synchronize()
     kt = drv.get_timing()
     drv.close()

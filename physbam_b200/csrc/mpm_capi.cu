@@ -88,43 +88,34 @@ static int read_flags(mpm_handle* h)
 
 static int release_graph(mpm_handle* h)
 {
-    for(auto& seg: h->graphs)
-        for(cudaGraphExec_t& g: seg) {
-            if(g) cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
+    for(cudaGraphExec_t& g: h->graphs) {
+        if(g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
     h->graph_dt = 0;
     return MPM_OK;
 }
 
-// Enqueue one segment of the substep loop (see mpm_handle::graphs).
-static int enqueue_segment(mpm_handle* h, int seg, double dt, double time)
+// One substep: the three phases back to back.
+static int enqueue_substep(mpm_handle* h, double dt, double time)
 {
-    int rc = MPM_OK;
-    switch(seg) {
-        case 0:
-            if(!(rc = mpm_particle_to_grid(h, dt, time)) && !(rc = mpm_apply_forces(h, dt, time)))
-                rc = mpm_grid_to_particle(h, dt, time);
-            return rc;
-        case 1: if(!(rc = fast_p2g(h, dt, time))) rc = fast_forces(h, dt, time); return rc;
-        case 2:
-            if(!(rc = fast_g2p2g(h, dt)) && !(rc = fast_forces(h, dt, time))) rc = fast_resort(h, dt);
-            return rc;
-        default: return fast_g2p(h, dt, time);
-    }
+    int rc = mpm_particle_to_grid(h, dt, time);
+    if(!rc && !(rc = mpm_apply_forces(h, dt, time))) rc = mpm_grid_to_particle(h, dt, time);
+    return rc;
 }
 
-// Run a segment from its captured graph (captured on first use), or eagerly
-// when per-kernel timing is on (events cannot live inside a graph).
-static int run_segment(mpm_handle* h, int seg, double dt, double time)
+// Run a substep from its captured graph (captured on first use), or eagerly
+// when per-kernel timing is on (events cannot live inside a graph).  The fast
+// path alternates its particle buffers, so it keeps one graph per parity.
+static int run_substep(mpm_handle* h, double dt, double time)
 {
-    if(h->timing) return enqueue_segment(h, seg, dt, time);
+    if(h->timing) return enqueue_substep(h, dt, time);
     const int par = fast(h) ? h->fast.cur : 0;
-    cudaGraphExec_t& ge = h->graphs[seg][par];
+    cudaGraphExec_t& ge = h->graphs[par];
     if(!ge) {
         cudaGraph_t g;
         MPM_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        int crc = enqueue_segment(h, seg, dt, time);
+        int crc = enqueue_substep(h, dt, time);
         cudaError_t e = cudaStreamEndCapture(h->stream, &g);
         if(fast(h)) h->fast.cur = par;     // capture executed nothing
         if(crc) { if(e == cudaSuccess) cudaGraphDestroy(g); return crc; }
@@ -135,8 +126,7 @@ static int run_segment(mpm_handle* h, int seg, double dt, double time)
         h->graph_dt = dt;
     }
     MPM_CUDA(h, cudaGraphLaunch(ge, h->stream));
-    // segments 0, 2 and 3 end with a G2P, which swaps the particle buffers
-    if(fast(h) && seg != 1) h->fast.cur = 1 - par;
+    if(fast(h)) h->fast.cur = 1 - par;
     return MPM_OK;
 }
 
@@ -338,19 +328,9 @@ int mpm_advance(mpm_handle* h, double dt, double time, int nsteps)
     int rc = check_dt(h, dt);
     if(rc) return rc;
     if(nsteps < 0) return set_error(h, MPM_ERR_ARG, "nsteps < 0");
-    // One captured graph per segment (run eagerly when per-kernel timing is on); the fast path alternates its particle
-    // buffers, so it keeps one graph per buffer parity.
     if(h->graph_dt != dt) release_graph(h);
-    if(!nsteps) return MPM_OK;
-    if(fast(h) && h->fast.p2g_variant == MPM_P2G_FUSED) {
-        // P2G + grid, then (G2P2G + grid + sort) per further substep, then G2P
-        if((rc = run_segment(h, 1, dt, time))) return rc;
-        for(int s = 1; s < nsteps; s++)
-            if((rc = run_segment(h, 2, dt, time + s * dt))) return rc;
-        return run_segment(h, 3, dt, time);
-    }
     for(int s = 0; s < nsteps; s++)
-        if((rc = run_segment(h, 0, dt, time + s * dt))) return rc;
+        if((rc = run_substep(h, dt, time + s * dt))) return rc;
     return MPM_OK;
 }
 
@@ -412,7 +392,7 @@ int mpm_set_launch_shape(mpm_handle* h, int p2g_variant, int g2p_threads, int ct
 {
     if(!h) return MPM_ERR_ARG;
     if(!fast(h)) return set_error(h, MPM_ERR_ARG, "launch shapes belong to the fast path");
-    if(p2g_variant < MPM_P2G_CELLS || p2g_variant > MPM_P2G_FUSED) return set_error(h, MPM_ERR_ARG, "unknown P2G variant");
+    if(p2g_variant < MPM_P2G_CELLS || p2g_variant > MPM_P2G_PAIRX) return set_error(h, MPM_ERR_ARG, "unknown P2G variant");
     if(g2p_threads != 64 && g2p_threads != 128 && g2p_threads != 256) return set_error(h, MPM_ERR_ARG, "G2P threads: 64, 128 or 256");
     if(cta_mult != 1 && cta_mult != 2) return set_error(h, MPM_ERR_ARG, "CTA multiplier: 1 or 2");
     release_graph(h);

@@ -385,19 +385,16 @@ __device__ __forceinline__ void p2g_end(const FastArgs& a, P2GTile& T, uint32_t 
 // Their nodes lie in their block's tile, whose node blocks P2G already
 // marked.  The CTA of the P2G launch that finishes last does this, once every
 // other CTA has listed its particles.
-// from_dst: the particle's state is its new one in slot j of the other
-// buffer (G2P fused with P2G), else the current one at perm[j].
-__device__ __noinline__ void p2g_fallback_force(const FastArgs& a, uint32_t k, bool from_dst)
+__device__ __noinline__ void p2g_fallback_force(const FastArgs& a, uint32_t k)
 {
-    const uint32_t j = a.fallback[k], i = from_dst ? j : a.perm[j];
-    const float* const state = from_dst ? a.dst : a.src;
+    const uint32_t j = a.fallback[k], i = a.perm[j];
     const SceneDev& sc = a.scenes[a.block_scene[a.sorted_keys[j] >> 6]];
     float X[3], F[9], S[9];
 #pragma unroll
-    for(int r = 0; r < 3; r++) X[r] = state[(C_X + r) * a.npad + i];
+    for(int r = 0; r < 3; r++) X[r] = a.src[(C_X + r) * a.npad + i];
 #pragma unroll
-    for(int r = 0; r < 9; r++) F[r] = state[(C_F + r) * a.npad + i];
-    const float4 at = from_dst ? a.dst_attr[j] : a.src_attr[i];
+    for(int r = 0; r < 9; r++) F[r] = a.src[(C_F + r) * a.npad + i];
+    const float4 at = a.src_attr[i];
     if(!stress_fp64(sc.model, F, at.z, at.w, S)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
     const float sv = a.dt * at.y;
     const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
@@ -413,15 +410,10 @@ __device__ __noinline__ void p2g_fallback_force(const FastArgs& a, uint32_t k, b
                 for(int r = 0; r < 3; r++) f[r] = -sv * (S[r] * g0 + S[r + 3] * g1 + S[r + 6] * g2);
                 const int qx = wx.base + MPM_GHOST + ii, qy = wy.base + MPM_GHOST + jj, qz = wz.base + MPM_GHOST + kk;
                 atomicAdd(&a.acc[node_index(sc, qx, qy, qz)], make_float4(f[0], f[1], f[2], 0.f));
-                // after G2P the particle may sit outside the tile its block marked
-                if(from_dst) {
-                    const uint32_t nb = sc.nb_base + ((uint32_t)(qx >> 2) * sc.NN[1] + (qy >> 2)) * sc.NN[2] + (qz >> 2);
-                    if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.counters[CNT_NODE_BLOCKS], 1u)] = nb;
-                }
             }
 }
 
-__device__ __forceinline__ void p2g_finish(const FastArgs& a, int* s_last, bool from_dst = false)
+__device__ __forceinline__ void p2g_finish(const FastArgs& a, int* s_last)
 {
     __syncthreads();
     if(threadIdx.x == 0) {
@@ -432,7 +424,7 @@ __device__ __forceinline__ void p2g_finish(const FastArgs& a, int* s_last, bool 
     if(!*s_last) return;
     __threadfence();
     const uint32_t count = *(volatile uint32_t*)&a.counters[CNT_FALLBACK];
-    for(uint32_t k = threadIdx.x; k < count; k += blockDim.x) p2g_fallback_force(a, k, from_dst);
+    for(uint32_t k = threadIdx.x; k < count; k += blockDim.x) p2g_fallback_force(a, k);
 }
 
 // P2G variant 0: one thread per cell of the block.  A thread walks the
@@ -1008,7 +1000,7 @@ __device__ __forceinline__ bool g2p_stage(const FastArgs& a, const SceneDev& sc,
 
 // G2P of the particle at sorted position j against the staged tile `tv`
 // (origin node (ox, oy, oz)): writes its new state to slot j of the other
-// buffer and its next key; returns it in `o` for a fused P2G.
+// buffer and its next key; also returns it in `out`.
 struct G2PState {
     float xn[3], Vf[3], Fn[9], Bn[9];
     float4 at;
@@ -1148,119 +1140,6 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
     }
 }
 
-// G2P of substep n fused with P2G of substep n + 1 (used by mpm_advance when
-// substeps run back to back): a thread finishes a particle's G2P, keeps the new
-// state in registers and scatters it at once into the accumulator of the next
-// grid, so the particle state is read once per substep instead of twice and
-// the separate P2G launch goes away.  The scatter goes to an 8^3 shared tile
-// around the particle block (its 6^3 stencil tile grown by one node on each
-// side): a particle that moved at most one cell stays inside it (the CFL
-// condition keeps |v| dt below a cell); one that moved further adds its 27 node
-// values straight to the global accumulator.  Particles are handed out
-// round-robin over the block's cells, as in the interleaved P2G, so the lanes
-// of one shared atomic hit different nodes.
-constexpr int TE2 = BS + 4;                 // grown tile edge in nodes
-constexpr int TN2 = TE2 * TE2 * TE2;        // 512 nodes
-
-struct FusedTile {
-    float4 tv[2 * TN];                      // G2P: (v_new, v_fric, mass) of the 6^3 tile
-    float m[TN2], x[TN2], y[TN2], z[TN2];   // P2G of the next substep, 8^3 tile
-    uint32_t ccount[64], cstart[64];
-    uint32_t maxc;
-    uint32_t nbmark[27];                    // node blocks around the particle block that got mass
-    SceneDev sc;
-    int work;
-};
-
-__device__ __forceinline__ void mark_node_block(const FastArgs& a, const SceneDev& sc, int nx, int ny, int nz)
-{
-    const uint32_t nb = sc.nb_base + ((uint32_t)nx * sc.NN[1] + ny) * sc.NN[2] + nz;
-    if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.counters[CNT_NODE_BLOCKS], 1u)] = nb;
-}
-
-template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p2g(FastArgs a)
-{
-    __shared__ FusedTile T;
-    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    for(int w = next_work(&a.counters[CNT_G2P_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_G2P_WORK], &T.work)) {
-        const uint32_t b = a.active[w];
-        stage_scene(a, a.block_scene[b], &T.sc);
-        for(int t = threadIdx.x; t < TN2; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
-        if(threadIdx.x < 64) T.ccount[threadIdx.x] = 0;
-        if(threadIdx.x < 27) T.nbmark[threadIdx.x] = 0;
-        __syncthreads();
-        const SceneDev& sc = T.sc;
-        int bx, by, bz;
-        block_coords(sc, b - sc.block_base, bx, by, bz);
-        const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;
-        const uint32_t s = a.bstart[b], e = a.bend[b];
-        for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) atomicAdd(&T.ccount[a.sorted_keys[j] & 63u], 1u);
-        const bool anti = g2p_stage(a, sc, T.tv, ox, oy, oz, THREADS);   // synchronises
-        if(threadIdx.x < 32) {
-            const int c = threadIdx.x;
-            uint32_t c0 = T.ccount[2 * c], c1 = T.ccount[2 * c + 1];
-            uint32_t sum = c0 + c1, x = sum, mx = c0 > c1 ? c0 : c1;
-#pragma unroll
-            for(int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-                if(c >= o) x += y;
-                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            }
-            T.cstart[2 * c] = x - sum;
-            T.cstart[2 * c + 1] = x - sum + c0;
-            if(c == 0) T.maxc = mx;
-        }
-        __syncthreads();
-        const uint32_t slots = T.maxc * 64u;
-        for(uint32_t q = threadIdx.x; q < slots; q += THREADS) {
-            const uint32_t c = q & 63u, r = q >> 6;
-            if(r >= T.ccount[c]) continue;
-            const uint32_t j = s + T.cstart[c] + r;
-            G2PState g;
-            g2p_particle(a, sc, T.tv, anti, ox, oy, oz, j, g);
-            if(!g.ok) continue;
-            P2GFactors P;
-            factors_from(a, sc, g.xn, g.Vf, g.Fn, g.Bn, g.at, j, P);
-            // first stencil node relative to the grown tile's origin (ox - 1, oy - 1, oz - 1)
-            const int sx = P.base[0] + MPM_GHOST - ox + 1, sy = P.base[1] + MPM_GHOST - oy + 1, sz = P.base[2] + MPM_GHOST - oz + 1;
-            if(sx >= 0 && sx <= TE2 - 3 && sy >= 0 && sy <= TE2 - 3 && sz >= 0 && sz <= TE2 - 3) {
-                const int t0 = (sx * TE2 + sy) * TE2 + sz;
-                factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
-                    const int t = t0 + (ii * TE2 + jj) * TE2 + kk;
-                    atomicAdd(&T.m[t], m);
-                    atomicAdd(&T.x[t], px);
-                    atomicAdd(&T.y[t], py);
-                    atomicAdd(&T.z[t], pz);
-                });
-            } else {
-                const int qx0 = P.base[0] + MPM_GHOST, qy0 = P.base[1] + MPM_GHOST, qz0 = P.base[2] + MPM_GHOST;
-                factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
-                    const int qx = qx0 + ii, qy = qy0 + jj, qz = qz0 + kk;
-                    atomicAdd(&a.acc[node_index(sc, qx, qy, qz)], make_float4(px, py, pz, m));
-                    mark_node_block(a, sc, qx >> 2, qy >> 2, qz >> 2);
-                });
-            }
-        }
-        __syncthreads();
-        // flush the grown tile; nodes with mass mark their node block
-        for(int t = threadIdx.x; t < TN2; t += THREADS) {
-            const float mm = T.m[t];
-            if(mm != 0.f) {
-                const int tx = t / (TE2 * TE2), ty = (t / TE2) % TE2, tz = t % TE2;
-                const int qx = ox - 1 + tx, qy = oy - 1 + ty, qz = oz - 1 + tz;
-                atomicAdd(&a.acc[node_index(sc, qx, qy, qz)], make_float4(T.x[t], T.y[t], T.z[t], mm));
-                T.nbmark[((qx >> 2) - bx + 1) * 9 + ((qy >> 2) - by + 1) * 3 + ((qz >> 2) - bz + 1)] = 1u;
-            }
-        }
-        __syncthreads();
-        if(threadIdx.x < 27 && T.nbmark[threadIdx.x]) {
-            const int k = threadIdx.x;
-            mark_node_block(a, sc, bx - 1 + k / 9, by - 1 + (k / 3) % 3, bz - 1 + k % 3);
-        }
-    }
-    p2g_finish(a, &T.work, true);
-}
-
 // Reference layout <-> sorted SoA
 template<class T> __global__ void k_scatter_in(FastArgs a, const T* X, const T* V, const T* F, const T* B, const T* m,
     const T* vol, const T* mu, const T* la, const uint8_t* valid, uint8_t* valid_slot)
@@ -1351,7 +1230,7 @@ int grid_stride_blocks(mpm_handle* h, int64_t n, int t)
 
 // Launch shapes the autotuner chooses among.
 const int kG2PThreads[] = {64, 128, 256};
-const char* const kP2GNames[] = {"cells", "interleaved", "pairs", "pairx", "fused"};
+const char* const kP2GNames[] = {"cells", "interleaved", "pairs", "pairx"};
 
 int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult)
 {
@@ -1631,9 +1510,8 @@ int fast_get_particles(mpm_handle* h, mpm_particles_view* v)
 }
 
 // sort + ranges + tail copy + P2G (with fused stress and gravity)
-// Sort the keys, then block ranges and the active list.  `counters` words
-// [0, first_kept) are cleared first (the whole set for a standalone P2G; the
-// fused loop keeps the node-block count its grid update and mpm_get_grid read).
+// Sort the keys, then block ranges and the active list; the first `cleared`
+// words of `counters` are zeroed before the ranges kernel counts into them.
 static int fast_sort_ranges(mpm_handle* h, double dt, int cleared)
 {
     FastState& f = h->fast;
@@ -1664,8 +1542,7 @@ int fast_p2g(mpm_handle* h, double dt, double)
     int slot = timer_begin(h, "fast_p2g");
     if(f.p2g_variant == 0) k_p2g_cells<<<occupancy_ctas(h, (const void*)k_p2g_cells, 64, f.cta_mult), 64, 0, h->stream>>>(a);
     else {
-        // the fused mode's first P2G of an mpm_advance call is the interleaved one
-        if(f.p2g_variant == 1 || f.p2g_variant == MPM_P2G_FUSED)
+        if(f.p2g_variant == 1)
             k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
         else if(f.p2g_variant == 2)
             k_p2g_pairs<128><<<occupancy_ctas(h, (const void*)k_p2g_pairs<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
@@ -1676,34 +1553,6 @@ int fast_p2g(mpm_handle* h, double dt, double)
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_p2g");
     return MPM_OK;
-}
-
-// Fused loop segment: G2P of this substep with P2G of the next (k_g2p2g), then
-// the next substep's sort and ranges.  Its grid update (fast_forces) runs
-// between the two.
-int fast_g2p2g(mpm_handle* h, double dt)
-{
-    FastState& f = h->fast;
-    if(!f.n) return MPM_OK;
-    FastArgs a = make_args(h, dt);
-    int slot = timer_begin(h, "fast_g2p2g");
-    // node-block count, fallback list and finish counter of the next P2G
-    MPM_CUDA(h, cudaMemsetAsync(f.counters + CNT_NODE_BLOCKS, 0, (CNT_COUNT - CNT_NODE_BLOCKS) * sizeof(uint32_t), h->stream));
-    switch(f.g2p_threads) {
-        case 64: k_g2p2g<64><<<occupancy_ctas(h, (const void*)k_g2p2g<64>, 64, f.cta_mult), 64, 0, h->stream>>>(a); break;
-        case 256: k_g2p2g<256><<<occupancy_ctas(h, (const void*)k_g2p2g<256>, 256, f.cta_mult), 256, 0, h->stream>>>(a); break;
-        default: k_g2p2g<128><<<occupancy_ctas(h, (const void*)k_g2p2g<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a); break;
-    }
-    timer_end(h, slot);
-    MPM_LAUNCHED(h, "k_g2p2g");
-    f.cur = 1 - f.cur;
-    return MPM_OK;
-}
-
-int fast_resort(mpm_handle* h, double dt)
-{
-    if(!h->fast.n) return MPM_OK;
-    return fast_sort_ranges(h, dt, CNT_NODE_BLOCKS);
 }
 
 int fast_forces(mpm_handle* h, double dt, double)
@@ -1825,7 +1674,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
     const bool timing = h->timing;
     h->timing = false;
     int rc = MPM_OK;
-    for(int variant = 0; variant <= MPM_P2G_FUSED && !rc; variant++)
+    for(int variant = 0; variant <= MPM_P2G_PAIRX && !rc; variant++)
         for(int ti = 0; ti < 3 && !rc; ti++)
             for(int mult = 1; mult <= 2 && !rc; mult++) {
                 f.p2g_variant = variant;
@@ -1837,22 +1686,11 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
                 cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
-                if(variant == MPM_P2G_FUSED) {
-                    // the fused loop: one P2G, then G2P2G + grid + sort per substep
-                    if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0))) break;
-                    if((rc = fast_g2p2g(h, dt)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_resort(h, dt))) break;
-                    cudaEventRecord(e0, h->stream);
-                    for(int s = 0; s < substeps && !rc; s++)
-                        if(!(rc = fast_g2p2g(h, dt)) && !(rc = fast_forces(h, dt, 0))) rc = fast_resort(h, dt);
-                    cudaEventRecord(e1, h->stream);
-                    if(!rc) rc = fast_g2p(h, dt, 0);   // leaves the grid accumulator empty
-                } else {
-                    if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_g2p(h, dt, 0))) break;
-                    cudaEventRecord(e0, h->stream);
-                    for(int s = 0; s < substeps && !rc; s++)
-                        if(!(rc = fast_p2g(h, dt, 0)) && !(rc = fast_forces(h, dt, 0))) rc = fast_g2p(h, dt, 0);
-                    cudaEventRecord(e1, h->stream);
-                }
+                if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_g2p(h, dt, 0))) break;
+                cudaEventRecord(e0, h->stream);
+                for(int s = 0; s < substeps && !rc; s++)
+                    if(!(rc = fast_p2g(h, dt, 0)) && !(rc = fast_forces(h, dt, 0))) rc = fast_g2p(h, dt, 0);
+                cudaEventRecord(e1, h->stream);
                 if(cudaEventSynchronize(e1) != cudaSuccess) { rc = check_cuda(h, cudaGetLastError(), "autotune"); break; }
                 float ms = 0;
                 cudaEventElapsedTime(&ms, e0, e1);

@@ -127,10 +127,7 @@ struct mpm_handle {
     std::vector<PendingEvent> pending;
     std::vector<cudaEvent_t> event_pool;
     // one captured substep per particle-buffer parity (the fast path swaps buffers)
-    // captured substep graphs: [segment][buffer parity]; segment 0 = one whole
-    // substep, 1 = P2G + grid (head of a fused loop), 2 = G2P2G + grid + sort
-    // (middle), 3 = G2P (tail)
-    cudaGraphExec_t graphs[4][2] = {};
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};   // one captured substep per buffer parity
     double graph_dt = 0;
     // checkpoints of the last mpm_diff_forward (mpm_adjoint.cu)
     void* diff = nullptr;
@@ -166,8 +163,6 @@ int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_k
 int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, const mpm_collision_object* objs, int nobjs);
 int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len);
 int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm);
-int fast_g2p2g(mpm_handle* h, double dt);
-int fast_resort(mpm_handle* h, double dt);
 int fast_particle_totals(mpm_handle* h, mpm_totals* out);
 int fast_grid_totals(mpm_handle* h, mpm_totals* out);
 int plain_particle_totals(mpm_handle* h, mpm_totals* out);

@@ -42,29 +42,6 @@ def test_batch_matches_individual_scenes(cuda_device):
         assert ex < 1e-6 and ef < 1e-4, (s.name, s.counts, ex, ef)
 
 
-def test_fused_batch_matches_individual_scenes(cuda_device):
-    """The fused G2P/P2G loop over a batch against each scene run alone unfused."""
-    from physbam_b200 import driver as D
-    scenes = small_batch(seed=78)
-    nsteps = 10
-    batch = D.MPM_BATCH(scenes)
-    batch.set_launch_shape(D.P2G_FUSED, 64, 2)
-    batch.set_scene_particles()
-    batch.advance(nsteps)
-    got = batch.split(batch.get_particles())
-    batch.close()
-    for s, g in zip(scenes, got):
-        drv = D.MPM_DRIVER(s)
-        drv.set_scene_particles(s)
-        drv.advance(nsteps)
-        ref = drv.get_particles()
-        drv.close()
-        np.testing.assert_array_equal(g["valid"], ref["valid"])
-        ex = np.max(np.abs(g["X"] - ref["X"]))
-        ef = np.max(np.abs(g["F"] - ref["F"]))
-        assert ex < 1e-6 and ef < 1e-4, (s.name, s.counts, ex, ef)
-
-
 def test_autotune_keeps_state_and_results(cuda_device):
     from physbam_b200 import driver as D
     scenes = small_batch(count=4, seed=3)

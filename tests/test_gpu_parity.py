@@ -80,7 +80,7 @@ def test_plain_fp64_matches_reference(cuda_device, name):
 
 
 # launch shapes: (P2G variant, G2P threads per CTA, CTA multiplier)
-SHAPES = [(0, 128, 1), (1, 64, 2), (2, 256, 1), (2, 128, 2), (3, 64, 1), (3, 128, 2), (4, 128, 1)]
+SHAPES = [(0, 128, 1), (1, 64, 2), (2, 256, 1), (2, 128, 2), (3, 64, 1), (3, 128, 2)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "p2g%d-g2p%d-x%d" % s)
@@ -126,7 +126,7 @@ def test_launch_shape_round_trip(cuda_device):
     drv = D().MPM_DRIVER(scene)
     drv.set_launch_shape(2, 64, 2)
     assert drv.get_launch_shape() == (2, 64, 2)
-    for bad in [(5, 128, 1), (-1, 128, 1), (0, 96, 1), (0, 128, 3)]:
+    for bad in [(4, 128, 1), (-1, 128, 1), (0, 96, 1), (0, 128, 3)]:
         with pytest.raises(D().MPMError):
             drv.set_launch_shape(*bad)
     assert drv.get_launch_shape() == (2, 64, 2)
@@ -220,62 +220,6 @@ def test_graph_advance_matches_eager(cuda_device):
         drv.close()
     for k in ("X", "F"):
         assert rel(res[1][k], res[0][k], 1.0) < 1e-6
-
-
-@pytest.mark.parametrize("g2p_threads", [64, 256])
-@pytest.mark.parametrize("name", ["small3d_corotated", "small3d_neohookean_friction"])
-def test_fused_advance_matches_reference(cuda_device, name, g2p_threads):
-    """mpm_advance with G2P fused into the next substep's P2G, against the
-    reference's own dumps of the last substep (the golden fixtures)."""
-    scene, dumps = load(name)
-    last = max(dumps)
-    drv = D().MPM_DRIVER(scene)
-    drv.set_launch_shape(D().P2G_FUSED, g2p_threads, 1)
-    drv.set_scene_particles(scene)
-    drv.advance(last + 1)
-    got, ref = drv.get_particles(), dumps[last]
-    np.testing.assert_array_equal(got["valid"], ref["valid"])
-    fl = floors(scene, ref)
-    for k in ("X", "V", "F", "B"):
-        assert rel(got[k], ref[k], fl[k]) < TOL_FP32[k], (name, k)
-    if "grid_m" in ref:
-        g = drv.get_grid()
-        for k in ("grid_m", "grid_v", "grid_vf"):
-            assert rel(g[k], ref[k], fl[k]) < TOL_FP32[k], (name, k)
-    drv.close()
-
-
-@pytest.mark.parametrize("model", [S.COROTATED, S.NEO_HOOKEAN])
-def test_fused_advance_fallback_and_fast_motion(cuda_device, model):
-    """Fused loop with inverted / flat F (FP64 stress route from the new state)
-    and particles fast enough to leave the grown P2G tile, against the plain
-    FP64 path."""
-    scene = S.small_3d(model=model, nsteps=6, with_walls=False)
-    rng = np.random.default_rng(9)
-    n = scene.n
-    F = scene.F.copy()
-    inv = rng.random(n) < 0.2
-    F[inv, :, 0] *= -1.0
-    scene.F = F
-    fast = rng.random(n) < 0.1
-    V = scene.V.copy()
-    V[fast] += np.array([1.3, 0.0, -1.2]) * (scene.dx / scene.dt)   # 1.3 and 1.2 cells per substep
-    scene.V = V
-    out = {}
-    for prec, path, shape in ((D().FP64, D().PATH_PLAIN, None), (D().FP32, D().PATH_FAST, (D().P2G_FUSED, 128, 1))):
-        drv = D().MPM_DRIVER(scene, precision=prec, path=path)
-        if shape:
-            drv.set_launch_shape(*shape)
-        drv.set_scene_particles(scene)
-        drv.advance(scene.nsteps)
-        out[path] = drv.get_particles()
-        drv.close()
-    ref, got = out[D().PATH_PLAIN], out[D().PATH_FAST]
-    np.testing.assert_array_equal(got["valid"], ref["valid"])
-    vmax = float(np.abs(ref["V"]).max())
-    assert rel(got["X"], ref["X"], 1.0) < 2e-6
-    assert rel(got["V"], ref["V"], vmax) < 2e-3
-    assert rel(got["F"], ref["F"], 1.0) < 1e-4
 
 
 def test_empty_and_leaving_particles(cuda_device):
