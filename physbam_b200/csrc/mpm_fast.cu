@@ -57,7 +57,9 @@ struct FastArgs {
     const uint32_t* sorted_keys;
     uint32_t* keys_next;
     uint32_t *bstart, *bend, *active, *nb_flag, *nb_list, *counters;
-    uint32_t* fallback;   // sorted positions whose stress takes the FP64 route (P2G variant 2)
+    uint32_t* fallback;   // sorted positions whose stress takes the FP64 route (P2G)
+    uint32_t* sort_scratch;   // digit histograms of the next sort live at its start
+    int key_bits;
     float4* acc;
     float4* vel;
     const SceneDev* scenes;
@@ -213,6 +215,8 @@ __global__ void k_init_keys(FastArgs a, const uint8_t* valid_by_slot)
 // copied to their sorted slot here, as G2P does for the valid ones.
 __global__ void k_ranges(FastArgs a)
 {
+    // the sort has read its histograms: G2P builds the next ones
+    if(blockIdx.x == 0) mpm_sort::hist_reset(a.sort_scratch);
     for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < a.n; j += (int64_t)gridDim.x * blockDim.x) {
         uint32_t k = a.sorted_keys[j];
         uint32_t kp = j ? a.sorted_keys[j - 1] : SENTINEL;
@@ -244,82 +248,6 @@ __device__ __forceinline__ int next_work(uint32_t* ctr, int* s_work)
     if(threadIdx.x == 0) *s_work = (int)atomicAdd(ctr, 1u);
     __syncthreads();
     return *s_work;
-}
-
-// Per-particle P2G coefficients.  For node (ii, jj, kk) the contribution is
-//   mass += mxy[ii][jj] wz[kk]
-//   p_r  += wz[kk] P_r(ii,jj) + w uz[kk][r] - Cc_r(ii,jj) dwz[kk],   w = wxy wz[kk]
-// where p_i = w m (V + B D (Z_i - X)) - dt vol S g collects momentum and dt * force.
-struct P2GParticle {
-    Axis<float> wx, wy, wz;
-    float m;
-    float ux[3][3], uy[3][3], uz[3][3];
-    float S[9];
-};
-
-__device__ __forceinline__ void p2g_particle(const FastArgs& a, const SceneDev& sc, uint32_t i, P2GParticle& P)
-{
-    float X[3], V[3], F[9], Bm[9];
-#pragma unroll
-    for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
-#pragma unroll
-    for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; Bm[r] = a.src[(C_B + r) * a.npad + i]; }
-    const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
-    if(!stress_fast(sc.model, F, at.z, at.w, P.S)) {
-        // only this rare branch needs an addressable array for the out-of-line call
-        float T[9];
-        atomicAdd(&a.counters[CNT_FALLBACK], 1u);
-        if(!stress_fp64(sc.model, F, at.z, at.w, T)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
-#pragma unroll
-        for(int r = 0; r < 9; r++) P.S[r] = T[r];
-    }
-    const float sv = a.dt * at.y, m = at.x;
-    P.m = m;
-#pragma unroll
-    for(int r = 0; r < 9; r++) P.S[r] *= sv;
-    P.wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
-    P.wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
-    P.wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
-    const float Dx = 4.f * sc.inv[0] * sc.inv[0] * m, Dy = 4.f * sc.inv[1] * sc.inv[1] * m, Dz = 4.f * sc.inv[2] * sc.inv[2] * m;
-#pragma unroll
-    for(int o = 0; o < 3; o++) {
-        float dxo = (sc.dmin[0] + ((float)(P.wx.base + o) + 0.5f) * sc.dx[0] - X[0]) * Dx;
-        float dyo = (sc.dmin[1] + ((float)(P.wy.base + o) + 0.5f) * sc.dx[1] - X[1]) * Dy;
-        float dzo = (sc.dmin[2] + ((float)(P.wz.base + o) + 0.5f) * sc.dx[2] - X[2]) * Dz;
-#pragma unroll
-        for(int r = 0; r < 3; r++) {
-            P.ux[o][r] = Bm[r] * dxo + m * V[r];   // the x factor also carries m V
-            P.uy[o][r] = Bm[r + 3] * dyo;
-            P.uz[o][r] = Bm[r + 6] * dzo;
-        }
-    }
-}
-
-// Visit the 27 node contributions of one particle: f(q, mass, px, py, pz).
-template<class FN> __device__ __forceinline__ void p2g_nodes(const P2GParticle& P, FN&& f)
-{
-#pragma unroll
-    for(int ii = 0; ii < 3; ii++)
-#pragma unroll
-        for(int jj = 0; jj < 3; jj++) {
-            const float wxy = P.wx.w[ii] * P.wy.w[jj];
-            const float gx0 = P.wx.dw[ii] * P.wy.w[jj], gy0 = P.wx.w[ii] * P.wy.dw[jj];
-            const float mxy = P.m * wxy;
-            float Pr[3], Cc[3];
-#pragma unroll
-            for(int r = 0; r < 3; r++) {
-                Pr[r] = wxy * (P.ux[ii][r] + P.uy[jj][r]) - (P.S[r] * gx0 + P.S[r + 3] * gy0);
-                Cc[r] = P.S[r + 6] * wxy;
-            }
-#pragma unroll
-            for(int kk = 0; kk < 3; kk++) {
-                const float wzk = P.wz.w[kk], dwz = P.wz.dw[kk], wq = wxy * wzk;
-                f((ii * 3 + jj) * 3 + kk, mxy * wzk,
-                  wzk * Pr[0] + wq * P.uz[kk][0] - Cc[0] * dwz,
-                  wzk * Pr[1] + wq * P.uz[kk][1] - Cc[1] * dwz,
-                  wzk * Pr[2] + wq * P.uz[kk][2] - Cc[2] * dwz);
-            }
-        }
 }
 
 struct P2GTile {
@@ -380,7 +308,112 @@ __device__ __forceinline__ void p2g_end(const FastArgs& a, P2GTile& T, uint32_t 
     }
 }
 
-// The elastic force of the particles the P2G variants 1-3 listed for the FP64
+// Every node quantity of a particle has the separable form (w = wx wy wz at
+// node (i, j, k))
+//   q_node = Hx[i] wy[j] wz[k] + wx[i] Hy[j] wz[k] + wx[i] wy[j] Hz[k]
+// with, for momentum component r and axis a,
+//   Ha[o] = wa[o] m B(r,a) Dinv_a (x_a(o) - X_a) - dt vol PF^T(r,a) wa'(o)
+//           (+ wa[o] m V_r on the x axis),
+// i.e. w m (V + B Dinv (x - X)) - dt vol PF^T grad w; mass is the same form
+// with V_r = 1, B = 0 and PF^T = 0 (MPM_DRIVER::Particle_To_Grid,
+// MPM_DRIVER.cpp:245-306, with MPM_FINITE_ELEMENTS::Add_Forces,
+// MPM_FINITE_ELEMENTS.cpp:84-99, folded in as dt f).
+struct PairSlot {
+    float Hx[3], Hy[3], Hz[3];
+};
+
+__device__ __forceinline__ void pair_slot(const Axis<float>& wx, const Axis<float>& wy, const Axis<float>& wz,
+    const float dX[3][3], float mV, const float mBD[3], const float S[3], PairSlot& q)
+{
+#pragma unroll
+    for(int o = 0; o < 3; o++) {
+        q.Hx[o] = wx.w[o] * fmaf(mBD[0], dX[0][o], mV) - S[0] * wx.dw[o];
+        q.Hy[o] = wy.w[o] * (mBD[1] * dX[1][o]) - S[1] * wy.dw[o];
+        q.Hz[o] = wz.w[o] * (mBD[2] * dX[2][o]) - S[2] * wz.dw[o];
+    }
+}
+
+// Weights and separable factors of all four node quantities of the particle
+// at sorted position j (mass: Hx = m wx, Hy = Hz = 0).  A particle whose
+// stress needs the FP64 route is listed for p2g_finish and contributes
+// mass and momentum here.
+struct P2GFactors {
+    float w[9];            // wx[3], wy[3], wz[3]
+    float mwx[3];          // mass factor m wx
+    PairSlot q[3];         // momentum components x, y, z
+    int base[3];           // first stencil node - ghost, per axis
+};
+
+// Factors from a particle state held in registers (X, V, F, B, attributes);
+// `j` is the sorted position recorded if the stress needs the FP64 route.
+__device__ __forceinline__ void factors_from(const FastArgs& a, const SceneDev& sc, const float* X, const float* V,
+    const float* F, const float* B, const float4 at, uint32_t j, P2GFactors& P)
+{
+    float S[9];
+    if(!stress_fast(sc.model, F, at.z, at.w, S)) {
+        a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
+#pragma unroll
+        for(int r = 0; r < 9; r++) S[r] = 0.f;
+    }
+    const float sv = a.dt * at.y, m = at.x;
+    const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
+    const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
+    const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
+    P.base[0] = wx.base; P.base[1] = wy.base; P.base[2] = wz.base;
+    float dX[3][3];
+    const float bx = (float)wx.base + 0.5f, by = (float)wy.base + 0.5f, bz = (float)wz.base + 0.5f;
+#pragma unroll
+    for(int o = 0; o < 3; o++) {
+        dX[0][o] = sc.dmin[0] + (bx + (float)o) * sc.dx[0] - X[0];
+        dX[1][o] = sc.dmin[1] + (by + (float)o) * sc.dx[1] - X[1];
+        dX[2][o] = sc.dmin[2] + (bz + (float)o) * sc.dx[2] - X[2];
+    }
+    const float Dm[3] = {4.f * sc.inv[0] * sc.inv[0] * m, 4.f * sc.inv[1] * sc.inv[1] * m, 4.f * sc.inv[2] * sc.inv[2] * m};
+#pragma unroll
+    for(int r = 0; r < 3; r++) {
+        const float mBD[3] = {B[r] * Dm[0], B[r + 3] * Dm[1], B[r + 6] * Dm[2]};
+        const float Sr[3] = {S[r] * sv, S[r + 3] * sv, S[r + 6] * sv};
+        pair_slot(wx, wy, wz, dX, m * V[r], mBD, Sr, P.q[r]);
+    }
+#pragma unroll
+    for(int o = 0; o < 3; o++) {
+        P.mwx[o] = m * wx.w[o];
+        P.w[o] = wx.w[o]; P.w[3 + o] = wy.w[o]; P.w[6 + o] = wz.w[o];
+    }
+}
+
+__device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneDev& sc, uint32_t j, P2GFactors& P)
+{
+    const uint32_t i = a.perm[j];
+    float X[3], V[3], F[9], B[9];
+#pragma unroll
+    for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
+#pragma unroll
+    for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; B[r] = a.src[(C_B + r) * a.npad + i]; }
+    factors_from(a, sc, X, V, F, B, a.src_attr[i], j, P);   // attributes: mass, volume, mu, lambda
+}
+
+// The 27 node values of one particle: f(ii, jj, kk, mass, px, py, pz).
+template<class FN> __device__ __forceinline__ void factor_nodes(const P2GFactors& P, FN&& f)
+{
+#pragma unroll
+    for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+        for(int jj = 0; jj < 3; jj++) {
+            const float wxy = P.w[ii] * P.w[3 + jj], mxy = P.mwx[ii] * P.w[3 + jj];
+            float A[3];
+#pragma unroll
+            for(int r2 = 0; r2 < 3; r2++) A[r2] = fmaf(P.q[r2].Hx[ii], P.w[3 + jj], P.w[ii] * P.q[r2].Hy[jj]);
+#pragma unroll
+            for(int kk = 0; kk < 3; kk++) {
+                const float wz = P.w[6 + kk];
+                f(ii, jj, kk, mxy * wz, fmaf(A[0], wz, wxy * P.q[0].Hz[kk]), fmaf(A[1], wz, wxy * P.q[1].Hz[kk]),
+                  fmaf(A[2], wz, wxy * P.q[2].Hz[kk]));
+            }
+        }
+}
+
+// The elastic force of the particles the P2G kernels listed for the FP64
 // stress route: -dt vol PF^T grad w added to the momentum of their 27 nodes.
 // Their nodes lie in their block's tile, whose node blocks P2G already
 // marked.  The CTA of the P2G launch that finishes last does this, once every
@@ -447,9 +480,10 @@ __global__ void __launch_bounds__(64) k_p2g_cells(FastArgs a)
 #pragma unroll
             for(int q = 0; q < 27; q++) { am[q] = 0; ax[q] = 0; ay[q] = 0; az[q] = 0; }
             for(uint32_t k = 0; k < cnt; k++) {
-                P2GParticle P;
-                p2g_particle(a, T.sc, a.perm[beg + k], P);
-                p2g_nodes(P, [&](int q, float m, float px, float py, float pz) {
+                P2GFactors P;
+                particle_factors(a, T.sc, beg + k, P);
+                factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
+                    const int q = (ii * 3 + jj) * 3 + kk;
                     am[q] += m; ax[q] += px; ay[q] += py; az[q] += pz;
                 });
             }
@@ -469,6 +503,7 @@ __global__ void __launch_bounds__(64) k_p2g_cells(FastArgs a)
         }
         p2g_end(a, T, b - T.sc.block_base);
     }
+    p2g_finish(a, &T.work);
 }
 
 // P2G variant 2: two lanes per contiguous range of the block's sorted
@@ -477,31 +512,6 @@ __global__ void __launch_bounds__(64) k_p2g_cells(FastArgs a)
 // lane accumulates mass and x momentum, the odd lane y and z momentum, so each
 // holds 54 accumulators instead of 108 and twice as many warps fit on an SM.
 // Accumulators go to the shared tile whenever the range moves to a new cell.
-//
-// Every quantity has the separable form (w = wx wy wz at node (i, j, k))
-//   q_node = Hx[i] wy[j] wz[k] + wx[i] Hy[j] wz[k] + wx[i] wy[j] Hz[k]
-// with, for momentum component r and axis a,
-//   Ha[o] = wa[o] m B(r,a) Dinv_a (x_a(o) - X_a) - dt vol PF^T(r,a) wa'(o)
-//           (+ wa[o] m V_r on the x axis),
-// i.e. w m (V + B Dinv (x - X)) - dt vol PF^T grad w; mass is the same form
-// with V_r = 1, B = 0 and PF^T = 0 (MPM_DRIVER::Particle_To_Grid,
-// MPM_DRIVER.cpp:245-306, with MPM_FINITE_ELEMENTS::Add_Forces,
-// MPM_FINITE_ELEMENTS.cpp:84-99, folded in as dt f).
-struct PairSlot {
-    float Hx[3], Hy[3], Hz[3];
-};
-
-__device__ __forceinline__ void pair_slot(const Axis<float>& wx, const Axis<float>& wy, const Axis<float>& wz,
-    const float dX[3][3], float mV, const float mBD[3], const float S[3], PairSlot& q)
-{
-#pragma unroll
-    for(int o = 0; o < 3; o++) {
-        q.Hx[o] = wx.w[o] * fmaf(mBD[0], dX[0][o], mV) - S[0] * wx.dw[o];
-        q.Hy[o] = wy.w[o] * (mBD[1] * dX[1][o]) - S[1] * wy.dw[o];
-        q.Hz[o] = wz.w[o] * (mBD[2] * dX[2][o]) - S[2] * wz.dw[o];
-    }
-}
-
 template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_p2g_pairs(FastArgs a)
 {
     __shared__ P2GTile T;
@@ -629,86 +639,6 @@ struct PairPrep {
     PairSlot keep0, keep1, send0, send1;
     int cell;
 };
-
-// Weights and separable factors of all four node quantities of the particle
-// at sorted position j (mass: Hx = m wx, Hy = Hz = 0).  A particle whose
-// stress needs the FP64 route is listed for p2g_finish and contributes
-// mass and momentum here.
-struct P2GFactors {
-    float w[9];            // wx[3], wy[3], wz[3]
-    float mwx[3];          // mass factor m wx
-    PairSlot q[3];         // momentum components x, y, z
-    int base[3];           // first stencil node - ghost, per axis
-};
-
-// Factors from a particle state held in registers (X, V, F, B, attributes);
-// `j` is the sorted position recorded if the stress needs the FP64 route.
-__device__ __forceinline__ void factors_from(const FastArgs& a, const SceneDev& sc, const float* X, const float* V,
-    const float* F, const float* B, const float4 at, uint32_t j, P2GFactors& P)
-{
-    float S[9];
-    if(!stress_fast(sc.model, F, at.z, at.w, S)) {
-        a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
-#pragma unroll
-        for(int r = 0; r < 9; r++) S[r] = 0.f;
-    }
-    const float sv = a.dt * at.y, m = at.x;
-    const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
-    const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
-    const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
-    P.base[0] = wx.base; P.base[1] = wy.base; P.base[2] = wz.base;
-    float dX[3][3];
-    const float bx = (float)wx.base + 0.5f, by = (float)wy.base + 0.5f, bz = (float)wz.base + 0.5f;
-#pragma unroll
-    for(int o = 0; o < 3; o++) {
-        dX[0][o] = sc.dmin[0] + (bx + (float)o) * sc.dx[0] - X[0];
-        dX[1][o] = sc.dmin[1] + (by + (float)o) * sc.dx[1] - X[1];
-        dX[2][o] = sc.dmin[2] + (bz + (float)o) * sc.dx[2] - X[2];
-    }
-    const float Dm[3] = {4.f * sc.inv[0] * sc.inv[0] * m, 4.f * sc.inv[1] * sc.inv[1] * m, 4.f * sc.inv[2] * sc.inv[2] * m};
-#pragma unroll
-    for(int r = 0; r < 3; r++) {
-        const float mBD[3] = {B[r] * Dm[0], B[r + 3] * Dm[1], B[r + 6] * Dm[2]};
-        const float Sr[3] = {S[r] * sv, S[r + 3] * sv, S[r + 6] * sv};
-        pair_slot(wx, wy, wz, dX, m * V[r], mBD, Sr, P.q[r]);
-    }
-#pragma unroll
-    for(int o = 0; o < 3; o++) {
-        P.mwx[o] = m * wx.w[o];
-        P.w[o] = wx.w[o]; P.w[3 + o] = wy.w[o]; P.w[6 + o] = wz.w[o];
-    }
-}
-
-__device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneDev& sc, uint32_t j, P2GFactors& P)
-{
-    const uint32_t i = a.perm[j];
-    float X[3], V[3], F[9], B[9];
-#pragma unroll
-    for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
-#pragma unroll
-    for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; B[r] = a.src[(C_B + r) * a.npad + i]; }
-    factors_from(a, sc, X, V, F, B, a.src_attr[i], j, P);   // attributes: mass, volume, mu, lambda
-}
-
-// The 27 node values of one particle: f(ii, jj, kk, mass, px, py, pz).
-template<class FN> __device__ __forceinline__ void factor_nodes(const P2GFactors& P, FN&& f)
-{
-#pragma unroll
-    for(int ii = 0; ii < 3; ii++)
-#pragma unroll
-        for(int jj = 0; jj < 3; jj++) {
-            const float wxy = P.w[ii] * P.w[3 + jj], mxy = P.mwx[ii] * P.w[3 + jj];
-            float A[3];
-#pragma unroll
-            for(int r2 = 0; r2 < 3; r2++) A[r2] = fmaf(P.q[r2].Hx[ii], P.w[3 + jj], P.w[ii] * P.q[r2].Hy[jj]);
-#pragma unroll
-            for(int kk = 0; kk < 3; kk++) {
-                const float wz = P.w[6 + kk];
-                f(ii, jj, kk, mxy * wz, fmaf(A[0], wz, wxy * P.q[0].Hz[kk]), fmaf(A[1], wz, wxy * P.q[1].Hz[kk]),
-                  fmaf(A[2], wz, wxy * P.q[2].Hz[kk]));
-            }
-        }
-}
 
 __device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc, uint32_t j, bool odd, PairPrep& P)
 {
@@ -1004,6 +934,7 @@ __device__ __forceinline__ bool g2p_stage(const FastArgs& a, const SceneDev& sc,
 struct G2PState {
     float xn[3], Vf[3], Fn[9], Bn[9];
     float4 at;
+    uint32_t key;
     bool ok;
 };
 
@@ -1114,6 +1045,7 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
 #pragma unroll
     for(int k = 0; k < 9; k++) out.Bn[k] = Bn[k];
     out.at = at;
+    out.key = key;
     out.ok = ok;
 }
 
@@ -1122,6 +1054,12 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
     __shared__ float4 tv[2 * TN];
     __shared__ int s_work;
     __shared__ SceneDev s_sc;
+    // digit histograms of the keys this CTA writes (for the next sort)
+    __shared__ uint32_t s_hist[mpm_sort::kMaxPasses][mpm_sort::kRadix];
+    for(int i = threadIdx.x; i < mpm_sort::kMaxPasses * mpm_sort::kRadix; i += THREADS) (&s_hist[0][0])[i] = 0;
+    // invalid particles, copied to the tail by k_ranges, keep sentinel keys
+    if(blockIdx.x == 0 && threadIdx.x == 0)
+        mpm_sort::hist_add_sentinels(a.sort_scratch, (uint32_t)(a.n - a.counters[CNT_ACTIVE_PARTICLES]), a.key_bits);
     const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
     for(int w = next_work(&a.counters[CNT_G2P_WORK], &s_work); w < (int)nblocks; w = next_work(&a.counters[CNT_G2P_WORK], &s_work)) {
         const uint32_t b = a.active[w];
@@ -1136,7 +1074,13 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
         for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
             G2PState o;
             g2p_particle(a, sc, tv, anti, ox, oy, oz, j, o);
+            mpm_sort::hist_add(s_hist, o.key, a.key_bits);
         }
+    }
+    __syncthreads();
+    for(int i = threadIdx.x; i < mpm_sort::kMaxPasses * mpm_sort::kRadix; i += THREADS) {
+        const uint32_t c = (&s_hist[0][0])[i];
+        if(c) atomicAdd(&a.sort_scratch[i], c);
     }
 }
 
@@ -1213,6 +1157,8 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.nb_flag = f.nb_flag; a.nb_list = f.nb_list; a.counters = f.counters;
     a.acc = f.acc; a.vel = f.vel;
     a.fallback = f.sort_keys_alt;   // the sort's ping-pong buffer is free until the next sort
+    a.sort_scratch = f.sort_scratch;
+    a.key_bits = f.key_bits;
     a.scenes = f.scenes; a.block_scene = f.block_scene; a.nb_scene = f.nb_scene; a.pbase = f.pbase;
     a.objs = f.objs;
     a.nscenes = f.nscenes;
@@ -1422,6 +1368,7 @@ int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
     int64_t n = v->n;
     f.cur = 0;
     f.keys_ready = n == 0;
+    f.hist_ready = false;
     if(!n) return MPM_OK;
     // stage caller arrays on the device if needed
     bool dev = v->on_device != 0;
@@ -1517,10 +1464,13 @@ static int fast_sort_ranges(mpm_handle* h, double dt, int cleared)
     FastState& f = h->fast;
     const int64_t n = f.n;
     int slot = timer_begin(h, "fast_sort");
-    // sort the slot keys (f.keys, left intact for get_particles) into sorted_keys / perm
+    // sort the slot keys (f.keys, left intact for get_particles) into sorted_keys / perm;
+    // the histograms come from the G2P that wrote the keys, else they are counted here
     cudaError_t e = mpm_sort::radix_sort(f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, n, f.key_bits,
-                                         f.sort_scratch, h->d_flags, MPM_FLAG_TIMEOUT, h->sm_count * 4, h->stream);
+                                         f.sort_scratch, h->d_flags, MPM_FLAG_TIMEOUT, h->sm_count * 4, h->stream,
+                                         true, f.hist_ready);
     if(e != cudaSuccess) return check_cuda(h, e, "radix_sort");
+    f.hist_ready = false;
     timer_end(h, slot);
     FastArgs a = make_args(h, dt);
     slot = timer_begin(h, "fast_ranges");
@@ -1581,6 +1531,7 @@ int fast_g2p(mpm_handle* h, double dt, double)
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_g2p");
     f.cur = 1 - f.cur;
+    f.hist_ready = true;
     return MPM_OK;
 }
 
@@ -1686,6 +1637,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
                 cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
+                f.hist_ready = false;
                 if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_g2p(h, dt, 0))) break;
                 cudaEventRecord(e0, h->stream);
                 for(int s = 0; s < substeps && !rc; s++)
@@ -1710,6 +1662,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
     cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
+    f.hist_ready = false;
     cudaStreamSynchronize(h->stream);
     cudaFree(save_soa); cudaFree(save_attr); cudaFree(save_pid); cudaFree(save_keys);
     cudaEventDestroy(e0);

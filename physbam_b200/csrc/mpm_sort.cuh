@@ -106,6 +106,41 @@ __global__ void __launch_bounds__(kThreads) k_upfront_hist(const uint32_t* __res
     }
 }
 
+// Pieces for callers that build the histograms themselves while they write
+// the keys (radix_sort(..., have_hist = true)).
+//
+// Count `key` into the shared histograms `cnt[kMaxPasses][kRadix]`: one
+// atomic per distinct digit among the converged lanes that call it.
+__device__ __forceinline__ void hist_add(uint32_t (*cnt)[kRadix], uint32_t key, int bits)
+{
+    const int passes = passes_for(bits);
+    const int lane = threadIdx.x & 31;
+    const unsigned active = __activemask();
+    for(int p = 0; p < passes; p++) {
+        const uint32_t dg = (key >> (8 * p)) & digit_mask(bits, p);
+        const uint32_t peers = __match_any_sync(active, dg);
+        if((__ffs(peers) - 1) == lane) atomicAdd(&cnt[p][dg], (uint32_t)__popc(peers));
+    }
+}
+
+// Add `count` sentinel keys (all bits set) to the global histograms.
+__device__ __forceinline__ void hist_add_sentinels(uint32_t* scratch, uint32_t count, int bits)
+{
+    if(!count) return;
+    for(int p = 0; p < passes_for(bits); p++) atomicAdd(&scratch[p * kRadix + digit_mask(bits, p)], count);
+}
+
+// After a sort has run: clear the histograms for the next one, reset the tile
+// tickets and start a new epoch (one CTA; nothing else may touch the scratch).
+__device__ __forceinline__ void hist_reset(uint32_t* scratch)
+{
+    for(int i = threadIdx.x; i < kHistWords; i += blockDim.x) scratch[i] = 0;
+    if(threadIdx.x == 0) {
+        for(int p = 0; p < kMaxPasses; p++) scratch[kTicketOff + p] = 0;
+        scratch[kEpochOff] += 1;
+    }
+}
+
 __device__ inline uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem, uint32_t& total)
 {
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -279,21 +314,25 @@ inline cudaError_t prepare()
 // the result lands in (keys_out, vals_out), which must not alias keys;
 // (keys_alt, vals_alt) are ping-pong buffers.  scratch = scratch_words(n)
 // words whose epoch region persists between sorts.  n < 2^30.
-// `small_tiles` allows 1024-key tiles for n <= kSmallSortMax.
+// `small_tiles` allows 1024-key tiles for n <= kSmallSortMax.  `have_hist`:
+// the caller built the histograms of `keys` in the scratch (hist_add), reset
+// the tickets and started a new epoch after the previous sort (hist_reset).
 inline cudaError_t radix_sort(const uint32_t* keys, uint32_t* keys_out, uint32_t* vals_out, uint32_t* keys_alt,
     uint32_t* vals_alt, int64_t n, int bits, uint32_t* scratch, unsigned* err_flags, unsigned timeout_flag,
-    int hist_blocks, cudaStream_t st, bool small_tiles = true)
+    int hist_blocks, cudaStream_t st, bool small_tiles = true, bool have_hist = false)
 {
     if(n == 0) return cudaSuccess;
     int passes = (bits + 7) / 8;
     const bool small = small_tiles && n <= kSmallSortMax;
     int64_t tiles = small ? tiles_for(n, kSmallTile) : tiles_for(n);
-    cudaError_t e = cudaMemsetAsync(scratch, 0, kHistWords * sizeof(uint32_t), st);
-    if(e != cudaSuccess) return e;
-    int hb = (int)((n + kThreads * 4 - 1) / (kThreads * 4));
-    if(hb > hist_blocks) hb = hist_blocks;
-    if(hb < 1) hb = 1;
-    k_upfront_hist<<<hb, kThreads, 0, st>>>(keys, n, bits, scratch);
+    if(!have_hist) {
+        cudaError_t e = cudaMemsetAsync(scratch, 0, kHistWords * sizeof(uint32_t), st);
+        if(e != cudaSuccess) return e;
+        int hb = (int)((n + kThreads * 4 - 1) / (kThreads * 4));
+        if(hb > hist_blocks) hb = hist_blocks;
+        if(hb < 1) hb = 1;
+        k_upfront_hist<<<hb, kThreads, 0, st>>>(keys, n, bits, scratch);
+    }
     // ping-pong so that the last pass writes (keys_out, vals_out)
     const uint32_t* kin = keys;
     const uint32_t* vin = nullptr;
