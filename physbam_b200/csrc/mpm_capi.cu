@@ -329,6 +329,7 @@ int mpm_advance(mpm_handle* h, double dt, double time, int nsteps)
     if(rc) return rc;
     if(nsteps < 0) return set_error(h, MPM_ERR_ARG, "nsteps < 0");
     if(h->graph_dt != dt) release_graph(h);
+    if(fast(h) && nsteps && (rc = fast_prepare_sort(h))) return rc;
     for(int s = 0; s < nsteps; s++)
         if((rc = run_substep(h, dt, time + s * dt))) return rc;
     return MPM_OK;

@@ -1481,6 +1481,20 @@ static int fast_sort_ranges(mpm_handle* h, double dt, int cleared)
     return MPM_OK;
 }
 
+// Count the digit histograms of the current keys (after mpm_set_particles or
+// the autotuner's restore), so that a captured substep never has to.
+int fast_prepare_sort(mpm_handle* h)
+{
+    FastState& f = h->fast;
+    if(f.hist_ready || !f.keys_ready || !f.n) return MPM_OK;
+    MPM_CUDA(h, cudaMemsetAsync(f.sort_scratch, 0, mpm_sort::kHistWords * sizeof(uint32_t), h->stream));
+    const int hb = std::min((int)((f.n + 1023) / 1024), h->sm_count * 4);
+    mpm_sort::k_upfront_hist<<<std::max(hb, 1), mpm_sort::kThreads, 0, h->stream>>>(f.keys, f.n, f.key_bits, f.sort_scratch);
+    MPM_LAUNCHED(h, "k_upfront_hist");
+    f.hist_ready = true;
+    return MPM_OK;
+}
+
 int fast_p2g(mpm_handle* h, double dt, double)
 {
     FastState& f = h->fast;
