@@ -247,11 +247,10 @@ int mpm_autotune(mpm_handle* h, double dt, int substeps, char* report, int repor
  * p2g_variant: MPM_P2G_CELLS (one thread per cell), MPM_P2G_INTERLEAVED (one
  * thread per particle), MPM_P2G_PAIRS (two threads per range of particles,
  * splitting the node quantities), MPM_P2G_PAIRX (as PAIRS, the two threads
- * also splitting the per-particle work), MPM_P2G_STAGED (as PAIRS, with each
- * block's particles first copied into shared memory asynchronously);
+ * also splitting the per-particle work);
  * g2p_threads: 64, 128 or 256 per CTA; cta_mult: 1 or 2 times the resident
  * CTAs per SM. */
-enum { MPM_P2G_CELLS = 0, MPM_P2G_INTERLEAVED = 1, MPM_P2G_PAIRS = 2, MPM_P2G_PAIRX = 3, MPM_P2G_STAGED = 4 };
+enum { MPM_P2G_CELLS = 0, MPM_P2G_INTERLEAVED = 1, MPM_P2G_PAIRS = 2, MPM_P2G_PAIRX = 3 };
 int mpm_set_launch_shape(mpm_handle* h, int p2g_variant, int g2p_threads, int cta_mult);
 int mpm_get_launch_shape(mpm_handle* h, int* p2g_variant, int* g2p_threads, int* cta_mult);
 

@@ -393,7 +393,7 @@ int mpm_set_launch_shape(mpm_handle* h, int p2g_variant, int g2p_threads, int ct
 {
     if(!h) return MPM_ERR_ARG;
     if(!fast(h)) return set_error(h, MPM_ERR_ARG, "launch shapes belong to the fast path");
-    if(p2g_variant < MPM_P2G_CELLS || p2g_variant > MPM_P2G_STAGED) return set_error(h, MPM_ERR_ARG, "unknown P2G variant");
+    if(p2g_variant < MPM_P2G_CELLS || p2g_variant > MPM_P2G_PAIRX) return set_error(h, MPM_ERR_ARG, "unknown P2G variant");
     if(g2p_threads != 64 && g2p_threads != 128 && g2p_threads != 256) return set_error(h, MPM_ERR_ARG, "G2P threads: 64, 128 or 256");
     if(cta_mult != 1 && cta_mult != 2) return set_error(h, MPM_ERR_ARG, "CTA multiplier: 1 or 2");
     release_graph(h);

@@ -728,140 +728,6 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
     p2g_finish(a, &T.work);
 }
 
-// P2G variant 4: variant 2 with the block's particles staged in shared memory
-// first.  The CTA issues asynchronous copies (cp.async) of every staged
-// particle's 28 values at once, so the gather through the permutation costs one
-// memory latency per round of up to kStage particles instead of one per
-// particle and lane; the pairs then read their particles from shared memory.
-// Particle k of a round sits at column k + k/8 of each row, so the 16 pairs of
-// a warp, each on its own run of 8 particles, read 16 different banks.
-constexpr int kStage = 512;
-constexpr int kStageRow = kStage + kStage / 8;
-
-struct StageBuf {
-    float f[NCOMP][kStageRow];   // x y z, vx vy vz, F (9), B (9)
-    float4 at[kStageRow];        // mass, volume, mu, lambda
-    uint32_t cell[kStage];
-};
-
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_wait_all()
-{
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
-
-// Stage sorted positions [c0, c0 + nc) (nc <= kStage); synchronises.
-__device__ __forceinline__ void stage_particles(const FastArgs& a, StageBuf& B, uint32_t c0, uint32_t nc)
-{
-    for(uint32_t k = threadIdx.x; k < nc; k += blockDim.x) {
-        const uint32_t i = a.perm[c0 + k], ks = k + (k >> 3);
-#pragma unroll
-        for(int f = 0; f < NCOMP; f++) cp_async4(&B.f[f][ks], a.src + f * a.npad + i);
-        cp_async16(&B.at[ks], a.src_attr + i);
-        B.cell[k] = a.sorted_keys[c0 + k] & 63u;
-    }
-    cp_async_wait_all();
-    __syncthreads();
-}
-
-template<int THREADS> __global__ void __launch_bounds__(THREADS, 384 / THREADS) k_p2g_staged(FastArgs a)
-{
-    __shared__ P2GTile T;
-    extern __shared__ float4 stage_raw[];
-    StageBuf& B = *reinterpret_cast<StageBuf*>(stage_raw);
-    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    const bool odd = threadIdx.x & 1;
-    const int pair = threadIdx.x >> 1;
-    constexpr int kPairs = THREADS / 2;
-    const int r0 = odd ? 1 : 0, r1 = odd ? 2 : 0;
-    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
-        const uint32_t b = a.active[w];
-        stage_scene(a, a.block_scene[b], &T.sc);
-        for(int t = threadIdx.x; t < TN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
-        const SceneDev& sc = T.sc;
-        const uint32_t s = a.bstart[b], e = a.bend[b];
-        float* const out0 = odd ? T.y : T.m;
-        float* const out1 = odd ? T.z : T.x;
-        for(uint32_t c0 = s; c0 < e; c0 += kStage) {
-            const uint32_t nc = min((uint32_t)kStage, e - c0);
-            stage_particles(a, B, c0, nc);
-            const uint32_t per = (nc + kPairs - 1) / kPairs;
-            const uint32_t k0 = pair * per, k1 = min(k0 + per, nc);
-            float acc0[27], acc1[27];
-#pragma unroll
-            for(int q = 0; q < 27; q++) { acc0[q] = 0.f; acc1[q] = 0.f; }
-            int cell = -1;
-            for(uint32_t k = k0; k < k1; k++) {
-                const int c = (int)B.cell[k];
-                if(c != cell) {
-                    if(cell >= 0) pair_flush(cell, out0, out1, acc0, acc1);
-                    cell = c;
-                }
-                const uint32_t ks = k + (k >> 3);
-                float X[3], F[9], B0[3], B1[3];
-#pragma unroll
-                for(int r = 0; r < 3; r++) X[r] = B.f[C_X + r][ks];
-#pragma unroll
-                for(int r = 0; r < 9; r++) F[r] = B.f[C_F + r][ks];
-                const float4 at = B.at[ks];
-                const float V0 = B.f[C_V + r0][ks], V1 = B.f[C_V + r1][ks];
-#pragma unroll
-                for(int c2 = 0; c2 < 3; c2++) { B0[c2] = B.f[C_B + r0 + 3 * c2][ks]; B1[c2] = B.f[C_B + r1 + 3 * c2][ks]; }
-                float S[9];
-                if(!stress_fast(sc.model, F, at.z, at.w, S)) {
-                    if(!odd) a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = c0 + k;
-#pragma unroll
-                    for(int r = 0; r < 9; r++) S[r] = 0.f;
-                }
-                const float sv = a.dt * at.y, m = at.x;
-                const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
-                const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
-                const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
-                float dX[3][3];
-                const float bx = (float)wx.base + 0.5f, by = (float)wy.base + 0.5f, bz = (float)wz.base + 0.5f;
-#pragma unroll
-                for(int o = 0; o < 3; o++) {
-                    dX[0][o] = sc.dmin[0] + (bx + (float)o) * sc.dx[0] - X[0];
-                    dX[1][o] = sc.dmin[1] + (by + (float)o) * sc.dx[1] - X[1];
-                    dX[2][o] = sc.dmin[2] + (bz + (float)o) * sc.dx[2] - X[2];
-                }
-                const float Dm[3] = {4.f * sc.inv[0] * sc.inv[0] * m, 4.f * sc.inv[1] * sc.inv[1] * m,
-                                     4.f * sc.inv[2] * sc.inv[2] * m};
-                float mBD0[3], mBD1[3], S0[3], S1[3];
-#pragma unroll
-                for(int c2 = 0; c2 < 3; c2++) {
-                    // slot 0 of the even lane is the mass: V = 1, B = 0, PF^T = 0
-                    mBD0[c2] = odd ? B0[c2] * Dm[c2] : 0.f;
-                    mBD1[c2] = B1[c2] * Dm[c2];
-                    S0[c2] = odd ? S[1 + 3 * c2] * sv : 0.f;
-                    S1[c2] = (odd ? S[2 + 3 * c2] : S[3 * c2]) * sv;
-                }
-                PairSlot q0, q1;
-                pair_slot(wx, wy, wz, dX, odd ? m * V0 : m, mBD0, S0, q0);
-                pair_slot(wx, wy, wz, dX, m * V1, mBD1, S1, q1);
-                const float w9[9] = {wx.w[0], wx.w[1], wx.w[2], wy.w[0], wy.w[1], wy.w[2], wz.w[0], wz.w[1], wz.w[2]};
-                pair_accumulate(w9, q0, q1, acc0, acc1);
-            }
-            if(cell >= 0) pair_flush(cell, out0, out1, acc0, acc1);
-            __syncthreads();   // the next round overwrites the staged particles
-        }
-        p2g_end(a, T, b - sc.block_base);
-    }
-    p2g_finish(a, &T.work);
-}
-
 // Swap with the other lane of the pair.  Only the pair takes part: pairs of
 // one warp may run different trip counts.
 __device__ __forceinline__ unsigned pair_mask() { return 3u << ((threadIdx.x & 31) & ~1u); }
@@ -1310,12 +1176,12 @@ int grid_stride_blocks(mpm_handle* h, int64_t n, int t)
 
 // Launch shapes the autotuner chooses among.
 const int kG2PThreads[] = {64, 128, 256};
-const char* const kP2GNames[] = {"cells", "interleaved", "pairs", "pairx", "staged"};
+const char* const kP2GNames[] = {"cells", "interleaved", "pairs", "pairx"};
 
-int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult, size_t dyn_smem = 0)
+int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult)
 {
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, dyn_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, 0);
     return h->sm_count * (occ > 0 ? occ : 1) * mult;
 }
 
@@ -1475,7 +1341,6 @@ int fast_alloc(mpm_handle* h, int64_t n)
         MPM_CUDA(h, cudaMalloc(&f.sort_scratch, mpm_sort::scratch_words(np) * sizeof(uint32_t)));
         MPM_CUDA(h, cudaMemsetAsync(f.sort_scratch, 0, mpm_sort::scratch_words(np) * sizeof(uint32_t), h->stream));
         MPM_CUDA(h, mpm_sort::prepare());
-        MPM_CUDA(h, cudaFuncSetAttribute(k_p2g_staged<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(StageBuf)));
         f.n = n;
     }
     return MPM_OK;
@@ -1645,13 +1510,8 @@ int fast_p2g(mpm_handle* h, double dt, double)
             k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
         else if(f.p2g_variant == 2)
             k_p2g_pairs<128><<<occupancy_ctas(h, (const void*)k_p2g_pairs<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
-        else if(f.p2g_variant == 3)
+        else
             k_p2g_pairx<128><<<occupancy_ctas(h, (const void*)k_p2g_pairx<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
-        else {
-            static_assert(sizeof(StageBuf) % 16 == 0, "staging buffer alignment");
-            k_p2g_staged<128><<<occupancy_ctas(h, (const void*)k_p2g_staged<128>, 128, f.cta_mult, sizeof(StageBuf)), 128,
-                                sizeof(StageBuf), h->stream>>>(a);
-        }
         MPM_LAUNCHED(h, "k_p2g_pairs");
     }
     timer_end(h, slot);
@@ -1779,7 +1639,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
     const bool timing = h->timing;
     h->timing = false;
     int rc = MPM_OK;
-    for(int variant = 0; variant <= MPM_P2G_STAGED && !rc; variant++)
+    for(int variant = 0; variant <= MPM_P2G_PAIRX && !rc; variant++)
         for(int ti = 0; ti < 3 && !rc; ti++)
             for(int mult = 1; mult <= 2 && !rc; mult++) {
                 f.p2g_variant = variant;

@@ -23,7 +23,7 @@ LIB_PATH = os.path.join(HERE, "libphysbam_mpm.so")
 
 MPM_OK = 0
 FP32, FP64 = 0, 1
-P2G_CELLS, P2G_INTERLEAVED, P2G_PAIRS, P2G_PAIRX, P2G_STAGED = 0, 1, 2, 3, 4
+P2G_CELLS, P2G_INTERLEAVED, P2G_PAIRS, P2G_PAIRX = 0, 1, 2, 3
 PATH_FAST, PATH_PLAIN = 0, 1
 MAX_OBJECTS = 8
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "non-finite value", 4: "particle outside the grid",
