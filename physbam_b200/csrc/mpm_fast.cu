@@ -1056,6 +1056,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
     __shared__ SceneDev s_sc;
     // digit histograms of the keys this CTA writes (for the next sort)
     __shared__ uint32_t s_hist[mpm_sort::kMaxPasses][mpm_sort::kRadix];
+    __shared__ uint32_t s_stay;
     for(int i = threadIdx.x; i < mpm_sort::kMaxPasses * mpm_sort::kRadix; i += THREADS) (&s_hist[0][0])[i] = 0;
     // invalid particles, copied to the tail by k_ranges, keep sentinel keys
     if(blockIdx.x == 0 && threadIdx.x == 0)
@@ -1069,13 +1070,26 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
         int bx, by, bz;
         block_coords(sc, b - sc.block_base, bx, by, bz);
         const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;
+        if(threadIdx.x == 0) s_stay = 0;
         const bool anti = g2p_stage(a, sc, tv, ox, oy, oz, THREADS);
         const uint32_t s = a.bstart[b], e = a.bend[b];
+        uint32_t stay = 0;
         for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
             G2PState o;
             g2p_particle(a, sc, tv, anti, ox, oy, oz, j, o);
-            mpm_sort::hist_add(s_hist, o.key, a.key_bits);
+            // most particles stay in their block: their keys differ from the
+            // block's only in the lowest digit, counted per particle; the
+            // block's higher digits are counted once below
+            if((o.key >> 6) == b) {
+                mpm_sort::hist_add_low(s_hist, o.key, a.key_bits);
+                stay++;
+            } else {
+                mpm_sort::hist_add(s_hist, o.key, a.key_bits);
+            }
         }
+        if(stay) atomicAdd(&s_stay, stay);
+        __syncthreads();
+        if(threadIdx.x == 0 && s_stay) mpm_sort::hist_add_high(s_hist, b << 6, s_stay, a.key_bits);
     }
     __syncthreads();
     for(int i = threadIdx.x; i < mpm_sort::kMaxPasses * mpm_sort::kRadix; i += THREADS) {

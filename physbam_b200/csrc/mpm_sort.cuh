@@ -123,6 +123,22 @@ __device__ __forceinline__ void hist_add(uint32_t (*cnt)[kRadix], uint32_t key, 
     }
 }
 
+// Count the lowest digit only (the caller accounts for the others).
+__device__ __forceinline__ void hist_add_low(uint32_t (*cnt)[kRadix], uint32_t key, int bits)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned active = __activemask();
+    const uint32_t dg = key & digit_mask(bits, 0);
+    const uint32_t peers = __match_any_sync(active, dg);
+    if((__ffs(peers) - 1) == lane) atomicAdd(&cnt[0][dg], (uint32_t)__popc(peers));
+}
+
+// Add `count` keys that share `key`'s digits of passes 1 and up.
+__device__ __forceinline__ void hist_add_high(uint32_t (*cnt)[kRadix], uint32_t key, uint32_t count, int bits)
+{
+    for(int p = 1; p < passes_for(bits); p++) atomicAdd(&cnt[p][(key >> (8 * p)) & digit_mask(bits, p)], count);
+}
+
 // Add `count` sentinel keys (all bits set) to the global histograms.
 __device__ __forceinline__ void hist_add_sentinels(uint32_t* scratch, uint32_t count, int bits)
 {
