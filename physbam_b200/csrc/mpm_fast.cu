@@ -1206,6 +1206,7 @@ int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult)
 // ---------------------------------------------------------------------------
 int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, const mpm_collision_object* objs, int nobjs)
 {
+    h->fast.generation++;
     FastState& f = h->fast;
     if(count < 1 || count > 65535) return set_error(h, MPM_ERR_ARG, "between 1 and 65535 scenes");
     std::vector<SceneDev> sc(count);
@@ -1285,6 +1286,9 @@ int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, con
     }
     MPM_CUDA(h, cudaMalloc(&f.objs, f.objs_h.size() * sizeof(DevObject)));
     MPM_CUDA(h, cudaMemcpy(f.objs, f.objs_h.data(), f.objs_h.size() * sizeof(DevObject), cudaMemcpyHostToDevice));
+    f.grid_nodes = nodes;
+    f.grid_node_blocks = nblocks;
+    f.grid_dirty = false;
     MPM_CUDA(h, cudaMalloc(&f.acc, nodes * sizeof(float4)));
     MPM_CUDA(h, cudaMalloc(&f.vel, nodes * 2 * sizeof(float4)));
     MPM_CUDA(h, cudaMemset(f.acc, 0, nodes * sizeof(float4)));
@@ -1331,12 +1335,15 @@ int fast_alloc(mpm_handle* h, int64_t n)
     if(n >= (1LL << 30)) return set_error(h, MPM_ERR_ARG, "more than 2^30 - 1 particles");
     if(f.batch) {
         if(n != f.pbase_h.back()) return set_error(h, MPM_ERR_ARG, "particle count differs from the scenes' total");
-    } else {
+    } else if(!f.scenes || f.n != n) {
+        // a new particle count rebuilds the scene tables and every buffer;
+        // re-uploading the same count keeps them (and the captured graphs)
         int rc;
         f.n = n;
         if((rc = fast_single_scene(h))) return rc;
     }
     if(f.n != n || !f.soa[0]) {
+        f.generation++;
         for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; }
         uint32_t** ps[] = {&f.keys, &f.sorted_keys, &f.perm, &f.sort_keys_alt, &f.sort_vals_alt, &f.sort_scratch};
         for(uint32_t** p: ps) { cudaFree(*p); *p = nullptr; }
@@ -1380,6 +1387,11 @@ int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
     if(rc) return rc;
     FastState& f = h->fast;
     int64_t n = v->n;
+    if(f.grid_dirty) {   // a P2G without its grid update left mass in the kept accumulator
+        MPM_CUDA(h, cudaMemsetAsync(f.acc, 0, f.grid_nodes * sizeof(float4), h->stream));
+        MPM_CUDA(h, cudaMemsetAsync(f.nb_flag, 0, f.grid_node_blocks * sizeof(uint32_t), h->stream));
+        f.grid_dirty = false;
+    }
     f.cur = 0;
     f.keys_ready = n == 0;
     f.hist_ready = false;
@@ -1530,6 +1542,7 @@ int fast_p2g(mpm_handle* h, double dt, double)
     }
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_p2g");
+    f.grid_dirty = true;   // until the grid update reads and clears the accumulator
     return MPM_OK;
 }
 
@@ -1540,6 +1553,7 @@ int fast_forces(mpm_handle* h, double dt, double)
     FastArgs a = make_args(h, dt);
     int slot = timer_begin(h, "fast_grid");
     k_grid<<<h->sm_count * 8, 256, 0, h->stream>>>(a);
+    f.grid_dirty = false;
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_grid");
     return MPM_OK;

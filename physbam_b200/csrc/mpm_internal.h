@@ -79,7 +79,11 @@ struct FastState {
     float4* acc = nullptr;                    // P2G accumulator: momentum+dt*force (xyz), mass (w)
     float4* vel = nullptr;                    // per node 2 x float4: vnew.xyz, vfric.x | vfric.yz, mass, 0
     bool keys_ready = false;
-    bool hist_ready = false;   // sort_scratch holds the digit histograms of `keys` (built by G2P)
+    bool hist_ready = false;
+    uint64_t generation = 0;   // bumped whenever device buffers are (re)allocated
+    int64_t grid_nodes = 0;
+    uint32_t grid_node_blocks = 0;
+    bool grid_dirty = false;   // the accumulator holds a P2G that no grid update consumed   // sort_scratch holds the digit histograms of `keys` (built by G2P)
     // launch shapes (mpm_autotune)
     int p2g_variant = 0;                      // 0: thread per cell, 1: thread per particle, cells interleaved
     int g2p_threads = 128;
