@@ -374,6 +374,7 @@ int blocks_for(mpm_handle* h, int64_t n, int t, bool cap)
 
 // State snapshot sizes (elements of T): X 3n, V 3n, F 9n, B 9n, valid n bytes.
 struct DiffTape {
+    bool recorded = false;           // holds the forward pass of the current particles
     int64_t n = 0, gn = 0;
     int nsteps = 0, every = 0;
     double dt = 0;
@@ -390,6 +391,14 @@ struct DiffTape {
 };
 
 static DiffTape* tape(mpm_handle* h) { return reinterpret_cast<DiffTape*>(h->diff); }
+
+// New particles: the recorded rollout no longer applies; its buffers are kept
+// for the next mpm_diff_forward of the same shape.
+void diff_invalidate(mpm_handle* h)
+{
+    DiffTape* t = tape(h);
+    if(t) t->recorded = false;
+}
 
 void diff_free(mpm_handle* h)
 {
@@ -426,18 +435,28 @@ int diff_forward(mpm_handle* h, double dt, int nsteps, int every)
         return set_error(h, MPM_ERR_ARG, "the adjoint runs on the 3D plain path");
     if(h->sp.nobj) return set_error(h, MPM_ERR_ARG, "the adjoint does not differentiate collision objects");
     if(nsteps < 1 || every < 1) return set_error(h, MPM_ERR_ARG, "nsteps and checkpoint interval must be >= 1");
-    diff_free(h);
-    DiffTape* t = new DiffTape();
-    h->diff = t;
     PlainState& s = h->plain;
-    t->n = s.n; t->gn = s.gn; t->nsteps = nsteps; t->every = every; t->dt = dt;
-    t->esz = h->model.precision == MPM_FP64 ? 8 : 4;
+    const size_t esz = h->model.precision == MPM_FP64 ? 8 : 4;
+    DiffTape* t = tape(h);
+    // a tape of the same shape is reused as it is (no allocation)
+    const bool reuse = t && t->n == s.n && t->gn == s.gn && t->nsteps == nsteps && t->every == every && t->esz == esz;
+    if(!reuse) {
+        diff_free(h);
+        t = new DiffTape();
+        h->diff = t;
+        t->n = s.n; t->gn = s.gn; t->nsteps = nsteps; t->every = every;
+        t->esz = esz;
+    }
+    t->recorded = false;
+    t->dt = dt;
     size_t st = 24 * s.n * t->esz;
     int nck = (nsteps + every - 1) / every;
-    MPM_CUDA(h, cudaMalloc(&t->ckpt, nck * st + 1));
-    MPM_CUDA(h, cudaMalloc(&t->ckpt_valid, nck * s.n + 1));
-    MPM_CUDA(h, cudaMalloc(&t->final_state, st + 1));
-    MPM_CUDA(h, cudaMalloc(&t->final_valid, s.n + 1));
+    if(!reuse) {
+        MPM_CUDA(h, cudaMalloc(&t->ckpt, nck * st + 1));
+        MPM_CUDA(h, cudaMalloc(&t->ckpt_valid, nck * s.n + 1));
+        MPM_CUDA(h, cudaMalloc(&t->final_state, st + 1));
+        MPM_CUDA(h, cudaMalloc(&t->final_valid, s.n + 1));
+    }
     int rc;
     for(int k = 0; k < nsteps; k++) {
         if(k % every == 0) {
@@ -448,7 +467,9 @@ int diff_forward(mpm_handle* h, double dt, int nsteps, int every)
         if((rc = plain_forces(h, dt, 0))) return rc;
         if((rc = plain_g2p(h, dt, 0))) return rc;
     }
-    return state_copy(h, t->final_state, t->final_valid, true);
+    if((rc = state_copy(h, t->final_state, t->final_valid, true))) return rc;
+    t->recorded = true;
+    return MPM_OK;
 }
 
 template<class T> static int backward_t(mpm_handle* h, const void* gX, const void* gV, const void* gF, const void* gB,
@@ -551,7 +572,7 @@ template<class T> static int backward_t(mpm_handle* h, const void* gX, const voi
 int diff_backward(mpm_handle* h, const mpm_particles_view* gout, mpm_particles_view* gin, void* gmu, void* glam)
 {
     DiffTape* t = tape(h);
-    if(!t) return set_error(h, MPM_ERR_STATE, "mpm_diff_backward needs a recorded mpm_diff_forward");
+    if(!t || !t->recorded) return set_error(h, MPM_ERR_STATE, "mpm_diff_backward needs a recorded mpm_diff_forward");
     int prec = h->model.precision;
     if(gout->n != t->n || gin->n != t->n) return set_error(h, MPM_ERR_ARG, "particle count");
     if(gout->dtype != prec || gin->dtype != prec) return set_error(h, MPM_ERR_ARG, "gradient dtype must match the path precision");

@@ -267,7 +267,7 @@ int mpm_set_particles(mpm_handle* h, const mpm_particles_view* v)
 {
     if(!h || !v || v->n < 0) return MPM_ERR_ARG;
     if(v->dtype != MPM_FP32 && v->dtype != MPM_FP64) return set_error(h, MPM_ERR_ARG, "dtype");
-    diff_free(h);
+    diff_invalidate(h);
     const uint64_t gen = h->fast.generation;
     int rc = fast(h) ? fast_set_particles(h, v) : plain_set_particles(h, v);
     // captured substeps hold buffer addresses: keep them only if none moved

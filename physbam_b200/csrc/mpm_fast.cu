@@ -1376,9 +1376,29 @@ void fast_free(mpm_handle* h)
                    (void**)&f.nb_list, (void**)&f.counters, (void**)&f.acc, (void**)&f.vel, (void**)&f.scenes,
                    (void**)&f.block_scene, (void**)&f.nb_scene, (void**)&f.pbase, (void**)&f.objs};
     for(void** p: ps) { cudaFree(*p); *p = nullptr; }
+    cudaFree(f.staging);
+    f.staging = nullptr;
+    f.staging_bytes = 0;
     f.n = 0;
     f.npad = 0;
     f.keys_ready = false;
+}
+
+// The handle's staging buffer for host arrays, grown on demand and kept (the
+// stream is drained before it is replaced, since queued copies may use it).
+static int fast_staging(mpm_handle* h, size_t bytes, uint8_t** out)
+{
+    FastState& f = h->fast;
+    if(f.staging_bytes < bytes) {
+        MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+        cudaFree(f.staging);
+        f.staging = nullptr;
+        f.staging_bytes = 0;
+        MPM_CUDA(h, cudaMalloc(&f.staging, bytes));
+        f.staging_bytes = bytes;
+    }
+    *out = (uint8_t*)f.staging;
+    return MPM_OK;
 }
 
 int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
@@ -1402,25 +1422,29 @@ int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
     const void* src[8] = {v->X, v->V, v->F, v->B, v->mass, v->volume, v->mu, v->lambda};
     int64_t cnt[8] = {3 * n, 3 * n, 9 * n, 9 * n, n, n, n, n};
     void* dptr[8] = {};
-    void* owned[8] = {};
+    // host arrays go through the handle's staging buffer (kept between calls,
+    // so a re-upload allocates nothing): 28 scalars and 2 bytes per particle
+    uint8_t* stage = nullptr;
+    rc = fast_staging(h, (size_t)n * (28 * e + 2) + 256, &stage);
+    if(rc) return rc;
+    size_t off = 0;
     for(int i = 0; i < 8; i++) {
         if(!src[i]) return set_error(h, MPM_ERR_ARG, "null particle array");
         if(dev) dptr[i] = const_cast<void*>(src[i]);
         else {
-            MPM_CUDA(h, cudaMallocAsync(&owned[i], cnt[i] * e, h->stream));
-            MPM_CUDA(h, cudaMemcpyAsync(owned[i], src[i], cnt[i] * e, cudaMemcpyHostToDevice, h->stream));
-            dptr[i] = owned[i];
+            dptr[i] = stage + off;
+            off += cnt[i] * e;
+            MPM_CUDA(h, cudaMemcpyAsync(dptr[i], src[i], cnt[i] * e, cudaMemcpyHostToDevice, h->stream));
         }
     }
-    uint8_t *dvalid = nullptr, *valid_slot = nullptr;
+    uint8_t *dvalid = nullptr, *valid_slot = stage + (size_t)n * 28 * e + n;
     if(v->valid) {
         if(dev) dvalid = v->valid;
         else {
-            MPM_CUDA(h, cudaMallocAsync((void**)&dvalid, n, h->stream));
+            dvalid = stage + (size_t)n * 28 * e;
             MPM_CUDA(h, cudaMemcpyAsync(dvalid, v->valid, n, cudaMemcpyHostToDevice, h->stream));
         }
     }
-    MPM_CUDA(h, cudaMallocAsync((void**)&valid_slot, n, h->stream));
     FastArgs a = make_args(h, 0.0);
     a.dst = f.soa[0]; a.dst_attr = f.attr[0]; a.dst_pid = f.pid[0];
     int blocks = grid_stride_blocks(h, n, 256);
@@ -1434,9 +1458,7 @@ int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
     a = make_args(h, 0.0);
     k_init_keys<<<blocks, 256, 0, h->stream>>>(a, valid_slot);
     MPM_LAUNCHED(h, "k_init_keys");
-    for(int i = 0; i < 8; i++) if(owned[i]) MPM_CUDA(h, cudaFreeAsync(owned[i], h->stream));
-    if(v->valid && !dev) MPM_CUDA(h, cudaFreeAsync(dvalid, h->stream));
-    MPM_CUDA(h, cudaFreeAsync(valid_slot, h->stream));
+
     f.keys_ready = true;
     return MPM_OK;
 }
@@ -1452,16 +1474,19 @@ int fast_get_particles(mpm_handle* h, mpm_particles_view* v)
     void* dst[4] = {v->X, v->V, v->F, v->B};
     int64_t cnt[4] = {3 * n, 3 * n, 9 * n, 9 * n};
     void* dptr[4] = {};
+    uint8_t* stage = nullptr;
+    if(!dev) {
+        int rc = fast_staging(h, (size_t)n * (24 * e + 1) + 256, &stage);
+        if(rc) return rc;
+    }
+    size_t off = 0;
     for(int i = 0; i < 4; i++) {
         if(!dst[i]) continue;
         if(dev) dptr[i] = dst[i];
-        else MPM_CUDA(h, cudaMallocAsync(&dptr[i], cnt[i] * e, h->stream));
+        else { dptr[i] = stage + off; off += cnt[i] * e; }
     }
     uint8_t* dvalid = nullptr;
-    if(v->valid) {
-        if(dev) dvalid = v->valid;
-        else MPM_CUDA(h, cudaMallocAsync((void**)&dvalid, n, h->stream));
-    }
+    if(v->valid) dvalid = dev ? v->valid : stage + (size_t)n * 24 * e;
     FastArgs a = make_args(h, 0.0);
     int blocks = grid_stride_blocks(h, n, 256);
     if(e == 8) k_gather_out<double><<<blocks, 256, 0, h->stream>>>(a, f.keys, (double*)dptr[0], (double*)dptr[1], (double*)dptr[2], (double*)dptr[3], dvalid);
@@ -1471,12 +1496,8 @@ int fast_get_particles(mpm_handle* h, mpm_particles_view* v)
         for(int i = 0; i < 4; i++) {
             if(!dst[i]) continue;
             MPM_CUDA(h, cudaMemcpyAsync(dst[i], dptr[i], cnt[i] * e, cudaMemcpyDeviceToHost, h->stream));
-            MPM_CUDA(h, cudaFreeAsync(dptr[i], h->stream));
         }
-        if(dvalid) {
-            MPM_CUDA(h, cudaMemcpyAsync(v->valid, dvalid, n, cudaMemcpyDeviceToHost, h->stream));
-            MPM_CUDA(h, cudaFreeAsync(dvalid, h->stream));
-        }
+        if(dvalid) MPM_CUDA(h, cudaMemcpyAsync(v->valid, dvalid, n, cudaMemcpyDeviceToHost, h->stream));
     }
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;

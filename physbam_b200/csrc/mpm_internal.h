@@ -83,7 +83,9 @@ struct FastState {
     uint64_t generation = 0;   // bumped whenever device buffers are (re)allocated
     int64_t grid_nodes = 0;
     uint32_t grid_node_blocks = 0;
-    bool grid_dirty = false;   // the accumulator holds a P2G that no grid update consumed   // sort_scratch holds the digit histograms of `keys` (built by G2P)
+    bool grid_dirty = false;   // the accumulator holds a P2G that no grid update consumed
+    void* staging = nullptr;   // device copies of host particle arrays (set / get)
+    size_t staging_bytes = 0;   // sort_scratch holds the digit histograms of `keys` (built by G2P)
     // launch shapes (mpm_autotune)
     int p2g_variant = 0;                      // 0: thread per cell, 1: thread per particle, cells interleaved
     int g2p_threads = 128;
@@ -178,6 +180,7 @@ int plain_grid_totals(mpm_handle* h, mpm_totals* out);
 int diff_forward(mpm_handle* h, double dt, int nsteps, int every);
 int diff_backward(mpm_handle* h, const mpm_particles_view* gout, mpm_particles_view* gin, void* gmu, void* glam);
 void diff_free(mpm_handle* h);
+void diff_invalidate(mpm_handle* h);
 
 // helpers
 int set_error(mpm_handle* h, int code, const std::string& msg);
