@@ -242,6 +242,12 @@ int mpm_batch_create(const mpm_scene_desc* scenes, int count, const mpm_collisio
  * NULL) receives the timings. */
 int mpm_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len);
 
+/* mpm_autotune with flags.  MPM_AUTOTUNE_COLD_L2: write a buffer of twice the
+ * L2 size before each timed substep (untimed), so the choice holds for a
+ * caller whose substeps do not find the particles in L2 (substeps up to 64). */
+#define MPM_AUTOTUNE_COLD_L2 1
+int mpm_autotune_ex(mpm_handle* h, double dt, int substeps, int flags, char* report, int report_len);
+
 /* The fast path's launch shape, as mpm_autotune chooses it (no reference
  * counterpart: the reference's OpenMP loops have no launch configuration).
  * p2g_variant: MPM_P2G_CELLS (one thread per cell), MPM_P2G_INTERLEAVED (one

@@ -381,14 +381,20 @@ int mpm_batch_create(const mpm_scene_desc* scenes, int count, const mpm_collisio
     return MPM_OK;
 }
 
-int mpm_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len)
+int mpm_autotune_ex(mpm_handle* h, double dt, int substeps, int flags, char* report, int report_len)
 {
     int rc = check_dt(h, dt);
     if(rc) return rc;
     if(!fast(h)) return set_error(h, MPM_ERR_ARG, "the autotuner tunes the fast path");
+    if(flags & ~MPM_AUTOTUNE_COLD_L2) return set_error(h, MPM_ERR_ARG, "unknown autotune flag");
     release_graph(h);
-    if((rc = fast_autotune(h, dt, substeps, report, report_len))) return rc;
+    if((rc = fast_autotune(h, dt, substeps, flags, report, report_len))) return rc;
     return read_flags(h);
+}
+
+int mpm_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len)
+{
+    return mpm_autotune_ex(h, dt, substeps, 0, report, report_len);
 }
 
 int mpm_set_launch_shape(mpm_handle* h, int p2g_variant, int g2p_threads, int cta_mult)

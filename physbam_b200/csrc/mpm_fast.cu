@@ -1659,11 +1659,22 @@ int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_k
 // on the handle's own particles for a few substeps and keeps the fastest.  The
 // particle state is restored afterwards (the trials run on a copy).
 // ---------------------------------------------------------------------------
-int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len)
+int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* report, int report_len)
 {
     FastState& f = h->fast;
     if(!f.keys_ready || !f.n) return set_error(h, MPM_ERR_STATE, "particles not set");
     if(substeps < 1) substeps = 1;
+    if(substeps > 64) substeps = 64;
+    // cold L2: a buffer twice the L2 is written before every timed substep
+    const bool cold = flags & MPM_AUTOTUNE_COLD_L2;
+    void* scrub = nullptr;
+    size_t scrub_bytes = 0;
+    if(cold) {
+        int l2 = 0;
+        cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, h->device);
+        scrub_bytes = 2 * (size_t)(l2 > 0 ? l2 : (64 << 20));
+        MPM_CUDA(h, cudaMalloc(&scrub, scrub_bytes));
+    }
     // keep the current state: both buffers + keys
     const int64_t np = f.npad;
     float* save_soa = nullptr;
@@ -1679,9 +1690,8 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
     MPM_CUDA(h, cudaMemcpyAsync(save_attr, f.attr[cur0], np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream));
     MPM_CUDA(h, cudaMemcpyAsync(save_pid, f.pid[cur0], np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
     MPM_CUDA(h, cudaMemcpyAsync(save_keys, f.keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
+    cudaEvent_t e0[64], e1[64];
+    for(int k = 0; k < substeps; k++) { cudaEventCreate(&e0[k]); cudaEventCreate(&e1[k]); }
     std::string rep;
     float best = 1e30f;
     int best_v = f.p2g_variant, best_t = f.g2p_threads, best_m = f.cta_mult;
@@ -1702,13 +1712,20 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
                 cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
                 f.hist_ready = false;
                 if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_g2p(h, dt, 0))) break;
-                cudaEventRecord(e0, h->stream);
-                for(int s = 0; s < substeps && !rc; s++)
+                for(int s = 0; s < substeps && !rc; s++) {
+                    if(cold) cudaMemsetAsync(scrub, s & 0xff, scrub_bytes, h->stream);
+                    cudaEventRecord(e0[s], h->stream);
                     if(!(rc = fast_p2g(h, dt, 0)) && !(rc = fast_forces(h, dt, 0))) rc = fast_g2p(h, dt, 0);
-                cudaEventRecord(e1, h->stream);
-                if(cudaEventSynchronize(e1) != cudaSuccess) { rc = check_cuda(h, cudaGetLastError(), "autotune"); break; }
+                    cudaEventRecord(e1[s], h->stream);
+                }
+                if(rc) break;
+                if(cudaEventSynchronize(e1[substeps - 1]) != cudaSuccess) { rc = check_cuda(h, cudaGetLastError(), "autotune"); break; }
                 float ms = 0;
-                cudaEventElapsedTime(&ms, e0, e1);
+                for(int s = 0; s < substeps; s++) {
+                    float one = 0;
+                    cudaEventElapsedTime(&one, e0[s], e1[s]);
+                    ms += one;
+                }
                 ms /= substeps;
                 char line[128];
                 snprintf(line, sizeof line, "%sp2g=%s g2p=%d ctas=x%d: %.4f ms", rep.empty() ? "" : "; ",
@@ -1728,10 +1745,11 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int repo
     f.hist_ready = false;
     cudaStreamSynchronize(h->stream);
     cudaFree(save_soa); cudaFree(save_attr); cudaFree(save_pid); cudaFree(save_keys);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    for(int k = 0; k < substeps; k++) { cudaEventDestroy(e0[k]); cudaEventDestroy(e1[k]); }
+    cudaFree(scrub);
     char tail[128];
-    snprintf(tail, sizeof tail, " | chosen p2g=%s g2p=%d ctas=x%d (%.4f ms/substep)", kP2GNames[best_v], best_t, best_m, best);
+    snprintf(tail, sizeof tail, " | chosen p2g=%s g2p=%d ctas=x%d (%.4f ms/substep%s)", kP2GNames[best_v], best_t, best_m, best,
+             cold ? ", cold L2" : "");
     rep += tail;
     if(report && report_len > 0) snprintf(report, (size_t)report_len, "%s", rep.c_str());
     return rc;

@@ -168,7 +168,7 @@ int fast_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf);
 int fast_count_valid(mpm_handle* h, int64_t* c);
 int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm);
 int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, const mpm_collision_object* objs, int nobjs);
-int fast_autotune(mpm_handle* h, double dt, int substeps, char* report, int report_len);
+int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* report, int report_len);
 int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm);
 int fast_prepare_sort(mpm_handle* h);
 int fast_particle_totals(mpm_handle* h, mpm_totals* out);

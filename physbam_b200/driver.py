@@ -74,7 +74,7 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_grid_to_particle", "mpm_synchronize", "mpm_get_grid", "mpm_count_valid", "mpm_set_timing",
            "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state",
            "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune", "mpm_particle_totals",
-           "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape"]
+           "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex"]
 
 _lib = None
 
@@ -108,6 +108,7 @@ def load_library(path: str = LIB_PATH):
     L.mpm_diff_backward.argtypes = [P, ctypes.POINTER(ParticlesView), ctypes.POINTER(ParticlesView), P, P]
     L.mpm_radix_sort_u32.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P]
     L.mpm_autotune.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+    L.mpm_autotune_ex.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
     L.mpm_set_launch_shape.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.mpm_get_launch_shape.argtypes = [P] + [ctypes.POINTER(ctypes.c_int)] * 3
     L.mpm_particle_totals.argtypes = [P, ctypes.POINTER(Totals)]
@@ -371,12 +372,13 @@ class MPM_DRIVER:
         self._check(self.L.mpm_debug_sort_state(self.h, _ptr(keys), _ptr(sk), _ptr(perm)), "mpm_debug_sort_state")
         return keys, sk, perm
 
-    def autotune(self, substeps=3, dt=None):
+    def autotune(self, substeps=3, dt=None, cold_l2=False):
         """Time every launch-shape choice of the fast path on the current state
-        (restored after each trial) and keep the fastest; returns the report."""
+        (restored after each trial) and keep the fastest; returns the report.
+        cold_l2: scrub the L2 before every timed substep."""
         dt = self.scene.dt if dt is None else dt
         buf = ctypes.create_string_buffer(4096)
-        self._check(self.L.mpm_autotune(self.h, dt, substeps, buf, 4096), "mpm_autotune")
+        self._check(self.L.mpm_autotune_ex(self.h, dt, substeps, 1 if cold_l2 else 0, buf, 4096), "mpm_autotune_ex")
         return buf.value.decode()
 
     def set_launch_shape(self, p2g_variant, g2p_threads=128, cta_mult=1):

@@ -42,14 +42,15 @@ def test_batch_matches_individual_scenes(cuda_device):
         assert ex < 1e-6 and ef < 1e-4, (s.name, s.counts, ex, ef)
 
 
-def test_autotune_keeps_state_and_results(cuda_device):
+@pytest.mark.parametrize("cold", [False, True])
+def test_autotune_keeps_state_and_results(cuda_device, cold):
     from physbam_b200 import driver as D
     scenes = small_batch(count=4, seed=3)
     b1 = D.MPM_BATCH(scenes)
     b1.set_scene_particles()
     before = b1.get_particles()
-    report = b1.autotune(substeps=2)
-    assert "chosen" in report
+    report = b1.autotune(substeps=2, cold_l2=cold)
+    assert "chosen" in report and (("cold L2" in report) == cold)
     after = b1.get_particles()
     np.testing.assert_array_equal(before["X"], after["X"])
     b1.advance(6)
