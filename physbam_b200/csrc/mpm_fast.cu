@@ -733,7 +733,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 __device__ __forceinline__ unsigned pair_mask() { return 3u << ((threadIdx.x & 31) & ~1u); }
 __device__ __forceinline__ float shfl1(float v) { return __shfl_xor_sync(pair_mask(), v, 1); }
 
-template<int THREADS> __global__ void __launch_bounds__(THREADS, 384 / THREADS) k_p2g_pairx(FastArgs a)
+template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_p2g_pairx(FastArgs a)
 {
     __shared__ P2GTile T;
     const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
