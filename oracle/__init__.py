@@ -76,6 +76,8 @@ def lib():
         _lib.oracle_pft.argtypes = [ctypes.c_int, ctypes.c_int, P, ctypes.c_double, ctypes.c_double, P]
         _lib.oracle_svd3.argtypes = [P, P, P, P]
         _lib.oracle_svd3.restype = ctypes.c_int
+        _lib.oracle_plastic_clamp.argtypes = [ctypes.c_int, ctypes.c_longlong, P, P, P, P, P, P,
+                                              ctypes.POINTER(ctypes.c_ubyte), P]
     return _lib
 
 
@@ -118,6 +120,24 @@ class State:
         self.lam = np.ascontiguousarray(scene.lam, np.float64)
         self.valid = np.ones(scene.n, np.uint8)
         self.time = 0.0
+        if scene.plasticity is not None:   # as the reference seeds them (STANDARD_TESTS_BASE.cpp:299,568-586)
+            self.Fp = np.ascontiguousarray(np.tile(np.eye(d).reshape(1, d * d), (scene.n, 1)), np.float64)
+            self.mu0, self.lam0 = self.mu.copy(), self.lam.copy()
+            self.mu, self.lam = self.mu.copy(), self.lam.copy()
+
+    def Fp_rowmajor(self):
+        d = self.scene.dim
+        return np.swapaxes(self.Fp.reshape(-1, d, d), 1, 2)
+
+    def plasticity(self):
+        """Update_Plasticity_And_Hardening (MPM_DRIVER.cpp:922-928) after G2P."""
+        pl = self.scene.plasticity
+        if pl is None:
+            return
+        prm = np.array([pl.theta_c, pl.theta_s, pl.max_hardening, pl.hardening_factor], np.float64)
+        lib().oracle_plastic_clamp(self.scene.dim, self.scene.n, _ptr(self.F), _ptr(self.Fp), _ptr(self.mu),
+                                   _ptr(self.lam), _ptr(self.mu0), _ptr(self.lam0),
+                                   self.valid.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), _ptr(prm))
 
     def F_rowmajor(self):
         d = self.scene.dim
@@ -143,6 +163,7 @@ def substep(state: State, want_grid: bool = False):
                           state.valid.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), s.dt, state.time, *args)
     if rc:
         raise RuntimeError("oracle_substep failed: %d" % rc)
+    state.plasticity()
     state.time += s.dt
     if want_grid:
         shape = tuple(c + 6 for c in s.counts[:s.dim])
@@ -153,6 +174,10 @@ def substep(state: State, want_grid: bool = False):
 
 def run(state: State, nsteps: int):
     s = state.scene
+    if s.plasticity is not None:
+        for _ in range(nsteps):
+            substep(state)
+        return
     sc = _scene_struct(s)
     rc = lib().oracle_run(ctypes.byref(sc), s.n, _ptr(state.X), _ptr(state.V), _ptr(state.F), _ptr(state.B),
                           _ptr(state.mass), _ptr(state.vol), _ptr(state.mu), _ptr(state.lam),
@@ -192,7 +217,7 @@ def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timin
         if totals is not None:
             cmd += ["-totals", repr(float(totals[0])), repr(float(totals[1]))]
         out = subprocess.run(cmd, check=True, capture_output=True, text=True)
-        res = S.read_dump(dp, scene.dim, scene.n, scene.counts) if dumps else {}
+        res = S.read_dump(dp, scene.dim, scene.n, scene.counts, plastic=scene.plasticity is not None) if dumps else {}
         if totals is not None:
             import json
             lines = [ln for ln in out.stdout.splitlines() if ln.startswith('{"mass"')]

@@ -728,3 +728,73 @@ int oracle_run(const oracle_scene* sc, long long n, double* X, double* V, double
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* plasticity                                                           */
+/* ------------------------------------------------------------------ */
+static double det_cm(int d, const double* A)
+{
+    if(d == 2) return A[0] * A[3] - A[2] * A[1];
+    return A[0] * (A[4] * A[8] - A[7] * A[5]) - A[3] * (A[1] * A[8] - A[7] * A[2]) + A[6] * (A[1] * A[5] - A[4] * A[2]);
+}
+
+/* C = A B, column-major d x d */
+static void mul_cm(int d, const double* A, const double* B, double* C)
+{
+    for(int c = 0; c < d; c++)
+        for(int r = 0; r < d; r++) {
+            double s = 0;
+            for(int k = 0; k < d; k++) s += A[r + d * k] * B[k + d * c];
+            C[r + d * c] = s;
+        }
+}
+
+/* MPM_PLASTICITY_MODEL::Update_Particles (Hybrid_Methods/Forces/MPM_PLASTICITY_MODEL.cpp:35-49)
+ * with MPM_PLASTICITY_CLAMP::Compute (Hybrid_Methods/Forces/MPM_PLASTICITY_CLAMP.cpp:28-45),
+ * over the valid particles after G2P.  prm = theta_c, theta_s, max_hardening,
+ * hardening_factor.  F, Fp column-major per particle. */
+void oracle_plastic_clamp(int d, long long n, double* F, double* Fp, double* mu, double* la,
+    const double* mu0, const double* la0, const unsigned char* valid, const double* prm)
+{
+    const double lo = 1 - prm[0], hi = 1 + prm[1];
+    const int dd = d * d;
+    for(long long p = 0; p < n; p++) {
+        if(!valid[p]) continue;
+        double* Fe = F + p * dd;
+        double U[9], S[3], V[9];
+        if(d == 3) oracle_svd3(Fe, U, S, V);
+        else svd2(Fe, U, S, V);
+        double st[3];
+        int same = 1;
+        for(int a = 0; a < d; a++) {
+            st[a] = S[a] < lo ? lo : (S[a] > hi ? hi : S[a]);
+            if(st[a] != S[a]) same = 0;
+        }
+        if(same) continue;
+        /* hardening from det of the new Fp: det(Fe) / det(strain) * det(Fp) */
+        double pf = 1, ps = 1;
+        for(int a = 0; a < d; a++) { pf *= S[a]; ps *= st[a]; }
+        double det = pf / ps * det_cm(d, Fp + p * dd);
+        double e = prm[3] * (1 - det);
+        double coeff = exp(e < prm[2] ? e : prm[2]);
+        if(coeff < 1e-8) coeff = 1e-8;
+        mu[p] = mu0[p] * coeff;
+        la[p] = la0[p] * coeff;
+        /* F = U strain V^T;  Fp = V strain^-1 U^T Fe Fp */
+        double Us[9], Vi[9], Fn[9], T1[9], T2[9], Fe0[9];
+        memcpy(Fe0, Fe, dd * sizeof(double));
+        for(int c = 0; c < d; c++)
+            for(int r = 0; r < d; r++) { Us[r + d * c] = U[r + d * c] * st[c]; Vi[r + d * c] = V[r + d * c] / st[c]; }
+        for(int c = 0; c < d; c++)
+            for(int r = 0; r < d; r++) {
+                double s = 0, t = 0;
+                for(int k = 0; k < d; k++) { s += Us[r + d * k] * V[c + d * k]; t += Vi[r + d * k] * U[c + d * k]; }
+                Fn[r + d * c] = s;
+                T1[r + d * c] = t;
+            }
+        mul_cm(d, T1, Fe0, T2);
+        mul_cm(d, T2, Fp + p * dd, T1);
+        memcpy(Fe, Fn, dd * sizeof(double));
+        memcpy(Fp + p * dd, T1, dd * sizeof(double));
+    }
+}

@@ -25,6 +25,7 @@
 #include <Hybrid_Methods/Examples_And_Drivers/MPM_PARTICLES.h>
 #include <Hybrid_Methods/Forces/MPM_FINITE_ELEMENTS.h>
 #include <Hybrid_Methods/Forces/MPM_GRAVITY.h>
+#include <Hybrid_Methods/Forces/MPM_PLASTICITY_CLAMP.h>
 #include <Hybrid_Methods/Forces/MPM_FORCE_HELPER.h>
 #include <Hybrid_Methods/Iterators/GATHER_SCATTER.h>
 #include <chrono>
@@ -42,7 +43,8 @@ namespace {
 struct OBJ { int kind, type; double friction, a[3], b[3]; };
 struct SCENE_FILE
 {
-    int dim, counts[3], model, nsteps, nobj, ndump;
+    int dim, counts[3], model, nsteps, nobj, ndump, plasticity;
+    double plastic[4];   // theta_c, theta_s, max_hardening, hardening_factor
     double dmin[3], dmax[3], gravity[3], dt, t0;
     std::vector<int> dumps;
     std::vector<OBJ> objs;
@@ -66,7 +68,7 @@ SCENE_FILE Read_Scene(const char* path)
     int hdr[9];
     rd(f, hdr, 9);
     s.dim = hdr[0]; s.counts[0] = hdr[1]; s.counts[1] = hdr[2]; s.counts[2] = hdr[3];
-    s.model = hdr[4]; s.nsteps = hdr[5]; s.nobj = hdr[6]; s.ndump = hdr[7];
+    s.model = hdr[4]; s.nsteps = hdr[5]; s.nobj = hdr[6]; s.ndump = hdr[7]; s.plasticity = hdr[8];
     double dh[11];
     rd(f, dh, 11);
     for(int i = 0; i < 3; i++) { s.dmin[i] = dh[i]; s.dmax[i] = dh[3 + i]; s.gravity[i] = dh[6 + i]; }
@@ -78,6 +80,7 @@ SCENE_FILE Read_Scene(const char* path)
         rd(f, &o.kind, 1); rd(f, &o.type, 1); rd(f, &o.friction, 1); rd(f, o.a, 3); rd(f, o.b, 3);
         s.objs.push_back(o);
     }
+    if(s.plasticity) rd(f, s.plastic, 4);
     rd(f, &s.n, 1);
     size_t n = s.n, d = s.dim;
     s.X.resize(n * d); s.V.resize(n * d); s.F.resize(n * d * d); s.B.resize(n * d * d);
@@ -118,6 +121,7 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
         grid.Initialize(counts, RANGE<TV>(lo, hi), true);
         this->Set_Weights(2);
         particles.Store_Lame(true);
+        if(s.plasticity) particles.Store_Fp(true);   // also stores mu0, lambda0
         particles.Add_Elements((int)s.n);
         for(int p = 0; p < s.n; p++) {
             for(int a = 0; a < d; a++) {
@@ -133,7 +137,15 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
             particles.mu(p) = (T)s.mu[p];
             particles.lambda(p) = (T)s.lambda[p];
             particles.valid(p) = true;
+            if(s.plasticity) {   // as STANDARD_TESTS_BASE seeds and Set_Lame_On_Particles
+                particles.Fp(p).Set_Identity_Matrix();
+                particles.mu0(p) = particles.mu(p);
+                particles.lambda0(p) = particles.lambda(p);
+            }
         }
+        if(s.plasticity == 1)
+            this->plasticity_models.Append(new MPM_PLASTICITY_CLAMP<TV>(particles, &gather_scatter, (T)s.plastic[0],
+                (T)s.plastic[1], (T)s.plastic[2], (T)s.plastic[3]));
         ISOTROPIC_CONSTITUTIVE_MODEL<T, TV::m>* model;
         if(s.model == 0) model = new COROTATED_FIXED<T, TV::m>((T)1, (T).3);
         else model = new NEO_HOOKEAN<T, TV::m>((T)1, (T).3);
@@ -229,6 +241,16 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
         wr(f, gv0.data(), gv0.size());
         wr(f, gv.data(), gv.size());
         wr(f, gvf.data(), gvf.size());
+        if(s.plasticity) {
+            buf.resize(n * d * d);
+            for(size_t p = 0; p < n; p++) for(int k = 0; k < d * d; k++) buf[p * d * d + k] = example.particles.Fp(p).x[k];
+            wr(f, buf.data(), buf.size());
+            buf.resize(n);
+            for(size_t p = 0; p < n; p++) buf[p] = example.particles.mu(p);
+            wr(f, buf.data(), n);
+            for(size_t p = 0; p < n; p++) buf[p] = example.particles.lambda(p);
+            wr(f, buf.data(), n);
+        }
     }
     fclose(f);
     if(totals.on) {

@@ -58,6 +58,22 @@ class CollisionObject:
     b: Sequence[float]
 
 
+PLASTICITY_NONE, PLASTICITY_CLAMP = 0, 1
+
+
+@dataclasses.dataclass
+class Plasticity:
+    """Snow-like plasticity, MPM_PLASTICITY_CLAMP (`Hybrid_Methods/Forces/MPM_PLASTICITY_CLAMP.cpp:28-45`):
+    the singular values of F are clamped to [1 - theta_c, 1 + theta_s] after each G2P, the
+    clamped-off part goes to the plastic deformation Fp, and mu, lambda harden as
+    mu0 exp(min(max_hardening, hardening_factor (1 - det Fp)))."""
+    kind: int = PLASTICITY_CLAMP
+    theta_c: float = 2.5e-2
+    theta_s: float = 7.5e-3
+    max_hardening: float = 5.0
+    hardening_factor: float = 10.0
+
+
 @dataclasses.dataclass
 class Scene:
     name: str
@@ -78,6 +94,7 @@ class Scene:
     volume: np.ndarray
     mu: np.ndarray
     lam: np.ndarray
+    plasticity: Optional[Plasticity] = None
 
     @property
     def n(self) -> int:
@@ -305,6 +322,31 @@ def small_2d(seed=11, G=16, ppc=4, model=COROTATED, nsteps=20, dt=1e-4, friction
     return s
 
 
+def small_snow_3d(seed=21, G=16, nsteps=20, dt=1e-4, model=COROTATED):
+    """A small snow block thrown against a sticky floor: small_3d with clamped plasticity
+    (the initial shear already pushes singular values past the clamp)."""
+    s = small_3d(seed=seed, G=G, model=model, nsteps=nsteps, dt=dt, E=(1e4, 4e4), v=(0.5, -3.0, 0.25))
+    s.name = "smallsnow3d"
+    s.plasticity = Plasticity()
+    return s
+
+
+def small_snow_2d(seed=23, G=16, nsteps=20, dt=1e-4):
+    s = small_2d(seed=seed, G=G, nsteps=nsteps, dt=dt)
+    s.name = "smallsnow2d"
+    s.plasticity = Plasticity(theta_c=2e-2, theta_s=6e-3, max_hardening=4.0, hardening_factor=8.0)
+    return s
+
+
+def snowballs_3d(seed=1234, G=128, ppc=8, E=1.4e5, nu=0.2, density=400.0, dt=5e-5, nsteps=200):
+    """Two snowballs (r = 0.12) colliding in a 128^3 box, the spheres_3d geometry with the
+    Stomakhin et al. 2013 snow parameters (theta_c 2.5e-2, theta_s 7.5e-3, hardening 10)."""
+    s = spheres_3d(seed=seed, G=G, ppc=ppc, E=E, nu=nu, density=density, dt=dt, nsteps=nsteps, model=COROTATED)
+    s.name = "snowballs3d"
+    s.plasticity = Plasticity(max_hardening=10.0)
+    return s
+
+
 # --------------------------------------------------------------------------------------------
 # Scene file: read by the reference runner (oracle/ref_scene.cpp) and by the C oracle harness.
 # --------------------------------------------------------------------------------------------
@@ -318,11 +360,14 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
     with open(path, "wb") as f:
         f.write(MAGIC)
         counts = list(s.counts) + [1] * (3 - d)
-        f.write(struct.pack("<9i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), 0))
+        pl = s.plasticity
+        f.write(struct.pack("<9i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0))
         f.write(struct.pack("<11d", *pad3(s.domain_min), *pad3(s.domain_max), *pad3(s.gravity), s.dt, 0.0))
         f.write(struct.pack("<%di" % len(dumps), *dumps))
         for o in s.objects:
             f.write(struct.pack("<2i7d", o.kind, o.type, o.friction, *pad3(o.a), *pad3(o.b)))
+        if pl:
+            f.write(struct.pack("<4d", pl.theta_c, pl.theta_s, pl.max_hardening, pl.hardening_factor))
         f.write(struct.pack("<q", s.n))
         f.write(np.ascontiguousarray(s.X, np.float64).tobytes())
         f.write(np.ascontiguousarray(s.V, np.float64).tobytes())
@@ -333,12 +378,13 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
             f.write(np.ascontiguousarray(a, np.float64).tobytes())
 
 
-def read_dump(path, dim, n, counts):
+def read_dump(path, dim, n, counts, plastic=False):
     """Read the per-substep dumps written by the reference runner / C oracle.
 
     Record: int32 step; X (n,d); V (n,d); F (n,d,d col-major); B (same); valid u8[n];
     grid mass after P2G; grid velocity after P2G (``v = mv/m``, d per node); grid
-    velocity after forces; grid friction velocity after forces.  Grids cover the ghosted domain
+    velocity after forces; grid friction velocity after forces; with plasticity
+    also Fp (n,d,d col-major), mu (n), lambda (n).  Grids cover the ghosted domain
     (G+6)^d, last index fastest (`Core/Math_Tools/RANGE_ITERATOR.h`).
     """
     gshape = tuple(c + 2 * GHOST for c in counts[:dim])
@@ -360,6 +406,10 @@ def read_dump(path, dim, n, counts):
             rec["grid_v0"] = np.frombuffer(f.read(8 * gn * dim), np.float64).reshape(gshape + (dim,))
             rec["grid_v"] = np.frombuffer(f.read(8 * gn * dim), np.float64).reshape(gshape + (dim,))
             rec["grid_vf"] = np.frombuffer(f.read(8 * gn * dim), np.float64).reshape(gshape + (dim,))
+            if plastic:
+                rec["Fp"] = np.swapaxes(np.frombuffer(f.read(8 * n * dim * dim), np.float64).reshape(n, dim, dim), 1, 2)
+                rec["mu"] = np.frombuffer(f.read(8 * n), np.float64).copy()
+                rec["lam"] = np.frombuffer(f.read(8 * n), np.float64).copy()
             out[step] = rec
     return out
 
@@ -371,4 +421,7 @@ CONFIGS = {
     "cube3d": cube_3d,
     "small3d": small_3d,
     "small2d": small_2d,
+    "smallsnow3d": small_snow_3d,
+    "smallsnow2d": small_snow_2d,
+    "snowballs3d": snowballs_3d,
 }

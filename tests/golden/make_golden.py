@@ -6,7 +6,7 @@ scenes and freezes inputs plus dumps into ``<name>.npz``.  Needs the reference
 tree, so it runs only where that is present; the fixtures are committed so the
 tests never need it.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 """
 import os
 import sys
@@ -29,14 +29,19 @@ CASES = {
     "small3d_neohookean_friction": (lambda: S.small_3d(model=S.NEO_HOOKEAN, seed=9, friction=0.4), [0, 19], [0]),
     # BASELINE 2D case, exactly: 64^2, block 0.25^2 at (0.5,0.6), 4 ppc, corotated, sticky ground, 100 substeps
     "block2d_cfg": (lambda: S.block_2d(), [0, 9, 99], [0, 99]),
+    # snow: MPM_PLASTICITY_CLAMP after every G2P (Fp, hardened mu and lambda dumped too)
+    "smallsnow3d_corotated": (lambda: S.small_snow_3d(), [0, 19], [0, 19]),
+    "smallsnow2d_corotated": (lambda: S.small_snow_2d(), [0, 19], [19]),
 }
 
 
-def main():
+def main(names=None):
     oracle.build()
     if not oracle.ref_available():
         oracle.build_ref()
     for name, (make, dumps, grid_steps) in CASES.items():
+        if names and name not in names:
+            continue
         scene = make()
         ref = oracle.run_reference(scene, dumps, threads=1)
         arrays = dict(
@@ -50,9 +55,12 @@ def main():
             obj_b=np.array([o.b for o in scene.objects]).reshape(-1, scene.dim),
             X=scene.X, V=scene.V, F=scene.F, B=scene.B, mass=scene.mass, volume=scene.volume,
             mu=scene.mu, lam=scene.lam, dumps=np.array(dumps))
+        pl = scene.plasticity
+        if pl is not None:
+            arrays["plasticity"] = np.array([pl.kind, pl.theta_c, pl.theta_s, pl.max_hardening, pl.hardening_factor])
         for step in dumps:
             r = ref[step]
-            for k in ("X", "V", "F", "B", "valid"):
+            for k in ("X", "V", "F", "B", "valid") + (("Fp", "mu", "lam") if pl is not None else ()):
                 arrays["s%d_%s" % (step, k)] = r[k]
             if step in grid_steps:
                 for k in ("grid_m", "grid_v0", "grid_v", "grid_vf"):
@@ -71,11 +79,14 @@ def load(name):
                     list(z["gravity"]), float(z["dt"]), int(z["nsteps"]), objs,
                     z["X"].copy(), z["V"].copy(), z["F"].copy(), z["B"].copy(), z["mass"].copy(),
                     z["volume"].copy(), z["mu"].copy(), z["lam"].copy())
+    if "plasticity" in z:
+        p = z["plasticity"]
+        scene.plasticity = S.Plasticity(int(p[0]), float(p[1]), float(p[2]), float(p[3]), float(p[4]))
     dumps = {}
     for step in z["dumps"]:
         step = int(step)
         rec = {}
-        for k in ("X", "V", "F", "B", "valid", "grid_m", "grid_v0", "grid_v", "grid_vf"):
+        for k in ("X", "V", "F", "B", "valid", "grid_m", "grid_v0", "grid_v", "grid_vf", "Fp", "mu", "lam"):
             key = "s%d_%s" % (step, k)
             if key in z:
                 rec[k] = z[key]
@@ -84,4 +95,4 @@ def load(name):
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

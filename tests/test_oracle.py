@@ -15,7 +15,7 @@ from physbam_b200 import scenes as S
 # few ulps per step; B carries a cancellation (sum w vf Z - Vpf X) that
 # amplifies ulps by |Z|/dx, hence its looser bound.
 TOL = {"X": 1e-13, "V": 1e-12, "F": 1e-12, "B": 1e-11, "grid_m": 1e-13, "grid_v0": 1e-12,
-       "grid_v": 1e-12, "grid_vf": 1e-12}
+       "grid_v": 1e-12, "grid_vf": 1e-12, "Fp": 1e-12, "mu": 1e-12, "lam": 1e-12}
 
 
 def rel(a, b, floor=1e-300):
@@ -28,7 +28,7 @@ def rel(a, b, floor=1e-300):
 def floors(scene, ref):
     vmax = max(float(np.max(np.abs(ref["V"]))), 1e-12)
     return {"X": 1.0, "V": vmax, "F": 1.0, "B": vmax / scene.dx, "grid_m": 1e-300, "grid_v0": vmax,
-            "grid_v": vmax, "grid_vf": vmax}
+            "grid_v": vmax, "grid_vf": vmax, "Fp": 1.0, "mu": 1e-300, "lam": 1e-300}
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -44,6 +44,8 @@ def test_oracle_matches_reference_dumps(name):
         np.testing.assert_array_equal(st.valid.astype(bool), ref["valid"])
         fl = floors(scene, ref)
         got = {"X": st.X, "V": st.V, "F": st.F_rowmajor(), "B": st.B_rowmajor()}
+        if scene.plasticity is not None:
+            got.update(Fp=st.Fp_rowmajor(), mu=st.mu, lam=st.lam)
         for k, v in got.items():
             e = rel(v, ref[k], fl[k])
             assert e < TOL[k], (name, step, k, e)
@@ -125,3 +127,17 @@ def test_totals_match_reference(dim):
     dt = oracle.compute_dt(got["max_affine_speed"], scene.dx, cfl, max_dt)
     assert dt < max_dt
     assert dt == pytest.approx(ref["dt"], rel=1e-13)
+
+
+def test_snow_fixtures_exercise_plasticity():
+    """The snow fixtures clamp singular values and harden: Fp leaves the identity
+    and mu grows for some particles."""
+    for name in ("smallsnow3d_corotated", "smallsnow2d_corotated"):
+        scene, dumps = load(name)
+        ref = dumps[max(dumps)]
+        d = scene.dim
+        assert np.abs(ref["Fp"] - np.eye(d)).max() > 1e-3, name
+        assert (ref["mu"] / scene.mu).max() > 1.05, name
+        sv = np.linalg.svd(ref["F"], compute_uv=False)
+        pl = scene.plasticity
+        assert sv.min() >= 1 - pl.theta_c - 1e-12 and sv.max() <= 1 + pl.theta_s + 1e-12, name
