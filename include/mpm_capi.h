@@ -169,6 +169,43 @@ int mpm_grid_to_particle(mpm_handle* h, double dt, double time);  /* MPM_DRIVER:
  * (NaN, domain, non-convergence). */
 int mpm_synchronize(mpm_handle* h);
 
+/* ---- plasticity ----------------------------------------------------------- */
+
+/* Snow plasticity, MPM_PLASTICITY_CLAMP (Hybrid_Methods/Forces/
+ * MPM_PLASTICITY_CLAMP.cpp:28-45), applied after each G2P to every particle
+ * simulated in the substep (valid at its start, including one that left the
+ * domain in that G2P) as MPM_DRIVER::Update_Plasticity_And_Hardening
+ * (MPM_DRIVER.cpp:156,922-928).  The fast path runs it in FP32 inside G2P. */
+enum mpm_plasticity_kind { MPM_PLASTICITY_NONE = 0, MPM_PLASTICITY_CLAMP = 1 };
+typedef struct {
+    int kind;
+    double theta_c;            /* singular values are clamped to [1 - theta_c, 1 + theta_s] */
+    double theta_s;
+    double max_hardening;      /* hardening = exp(min(max_hardening, hardening_factor (1 - det Fp))) */
+    double hardening_factor;
+} mpm_plasticity_desc;
+
+/* Turn plasticity on or off (before or after mpm_set_particles).  Particles
+ * then start unplastic: Fp = I, mu0 = mu, lambda0 = lambda, as the
+ * reference's scenes seed them (Projects/mpm/STANDARD_TESTS_BASE.cpp:299,568-586). */
+int mpm_set_plasticity(mpm_handle* h, const mpm_plasticity_desc* p);
+
+/* The plastic state of MPM_PARTICLES (Fp, and mu0/lambda0 with the hardened
+ * mu/lambda): Fp n*d*d column-major, the others n scalars.  Any pointer may be
+ * NULL (not copied). */
+typedef struct {
+    int64_t n;
+    int dtype;
+    int on_device;
+    void* Fp;
+    void* mu;
+    void* lambda;
+    void* mu0;
+    void* lambda0;
+} mpm_plastic_view;
+int mpm_get_plastic_state(mpm_handle* h, mpm_plastic_view* view);
+int mpm_set_plastic_state(mpm_handle* h, const mpm_plastic_view* view);
+
 /* ---- inspection ---------------------------------------------------------- */
 
 /* Grids of the last substep as doubles on the host, each (G+6)^d nodes (times

@@ -129,15 +129,17 @@ class State:
         d = self.scene.dim
         return np.swapaxes(self.Fp.reshape(-1, d, d), 1, 2)
 
-    def plasticity(self):
-        """Update_Plasticity_And_Hardening (MPM_DRIVER.cpp:922-928) after G2P."""
+    def plasticity(self, simulated):
+        """Update_Plasticity_And_Hardening (MPM_DRIVER.cpp:922-928) after G2P, over the particles
+        simulated in the substep (valid at its start, MPM_DRIVER::Update_Simulated_Particles)."""
         pl = self.scene.plasticity
         if pl is None:
             return
         prm = np.array([pl.theta_c, pl.theta_s, pl.max_hardening, pl.hardening_factor], np.float64)
+        sim = np.ascontiguousarray(simulated, np.uint8)
         lib().oracle_plastic_clamp(self.scene.dim, self.scene.n, _ptr(self.F), _ptr(self.Fp), _ptr(self.mu),
                                    _ptr(self.lam), _ptr(self.mu0), _ptr(self.lam0),
-                                   self.valid.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), _ptr(prm))
+                                   sim.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), _ptr(prm))
 
     def F_rowmajor(self):
         d = self.scene.dim
@@ -158,12 +160,13 @@ def substep(state: State, want_grid: bool = False):
     if want_grid:
         grids = [np.zeros(gn), np.zeros(gn * s.dim), np.zeros(gn * s.dim), np.zeros(gn * s.dim)]
         args = [_ptr(g) for g in grids]
+    simulated = state.valid.copy()
     rc = L.oracle_substep(ctypes.byref(sc), s.n, _ptr(state.X), _ptr(state.V), _ptr(state.F), _ptr(state.B),
                           _ptr(state.mass), _ptr(state.vol), _ptr(state.mu), _ptr(state.lam),
                           state.valid.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), s.dt, state.time, *args)
     if rc:
         raise RuntimeError("oracle_substep failed: %d" % rc)
-    state.plasticity()
+    state.plasticity(simulated)
     state.time += s.dt
     if want_grid:
         shape = tuple(c + 6 for c in s.counts[:s.dim])

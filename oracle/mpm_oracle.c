@@ -751,7 +751,8 @@ static void mul_cm(int d, const double* A, const double* B, double* C)
 
 /* MPM_PLASTICITY_MODEL::Update_Particles (Hybrid_Methods/Forces/MPM_PLASTICITY_MODEL.cpp:35-49)
  * with MPM_PLASTICITY_CLAMP::Compute (Hybrid_Methods/Forces/MPM_PLASTICITY_CLAMP.cpp:28-45),
- * over the valid particles after G2P.  prm = theta_c, theta_s, max_hardening,
+ * after G2P over the particles simulated in the substep (`valid` holds their
+ * validity at its start).  prm = theta_c, theta_s, max_hardening,
  * hardening_factor.  F, Fp column-major per particle. */
 void oracle_plastic_clamp(int d, long long n, double* F, double* Fp, double* mu, double* la,
     const double* mu0, const double* la0, const unsigned char* valid, const double* prm)

@@ -452,6 +452,46 @@ int mpm_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_ke
     return fast_debug_sort_state(h, slot_keys, sorted_keys, perm);
 }
 
+int mpm_set_plasticity(mpm_handle* h, const mpm_plasticity_desc* p)
+{
+    if(!h || !p) return MPM_ERR_ARG;
+    if(p->kind != MPM_PLASTICITY_NONE && p->kind != MPM_PLASTICITY_CLAMP) return set_error(h, MPM_ERR_ARG, "unknown plasticity kind");
+    if(p->kind) {
+        if(!(p->theta_c >= 0 && p->theta_c < 1) || !(p->theta_s >= 0) || !std::isfinite(p->theta_s))
+            return set_error(h, MPM_ERR_ARG, "clamp bounds: 0 <= theta_c < 1, 0 <= theta_s");
+        if(std::isnan(p->max_hardening) || !std::isfinite(p->hardening_factor))
+            return set_error(h, MPM_ERR_ARG, "hardening parameters");
+    }
+    release_graph(h);
+    const bool was_on = h->plastic.kind != MPM_PLASTICITY_NONE;
+    h->plastic = *p;
+    if(p->kind && !was_on && h->have_particles) {
+        int rc = fast(h) ? fast_plastic_init(h) : plain_plastic_init(h);
+        if(rc) return rc;
+        MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    return MPM_OK;
+}
+
+int mpm_get_plastic_state(mpm_handle* h, mpm_plastic_view* v)
+{
+    if(!h || !v) return MPM_ERR_ARG;
+    if(!h->plastic.kind) return set_error(h, MPM_ERR_STATE, "plasticity is off");
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    if(v->dtype != MPM_FP32 && v->dtype != MPM_FP64) return set_error(h, MPM_ERR_ARG, "dtype");
+    return fast(h) ? fast_get_plastic(h, v) : plain_get_plastic(h, v);
+}
+
+int mpm_set_plastic_state(mpm_handle* h, const mpm_plastic_view* v)
+{
+    if(!h || !v) return MPM_ERR_ARG;
+    if(!h->plastic.kind) return set_error(h, MPM_ERR_STATE, "plasticity is off");
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    if(v->dtype != MPM_FP32 && v->dtype != MPM_FP64) return set_error(h, MPM_ERR_ARG, "dtype");
+    release_graph(h);
+    return fast(h) ? fast_set_plastic(h, v) : plain_set_plastic(h, v);
+}
+
 int mpm_particle_totals(mpm_handle* h, mpm_totals* out)
 {
     if(!h || !out) return MPM_ERR_ARG;

@@ -44,6 +44,7 @@ constexpr int TN = TE * TE * TE;           // 216 nodes per tile
 constexpr uint32_t SENTINEL = 0xffffffffu;
 constexpr int NCOMP = 24;                  // x3 v3 F9 B9 floats per particle
 constexpr int C_X = 0, C_V = 3, C_F = 6, C_B = 15;
+constexpr int NPLAS = 11;                  // plastic state: Fp0..8, mu0, lambda0 floats per particle
 
 struct FastArgs {
     int64_t n, npad;
@@ -70,6 +71,9 @@ struct FastArgs {
     int nscenes;
     float dt;
     unsigned* flags;
+    const float* psrc;    // plastic state (null: plasticity off), current and next buffer
+    float* pdst;
+    float prm[4];         // theta_c, theta_s, max_hardening, hardening_factor
 };
 
 __device__ __forceinline__ int64_t node_index(const SceneDev& sc, int qx, int qy, int qz)
@@ -227,6 +231,8 @@ __global__ void k_ranges(FastArgs a)
             for(int c = 0; c < NCOMP; c++) a.dst[c * a.npad + j] = a.src[c * a.npad + i];
             a.dst_attr[j] = a.src_attr[i];
             a.dst_pid[j] = a.src_pid[i];
+            if(a.psrc)
+                for(int c = 0; c < NPLAS; c++) a.pdst[c * a.npad + j] = a.psrc[c * a.npad + i];
             a.keys_next[j] = SENTINEL;
             continue;
         }
@@ -938,6 +944,19 @@ struct G2PState {
     bool ok;
 };
 
+// MPM_DRIVER::Update_Plasticity_And_Hardening (MPM_DRIVER.cpp:922-928) with
+// MPM_PLASTICITY_CLAMP for one particle after its G2P: F, Fp and the Lame
+// parameters (at.z, at.w) in place.  Out of line: the SVD's registers stay
+// off the G2P loop.
+__device__ __noinline__ void plastic_fast(float* F, float* Fp, float4& at, float mu0, float la0, const float* prm, unsigned* flags)
+{
+    bool ok;
+    float mu = at.z, la = at.w;
+    if(plastic_clamp<float, 3>(F, Fp, mu, la, mu0, la0, prm, ok)) { at.z = mu; at.w = la; }
+    if(!ok) atomicOr(flags, MPM_FLAG_NOT_CONVERGED);
+}
+
+template<bool PLASTIC>
 __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& sc, const float4* tv, bool anti,
     int ox, int oy, int oz, uint32_t j, G2PState& out)
 {
@@ -948,7 +967,7 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
     for(int k = 0; k < 3; k++) X[k] = a.src[(C_X + k) * a.npad + i];
 #pragma unroll
     for(int k = 0; k < 9; k++) F[k] = a.src[(C_F + k) * a.npad + i];
-    const float4 at = a.src_attr[i];
+    float4 at = a.src_attr[i];
     const int pid = a.src_pid[i];
     Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
     Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
@@ -1034,6 +1053,18 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
     for(int k = 0; k < 9; k++) finite = finite && isfinite(Fn[k]);
     finite = finite && isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]);
     if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); ok = false; }
+    if(PLASTIC) {
+        // every particle of this substep, including one that just left
+        float Fp[9];
+#pragma unroll
+        for(int k = 0; k < 9; k++) Fp[k] = a.psrc[k * a.npad + i];
+        const float mu0 = a.psrc[9 * a.npad + i], la0 = a.psrc[10 * a.npad + i];
+        if(finite) plastic_fast(Fn, Fp, at, mu0, la0, a.prm, a.flags);
+#pragma unroll
+        for(int k = 0; k < 9; k++) a.pdst[k * a.npad + j] = Fp[k];
+        a.pdst[9 * a.npad + j] = mu0;
+        a.pdst[10 * a.npad + j] = la0;
+    }
     const uint32_t key = ok ? cell_key(sc, xn) : SENTINEL;
 #pragma unroll
     for(int k = 0; k < 3; k++) { a.dst[(C_X + k) * a.npad + j] = xn[k]; a.dst[(C_V + k) * a.npad + j] = Vf[k]; }
@@ -1049,7 +1080,7 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
     out.ok = ok;
 }
 
-template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
+template<int THREADS, bool PLASTIC> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
 {
     __shared__ float4 tv[2 * TN];
     __shared__ int s_work;
@@ -1076,7 +1107,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs 
         uint32_t stay = 0;
         for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
             G2PState o;
-            g2p_particle(a, sc, tv, anti, ox, oy, oz, j, o);
+            g2p_particle<PLASTIC>(a, sc, tv, anti, ox, oy, oz, j, o);
             // most particles stay in their block: their keys differ from the
             // block's only in the lowest digit, counted per particle; the
             // block's higher digits are counted once below
@@ -1129,6 +1160,47 @@ template<class T> __global__ void k_gather_out(FastArgs a, const uint32_t* keys,
     }
 }
 
+// Plastic state of the current buffer: unplastic start (Fp = I, mu0 = mu,
+// lambda0 = lambda), and exchange with the caller's particle order.
+__global__ void k_plastic_init(int64_t n, int64_t npad, float* P, const float4* attr)
+{
+    for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for(int k = 0; k < 9; k++) P[k * npad + j] = k % 4 == 0 ? 1.f : 0.f;
+        const float4 at = attr[j];
+        P[9 * npad + j] = at.z;
+        P[10 * npad + j] = at.w;
+    }
+}
+
+template<class T> __global__ void k_plastic_out(int64_t n, int64_t npad, const float* P, const float4* attr, const int* pid,
+    T* Fp, T* mu, T* la, T* mu0, T* la0)
+{
+    for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = pid[j];
+        if(Fp)
+            for(int k = 0; k < 9; k++) Fp[p * 9 + k] = (T)P[k * npad + j];
+        if(mu) mu[p] = (T)attr[j].z;
+        if(la) la[p] = (T)attr[j].w;
+        if(mu0) mu0[p] = (T)P[9 * npad + j];
+        if(la0) la0[p] = (T)P[10 * npad + j];
+    }
+}
+
+template<class T> __global__ void k_plastic_in(int64_t n, int64_t npad, float* P, float4* attr, const int* pid,
+    const T* Fp, const T* mu, const T* la, const T* mu0, const T* la0)
+{
+    for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = pid[j];
+        if(Fp)
+            for(int k = 0; k < 9; k++) P[k * npad + j] = (float)Fp[p * 9 + k];
+        if(mu) attr[j].z = (float)mu[p];
+        if(la) attr[j].w = (float)la[p];
+        if(mu0) P[9 * npad + j] = (float)mu0[p];
+        if(la0) P[10 * npad + j] = (float)la0[p];
+    }
+}
+
 // Grids of scene 0 in the reference's ghosted layout (single-scene handles).
 __global__ void k_grid_out(FastArgs a, const uint32_t* list, uint32_t count, double* m, double* v, double* vf, int G0, int G1, int G2)
 {
@@ -1178,6 +1250,13 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.nscenes = f.nscenes;
     a.dt = (float)dt;
     a.flags = h->d_flags;
+    const bool plastic = h->plastic.kind != MPM_PLASTICITY_NONE && f.plas[0];
+    a.psrc = plastic ? f.plas[c] : nullptr;
+    a.pdst = plastic ? f.plas[o] : nullptr;
+    a.prm[0] = (float)h->plastic.theta_c;
+    a.prm[1] = (float)h->plastic.theta_s;
+    a.prm[2] = (float)h->plastic.max_hardening;
+    a.prm[3] = (float)h->plastic.hardening_factor;
     return a;
 }
 
@@ -1344,7 +1423,10 @@ int fast_alloc(mpm_handle* h, int64_t n)
     }
     if(f.n != n || !f.soa[0]) {
         f.generation++;
-        for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; }
+        for(int b = 0; b < 2; b++) {
+            cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); cudaFree(f.plas[b]);
+            f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; f.plas[b] = nullptr;
+        }
         uint32_t** ps[] = {&f.keys, &f.sorted_keys, &f.perm, &f.sort_keys_alt, &f.sort_vals_alt, &f.sort_scratch};
         for(uint32_t** p: ps) { cudaFree(*p); *p = nullptr; }
         int64_t np = ((n ? n : 1) + 31) / 32 * 32;
@@ -1370,7 +1452,10 @@ int fast_alloc(mpm_handle* h, int64_t n)
 void fast_free(mpm_handle* h)
 {
     FastState& f = h->fast;
-    for(int b = 0; b < 2; b++) { cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; }
+    for(int b = 0; b < 2; b++) {
+        cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); cudaFree(f.plas[b]);
+        f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; f.plas[b] = nullptr;
+    }
     void** ps[] = {(void**)&f.keys, (void**)&f.sorted_keys, (void**)&f.perm, (void**)&f.sort_keys_alt, (void**)&f.sort_vals_alt,
                    (void**)&f.sort_scratch, (void**)&f.bstart, (void**)&f.bend, (void**)&f.active, (void**)&f.nb_flag,
                    (void**)&f.nb_list, (void**)&f.counters, (void**)&f.acc, (void**)&f.vel, (void**)&f.scenes,
@@ -1460,6 +1545,97 @@ int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
     MPM_LAUNCHED(h, "k_init_keys");
 
     f.keys_ready = true;
+    if(h->plastic.kind) return fast_plastic_init(h);
+    return MPM_OK;
+}
+
+// Allocate the plastic state if needed and start it unplastic.
+int fast_plastic_init(mpm_handle* h)
+{
+    FastState& f = h->fast;
+    if(!f.soa[0]) return MPM_OK;
+    if(!f.plas[0])
+        for(int b = 0; b < 2; b++) MPM_CUDA(h, cudaMalloc(&f.plas[b], NPLAS * f.npad * sizeof(float)));
+    if(!f.n) return MPM_OK;
+    k_plastic_init<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(f.n, f.npad, f.plas[f.cur], f.attr[f.cur]);
+    MPM_LAUNCHED(h, "k_plastic_init");
+    return MPM_OK;
+}
+
+int fast_get_plastic(mpm_handle* h, mpm_plastic_view* v)
+{
+    FastState& f = h->fast;
+    if(v->n != f.n) return set_error(h, MPM_ERR_ARG, "particle count differs from mpm_set_particles");
+    if(!f.plas[0]) return set_error(h, MPM_ERR_STATE, "no plastic state");
+    const int64_t n = v->n;
+    if(!n) return MPM_OK;
+    const bool dev = v->on_device != 0;
+    const size_t e = v->dtype == MPM_FP64 ? 8 : 4;
+    void* dst[5] = {v->Fp, v->mu, v->lambda, v->mu0, v->lambda0};
+    const int64_t cnt[5] = {9 * n, n, n, n, n};
+    void* dptr[5] = {};
+    uint8_t* stage = nullptr;
+    if(!dev) {
+        int rc = fast_staging(h, (size_t)n * 13 * e + 256, &stage);
+        if(rc) return rc;
+    }
+    size_t off = 0;
+    for(int i = 0; i < 5; i++) {
+        if(!dst[i]) continue;
+        if(dev) dptr[i] = dst[i];
+        else { dptr[i] = stage + off; off += cnt[i] * e; }
+    }
+    const int blocks = grid_stride_blocks(h, n, 256), c = f.cur;
+    if(e == 8)
+        k_plastic_out<double><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], (double*)dptr[0],
+            (double*)dptr[1], (double*)dptr[2], (double*)dptr[3], (double*)dptr[4]);
+    else
+        k_plastic_out<float><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], (float*)dptr[0],
+            (float*)dptr[1], (float*)dptr[2], (float*)dptr[3], (float*)dptr[4]);
+    MPM_LAUNCHED(h, "k_plastic_out");
+    if(!dev)
+        for(int i = 0; i < 5; i++)
+            if(dst[i]) MPM_CUDA(h, cudaMemcpyAsync(dst[i], dptr[i], cnt[i] * e, cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+int fast_set_plastic(mpm_handle* h, const mpm_plastic_view* v)
+{
+    FastState& f = h->fast;
+    if(v->n != f.n) return set_error(h, MPM_ERR_ARG, "particle count differs from mpm_set_particles");
+    if(!f.plas[0]) return set_error(h, MPM_ERR_STATE, "no plastic state");
+    const int64_t n = v->n;
+    if(!n) return MPM_OK;
+    const bool dev = v->on_device != 0;
+    const size_t e = v->dtype == MPM_FP64 ? 8 : 4;
+    const void* src[5] = {v->Fp, v->mu, v->lambda, v->mu0, v->lambda0};
+    const int64_t cnt[5] = {9 * n, n, n, n, n};
+    const void* dptr[5] = {};
+    uint8_t* stage = nullptr;
+    if(!dev) {
+        int rc = fast_staging(h, (size_t)n * 13 * e + 256, &stage);
+        if(rc) return rc;
+    }
+    size_t off = 0;
+    for(int i = 0; i < 5; i++) {
+        if(!src[i]) continue;
+        if(dev) dptr[i] = src[i];
+        else {
+            dptr[i] = stage + off;
+            MPM_CUDA(h, cudaMemcpyAsync(stage + off, src[i], cnt[i] * e, cudaMemcpyHostToDevice, h->stream));
+            off += cnt[i] * e;
+        }
+    }
+    const int blocks = grid_stride_blocks(h, n, 256), c = f.cur;
+    if(e == 8)
+        k_plastic_in<double><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], (const double*)dptr[0],
+            (const double*)dptr[1], (const double*)dptr[2], (const double*)dptr[3], (const double*)dptr[4]);
+    else
+        k_plastic_in<float><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], (const float*)dptr[0],
+            (const float*)dptr[1], (const float*)dptr[2], (const float*)dptr[3], (const float*)dptr[4]);
+    MPM_LAUNCHED(h, "k_plastic_in");
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
 }
 
@@ -1586,10 +1762,18 @@ int fast_g2p(mpm_handle* h, double dt, double)
     if(!f.n) return MPM_OK;
     FastArgs a = make_args(h, dt);
     int slot = timer_begin(h, "fast_g2p");
-    switch(f.g2p_threads) {
-        case 64: k_g2p<64><<<occupancy_ctas(h, (const void*)k_g2p<64>, 64, f.cta_mult), 64, 0, h->stream>>>(a); break;
-        case 256: k_g2p<256><<<occupancy_ctas(h, (const void*)k_g2p<256>, 256, f.cta_mult), 256, 0, h->stream>>>(a); break;
-        default: k_g2p<128><<<occupancy_ctas(h, (const void*)k_g2p<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a); break;
+    if(a.psrc) {
+        switch(f.g2p_threads) {
+            case 64: k_g2p<64, true><<<occupancy_ctas(h, (const void*)k_g2p<64, true>, 64, f.cta_mult), 64, 0, h->stream>>>(a); break;
+            case 256: k_g2p<256, true><<<occupancy_ctas(h, (const void*)k_g2p<256, true>, 256, f.cta_mult), 256, 0, h->stream>>>(a); break;
+            default: k_g2p<128, true><<<occupancy_ctas(h, (const void*)k_g2p<128, true>, 128, f.cta_mult), 128, 0, h->stream>>>(a); break;
+        }
+    } else {
+        switch(f.g2p_threads) {
+            case 64: k_g2p<64, false><<<occupancy_ctas(h, (const void*)k_g2p<64, false>, 64, f.cta_mult), 64, 0, h->stream>>>(a); break;
+            case 256: k_g2p<256, false><<<occupancy_ctas(h, (const void*)k_g2p<256, false>, 256, f.cta_mult), 256, 0, h->stream>>>(a); break;
+            default: k_g2p<128, false><<<occupancy_ctas(h, (const void*)k_g2p<128, false>, 128, f.cta_mult), 128, 0, h->stream>>>(a); break;
+        }
     }
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_g2p");
@@ -1690,6 +1874,12 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* repor
     MPM_CUDA(h, cudaMemcpyAsync(save_attr, f.attr[cur0], np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream));
     MPM_CUDA(h, cudaMemcpyAsync(save_pid, f.pid[cur0], np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
     MPM_CUDA(h, cudaMemcpyAsync(save_keys, f.keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    float* save_plas = nullptr;
+    const bool plastic = h->plastic.kind && f.plas[0];
+    if(plastic) {
+        MPM_CUDA(h, cudaMalloc(&save_plas, NPLAS * np * sizeof(float)));
+        MPM_CUDA(h, cudaMemcpyAsync(save_plas, f.plas[cur0], NPLAS * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    }
     cudaEvent_t e0[64], e1[64];
     for(int k = 0; k < substeps; k++) { cudaEventCreate(&e0[k]); cudaEventCreate(&e1[k]); }
     std::string rep;
@@ -1710,6 +1900,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* repor
                 cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
+                if(plastic) cudaMemcpyAsync(f.plas[cur0], save_plas, NPLAS * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
                 f.hist_ready = false;
                 if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_g2p(h, dt, 0))) break;
                 for(int s = 0; s < substeps && !rc; s++) {
@@ -1742,9 +1933,10 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* repor
     cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
+    if(plastic) cudaMemcpyAsync(f.plas[cur0], save_plas, NPLAS * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
     f.hist_ready = false;
     cudaStreamSynchronize(h->stream);
-    cudaFree(save_soa); cudaFree(save_attr); cudaFree(save_pid); cudaFree(save_keys);
+    cudaFree(save_soa); cudaFree(save_attr); cudaFree(save_pid); cudaFree(save_keys); cudaFree(save_plas);
     for(int k = 0; k < substeps; k++) { cudaEventDestroy(e0[k]); cudaEventDestroy(e1[k]); }
     cudaFree(scrub);
     char tail[128];

@@ -27,6 +27,7 @@ struct PlainState {
     void *mass = nullptr, *vol = nullptr, *mu = nullptr, *lam = nullptr, *pft = nullptr;
     uint8_t* valid = nullptr;
     void *gm = nullptr, *gmv = nullptr, *gv0 = nullptr, *gf = nullptr, *gv = nullptr, *gvf = nullptr;
+    void *Fp = nullptr, *mu0 = nullptr, *lam0 = nullptr;   // plastic state (plasticity on)
 };
 
 // One scene of a batch, as the fast-path kernels see it.
@@ -64,6 +65,7 @@ struct FastState {
     float* soa[2] = {nullptr, nullptr};       // 24 * npad floats: x y z, vx vy vz, F0..8, B0..8
     float4* attr[2] = {nullptr, nullptr};     // mass, volume, mu, lambda
     int* pid[2] = {nullptr, nullptr};         // caller's particle index
+    float* plas[2] = {nullptr, nullptr};      // plasticity on: 11 * npad floats: Fp0..8, mu0, lambda0
     uint32_t* keys = nullptr;                 // keys of the current buffer's slots
     uint32_t* sorted_keys = nullptr;
     uint32_t* perm = nullptr;                 // sorted position -> slot in the current buffer
@@ -128,6 +130,7 @@ struct mpm_handle {
     unsigned* d_flags = nullptr;
     PlainState plain;
     FastState fast;
+    mpm_plasticity_desc plastic{};   // kind MPM_PLASTICITY_NONE: off
     // timing
     bool timing = false;
     std::vector<KernelTimer> timers;
@@ -174,6 +177,12 @@ int fast_prepare_sort(mpm_handle* h);
 int fast_particle_totals(mpm_handle* h, mpm_totals* out);
 int fast_grid_totals(mpm_handle* h, mpm_totals* out);
 int plain_particle_totals(mpm_handle* h, mpm_totals* out);
+int plain_plastic_init(mpm_handle* h);
+int fast_plastic_init(mpm_handle* h);
+int fast_get_plastic(mpm_handle* h, mpm_plastic_view* v);
+int fast_set_plastic(mpm_handle* h, const mpm_plastic_view* v);
+int plain_get_plastic(mpm_handle* h, mpm_plastic_view* v);
+int plain_set_plastic(mpm_handle* h, const mpm_plastic_view* v);
 int plain_grid_totals(mpm_handle* h, mpm_totals* out);
 
 // adjoint (mpm_adjoint.cu)

@@ -530,4 +530,81 @@ template<class T, int d, class O> __device__ void collide_node(const O* objs, in
     }
 }
 
+// ---------------------------------------------------------------------------
+// Snow plasticity for one particle after G2P: MPM_PLASTICITY_MODEL::
+// Update_Particles (Hybrid_Methods/Forces/MPM_PLASTICITY_MODEL.cpp:35-49) with
+// MPM_PLASTICITY_CLAMP::Compute (MPM_PLASTICITY_CLAMP.cpp:28-45).  The
+// singular values of F are clamped to [1 - theta_c, 1 + theta_s]; when any
+// moved, mu and lambda harden to mu0, lambda0 times
+// exp(min(max_hardening, hardening_factor (1 - det Fp_new))) (at least 1e-8),
+// F becomes U strain V^T and Fp becomes V strain^-1 U^T F_old Fp.  F and Fp
+// are column-major.  prm = theta_c, theta_s, max_hardening, hardening_factor.
+// Returns whether the particle changed; `ok` is false if the SVD did not
+// converge (the particle is left as it is).
+template<class T, int d> __device__ bool plastic_clamp(T* F, T* Fp, T& mu, T& la, T mu0, T la0, const T* prm, bool& ok)
+{
+    T U[9], S[3], V[9];
+    ok = true;
+    if(d == 3) ok = svd3<T>(F, U, S, V);
+    else svd2<T>(F, U, S, V);
+    if(!ok) return false;
+    const T lo = (T)1 - prm[0], hi = (T)1 + prm[1];
+    T st[3];
+    bool same = true;
+#pragma unroll
+    for(int a = 0; a < d; a++) {
+        st[a] = S[a] < lo ? lo : (S[a] > hi ? hi : S[a]);
+        if(st[a] != S[a]) same = false;
+    }
+    if(same) return false;
+    T pf = 1, ps = 1;
+#pragma unroll
+    for(int a = 0; a < d; a++) { pf *= S[a]; ps *= st[a]; }
+    const T* P = Fp;
+    const T detp = d == 2 ? P[0] * P[3] - P[2] * P[1]
+                          : P[0] * (P[4] * P[8] - P[7] * P[5]) - P[3] * (P[1] * P[8] - P[7] * P[2]) + P[6] * (P[1] * P[5] - P[4] * P[2]);
+    const T e = prm[3] * ((T)1 - pf / ps * detp);
+    T coeff = exp(e < prm[2] ? e : prm[2]);
+    if(coeff < (T)1e-8) coeff = (T)1e-8;
+    mu = mu0 * coeff;
+    la = la0 * coeff;
+    T Fe[9], T1[9], T2[9];
+#pragma unroll
+    for(int k = 0; k < d * d; k++) Fe[k] = F[k];
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T f = 0, t = 0;
+#pragma unroll
+            for(int k = 0; k < d; k++) {
+                f += U[r + d * k] * st[k] * V[c + d * k];
+                t += V[r + d * k] / st[k] * U[c + d * k];
+            }
+            F[r + d * c] = f;
+            T1[r + d * c] = t;
+        }
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T s2 = 0;
+#pragma unroll
+            for(int k = 0; k < d; k++) s2 += T1[r + d * k] * Fe[k + d * c];
+            T2[r + d * c] = s2;
+        }
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T s2 = 0;
+#pragma unroll
+            for(int k = 0; k < d; k++) s2 += T2[r + d * k] * P[k + d * c];
+            T1[r + d * c] = s2;
+        }
+#pragma unroll
+    for(int k = 0; k < d * d; k++) Fp[k] = T1[k];
+    return true;
+}
+
 }  // namespace mpm

@@ -16,6 +16,8 @@ namespace {
 
 using namespace mpm;
 
+template<class T> struct Vec4 { T v[4]; };
+
 template<class T> struct PlainArgs {
     SceneParams sp;
     int64_t n, gn;
@@ -27,6 +29,7 @@ template<class T> struct PlainArgs {
     T *gm, *gmv, *gv0, *gf, *gv, *gvf;
     T dt;
     unsigned* flags;
+    int mark_left;
 };
 
 template<class T, int d> struct Stencil {
@@ -273,7 +276,9 @@ template<class T, int d> __global__ void k_g2p(PlainArgs<T> a)
         else if(xn[k] > (T)a.sp.dmax[k] - eps) keep = false;
     }
     if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); keep = false; }
-    if(!keep) a.valid[p] = 0;
+    // a particle that leaves is marked 2 while plasticity still has to see it
+    // (the reference updates every particle simulated in this substep)
+    if(!keep) a.valid[p] = a.mark_left ? 2 : 0;
 }
 
 template<class T> __global__ void k_count_valid(const uint8_t* valid, int64_t n, unsigned long long* out)
@@ -297,6 +302,7 @@ template<class T> PlainArgs<T> args(mpm_handle* h, double dt)
     a.gm = (T*)s.gm; a.gmv = (T*)s.gmv; a.gv0 = (T*)s.gv0; a.gf = (T*)s.gf; a.gv = (T*)s.gv; a.gvf = (T*)s.gvf;
     a.dt = (T)dt;
     a.flags = h->d_flags;
+    a.mark_left = h->plastic.kind != MPM_PLASTICITY_NONE;
     return a;
 }
 
@@ -356,6 +362,41 @@ template<class T> int forces_t(mpm_handle* h, double dt)
     return MPM_OK;
 }
 
+// MPM_DRIVER::Update_Plasticity_And_Hardening (MPM_DRIVER.cpp:922-928) with
+// MPM_PLASTICITY_CLAMP, over the valid particles after G2P.
+template<class T, int d> __global__ void k_plastic_clamp(PlainArgs<T> a, T* Fp, const T* mu0, const T* lam0, Vec4<T> prm)
+{
+    T* mu = const_cast<T*>(a.mu);
+    T* lam = const_cast<T*>(a.lam);
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+        if(!a.valid[p]) continue;
+        if(a.valid[p] == 2) a.valid[p] = 0;   // left the domain in this G2P: updated once more
+        T F[d * d], P[d * d];
+#pragma unroll
+        for(int k = 0; k < d * d; k++) { F[k] = a.F[p * d * d + k]; P[k] = Fp[p * d * d + k]; }
+        T m = mu[p], l = lam[p];
+        bool ok;
+        if(plastic_clamp<T, d>(F, P, m, l, mu0[p], lam0[p], prm.v, ok)) {
+#pragma unroll
+            for(int k = 0; k < d * d; k++) { a.F[p * d * d + k] = F[k]; Fp[p * d * d + k] = P[k]; }
+            mu[p] = m;
+            lam[p] = l;
+        }
+        if(!ok) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
+    }
+}
+
+// Unplastic start: Fp = I, mu0 = mu, lambda0 = lambda.
+template<class T, int d> __global__ void k_plastic_init(int64_t n, T* Fp, T* mu0, T* lam0, const T* mu, const T* lam)
+{
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for(int k = 0; k < d * d; k++) Fp[p * d * d + k] = k % (d + 1) == 0 ? (T)1 : (T)0;
+        mu0[p] = mu[p];
+        lam0[p] = lam[p];
+    }
+}
+
 template<class T> int g2p_t(mpm_handle* h, double dt)
 {
     PlainArgs<T> a = args<T>(h, dt);
@@ -366,6 +407,15 @@ template<class T> int g2p_t(mpm_handle* h, double dt)
     else k_g2p<T, 2><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_g2p");
+    if(h->plastic.kind == MPM_PLASTICITY_CLAMP) {
+        PlainState& s = h->plain;
+        Vec4<T> prm = {{(T)h->plastic.theta_c, (T)h->plastic.theta_s, (T)h->plastic.max_hardening, (T)h->plastic.hardening_factor}};
+        slot = timer_begin(h, "plain_plasticity");
+        if(h->sp.dim == 3) k_plastic_clamp<T, 3><<<pblocks(a.n, t), t, 0, h->stream>>>(a, (T*)s.Fp, (const T*)s.mu0, (const T*)s.lam0, prm);
+        else k_plastic_clamp<T, 2><<<pblocks(a.n, t), t, 0, h->stream>>>(a, (T*)s.Fp, (const T*)s.mu0, (const T*)s.lam0, prm);
+        timer_end(h, slot);
+        MPM_LAUNCHED(h, "k_plastic_clamp");
+    }
     return MPM_OK;
 }
 
@@ -392,7 +442,7 @@ int plain_alloc(mpm_handle* h, int64_t n)
         for(void** p: g) MPM_CUDA(h, cudaMemsetAsync(*p, 0, (p == &s.gm ? gn : gn * d) * e, h->stream));
     }
     if(s.n != n) {
-        void** pa[] = {&s.X, &s.V, &s.F, &s.B, &s.mass, &s.vol, &s.mu, &s.lam, &s.pft};
+        void** pa[] = {&s.X, &s.V, &s.F, &s.B, &s.mass, &s.vol, &s.mu, &s.lam, &s.pft, &s.Fp, &s.mu0, &s.lam0};
         for(void** p: pa) { cudaFree(*p); *p = nullptr; }
         cudaFree(s.valid); s.valid = nullptr;
         int64_t m = n ? n : 1;
@@ -414,7 +464,8 @@ int plain_alloc(mpm_handle* h, int64_t n)
 void plain_free(mpm_handle* h)
 {
     PlainState& s = h->plain;
-    void* ps[] = {s.X, s.V, s.F, s.B, s.mass, s.vol, s.mu, s.lam, s.pft, s.valid, s.gm, s.gmv, s.gv0, s.gf, s.gv, s.gvf};
+    void* ps[] = {s.X, s.V, s.F, s.B, s.mass, s.vol, s.mu, s.lam, s.pft, s.valid, s.gm, s.gmv, s.gv0, s.gf, s.gv, s.gvf,
+                  s.Fp, s.mu0, s.lam0};
     for(void* p: ps) cudaFree(p);
     s = PlainState();
 }
@@ -491,6 +542,68 @@ int plain_set_particles(mpm_handle* h, const mpm_particles_view* v)
     if((rc = copy_in(h, s.lam, v->lambda, n, v->dtype, dev))) return rc;
     if(v->valid) MPM_CUDA(h, cudaMemcpyAsync(s.valid, v->valid, n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
     else MPM_CUDA(h, cudaMemsetAsync(s.valid, 1, n, h->stream));
+    if(h->plastic.kind) return plain_plastic_init(h);
+    return MPM_OK;
+}
+
+// Allocate the plastic state if needed and start it unplastic.
+int plain_plastic_init(mpm_handle* h)
+{
+    PlainState& s = h->plain;
+    const int d = h->sp.dim;
+    const size_t e = esize(h);
+    const int64_t m = s.n ? s.n : 1;
+    if(!s.Fp) {
+        MPM_CUDA(h, cudaMalloc(&s.Fp, m * d * d * e));
+        MPM_CUDA(h, cudaMalloc(&s.mu0, m * e));
+        MPM_CUDA(h, cudaMalloc(&s.lam0, m * e));
+    }
+    if(!s.n) return MPM_OK;
+    const int b = gblocks(h, s.n, 256);
+    if(e == 8) {
+        if(d == 3) k_plastic_init<double, 3><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.mu0, (double*)s.lam0, (const double*)s.mu, (const double*)s.lam);
+        else k_plastic_init<double, 2><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.mu0, (double*)s.lam0, (const double*)s.mu, (const double*)s.lam);
+    } else {
+        if(d == 3) k_plastic_init<float, 3><<<b, 256, 0, h->stream>>>(s.n, (float*)s.Fp, (float*)s.mu0, (float*)s.lam0, (const float*)s.mu, (const float*)s.lam);
+        else k_plastic_init<float, 2><<<b, 256, 0, h->stream>>>(s.n, (float*)s.Fp, (float*)s.mu0, (float*)s.lam0, (const float*)s.mu, (const float*)s.lam);
+    }
+    MPM_LAUNCHED(h, "k_plastic_init");
+    return MPM_OK;
+}
+
+int plain_get_plastic(mpm_handle* h, mpm_plastic_view* v)
+{
+    PlainState& s = h->plain;
+    const int d = h->sp.dim;
+    if(v->n != s.n) return set_error(h, MPM_ERR_ARG, "particle count differs from mpm_set_particles");
+    if(!v->n) return MPM_OK;
+    const bool dev = v->on_device != 0;
+    const int64_t n = v->n;
+    int rc;
+    if(v->Fp && (rc = copy_out(h, v->Fp, s.Fp, n * d * d, v->dtype, dev))) return rc;
+    if(v->mu && (rc = copy_out(h, v->mu, s.mu, n, v->dtype, dev))) return rc;
+    if(v->lambda && (rc = copy_out(h, v->lambda, s.lam, n, v->dtype, dev))) return rc;
+    if(v->mu0 && (rc = copy_out(h, v->mu0, s.mu0, n, v->dtype, dev))) return rc;
+    if(v->lambda0 && (rc = copy_out(h, v->lambda0, s.lam0, n, v->dtype, dev))) return rc;
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
+int plain_set_plastic(mpm_handle* h, const mpm_plastic_view* v)
+{
+    PlainState& s = h->plain;
+    const int d = h->sp.dim;
+    if(v->n != s.n) return set_error(h, MPM_ERR_ARG, "particle count differs from mpm_set_particles");
+    if(!v->n) return MPM_OK;
+    const bool dev = v->on_device != 0;
+    const int64_t n = v->n;
+    int rc;
+    if(v->Fp && (rc = copy_in(h, s.Fp, v->Fp, n * d * d, v->dtype, dev))) return rc;
+    if(v->mu && (rc = copy_in(h, s.mu, v->mu, n, v->dtype, dev))) return rc;
+    if(v->lambda && (rc = copy_in(h, s.lam, v->lambda, n, v->dtype, dev))) return rc;
+    if(v->mu0 && (rc = copy_in(h, s.mu0, v->mu0, n, v->dtype, dev))) return rc;
+    if(v->lambda0 && (rc = copy_in(h, s.lam0, v->lambda0, n, v->dtype, dev))) return rc;
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
 }
 

@@ -69,12 +69,24 @@ class ParticlesView(ctypes.Structure):
                 ("lambda_", ctypes.c_void_p), ("valid", ctypes.c_void_p)]
 
 
+class PlasticityDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("theta_c", ctypes.c_double), ("theta_s", ctypes.c_double),
+                ("max_hardening", ctypes.c_double), ("hardening_factor", ctypes.c_double)]
+
+
+class PlasticView(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("dtype", ctypes.c_int), ("on_device", ctypes.c_int),
+                ("Fp", ctypes.c_void_p), ("mu", ctypes.c_void_p), ("lambda_", ctypes.c_void_p),
+                ("mu0", ctypes.c_void_p), ("lambda0", ctypes.c_void_p)]
+
+
 EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_objects", "mpm_set_particles",
            "mpm_get_particles", "mpm_substep", "mpm_advance", "mpm_particle_to_grid", "mpm_apply_forces",
            "mpm_grid_to_particle", "mpm_synchronize", "mpm_get_grid", "mpm_count_valid", "mpm_set_timing",
            "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state",
            "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune", "mpm_particle_totals",
-           "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex"]
+           "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex",
+           "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state"]
 
 _lib = None
 
@@ -115,6 +127,9 @@ def load_library(path: str = LIB_PATH):
     L.mpm_grid_totals.argtypes = [P, ctypes.POINTER(Totals)]
     L.mpm_compute_dt.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
     L.mpm_debug_sort_state.argtypes = [P, P, P, P]
+    L.mpm_set_plasticity.argtypes = [P, ctypes.POINTER(PlasticityDesc)]
+    L.mpm_get_plastic_state.argtypes = [P, ctypes.POINTER(PlasticView)]
+    L.mpm_set_plastic_state.argtypes = [P, ctypes.POINTER(PlasticView)]
     L.mpm_status_string.argtypes = [ctypes.c_int]
     L.mpm_status_string.restype = ctypes.c_char_p
     for f in EXPORTS:
@@ -151,6 +166,8 @@ class MPM_DRIVER:
         self.h = ctypes.c_void_p()
         self._check(self.L.mpm_create(ctypes.byref(g), ctypes.byref(m), ctypes.byref(self.h)), "mpm_create")
         self.set_collision_objects(scene.objects)
+        if scene.plasticity is not None:
+            self.set_plasticity(scene.plasticity)
         self.time = 0.0
         self.n = 0
 
@@ -300,6 +317,41 @@ class MPM_DRIVER:
         v = self._dev_view(X, V, Fc, Bc, valid=valid)
         self._check(self.L.mpm_get_particles(self.h, ctypes.byref(v)), "mpm_get_particles")
         return X, V, Fc, Bc, valid
+
+    # -- plasticity (MPM_PLASTICITY_CLAMP) -------------------------------------
+    def set_plasticity(self, plasticity: Optional[S.Plasticity]):
+        """Snow clamp after every G2P (None: off).  Particles start unplastic."""
+        d = PlasticityDesc()
+        if plasticity is not None:
+            d.kind, d.theta_c, d.theta_s = plasticity.kind, plasticity.theta_c, plasticity.theta_s
+            d.max_hardening, d.hardening_factor = plasticity.max_hardening, plasticity.hardening_factor
+        self._check(self.L.mpm_set_plasticity(self.h, ctypes.byref(d)), "mpm_set_plasticity")
+
+    def get_plastic_state(self, dtype=np.float64):
+        """{"Fp": (n,d,d), "mu", "lam", "mu0", "lam0": (n,)} in the caller's particle order."""
+        d, n = self.dim, self.n
+        Fp = np.empty((n, d * d), dtype)
+        arrs = [np.empty(n, dtype) for _ in range(4)]
+        v = PlasticView()
+        v.n, v.dtype, v.on_device = n, FP64 if dtype == np.float64 else FP32, 0
+        v.Fp = Fp.ctypes.data
+        v.mu, v.lambda_, v.mu0, v.lambda0 = [a.ctypes.data for a in arrs]
+        self._check(self.L.mpm_get_plastic_state(self.h, ctypes.byref(v)), "mpm_get_plastic_state")
+        return {"Fp": np.swapaxes(Fp.reshape(n, d, d), 1, 2), "mu": arrs[0], "lam": arrs[1], "mu0": arrs[2],
+                "lam0": arrs[3]}
+
+    def set_plastic_state(self, Fp=None, mu=None, lam=None, mu0=None, lam0=None, dtype=np.float64):
+        """Overwrite any subset of the plastic state (Fp as (n,d,d) matrices)."""
+        d, n = self.dim, self.n
+        keep = [None if Fp is None else np.ascontiguousarray(np.swapaxes(np.asarray(Fp), 1, 2).reshape(n, d * d), dtype)]
+        keep += [None if a is None else np.ascontiguousarray(a, dtype) for a in (mu, lam, mu0, lam0)]
+        for k in keep:
+            if k is not None and k.shape[0] != n:
+                raise ValueError("set_plastic_state: arrays of n = %d particles" % n)
+        v = PlasticView()
+        v.n, v.dtype, v.on_device = n, FP64 if dtype == np.float64 else FP32, 0
+        v.Fp, v.mu, v.lambda_, v.mu0, v.lambda0 = [None if k is None else k.ctypes.data for k in keep]
+        self._check(self.L.mpm_set_plastic_state(self.h, ctypes.byref(v)), "mpm_set_plastic_state")
 
     # -- differentiation -------------------------------------------------------
     def diff_forward(self, nsteps, checkpoint_every=8, dt=None):
@@ -478,6 +530,12 @@ class MPM_BATCH(MPM_DRIVER):
                 arr[i].a[a], arr[i].b[a] = o.a[a], o.b[a]
         self.h = ctypes.c_void_p()
         self._check(L.mpm_batch_create(descs, len(self.scenes), arr, len(objs), ctypes.byref(self.h)), "mpm_batch_create")
+        # one plasticity per handle: the scenes of a batch share it
+        pl = self.scenes[0].plasticity
+        if any(s.plasticity != pl for s in self.scenes):
+            raise ValueError("the scenes of a batch share one plasticity (or none)")
+        if pl is not None:
+            self.set_plasticity(pl)
         self.time = 0.0
         self.n = 0
         self.offsets = np.cumsum([0] + [s.n for s in self.scenes])
