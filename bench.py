@@ -36,6 +36,8 @@ METRIC = "particle-substeps/s"
 WORKLOAD = "spheres3d-128^3-neohookean-8ppc-fp32"
 LARGE_WORKLOAD = "dam3d-256^3-corotated-8ppc-fp32"
 ALG_BYTES = {"p2g": 112, "g2p": 144, "substep": 256}    # bytes per particle (FP32, 3D)
+PLASTIC_BYTES = 88                                      # snow: Fp, mu0, lambda0 read and written by G2P
+SNOW_LEAD_SUBSTEPS = 600                                # snow leg: substeps run before timing
 GRID_BYTES_PER_NODE = 48                                # grid update: read 16, write 32
 
 
@@ -305,9 +307,11 @@ def our_arm(args):
     roof = roofline_of(ktimes, n, peak, peak_kind, WORKLOAD)
     total_k = sum(v[0] for v in ktimes.values())
 
-    large = batch = adjoint = plain = None
+    large = batch = adjoint = plain = snow = None
     if world == 1 and not args.no_plain:
         plain = measure_plain_fp64(args, D, S, stream, flush, substep_ms)
+    if world == 1 and not args.no_snow:
+        snow = measure_snow(args, D, S, stream, flush, peak, substep_ms)
     if world == 1 and not args.no_large:
         large = measure_large(args, D, S, stream, flush, peak, peak_kind)
     if not args.no_batch:
@@ -337,6 +341,7 @@ def our_arm(args):
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()},
             "kernel_share": {k: v[0] / total_k for k, v in ktimes.items()},
             "plain_fp64": plain,
+            "snow": snow,
             "large_config": large,
             "batch_config": batch,
             "adjoint": adjoint,
@@ -398,6 +403,40 @@ def measure_plain_fp64(args, D, S, stream, flush, fast_ms):
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
 
 
+def measure_snow(args, D, S, stream, flush, peak, elastic_ms):
+    """Two snowballs with the same geometry as the headline case (128^3, 8 ppc,
+    COROTATED_FIXED, Stomakhin et al. 2013 parameters) and MPM_PLASTICITY_CLAMP
+    after every G2P, fused into the fast path's G2P: the cost of plasticity."""
+    scene = S.snowballs_3d()
+    n = scene.n
+    drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+    drv.set_stream(stream.cuda_stream)
+    drv.set_scene_particles(scene)
+    # timed mid-collision: the balls touch after ~300 substeps, and from then on
+    # the clamp acts and hardens (before, the SVD is skipped for every particle)
+    drv.advance(SNOW_LEAD_SUBSTEPS)
+    tuned = drv.autotune(substeps=3, cold_l2=True)
+    steps = max(5, min(args.steps, 20))
+    ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
+    plastic = drv.get_plastic_state(np.float32)
+    drv.close()
+    sub = ms / steps
+    g2p = ktimes.get("fast_g2p")
+    g2p_ms = g2p[0] / max(g2p[1], 1) if g2p else None
+    g2p_bytes = (ALG_BYTES["g2p"] + PLASTIC_BYTES) * n
+    return {"workload": "snowballs3d-128^3-corotated-8ppc-clamp-fp32", "particles": n, "steps": steps,
+            "timed_after_substeps": SNOW_LEAD_SUBSTEPS,
+            "ms_per_step": sub, "value": n * steps / (ms / 1e3), "unit": METRIC,
+            "over_elastic_headline": sub / elastic_ms,
+            "plastic_fraction": float(np.mean(np.abs(plastic["mu"] / plastic["mu0"] - 1.0) > 1e-4)),
+            "g2p_roofline": None if g2p_ms is None else {
+                "achieved": g2p_bytes / (g2p_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": g2p_bytes / (g2p_ms / 1e3) / 1e9 / peak,
+                "alg_bytes_per_particle": ALG_BYTES["g2p"] + PLASTIC_BYTES},
+            "autotune": tuned,
+            "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
+
+
 def measure_adjoint(D, S):
     """64^3 cube, 64 substeps, checkpoint every 8; FP32 forward and
     backward through the C ABI (device arrays), timed with CUDA events."""
@@ -434,12 +473,15 @@ def profile_case(args, D, S):
     """Small single-scene run for profilers: `--scene NAME --grid G` (no e2e, no CPU, no flush).
     Prints one JSON line with the per-kernel times; used to make the ncu summaries."""
     import torch
-    make = {"spheres3d": S.spheres_3d, "dam3d": S.dam_3d, "cube3d": S.cube_3d}[args.scene]
+    make = {"spheres3d": S.spheres_3d, "dam3d": S.dam_3d, "cube3d": S.cube_3d,
+            "snowballs3d": S.snowballs_3d}[args.scene]
     scene = make(G=args.grid) if args.grid else make()
     drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
     if args.shape:
         drv.set_launch_shape(*[int(x) for x in args.shape.split(",")])
     drv.set_scene_particles(scene, dtype=np.float32)
+    if scene.plasticity is not None:
+        drv.advance(SNOW_LEAD_SUBSTEPS)   # into the collision, where the clamp acts
     drv.advance(args.warmup)
     drv.synchronize()
     drv.set_timing(True)
@@ -488,7 +530,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-scene batched measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward/backward timing")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 path on the same workload")
-    ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d"], help="profiling run of one scene only")
+    ap.add_argument("--no-snow", action="store_true", help="skip the snow (plasticity) measurement")
+    ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d", "snowballs3d"],
+                    help="profiling run of one scene only")
     ap.add_argument("--grid", type=int, default=0, help="grid cells per side for --scene")
     ap.add_argument("--shape", default="", help="launch shape for --scene: P2G variant,G2P threads,CTA multiplier")
     args = ap.parse_args()

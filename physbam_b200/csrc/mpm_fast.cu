@@ -945,15 +945,168 @@ struct G2PState {
 };
 
 // MPM_DRIVER::Update_Plasticity_And_Hardening (MPM_DRIVER.cpp:922-928) with
-// MPM_PLASTICITY_CLAMP for one particle after its G2P: F, Fp and the Lame
-// parameters (at.z, at.w) in place.  Out of line: the SVD's registers stay
-// off the G2P loop.
-__device__ __noinline__ void plastic_fast(float* F, float* Fp, float4& at, float mu0, float la0, const float* prm, unsigned* flags)
+// MPM_PLASTICITY_CLAMP through the SVD, for the particle already written to
+// slot j (F, Fp and the Lame parameters rewritten in place).  Out of line and
+// fed from memory, so that neither its registers nor a stack copy of its
+// operands weigh on the G2P loop; G2P calls it only where the SVD-free form
+// below does not apply (det F <= 0 or sigma_max / sigma_min > 10).
+__device__ __noinline__ void plastic_svd_slot(float* dst, float* pdst, float4* dst_attr, int64_t npad, uint32_t j,
+    float tc, float ts, float mh, float hf, unsigned* flags)
 {
+    float F[9], Fp[9];
+    for(int k = 0; k < 9; k++) { F[k] = dst[(C_F + k) * npad + j]; Fp[k] = pdst[k * npad + j]; }
+    float4 at = dst_attr[j];
+    const float prm[4] = {tc, ts, mh, hf};
     bool ok;
     float mu = at.z, la = at.w;
-    if(plastic_clamp<float, 3>(F, Fp, mu, la, mu0, la0, prm, ok)) { at.z = mu; at.w = la; }
+    if(plastic_clamp<float, 3>(F, Fp, mu, la, pdst[9 * npad + j], pdst[10 * npad + j], prm, ok)) {
+        for(int k = 0; k < 9; k++) { dst[(C_F + k) * npad + j] = F[k]; pdst[k * npad + j] = Fp[k]; }
+        at.z = mu;
+        at.w = la;
+        dst_attr[j] = at;
+    }
     if(!ok) atomicOr(flags, MPM_FLAG_NOT_CONVERGED);
+}
+
+// True when every singular value of F lies strictly inside the clamp band
+// [1 - theta_c, 1 + theta_s] with a relative margin of 1e-5 and det F > 0:
+// the clamp then leaves F, Fp, mu and lambda unchanged, so the SVD is skipped.
+// Test: C - a I and b I - C positive definite (LDL^T pivots > 0) for
+// C = F^T F, a = (1 - theta_c)^2 (1 + 1e-5), b = (1 + theta_s)^2 (1 - 1e-5).
+// FP32 rounding in C and in the pivots is ~1e-7, well inside the margin.
+__device__ __forceinline__ bool pd3(float m00, float m01, float m02, float m11, float m12, float m22)
+{
+    if(!(m00 > 0.f)) return false;
+    const float i0 = __fdividef(1.f, m00);
+    const float d1 = m11 - m01 * m01 * i0;
+    if(!(d1 > 0.f)) return false;
+    const float e12 = m12 - m01 * m02 * i0;
+    return m22 - m02 * m02 * i0 - __fdividef(e12 * e12, d1) > 0.f;
+}
+
+__device__ __forceinline__ bool clamp_inactive(const float* F, const float* prm)
+{
+    const float J = F[0] * (F[4] * F[8] - F[7] * F[5]) - F[3] * (F[1] * F[8] - F[7] * F[2]) + F[6] * (F[1] * F[5] - F[4] * F[2]);
+    if(!(J > 0.f)) return false;
+    float c[6];   // C = F^T F: 00 01 02 11 12 22
+    const int I[6] = {0, 0, 0, 1, 1, 2}, K[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for(int e = 0; e < 6; e++)
+        c[e] = F[3 * I[e]] * F[3 * K[e]] + F[3 * I[e] + 1] * F[3 * K[e] + 1] + F[3 * I[e] + 2] * F[3 * K[e] + 2];
+    const float lo = 1.f - prm[0], hi = 1.f + prm[1];
+    const float a = lo * lo * (1.f + 1e-5f), b = hi * hi * (1.f - 1e-5f);
+    return pd3(c[0] - a, c[1], c[2], c[3] - a, c[4], c[5] - a) && pd3(b - c[0], -c[1], -c[2], b - c[3], -c[4], b - c[5]);
+}
+
+// The clamp without an SVD, for det F > 0 and sigma_min / sigma_max > 0.1.
+// With F = U S V^T (det U = det V = 1) and S' the clamped singular values,
+// the reference's updates only need V and S (U^T F = S V^T):
+//   F  <- U S' V^T       = F  (V diag(S'/S) V^T)
+//   Fp <- V S'^-1 U^T F Fp = (V diag(S/S') V^T) Fp
+// V diag(S) V^T is the eigendecomposition of C = F^T F, found by cyclic
+// Jacobi rotations (Golub & Van Loan, Matrix Computations, 4th ed., 8.5.2:
+// the symmetric Schur rotation, cyclic sweeps of the 3 pivots), in registers.
+// Both matrix functions depend only on C, so they are stable for repeated
+// singular values.  Returns 0 (unchanged), 1 (clamped) or -1 (outside the
+// conditions above: the caller takes the SVD route).
+template<int P, int Q>
+__device__ __forceinline__ void jacobi_rotate(float (&A)[3][3], float (&V)[3][3])
+{
+    constexpr int R = 3 - P - Q;
+    const float apq = A[P][Q];
+    const float d = A[Q][Q] - A[P][P];
+    // t = tan of the rotation angle: an approximate t still gives an exact
+    // rotation (c and s come from t) and only leaves a residual that the next
+    // sweep removes; c to full precision keeps V orthogonal
+    const float h = d * d + 4.f * apq * apq;
+    const float den = fabsf(d) + h * rsqrtf(h);
+    float t = h > 0.f ? __fdividef(2.f * apq, den) : 0.f;
+    if(d < 0.f) t = -t;
+    const float x = 1.f + t * t;
+    float c = rsqrtf(x);
+    c = c * (1.5f - 0.5f * x * c * c);   // one Newton step
+    const float s = t * c;
+    A[P][P] -= t * apq;
+    A[Q][Q] += t * apq;
+    A[P][Q] = A[Q][P] = 0.f;
+    const float arp = A[R][P], arq = A[R][Q];
+    A[R][P] = A[P][R] = c * arp - s * arq;
+    A[R][Q] = A[Q][R] = s * arp + c * arq;
+#pragma unroll
+    for(int k = 0; k < 3; k++) {
+        const float vp = V[k][P], vq = V[k][Q];
+        V[k][P] = c * vp - s * vq;
+        V[k][Q] = s * vp + c * vq;
+    }
+}
+
+__device__ __forceinline__ int plastic_eig(float* F, float* Fp, float4& at, float mu0, float la0, const float* prm)
+{
+    const float J = F[0] * (F[4] * F[8] - F[7] * F[5]) - F[3] * (F[1] * F[8] - F[7] * F[2]) + F[6] * (F[1] * F[5] - F[4] * F[2]);
+    if(!(J > 0.f)) return -1;
+    float A[3][3], V[3][3];
+#pragma unroll
+    for(int i = 0; i < 3; i++)
+#pragma unroll
+        for(int k = 0; k < 3; k++) {
+            A[i][k] = F[3 * i] * F[3 * k] + F[3 * i + 1] * F[3 * k + 1] + F[3 * i + 2] * F[3 * k + 2];
+            V[i][k] = i == k ? 1.f : 0.f;
+        }
+    // three sweeps reach FP32 accuracy for sigma_max / sigma_min <= 10; a
+    // fourth runs where the off-diagonal part is not yet at rounding level
+#pragma unroll
+    for(int sweep = 0; sweep < 3; sweep++) {
+        jacobi_rotate<0, 1>(A, V);
+        jacobi_rotate<0, 2>(A, V);
+        jacobi_rotate<1, 2>(A, V);
+    }
+    const float off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+    const float dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+    if(off > 1e-14f * dia) {
+        jacobi_rotate<0, 1>(A, V);
+        jacobi_rotate<0, 2>(A, V);
+        jacobi_rotate<1, 2>(A, V);
+    }
+    const float lmax = fmaxf(A[0][0], fmaxf(A[1][1], A[2][2])), lmin = fminf(A[0][0], fminf(A[1][1], A[2][2]));
+    if(!(lmin > 1e-2f * lmax)) return -1;
+    const float lo = 1.f - prm[0], hi = 1.f + prm[1];
+    float S[3], St[3];
+    bool same = true;
+#pragma unroll
+    for(int i = 0; i < 3; i++) {
+        S[i] = sqrtf(A[i][i]);
+        St[i] = fminf(fmaxf(S[i], lo), hi);
+        same = same && St[i] == S[i];
+    }
+    if(same) return 0;
+    const float* P = Fp;
+    const float detp = P[0] * (P[4] * P[8] - P[7] * P[5]) - P[3] * (P[1] * P[8] - P[7] * P[2]) + P[6] * (P[1] * P[5] - P[4] * P[2]);
+    const float e = prm[3] * (1.f - S[0] * S[1] * S[2] / (St[0] * St[1] * St[2]) * detp);
+    const float coeff = fmaxf(expf(fminf(e, prm[2])), 1e-8f);
+    at.z = mu0 * coeff;
+    at.w = la0 * coeff;
+    float g[3], h[3];
+#pragma unroll
+    for(int i = 0; i < 3; i++) { g[i] = __fdividef(St[i], S[i]); h[i] = __fdividef(S[i], St[i]); }
+    float M[3][3], N[3][3];
+#pragma unroll
+    for(int j = 0; j < 3; j++)
+#pragma unroll
+        for(int k = 0; k < 3; k++) {
+            M[j][k] = V[j][0] * g[0] * V[k][0] + V[j][1] * g[1] * V[k][1] + V[j][2] * g[2] * V[k][2];
+            N[j][k] = V[j][0] * h[0] * V[k][0] + V[j][1] * h[1] * V[k][1] + V[j][2] * h[2] * V[k][2];
+        }
+    float Fo[9], Po[9];
+#pragma unroll
+    for(int k = 0; k < 9; k++) { Fo[k] = F[k]; Po[k] = Fp[k]; }
+#pragma unroll
+    for(int r = 0; r < 3; r++)
+#pragma unroll
+        for(int c = 0; c < 3; c++) {
+            F[r + 3 * c] = Fo[r] * M[0][c] + Fo[r + 3] * M[1][c] + Fo[r + 6] * M[2][c];
+            Fp[r + 3 * c] = N[r][0] * Po[3 * c] + N[r][1] * Po[3 * c + 1] + N[r][2] * Po[3 * c + 2];
+        }
+    return 1;
 }
 
 template<bool PLASTIC>
@@ -1053,13 +1206,14 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
     for(int k = 0; k < 9; k++) finite = finite && isfinite(Fn[k]);
     finite = finite && isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]);
     if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); ok = false; }
+    bool svd = false;
     if(PLASTIC) {
         // every particle of this substep, including one that just left
         float Fp[9];
 #pragma unroll
         for(int k = 0; k < 9; k++) Fp[k] = a.psrc[k * a.npad + i];
         const float mu0 = a.psrc[9 * a.npad + i], la0 = a.psrc[10 * a.npad + i];
-        if(finite) plastic_fast(Fn, Fp, at, mu0, la0, a.prm, a.flags);
+        svd = finite && !clamp_inactive(Fn, a.prm) && plastic_eig(Fn, Fp, at, mu0, la0, a.prm) < 0;
 #pragma unroll
         for(int k = 0; k < 9; k++) a.pdst[k * a.npad + j] = Fp[k];
         a.pdst[9 * a.npad + j] = mu0;
@@ -1073,6 +1227,8 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
     a.dst_attr[j] = at;
     a.dst_pid[j] = pid;
     a.keys_next[j] = key;
+    if(PLASTIC && svd)
+        plastic_svd_slot(a.dst, a.pdst, a.dst_attr, a.npad, j, a.prm[0], a.prm[1], a.prm[2], a.prm[3], a.flags);
 #pragma unroll
     for(int k = 0; k < 9; k++) out.Bn[k] = Bn[k];
     out.at = at;
