@@ -78,6 +78,9 @@ def lib():
         _lib.oracle_svd3.restype = ctypes.c_int
         _lib.oracle_plastic_clamp.argtypes = [ctypes.c_int, ctypes.c_longlong, P, P, P, P, P, P,
                                               ctypes.POINTER(ctypes.c_ubyte), P]
+        _lib.oracle_dp_init.argtypes = [ctypes.c_longlong, P, P, P, P, ctypes.c_double, P]
+        _lib.oracle_plastic_dp.argtypes = [ctypes.c_int, ctypes.c_longlong, P, P, P, P, P, P, P, P,
+                                           ctypes.POINTER(ctypes.c_ubyte), P]
     return _lib
 
 
@@ -120,10 +123,28 @@ class State:
         self.lam = np.ascontiguousarray(scene.lam, np.float64)
         self.valid = np.ones(scene.n, np.uint8)
         self.time = 0.0
-        if scene.plasticity is not None:   # as the reference seeds them (STANDARD_TESTS_BASE.cpp:299,568-586)
+        pl = scene.plasticity
+        if pl is not None:   # as the reference seeds them (STANDARD_TESTS_BASE.cpp:299,568-586)
             self.Fp = np.ascontiguousarray(np.tile(np.eye(d).reshape(1, d * d), (scene.n, 1)), np.float64)
             self.mu0, self.lam0 = self.mu.copy(), self.lam.copy()
             self.mu, self.lam = self.mu.copy(), self.lam.copy()
+        if pl is not None and pl.kind == 2:   # MPM_DRUCKER_PRAGER::Initialize_Particles
+            n = scene.n
+            self.pdef, self.rho_F, self.cohesion, self.vc = (np.zeros(n) for _ in range(4))
+            lib().oracle_dp_init(n, _ptr(self.pdef), _ptr(self.rho_F), _ptr(self.cohesion), _ptr(self.vc),
+                                 pl.cohesion, _ptr(self._dp_prm()))
+
+    def _dp_prm(self):
+        pl = self.scene.plasticity
+        return np.array([pl.a0, pl.a1, pl.a3, pl.a4, 1.0 if pl.use_vc else 0.0], np.float64)
+
+    def plastic_state(self):
+        """The plastic state with the keys of `scenes.plastic_keys` (Fp as (n,d,d) matrices)."""
+        from physbam_b200 import scenes as S
+        out = {}
+        for k in S.plastic_keys(self.scene.plasticity):
+            out[k] = self.Fp_rowmajor() if k == "Fp" else getattr(self, k)
+        return out
 
     def Fp_rowmajor(self):
         d = self.scene.dim
@@ -135,8 +156,14 @@ class State:
         pl = self.scene.plasticity
         if pl is None:
             return
-        prm = np.array([pl.theta_c, pl.theta_s, pl.max_hardening, pl.hardening_factor], np.float64)
         sim = np.ascontiguousarray(simulated, np.uint8)
+        if pl.kind == 2:
+            lib().oracle_plastic_dp(self.scene.dim, self.scene.n, _ptr(self.F), _ptr(self.Fp), _ptr(self.mu),
+                                    _ptr(self.lam), _ptr(self.pdef), _ptr(self.rho_F), _ptr(self.cohesion),
+                                    _ptr(self.vc), sim.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                                    _ptr(self._dp_prm()))
+            return
+        prm = np.array([pl.theta_c, pl.theta_s, pl.max_hardening, pl.hardening_factor], np.float64)
         lib().oracle_plastic_clamp(self.scene.dim, self.scene.n, _ptr(self.F), _ptr(self.Fp), _ptr(self.mu),
                                    _ptr(self.lam), _ptr(self.mu0), _ptr(self.lam0),
                                    sim.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), _ptr(prm))
@@ -220,7 +247,7 @@ def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timin
         if totals is not None:
             cmd += ["-totals", repr(float(totals[0])), repr(float(totals[1]))]
         out = subprocess.run(cmd, check=True, capture_output=True, text=True)
-        res = S.read_dump(dp, scene.dim, scene.n, scene.counts, plastic=scene.plasticity is not None) if dumps else {}
+        res = S.read_dump(dp, scene.dim, scene.n, scene.counts, plastic=S.plastic_keys(scene.plasticity)) if dumps else {}
         if totals is not None:
             import json
             lines = [ln for ln in out.stdout.splitlines() if ln.startswith('{"mass"')]

@@ -39,7 +39,7 @@ typedef struct {
     int dim;
     int counts[3];
     double dmin[3], dmax[3];
-    int model;           /* 0 = COROTATED_FIXED, 1 = NEO_HOOKEAN */
+    int model;           /* 0 = COROTATED_FIXED, 1 = NEO_HOOKEAN, 2 = ST_VENANT_KIRCHHOFF_HENCKY_STRAIN */
     double gravity[3];
     int nobj;
     oracle_object obj[MAXOBJ];
@@ -315,6 +315,21 @@ static void neohookean_phat(int d, const double* s, double mu, double la, double
     for(int a = 0; a < d; a++) P[a] = mu * s[a] + c * (sqr(Fi[a]) * dF[a] - Fi[a]) + la * inner * Fi[a];
 }
 
+/* ST_VENANT_KIRCHHOFF_HENCKY_STRAIN::P_From_Strain
+ * (Deformables/Constitutive_Models/ST_VENANT_KIRCHHOFF_HENCKY_STRAIN.cpp:67-78):
+ * Phat = (2 mu ln S + lambda tr(ln S)) S^-1, zero once the smallest signed
+ * singular value is <= 0. */
+static void hencky_phat(int d, const double* s, double mu, double la, double* P)
+{
+    if(s[d - 1] <= 0) {
+        for(int a = 0; a < d; a++) P[a] = 0;
+        return;
+    }
+    double l[3], tr = 0;
+    for(int a = 0; a < d; a++) { l[a] = log(s[a]); tr += l[a]; }
+    for(int a = 0; a < d; a++) P[a] = (2 * mu * l[a] + la * tr) / s[a];
+}
+
 /* MPM_FINITE_ELEMENTS::Precompute, MPM_FINITE_ELEMENTS.cpp:47-67:
  * PFT = U * Phat(sigma) * (Fn*V)^T with Fn = F (MPM_EXAMPLE::Capture_Stress). */
 void oracle_pft(int d, int model, const double* F, double mu, double la, double* PFT)
@@ -326,7 +341,8 @@ void oracle_pft(int d, int model, const double* F, double mu, double la, double*
         oracle_svd3(F, U, s, V);
     }
     if(model == 0) corotated_phat(d, s, mu, la, P);
-    else neohookean_phat(d, s, mu, la, P);
+    else if(model == 1) neohookean_phat(d, s, mu, la, P);
+    else hencky_phat(d, s, mu, la, P);
     if(d == 2) {
         double FV[4];
         FV[0] = F[0] * V[0] + F[2] * V[1]; FV[1] = F[1] * V[0] + F[3] * V[1];
@@ -792,6 +808,98 @@ void oracle_plastic_clamp(int d, long long n, double* F, double* Fp, double* mu,
                 for(int k = 0; k < d; k++) { s += Us[r + d * k] * V[c + d * k]; t += Vi[r + d * k] * U[c + d * k]; }
                 Fn[r + d * c] = s;
                 T1[r + d * c] = t;
+            }
+        mul_cm(d, T1, Fe0, T2);
+        mul_cm(d, T2, Fp + p * dd, T1);
+        memcpy(Fe, Fn, dd * sizeof(double));
+        memcpy(Fp + p * dd, T1, dd * sizeof(double));
+    }
+}
+
+/* MPM_DRUCKER_PRAGER::Update_Hardening (Hybrid_Methods/Forces/MPM_DRUCKER_PRAGER.cpp:118-125):
+ * q += increment; phi = pi/180 (a0 + (a1 q - a4) exp(-a3 q));
+ * rho_F = sqrt(2/3) 2 sin(phi) / (3 - sin(phi)).  prm = a0, a1, a3, a4, use_vc. */
+static const double kPi = 3.14159265358979323846;
+
+static void dp_hardening(double* pdef, double* rho_F, double inc, const double* prm)
+{
+    *pdef += inc;
+    const double q = *pdef;
+    const double phi = kPi / 180 * (prm[0] + (prm[1] * q - prm[3]) * exp(-prm[2] * q));
+    const double sp = sin(phi);
+    *rho_F = sqrt(2.0 / 3.0) * 2 * sp / (3 - sp);
+}
+
+/* MPM_DRUCKER_PRAGER::Initialize_Particles (MPM_DRUCKER_PRAGER.cpp:42-58): sigma_Y = sigma_Y0,
+ * rho_F from a zero hardening increment; plastic_def and vc start at 0. */
+void oracle_dp_init(long long n, double* pdef, double* rho_F, double* sigma_Y, double* vc, double sigma_Y0,
+    const double* prm)
+{
+    for(long long p = 0; p < n; p++) {
+        pdef[p] = 0;
+        vc[p] = 0;
+        sigma_Y[p] = sigma_Y0;
+        dp_hardening(pdef + p, rho_F + p, 0, prm);
+    }
+}
+
+/* MPM_PLASTICITY_MODEL::Update_Particles (MPM_PLASTICITY_MODEL.cpp:35-49) with
+ * MPM_DRUCKER_PRAGER::Compute (MPM_DRUCKER_PRAGER.cpp:62-89, store_hardening on):
+ * the trial Hencky strain ln|S| + beta + vc/d, beta = -sigma_Y g / (rho_F d),
+ * g = 1 / (d lambda + 2 mu), b = 1 / (2 mu); k its trace, sh its deviator,
+ * q = |sh|, r = rho_F k / g, dg = q + b r.  dg <= 0: elastic, unchanged.
+ * q = 0 or k > 0 (the tip): strain = exp(-beta) (or 1 without cohesion),
+ * vc += tr ln|S| + d beta, hardening by |ln|S||.  Else onto the cone:
+ * strain = exp(k/d - (r b / q) sh - beta), vc = 0, hardening by dg.
+ * Then F = U strain V^T, Fp = V strain^-1 U^T Fe Fp, over the particles simulated
+ * in the substep.  F, Fp column-major per particle. */
+void oracle_plastic_dp(int d, long long n, double* F, double* Fp, const double* mu, const double* la,
+    double* pdef, double* rho_F, double* sigma_Y, double* vc, const unsigned char* valid, const double* prm)
+{
+    const int dd = d * d;
+    const int use_vc = prm[4] != 0;
+    for(long long p = 0; p < n; p++) {
+        if(!valid[p]) continue;
+        double* Fe = F + p * dd;
+        double U[9], S[3], V[9];
+        if(d == 3) oracle_svd3(Fe, U, S, V);
+        else svd2(Fe, U, S, V);
+        const double g = 1 / (d * la[p] + 2 * mu[p]), b = 1 / (2 * mu[p]);
+        const double beta = -sigma_Y[p] * g / (rho_F[p] * d);
+        double lf[3], st[3], k = 0, lsum = 0, lmag = 0;
+        for(int a = 0; a < d; a++) {
+            lf[a] = log(fabs(S[a]));
+            st[a] = lf[a] + beta + vc[p] / d;
+            k += st[a];
+            lsum += lf[a];
+            lmag += lf[a] * lf[a];
+        }
+        double sh[3], q = 0;
+        for(int a = 0; a < d; a++) { sh[a] = st[a] - k / d; q += sh[a] * sh[a]; }
+        q = sqrt(q);
+        const double r = rho_F[p] * k / g, dg = q + b * r;
+        if(dg <= 0) continue;
+        double strain[3];
+        if(q == 0 || k > 0) {
+            for(int a = 0; a < d; a++) strain[a] = sigma_Y[p] != 0 ? exp(-beta) : 1;
+            if(use_vc) vc[p] += lsum + beta * d;
+            dp_hardening(pdef + p, rho_F + p, sqrt(lmag), prm);
+        } else {
+            const double pp = r * b / q;
+            for(int a = 0; a < d; a++) strain[a] = exp(k / d - pp * sh[a] - beta);
+            vc[p] = 0;
+            dp_hardening(pdef + p, rho_F + p, dg, prm);
+        }
+        double Us[9], Vi[9], Fn[9], T1[9], T2[9], Fe0[9];
+        memcpy(Fe0, Fe, dd * sizeof(double));
+        for(int c = 0; c < d; c++)
+            for(int rr = 0; rr < d; rr++) { Us[rr + d * c] = U[rr + d * c] * strain[c]; Vi[rr + d * c] = V[rr + d * c] / strain[c]; }
+        for(int c = 0; c < d; c++)
+            for(int rr = 0; rr < d; rr++) {
+                double s1 = 0, t = 0;
+                for(int kk = 0; kk < d; kk++) { s1 += Us[rr + d * kk] * V[c + d * kk]; t += Vi[rr + d * kk] * U[c + d * kk]; }
+                Fn[rr + d * c] = s1;
+                T1[rr + d * c] = t;
             }
         mul_cm(d, T1, Fe0, T2);
         mul_cm(d, T2, Fp + p * dd, T1);

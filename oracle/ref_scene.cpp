@@ -8,8 +8,10 @@
 //
 // The scene is set up through the reference's public API exactly as
 // Projects/mpm/STANDARD_TESTS_BASE.cpp does it: quadratic weights
-// (MPM_EXAMPLE.cpp:197-205), MPM_FINITE_ELEMENTS + COROTATED_FIXED or
-// NEO_HOOKEAN with per-particle Lame arrays (STANDARD_TESTS_BASE.cpp:372-392),
+// (MPM_EXAMPLE.cpp:197-205), MPM_FINITE_ELEMENTS + COROTATED_FIXED,
+// NEO_HOOKEAN or ST_VENANT_KIRCHHOFF_HENCKY_STRAIN with per-particle Lame
+// arrays (STANDARD_TESTS_BASE.cpp:372-404), MPM_PLASTICITY_CLAMP or
+// MPM_DRUCKER_PRAGER after G2P (l.409-486),
 // MPM_GRAVITY (l.354-358), collision objects through Add_Collision_Object,
 // symplectic Euler, APIC (use_affine), flip=0, fixed dt.
 #include <Core/Log/LOG.h>
@@ -20,12 +22,14 @@
 #include <Geometry/Implicit_Objects/ANALYTIC_IMPLICIT_OBJECT.h>
 #include <Deformables/Constitutive_Models/COROTATED_FIXED.h>
 #include <Deformables/Constitutive_Models/NEO_HOOKEAN.h>
+#include <Deformables/Constitutive_Models/ST_VENANT_KIRCHHOFF_HENCKY_STRAIN.h>
 #include <Hybrid_Methods/Examples_And_Drivers/MPM_DRIVER.h>
 #include <Hybrid_Methods/Examples_And_Drivers/MPM_EXAMPLE.h>
 #include <Hybrid_Methods/Examples_And_Drivers/MPM_PARTICLES.h>
 #include <Hybrid_Methods/Forces/MPM_FINITE_ELEMENTS.h>
 #include <Hybrid_Methods/Forces/MPM_GRAVITY.h>
 #include <Hybrid_Methods/Forces/MPM_PLASTICITY_CLAMP.h>
+#include <Hybrid_Methods/Forces/MPM_DRUCKER_PRAGER.h>
 #include <Hybrid_Methods/Forces/MPM_FORCE_HELPER.h>
 #include <Hybrid_Methods/Iterators/GATHER_SCATTER.h>
 #include <chrono>
@@ -44,7 +48,9 @@ struct OBJ { int kind, type; double friction, a[3], b[3]; };
 struct SCENE_FILE
 {
     int dim, counts[3], model, nsteps, nobj, ndump, plasticity;
-    double plastic[4];   // theta_c, theta_s, max_hardening, hardening_factor
+    // clamp (1): theta_c, theta_s, max_hardening, hardening_factor;
+    // Drucker-Prager (2): a0, a1, a3, a4, sigma_Y0, use_vc
+    double plastic[6];
     double dmin[3], dmax[3], gravity[3], dt, t0;
     std::vector<int> dumps;
     std::vector<OBJ> objs;
@@ -80,7 +86,9 @@ SCENE_FILE Read_Scene(const char* path)
         rd(f, &o.kind, 1); rd(f, &o.type, 1); rd(f, &o.friction, 1); rd(f, o.a, 3); rd(f, o.b, 3);
         s.objs.push_back(o);
     }
-    if(s.plasticity) rd(f, s.plastic, 4);
+    if(s.plasticity == 1) rd(f, s.plastic, 4);
+    else if(s.plasticity == 2) rd(f, s.plastic, 6);
+    else if(s.plasticity) throw std::runtime_error("unknown plasticity");
     rd(f, &s.n, 1);
     size_t n = s.n, d = s.dim;
     s.X.resize(n * d); s.V.resize(n * d); s.F.resize(n * d * d); s.B.resize(n * d * d);
@@ -100,6 +108,7 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
     typedef typename BASE::COLLISION_TYPE COLLISION_TYPE;
     using BASE::grid; using BASE::particles; using BASE::gather_scatter; using BASE::force_helper;
     const SCENE_FILE& s;
+    MPM_DRUCKER_PRAGER<TV>* dp = 0;
 
     FILE_SCENE(const SCENE_FILE& s_, int threads)
         : BASE(STREAM_TYPE(T())), s(s_)
@@ -146,9 +155,17 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
         if(s.plasticity == 1)
             this->plasticity_models.Append(new MPM_PLASTICITY_CLAMP<TV>(particles, &gather_scatter, (T)s.plastic[0],
                 (T)s.plastic[1], (T)s.plastic[2], (T)s.plastic[3]));
+        if(s.plasticity == 2) {   // as STANDARD_TESTS_BASE::Add_Drucker_Prager (explicit)
+            dp = new MPM_DRUCKER_PRAGER<TV>(particles, &gather_scatter, (T)s.plastic[0], (T)s.plastic[1],
+                (T)s.plastic[2], (T)s.plastic[3]);
+            dp->use_vc = s.plastic[5] != 0;
+            dp->Initialize_Particles(0, (T)s.plastic[4]);
+            this->plasticity_models.Append(dp);
+        }
         ISOTROPIC_CONSTITUTIVE_MODEL<T, TV::m>* model;
         if(s.model == 0) model = new COROTATED_FIXED<T, TV::m>((T)1, (T).3);
-        else model = new NEO_HOOKEAN<T, TV::m>((T)1, (T).3);
+        else if(s.model == 1) model = new NEO_HOOKEAN<T, TV::m>((T)1, (T).3);
+        else model = new ST_VENANT_KIRCHHOFF_HENCKY_STRAIN<T, TV::m>((T)1, (T).3);
         this->Add_Force(*new MPM_FINITE_ELEMENTS<TV>(force_helper, *model, gather_scatter, 0));
         TV g;
         for(int a = 0; a < d; a++) g(a) = (T)s.gravity[a];
@@ -246,10 +263,17 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
             for(size_t p = 0; p < n; p++) for(int k = 0; k < d * d; k++) buf[p * d * d + k] = example.particles.Fp(p).x[k];
             wr(f, buf.data(), buf.size());
             buf.resize(n);
-            for(size_t p = 0; p < n; p++) buf[p] = example.particles.mu(p);
-            wr(f, buf.data(), n);
-            for(size_t p = 0; p < n; p++) buf[p] = example.particles.lambda(p);
-            wr(f, buf.data(), n);
+            auto put = [&](auto get){for(size_t p = 0; p < n; p++) buf[p] = get(p); wr(f, buf.data(), n);};
+            if(s.plasticity == 1) {
+                put([&](size_t p){return (double)example.particles.mu(p);});
+                put([&](size_t p){return (double)example.particles.lambda(p);});
+            } else {
+                const MPM_DRUCKER_PRAGER<TV>& dp = *example.dp;
+                put([&](size_t p){return (double)dp.plastic_def(p);});
+                put([&](size_t p){return (double)dp.rho_F(p);});
+                put([&](size_t p){return (double)dp.sigma_Y(p);});
+                put([&](size_t p){return (double)dp.vc(p);});
+            }
         }
     }
     fclose(f);

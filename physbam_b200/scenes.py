@@ -32,6 +32,7 @@ import numpy as np
 
 COROTATED = 0
 NEO_HOOKEAN = 1
+HENCKY = 2          # ST_VENANT_KIRCHHOFF_HENCKY_STRAIN (the sand scenes' elastic model)
 
 STICK = 0
 SLIP = 1
@@ -58,7 +59,7 @@ class CollisionObject:
     b: Sequence[float]
 
 
-PLASTICITY_NONE, PLASTICITY_CLAMP = 0, 1
+PLASTICITY_NONE, PLASTICITY_CLAMP, PLASTICITY_DRUCKER_PRAGER = 0, 1, 2
 
 
 @dataclasses.dataclass
@@ -72,6 +73,45 @@ class Plasticity:
     theta_s: float = 7.5e-3
     max_hardening: float = 5.0
     hardening_factor: float = 10.0
+
+
+@dataclasses.dataclass
+class DruckerPrager:
+    """Sand plasticity, MPM_DRUCKER_PRAGER (`Hybrid_Methods/Forces/MPM_DRUCKER_PRAGER.cpp:60-125`):
+    the Hencky strain is projected onto the Drucker-Prager cone after each G2P.  Friction
+    angle (degrees) a0 + (a1 q - a4) exp(-a3 q) of the accumulated plastic deformation q
+    (the Mast et al. hardening of `Update_Hardening`); `cohesion` is the initial sigma_Y
+    (`Initialize_Particles`); `use_vc` keeps the volume-correction term."""
+    kind: int = PLASTICITY_DRUCKER_PRAGER
+    a0: float = 35.0
+    a1: float = 0.0
+    a3: float = 0.2
+    a4: float = 10.0
+    cohesion: float = 0.0
+    use_vc: bool = True
+
+
+def plastic_keys(pl) -> tuple:
+    """Per-particle plastic state a dump / fixture carries for plasticity `pl`."""
+    if pl is None:
+        return ()
+    if pl.kind == PLASTICITY_CLAMP:
+        return ("Fp", "mu", "lam")
+    return ("Fp", "pdef", "rho_F", "cohesion", "vc")
+
+
+def plastic_params(pl) -> list:
+    """The plasticity as the flat list the scene file and the fixtures hold (kind first)."""
+    if pl.kind == PLASTICITY_CLAMP:
+        return [pl.kind, pl.theta_c, pl.theta_s, pl.max_hardening, pl.hardening_factor]
+    return [pl.kind, pl.a0, pl.a1, pl.a3, pl.a4, pl.cohesion, 1.0 if pl.use_vc else 0.0]
+
+
+def plastic_from_params(p):
+    p = [float(x) for x in p]
+    if int(p[0]) == PLASTICITY_CLAMP:
+        return Plasticity(int(p[0]), *p[1:5])
+    return DruckerPrager(int(p[0]), *p[1:6], bool(p[6]))
 
 
 @dataclasses.dataclass
@@ -338,6 +378,41 @@ def small_snow_2d(seed=23, G=16, nsteps=20, dt=1e-4):
     return s
 
 
+def small_sand_3d(seed=31, G=16, nsteps=20, dt=1e-4):
+    """A small sand block (St. Venant-Kirchhoff Hencky + Drucker-Prager with Mast hardening)
+    thrown against a sticky floor; a random initial F per particle, compressed by 3 % for
+    x > 0.4, starts particles in every branch of the return mapping (elastic, cone, tip)."""
+    s = small_3d(seed=seed, G=G, model=HENCKY, nsteps=nsteps, dt=dt, E=(1e5, 3e5), v=(0.5, -3.0, 0.25))
+    s.name = "smallsand3d"
+    rng = np.random.default_rng(seed + 1)
+    s.F = np.eye(3) + 0.04 * rng.standard_normal((s.n, 3, 3))
+    s.F[s.X[:, 0] > 0.4] *= 0.97
+    s.plasticity = DruckerPrager(a0=35.0, a1=9.0, a3=0.3, a4=10.0)
+    return s
+
+
+def small_sand_2d(seed=33, G=16, nsteps=20, dt=1e-4):
+    """The 2D sand block, with cohesion (sigma_Y = 100 Pa) and no volume correction."""
+    s = small_2d(seed=seed, G=G, model=HENCKY, nsteps=nsteps, dt=dt)
+    s.name = "smallsand2d"
+    s.mu *= 5.0
+    s.lam *= 5.0
+    rng = np.random.default_rng(seed + 1)
+    s.F = np.eye(2) + 0.04 * rng.standard_normal((s.n, 2, 2))
+    s.F[s.X[:, 0] > 0.5] *= 0.97
+    s.plasticity = DruckerPrager(cohesion=100.0, use_vc=False)
+    return s
+
+
+def sand_3d(seed=1234, G=128, ppc=8, E=3.537e5, nu=0.3, density=2200.0, dt=5e-5, nsteps=200):
+    """Two balls of sand colliding on the 128^3 grid (the spheres_3d geometry): St. Venant-Kirchhoff
+    Hencky with Drucker-Prager (Mast et al. case 2 hardening: 35, 9, 0.3, 10)."""
+    s = spheres_3d(seed=seed, G=G, ppc=ppc, E=E, nu=nu, density=density, dt=dt, nsteps=nsteps, model=HENCKY)
+    s.name = "sand3d"
+    s.plasticity = DruckerPrager(a0=35.0, a1=9.0, a3=0.3, a4=10.0)
+    return s
+
+
 def snowballs_3d(seed=1234, G=128, ppc=8, E=1.4e5, nu=0.2, density=400.0, dt=5e-5, nsteps=200):
     """Two snowballs (r = 0.12) colliding in a 128^3 box, the spheres_3d geometry with the
     Stomakhin et al. 2013 snow parameters (theta_c 2.5e-2, theta_s 7.5e-3, hardening 10)."""
@@ -367,7 +442,8 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         for o in s.objects:
             f.write(struct.pack("<2i7d", o.kind, o.type, o.friction, *pad3(o.a), *pad3(o.b)))
         if pl:
-            f.write(struct.pack("<4d", pl.theta_c, pl.theta_s, pl.max_hardening, pl.hardening_factor))
+            prm = plastic_params(pl)[1:]
+            f.write(struct.pack("<%dd" % len(prm), *prm))
         f.write(struct.pack("<q", s.n))
         f.write(np.ascontiguousarray(s.X, np.float64).tobytes())
         f.write(np.ascontiguousarray(s.V, np.float64).tobytes())
@@ -378,13 +454,14 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
             f.write(np.ascontiguousarray(a, np.float64).tobytes())
 
 
-def read_dump(path, dim, n, counts, plastic=False):
+def read_dump(path, dim, n, counts, plastic=()):
     """Read the per-substep dumps written by the reference runner / C oracle.
 
     Record: int32 step; X (n,d); V (n,d); F (n,d,d col-major); B (same); valid u8[n];
     grid mass after P2G; grid velocity after P2G (``v = mv/m``, d per node); grid
-    velocity after forces; grid friction velocity after forces; with plasticity
-    also Fp (n,d,d col-major), mu (n), lambda (n).  Grids cover the ghosted domain
+    velocity after forces; grid friction velocity after forces; then the plastic
+    state named by `plastic` (`plastic_keys`): Fp (n,d,d col-major) and n scalars
+    per other key.  Grids cover the ghosted domain
     (G+6)^d, last index fastest (`Core/Math_Tools/RANGE_ITERATOR.h`).
     """
     gshape = tuple(c + 2 * GHOST for c in counts[:dim])
@@ -406,10 +483,11 @@ def read_dump(path, dim, n, counts, plastic=False):
             rec["grid_v0"] = np.frombuffer(f.read(8 * gn * dim), np.float64).reshape(gshape + (dim,))
             rec["grid_v"] = np.frombuffer(f.read(8 * gn * dim), np.float64).reshape(gshape + (dim,))
             rec["grid_vf"] = np.frombuffer(f.read(8 * gn * dim), np.float64).reshape(gshape + (dim,))
-            if plastic:
-                rec["Fp"] = np.swapaxes(np.frombuffer(f.read(8 * n * dim * dim), np.float64).reshape(n, dim, dim), 1, 2)
-                rec["mu"] = np.frombuffer(f.read(8 * n), np.float64).copy()
-                rec["lam"] = np.frombuffer(f.read(8 * n), np.float64).copy()
+            for k in plastic:
+                if k == "Fp":
+                    rec[k] = np.swapaxes(np.frombuffer(f.read(8 * n * dim * dim), np.float64).reshape(n, dim, dim), 1, 2)
+                else:
+                    rec[k] = np.frombuffer(f.read(8 * n), np.float64).copy()
             out[step] = rec
     return out
 

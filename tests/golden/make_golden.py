@@ -32,6 +32,9 @@ CASES = {
     # snow: MPM_PLASTICITY_CLAMP after every G2P (Fp, hardened mu and lambda dumped too)
     "smallsnow3d_corotated": (lambda: S.small_snow_3d(), [0, 19], [0, 19]),
     "smallsnow2d_corotated": (lambda: S.small_snow_2d(), [0, 19], [19]),
+    # sand: ST_VENANT_KIRCHHOFF_HENCKY_STRAIN + MPM_DRUCKER_PRAGER (Fp, plastic_def, rho_F, sigma_Y, vc dumped)
+    "smallsand3d_hencky": (lambda: S.small_sand_3d(), [0, 1, 19], [0, 19]),
+    "smallsand2d_hencky": (lambda: S.small_sand_2d(), [0, 19], [19]),
 }
 
 
@@ -57,10 +60,10 @@ def main(names=None):
             mu=scene.mu, lam=scene.lam, dumps=np.array(dumps))
         pl = scene.plasticity
         if pl is not None:
-            arrays["plasticity"] = np.array([pl.kind, pl.theta_c, pl.theta_s, pl.max_hardening, pl.hardening_factor])
+            arrays["plasticity"] = np.array(S.plastic_params(pl), np.float64)
         for step in dumps:
             r = ref[step]
-            for k in ("X", "V", "F", "B", "valid") + (("Fp", "mu", "lam") if pl is not None else ()):
+            for k in ("X", "V", "F", "B", "valid") + S.plastic_keys(pl):
                 arrays["s%d_%s" % (step, k)] = r[k]
             if step in grid_steps:
                 for k in ("grid_m", "grid_v0", "grid_v", "grid_vf"):
@@ -80,13 +83,12 @@ def load(name):
                     z["X"].copy(), z["V"].copy(), z["F"].copy(), z["B"].copy(), z["mass"].copy(),
                     z["volume"].copy(), z["mu"].copy(), z["lam"].copy())
     if "plasticity" in z:
-        p = z["plasticity"]
-        scene.plasticity = S.Plasticity(int(p[0]), float(p[1]), float(p[2]), float(p[3]), float(p[4]))
+        scene.plasticity = S.plastic_from_params(z["plasticity"])
     dumps = {}
     for step in z["dumps"]:
         step = int(step)
         rec = {}
-        for k in ("X", "V", "F", "B", "valid", "grid_m", "grid_v0", "grid_v", "grid_vf", "Fp", "mu", "lam"):
+        for k in ("X", "V", "F", "B", "valid", "grid_m", "grid_v0", "grid_v", "grid_vf") + S.plastic_keys(scene.plasticity):
             key = "s%d_%s" % (step, k)
             if key in z:
                 rec[k] = z[key]

@@ -15,7 +15,8 @@ from physbam_b200 import scenes as S
 # few ulps per step; B carries a cancellation (sum w vf Z - Vpf X) that
 # amplifies ulps by |Z|/dx, hence its looser bound.
 TOL = {"X": 1e-13, "V": 1e-12, "F": 1e-12, "B": 1e-11, "grid_m": 1e-13, "grid_v0": 1e-12,
-       "grid_v": 1e-12, "grid_vf": 1e-12, "Fp": 1e-12, "mu": 1e-12, "lam": 1e-12}
+       "grid_v": 1e-12, "grid_vf": 1e-12, "Fp": 1e-12, "mu": 1e-12, "lam": 1e-12,
+       "pdef": 1e-12, "rho_F": 1e-12, "cohesion": 1e-15, "vc": 1e-12}
 
 
 def rel(a, b, floor=1e-300):
@@ -28,7 +29,8 @@ def rel(a, b, floor=1e-300):
 def floors(scene, ref):
     vmax = max(float(np.max(np.abs(ref["V"]))), 1e-12)
     return {"X": 1.0, "V": vmax, "F": 1.0, "B": vmax / scene.dx, "grid_m": 1e-300, "grid_v0": vmax,
-            "grid_v": vmax, "grid_vf": vmax, "Fp": 1.0, "mu": 1e-300, "lam": 1e-300}
+            "grid_v": vmax, "grid_vf": vmax, "Fp": 1.0, "mu": 1e-300, "lam": 1e-300,
+            "pdef": 1e-300, "rho_F": 1e-300, "cohesion": 1.0, "vc": 1e-300}
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -45,7 +47,7 @@ def test_oracle_matches_reference_dumps(name):
         fl = floors(scene, ref)
         got = {"X": st.X, "V": st.V, "F": st.F_rowmajor(), "B": st.B_rowmajor()}
         if scene.plasticity is not None:
-            got.update(Fp=st.Fp_rowmajor(), mu=st.mu, lam=st.lam)
+            got.update(st.plastic_state())
         for k, v in got.items():
             e = rel(v, ref[k], fl[k])
             assert e < TOL[k], (name, step, k, e)
@@ -141,3 +143,18 @@ def test_snow_fixtures_exercise_plasticity():
         sv = np.linalg.svd(ref["F"], compute_uv=False)
         pl = scene.plasticity
         assert sv.min() >= 1 - pl.theta_c - 1e-12 and sv.max() <= 1 + pl.theta_s + 1e-12, name
+
+
+def test_sand_fixtures_exercise_every_branch():
+    """The sand fixtures leave particles in all three cases of the Drucker-Prager
+    return mapping: elastic (no plastic deformation yet), the tip (vc != 0) and
+    the cone (plastic deformation, vc = 0)."""
+    for name in ("smallsand3d_hencky", "smallsand2d_hencky"):
+        scene, dumps = load(name)
+        ref = dumps[max(dumps)]
+        elastic = ref["pdef"] == 0
+        assert 0.05 < elastic.mean() < 0.95, name
+        if scene.plasticity.use_vc:
+            assert (ref["vc"] != 0).mean() > 0.05, name
+        assert ((ref["pdef"] > 0) & (ref["vc"] == 0)).mean() > 0.05, name
+        assert scene.model == S.HENCKY
