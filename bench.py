@@ -36,8 +36,10 @@ METRIC = "particle-substeps/s"
 WORKLOAD = "spheres3d-128^3-neohookean-8ppc-fp32"
 LARGE_WORKLOAD = "dam3d-256^3-corotated-8ppc-fp32"
 ALG_BYTES = {"p2g": 112, "g2p": 144, "substep": 256}    # bytes per particle (FP32, 3D)
-PLASTIC_BYTES = 88                                      # snow: Fp, mu0, lambda0 read and written by G2P
-SNOW_LEAD_SUBSTEPS = 600                                # snow leg: substeps run before timing
+# plastic state read and written by G2P per particle: snow Fp, mu0, lambda0;
+# sand Fp, plastic_def, rho_F, sigma_Y, vc
+PLASTIC_BYTES = {1: 88, 2: 104}
+SNOW_LEAD_SUBSTEPS = 600                                # plastic legs: substeps run before timing
 GRID_BYTES_PER_NODE = 48                                # grid update: read 16, write 32
 
 
@@ -307,11 +309,14 @@ def our_arm(args):
     roof = roofline_of(ktimes, n, peak, peak_kind, WORKLOAD)
     total_k = sum(v[0] for v in ktimes.values())
 
-    large = batch = adjoint = plain = snow = None
+    large = batch = adjoint = plain = snow = sand = None
     if world == 1 and not args.no_plain:
         plain = measure_plain_fp64(args, D, S, stream, flush, substep_ms)
     if world == 1 and not args.no_snow:
-        snow = measure_snow(args, D, S, stream, flush, peak, substep_ms)
+        snow = measure_plastic(args, D, S, stream, flush, peak, substep_ms, S.snowballs_3d(),
+                               "snowballs3d-128^3-corotated-8ppc-clamp-fp32")
+        sand = measure_plastic(args, D, S, stream, flush, peak, substep_ms, S.sand_3d(),
+                               "sand3d-128^3-hencky-8ppc-druckerprager-fp32")
     if world == 1 and not args.no_large:
         large = measure_large(args, D, S, stream, flush, peak, peak_kind)
     if not args.no_batch:
@@ -342,6 +347,7 @@ def our_arm(args):
             "kernel_share": {k: v[0] / total_k for k, v in ktimes.items()},
             "plain_fp64": plain,
             "snow": snow,
+            "sand": sand,
             "large_config": large,
             "batch_config": batch,
             "adjoint": adjoint,
@@ -403,11 +409,12 @@ def measure_plain_fp64(args, D, S, stream, flush, fast_ms):
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
 
 
-def measure_snow(args, D, S, stream, flush, peak, elastic_ms):
-    """Two snowballs with the same geometry as the headline case (128^3, 8 ppc,
-    COROTATED_FIXED, Stomakhin et al. 2013 parameters) and MPM_PLASTICITY_CLAMP
-    after every G2P, fused into the fast path's G2P: the cost of plasticity."""
-    scene = S.snowballs_3d()
+def measure_plastic(args, D, S, stream, flush, peak, elastic_ms, scene, workload):
+    """Two balls with the geometry of the headline case (128^3, 8 ppc) and
+    plasticity after every G2P, fused into the fast path's G2P: snow
+    (COROTATED_FIXED + MPM_PLASTICITY_CLAMP, Stomakhin et al. 2013 parameters)
+    or sand (St. Venant-Kirchhoff Hencky + MPM_DRUCKER_PRAGER, Mast et al.
+    hardening).  The cost of plasticity against the elastic headline."""
     n = scene.n
     drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
     drv.set_stream(stream.cuda_stream)
@@ -423,16 +430,21 @@ def measure_snow(args, D, S, stream, flush, peak, elastic_ms):
     sub = ms / steps
     g2p = ktimes.get("fast_g2p")
     g2p_ms = g2p[0] / max(g2p[1], 1) if g2p else None
-    g2p_bytes = (ALG_BYTES["g2p"] + PLASTIC_BYTES) * n
-    return {"workload": "snowballs3d-128^3-corotated-8ppc-clamp-fp32", "particles": n, "steps": steps,
+    extra = PLASTIC_BYTES[scene.plasticity.kind]
+    g2p_bytes = (ALG_BYTES["g2p"] + extra) * n
+    if scene.plasticity.kind == S.PLASTICITY_CLAMP:
+        frac = float(np.mean(np.abs(plastic["mu"] / plastic["mu0"] - 1.0) > 1e-4))
+    else:
+        frac = float(np.mean(plastic["pdef"] > 0))
+    return {"workload": workload, "particles": n, "steps": steps,
             "timed_after_substeps": SNOW_LEAD_SUBSTEPS,
             "ms_per_step": sub, "value": n * steps / (ms / 1e3), "unit": METRIC,
             "over_elastic_headline": sub / elastic_ms,
-            "plastic_fraction": float(np.mean(np.abs(plastic["mu"] / plastic["mu0"] - 1.0) > 1e-4)),
+            "plastic_fraction": frac,
             "g2p_roofline": None if g2p_ms is None else {
                 "achieved": g2p_bytes / (g2p_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                 "frac": g2p_bytes / (g2p_ms / 1e3) / 1e9 / peak,
-                "alg_bytes_per_particle": ALG_BYTES["g2p"] + PLASTIC_BYTES},
+                "alg_bytes_per_particle": ALG_BYTES["g2p"] + extra},
             "autotune": tuned,
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
 
@@ -474,7 +486,7 @@ def profile_case(args, D, S):
     Prints one JSON line with the per-kernel times; used to make the ncu summaries."""
     import torch
     make = {"spheres3d": S.spheres_3d, "dam3d": S.dam_3d, "cube3d": S.cube_3d,
-            "snowballs3d": S.snowballs_3d}[args.scene]
+            "snowballs3d": S.snowballs_3d, "sand3d": S.sand_3d}[args.scene]
     scene = make(G=args.grid) if args.grid else make()
     drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
     if args.shape:
@@ -530,8 +542,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-scene batched measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward/backward timing")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 path on the same workload")
-    ap.add_argument("--no-snow", action="store_true", help="skip the snow (plasticity) measurement")
-    ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d", "snowballs3d"],
+    ap.add_argument("--no-snow", action="store_true", help="skip the snow and sand (plasticity) measurements")
+    ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d", "snowballs3d", "sand3d"],
                     help="profiling run of one scene only")
     ap.add_argument("--grid", type=int, default=0, help="grid cells per side for --scene")
     ap.add_argument("--shape", default="", help="launch shape for --scene: P2G variant,G2P threads,CTA multiplier")

@@ -47,8 +47,10 @@ enum mpm_status {
 enum mpm_precision { MPM_FP32 = 0, MPM_FP64 = 1 };
 
 /* COROTATED_FIXED (Deformables/Constitutive_Models/COROTATED_FIXED.cpp:59-65),
- * NEO_HOOKEAN with failure threshold .25 (NEO_HOOKEAN.cpp:42-82). */
-enum mpm_model { MPM_COROTATED_FIXED = 0, MPM_NEO_HOOKEAN = 1 };
+ * NEO_HOOKEAN with failure threshold .25 (NEO_HOOKEAN.cpp:42-82),
+ * ST_VENANT_KIRCHHOFF_HENCKY_STRAIN (ST_VENANT_KIRCHHOFF_HENCKY_STRAIN.cpp:67-78,
+ * the elastic model of the reference's sand scenes). */
+enum mpm_model { MPM_COROTATED_FIXED = 0, MPM_NEO_HOOKEAN = 1, MPM_STVK_HENCKY = 2 };
 
 /* MPM_COLLISION_OBJECT::COLLISION_TYPE (Hybrid_Methods/Collisions/MPM_COLLISION_OBJECT.h:21) */
 enum mpm_collision_type { MPM_STICK = 0, MPM_SLIP = 1, MPM_SEPARATE = 2 };
@@ -171,28 +173,44 @@ int mpm_synchronize(mpm_handle* h);
 
 /* ---- plasticity ----------------------------------------------------------- */
 
-/* Snow plasticity, MPM_PLASTICITY_CLAMP (Hybrid_Methods/Forces/
- * MPM_PLASTICITY_CLAMP.cpp:28-45), applied after each G2P to every particle
- * simulated in the substep (valid at its start, including one that left the
- * domain in that G2P) as MPM_DRIVER::Update_Plasticity_And_Hardening
- * (MPM_DRIVER.cpp:156,922-928).  The fast path runs it in FP32 inside G2P. */
-enum mpm_plasticity_kind { MPM_PLASTICITY_NONE = 0, MPM_PLASTICITY_CLAMP = 1 };
+/* Plasticity, applied after each G2P to every particle simulated in the
+ * substep (valid at its start, including one that left the domain in that
+ * G2P) as MPM_DRIVER::Update_Plasticity_And_Hardening (MPM_DRIVER.cpp:156,
+ * 922-928) through MPM_PLASTICITY_MODEL::Update_Particles
+ * (MPM_PLASTICITY_MODEL.cpp:35-49).  The fast path runs it in FP32 inside G2P.
+ *   MPM_PLASTICITY_CLAMP (snow; Hybrid_Methods/Forces/MPM_PLASTICITY_CLAMP.cpp:28-45)
+ *   MPM_PLASTICITY_DRUCKER_PRAGER (sand; MPM_DRUCKER_PRAGER.cpp:42-125, explicit) */
+enum mpm_plasticity_kind { MPM_PLASTICITY_NONE = 0, MPM_PLASTICITY_CLAMP = 1, MPM_PLASTICITY_DRUCKER_PRAGER = 2 };
 typedef struct {
     int kind;
+    /* clamp */
     double theta_c;            /* singular values are clamped to [1 - theta_c, 1 + theta_s] */
     double theta_s;
     double max_hardening;      /* hardening = exp(min(max_hardening, hardening_factor (1 - det Fp))) */
     double hardening_factor;
+    /* Drucker-Prager: friction angle (degrees) a0 + (a1 q - a4) exp(-a3 q) of the
+     * accumulated plastic deformation q; cohesion = the initial sigma_Y; use_vc
+     * keeps the volume-correction term (MPM_DRUCKER_PRAGER::use_vc) */
+    double dp_a0;
+    double dp_a1;
+    double dp_a3;
+    double dp_a4;
+    double cohesion;
+    int use_vc;
 } mpm_plasticity_desc;
 
 /* Turn plasticity on or off (before or after mpm_set_particles).  Particles
- * then start unplastic: Fp = I, mu0 = mu, lambda0 = lambda, as the
- * reference's scenes seed them (Projects/mpm/STANDARD_TESTS_BASE.cpp:299,568-586). */
+ * then start unplastic, as the reference's scenes seed them: Fp = I; for the
+ * clamp mu0 = mu, lambda0 = lambda (Projects/mpm/STANDARD_TESTS_BASE.cpp:299,
+ * 568-586); for Drucker-Prager plastic_def = vc = 0, sigma_Y = cohesion and
+ * rho_F from the friction angle at q = 0 (MPM_DRUCKER_PRAGER::Initialize_Particles).
+ * The Drucker-Prager scenes pair it with MPM_STVK_HENCKY. */
 int mpm_set_plasticity(mpm_handle* h, const mpm_plasticity_desc* p);
 
-/* The plastic state of MPM_PARTICLES (Fp, and mu0/lambda0 with the hardened
- * mu/lambda): Fp n*d*d column-major, the others n scalars.  Any pointer may be
- * NULL (not copied). */
+/* The plastic state of MPM_PARTICLES: Fp (n*d*d column-major) and n scalars
+ * per other array; the clamp's (mu0, lambda0 and the hardened mu, lambda) or
+ * Drucker-Prager's (plastic_def, rho_F, sigma_Y = cohesion, vc).  Any pointer
+ * may be NULL (not copied); the other kind's arrays must be NULL. */
 typedef struct {
     int64_t n;
     int dtype;
@@ -202,6 +220,10 @@ typedef struct {
     void* lambda;
     void* mu0;
     void* lambda0;
+    void* plastic_def;
+    void* rho_F;
+    void* cohesion;
+    void* vc;
 } mpm_plastic_view;
 int mpm_get_plastic_state(mpm_handle* h, mpm_plastic_view* view);
 int mpm_set_plastic_state(mpm_handle* h, const mpm_plastic_view* view);

@@ -161,7 +161,7 @@ int mpm_create(const mpm_grid_desc* g, const mpm_model_desc* m, mpm_handle** out
     *out = nullptr;
     if(g->dim != 2 && g->dim != 3) return MPM_ERR_ARG;
     if(g->ghost != MPM_GHOST) return MPM_ERR_ARG;
-    if(m->model != MPM_COROTATED_FIXED && m->model != MPM_NEO_HOOKEAN) return MPM_ERR_ARG;
+    if(m->model != MPM_COROTATED_FIXED && m->model != MPM_NEO_HOOKEAN && m->model != MPM_STVK_HENCKY) return MPM_ERR_ARG;
     if(m->precision != MPM_FP32 && m->precision != MPM_FP64) return MPM_ERR_ARG;
     if(m->path != MPM_PATH_FAST && m->path != MPM_PATH_PLAIN) return MPM_ERR_ARG;
     if(m->path == MPM_PATH_FAST && (g->dim != 3 || m->precision != MPM_FP32)) return MPM_ERR_ARG;
@@ -364,6 +364,8 @@ int mpm_batch_create(const mpm_scene_desc* scenes, int count, const mpm_collisio
 {
     if(!scenes || !out || count < 1 || object_count < 0 || (object_count && !objects)) return MPM_ERR_ARG;
     *out = nullptr;
+    for(int i = 0; i < count; i++)
+        if(scenes[i].model < MPM_COROTATED_FIXED || scenes[i].model > MPM_STVK_HENCKY) return MPM_ERR_ARG;
     mpm_model_desc m;
     memset(&m, 0, sizeof(m));
     m.model = scenes[0].model;
@@ -455,22 +457,38 @@ int mpm_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_ke
 int mpm_set_plasticity(mpm_handle* h, const mpm_plasticity_desc* p)
 {
     if(!h || !p) return MPM_ERR_ARG;
-    if(p->kind != MPM_PLASTICITY_NONE && p->kind != MPM_PLASTICITY_CLAMP) return set_error(h, MPM_ERR_ARG, "unknown plasticity kind");
-    if(p->kind) {
+    if(p->kind != MPM_PLASTICITY_NONE && p->kind != MPM_PLASTICITY_CLAMP && p->kind != MPM_PLASTICITY_DRUCKER_PRAGER)
+        return set_error(h, MPM_ERR_ARG, "unknown plasticity kind");
+    if(p->kind == MPM_PLASTICITY_CLAMP) {
         if(!(p->theta_c >= 0 && p->theta_c < 1) || !(p->theta_s >= 0) || !std::isfinite(p->theta_s))
             return set_error(h, MPM_ERR_ARG, "clamp bounds: 0 <= theta_c < 1, 0 <= theta_s");
         if(std::isnan(p->max_hardening) || !std::isfinite(p->hardening_factor))
             return set_error(h, MPM_ERR_ARG, "hardening parameters");
     }
+    if(p->kind == MPM_PLASTICITY_DRUCKER_PRAGER) {
+        const double v[] = {p->dp_a0, p->dp_a1, p->dp_a3, p->dp_a4, p->cohesion};
+        for(double x: v)
+            if(!std::isfinite(x)) return set_error(h, MPM_ERR_ARG, "Drucker-Prager parameters must be finite");
+        // rho_F divides the cohesion term: the friction angle must stay in (0, 90) degrees at q = 0
+        const double phi0 = p->dp_a0 - p->dp_a4;
+        if(!(phi0 > 0 && phi0 < 90)) return set_error(h, MPM_ERR_ARG, "friction angle a0 - a4 outside (0, 90) degrees");
+    }
     release_graph(h);
-    const bool was_on = h->plastic.kind != MPM_PLASTICITY_NONE;
+    const int was = h->plastic.kind;
     h->plastic = *p;
-    if(p->kind && !was_on && h->have_particles) {
+    if(p->kind && p->kind != was && h->have_particles) {
         int rc = fast(h) ? fast_plastic_init(h) : plain_plastic_init(h);
         if(rc) return rc;
         MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     }
     return MPM_OK;
+}
+
+// mu0 / lambda0 belong to the clamp, plastic_def .. vc to Drucker-Prager
+static bool plastic_view_matches(const mpm_handle* h, const mpm_plastic_view* v)
+{
+    if(h->plastic.kind == MPM_PLASTICITY_CLAMP) return !v->plastic_def && !v->rho_F && !v->cohesion && !v->vc;
+    return !v->mu0 && !v->lambda0;
 }
 
 int mpm_get_plastic_state(mpm_handle* h, mpm_plastic_view* v)
@@ -479,6 +497,7 @@ int mpm_get_plastic_state(mpm_handle* h, mpm_plastic_view* v)
     if(!h->plastic.kind) return set_error(h, MPM_ERR_STATE, "plasticity is off");
     if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
     if(v->dtype != MPM_FP32 && v->dtype != MPM_FP64) return set_error(h, MPM_ERR_ARG, "dtype");
+    if(!plastic_view_matches(h, v)) return set_error(h, MPM_ERR_ARG, "plastic state arrays of the other plasticity kind");
     return fast(h) ? fast_get_plastic(h, v) : plain_get_plastic(h, v);
 }
 
@@ -488,6 +507,7 @@ int mpm_set_plastic_state(mpm_handle* h, const mpm_plastic_view* v)
     if(!h->plastic.kind) return set_error(h, MPM_ERR_STATE, "plasticity is off");
     if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
     if(v->dtype != MPM_FP32 && v->dtype != MPM_FP64) return set_error(h, MPM_ERR_ARG, "dtype");
+    if(!plastic_view_matches(h, v)) return set_error(h, MPM_ERR_ARG, "plastic state arrays of the other plasticity kind");
     release_graph(h);
     return fast(h) ? fast_set_plastic(h, v) : plain_set_plastic(h, v);
 }

@@ -44,7 +44,8 @@ constexpr int TN = TE * TE * TE;           // 216 nodes per tile
 constexpr uint32_t SENTINEL = 0xffffffffu;
 constexpr int NCOMP = 24;                  // x3 v3 F9 B9 floats per particle
 constexpr int C_X = 0, C_V = 3, C_F = 6, C_B = 15;
-constexpr int NPLAS = 11;                  // plastic state: Fp0..8, mu0, lambda0 floats per particle
+constexpr int NPLAS = 13;                  // plastic state floats per particle: Fp0..8, then
+                                           // mu0, lambda0 (clamp) or plastic_def, rho_F, sigma_Y, vc
 
 struct FastArgs {
     int64_t n, npad;
@@ -73,7 +74,9 @@ struct FastArgs {
     unsigned* flags;
     const float* psrc;    // plastic state (null: plasticity off), current and next buffer
     float* pdst;
-    float prm[4];         // theta_c, theta_s, max_hardening, hardening_factor
+    int pkind, nplas;     // plasticity kind; plastic floats per particle
+    float prm[5];         // clamp: theta_c, theta_s, max_hardening, hardening_factor;
+                          // Drucker-Prager: a0, a1, a3, a4, use_vc
 };
 
 __device__ __forceinline__ int64_t node_index(const SceneDev& sc, int qx, int qy, int qz)
@@ -133,6 +136,30 @@ __device__ __forceinline__ bool stress_fast(int model, const float* F, float mu,
     float b02 = F[0] * F[2] + F[3] * F[5] + F[6] * F[8];
     float b12 = F[1] * F[2] + F[4] * F[5] + F[7] * F[8];
     float J = F[0] * (F[4] * F[8] - F[7] * F[5]) - F[3] * (F[1] * F[8] - F[7] * F[2]) + F[6] * (F[1] * F[5] - F[4] * F[2]);
+    if(model == MPM_STVK_HENCKY) {
+        // P F^T = U diag(2 mu ln S + lambda tr ln S) U^T = mu ln b + (lambda / 2) tr(ln b) I,
+        // U diag(S^2) U^T = b = F F^T; zero stress once det F <= 0 (the reference's
+        // test on the last signed singular value)
+        if(!(J > 0.f)) {
+#pragma unroll
+            for(int e = 0; e < 9; e++) PFT[e] = 0.f;
+            return true;
+        }
+        float A[3][3] = {{b00, b01, b02}, {b01, b11, b12}, {b02, b12, b22}}, W[3][3];
+        sym_eig3f(A, W);
+        const float lmax = fmaxf(A[0][0], fmaxf(A[1][1], A[2][2])), lmin = fminf(A[0][0], fminf(A[1][1], A[2][2]));
+        if(!(lmin > 1e-4f * lmax)) return false;     // sigma_min / sigma_max < 1e-2: FP64 SVD
+        float l[3];
+#pragma unroll
+        for(int i = 0; i < 3; i++) l[i] = mu * logf(A[i][i]);
+        const float pr = 0.5f * la * (logf(A[0][0]) + logf(A[1][1]) + logf(A[2][2]));
+#pragma unroll
+        for(int r = 0; r < 3; r++)
+#pragma unroll
+            for(int c = 0; c < 3; c++)
+                PFT[r + 3 * c] = W[r][0] * l[0] * W[c][0] + W[r][1] * l[1] * W[c][1] + W[r][2] * l[2] * W[c][2] + (r == c ? pr : 0.f);
+        return true;
+    }
     if(model == MPM_NEO_HOOKEAN) {
         if(!(J >= (float)kNeoHookeanThreshold)) return false;
         float d = la * logf(J) - mu;
@@ -232,7 +259,7 @@ __global__ void k_ranges(FastArgs a)
             a.dst_attr[j] = a.src_attr[i];
             a.dst_pid[j] = a.src_pid[i];
             if(a.psrc)
-                for(int c = 0; c < NPLAS; c++) a.pdst[c * a.npad + j] = a.psrc[c * a.npad + i];
+                for(int c = 0; c < a.nplas; c++) a.pdst[c * a.npad + j] = a.psrc[c * a.npad + i];
             a.keys_next[j] = SENTINEL;
             continue;
         }
@@ -1003,88 +1030,34 @@ __device__ __forceinline__ bool clamp_inactive(const float* F, const float* prm)
 // the reference's updates only need V and S (U^T F = S V^T):
 //   F  <- U S' V^T       = F  (V diag(S'/S) V^T)
 //   Fp <- V S'^-1 U^T F Fp = (V diag(S/S') V^T) Fp
-// V diag(S) V^T is the eigendecomposition of C = F^T F, found by cyclic
-// Jacobi rotations (Golub & Van Loan, Matrix Computations, 4th ed., 8.5.2:
-// the symmetric Schur rotation, cyclic sweeps of the 3 pivots), in registers.
-// Both matrix functions depend only on C, so they are stable for repeated
-// singular values.  Returns 0 (unchanged), 1 (clamped) or -1 (outside the
-// conditions above: the caller takes the SVD route).
-template<int P, int Q>
-__device__ __forceinline__ void jacobi_rotate(float (&A)[3][3], float (&V)[3][3])
-{
-    constexpr int R = 3 - P - Q;
-    const float apq = A[P][Q];
-    const float d = A[Q][Q] - A[P][P];
-    // t = tan of the rotation angle: an approximate t still gives an exact
-    // rotation (c and s come from t) and only leaves a residual that the next
-    // sweep removes; c to full precision keeps V orthogonal
-    const float h = d * d + 4.f * apq * apq;
-    const float den = fabsf(d) + h * rsqrtf(h);
-    float t = h > 0.f ? __fdividef(2.f * apq, den) : 0.f;
-    if(d < 0.f) t = -t;
-    const float x = 1.f + t * t;
-    float c = rsqrtf(x);
-    c = c * (1.5f - 0.5f * x * c * c);   // one Newton step
-    const float s = t * c;
-    A[P][P] -= t * apq;
-    A[Q][Q] += t * apq;
-    A[P][Q] = A[Q][P] = 0.f;
-    const float arp = A[R][P], arq = A[R][Q];
-    A[R][P] = A[P][R] = c * arp - s * arq;
-    A[R][Q] = A[Q][R] = s * arp + c * arq;
-#pragma unroll
-    for(int k = 0; k < 3; k++) {
-        const float vp = V[k][P], vq = V[k][Q];
-        V[k][P] = c * vp - s * vq;
-        V[k][Q] = s * vp + c * vq;
-    }
-}
-
-__device__ __forceinline__ int plastic_eig(float* F, float* Fp, float4& at, float mu0, float la0, const float* prm)
+// V diag(S^2) V^T is the eigensystem of C = F^T F (sym_eig3f).  Both matrix
+// functions depend only on C, so they are stable for repeated singular values
+// (and the Drucker-Prager strain, an isotropic function of S, keeps that).
+// plastic_eig / plastic_dp_eig return 0 (unchanged), 1 (projected) or -1
+// (outside the conditions above: the caller takes the SVD route).
+// Singular values S and right singular vectors V of F from the eigensystem of
+// F^T F (sym_eig3f); false where det F <= 0 or sigma_max / sigma_min > 10 (the
+// caller takes the SVD route).
+__device__ __forceinline__ bool ftf_eig(const float* F, float* S, float (&V)[3][3])
 {
     const float J = F[0] * (F[4] * F[8] - F[7] * F[5]) - F[3] * (F[1] * F[8] - F[7] * F[2]) + F[6] * (F[1] * F[5] - F[4] * F[2]);
-    if(!(J > 0.f)) return -1;
-    float A[3][3], V[3][3];
+    if(!(J > 0.f)) return false;
+    float A[3][3];
 #pragma unroll
     for(int i = 0; i < 3; i++)
 #pragma unroll
-        for(int k = 0; k < 3; k++) {
-            A[i][k] = F[3 * i] * F[3 * k] + F[3 * i + 1] * F[3 * k + 1] + F[3 * i + 2] * F[3 * k + 2];
-            V[i][k] = i == k ? 1.f : 0.f;
-        }
-    // three sweeps reach FP32 accuracy for sigma_max / sigma_min <= 10; a
-    // fourth runs where the off-diagonal part is not yet at rounding level
-#pragma unroll
-    for(int sweep = 0; sweep < 3; sweep++) {
-        jacobi_rotate<0, 1>(A, V);
-        jacobi_rotate<0, 2>(A, V);
-        jacobi_rotate<1, 2>(A, V);
-    }
-    const float off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
-    const float dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
-    if(off > 1e-14f * dia) {
-        jacobi_rotate<0, 1>(A, V);
-        jacobi_rotate<0, 2>(A, V);
-        jacobi_rotate<1, 2>(A, V);
-    }
+        for(int k = 0; k < 3; k++) A[i][k] = F[3 * i] * F[3 * k] + F[3 * i + 1] * F[3 * k + 1] + F[3 * i + 2] * F[3 * k + 2];
+    sym_eig3f(A, V);
     const float lmax = fmaxf(A[0][0], fmaxf(A[1][1], A[2][2])), lmin = fminf(A[0][0], fminf(A[1][1], A[2][2]));
-    if(!(lmin > 1e-2f * lmax)) return -1;
-    const float lo = 1.f - prm[0], hi = 1.f + prm[1];
-    float S[3], St[3];
-    bool same = true;
+    if(!(lmin > 1e-2f * lmax)) return false;
 #pragma unroll
-    for(int i = 0; i < 3; i++) {
-        S[i] = sqrtf(A[i][i]);
-        St[i] = fminf(fmaxf(S[i], lo), hi);
-        same = same && St[i] == S[i];
-    }
-    if(same) return 0;
-    const float* P = Fp;
-    const float detp = P[0] * (P[4] * P[8] - P[7] * P[5]) - P[3] * (P[1] * P[8] - P[7] * P[2]) + P[6] * (P[1] * P[5] - P[4] * P[2]);
-    const float e = prm[3] * (1.f - S[0] * S[1] * S[2] / (St[0] * St[1] * St[2]) * detp);
-    const float coeff = fmaxf(expf(fminf(e, prm[2])), 1e-8f);
-    at.z = mu0 * coeff;
-    at.w = la0 * coeff;
+    for(int i = 0; i < 3; i++) S[i] = sqrtf(A[i][i]);
+    return true;
+}
+
+// F <- U St V^T = F (V diag(St/S) V^T),  Fp <- V St^-1 U^T F Fp = (V diag(S/St) V^T) Fp.
+__device__ __forceinline__ void apply_strain(float* F, float* Fp, const float* S, const float* St, const float (&V)[3][3])
+{
     float g[3], h[3];
 #pragma unroll
     for(int i = 0; i < 3; i++) { g[i] = __fdividef(St[i], S[i]); h[i] = __fdividef(S[i], St[i]); }
@@ -1106,10 +1079,63 @@ __device__ __forceinline__ int plastic_eig(float* F, float* Fp, float4& at, floa
             F[r + 3 * c] = Fo[r] * M[0][c] + Fo[r + 3] * M[1][c] + Fo[r + 6] * M[2][c];
             Fp[r + 3 * c] = N[r][0] * Po[3 * c] + N[r][1] * Po[3 * c + 1] + N[r][2] * Po[3 * c + 2];
         }
+}
+
+__device__ __forceinline__ int plastic_eig(float* F, float* Fp, float4& at, float mu0, float la0, const float* prm)
+{
+    float S[3], V[3][3];
+    if(!ftf_eig(F, S, V)) return -1;
+    const float lo = 1.f - prm[0], hi = 1.f + prm[1];
+    float St[3];
+    bool same = true;
+#pragma unroll
+    for(int i = 0; i < 3; i++) {
+        St[i] = fminf(fmaxf(S[i], lo), hi);
+        same = same && St[i] == S[i];
+    }
+    if(same) return 0;
+    const float* P = Fp;
+    const float detp = P[0] * (P[4] * P[8] - P[7] * P[5]) - P[3] * (P[1] * P[8] - P[7] * P[2]) + P[6] * (P[1] * P[5] - P[4] * P[2]);
+    const float e = prm[3] * (1.f - S[0] * S[1] * S[2] / (St[0] * St[1] * St[2]) * detp);
+    const float coeff = fmaxf(expf(fminf(e, prm[2])), 1e-8f);
+    at.z = mu0 * coeff;
+    at.w = la0 * coeff;
+    apply_strain(F, Fp, S, St, V);
     return 1;
 }
 
-template<bool PLASTIC>
+// Drucker-Prager by the same SVD-free route (det F > 0, well conditioned):
+// the return mapping on S, then F and Fp as for the clamp.  `st` = plastic_def,
+// rho_F, sigma_Y, vc, updated in place.  Returns 0 (elastic), 1 or -1.
+__device__ __forceinline__ int plastic_dp_eig(float* F, float* Fp, float mu, float la, float* st, const float* prm)
+{
+    float S[3], V[3][3], strain[3];
+    if(!ftf_eig(F, S, V)) return -1;
+    if(!dp_strain<float, 3>(S, mu, la, st[0], st[1], st[2], st[3], prm, strain)) return 0;
+    apply_strain(F, Fp, S, strain, V);
+    return 1;
+}
+
+// The Drucker-Prager update through the SVD for the particle already written
+// to slot j, out of line and fed from memory (as plastic_svd_slot).
+__device__ __noinline__ void plastic_dp_svd_slot(float* dst, float* pdst, const float4* dst_attr, int64_t npad, uint32_t j,
+    float a0, float a1, float a3, float a4, float use_vc, unsigned* flags)
+{
+    float F[9], Fp[9], st[4];
+    for(int k = 0; k < 9; k++) { F[k] = dst[(C_F + k) * npad + j]; Fp[k] = pdst[k * npad + j]; }
+    for(int k = 0; k < 4; k++) st[k] = pdst[(9 + k) * npad + j];
+    const float4 at = dst_attr[j];
+    const float prm[5] = {a0, a1, a3, a4, use_vc};
+    bool ok;
+    if(plastic_dp<float, 3>(F, Fp, at.z, at.w, st, prm, ok)) {
+        for(int k = 0; k < 9; k++) { dst[(C_F + k) * npad + j] = F[k]; pdst[k * npad + j] = Fp[k]; }
+    }
+    for(int k = 0; k < 4; k++) pdst[(9 + k) * npad + j] = st[k];
+    if(!ok) atomicOr(flags, MPM_FLAG_NOT_CONVERGED);
+}
+
+// PK: the plasticity fused after the update (0 none, 1 clamp, 2 Drucker-Prager).
+template<int PK>
 __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& sc, const float4* tv, bool anti,
     int ox, int oy, int oz, uint32_t j, G2PState& out)
 {
@@ -1207,17 +1233,21 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
     finite = finite && isfinite(xn[0]) && isfinite(xn[1]) && isfinite(xn[2]);
     if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); ok = false; }
     bool svd = false;
-    if(PLASTIC) {
+    if(PK) {
         // every particle of this substep, including one that just left
-        float Fp[9];
+        float Fp[9], st[4];
 #pragma unroll
         for(int k = 0; k < 9; k++) Fp[k] = a.psrc[k * a.npad + i];
-        const float mu0 = a.psrc[9 * a.npad + i], la0 = a.psrc[10 * a.npad + i];
-        svd = finite && !clamp_inactive(Fn, a.prm) && plastic_eig(Fn, Fp, at, mu0, la0, a.prm) < 0;
+#pragma unroll
+        for(int k = 0; k < (PK == 1 ? 2 : 4); k++) st[k] = a.psrc[(9 + k) * a.npad + i];
+        if(PK == 1)   // st = mu0, lambda0
+            svd = finite && !clamp_inactive(Fn, a.prm) && plastic_eig(Fn, Fp, at, st[0], st[1], a.prm) < 0;
+        else
+            svd = finite && plastic_dp_eig(Fn, Fp, at.z, at.w, st, a.prm) < 0;
 #pragma unroll
         for(int k = 0; k < 9; k++) a.pdst[k * a.npad + j] = Fp[k];
-        a.pdst[9 * a.npad + j] = mu0;
-        a.pdst[10 * a.npad + j] = la0;
+#pragma unroll
+        for(int k = 0; k < (PK == 1 ? 2 : 4); k++) a.pdst[(9 + k) * a.npad + j] = st[k];
     }
     const uint32_t key = ok ? cell_key(sc, xn) : SENTINEL;
 #pragma unroll
@@ -1227,8 +1257,10 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
     a.dst_attr[j] = at;
     a.dst_pid[j] = pid;
     a.keys_next[j] = key;
-    if(PLASTIC && svd)
+    if(PK == 1 && svd)
         plastic_svd_slot(a.dst, a.pdst, a.dst_attr, a.npad, j, a.prm[0], a.prm[1], a.prm[2], a.prm[3], a.flags);
+    if(PK == 2 && svd)
+        plastic_dp_svd_slot(a.dst, a.pdst, a.dst_attr, a.npad, j, a.prm[0], a.prm[1], a.prm[2], a.prm[3], a.prm[4], a.flags);
 #pragma unroll
     for(int k = 0; k < 9; k++) out.Bn[k] = Bn[k];
     out.at = at;
@@ -1236,7 +1268,7 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
     out.ok = ok;
 }
 
-template<int THREADS, bool PLASTIC> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
+template<int THREADS, int PK> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
 {
     __shared__ float4 tv[2 * TN];
     __shared__ int s_work;
@@ -1263,7 +1295,7 @@ template<int THREADS, bool PLASTIC> __global__ void __launch_bounds__(THREADS) k
         uint32_t stay = 0;
         for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
             G2PState o;
-            g2p_particle<PLASTIC>(a, sc, tv, anti, ox, oy, oz, j, o);
+            g2p_particle<PK>(a, sc, tv, anti, ox, oy, oz, j, o);
             // most particles stay in their block: their keys differ from the
             // block's only in the lowest digit, counted per particle; the
             // block's higher digits are counted once below
@@ -1329,31 +1361,57 @@ __global__ void k_plastic_init(int64_t n, int64_t npad, float* P, const float4* 
     }
 }
 
+// Drucker-Prager start (MPM_DRUCKER_PRAGER::Initialize_Particles): Fp = I,
+// plastic_def = vc = 0, sigma_Y = cohesion, rho_F at zero plastic deformation.
+__global__ void k_dp_init(int64_t n, int64_t npad, float* P, float cohesion, float a0, float a1, float a3, float a4)
+{
+    const float prm[5] = {a0, a1, a3, a4, 0.f};
+    float q = 0.f, rho = 0.f;
+    dp_hardening<float>(q, rho, 0.f, prm);
+    for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for(int k = 0; k < 9; k++) P[k * npad + j] = k % 4 == 0 ? 1.f : 0.f;
+        P[9 * npad + j] = q;
+        P[10 * npad + j] = rho;
+        P[11 * npad + j] = cohesion;
+        P[12 * npad + j] = 0.f;
+    }
+}
+
+// Caller-order arrays of the plastic state: Fp, the Lame parameters (in the
+// attributes) and the per-particle scalars at plastic components 9, 10, ...
+template<class T> struct PlasticArrays {
+    T* Fp;
+    T* mu;
+    T* la;
+    T* sc[4];
+};
+
 template<class T> __global__ void k_plastic_out(int64_t n, int64_t npad, const float* P, const float4* attr, const int* pid,
-    T* Fp, T* mu, T* la, T* mu0, T* la0)
+    PlasticArrays<T> o)
 {
     for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t p = pid[j];
-        if(Fp)
-            for(int k = 0; k < 9; k++) Fp[p * 9 + k] = (T)P[k * npad + j];
-        if(mu) mu[p] = (T)attr[j].z;
-        if(la) la[p] = (T)attr[j].w;
-        if(mu0) mu0[p] = (T)P[9 * npad + j];
-        if(la0) la0[p] = (T)P[10 * npad + j];
+        if(o.Fp)
+            for(int k = 0; k < 9; k++) o.Fp[p * 9 + k] = (T)P[k * npad + j];
+        if(o.mu) o.mu[p] = (T)attr[j].z;
+        if(o.la) o.la[p] = (T)attr[j].w;
+        for(int k = 0; k < 4; k++)
+            if(o.sc[k]) o.sc[k][p] = (T)P[(9 + k) * npad + j];
     }
 }
 
 template<class T> __global__ void k_plastic_in(int64_t n, int64_t npad, float* P, float4* attr, const int* pid,
-    const T* Fp, const T* mu, const T* la, const T* mu0, const T* la0)
+    PlasticArrays<T> in)
 {
     for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t p = pid[j];
-        if(Fp)
-            for(int k = 0; k < 9; k++) P[k * npad + j] = (float)Fp[p * 9 + k];
-        if(mu) attr[j].z = (float)mu[p];
-        if(la) attr[j].w = (float)la[p];
-        if(mu0) P[9 * npad + j] = (float)mu0[p];
-        if(la0) P[10 * npad + j] = (float)la0[p];
+        if(in.Fp)
+            for(int k = 0; k < 9; k++) P[k * npad + j] = (float)in.Fp[p * 9 + k];
+        if(in.mu) attr[j].z = (float)in.mu[p];
+        if(in.la) attr[j].w = (float)in.la[p];
+        for(int k = 0; k < 4; k++)
+            if(in.sc[k]) P[(9 + k) * npad + j] = (float)in.sc[k][p];
     }
 }
 
@@ -1409,10 +1467,16 @@ FastArgs make_args(mpm_handle* h, double dt)
     const bool plastic = h->plastic.kind != MPM_PLASTICITY_NONE && f.plas[0];
     a.psrc = plastic ? f.plas[c] : nullptr;
     a.pdst = plastic ? f.plas[o] : nullptr;
-    a.prm[0] = (float)h->plastic.theta_c;
-    a.prm[1] = (float)h->plastic.theta_s;
-    a.prm[2] = (float)h->plastic.max_hardening;
-    a.prm[3] = (float)h->plastic.hardening_factor;
+    const mpm_plasticity_desc& pl = h->plastic;
+    a.pkind = pl.kind;
+    a.nplas = pl.kind == MPM_PLASTICITY_CLAMP ? 11 : 13;
+    if(pl.kind == MPM_PLASTICITY_DRUCKER_PRAGER) {
+        a.prm[0] = (float)pl.dp_a0; a.prm[1] = (float)pl.dp_a1; a.prm[2] = (float)pl.dp_a3; a.prm[3] = (float)pl.dp_a4;
+        a.prm[4] = pl.use_vc ? 1.f : 0.f;
+    } else {
+        a.prm[0] = (float)pl.theta_c; a.prm[1] = (float)pl.theta_s; a.prm[2] = (float)pl.max_hardening;
+        a.prm[3] = (float)pl.hardening_factor; a.prm[4] = 0.f;
+    }
     return a;
 }
 
@@ -1450,7 +1514,8 @@ int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, con
     for(int s = 0; s < count; s++) {
         const mpm_scene_desc& d = descs[s];
         if(d.grid.dim != 3 || d.grid.ghost != MPM_GHOST) return set_error(h, MPM_ERR_ARG, "batched scenes are 3D with ghost 3");
-        if(d.model != MPM_COROTATED_FIXED && d.model != MPM_NEO_HOOKEAN) return set_error(h, MPM_ERR_ARG, "model");
+        if(d.model != MPM_COROTATED_FIXED && d.model != MPM_NEO_HOOKEAN && d.model != MPM_STVK_HENCKY)
+            return set_error(h, MPM_ERR_ARG, "model");
         if(d.particle_count < 0) return set_error(h, MPM_ERR_ARG, "particle_count");
         if(d.object_count < 0 || d.object_count > MPM_MAX_OBJECTS || d.first_object < 0 || d.first_object + d.object_count > nobjs)
             return set_error(h, MPM_ERR_ARG, "scene collision-object range");
@@ -1713,9 +1778,34 @@ int fast_plastic_init(mpm_handle* h)
     if(!f.plas[0])
         for(int b = 0; b < 2; b++) MPM_CUDA(h, cudaMalloc(&f.plas[b], NPLAS * f.npad * sizeof(float)));
     if(!f.n) return MPM_OK;
+    const mpm_plasticity_desc& pl = h->plastic;
+    if(pl.kind == MPM_PLASTICITY_DRUCKER_PRAGER) {
+        k_dp_init<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(f.n, f.npad, f.plas[f.cur], (float)pl.cohesion,
+            (float)pl.dp_a0, (float)pl.dp_a1, (float)pl.dp_a3, (float)pl.dp_a4);
+        MPM_LAUNCHED(h, "k_dp_init");
+        return MPM_OK;
+    }
     k_plastic_init<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(f.n, f.npad, f.plas[f.cur], f.attr[f.cur]);
     MPM_LAUNCHED(h, "k_plastic_init");
     return MPM_OK;
+}
+
+// The view's arrays in the order of PlasticArrays: Fp, mu, lambda, then the
+// scalars at plastic components 9.. of the handle's kind.
+static void plastic_view_arrays(const mpm_handle* h, const mpm_plastic_view* v, void* out[7])
+{
+    const bool dp = h->plastic.kind == MPM_PLASTICITY_DRUCKER_PRAGER;
+    void* a[7] = {v->Fp, v->mu, v->lambda, dp ? v->plastic_def : v->mu0, dp ? v->rho_F : v->lambda0,
+                  dp ? v->cohesion : nullptr, dp ? v->vc : nullptr};
+    for(int i = 0; i < 7; i++) out[i] = a[i];
+}
+
+template<class T> static PlasticArrays<T> plastic_arrays(void* const* p)
+{
+    PlasticArrays<T> r;
+    r.Fp = (T*)p[0]; r.mu = (T*)p[1]; r.la = (T*)p[2];
+    for(int k = 0; k < 4; k++) r.sc[k] = (T*)p[3 + k];
+    return r;
 }
 
 int fast_get_plastic(mpm_handle* h, mpm_plastic_view* v)
@@ -1727,30 +1817,27 @@ int fast_get_plastic(mpm_handle* h, mpm_plastic_view* v)
     if(!n) return MPM_OK;
     const bool dev = v->on_device != 0;
     const size_t e = v->dtype == MPM_FP64 ? 8 : 4;
-    void* dst[5] = {v->Fp, v->mu, v->lambda, v->mu0, v->lambda0};
-    const int64_t cnt[5] = {9 * n, n, n, n, n};
-    void* dptr[5] = {};
+    void* dst[7];
+    plastic_view_arrays(h, v, dst);
+    const int64_t cnt[7] = {9 * n, n, n, n, n, n, n};
+    void* dptr[7] = {};
     uint8_t* stage = nullptr;
     if(!dev) {
-        int rc = fast_staging(h, (size_t)n * 13 * e + 256, &stage);
+        int rc = fast_staging(h, (size_t)n * 15 * e + 256, &stage);
         if(rc) return rc;
     }
     size_t off = 0;
-    for(int i = 0; i < 5; i++) {
+    for(int i = 0; i < 7; i++) {
         if(!dst[i]) continue;
         if(dev) dptr[i] = dst[i];
         else { dptr[i] = stage + off; off += cnt[i] * e; }
     }
     const int blocks = grid_stride_blocks(h, n, 256), c = f.cur;
-    if(e == 8)
-        k_plastic_out<double><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], (double*)dptr[0],
-            (double*)dptr[1], (double*)dptr[2], (double*)dptr[3], (double*)dptr[4]);
-    else
-        k_plastic_out<float><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], (float*)dptr[0],
-            (float*)dptr[1], (float*)dptr[2], (float*)dptr[3], (float*)dptr[4]);
+    if(e == 8) k_plastic_out<double><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], plastic_arrays<double>(dptr));
+    else k_plastic_out<float><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], plastic_arrays<float>(dptr));
     MPM_LAUNCHED(h, "k_plastic_out");
     if(!dev)
-        for(int i = 0; i < 5; i++)
+        for(int i = 0; i < 7; i++)
             if(dst[i]) MPM_CUDA(h, cudaMemcpyAsync(dst[i], dptr[i], cnt[i] * e, cudaMemcpyDeviceToHost, h->stream));
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
@@ -1765,16 +1852,17 @@ int fast_set_plastic(mpm_handle* h, const mpm_plastic_view* v)
     if(!n) return MPM_OK;
     const bool dev = v->on_device != 0;
     const size_t e = v->dtype == MPM_FP64 ? 8 : 4;
-    const void* src[5] = {v->Fp, v->mu, v->lambda, v->mu0, v->lambda0};
-    const int64_t cnt[5] = {9 * n, n, n, n, n};
-    const void* dptr[5] = {};
+    void* src[7];
+    plastic_view_arrays(h, v, src);
+    const int64_t cnt[7] = {9 * n, n, n, n, n, n, n};
+    void* dptr[7] = {};
     uint8_t* stage = nullptr;
     if(!dev) {
-        int rc = fast_staging(h, (size_t)n * 13 * e + 256, &stage);
+        int rc = fast_staging(h, (size_t)n * 15 * e + 256, &stage);
         if(rc) return rc;
     }
     size_t off = 0;
-    for(int i = 0; i < 5; i++) {
+    for(int i = 0; i < 7; i++) {
         if(!src[i]) continue;
         if(dev) dptr[i] = src[i];
         else {
@@ -1784,12 +1872,8 @@ int fast_set_plastic(mpm_handle* h, const mpm_plastic_view* v)
         }
     }
     const int blocks = grid_stride_blocks(h, n, 256), c = f.cur;
-    if(e == 8)
-        k_plastic_in<double><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], (const double*)dptr[0],
-            (const double*)dptr[1], (const double*)dptr[2], (const double*)dptr[3], (const double*)dptr[4]);
-    else
-        k_plastic_in<float><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], (const float*)dptr[0],
-            (const float*)dptr[1], (const float*)dptr[2], (const float*)dptr[3], (const float*)dptr[4]);
+    if(e == 8) k_plastic_in<double><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], plastic_arrays<double>(dptr));
+    else k_plastic_in<float><<<blocks, 256, 0, h->stream>>>(n, f.npad, f.plas[c], f.attr[c], f.pid[c], plastic_arrays<float>(dptr));
     MPM_LAUNCHED(h, "k_plastic_in");
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
@@ -1912,25 +1996,25 @@ int fast_forces(mpm_handle* h, double dt, double)
     return MPM_OK;
 }
 
+template<int PK> static void launch_g2p(mpm_handle* h, const FastArgs& a)
+{
+    const FastState& f = h->fast;
+    switch(f.g2p_threads) {
+        case 64: k_g2p<64, PK><<<occupancy_ctas(h, (const void*)k_g2p<64, PK>, 64, f.cta_mult), 64, 0, h->stream>>>(a); break;
+        case 256: k_g2p<256, PK><<<occupancy_ctas(h, (const void*)k_g2p<256, PK>, 256, f.cta_mult), 256, 0, h->stream>>>(a); break;
+        default: k_g2p<128, PK><<<occupancy_ctas(h, (const void*)k_g2p<128, PK>, 128, f.cta_mult), 128, 0, h->stream>>>(a); break;
+    }
+}
+
 int fast_g2p(mpm_handle* h, double dt, double)
 {
     FastState& f = h->fast;
     if(!f.n) return MPM_OK;
     FastArgs a = make_args(h, dt);
     int slot = timer_begin(h, "fast_g2p");
-    if(a.psrc) {
-        switch(f.g2p_threads) {
-            case 64: k_g2p<64, true><<<occupancy_ctas(h, (const void*)k_g2p<64, true>, 64, f.cta_mult), 64, 0, h->stream>>>(a); break;
-            case 256: k_g2p<256, true><<<occupancy_ctas(h, (const void*)k_g2p<256, true>, 256, f.cta_mult), 256, 0, h->stream>>>(a); break;
-            default: k_g2p<128, true><<<occupancy_ctas(h, (const void*)k_g2p<128, true>, 128, f.cta_mult), 128, 0, h->stream>>>(a); break;
-        }
-    } else {
-        switch(f.g2p_threads) {
-            case 64: k_g2p<64, false><<<occupancy_ctas(h, (const void*)k_g2p<64, false>, 64, f.cta_mult), 64, 0, h->stream>>>(a); break;
-            case 256: k_g2p<256, false><<<occupancy_ctas(h, (const void*)k_g2p<256, false>, 256, f.cta_mult), 256, 0, h->stream>>>(a); break;
-            default: k_g2p<128, false><<<occupancy_ctas(h, (const void*)k_g2p<128, false>, 128, f.cta_mult), 128, 0, h->stream>>>(a); break;
-        }
-    }
+    if(!a.psrc) launch_g2p<0>(h, a);
+    else if(a.pkind == MPM_PLASTICITY_CLAMP) launch_g2p<1>(h, a);
+    else launch_g2p<2>(h, a);
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_g2p");
     f.cur = 1 - f.cur;

@@ -27,7 +27,8 @@ struct PlainState {
     void *mass = nullptr, *vol = nullptr, *mu = nullptr, *lam = nullptr, *pft = nullptr;
     uint8_t* valid = nullptr;
     void *gm = nullptr, *gmv = nullptr, *gv0 = nullptr, *gf = nullptr, *gv = nullptr, *gvf = nullptr;
-    void *Fp = nullptr, *mu0 = nullptr, *lam0 = nullptr;   // plastic state (plasticity on)
+    void *Fp = nullptr, *mu0 = nullptr, *lam0 = nullptr;   // plastic state (plasticity on): clamp
+    void *pdef = nullptr, *rhoF = nullptr, *sigY = nullptr, *vc = nullptr;   // Drucker-Prager
 };
 
 // One scene of a batch, as the fast-path kernels see it.
@@ -65,7 +66,8 @@ struct FastState {
     float* soa[2] = {nullptr, nullptr};       // 24 * npad floats: x y z, vx vy vz, F0..8, B0..8
     float4* attr[2] = {nullptr, nullptr};     // mass, volume, mu, lambda
     int* pid[2] = {nullptr, nullptr};         // caller's particle index
-    float* plas[2] = {nullptr, nullptr};      // plasticity on: 11 * npad floats: Fp0..8, mu0, lambda0
+    float* plas[2] = {nullptr, nullptr};      // plasticity on: 13 * npad floats: Fp0..8, then mu0, lambda0
+                                              // (clamp) or plastic_def, rho_F, sigma_Y, vc (Drucker-Prager)
     uint32_t* keys = nullptr;                 // keys of the current buffer's slots
     uint32_t* sorted_keys = nullptr;
     uint32_t* perm = nullptr;                 // sorted position -> slot in the current buffer

@@ -278,6 +278,21 @@ constexpr double kNeoHookeanThreshold = 0.25;
 template<class T, int d> __device__ void phat(int model, const T* s, T mu, T la, T* P)
 {
     T J = d == 2 ? s[0] * s[1] : s[0] * s[1] * s[2];
+    if(model == MPM_STVK_HENCKY) {
+        // ST_VENANT_KIRCHHOFF_HENCKY_STRAIN::P_From_Strain (ST_VENANT_KIRCHHOFF_HENCKY_STRAIN.cpp:67-78):
+        // Phat = (2 mu ln S + lambda tr ln S) S^-1, zero once the last signed singular value is <= 0
+        if(!(s[d - 1] > 0)) {
+#pragma unroll
+            for(int a = 0; a < d; a++) P[a] = 0;
+            return;
+        }
+        T l[3], tr = 0;
+#pragma unroll
+        for(int a = 0; a < d; a++) { l[a] = log(s[a]); tr += l[a]; }
+#pragma unroll
+        for(int a = 0; a < d; a++) P[a] = (2 * mu * l[a] + la * tr) / s[a];
+        return;
+    }
     if(model == MPM_COROTATED_FIXED) {
         T cof[3];
         if(d == 2) { cof[0] = s[1]; cof[1] = s[0]; }
@@ -600,6 +615,172 @@ template<class T, int d> __device__ bool plastic_clamp(T* F, T* Fp, T& mu, T& la
             T s2 = 0;
 #pragma unroll
             for(int k = 0; k < d; k++) s2 += T2[r + d * k] * P[k + d * c];
+            T1[r + d * c] = s2;
+        }
+#pragma unroll
+    for(int k = 0; k < d * d; k++) Fp[k] = T1[k];
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Eigensystem of a symmetric 3x3 matrix in FP32 registers by cyclic Jacobi
+// rotations (Golub & Van Loan, Matrix Computations, 4th ed., 8.5.2: the
+// symmetric Schur rotation): A <- V^T A V becomes diagonal, V accumulates the
+// rotations (columns = eigenvectors), unsorted.  Used for the SVD-free
+// plasticity updates (eigensystem of F^T F) and the Hencky stress (of F F^T).
+// ---------------------------------------------------------------------------
+template<int P, int Q>
+__device__ __forceinline__ void jacobi_rotate(float (&A)[3][3], float (&V)[3][3])
+{
+    constexpr int R = 3 - P - Q;
+    const float apq = A[P][Q];
+    const float d = A[Q][Q] - A[P][P];
+    // t = tan of the rotation angle: an approximate t still gives an exact
+    // rotation (c and s come from t) and only leaves a residual that the next
+    // sweep removes; c to full precision keeps V orthogonal
+    const float h = d * d + 4.f * apq * apq;
+    const float den = fabsf(d) + h * rsqrtf(h);
+    float t = h > 0.f ? __fdividef(2.f * apq, den) : 0.f;
+    if(d < 0.f) t = -t;
+    const float x = 1.f + t * t;
+    float c = rsqrtf(x);
+    c = c * (1.5f - 0.5f * x * c * c);   // one Newton step
+    const float s = t * c;
+    A[P][P] -= t * apq;
+    A[Q][Q] += t * apq;
+    A[P][Q] = A[Q][P] = 0.f;
+    const float arp = A[R][P], arq = A[R][Q];
+    A[R][P] = A[P][R] = c * arp - s * arq;
+    A[R][Q] = A[Q][R] = s * arp + c * arq;
+#pragma unroll
+    for(int k = 0; k < 3; k++) {
+        const float vp = V[k][P], vq = V[k][Q];
+        V[k][P] = c * vp - s * vq;
+        V[k][Q] = s * vp + c * vq;
+    }
+}
+
+
+__device__ __forceinline__ void sym_eig3f(float (&A)[3][3], float (&V)[3][3])
+{
+#pragma unroll
+    for(int i = 0; i < 3; i++)
+#pragma unroll
+        for(int k = 0; k < 3; k++) V[i][k] = i == k ? 1.f : 0.f;
+    // three sweeps reach FP32 accuracy for eigenvalue ratios up to 100; a
+    // fourth runs where the off-diagonal part is not yet at rounding level
+#pragma unroll
+    for(int sweep = 0; sweep < 3; sweep++) {
+        jacobi_rotate<0, 1>(A, V);
+        jacobi_rotate<0, 2>(A, V);
+        jacobi_rotate<1, 2>(A, V);
+    }
+    const float off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+    const float dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+    if(off > 1e-14f * dia) {
+        jacobi_rotate<0, 1>(A, V);
+        jacobi_rotate<0, 2>(A, V);
+        jacobi_rotate<1, 2>(A, V);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// MPM_DRUCKER_PRAGER (Hybrid_Methods/Forces/MPM_DRUCKER_PRAGER.cpp).
+// prm = a0, a1, a3, a4, use_vc.  Per particle: q = plastic_def, rho_F,
+// sigma_Y (cohesion), vc.
+// ---------------------------------------------------------------------------
+// Update_Hardening (l.118-125): q += inc; phi = pi/180 (a0 + (a1 q - a4) exp(-a3 q));
+// rho_F = sqrt(2/3) 2 sin(phi) / (3 - sin(phi)).
+template<class T> __device__ __forceinline__ void dp_hardening(T& q, T& rho_F, T inc, const T* prm)
+{
+    q += inc;
+    const T phi = (T)(3.14159265358979323846 / 180) * (prm[0] + (prm[1] * q - prm[3]) * exp(-prm[2] * q));
+    const T sp = sin(phi);
+    rho_F = (T)0.81649658092772603 * 2 * sp / (3 - sp);   // sqrt(2/3)
+}
+
+// Compute with store_hardening (l.62-89) on the singular values S (the last
+// may be negative): writes the projected strain and returns true, or returns
+// false where the trial state is elastic (dg <= 0: no change at all).
+template<class T, int d> __device__ bool dp_strain(const T* S, T mu, T la, T& q, T& rho_F, T sigma_Y, T& vc,
+    const T* prm, T* strain)
+{
+    const T g = 1 / (d * la + 2 * mu), b = 1 / (2 * mu);
+    const T beta = -sigma_Y * g / (rho_F * d);
+    T lf[3], st[3], k = 0, lsum = 0, lmag = 0;
+#pragma unroll
+    for(int a = 0; a < d; a++) {
+        lf[a] = log(fabs(S[a]));
+        st[a] = lf[a] + beta + vc / d;
+        k += st[a];
+        lsum += lf[a];
+        lmag += lf[a] * lf[a];
+    }
+    T sh[3], qq = 0;
+#pragma unroll
+    for(int a = 0; a < d; a++) { sh[a] = st[a] - k / d; qq += sh[a] * sh[a]; }
+    qq = sqrt(qq);
+    const T r = rho_F * k / g, dg = qq + b * r;
+    if(!(dg > 0)) return false;
+    if(qq == 0 || k > 0) {
+        const T e = sigma_Y != 0 ? exp(-beta) : (T)1;
+#pragma unroll
+        for(int a = 0; a < d; a++) strain[a] = e;
+        if(prm[4] != 0) vc += lsum + beta * d;
+        dp_hardening(q, rho_F, sqrt(lmag), prm);
+        return true;
+    }
+    const T pp = r * b / qq;
+#pragma unroll
+    for(int a = 0; a < d; a++) strain[a] = exp(k / d - pp * sh[a] - beta);
+    vc = 0;
+    dp_hardening(q, rho_F, dg, prm);
+    return true;
+}
+
+// MPM_PLASTICITY_MODEL::Update_Particles (MPM_PLASTICITY_MODEL.cpp:35-49) with
+// Drucker-Prager on the signed SVD: F = U strain V^T, Fp = V strain^-1 U^T Fe Fp.
+// `st` = q, rho_F, sigma_Y, vc.  Returns whether F and Fp changed.
+template<class T, int d> __device__ bool plastic_dp(T* F, T* Fp, T mu, T la, T* st, const T* prm, bool& ok)
+{
+    T U[9], S[3], V[9], strain[3];
+    ok = true;
+    if(d == 3) ok = svd3<T>(F, U, S, V);
+    else svd2<T>(F, U, S, V);
+    if(!ok) return false;
+    if(!dp_strain<T, d>(S, mu, la, st[0], st[1], st[2], st[3], prm, strain)) return false;
+    T Fe[9], T1[9], T2[9];
+#pragma unroll
+    for(int k = 0; k < d * d; k++) Fe[k] = F[k];
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T f = 0, t = 0;
+#pragma unroll
+            for(int k = 0; k < d; k++) {
+                f += U[r + d * k] * strain[k] * V[c + d * k];
+                t += V[r + d * k] / strain[k] * U[c + d * k];
+            }
+            F[r + d * c] = f;
+            T1[r + d * c] = t;
+        }
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T s2 = 0;
+#pragma unroll
+            for(int k = 0; k < d; k++) s2 += T1[r + d * k] * Fe[k + d * c];
+            T2[r + d * c] = s2;
+        }
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T s2 = 0;
+#pragma unroll
+            for(int k = 0; k < d; k++) s2 += T2[r + d * k] * Fp[k + d * c];
             T1[r + d * c] = s2;
         }
 #pragma unroll

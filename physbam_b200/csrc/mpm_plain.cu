@@ -17,6 +17,7 @@ namespace {
 using namespace mpm;
 
 template<class T> struct Vec4 { T v[4]; };
+template<class T> struct Vec5 { T v[5]; };
 
 template<class T> struct PlainArgs {
     SceneParams sp;
@@ -386,6 +387,44 @@ template<class T, int d> __global__ void k_plastic_clamp(PlainArgs<T> a, T* Fp, 
     }
 }
 
+// MPM_DRUCKER_PRAGER after G2P over the particles simulated in the substep.
+template<class T, int d> __global__ void k_plastic_dp(PlainArgs<T> a, T* Fp, T* q, T* rhoF, T* sigY, T* vc, Vec5<T> prm)
+{
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+        if(!a.valid[p]) continue;
+        if(a.valid[p] == 2) a.valid[p] = 0;
+        T F[d * d], P[d * d], st[4] = {q[p], rhoF[p], sigY[p], vc[p]};
+#pragma unroll
+        for(int k = 0; k < d * d; k++) { F[k] = a.F[p * d * d + k]; P[k] = Fp[p * d * d + k]; }
+        bool ok;
+        const bool changed = plastic_dp<T, d>(F, P, a.mu[p], a.lam[p], st, prm.v, ok);
+        if(changed) {
+#pragma unroll
+            for(int k = 0; k < d * d; k++) { a.F[p * d * d + k] = F[k]; Fp[p * d * d + k] = P[k]; }
+        }
+        q[p] = st[0]; rhoF[p] = st[1]; vc[p] = st[3];
+        if(!ok) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
+    }
+}
+
+// Drucker-Prager start (MPM_DRUCKER_PRAGER::Initialize_Particles): Fp = I,
+// plastic_def = vc = 0, sigma_Y = cohesion, rho_F at zero plastic deformation.
+template<class T, int d> __global__ void k_dp_init(int64_t n, T* Fp, T* q, T* rhoF, T* sigY, T* vc, T cohesion, Vec5<T> prm)
+{
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for(int k = 0; k < d * d; k++) Fp[p * d * d + k] = k % (d + 1) == 0 ? (T)1 : (T)0;
+        T qq = 0, r = 0;
+        dp_hardening<T>(qq, r, (T)0, prm.v);
+        q[p] = qq; rhoF[p] = r; sigY[p] = cohesion; vc[p] = 0;
+    }
+}
+
+template<class T> Vec5<T> dp_params(const mpm_plasticity_desc& pl)
+{
+    return {{(T)pl.dp_a0, (T)pl.dp_a1, (T)pl.dp_a3, (T)pl.dp_a4, (T)(pl.use_vc ? 1 : 0)}};
+}
+
 // Unplastic start: Fp = I, mu0 = mu, lambda0 = lambda.
 template<class T, int d> __global__ void k_plastic_init(int64_t n, T* Fp, T* mu0, T* lam0, const T* mu, const T* lam)
 {
@@ -415,6 +454,16 @@ template<class T> int g2p_t(mpm_handle* h, double dt)
         else k_plastic_clamp<T, 2><<<pblocks(a.n, t), t, 0, h->stream>>>(a, (T*)s.Fp, (const T*)s.mu0, (const T*)s.lam0, prm);
         timer_end(h, slot);
         MPM_LAUNCHED(h, "k_plastic_clamp");
+    } else if(h->plastic.kind == MPM_PLASTICITY_DRUCKER_PRAGER) {
+        PlainState& s = h->plain;
+        const Vec5<T> prm = dp_params<T>(h->plastic);
+        slot = timer_begin(h, "plain_plasticity");
+        if(h->sp.dim == 3)
+            k_plastic_dp<T, 3><<<pblocks(a.n, t), t, 0, h->stream>>>(a, (T*)s.Fp, (T*)s.pdef, (T*)s.rhoF, (T*)s.sigY, (T*)s.vc, prm);
+        else
+            k_plastic_dp<T, 2><<<pblocks(a.n, t), t, 0, h->stream>>>(a, (T*)s.Fp, (T*)s.pdef, (T*)s.rhoF, (T*)s.sigY, (T*)s.vc, prm);
+        timer_end(h, slot);
+        MPM_LAUNCHED(h, "k_plastic_dp");
     }
     return MPM_OK;
 }
@@ -442,7 +491,8 @@ int plain_alloc(mpm_handle* h, int64_t n)
         for(void** p: g) MPM_CUDA(h, cudaMemsetAsync(*p, 0, (p == &s.gm ? gn : gn * d) * e, h->stream));
     }
     if(s.n != n) {
-        void** pa[] = {&s.X, &s.V, &s.F, &s.B, &s.mass, &s.vol, &s.mu, &s.lam, &s.pft, &s.Fp, &s.mu0, &s.lam0};
+        void** pa[] = {&s.X, &s.V, &s.F, &s.B, &s.mass, &s.vol, &s.mu, &s.lam, &s.pft, &s.Fp, &s.mu0, &s.lam0,
+                       &s.pdef, &s.rhoF, &s.sigY, &s.vc};
         for(void** p: pa) { cudaFree(*p); *p = nullptr; }
         cudaFree(s.valid); s.valid = nullptr;
         int64_t m = n ? n : 1;
@@ -465,7 +515,7 @@ void plain_free(mpm_handle* h)
 {
     PlainState& s = h->plain;
     void* ps[] = {s.X, s.V, s.F, s.B, s.mass, s.vol, s.mu, s.lam, s.pft, s.valid, s.gm, s.gmv, s.gv0, s.gf, s.gv, s.gvf,
-                  s.Fp, s.mu0, s.lam0};
+                  s.Fp, s.mu0, s.lam0, s.pdef, s.rhoF, s.sigY, s.vc};
     for(void* p: ps) cudaFree(p);
     s = PlainState();
 }
@@ -555,11 +605,25 @@ int plain_plastic_init(mpm_handle* h)
     const int64_t m = s.n ? s.n : 1;
     if(!s.Fp) {
         MPM_CUDA(h, cudaMalloc(&s.Fp, m * d * d * e));
-        MPM_CUDA(h, cudaMalloc(&s.mu0, m * e));
-        MPM_CUDA(h, cudaMalloc(&s.lam0, m * e));
+        void** pa[] = {&s.mu0, &s.lam0, &s.pdef, &s.rhoF, &s.sigY, &s.vc};
+        for(void** p: pa) MPM_CUDA(h, cudaMalloc(p, m * e));
     }
     if(!s.n) return MPM_OK;
     const int b = gblocks(h, s.n, 256);
+    if(h->plastic.kind == MPM_PLASTICITY_DRUCKER_PRAGER) {
+        const double c = h->plastic.cohesion;
+        if(e == 8) {
+            const Vec5<double> prm = dp_params<double>(h->plastic);
+            if(d == 3) k_dp_init<double, 3><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.pdef, (double*)s.rhoF, (double*)s.sigY, (double*)s.vc, c, prm);
+            else k_dp_init<double, 2><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.pdef, (double*)s.rhoF, (double*)s.sigY, (double*)s.vc, c, prm);
+        } else {
+            const Vec5<float> prm = dp_params<float>(h->plastic);
+            if(d == 3) k_dp_init<float, 3><<<b, 256, 0, h->stream>>>(s.n, (float*)s.Fp, (float*)s.pdef, (float*)s.rhoF, (float*)s.sigY, (float*)s.vc, (float)c, prm);
+            else k_dp_init<float, 2><<<b, 256, 0, h->stream>>>(s.n, (float*)s.Fp, (float*)s.pdef, (float*)s.rhoF, (float*)s.sigY, (float*)s.vc, (float)c, prm);
+        }
+        MPM_LAUNCHED(h, "k_dp_init");
+        return MPM_OK;
+    }
     if(e == 8) {
         if(d == 3) k_plastic_init<double, 3><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.mu0, (double*)s.lam0, (const double*)s.mu, (const double*)s.lam);
         else k_plastic_init<double, 2><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.mu0, (double*)s.lam0, (const double*)s.mu, (const double*)s.lam);
@@ -585,6 +649,10 @@ int plain_get_plastic(mpm_handle* h, mpm_plastic_view* v)
     if(v->lambda && (rc = copy_out(h, v->lambda, s.lam, n, v->dtype, dev))) return rc;
     if(v->mu0 && (rc = copy_out(h, v->mu0, s.mu0, n, v->dtype, dev))) return rc;
     if(v->lambda0 && (rc = copy_out(h, v->lambda0, s.lam0, n, v->dtype, dev))) return rc;
+    if(v->plastic_def && (rc = copy_out(h, v->plastic_def, s.pdef, n, v->dtype, dev))) return rc;
+    if(v->rho_F && (rc = copy_out(h, v->rho_F, s.rhoF, n, v->dtype, dev))) return rc;
+    if(v->cohesion && (rc = copy_out(h, v->cohesion, s.sigY, n, v->dtype, dev))) return rc;
+    if(v->vc && (rc = copy_out(h, v->vc, s.vc, n, v->dtype, dev))) return rc;
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
 }
@@ -603,6 +671,10 @@ int plain_set_plastic(mpm_handle* h, const mpm_plastic_view* v)
     if(v->lambda && (rc = copy_in(h, s.lam, v->lambda, n, v->dtype, dev))) return rc;
     if(v->mu0 && (rc = copy_in(h, s.mu0, v->mu0, n, v->dtype, dev))) return rc;
     if(v->lambda0 && (rc = copy_in(h, s.lam0, v->lambda0, n, v->dtype, dev))) return rc;
+    if(v->plastic_def && (rc = copy_in(h, s.pdef, v->plastic_def, n, v->dtype, dev))) return rc;
+    if(v->rho_F && (rc = copy_in(h, s.rhoF, v->rho_F, n, v->dtype, dev))) return rc;
+    if(v->cohesion && (rc = copy_in(h, s.sigY, v->cohesion, n, v->dtype, dev))) return rc;
+    if(v->vc && (rc = copy_in(h, s.vc, v->vc, n, v->dtype, dev))) return rc;
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
 }

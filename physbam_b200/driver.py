@@ -71,13 +71,21 @@ class ParticlesView(ctypes.Structure):
 
 class PlasticityDesc(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("theta_c", ctypes.c_double), ("theta_s", ctypes.c_double),
-                ("max_hardening", ctypes.c_double), ("hardening_factor", ctypes.c_double)]
+                ("max_hardening", ctypes.c_double), ("hardening_factor", ctypes.c_double),
+                ("dp_a0", ctypes.c_double), ("dp_a1", ctypes.c_double), ("dp_a3", ctypes.c_double),
+                ("dp_a4", ctypes.c_double), ("cohesion", ctypes.c_double), ("use_vc", ctypes.c_int)]
 
 
 class PlasticView(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("dtype", ctypes.c_int), ("on_device", ctypes.c_int),
                 ("Fp", ctypes.c_void_p), ("mu", ctypes.c_void_p), ("lambda_", ctypes.c_void_p),
-                ("mu0", ctypes.c_void_p), ("lambda0", ctypes.c_void_p)]
+                ("mu0", ctypes.c_void_p), ("lambda0", ctypes.c_void_p), ("plastic_def", ctypes.c_void_p),
+                ("rho_F", ctypes.c_void_p), ("cohesion", ctypes.c_void_p), ("vc", ctypes.c_void_p)]
+
+
+# plastic-state keys (scenes.plastic_keys and the mu/lam pair) -> PlasticView fields
+_PLASTIC_FIELDS = {"Fp": "Fp", "mu": "mu", "lam": "lambda_", "mu0": "mu0", "lam0": "lambda0",
+                   "pdef": "plastic_def", "rho_F": "rho_F", "cohesion": "cohesion", "vc": "vc"}
 
 
 EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_objects", "mpm_set_particles",
@@ -319,38 +327,64 @@ class MPM_DRIVER:
         return X, V, Fc, Bc, valid
 
     # -- plasticity (MPM_PLASTICITY_CLAMP) -------------------------------------
-    def set_plasticity(self, plasticity: Optional[S.Plasticity]):
-        """Snow clamp after every G2P (None: off).  Particles start unplastic."""
+    def set_plasticity(self, plasticity):
+        """Plasticity after every G2P: a `scenes.Plasticity` (snow clamp), a
+        `scenes.DruckerPrager` (sand) or None (off).  Particles start unplastic."""
         d = PlasticityDesc()
         if plasticity is not None:
-            d.kind, d.theta_c, d.theta_s = plasticity.kind, plasticity.theta_c, plasticity.theta_s
-            d.max_hardening, d.hardening_factor = plasticity.max_hardening, plasticity.hardening_factor
+            d.kind = plasticity.kind
+            if isinstance(plasticity, S.Plasticity):
+                d.theta_c, d.theta_s = plasticity.theta_c, plasticity.theta_s
+                d.max_hardening, d.hardening_factor = plasticity.max_hardening, plasticity.hardening_factor
+            else:
+                d.dp_a0, d.dp_a1, d.dp_a3, d.dp_a4 = plasticity.a0, plasticity.a1, plasticity.a3, plasticity.a4
+                d.cohesion, d.use_vc = plasticity.cohesion, 1 if plasticity.use_vc else 0
         self._check(self.L.mpm_set_plasticity(self.h, ctypes.byref(d)), "mpm_set_plasticity")
+        self.plasticity = plasticity
+
+    def _plastic_keys(self):
+        pl = getattr(self, "plasticity", None)
+        if pl is None:
+            return ("Fp", "mu", "lam")   # the library reports "plasticity is off"
+        if pl.kind == S.PLASTICITY_CLAMP:
+            return ("Fp", "mu", "lam", "mu0", "lam0")
+        return ("Fp", "mu", "lam") + S.plastic_keys(pl)[1:]
 
     def get_plastic_state(self, dtype=np.float64):
-        """{"Fp": (n,d,d), "mu", "lam", "mu0", "lam0": (n,)} in the caller's particle order."""
+        """The plastic state in the caller's particle order: "Fp" (n,d,d), the current
+        "mu", "lam", and per kind "mu0", "lam0" (clamp) or "pdef", "rho_F",
+        "cohesion", "vc" (Drucker-Prager), each (n,)."""
         d, n = self.dim, self.n
-        Fp = np.empty((n, d * d), dtype)
-        arrs = [np.empty(n, dtype) for _ in range(4)]
         v = PlasticView()
         v.n, v.dtype, v.on_device = n, FP64 if dtype == np.float64 else FP32, 0
-        v.Fp = Fp.ctypes.data
-        v.mu, v.lambda_, v.mu0, v.lambda0 = [a.ctypes.data for a in arrs]
+        out = {}
+        for k in self._plastic_keys():
+            out[k] = np.empty((n, d * d) if k == "Fp" else n, dtype)
+            setattr(v, _PLASTIC_FIELDS[k], out[k].ctypes.data)
         self._check(self.L.mpm_get_plastic_state(self.h, ctypes.byref(v)), "mpm_get_plastic_state")
-        return {"Fp": np.swapaxes(Fp.reshape(n, d, d), 1, 2), "mu": arrs[0], "lam": arrs[1], "mu0": arrs[2],
-                "lam0": arrs[3]}
+        out["Fp"] = np.swapaxes(out["Fp"].reshape(n, d, d), 1, 2)
+        return out
 
-    def set_plastic_state(self, Fp=None, mu=None, lam=None, mu0=None, lam0=None, dtype=np.float64):
-        """Overwrite any subset of the plastic state (Fp as (n,d,d) matrices)."""
+    def set_plastic_state(self, dtype=np.float64, **arrays):
+        """Overwrite any subset of the plastic state, by the keys of get_plastic_state
+        (Fp as (n,d,d) matrices)."""
         d, n = self.dim, self.n
-        keep = [None if Fp is None else np.ascontiguousarray(np.swapaxes(np.asarray(Fp), 1, 2).reshape(n, d * d), dtype)]
-        keep += [None if a is None else np.ascontiguousarray(a, dtype) for a in (mu, lam, mu0, lam0)]
-        for k in keep:
-            if k is not None and k.shape[0] != n:
-                raise ValueError("set_plastic_state: arrays of n = %d particles" % n)
         v = PlasticView()
         v.n, v.dtype, v.on_device = n, FP64 if dtype == np.float64 else FP32, 0
-        v.Fp, v.mu, v.lambda_, v.mu0, v.lambda0 = [None if k is None else k.ctypes.data for k in keep]
+        keep = []
+        for k, a in arrays.items():
+            if a is None:
+                continue
+            if k not in _PLASTIC_FIELDS:
+                raise ValueError("set_plastic_state: unknown array %r" % k)
+            a = np.asarray(a)
+            if k == "Fp":
+                a = np.swapaxes(a, 1, 2).reshape(n, d * d)
+            a = np.ascontiguousarray(a, dtype)
+            if a.shape[0] != n:
+                raise ValueError("set_plastic_state: arrays of n = %d particles" % n)
+            keep.append(a)
+            setattr(v, _PLASTIC_FIELDS[k], a.ctypes.data)
         self._check(self.L.mpm_set_plastic_state(self.h, ctypes.byref(v)), "mpm_set_plastic_state")
 
     # -- differentiation -------------------------------------------------------

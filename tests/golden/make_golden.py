@@ -32,6 +32,7 @@ CASES = {
     # snow: MPM_PLASTICITY_CLAMP after every G2P (Fp, hardened mu and lambda dumped too)
     "smallsnow3d_corotated": (lambda: S.small_snow_3d(), [0, 19], [0, 19]),
     "smallsnow2d_corotated": (lambda: S.small_snow_2d(), [0, 19], [19]),
+    "small3d_hencky": (lambda: S.small_3d(model=S.HENCKY, seed=13, E=(1e5, 3e5)), [0, 19], [0]),
     # sand: ST_VENANT_KIRCHHOFF_HENCKY_STRAIN + MPM_DRUCKER_PRAGER (Fp, plastic_def, rho_F, sigma_Y, vc dumped)
     "smallsand3d_hencky": (lambda: S.small_sand_3d(), [0, 1, 19], [0, 19]),
     "smallsand2d_hencky": (lambda: S.small_sand_2d(), [0, 19], [19]),

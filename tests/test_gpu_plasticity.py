@@ -1,8 +1,10 @@
-"""GPU tests of snow plasticity (MPM_PLASTICITY_CLAMP after every G2P).
+"""GPU tests of plasticity after every G2P: snow (MPM_PLASTICITY_CLAMP) and
+sand (MPM_DRUCKER_PRAGER with the St. Venant-Kirchhoff Hencky model).
 
-* FP64 plain path vs the reference's own FP64 dumps of the snow scenes (2D and
-  3D): F, Fp and the hardened mu, lambda as well as X, V, B.
-* FP32 fast path (clamp fused into G2P) vs the same dumps at FP32 tolerances.
+* FP64 plain path vs the reference's own FP64 dumps of the snow and sand
+  scenes (2D and 3D): F, Fp and the hardened mu, lambda (snow) or
+  plastic_def, rho_F, sigma_Y, vc (sand) as well as X, V, B.
+* FP32 fast path (plasticity fused into G2P) vs the same dumps at FP32 tolerances.
 * A particle that leaves the domain in a substep is still updated by that
   substep's plasticity (MPM_DRIVER updates every simulated particle).
 * The plastic state round-trips through the C ABI in the caller's order.
@@ -19,6 +21,7 @@ from physbam_b200 import scenes as S
 pytestmark = pytest.mark.gpu
 
 SNOW = sorted(n for n in CASES if n.startswith("smallsnow"))
+SAND = sorted(n for n in CASES if n.startswith("smallsand"))
 
 
 def D():
@@ -33,13 +36,17 @@ def rel(a, b, floor=1e-300):
 
 def floors(scene, ref):
     vmax = max(float(np.max(np.abs(ref["V"]))), 1e-12)
-    return {"X": 1.0, "V": vmax, "F": 1.0, "B": vmax / scene.dx, "Fp": 1.0, "mu": 1e-300, "lam": 1e-300}
+    return {"X": 1.0, "V": vmax, "F": 1.0, "B": vmax / scene.dx, "Fp": 1.0, "mu": 1e-300, "lam": 1e-300,
+            "pdef": 1e-300, "rho_F": 1e-300, "cohesion": 1.0, "vc": 1e-300}
 
 
-TOL_FP64 = {"X": 1e-12, "V": 1e-9, "F": 1e-10, "B": 1e-8, "Fp": 1e-10, "mu": 1e-10, "lam": 1e-10}
+TOL_FP64 = {"X": 1e-12, "V": 1e-9, "F": 1e-10, "B": 1e-8, "Fp": 1e-10, "mu": 1e-10, "lam": 1e-10,
+            "pdef": 1e-10, "rho_F": 1e-10, "cohesion": 1e-12, "vc": 1e-10}
 # FP32 after 20 substeps; the hardening exp(10 (1 - det Fp)) turns an FP32
-# error of det Fp into ten times that in mu and lambda.
-TOL_FP32 = {"X": 2e-6, "V": 2e-3, "F": 1e-4, "B": 2e-3, "Fp": 1e-4, "mu": 1e-3, "lam": 1e-3}
+# error of det Fp into ten times that in mu and lambda; the Drucker-Prager
+# state is a sum of FP32 logarithms of the singular values.
+TOL_FP32 = {"X": 2e-6, "V": 2e-3, "F": 1e-4, "B": 2e-3, "Fp": 1e-4, "mu": 1e-3, "lam": 1e-3,
+            "pdef": 1e-4, "rho_F": 1e-5, "cohesion": 1e-6, "vc": 1e-4}
 
 
 def run_snow(name, precision, path, tol, shape=None):
@@ -59,7 +66,7 @@ def run_snow(name, precision, path, tol, shape=None):
         got.update(drv.get_plastic_state())
         np.testing.assert_array_equal(got["valid"], ref["valid"])
         fl = floors(scene, ref)
-        for k in ("X", "V", "F", "B", "Fp", "mu", "lam"):
+        for k in ("X", "V", "F", "B") + S.plastic_keys(scene.plasticity):
             e = rel(got[k], ref[k], fl[k])
             worst[k] = max(worst.get(k, 0), e)
             assert e < tol[k], (name, step, k, e)
@@ -68,8 +75,8 @@ def run_snow(name, precision, path, tol, shape=None):
     return worst
 
 
-@pytest.mark.parametrize("name", SNOW)
-def test_plain_fp64_snow_matches_reference(cuda_device, name):
+@pytest.mark.parametrize("name", SNOW + SAND)
+def test_plain_fp64_plastic_matches_reference(cuda_device, name):
     run_snow(name, D().FP64, D().PATH_PLAIN, TOL_FP64)
 
 
@@ -77,9 +84,54 @@ SHAPES = [(0, 128, 1), (2, 64, 2), (3, 256, 1)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "p2g%d-g2p%d-x%d" % s)
-@pytest.mark.parametrize("name", [n for n in SNOW if "3d" in n])
-def test_fast_fp32_snow_matches_reference(cuda_device, name, shape):
+@pytest.mark.parametrize("name", [n for n in SNOW + SAND if "3d" in n])
+def test_fast_fp32_plastic_matches_reference(cuda_device, name, shape):
     run_snow(name, D().FP32, D().PATH_FAST, TOL_FP32, shape)
+
+
+@pytest.mark.parametrize("path", ["plain", "fast"])
+def test_drucker_prager_state_round_trip(cuda_device, path):
+    s = S.small_sand_3d(nsteps=3)
+    p, prec = (D().PATH_PLAIN, D().FP64) if path == "plain" else (D().PATH_FAST, D().FP32)
+    drv = D().MPM_DRIVER(s, precision=prec, path=p)
+    drv.set_scene_particles(s)
+    st = drv.get_plastic_state()
+    ref = oracle.State(s)
+    for k in ("pdef", "rho_F", "cohesion", "vc"):
+        np.testing.assert_allclose(st[k], getattr(ref, k), rtol=1e-6, atol=1e-30)
+    drv.advance(3)
+    before = drv.get_plastic_state()
+    rng = np.random.default_rng(2)
+    new = {"pdef": rng.uniform(0, 0.1, s.n), "vc": rng.uniform(-0.01, 0.01, s.n),
+           "cohesion": rng.uniform(0, 50, s.n), "Fp": np.eye(3) + 0.01 * rng.standard_normal((s.n, 3, 3))}
+    drv.set_plastic_state(**new)
+    back = drv.get_plastic_state()
+    r = 1e-15 if path == "plain" else 1e-7
+    for k, v in new.items():
+        np.testing.assert_allclose(back[k], v, rtol=r, atol=r * 1e-3)
+    np.testing.assert_array_equal(back["rho_F"], before["rho_F"])     # not set: unchanged
+    with pytest.raises(D().MPMError):          # the clamp's arrays on a Drucker-Prager handle
+        drv.set_plastic_state(mu0=np.ones(s.n))
+    drv.close()
+
+
+def test_drucker_prager_fast_vs_plain_after_collision(cuda_device):
+    """30 substeps of the sand block against the floor: the FP32 fast path (SVD-free
+    return mapping in G2P) follows the FP64 plain path (the reference's SVD route)."""
+    s = S.small_sand_3d(nsteps=30)
+    out = {}
+    for p, prec in ((D().PATH_PLAIN, D().FP64), (D().PATH_FAST, D().FP32)):
+        drv = D().MPM_DRIVER(s, precision=prec, path=p)
+        drv.set_scene_particles(s)
+        drv.advance(s.nsteps)
+        out[p] = (drv.get_particles(), drv.get_plastic_state())
+        drv.close()
+    (a, pa), (b, pb) = out[D().PATH_PLAIN], out[D().PATH_FAST]
+    np.testing.assert_array_equal(a["valid"], b["valid"])
+    assert rel(b["X"], a["X"], 1.0) < 2e-6
+    assert rel(b["F"], a["F"], 1.0) < 1e-4
+    assert rel(pb["pdef"], pa["pdef"]) < 1e-4
+    assert (pa["pdef"] > 0).mean() > 0.5
 
 
 def test_leaving_particle_gets_its_last_plastic_update(cuda_device):
@@ -243,7 +295,8 @@ def test_batch_with_plasticity_matches_individual(cuda_device):
 def test_bad_plasticity_arguments(cuda_device):
     s = S.small_snow_3d(nsteps=1)
     drv = D().MPM_DRIVER(s)
-    for bad in (S.Plasticity(theta_c=1.5), S.Plasticity(theta_s=-1.0), S.Plasticity(kind=7)):
+    for bad in (S.Plasticity(theta_c=1.5), S.Plasticity(theta_s=-1.0), S.Plasticity(kind=7),
+                S.DruckerPrager(a0=10.0, a4=10.0), S.DruckerPrager(cohesion=float("nan"))):
         with pytest.raises(D().MPMError):
             drv.set_plasticity(bad)
     drv.set_plasticity(None)
