@@ -228,6 +228,33 @@ typedef struct {
 int mpm_get_plastic_state(mpm_handle* h, mpm_plastic_view* view);
 int mpm_set_plastic_state(mpm_handle* h, const mpm_plastic_view* view);
 
+/* Backward-Euler force solve instead of symplectic Euler: the reference's
+ * default Apply_Forces (MPM_DRIVER.cpp:1024-1048), Newton's method on
+ * MPM_OBJECTIVE with conjugate gradients and a strong-Wolfe line search, stopping
+ * once the mass-weighted gradient norm is below newton_tolerance * dt; the CG
+ * tolerance is relative, min(.5, solver_tolerance sqrt(max(residual,
+ * tolerance))).  Defaults as MPM_EXAMPLE.h:119-122: 1, 100, .5, 1000.
+ * Plain path only (FP64 or FP32, 2D or 3D); substeps then run eagerly, not
+ * from CUDA graphs, since the host steers the iteration. */
+typedef struct {
+    int enabled;
+    double newton_tolerance;
+    int newton_iterations;
+    double solver_tolerance;
+    int solver_iterations;
+} mpm_implicit_desc;
+int mpm_set_implicit(mpm_handle* h, const mpm_implicit_desc* d);
+
+/* Iterations of the last implicit solve (NEWTONS_METHOD::iterations_used and
+ * the CG iterations summed over it) and its last gradient norm. */
+typedef struct {
+    int newton_iterations;
+    int krylov_iterations;
+    int converged;
+    double residual;
+} mpm_implicit_stats;
+int mpm_get_implicit_stats(mpm_handle* h, mpm_implicit_stats* s);
+
 /* ---- inspection ---------------------------------------------------------- */
 
 /* Grids of the last substep as doubles on the host, each (G+6)^d nodes (times

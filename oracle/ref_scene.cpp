@@ -13,7 +13,8 @@
 // arrays (STANDARD_TESTS_BASE.cpp:372-404), MPM_PLASTICITY_CLAMP or
 // MPM_DRUCKER_PRAGER after G2P (l.409-486),
 // MPM_GRAVITY (l.354-358), collision objects through Add_Collision_Object,
-// symplectic Euler, APIC (use_affine), flip=0, fixed dt.
+// symplectic Euler or (scene flag) the backward-Euler Newton solve, APIC
+// (use_affine), flip=0, fixed dt.
 #include <Core/Log/LOG.h>
 #include <Core/Math_Tools/RANGE.h>
 #include <Core/Matrices/MATRIX.h>
@@ -47,7 +48,8 @@ namespace {
 struct OBJ { int kind, type; double friction, a[3], b[3]; };
 struct SCENE_FILE
 {
-    int dim, counts[3], model, nsteps, nobj, ndump, plasticity;
+    int dim, counts[3], model, nsteps, nobj, ndump, plasticity, implicit;
+    double implicit_prm[4];   // newton_tolerance, newton_iterations, solver_tolerance, solver_iterations
     // clamp (1): theta_c, theta_s, max_hardening, hardening_factor;
     // Drucker-Prager (2): a0, a1, a3, a4, sigma_Y0, use_vc
     double plastic[6];
@@ -69,10 +71,11 @@ SCENE_FILE Read_Scene(const char* path)
     if(!f) throw std::runtime_error("cannot open scene");
     char magic[8];
     rd(f, magic, 8);
-    if(memcmp(magic, "MPMSCN01", 8)) throw std::runtime_error("bad scene magic");
+    if(memcmp(magic, "MPMSCN02", 8)) throw std::runtime_error("bad scene magic");
     SCENE_FILE s;
-    int hdr[9];
-    rd(f, hdr, 9);
+    int hdr[10];
+    rd(f, hdr, 10);
+    s.implicit = hdr[9];
     s.dim = hdr[0]; s.counts[0] = hdr[1]; s.counts[1] = hdr[2]; s.counts[2] = hdr[3];
     s.model = hdr[4]; s.nsteps = hdr[5]; s.nobj = hdr[6]; s.ndump = hdr[7]; s.plasticity = hdr[8];
     double dh[11];
@@ -89,6 +92,7 @@ SCENE_FILE Read_Scene(const char* path)
     if(s.plasticity == 1) rd(f, s.plastic, 4);
     else if(s.plasticity == 2) rd(f, s.plastic, 6);
     else if(s.plasticity) throw std::runtime_error("unknown plasticity");
+    if(s.implicit) rd(f, s.implicit_prm, 4);
     rd(f, &s.n, 1);
     size_t n = s.n, d = s.dim;
     s.X.resize(n * d); s.V.resize(n * d); s.F.resize(n * d * d); s.B.resize(n * d * d);
@@ -115,7 +119,13 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
     {
         this->threads = threads;
         gather_scatter.threads = threads;
-        this->use_symplectic_euler = true;
+        this->use_symplectic_euler = !s.implicit;
+        if(s.implicit) {   // MPM_EXAMPLE's Newton / Krylov controls (MPM_EXAMPLE.h:119-122)
+            this->newton_tolerance = (T)s.implicit_prm[0];
+            this->newton_iterations = (int)s.implicit_prm[1];
+            this->solver_tolerance = (T)s.implicit_prm[2];
+            this->solver_iterations = (int)s.implicit_prm[3];
+        }
         this->use_affine = true;
         this->flip = 0;
         this->min_dt = this->max_dt = (T)s.dt;

@@ -109,7 +109,7 @@ static int enqueue_substep(mpm_handle* h, double dt, double time)
 // path alternates its particle buffers, so it keeps one graph per parity.
 static int run_substep(mpm_handle* h, double dt, double time)
 {
-    if(h->timing) return enqueue_substep(h, dt, time);
+    if(h->timing || h->implicit.enabled) return enqueue_substep(h, dt, time);
     const int par = fast(h) ? h->fast.cur : 0;
     cudaGraphExec_t& ge = h->graphs[par];
     if(!ge) {
@@ -208,6 +208,7 @@ int mpm_destroy(mpm_handle* h)
     drain_timers(h);
     for(cudaEvent_t e: h->event_pool) cudaEventDestroy(e);
     diff_free(h);
+    implicit_free(h);
     plain_free(h);
     fast_free(h);
     cudaFree(h->d_flags);
@@ -306,7 +307,8 @@ int mpm_apply_forces(mpm_handle* h, double dt, double time)
 {
     int rc = check_dt(h, dt);
     if(rc) return rc;
-    return fast(h) ? fast_forces(h, dt, time) : plain_forces(h, dt, time);
+    if(fast(h)) return fast_forces(h, dt, time);
+    return h->implicit.enabled ? plain_implicit_forces(h, dt, time) : plain_forces(h, dt, time);
 }
 
 int mpm_grid_to_particle(mpm_handle* h, double dt, double time)
@@ -452,6 +454,28 @@ int mpm_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_ke
     if(!fast(h)) return set_error(h, MPM_ERR_ARG, "sort state exists on the fast path only");
     if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
     return fast_debug_sort_state(h, slot_keys, sorted_keys, perm);
+}
+
+int mpm_set_implicit(mpm_handle* h, const mpm_implicit_desc* d)
+{
+    if(!h || !d) return MPM_ERR_ARG;
+    if(d->enabled) {
+        if(fast(h)) return set_error(h, MPM_ERR_ARG, "the implicit solve runs on the plain path");
+        if(!(d->newton_tolerance >= 0) || !std::isfinite(d->newton_tolerance) || d->newton_iterations < 1 ||
+           !(d->solver_tolerance > 0) || !std::isfinite(d->solver_tolerance) || d->solver_iterations < 1)
+            return set_error(h, MPM_ERR_ARG, "implicit solve parameters");
+    }
+    release_graph(h);
+    h->implicit = *d;
+    h->implicit.enabled = d->enabled ? 1 : 0;
+    return MPM_OK;
+}
+
+int mpm_get_implicit_stats(mpm_handle* h, mpm_implicit_stats* s)
+{
+    if(!h || !s) return MPM_ERR_ARG;
+    *s = h->imp_stats;
+    return MPM_OK;
 }
 
 int mpm_set_plasticity(mpm_handle* h, const mpm_plasticity_desc* p)

@@ -108,6 +108,8 @@ enum FastCounter {
     CNT_COUNT = 8
 };
 
+struct ImplicitState;   // mpm_implicit.cu
+
 struct KernelTimer {
     std::string name;
     double ms = 0;
@@ -133,6 +135,9 @@ struct mpm_handle {
     PlainState plain;
     FastState fast;
     mpm_plasticity_desc plastic{};   // kind MPM_PLASTICITY_NONE: off
+    mpm_implicit_desc implicit{};    // enabled 0: symplectic Euler
+    mpm_implicit_stats imp_stats{};  // of the last implicit solve
+    ImplicitState* imp = nullptr;
     // timing
     bool timing = false;
     std::vector<KernelTimer> timers;
@@ -186,6 +191,10 @@ int fast_set_plastic(mpm_handle* h, const mpm_plastic_view* v);
 int plain_get_plastic(mpm_handle* h, mpm_plastic_view* v);
 int plain_set_plastic(mpm_handle* h, const mpm_plastic_view* v);
 int plain_grid_totals(mpm_handle* h, mpm_totals* out);
+
+// implicit solve (mpm_implicit.cu)
+int plain_implicit_forces(mpm_handle* h, double dt, double time);
+void implicit_free(mpm_handle* h);
 
 // adjoint (mpm_adjoint.cu)
 int diff_forward(mpm_handle* h, double dt, int nsteps, int every);

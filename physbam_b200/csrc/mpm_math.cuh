@@ -326,6 +326,157 @@ template<class T, int d> __device__ void phat(int model, const T* s, T mu, T la,
     for(int a = 0; a < d; a++) P[a] = mu * s[a] + c * (sqr(Fi[a]) * dF[a] - Fi[a]) + la * inner * Fi[a];
 }
 
+// ---------------------------------------------------------------------------
+// Second derivatives on singular values for the implicit solve: the
+// DIAGONALIZED_ISOTROPIC_STRESS_DERIVATIVE blocks H (H[i + d k] = x_iikk,
+// symmetric), B (x_ikik) and C (x_ikki) in the reference's pair order (2D: 01;
+// 3D: 12 20 01), with enforce_definiteness off (the constitutive models' default,
+// CONSTITUTIVE_MODEL.cpp:16).
+//   COROTATED_FIXED::Isotropic_Stress_Derivative_Helper (COROTATED_FIXED.cpp:125-163), panic 1e-6
+//   NEO_HOOKEAN::Isotropic_Stress_Derivative_Helper (NEO_HOOKEAN.cpp:144-179), on the
+//     hyperbola-clamped F below J = .25
+//   ST_VENANT_KIRCHHOFF_HENCKY_STRAIN::Isotropic_Stress_Derivative_Helper
+//     (ST_VENANT_KIRCHHOFF_HENCKY_STRAIN.cpp:92-150), zero once the last signed value is <= 0
+// (log(y) - log(x)) / (y - x) without cancellation: log1p(u)/u with u = (y - x)/x.
+template<class T> __device__ __forceinline__ T diff_log_over_diff(T x, T y)
+{
+    const T u = (y - x) / x;
+    const T r = fabs(u) < (T)1e-18 ? (T)1 : log1p(u) / u;
+    return r / x;
+}
+
+template<class T, int d> __device__ void stress_derivative(int model, const T* s, T mu, T la, T* H, T* Bv, T* Cv)
+{
+    const int P0[3] = {1, 2, 0}, P1[3] = {2, 0, 1};   // pair k of 3D: (1,2) (2,0) (0,1)
+    for(int e = 0; e < 9; e++) H[e] = 0;
+    for(int e = 0; e < 3; e++) Bv[e] = Cv[e] = 0;
+    if(model == MPM_COROTATED_FIXED) {
+        const T panic = (T)1e-6, mu2 = 2 * mu;
+        auto guard = [&](T x) { return fabs(x) < panic ? (x < 0 ? -panic : panic) : x; };
+        if(d == 2) {
+            const T J = s[0] * s[1], d01 = guard(s[0] + s[1]);
+            H[0] = mu2 + la * s[1] * s[1];
+            H[3] = mu2 + la * s[0] * s[0];
+            H[1] = H[2] = la * (2 * J - 1);
+            Cv[0] = mu2 / d01 - la * (J - 1);
+            Bv[0] = mu2 * (1 - 1 / d01);
+        } else {
+            const T J = s[0] * s[1] * s[2];
+            const T cof[3] = {s[1] * s[2], s[0] * s[2], s[0] * s[1]};
+            for(int a = 0; a < 3; a++) H[a + 3 * a] = mu2 + la * cof[a] * cof[a];
+            H[1] = H[3] = la * s[2] * (2 * J - 1);
+            H[2] = H[6] = la * s[1] * (2 * J - 1);
+            H[5] = H[7] = la * s[0] * (2 * J - 1);
+            for(int k = 0; k < 3; k++) {
+                const T dk = guard(s[P0[k]] + s[P1[k]]);
+                Cv[k] = mu2 / dk + la * s[k] * (1 - J);
+                Bv[k] = mu2 * (1 - 1 / dk);
+            }
+        }
+        return;
+    }
+    if(model == MPM_NEO_HOOKEAN) {
+        const T ft = (T)kNeoHookeanThreshold;
+        T J = 1;
+        for(int a = 0; a < d; a++) J *= s[a];
+        T Fc[3];
+        for(int a = 0; a < d; a++) Fc[a] = s[a];
+        if(!(J >= ft)) {   // NEO_HOOKEAN::Clamp_To_Hyperbola
+            if(d == 2) {
+                if(s[0] * s[0] > ft) { Fc[0] = s[0]; Fc[1] = ft / s[0]; }
+                else { Fc[0] = Fc[1] = sqrt(ft); }
+            } else {
+                if(s[0] * s[1] * s[1] > ft) { Fc[0] = s[0]; Fc[1] = s[1]; Fc[2] = ft / (s[0] * s[1]); }
+                else if(s[0] * s[0] * s[0] > ft) { T c = sqrt(ft / s[0]); Fc[0] = s[0]; Fc[1] = Fc[2] = c; }
+                else { Fc[0] = Fc[1] = Fc[2] = cbrt(ft); }
+            }
+        }
+        T Fi[3], detFi = 1;
+        for(int a = 0; a < d; a++) { Fi[a] = 1 / Fc[a]; detFi *= Fi[a]; }
+        const T mlj = mu + la * log(detFi);
+        for(int a = 0; a < d; a++) H[a + d * a] = mu + (la + mlj) * Fi[a] * Fi[a];
+        for(int a = 0; a < d; a++)
+            for(int b = 0; b < d; b++)
+                if(a != b) H[a + d * b] = la * Fi[a] * Fi[b];
+        if(d == 2) { Bv[0] = mu; Cv[0] = mlj * Fi[1] * Fi[0]; }
+        else
+            for(int k = 0; k < 3; k++) { Bv[k] = mu; Cv[k] = mlj * Fi[P0[k]] * Fi[P1[k]]; }
+        return;
+    }
+    // ST_VENANT_KIRCHHOFF_HENCKY_STRAIN (failure_threshold 0)
+    if(!(s[d - 1] > 0)) return;
+    const T l2m = la + 2 * mu, mu2 = 2 * mu;
+    T l[3], sum = 0;
+    for(int a = 0; a < d; a++) { l[a] = log(s[a]); sum += l[a]; }
+    for(int a = 0; a < d; a++) H[a + d * a] = (l2m - mu2 * l[a] - la * sum) / (s[a] * s[a]);
+    for(int a = 0; a < d; a++)
+        for(int b = 0; b < d; b++)
+            if(a != b) H[a + d * b] = la / (s[a] * s[b]);
+    auto pair = [&](int i, int j, T& B, T& C) {
+        const T m = (mu2 / s[i]) * (diff_log_over_diff(s[i], s[j]) - l[j] / s[j]) - la * sum / (s[i] * s[j]);
+        T p;
+        if(d == 2) p = ((la * s[0] + l2m * s[1]) * l[0] + (la * s[1] + l2m * s[0]) * l[1]) / (s[0] * s[1] * (s[0] + s[1]));
+        else p = (mu2 * (s[j] * l[i] + s[i] * l[j]) + la * (s[i] + s[j]) * sum) / (s[i] * s[j] * (s[i] + s[j]));
+        B = (T).5 * (m + p);
+        C = (T).5 * (m - p);
+    };
+    if(d == 2) pair(0, 1, Bv[0], Cv[0]);
+    else {
+        pair(0, 1, Bv[2], Cv[2]);
+        pair(0, 2, Bv[1], Cv[1]);
+        pair(1, 2, Bv[0], Cv[0]);
+    }
+}
+
+// DIAGONALIZED_ISOTROPIC_STRESS_DERIVATIVE::Differential: dP = dPhat/dF : dF in
+// the SVD frame (column-major d x d).
+template<class T, int d> __device__ __forceinline__ void stress_differential(const T* H, const T* Bv, const T* Cv, const T* G, T* dP)
+{
+    if(d == 2) {
+        dP[0] = H[0] * G[0] + H[1] * G[3];
+        dP[3] = H[1] * G[0] + H[3] * G[3];
+        dP[1] = Bv[0] * G[1] + Cv[0] * G[2];
+        dP[2] = Cv[0] * G[1] + Bv[0] * G[2];
+        return;
+    }
+    dP[0] = H[0] * G[0] + H[1] * G[4] + H[2] * G[8];
+    dP[4] = H[1] * G[0] + H[4] * G[4] + H[5] * G[8];
+    dP[8] = H[2] * G[0] + H[5] * G[4] + H[8] * G[8];
+    dP[1] = Bv[2] * G[1] + Cv[2] * G[3];
+    dP[3] = Cv[2] * G[1] + Bv[2] * G[3];
+    dP[2] = Bv[1] * G[2] + Cv[1] * G[6];
+    dP[6] = Cv[1] * G[2] + Bv[1] * G[6];
+    dP[5] = Bv[0] * G[5] + Cv[0] * G[7];
+    dP[7] = Cv[0] * G[5] + Bv[0] * G[7];
+}
+
+// Energy_Density on singular values:
+//   COROTATED_FIXED (COROTATED_FIXED.cpp:179-185): mu |S - I|^2 + lambda/2 (J - 1)^2
+//   NEO_HOOKEAN (NEO_HOOKEAN.cpp:191-199): mu (|S|^2/2 - d/2 - ln J) + lambda/2 ln^2 J, 1e16 for J <= 0
+//   ST_VENANT_KIRCHHOFF_HENCKY_STRAIN (l.52-63): mu |ln S|^2 + lambda/2 (tr ln S)^2, FLT_MAX
+//     once the last signed value is <= 0
+template<class T, int d> __device__ T energy_density(int model, const T* s, T mu, T la)
+{
+    T J = 1;
+    for(int a = 0; a < d; a++) J *= s[a];
+    if(model == MPM_COROTATED_FIXED) {
+        T e = 0;
+        for(int a = 0; a < d; a++) e += (s[a] - 1) * (s[a] - 1);
+        return mu * e + (T).5 * la * (J - 1) * (J - 1);
+    }
+    if(model == MPM_NEO_HOOKEAN) {
+        if(J <= 0) return (T)1e16;
+        T I1 = 0;
+        for(int a = 0; a < d; a++) I1 += s[a] * s[a];
+        const T lj = log(J);
+        return mu * ((T).5 * (I1 - d) - lj) + (T).5 * la * lj * lj;
+    }
+    if(s[d - 1] <= 0) return (T)FLT_MAX;
+    T n2 = 0, tr = 0;
+    for(int a = 0; a < d; a++) { const T l = log(s[a]); n2 += l * l; tr += l; }
+    return mu * n2 + (T).5 * la * tr * tr;
+}
+
 // MPM_FINITE_ELEMENTS::Precompute (Hybrid_Methods/Forces/MPM_FINITE_ELEMENTS.cpp:47-67):
 // PFT = U Phat(S) (F V)^T, i.e. P(F) F^T.  Returns false if the SVD did not converge.
 template<class T, int d> __device__ bool pft_svd(int model, const T* F, T mu, T la, T* PFT)

@@ -83,6 +83,16 @@ class PlasticView(ctypes.Structure):
                 ("rho_F", ctypes.c_void_p), ("cohesion", ctypes.c_void_p), ("vc", ctypes.c_void_p)]
 
 
+class ImplicitDesc(ctypes.Structure):
+    _fields_ = [("enabled", ctypes.c_int), ("newton_tolerance", ctypes.c_double), ("newton_iterations", ctypes.c_int),
+                ("solver_tolerance", ctypes.c_double), ("solver_iterations", ctypes.c_int)]
+
+
+class ImplicitStats(ctypes.Structure):
+    _fields_ = [("newton_iterations", ctypes.c_int), ("krylov_iterations", ctypes.c_int), ("converged", ctypes.c_int),
+                ("residual", ctypes.c_double)]
+
+
 # plastic-state keys (scenes.plastic_keys and the mu/lam pair) -> PlasticView fields
 _PLASTIC_FIELDS = {"Fp": "Fp", "mu": "mu", "lam": "lambda_", "mu0": "mu0", "lam0": "lambda0",
                    "pdef": "plastic_def", "rho_F": "rho_F", "cohesion": "cohesion", "vc": "vc"}
@@ -94,7 +104,8 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state",
            "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune", "mpm_particle_totals",
            "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex",
-           "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state"]
+           "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state", "mpm_set_implicit",
+           "mpm_get_implicit_stats"]
 
 _lib = None
 
@@ -138,6 +149,8 @@ def load_library(path: str = LIB_PATH):
     L.mpm_set_plasticity.argtypes = [P, ctypes.POINTER(PlasticityDesc)]
     L.mpm_get_plastic_state.argtypes = [P, ctypes.POINTER(PlasticView)]
     L.mpm_set_plastic_state.argtypes = [P, ctypes.POINTER(PlasticView)]
+    L.mpm_set_implicit.argtypes = [P, ctypes.POINTER(ImplicitDesc)]
+    L.mpm_get_implicit_stats.argtypes = [P, ctypes.POINTER(ImplicitStats)]
     L.mpm_status_string.argtypes = [ctypes.c_int]
     L.mpm_status_string.restype = ctypes.c_char_p
     for f in EXPORTS:
@@ -176,6 +189,8 @@ class MPM_DRIVER:
         self.set_collision_objects(scene.objects)
         if scene.plasticity is not None:
             self.set_plasticity(scene.plasticity)
+        if scene.implicit is not None:
+            self.set_implicit(scene.implicit)
         self.time = 0.0
         self.n = 0
 
@@ -325,6 +340,22 @@ class MPM_DRIVER:
         v = self._dev_view(X, V, Fc, Bc, valid=valid)
         self._check(self.L.mpm_get_particles(self.h, ctypes.byref(v)), "mpm_get_particles")
         return X, V, Fc, Bc, valid
+
+    # -- backward Euler ---------------------------------------------------------
+    def set_implicit(self, implicit: Optional[S.Implicit]):
+        """Newton backward-Euler force solve (a `scenes.Implicit`) or symplectic Euler (None)."""
+        d = ImplicitDesc()
+        if implicit is not None:
+            d.enabled = 1
+            d.newton_tolerance, d.newton_iterations = implicit.newton_tolerance, int(implicit.newton_iterations)
+            d.solver_tolerance, d.solver_iterations = implicit.solver_tolerance, int(implicit.solver_iterations)
+        self._check(self.L.mpm_set_implicit(self.h, ctypes.byref(d)), "mpm_set_implicit")
+
+    def implicit_stats(self):
+        st = ImplicitStats()
+        self._check(self.L.mpm_get_implicit_stats(self.h, ctypes.byref(st)), "mpm_get_implicit_stats")
+        return {"newton_iterations": st.newton_iterations, "krylov_iterations": st.krylov_iterations,
+                "converged": bool(st.converged), "residual": st.residual}
 
     # -- plasticity (MPM_PLASTICITY_CLAMP) -------------------------------------
     def set_plasticity(self, plasticity):

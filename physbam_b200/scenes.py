@@ -115,6 +115,18 @@ def plastic_from_params(p):
 
 
 @dataclasses.dataclass
+class Implicit:
+    """Backward-Euler force solve instead of symplectic Euler (the reference's default:
+    `MPM_DRIVER::Apply_Forces`, `MPM_DRIVER.cpp:1024-1048`): Newton's method on
+    `MPM_OBJECTIVE` with CG, tolerance `newton_tolerance * dt`, the Krylov tolerance
+    relative (`MPM_EXAMPLE.h:119-122` defaults)."""
+    newton_tolerance: float = 1.0
+    newton_iterations: int = 100
+    solver_tolerance: float = 0.5
+    solver_iterations: int = 1000
+
+
+@dataclasses.dataclass
 class Scene:
     name: str
     dim: int
@@ -135,6 +147,7 @@ class Scene:
     mu: np.ndarray
     lam: np.ndarray
     plasticity: Optional[Plasticity] = None
+    implicit: Optional[Implicit] = None
 
     @property
     def n(self) -> int:
@@ -378,6 +391,23 @@ def small_snow_2d(seed=23, G=16, nsteps=20, dt=1e-4):
     return s
 
 
+def small_3d_implicit(seed=41, G=16, nsteps=10, dt=1e-3):
+    """small_3d with the backward-Euler Newton solve at a step 10x the explicit one
+    (stick floor, slip walls with friction 0.3, corotated)."""
+    s = small_3d(seed=seed, G=G, nsteps=nsteps, dt=dt, friction=0.3)
+    s.name = "small3dimplicit"
+    s.implicit = Implicit()
+    return s
+
+
+def small_2d_implicit(seed=43, G=16, nsteps=10, dt=1e-3):
+    """small_2d, neo-Hookean, with the backward-Euler Newton solve."""
+    s = small_2d(seed=seed, G=G, nsteps=nsteps, dt=dt, model=NEO_HOOKEAN)
+    s.name = "small2dimplicit"
+    s.implicit = Implicit()
+    return s
+
+
 def small_sand_3d(seed=31, G=16, nsteps=20, dt=1e-4):
     """A small sand block (St. Venant-Kirchhoff Hencky + Drucker-Prager with Mast hardening)
     thrown against a sticky floor; a random initial F per particle, compressed by 3 % for
@@ -425,7 +455,7 @@ def snowballs_3d(seed=1234, G=128, ppc=8, E=1.4e5, nu=0.2, density=400.0, dt=5e-
 # --------------------------------------------------------------------------------------------
 # Scene file: read by the reference runner (oracle/ref_scene.cpp) and by the C oracle harness.
 # --------------------------------------------------------------------------------------------
-MAGIC = b"MPMSCN01"
+MAGIC = b"MPMSCN02"
 
 
 def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
@@ -436,7 +466,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         f.write(MAGIC)
         counts = list(s.counts) + [1] * (3 - d)
         pl = s.plasticity
-        f.write(struct.pack("<9i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0))
+        im = s.implicit
+        f.write(struct.pack("<10i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
+                            1 if im else 0))
         f.write(struct.pack("<11d", *pad3(s.domain_min), *pad3(s.domain_max), *pad3(s.gravity), s.dt, 0.0))
         f.write(struct.pack("<%di" % len(dumps), *dumps))
         for o in s.objects:
@@ -444,6 +476,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         if pl:
             prm = plastic_params(pl)[1:]
             f.write(struct.pack("<%dd" % len(prm), *prm))
+        if im:
+            f.write(struct.pack("<4d", im.newton_tolerance, im.newton_iterations, im.solver_tolerance,
+                                im.solver_iterations))
         f.write(struct.pack("<q", s.n))
         f.write(np.ascontiguousarray(s.X, np.float64).tobytes())
         f.write(np.ascontiguousarray(s.V, np.float64).tobytes())

@@ -33,6 +33,9 @@ CASES = {
     "smallsnow3d_corotated": (lambda: S.small_snow_3d(), [0, 19], [0, 19]),
     "smallsnow2d_corotated": (lambda: S.small_snow_2d(), [0, 19], [19]),
     "small3d_hencky": (lambda: S.small_3d(model=S.HENCKY, seed=13, E=(1e5, 3e5)), [0, 19], [0]),
+    # backward Euler (the reference's default solve), Newton tolerances as MPM_EXAMPLE's defaults
+    "small3d_implicit": (lambda: S.small_3d_implicit(), [0, 1, 9], [0, 9]),
+    "small2d_implicit": (lambda: S.small_2d_implicit(), [0, 9], [0, 9]),
     # sand: ST_VENANT_KIRCHHOFF_HENCKY_STRAIN + MPM_DRUCKER_PRAGER (Fp, plastic_def, rho_F, sigma_Y, vc dumped)
     "smallsand3d_hencky": (lambda: S.small_sand_3d(), [0, 1, 19], [0, 19]),
     "smallsand2d_hencky": (lambda: S.small_sand_2d(), [0, 19], [19]),
@@ -62,6 +65,10 @@ def main(names=None):
         pl = scene.plasticity
         if pl is not None:
             arrays["plasticity"] = np.array(S.plastic_params(pl), np.float64)
+        im = scene.implicit
+        if im is not None:
+            arrays["implicit"] = np.array([im.newton_tolerance, im.newton_iterations, im.solver_tolerance,
+                                           im.solver_iterations], np.float64)
         for step in dumps:
             r = ref[step]
             for k in ("X", "V", "F", "B", "valid") + S.plastic_keys(pl):
@@ -85,6 +92,9 @@ def load(name):
                     z["volume"].copy(), z["mu"].copy(), z["lam"].copy())
     if "plasticity" in z:
         scene.plasticity = S.plastic_from_params(z["plasticity"])
+    if "implicit" in z:
+        im = z["implicit"]
+        scene.implicit = S.Implicit(float(im[0]), int(im[1]), float(im[2]), int(im[3]))
     dumps = {}
     for step in z["dumps"]:
         step = int(step)

@@ -33,7 +33,12 @@ def floors(scene, ref):
             "pdef": 1e-300, "rho_F": 1e-300, "cohesion": 1.0, "vc": 1e-300}
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+# the backward-Euler cases pin the GPU solve directly against the reference's
+# dumps; the C restatement covers the symplectic-Euler substep
+EXPLICIT = sorted(n for n in CASES if "implicit" not in n)
+
+
+@pytest.mark.parametrize("name", EXPLICIT)
 def test_oracle_matches_reference_dumps(name):
     scene, dumps = load(name)
     st = oracle.State(scene)
