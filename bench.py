@@ -39,6 +39,7 @@ ALG_BYTES = {"p2g": 112, "g2p": 144, "substep": 256}    # bytes per particle (FP
 # plastic state read and written by G2P per particle: snow Fp, mu0, lambda0;
 # sand Fp, plastic_def, rho_F, sigma_Y, vc
 PLASTIC_BYTES = {1: 88, 2: 104}
+IMPLICIT_LEAD = 12                                      # implicit leg: substeps run before timing (contact)
 SNOW_LEAD_SUBSTEPS = 600                                # plastic legs: substeps run before timing
 GRID_BYTES_PER_NODE = 48                                # grid update: read 16, write 32
 
@@ -309,7 +310,7 @@ def our_arm(args):
     roof = roofline_of(ktimes, n, peak, peak_kind, WORKLOAD)
     total_k = sum(v[0] for v in ktimes.values())
 
-    large = batch = adjoint = plain = snow = sand = None
+    large = batch = adjoint = plain = snow = sand = implicit = None
     if world == 1 and not args.no_plain:
         plain = measure_plain_fp64(args, D, S, stream, flush, substep_ms)
     if world == 1 and not args.no_snow:
@@ -317,6 +318,8 @@ def our_arm(args):
                                "snowballs3d-128^3-corotated-8ppc-clamp-fp32")
         sand = measure_plastic(args, D, S, stream, flush, peak, substep_ms, S.sand_3d(),
                                "sand3d-128^3-hencky-8ppc-druckerprager-fp32")
+    if world == 1 and not args.no_implicit:
+        implicit = measure_implicit(args, D, S, stream, flush)
     if world == 1 and not args.no_large:
         large = measure_large(args, D, S, stream, flush, peak, peak_kind)
     if not args.no_batch:
@@ -346,6 +349,7 @@ def our_arm(args):
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()},
             "kernel_share": {k: v[0] / total_k for k, v in ktimes.items()},
             "plain_fp64": plain,
+            "implicit": implicit,
             "snow": snow,
             "sand": sand,
             "large_config": large,
@@ -449,6 +453,58 @@ def measure_plastic(args, D, S, stream, flush, peak, elastic_ms, scene, workload
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
 
 
+def measure_implicit(args, D, S, stream, flush):
+    """The headline geometry with the reference's default solve: backward Euler
+    (Newton + CG + Wolfe line search, MPM_EXAMPLE's default tolerances) at a
+    40x larger step, dt = 2e-3, timed once the spheres are in contact (after
+    IMPLICIT_LEAD substeps), on the plain path in FP64 and FP32; beside it the
+    reference's own implicit driver on the host cores, same scene, same steps."""
+    import torch
+    import oracle
+    scene = S.spheres_3d(dt=2e-3)
+    scene.implicit = S.Implicit()
+    out = {"workload": "spheres3d-128^3-neohookean-8ppc-implicit-dt2e-3", "particles": scene.n, "dt": scene.dt,
+           "timed_after_substeps": IMPLICIT_LEAD}
+    steps = max(3, min(args.steps, 8))
+    for name, prec in (("fp64", D.FP64), ("fp32", D.FP32)):
+        drv = D.MPM_DRIVER(scene, precision=prec, path=D.PATH_PLAIN)
+        drv.set_stream(stream.cuda_stream)
+        drv.set_scene_particles(scene)
+        for _ in range(IMPLICIT_LEAD):
+            drv.Advance_One_Time_Step()
+        drv.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        newton = cg = 0
+        for k in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+                evs[k][0].record(stream)
+            drv.Advance_One_Time_Step()
+            with torch.cuda.stream(stream):
+                evs[k][1].record(stream)
+            st = drv.implicit_stats()
+            newton += st["newton_iterations"]
+            cg += st["krylov_iterations"]
+        torch.cuda.synchronize()
+        drv.close()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+        out[name] = {"ms_per_step": ms, "value": scene.n / (ms / 1e3), "unit": METRIC,
+                     "newton_per_step": newton / steps, "cg_per_step": cg / steps}
+    if oracle.ref_available() and not args.no_cpu:
+        s = scene.copy()
+        s.nsteps = IMPLICIT_LEAD + 3
+        cores = os.cpu_count() or 1
+        _, t = oracle.run_reference(s, [], threads=cores, timing=True)
+        secs = t["step_seconds"][IMPLICIT_LEAD:]
+        ref_ms = 1e3 * sum(secs) / len(secs)
+        out["reference"] = {"ms_per_step": ref_ms, "value": scene.n / (ref_ms / 1e3), "unit": METRIC, "cores": cores,
+                            "kind": "reference",
+                            "sample": "3 substeps after the same %d lead substeps, PhysBAM MPM_DRIVER implicit FP64, "
+                                      "%d OpenMP threads" % (IMPLICIT_LEAD, cores)}
+        out["fp64_speedup_over_reference"] = ref_ms / out["fp64"]["ms_per_step"]
+    return out
+
+
 def measure_adjoint(D, S):
     """64^3 cube, 64 substeps, checkpoint every 8; FP32 forward and
     backward through the C ABI (device arrays), timed with CUDA events."""
@@ -542,6 +598,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-scene batched measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward/backward timing")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 path on the same workload")
+    ap.add_argument("--no-implicit", action="store_true", help="skip the backward-Euler measurement")
     ap.add_argument("--no-snow", action="store_true", help="skip the snow and sand (plasticity) measurements")
     ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d", "snowballs3d", "sand3d"],
                     help="profiling run of one scene only")
