@@ -255,6 +255,33 @@ typedef struct {
 } mpm_implicit_stats;
 int mpm_get_implicit_stats(mpm_handle* h, mpm_implicit_stats* s);
 
+/* Adaptive substeps: MPM_DRIVER::Simulate_To_Frame (MPM_DRIVER.cpp:161-201)
+ * and Reduce_Dt (l.519-545).  Each substep takes Compute_Dt (the affine CFL
+ * bound with `cfl`) clamped to [min_dt, max_dt] and fitted to the frame end;
+ * after the forces, with strong_cfl, Grid_To_Particle_Limit_Dt limits the change
+ * of F (cfl_F) and the displacement (cfl) of the coming G2P, and with
+ * sound_cfl the largest sound speed limits dt to cfl_sound dx / c; a step so
+ * shortened scales the grid velocity increments and ends early, and the frame
+ * takes more substeps.  Defaults as MPM_EXAMPLE.h:84-115.  The reductions
+ * of dt run on the plain path (they need the velocity after P2G and the stress
+ * derivative); the fast path takes Compute_Dt steps without them. */
+typedef struct {
+    double cfl;
+    double min_dt;
+    double max_dt;
+    int strong_cfl;
+    double cfl_F;
+    int sound_cfl;
+    double cfl_sound;
+} mpm_dt_control;
+int mpm_set_dt_control(mpm_handle* h, const mpm_dt_control* c);
+
+/* One frame of adaptive substeps from `time` to time + frame_dt; returns the
+ * time reached (the frame end) and the number of substeps taken.  Each step is
+ * one mpm_substep; mpm_last_dt gives the step the last substep took. */
+int mpm_simulate_frame(mpm_handle* h, double time, double frame_dt, double* time_out, int* substeps);
+int mpm_last_dt(mpm_handle* h, double* dt);
+
 /* ---- inspection ---------------------------------------------------------- */
 
 /* Grids of the last substep as doubles on the host, each (G+6)^d nodes (times

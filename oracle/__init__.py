@@ -231,6 +231,8 @@ def ref_available() -> bool:
 def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timing: bool = False, totals=None):
     """Run the reference's own driver on ``scene``; return {step: dump} (and timing JSON if asked).
 
+    With ``scene.dt_control`` the steps are frames of Simulate_To_Frame and the
+    result is ``(dumps, {"frame_substeps": [...], "time": t})``.
     ``totals=(cfl, max_dt)`` returns instead ``(dumps, diagnostics)``: the
     reference's Total_Particle_* momenta and energy, Max_Particle_Speed,
     Grid_V_Upper_Bound and Compute_Dt on the final state."""
@@ -248,6 +250,10 @@ def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timin
             cmd += ["-totals", repr(float(totals[0])), repr(float(totals[1]))]
         out = subprocess.run(cmd, check=True, capture_output=True, text=True)
         res = S.read_dump(dp, scene.dim, scene.n, scene.counts, plastic=S.plastic_keys(scene.plasticity)) if dumps else {}
+        if scene.dt_control is not None:   # frames: the substeps Simulate_To_Frame took per frame
+            import json
+            lines = [ln for ln in out.stdout.splitlines() if ln.startswith('{"frame_substeps"')]
+            res = (res, json.loads(lines[-1]))
         if totals is not None:
             import json
             lines = [ln for ln in out.stdout.splitlines() if ln.startswith('{"mass"')]

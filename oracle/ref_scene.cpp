@@ -48,7 +48,9 @@ namespace {
 struct OBJ { int kind, type; double friction, a[3], b[3]; };
 struct SCENE_FILE
 {
-    int dim, counts[3], model, nsteps, nobj, ndump, plasticity, implicit;
+    int dim, counts[3], model, nsteps, nobj, ndump, plasticity, implicit, dt_control;
+    // frame_dt, cfl, min_dt, max_dt, strong_cfl, cfl_F, sound_cfl, cfl_sound
+    double dtc[8];
     double implicit_prm[4];   // newton_tolerance, newton_iterations, solver_tolerance, solver_iterations
     // clamp (1): theta_c, theta_s, max_hardening, hardening_factor;
     // Drucker-Prager (2): a0, a1, a3, a4, sigma_Y0, use_vc
@@ -71,11 +73,12 @@ SCENE_FILE Read_Scene(const char* path)
     if(!f) throw std::runtime_error("cannot open scene");
     char magic[8];
     rd(f, magic, 8);
-    if(memcmp(magic, "MPMSCN02", 8)) throw std::runtime_error("bad scene magic");
+    if(memcmp(magic, "MPMSCN03", 8)) throw std::runtime_error("bad scene magic");
     SCENE_FILE s;
-    int hdr[10];
-    rd(f, hdr, 10);
+    int hdr[11];
+    rd(f, hdr, 11);
     s.implicit = hdr[9];
+    s.dt_control = hdr[10];
     s.dim = hdr[0]; s.counts[0] = hdr[1]; s.counts[1] = hdr[2]; s.counts[2] = hdr[3];
     s.model = hdr[4]; s.nsteps = hdr[5]; s.nobj = hdr[6]; s.ndump = hdr[7]; s.plasticity = hdr[8];
     double dh[11];
@@ -93,6 +96,7 @@ SCENE_FILE Read_Scene(const char* path)
     else if(s.plasticity == 2) rd(f, s.plastic, 6);
     else if(s.plasticity) throw std::runtime_error("unknown plasticity");
     if(s.implicit) rd(f, s.implicit_prm, 4);
+    if(s.dt_control) rd(f, s.dtc, 8);
     rd(f, &s.n, 1);
     size_t n = s.n, d = s.dim;
     s.X.resize(n * d); s.V.resize(n * d); s.F.resize(n * d * d); s.B.resize(n * d * d);
@@ -129,6 +133,16 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
         this->use_affine = true;
         this->flip = 0;
         this->min_dt = this->max_dt = (T)s.dt;
+        if(s.dt_control) {   // Simulate_To_Frame with MPM_EXAMPLE's step controls
+            this->frame_dt = (T)s.dtc[0];
+            this->cfl = (T)s.dtc[1];
+            this->min_dt = (T)s.dtc[2];
+            this->max_dt = (T)s.dtc[3];
+            this->use_strong_cfl = s.dtc[4] != 0;
+            this->cfl_F = (T)s.dtc[5];
+            this->use_sound_speed_cfl = s.dtc[6] != 0;
+            this->cfl_sound = (T)s.dtc[7];
+        }
         particles.Store_B(true);
     }
 
@@ -238,15 +252,24 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
     if(!f) { fprintf(stderr, "cannot open dump\n"); return 1; }
     double total = 0;
     std::vector<double> step_seconds;
+    int substeps = 0;
+    example.Add_Callbacks(false, "time-step", [&]() { substeps++; });
+    std::vector<int> frame_substeps;
     for(int step = 0; step < s.nsteps; step++) {
         current = step;
-        example.dt = (T)s.dt;
         auto t0 = std::chrono::steady_clock::now();
-        driver.Advance_One_Time_Step();
+        if(s.dt_control) {   // one frame: `step` counts frames
+            const int before = substeps;
+            driver.Simulate_To_Frame(step + 1);
+            frame_substeps.push_back(substeps - before);
+        } else {
+            example.dt = (T)s.dt;
+            driver.Advance_One_Time_Step();
+        }
         auto t1 = std::chrono::steady_clock::now();
         step_seconds.push_back(std::chrono::duration<double>(t1 - t0).count());
         total += step_seconds.back();
-        example.time += example.dt;
+        if(!s.dt_control) example.time += example.dt;
         if(!want(step)) continue;
         wr(f, &step, 1);
         std::vector<double> buf;
@@ -302,6 +325,11 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
         printf("], \"kinetic_energy\": %.17g, \"max_speed\": %.17g, \"max_affine_speed\": %.17g, \"dt\": %.17g}\n",
             (double)example.Total_Particle_Kinetic_Energy(), (double)driver.Max_Particle_Speed(),
             (double)driver.Grid_V_Upper_Bound(), (double)driver.Compute_Dt());
+    }
+    if(s.dt_control) {
+        printf("{\"frame_substeps\": [");
+        for(size_t i = 0; i < frame_substeps.size(); i++) printf("%s%d", i ? ", " : "", frame_substeps[i]);
+        printf("], \"time\": %.17g}\n", (double)example.time);
     }
     if(report_time) {
         printf("{\"substeps\": %d, \"particles\": %lld, \"seconds\": %.9g, \"threads\": %d, \"step_seconds\": [",

@@ -97,10 +97,17 @@ static int release_graph(mpm_handle* h)
 }
 
 // One substep: the three phases back to back.
+static bool reduces_dt(const mpm_handle* h) { return h->dt_control.strong_cfl || h->dt_control.sound_cfl; }
+
+// Advance_One_Time_Step: p2g, forces, Reduce_Dt (plain path, when asked), g2p
 static int enqueue_substep(mpm_handle* h, double dt, double time)
 {
     int rc = mpm_particle_to_grid(h, dt, time);
-    if(!rc && !(rc = mpm_apply_forces(h, dt, time))) rc = mpm_grid_to_particle(h, dt, time);
+    if(!rc) rc = mpm_apply_forces(h, dt, time);
+    double taken = dt;
+    if(!rc && !fast(h) && reduces_dt(h)) rc = plain_reduce_dt(h, dt, &taken);
+    if(!rc) rc = mpm_grid_to_particle(h, taken, time);
+    h->last_dt = taken;
     return rc;
 }
 
@@ -109,7 +116,7 @@ static int enqueue_substep(mpm_handle* h, double dt, double time)
 // path alternates its particle buffers, so it keeps one graph per parity.
 static int run_substep(mpm_handle* h, double dt, double time)
 {
-    if(h->timing || h->implicit.enabled) return enqueue_substep(h, dt, time);
+    if(h->timing || h->implicit.enabled || (!fast(h) && reduces_dt(h))) return enqueue_substep(h, dt, time);
     const int par = fast(h) ? h->fast.cur : 0;
     cudaGraphExec_t& ge = h->graphs[par];
     if(!ge) {
@@ -126,6 +133,7 @@ static int run_substep(mpm_handle* h, double dt, double time)
         h->graph_dt = dt;
     }
     MPM_CUDA(h, cudaGraphLaunch(ge, h->stream));
+    h->last_dt = dt;
     if(fast(h)) h->fast.cur = 1 - par;
     return MPM_OK;
 }
@@ -322,9 +330,7 @@ int mpm_substep(mpm_handle* h, double dt, double time)
 {
     int rc = check_dt(h, dt);
     if(rc) return rc;
-    if((rc = mpm_particle_to_grid(h, dt, time))) return rc;
-    if((rc = mpm_apply_forces(h, dt, time))) return rc;
-    return mpm_grid_to_particle(h, dt, time);
+    return enqueue_substep(h, dt, time);
 }
 
 int mpm_advance(mpm_handle* h, double dt, double time, int nsteps)
@@ -468,6 +474,58 @@ int mpm_set_implicit(mpm_handle* h, const mpm_implicit_desc* d)
     release_graph(h);
     h->implicit = *d;
     h->implicit.enabled = d->enabled ? 1 : 0;
+    return MPM_OK;
+}
+
+int mpm_set_dt_control(mpm_handle* h, const mpm_dt_control* c)
+{
+    if(!h || !c) return MPM_ERR_ARG;
+    if(!(c->cfl > 0) || !(c->min_dt >= 0) || !(c->max_dt > 0) || !(c->max_dt >= c->min_dt) || !std::isfinite(c->max_dt))
+        return set_error(h, MPM_ERR_ARG, "dt control: cfl > 0, 0 <= min_dt <= max_dt");
+    if((c->strong_cfl && !(c->cfl_F > 0)) || (c->sound_cfl && !(c->cfl_sound > 0)))
+        return set_error(h, MPM_ERR_ARG, "dt control: CFL numbers must be positive");
+    if(fast(h) && (c->strong_cfl || c->sound_cfl))
+        return set_error(h, MPM_ERR_ARG, "the strong and sound-speed CFL reductions run on the plain path");
+    release_graph(h);
+    h->dt_control = *c;
+    return MPM_OK;
+}
+
+int mpm_last_dt(mpm_handle* h, double* dt)
+{
+    if(!h || !dt) return MPM_ERR_ARG;
+    *dt = h->last_dt;
+    return MPM_OK;
+}
+
+int mpm_simulate_frame(mpm_handle* h, double time, double frame_dt, double* time_out, int* substeps)
+{
+    if(!h || !(frame_dt > 0)) return MPM_ERR_ARG;
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    const mpm_dt_control& c = h->dt_control;
+    if(!(c.max_dt > 0)) return set_error(h, MPM_ERR_STATE, "mpm_set_dt_control first");
+    const double time_at_frame = time + frame_dt;
+    int count = 0;
+    for(bool done = false; !done; count++) {
+        double dt = 0;
+        int rc = mpm_compute_dt(h, c.cfl, c.max_dt, &dt);
+        if(rc) return rc;
+        dt = dt < c.min_dt ? c.min_dt : (dt > c.max_dt ? c.max_dt : dt);
+        double next = time + dt;
+        if(next + .0001 * dt > time_at_frame) { next = time_at_frame; done = true; }   // roundoff
+        else if(next + dt > time_at_frame) next = (time + time_at_frame) / 2;
+        dt = next - time;
+        if(!(dt > 0)) return set_error(h, MPM_ERR_ARG, "substep dt is not positive");
+        const double original = dt;
+        if((rc = mpm_substep(h, dt, time))) return rc;
+        if(h->last_dt < original) {   // Reduce_Dt shortened the step
+            next = time + h->last_dt;
+            done = false;
+        }
+        time = next;
+    }
+    if(time_out) *time_out = time;
+    if(substeps) *substeps = count;
     return MPM_OK;
 }
 

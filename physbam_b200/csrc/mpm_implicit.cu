@@ -485,6 +485,26 @@ template<class T> __global__ void k_imp_sum_particles(const double* pe, int64_t 
     if(threadIdx.x == 0) partial[blockIdx.x] = t;
 }
 
+__device__ double block_sum_max(double v)
+{
+    __shared__ double sh[kRedThreads];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for(int s = kRedThreads / 2; s > 0; s >>= 1) {
+        if(threadIdx.x < s) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    return sh[0];
+}
+
+__global__ void k_imp_max_final(const double* partial, int count, double* out)
+{
+    if(threadIdx.x) return;
+    double r = partial[0];
+    for(int b = 1; b < count; b++) r = fmax(r, partial[b]);
+    *out = r;
+}
+
 __global__ void k_imp_final(const double* partial, int count, int slots, double* out)
 {
     // one thread per result slot, partials summed in block order
@@ -847,6 +867,42 @@ template<class T> int implicit_t(mpm_handle* h, double dt)
 }
 
 }  // namespace
+
+namespace {
+// Compute_Max_Sound_Speed on the singular values and stress derivative of the
+// solve's last force evaluation (what the reference's force holds then).
+template<class T, int d> __global__ void k_imp_sound(ImpArgs<T> ia, double* partial)
+{
+    const PlainArgs<T>& a = ia.a;
+    double smax = 0;
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+        if(!a.valid[p]) continue;
+        const T* blk = ia.dP + p * 15;
+        smax = fmax(smax, (double)sound_speed<T, d>(ia.sig + p * d, blk, blk + 9, a.mass[p] / a.vol[p]));
+    }
+    const double r = block_sum_max(smax);
+    if(threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+template<class T> int implicit_sound_t(mpm_handle* h, double* partial, double* out)
+{
+    if(!h->imp) return set_error(h, MPM_ERR_STATE, "no implicit solve yet");
+    if(h->sp.dim == 3) {
+        Solver<T, 3> sv(h, 0.0);
+        k_imp_sound<T, 3><<<kRedBlocks, kRedThreads, 0, h->stream>>>(sv.ia, partial);
+    } else {
+        Solver<T, 2> sv(h, 0.0);
+        k_imp_sound<T, 2><<<kRedBlocks, kRedThreads, 0, h->stream>>>(sv.ia, partial);
+    }
+    k_imp_max_final<<<1, 32, 0, h->stream>>>(partial, kRedBlocks, out);
+    return MPM_OK;
+}
+}  // namespace
+
+int implicit_max_sound_speed(mpm_handle* h, double* partial, double* out)
+{
+    return h->model.precision == MPM_FP64 ? implicit_sound_t<double>(h, partial, out) : implicit_sound_t<float>(h, partial, out);
+}
 
 void implicit_free(mpm_handle* h)
 {

@@ -477,6 +477,19 @@ template<class T, int d> __device__ T energy_density(int model, const T* s, T mu
     return mu * n2 + (T).5 * la * tr * tr;
 }
 
+// ISOTROPIC_CONSTITUTIVE_MODEL::Sound_Speed (ISOTROPIC_CONSTITUTIVE_MODEL.cpp:150-161)
+// from the singular values and the stress derivative blocks.
+template<class T, int d> __device__ T sound_speed(const T* S, const T* H, const T* Bv, T density)
+{
+    T F2[3], cm = -(T)INFINITY;
+    for(int a = 0; a < d; a++) { F2[a] = S[a] * S[a]; cm = fmax(cm, H[a + d * a] * F2[a]); }
+    const int spin = d == 3 ? 3 : 1;
+    for(int k = 0; k < spin; k++)
+        for(int i = 0; i < 2; i++) cm = fmax(cm, Bv[k] * F2[(k + i + 1) % spin]);
+    return sqrt(cm / density);
+}
+
+
 // MPM_FINITE_ELEMENTS::Precompute (Hybrid_Methods/Forces/MPM_FINITE_ELEMENTS.cpp:47-67):
 // PFT = U Phat(S) (F V)^T, i.e. P(F) F^T.  Returns false if the SVD did not converge.
 template<class T, int d> __device__ bool pft_svd(int model, const T* F, T mu, T la, T* PFT)

@@ -284,6 +284,158 @@ template<class T> int forces_t(mpm_handle* h, double dt)
     return MPM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// MPM_DRIVER::Reduce_Dt (MPM_DRIVER.cpp:519-545) after the forces.
+// ---------------------------------------------------------------------------
+// Enforce_Limit_Max (l.547-574): lower s so that t (a + t b) stays within the bound.
+template<class T> __device__ void limit_max(T& s, T bound, T a, T b)
+{
+    if(a < 0) { a = -a; b = -b; }
+    if(a * a + 4 * b * bound >= 0) {
+        if(s * (a + s * b) > bound) s = (2 * bound) / (a + sqrt(a * a + 4 * b * bound));
+    } else {
+        if(s * (a + s * b) < -bound) s = -(a + sqrt(a * a - 4 * b * bound)) / (2 * b);
+    }
+}
+
+__device__ __forceinline__ double block_reduce(double v, bool take_min)
+{
+    __shared__ double sh[256];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for(int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if(threadIdx.x < st) sh[threadIdx.x] = take_min ? fmin(sh[threadIdx.x], sh[threadIdx.x + st]) : fmax(sh[threadIdx.x], sh[threadIdx.x + st]);
+        __syncthreads();
+    }
+    return sh[0];
+}
+
+// Grid_To_Particle_Limit_Dt (l.577-625) per particle, min over particles:
+// the scale s <= 100 of dt at which the F change (cfl_F, entrywise) and the
+// displacement (cfl) of the G2P update reach their bounds.  velocity_save is
+// the velocity after P2G.
+template<class T, int d> __global__ void k_strong_cfl(PlainArgs<T> a, T cfl, T cfl_F, double* partial)
+{
+    double smin = 100;
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+        if(!a.valid[p]) continue;
+        Stencil<T, d> st;
+        if(!make_stencil<T, d>(a, a.X + p * d, st)) continue;
+        T Vp[3] = {0, 0, 0}, Vs[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Gs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const int nq = d == 3 ? 27 : 9;
+        for(int q = 0; q < nq; q++) {
+            int64_t i;
+            T w, g[3], Z[3];
+            node<T, d>(a, st, q, i, w, g, Z);
+            for(int r = 0; r < d; r++) {
+                const T vo = a.gv0[i * d + r], dvr = a.gv[i * d + r] - vo;
+                Vp[r] += w * vo;
+                Vs[r] += w * dvr;
+                for(int c = 0; c < d; c++) { G[r + d * c] += vo * g[c]; Gs[r + d * c] += dvr * g[c]; }
+            }
+        }
+        T s = 100;
+        for(int i = 0; i < d; i++)
+            for(int j = 0; j < d; j++) limit_max<T>(s, cfl_F, a.dt * G[i + d * j], a.dt * Gs[i + d * j]);
+        for(int i = 0; i < d; i++) limit_max<T>(s, cfl, a.dt * Vp[i], a.dt * Vs[i]);
+        smin = fmin(smin, (double)s);
+    }
+    const double r = block_reduce(smin, true);
+    if(threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+// Compute_Max_Sound_Speed (MPM_DRIVER.cpp:893-918): max over particles of
+// ISOTROPIC_CONSTITUTIVE_MODEL::Sound_Speed of the stress derivative of F.
+template<class T, int d> __global__ void k_sound_speed(PlainArgs<T> a, double* partial)
+{
+    double smax = 0;
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+        if(!a.valid[p]) continue;
+        T F[9], U[9], V[9], S[3], H[9], Bv[3], Cv[3];
+        for(int e = 0; e < d * d; e++) F[e] = a.F[p * d * d + e];
+        if(d == 3) svd3<T>(F, U, S, V);
+        else svd2<T>(F, U, S, V);
+        stress_derivative<T, d>(a.sp.model, S, a.mu[p], a.lam[p], H, Bv, Cv);
+        smax = fmax(smax, (double)sound_speed<T, d>(S, H, Bv, a.mass[p] / a.vol[p]));
+    }
+    const double r = block_reduce(smax, false);
+    if(threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+__global__ void k_fold(const double* partial, int count, int take_min, double* out)
+{
+    if(threadIdx.x) return;
+    double r = partial[0];
+    for(int b = 1; b < count; b++) r = take_min ? fmin(r, partial[b]) : fmax(r, partial[b]);
+    *out = r;
+}
+
+// v = (v - vs) s + vs for the velocity and the friction velocity (l.536-544)
+template<class T> __global__ void k_scale_dt(PlainArgs<T> a, T s)
+{
+    const int d = a.sp.dim;
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.gn; i += (int64_t)gridDim.x * blockDim.x) {
+        if(a.gm[i] == 0) continue;
+        for(int k = 0; k < d; k++) {
+            const T vs = a.gv0[i * d + k];
+            a.gv[i * d + k] = (a.gv[i * d + k] - vs) * s + vs;
+            a.gvf[i * d + k] = (a.gvf[i * d + k] - vs) * s + vs;
+        }
+    }
+}
+
+template<class T> int reduce_dt_t(mpm_handle* h, double dt, double* dt_out)
+{
+    PlainArgs<T> a = args<T>(h, dt);
+    const mpm_dt_control& c = h->dt_control;
+    *dt_out = dt;
+    if(!a.n || (!c.strong_cfl && !c.sound_cfl)) return MPM_OK;
+    constexpr int blocks = 128, t = 256, room = 256;   // room: partials per reduction (the implicit one uses 256)
+    double *partial = nullptr, res[2] = {100, 0};
+    MPM_CUDA(h, cudaMallocAsync(&partial, (2 * room + 2) * sizeof(double), h->stream));
+    double* out = partial + 2 * room;
+    if(c.strong_cfl) {
+        if(h->sp.dim == 3) k_strong_cfl<T, 3><<<blocks, t, 0, h->stream>>>(a, (T)c.cfl, (T)c.cfl_F, partial);
+        else k_strong_cfl<T, 2><<<blocks, t, 0, h->stream>>>(a, (T)c.cfl, (T)c.cfl_F, partial);
+        k_fold<<<1, 32, 0, h->stream>>>(partial, blocks, 1, out);
+        MPM_LAUNCHED(h, "k_strong_cfl");
+    }
+    if(c.sound_cfl) {
+        if(h->implicit.enabled) {
+            int rc = implicit_max_sound_speed(h, partial + room, out + 1);
+            if(rc) return rc;
+        } else {
+            if(h->sp.dim == 3) k_sound_speed<T, 3><<<blocks, t, 0, h->stream>>>(a, partial + room);
+            else k_sound_speed<T, 2><<<blocks, t, 0, h->stream>>>(a, partial + room);
+            k_fold<<<1, 32, 0, h->stream>>>(partial + room, blocks, 0, out + 1);
+            MPM_LAUNCHED(h, "k_sound_speed");
+        }
+    }
+    MPM_CUDA(h, cudaMemcpyAsync(res, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaFreeAsync(partial, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    double nd = dt;
+    if(c.strong_cfl && (T)(dt * res[0]) < (T)nd) nd = (T)(dt * res[0]);
+    if(c.sound_cfl) {   // Limit_Dt_Sound_Speed, with Robust_Divide
+        T dxm = (T)h->sp.dx[0];
+        for(int k = 1; k < h->sp.dim; k++) dxm = dxm < (T)h->sp.dx[k] ? dxm : (T)h->sp.dx[k];
+        const T sp = (T)res[1];
+        T q;
+        if(fabs(sp) == (T)FLT_MAX) q = 0;
+        else if(fabs(sp) > 1 || fabs(dxm) < (T)FLT_MAX * fabs(sp)) q = dxm / sp;
+        else q = ((dxm > 0) == (sp >= 0)) ? (T)FLT_MAX : -(T)FLT_MAX;
+        const T nds = q * (T)c.cfl_sound;
+        nd = (T)nd < nds ? nd : (double)nds;
+    }
+    nd = (T)nd > (T)c.min_dt ? nd : c.min_dt;
+    if((T)nd >= (T)dt * (T)0.99) return MPM_OK;
+    const T sc = (T)nd / (T)dt;
+    k_scale_dt<T><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a, sc);
+    MPM_LAUNCHED(h, "k_scale_dt");
+    *dt_out = (double)(T)nd;
+    return MPM_OK;
+}
+
 // MPM_DRIVER::Update_Plasticity_And_Hardening (MPM_DRIVER.cpp:922-928) with
 // MPM_PLASTICITY_CLAMP, over the valid particles after G2P.
 template<class T, int d> __global__ void k_plastic_clamp(PlainArgs<T> a, T* Fp, const T* mu0, const T* lam0, Vec4<T> prm)
@@ -625,6 +777,10 @@ int plain_p2g(mpm_handle* h, double dt, double)
 int plain_forces(mpm_handle* h, double dt, double)
 {
     return h->model.precision == MPM_FP64 ? forces_t<double>(h, dt) : forces_t<float>(h, dt);
+}
+int plain_reduce_dt(mpm_handle* h, double dt, double* dt_out)
+{
+    return h->model.precision == MPM_FP64 ? reduce_dt_t<double>(h, dt, dt_out) : reduce_dt_t<float>(h, dt, dt_out);
 }
 int plain_g2p(mpm_handle* h, double dt, double)
 {

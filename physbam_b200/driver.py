@@ -93,6 +93,12 @@ class ImplicitStats(ctypes.Structure):
                 ("residual", ctypes.c_double)]
 
 
+class DtControlDesc(ctypes.Structure):
+    _fields_ = [("cfl", ctypes.c_double), ("min_dt", ctypes.c_double), ("max_dt", ctypes.c_double),
+                ("strong_cfl", ctypes.c_int), ("cfl_F", ctypes.c_double), ("sound_cfl", ctypes.c_int),
+                ("cfl_sound", ctypes.c_double)]
+
+
 # plastic-state keys (scenes.plastic_keys and the mu/lam pair) -> PlasticView fields
 _PLASTIC_FIELDS = {"Fp": "Fp", "mu": "mu", "lam": "lambda_", "mu0": "mu0", "lam0": "lambda0",
                    "pdef": "plastic_def", "rho_F": "rho_F", "cohesion": "cohesion", "vc": "vc"}
@@ -105,7 +111,7 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune", "mpm_particle_totals",
            "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex",
            "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state", "mpm_set_implicit",
-           "mpm_get_implicit_stats"]
+           "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt"]
 
 _lib = None
 
@@ -151,6 +157,10 @@ def load_library(path: str = LIB_PATH):
     L.mpm_set_plastic_state.argtypes = [P, ctypes.POINTER(PlasticView)]
     L.mpm_set_implicit.argtypes = [P, ctypes.POINTER(ImplicitDesc)]
     L.mpm_get_implicit_stats.argtypes = [P, ctypes.POINTER(ImplicitStats)]
+    L.mpm_set_dt_control.argtypes = [P, ctypes.POINTER(DtControlDesc)]
+    L.mpm_simulate_frame.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_int)]
+    L.mpm_last_dt.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
     L.mpm_status_string.argtypes = [ctypes.c_int]
     L.mpm_status_string.restype = ctypes.c_char_p
     for f in EXPORTS:
@@ -191,6 +201,8 @@ class MPM_DRIVER:
             self.set_plasticity(scene.plasticity)
         if scene.implicit is not None:
             self.set_implicit(scene.implicit)
+        if scene.dt_control is not None:
+            self.set_dt_control(scene.dt_control)
         self.time = 0.0
         self.n = 0
 
@@ -340,6 +352,29 @@ class MPM_DRIVER:
         v = self._dev_view(X, V, Fc, Bc, valid=valid)
         self._check(self.L.mpm_get_particles(self.h, ctypes.byref(v)), "mpm_get_particles")
         return X, V, Fc, Bc, valid
+
+    # -- adaptive substeps (Simulate_To_Frame) -------------------------------------
+    def set_dt_control(self, control: S.DtControl):
+        c = DtControlDesc()
+        c.cfl, c.min_dt, c.max_dt = control.cfl, control.min_dt, control.max_dt
+        c.strong_cfl, c.cfl_F = 1 if control.strong_cfl else 0, control.cfl_F
+        c.sound_cfl, c.cfl_sound = 1 if control.sound_cfl else 0, control.cfl_sound
+        self._check(self.L.mpm_set_dt_control(self.h, ctypes.byref(c)), "mpm_set_dt_control")
+        self.dt_control = control
+
+    def simulate_frame(self, frame_dt: Optional[float] = None) -> int:
+        """MPM_DRIVER::Simulate_To_Frame for one frame; returns the substeps taken."""
+        frame_dt = self.dt_control.frame_dt if frame_dt is None else frame_dt
+        t, n = ctypes.c_double(), ctypes.c_int()
+        self._check(self.L.mpm_simulate_frame(self.h, self.time, frame_dt, ctypes.byref(t), ctypes.byref(n)),
+                    "mpm_simulate_frame")
+        self.time = t.value
+        return n.value
+
+    def last_dt(self) -> float:
+        x = ctypes.c_double()
+        self._check(self.L.mpm_last_dt(self.h, ctypes.byref(x)), "mpm_last_dt")
+        return x.value
 
     # -- backward Euler ---------------------------------------------------------
     def set_implicit(self, implicit: Optional[S.Implicit]):

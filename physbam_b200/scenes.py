@@ -127,6 +127,23 @@ class Implicit:
 
 
 @dataclasses.dataclass
+class DtControl:
+    """Adaptive substeps as MPM_DRIVER::Simulate_To_Frame takes them (`MPM_DRIVER.cpp:161-201`):
+    dt = Compute_Dt (the affine CFL bound, `cfl`) clamped to [min_dt, max_dt] and fitted to
+    the frame end, then Reduce_Dt after the forces (l.519-545): the strong CFL of
+    Grid_To_Particle_Limit_Dt (`cfl_F` on the change of F, `cfl` on the displacement) and
+    the sound-speed CFL (`cfl_sound`), each when switched on (`MPM_EXAMPLE.h:84-115`)."""
+    frame_dt: float = 1.0 / 24
+    cfl: float = 1.0
+    min_dt: float = 0.0
+    max_dt: float = 1.0 / 24
+    strong_cfl: bool = False
+    cfl_F: float = 0.5
+    sound_cfl: bool = False
+    cfl_sound: float = 0.9
+
+
+@dataclasses.dataclass
 class Scene:
     name: str
     dim: int
@@ -148,6 +165,7 @@ class Scene:
     lam: np.ndarray
     plasticity: Optional[Plasticity] = None
     implicit: Optional[Implicit] = None
+    dt_control: Optional[DtControl] = None     # set: nsteps counts frames of frame_dt
 
     @property
     def n(self) -> int:
@@ -408,6 +426,24 @@ def small_2d_implicit(seed=43, G=16, nsteps=10, dt=1e-3):
     return s
 
 
+def small_3d_adaptive(seed=51, G=16, nframes=3):
+    """A stiff small_3d (E 2e6..8e6) run frame by frame as Simulate_To_Frame does,
+    with the strong and the sound-speed CFL on: the sound speed shortens most steps."""
+    s = small_3d(seed=seed, G=G, nsteps=nframes, E=(2e6, 8e6))
+    s.name = "small3dadaptive"
+    s.dt_control = DtControl(frame_dt=1e-3, cfl=0.5, min_dt=1e-7, max_dt=5e-4, strong_cfl=True, cfl_F=0.01,
+                             sound_cfl=True, cfl_sound=0.5)
+    return s
+
+
+def small_2d_adaptive(seed=53, G=16, nframes=3):
+    """small_2d run frame by frame with the strong CFL only (a tight cfl_F)."""
+    s = small_2d(seed=seed, G=G, nsteps=nframes)
+    s.name = "small2dadaptive"
+    s.dt_control = DtControl(frame_dt=2e-3, cfl=0.5, min_dt=1e-7, max_dt=1e-3, strong_cfl=True, cfl_F=0.002)
+    return s
+
+
 def small_sand_3d(seed=31, G=16, nsteps=20, dt=1e-4):
     """A small sand block (St. Venant-Kirchhoff Hencky + Drucker-Prager with Mast hardening)
     thrown against a sticky floor; a random initial F per particle, compressed by 3 % for
@@ -455,7 +491,7 @@ def snowballs_3d(seed=1234, G=128, ppc=8, E=1.4e5, nu=0.2, density=400.0, dt=5e-
 # --------------------------------------------------------------------------------------------
 # Scene file: read by the reference runner (oracle/ref_scene.cpp) and by the C oracle harness.
 # --------------------------------------------------------------------------------------------
-MAGIC = b"MPMSCN02"
+MAGIC = b"MPMSCN03"
 
 
 def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
@@ -466,9 +502,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         f.write(MAGIC)
         counts = list(s.counts) + [1] * (3 - d)
         pl = s.plasticity
-        im = s.implicit
-        f.write(struct.pack("<10i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
-                            1 if im else 0))
+        im, dc = s.implicit, s.dt_control
+        f.write(struct.pack("<11i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
+                            1 if im else 0, 1 if dc else 0))
         f.write(struct.pack("<11d", *pad3(s.domain_min), *pad3(s.domain_max), *pad3(s.gravity), s.dt, 0.0))
         f.write(struct.pack("<%di" % len(dumps), *dumps))
         for o in s.objects:
@@ -479,6 +515,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         if im:
             f.write(struct.pack("<4d", im.newton_tolerance, im.newton_iterations, im.solver_tolerance,
                                 im.solver_iterations))
+        if dc:
+            f.write(struct.pack("<8d", dc.frame_dt, dc.cfl, dc.min_dt, dc.max_dt, 1.0 if dc.strong_cfl else 0.0,
+                                dc.cfl_F, 1.0 if dc.sound_cfl else 0.0, dc.cfl_sound))
         f.write(struct.pack("<q", s.n))
         f.write(np.ascontiguousarray(s.X, np.float64).tobytes())
         f.write(np.ascontiguousarray(s.V, np.float64).tobytes())

@@ -36,6 +36,9 @@ CASES = {
     # backward Euler (the reference's default solve), Newton tolerances as MPM_EXAMPLE's defaults
     "small3d_implicit": (lambda: S.small_3d_implicit(), [0, 1, 9], [0, 9]),
     "small2d_implicit": (lambda: S.small_2d_implicit(), [0, 9], [0, 9]),
+    # Simulate_To_Frame with Compute_Dt and Reduce_Dt (steps are frames; substep counts kept)
+    "small3d_adaptive": (lambda: S.small_3d_adaptive(), [0, 2], [2]),
+    "small2d_adaptive": (lambda: S.small_2d_adaptive(), [0, 2], [2]),
     # sand: ST_VENANT_KIRCHHOFF_HENCKY_STRAIN + MPM_DRUCKER_PRAGER (Fp, plastic_def, rho_F, sigma_Y, vc dumped)
     "smallsand3d_hencky": (lambda: S.small_sand_3d(), [0, 1, 19], [0, 19]),
     "smallsand2d_hencky": (lambda: S.small_sand_2d(), [0, 19], [19]),
@@ -51,6 +54,9 @@ def main(names=None):
             continue
         scene = make()
         ref = oracle.run_reference(scene, dumps, threads=1)
+        frames = None
+        if scene.dt_control is not None:
+            ref, frames = ref
         arrays = dict(
             dim=scene.dim, counts=np.array(scene.counts), dmin=np.array(scene.domain_min),
             dmax=np.array(scene.domain_max), model=scene.model, gravity=np.array(scene.gravity),
@@ -65,6 +71,11 @@ def main(names=None):
         pl = scene.plasticity
         if pl is not None:
             arrays["plasticity"] = np.array(S.plastic_params(pl), np.float64)
+        dc = scene.dt_control
+        if dc is not None:
+            arrays["dt_control"] = np.array([dc.frame_dt, dc.cfl, dc.min_dt, dc.max_dt, float(dc.strong_cfl), dc.cfl_F,
+                                             float(dc.sound_cfl), dc.cfl_sound])
+            arrays["frame_substeps"] = np.array(frames["frame_substeps"], np.int32)
         im = scene.implicit
         if im is not None:
             arrays["implicit"] = np.array([im.newton_tolerance, im.newton_iterations, im.solver_tolerance,
@@ -92,6 +103,12 @@ def load(name):
                     z["volume"].copy(), z["mu"].copy(), z["lam"].copy())
     if "plasticity" in z:
         scene.plasticity = S.plastic_from_params(z["plasticity"])
+    if "dt_control" in z:
+        c = z["dt_control"]
+        scene.dt_control = S.DtControl(float(c[0]), float(c[1]), float(c[2]), float(c[3]), bool(c[4]), float(c[5]),
+                                       bool(c[6]), float(c[7]))
+        dumps_meta = {"frame_substeps": [int(x) for x in z["frame_substeps"]]}
+        scene.frame_substeps = dumps_meta["frame_substeps"]
     if "implicit" in z:
         im = z["implicit"]
         scene.implicit = S.Implicit(float(im[0]), int(im[1]), float(im[2]), int(im[3]))
