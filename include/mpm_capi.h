@@ -282,6 +282,24 @@ int mpm_set_dt_control(mpm_handle* h, const mpm_dt_control* c);
 int mpm_simulate_frame(mpm_handle* h, double time, double frame_dt, double* time_out, int* substeps);
 int mpm_last_dt(mpm_handle* h, double* dt);
 
+/* Reflection boundary conditions on the faces of the grid domain (MPM_EXAMPLE::
+ * reflection_bc, side_bc_type; MPM_DRIVER.cpp:307-446, 1219-1239): the ghost
+ * layer mirrors the interior.  Per side (-x, +x, -y, +y, -z, +z) free, slip,
+ * no-slip or separating.  Without full_reflection, mass and momentum are
+ * folded across each face after P2G, forces after the force computation and
+ * velocities after the grid update; with full_reflection the velocities are
+ * reflected once with Coulomb friction (`friction`) instead (scenes without
+ * collision objects).  A particle that crosses a non-free face is mirrored
+ * back (position and velocity) instead of being invalidated.  Plain path. */
+enum mpm_bc_type { MPM_BC_FREE = 0, MPM_BC_SLIP = 1, MPM_BC_NOSLIP = 2, MPM_BC_SEP = 3 };
+typedef struct {
+    int enabled;
+    int side_type[6];
+    double friction;
+    int full_reflection;
+} mpm_reflection_desc;
+int mpm_set_reflection(mpm_handle* h, const mpm_reflection_desc* r);
+
 /* ---- inspection ---------------------------------------------------------- */
 
 /* Grids of the last substep as doubles on the host, each (G+6)^d nodes (times

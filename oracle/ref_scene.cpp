@@ -48,7 +48,8 @@ namespace {
 struct OBJ { int kind, type; double friction, a[3], b[3]; };
 struct SCENE_FILE
 {
-    int dim, counts[3], model, nsteps, nobj, ndump, plasticity, implicit, dt_control;
+    int dim, counts[3], model, nsteps, nobj, ndump, plasticity, implicit, dt_control, reflection;
+    double refl[8];   // side types (6), friction, full
     // frame_dt, cfl, min_dt, max_dt, strong_cfl, cfl_F, sound_cfl, cfl_sound
     double dtc[8];
     double implicit_prm[4];   // newton_tolerance, newton_iterations, solver_tolerance, solver_iterations
@@ -73,10 +74,11 @@ SCENE_FILE Read_Scene(const char* path)
     if(!f) throw std::runtime_error("cannot open scene");
     char magic[8];
     rd(f, magic, 8);
-    if(memcmp(magic, "MPMSCN03", 8)) throw std::runtime_error("bad scene magic");
+    if(memcmp(magic, "MPMSCN04", 8)) throw std::runtime_error("bad scene magic");
     SCENE_FILE s;
-    int hdr[11];
-    rd(f, hdr, 11);
+    int hdr[12];
+    rd(f, hdr, 12);
+    s.reflection = hdr[11];
     s.implicit = hdr[9];
     s.dt_control = hdr[10];
     s.dim = hdr[0]; s.counts[0] = hdr[1]; s.counts[1] = hdr[2]; s.counts[2] = hdr[3];
@@ -97,6 +99,7 @@ SCENE_FILE Read_Scene(const char* path)
     else if(s.plasticity) throw std::runtime_error("unknown plasticity");
     if(s.implicit) rd(f, s.implicit_prm, 4);
     if(s.dt_control) rd(f, s.dtc, 8);
+    if(s.reflection) rd(f, s.refl, 8);
     rd(f, &s.n, 1);
     size_t n = s.n, d = s.dim;
     s.X.resize(n * d); s.V.resize(n * d); s.F.resize(n * d * d); s.B.resize(n * d * d);
@@ -133,6 +136,12 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
         this->use_affine = true;
         this->flip = 0;
         this->min_dt = this->max_dt = (T)s.dt;
+        if(s.reflection) {   // as Add_Walls sets them with -use_reflect (STANDARD_TESTS_BASE.cpp:487-511)
+            this->reflection_bc = true;
+            for(int k = 0; k < 2 * TV::m; k++) this->side_bc_type(k) = (typename BASE::BC_TYPE)(int)s.refl[k];
+            this->reflection_bc_friction = (T)s.refl[6];
+            this->use_full_reflection = s.refl[7] != 0;
+        }
         if(s.dt_control) {   // Simulate_To_Frame with MPM_EXAMPLE's step controls
             this->frame_dt = (T)s.dtc[0];
             this->cfl = (T)s.dtc[1];

@@ -239,6 +239,8 @@ int mpm_set_stream(mpm_handle* h, void* stream)
 int mpm_set_collision_objects(mpm_handle* h, const mpm_collision_object* objs, int count)
 {
     if(!h || count < 0 || count > MPM_MAX_OBJECTS || (count && !objs)) return MPM_ERR_ARG;
+    if(count && h->reflect.enabled && h->reflect.full_reflection)
+        return set_error(h, MPM_ERR_ARG, "full reflection is built for scenes without collision objects");
     for(int i = 0; i < count; i++) {
         const mpm_collision_object& o = objs[i];
         if(o.kind != MPM_BOX && o.kind != MPM_PLANE) return set_error(h, MPM_ERR_ARG, "unknown object kind");
@@ -474,6 +476,24 @@ int mpm_set_implicit(mpm_handle* h, const mpm_implicit_desc* d)
     release_graph(h);
     h->implicit = *d;
     h->implicit.enabled = d->enabled ? 1 : 0;
+    return MPM_OK;
+}
+
+int mpm_set_reflection(mpm_handle* h, const mpm_reflection_desc* r)
+{
+    if(!h || !r) return MPM_ERR_ARG;
+    if(r->enabled) {
+        if(fast(h)) return set_error(h, MPM_ERR_ARG, "reflection boundary conditions run on the plain path");
+        for(int k = 0; k < 2 * h->sp.dim; k++)
+            if(r->side_type[k] < MPM_BC_FREE || r->side_type[k] > MPM_BC_SEP) return set_error(h, MPM_ERR_ARG, "side type");
+        if(!(r->friction >= 0) || !std::isfinite(r->friction)) return set_error(h, MPM_ERR_ARG, "reflection friction");
+        if(r->full_reflection && h->sp.nobj)
+            return set_error(h, MPM_ERR_ARG, "full reflection is built for scenes without collision objects");
+    }
+    release_graph(h);
+    h->reflect = *r;
+    h->reflect.enabled = r->enabled ? 1 : 0;
+    for(int k = 2 * h->sp.dim; k < 6; k++) h->reflect.side_type[k] = MPM_BC_FREE;
     return MPM_OK;
 }
 

@@ -819,6 +819,8 @@ template<class T, int d> struct Solver {
         }
         if(s.n) k_imp_restore<T, d><<<pb, 128, 0, st>>>(ia);
         k_imp_finish<T, d><<<gb, 256, 0, st>>>(ia, dv, v[V_VFS]);
+        // Reflect_Boundary_Velocity on velocity and velocity_friction_save (MPM_DRIVER.cpp:1055-1057)
+        if(h->reflect.enabled && !h->reflect.full_reflection) plain_reflect_velocity(h);
         check("implicit finish");
         h->imp_stats.newton_iterations = iters;
         h->imp_stats.krylov_iterations = krylov_total;

@@ -137,6 +137,7 @@ struct mpm_handle {
     mpm_plasticity_desc plastic{};   // kind MPM_PLASTICITY_NONE: off
     mpm_implicit_desc implicit{};    // enabled 0: symplectic Euler
     mpm_dt_control dt_control{};     // Compute_Dt / Reduce_Dt controls
+    mpm_reflection_desc reflect{};   // reflection boundary conditions (enabled 0: none)
     double last_dt = 0;              // step the last substep took (Reduce_Dt may shorten it)
     mpm_implicit_stats imp_stats{};  // of the last implicit solve
     ImplicitState* imp = nullptr;
@@ -198,6 +199,7 @@ int plain_grid_totals(mpm_handle* h, mpm_totals* out);
 int plain_implicit_forces(mpm_handle* h, double dt, double time);
 int implicit_max_sound_speed(mpm_handle* h, double* partial, double* out);
 int plain_reduce_dt(mpm_handle* h, double dt, double* dt_out);
+int plain_reflect_velocity(mpm_handle* h);
 void implicit_free(mpm_handle* h);
 
 // adjoint (mpm_adjoint.cu)

@@ -205,15 +205,24 @@ template<class T, int d> __global__ void k_g2p(PlainArgs<T> a)
             Bp[r + d * c] = Bh[r + d * c] - (T).5 * (Vpf[r] * (X[c] + xn[c]) + (X[r] - xn[r]) * Vpf[c]);
 #pragma unroll
     for(int e = 0; e < d * d; e++) { Fp[e] = Fn[e]; finite = finite && isfinite(Fn[e]); }
+    // Reflect_Or_Invalidate_Particle (l.1219-1239): mirrored back across a
+    // non-free face, invalidated across a free one
     bool keep = true;
 #pragma unroll
     for(int k = 0; k < d; k++) {
-        X[k] = xn[k];
-        a.V[p * d + k] = Vpf[k];
         finite = finite && isfinite(xn[k]) && isfinite(Vpf[k]);
         T eps = Lim<T>::eps * 4 * ((T)a.sp.dmax[k] - (T)a.sp.dmin[k]);
-        if(xn[k] < (T)a.sp.dmin[k] + eps) keep = false;
-        else if(xn[k] > (T)a.sp.dmax[k] - eps) keep = false;
+        const T A = (T)a.sp.dmin[k] + eps, B = (T)a.sp.dmax[k] - eps;
+        T x = xn[k], v = Vpf[k];
+        if(x < A) {
+            if(a.side[2 * k] != MPM_BC_FREE) { x = 2 * A - x; v = -v; }
+            else keep = false;
+        } else if(x > B) {
+            if(a.side[2 * k + 1] != MPM_BC_FREE) { x = 2 * B - x; v = -v; }
+            else keep = false;
+        }
+        X[k] = x;
+        a.V[p * d + k] = v;
     }
     if(!finite) { atomicOr(a.flags, MPM_FLAG_NAN); keep = false; }
     // a particle that leaves is marked 2 while plasticity still has to see it
@@ -238,6 +247,189 @@ int gblocks(mpm_handle* h, int64_t n, int t)
 
 size_t esize(mpm_handle* h) { return h->model.precision == MPM_FP64 ? 8 : 4; }
 
+// ---------------------------------------------------------------------------
+// Reflection boundary conditions (MPM_DRIVER.cpp:307-446).  One launch per
+// side, in side order, over that side's ghost slab including the corner
+// blocks (RANGE_ITERATOR with RI::ghost | RI::duplicate_corners): each ghost
+// node pairs with its mirror image across the face, image = 2 face - index - 1
+// along the side's axis.  No velocity boundary function (bc = 0).
+// ---------------------------------------------------------------------------
+template<class T, int d> __device__ __forceinline__ bool slab_node(const PlainArgs<T>& a, int side, int64_t t,
+    int64_t& ghost, int64_t& image)
+{
+    const int axis = side / 2, hi = side % 2;
+    int idx[3];
+    int64_t r = t;
+    for(int k = d - 1; k >= 0; k--) {
+        const int ext = k == axis ? MPM_GHOST : a.gs[k];
+        idx[k] = (int)(r % ext);
+        r /= ext;
+    }
+    if(r) return false;
+    const int G = a.gs[axis] - 2 * MPM_GHOST;
+    // ghost layer along the axis, in cell coordinates, and its mirror
+    const int c = hi ? G + idx[axis] : idx[axis] - MPM_GHOST;
+    const int cm = hi ? 2 * G - c - 1 : -c - 1;
+    int gi[3], ii[3];
+    for(int k = 0; k < d; k++) { gi[k] = idx[k]; ii[k] = idx[k]; }
+    gi[axis] = c + MPM_GHOST;
+    ii[axis] = cm + MPM_GHOST;
+    ghost = image = 0;
+    for(int k = 0; k < d; k++) { ghost = ghost * a.gs[k] + gi[k]; image = image * a.gs[k] + ii[k]; }
+    return true;
+}
+
+template<class T, int d> __device__ __forceinline__ int64_t slab_size(const PlainArgs<T>& a, int side)
+{
+    int64_t n = MPM_GHOST;
+    for(int k = 0; k < d; k++) if(k != side / 2) n *= a.gs[k];
+    return n;
+}
+
+// Reflect_Boundary_Mass_Momentum (l.310-341): both nodes take the total mass;
+// momentum sums (free), differences (no-slip) or sums with the normal part
+// differenced (slip, separate).
+template<class T, int d> __global__ void k_reflect_mm(PlainArgs<T> a, int side)
+{
+    const int type = a.side[side], axis = side / 2;
+    for(int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < slab_size<T, d>(a, side); t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o, i;
+        if(!slab_node<T, d>(a, side, t, o, i)) continue;
+        const T mt = a.gm[i] + a.gm[o];
+        T vi[3], vo[3];
+        for(int k = 0; k < d; k++) {
+            const T mi = a.gmv[i * d + k], mo = a.gmv[o * d + k];
+            T id = mi - mo, od = -id, in = mi + mo, on = in;
+            if(type == MPM_BC_SLIP && k == axis) { in = id; on = od; }
+            if(type == MPM_BC_NOSLIP) { vi[k] = id; vo[k] = od; }
+            else { vi[k] = in; vo[k] = on; }
+        }
+        for(int k = 0; k < d; k++) { a.gmv[i * d + k] = vi[k]; a.gmv[o * d + k] = vo[k]; }
+        a.gm[i] = a.gm[o] = mt;
+    }
+}
+
+// Reflect_Boundary_Force (l.424-446), the same folding on the forces.
+template<class T, int d> __global__ void k_reflect_force(PlainArgs<T> a, int side)
+{
+    const int type = a.side[side], axis = side / 2;
+    for(int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < slab_size<T, d>(a, side); t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o, i;
+        if(!slab_node<T, d>(a, side, t, o, i)) continue;
+        T fi[3], fo[3];
+        for(int k = 0; k < d; k++) {
+            const T xi = a.gf[i * d + k], xo = a.gf[o * d + k];
+            T id = xi - xo, od = -id, in = xi + xo, on = in;
+            if(type == MPM_BC_SLIP && k == axis) { in = id; on = od; }
+            if(type == MPM_BC_NOSLIP) { fi[k] = id; fo[k] = od; }
+            else { fi[k] = in; fo[k] = on; }
+        }
+        for(int k = 0; k < d; k++) { a.gf[i * d + k] = fi[k]; a.gf[o * d + k] = fo[k]; }
+    }
+}
+
+// Reflect_Boundary_Velocity (l.397-421): the ghost node (with mass) takes its
+// image's velocity, reversed (no-slip) or with the normal part reversed (slip).
+template<class T, int d> __global__ void k_reflect_vel(PlainArgs<T> a, int side, T* u)
+{
+    const int type = a.side[side], axis = side / 2;
+    for(int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < slab_size<T, d>(a, side); t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o, i;
+        if(!slab_node<T, d>(a, side, t, o, i) || a.gm[o] == 0) continue;
+        for(int k = 0; k < d; k++) {
+            const T vi = u[i * d + k];
+            T od = -vi, on = vi;
+            if(type == MPM_BC_SLIP && k == axis) on = od;
+            u[o * d + k] = type == MPM_BC_NOSLIP ? od : on;
+        }
+    }
+}
+
+// Reflect_Boundary_Friction with Reflect_Helper (l.342-395): the mass-weighted
+// pair velocities, separated with Coulomb friction for BC_SEP.
+template<class T, int d> __global__ void k_reflect_friction(PlainArgs<T> a, int side, T mu)
+{
+    const int type = a.side[side], axis = side / 2, hi = side % 2;
+    for(int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < slab_size<T, d>(a, side); t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t o, i;
+        if(!slab_node<T, d>(a, side, t, o, i)) continue;
+        const T mi = a.gm[i], mo = a.gm[o];
+        if(!mi || !mo) continue;
+        T vi[3], vo[3], ri[3], ro[3];
+        for(int k = 0; k < d; k++) { vi[k] = a.gv[i * d + k]; vo[k] = a.gv[o * d + k]; }
+        const T mt = mi + mo, ai = mi / mt, ao = 1 - ai;
+        T in[3], id[3], od[3];
+        for(int k = 0; k < d; k++) {
+            in[k] = ai * vi[k] + ao * vo[k];
+            id[k] = ai * vi[k] + ao * (-vo[k]);
+            od[k] = ao * vo[k] + ai * (-vi[k]);
+        }
+        if(type == MPM_BC_FREE) {
+            for(int k = 0; k < d; k++) ri[k] = ro[k] = in[k];
+        } else if(type == MPM_BC_NOSLIP) {
+            for(int k = 0; k < d; k++) { ri[k] = id[k]; ro[k] = od[k]; }
+        } else if(type == MPM_BC_SLIP) {
+            for(int k = 0; k < d; k++) { ri[k] = ro[k] = in[k]; }
+            ri[axis] = id[axis];
+            ro[axis] = od[axis];
+        } else {
+            const T dv = 2 * ao * ai * (-vi[axis] - vo[axis]);
+            const T dvn = hi ? -dv : dv;
+            if(dvn < 0) {
+                for(int k = 0; k < d; k++) { ri[k] = vi[k]; ro[k] = vo[k]; }
+            } else {
+                T idn[3] = {0, 0, 0}, odn[3] = {0, 0, 0}, tv[3];
+                idn[axis] = id[axis];
+                odn[axis] = od[axis];
+                for(int k = 0; k < d; k++) tv[k] = in[k];
+                tv[axis] = 0;
+                T mag = 0;
+                for(int k = 0; k < d; k++) mag += tv[k] * tv[k];
+                mag = sqrt(mag);
+                if(mag) { const T inv = 1 / mag; for(int k = 0; k < d; k++) tv[k] *= inv; }
+                else for(int k = 0; k < d; k++) tv[k] = k == 0 ? (T)1 : (T)0;   // VECTOR::Normalize
+                const T r = mag - mu * dvn;
+                for(int k = 0; k < d; k++) {
+                    ri[k] = r < 0 ? idn[k] : idn[k] + r * tv[k];
+                    ro[k] = r < 0 ? odn[k] : odn[k] + r * tv[k];
+                }
+            }
+        }
+        for(int k = 0; k < d; k++) { a.gv[i * d + k] = ri[k]; a.gv[o * d + k] = ro[k]; }
+    }
+}
+
+template<class T> __global__ void k_copy_vf(PlainArgs<T> a)
+{
+    const int d = a.sp.dim;
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.gn * d; i += (int64_t)gridDim.x * blockDim.x) a.gvf[i] = a.gv[i];
+}
+
+enum ReflectPass { REFLECT_MM, REFLECT_FORCE, REFLECT_VEL, REFLECT_FRICTION };
+
+template<class T> int reflect_pass(mpm_handle* h, const PlainArgs<T>& a, ReflectPass pass)
+{
+    const int d = h->sp.dim, t = 256;
+    for(int side = 0; side < 2 * d; side++) {
+        int64_t n = MPM_GHOST;
+        for(int k = 0; k < d; k++) if(k != side / 2) n *= a.gs[k];
+        const int b = gblocks(h, n, t);
+        if(d == 3) {
+            if(pass == REFLECT_MM) k_reflect_mm<T, 3><<<b, t, 0, h->stream>>>(a, side);
+            else if(pass == REFLECT_FORCE) k_reflect_force<T, 3><<<b, t, 0, h->stream>>>(a, side);
+            else if(pass == REFLECT_FRICTION) k_reflect_friction<T, 3><<<b, t, 0, h->stream>>>(a, side, (T)h->reflect.friction);
+            else { k_reflect_vel<T, 3><<<b, t, 0, h->stream>>>(a, side, a.gv); k_reflect_vel<T, 3><<<b, t, 0, h->stream>>>(a, side, a.gvf); }
+        } else {
+            if(pass == REFLECT_MM) k_reflect_mm<T, 2><<<b, t, 0, h->stream>>>(a, side);
+            else if(pass == REFLECT_FORCE) k_reflect_force<T, 2><<<b, t, 0, h->stream>>>(a, side);
+            else if(pass == REFLECT_FRICTION) k_reflect_friction<T, 2><<<b, t, 0, h->stream>>>(a, side, (T)h->reflect.friction);
+            else { k_reflect_vel<T, 2><<<b, t, 0, h->stream>>>(a, side, a.gv); k_reflect_vel<T, 2><<<b, t, 0, h->stream>>>(a, side, a.gvf); }
+        }
+    }
+    MPM_LAUNCHED(h, "k_reflect_*");
+    return MPM_OK;
+}
+
 template<class T> int p2g_t(mpm_handle* h, double dt)
 {
     PlainArgs<T> a = args<T>(h, dt);
@@ -252,6 +444,10 @@ template<class T> int p2g_t(mpm_handle* h, double dt)
         else k_p2g<T, 2><<<pblocks(a.n, t), t, 0, h->stream>>>(a);
         timer_end(h, slot);
         MPM_LAUNCHED(h, "k_p2g");
+    }
+    if(a.reflect && !h->reflect.full_reflection) {
+        int rc = reflect_pass<T>(h, a, REFLECT_MM);
+        if(rc) return rc;
     }
     slot = timer_begin(h, "plain_normalize");
     k_normalize<T><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a);
@@ -276,11 +472,25 @@ template<class T> int forces_t(mpm_handle* h, double dt)
         timer_end(h, slot);
         MPM_LAUNCHED(h, "k_forces");
     }
+    if(a.reflect && !h->reflect.full_reflection) {
+        int rc = reflect_pass<T>(h, a, REFLECT_FORCE);
+        if(rc) return rc;
+    }
     int slot = timer_begin(h, "plain_grid_update");
     if(h->sp.dim == 3) k_grid_update<T, 3><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a);
     else k_grid_update<T, 2><<<gblocks(h, a.gn, t), t, 0, h->stream>>>(a);
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_grid_update");
+    if(a.reflect) {
+        if(h->reflect.full_reflection) {   // no collision objects: the friction velocity is the velocity
+            int rc = reflect_pass<T>(h, a, REFLECT_FRICTION);
+            if(rc) return rc;
+            k_copy_vf<T><<<gblocks(h, a.gn * h->sp.dim, t), t, 0, h->stream>>>(a);
+            MPM_LAUNCHED(h, "k_copy_vf");
+        } else {
+            return reflect_pass<T>(h, a, REFLECT_VEL);
+        }
+    }
     return MPM_OK;
 }
 
@@ -777,6 +987,11 @@ int plain_p2g(mpm_handle* h, double dt, double)
 int plain_forces(mpm_handle* h, double dt, double)
 {
     return h->model.precision == MPM_FP64 ? forces_t<double>(h, dt) : forces_t<float>(h, dt);
+}
+int plain_reflect_velocity(mpm_handle* h)
+{
+    if(h->model.precision == MPM_FP64) return reflect_pass<double>(h, args<double>(h, 0.0), REFLECT_VEL);
+    return reflect_pass<float>(h, args<float>(h, 0.0), REFLECT_VEL);
 }
 int plain_reduce_dt(mpm_handle* h, double dt, double* dt_out)
 {

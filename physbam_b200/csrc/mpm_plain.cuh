@@ -19,6 +19,8 @@ template<class T> struct PlainArgs {
     T dt;
     unsigned* flags;
     int mark_left;
+    int reflect;          // reflection boundary conditions on
+    int side[6];          // their types per side (mpm_bc_type)
 };
 
 template<class T, int d> struct Stencil {
@@ -85,6 +87,8 @@ template<class T> inline PlainArgs<T> args(mpm_handle* h, double dt)
     a.dt = (T)dt;
     a.flags = h->d_flags;
     a.mark_left = h->plastic.kind != MPM_PLASTICITY_NONE;
+    a.reflect = h->reflect.enabled;
+    for(int k = 0; k < 6; k++) a.side[k] = h->reflect.enabled ? h->reflect.side_type[k] : MPM_BC_FREE;
     return a;
 }
 

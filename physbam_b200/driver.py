@@ -99,6 +99,11 @@ class DtControlDesc(ctypes.Structure):
                 ("cfl_sound", ctypes.c_double)]
 
 
+class ReflectionDesc(ctypes.Structure):
+    _fields_ = [("enabled", ctypes.c_int), ("side_type", ctypes.c_int * 6), ("friction", ctypes.c_double),
+                ("full_reflection", ctypes.c_int)]
+
+
 # plastic-state keys (scenes.plastic_keys and the mu/lam pair) -> PlasticView fields
 _PLASTIC_FIELDS = {"Fp": "Fp", "mu": "mu", "lam": "lambda_", "mu0": "mu0", "lam0": "lambda0",
                    "pdef": "plastic_def", "rho_F": "rho_F", "cohesion": "cohesion", "vc": "vc"}
@@ -111,7 +116,8 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune", "mpm_particle_totals",
            "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex",
            "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state", "mpm_set_implicit",
-           "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt"]
+           "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt",
+           "mpm_set_reflection"]
 
 _lib = None
 
@@ -161,6 +167,7 @@ def load_library(path: str = LIB_PATH):
     L.mpm_simulate_frame.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_int)]
     L.mpm_last_dt.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+    L.mpm_set_reflection.argtypes = [P, ctypes.POINTER(ReflectionDesc)]
     L.mpm_status_string.argtypes = [ctypes.c_int]
     L.mpm_status_string.restype = ctypes.c_char_p
     for f in EXPORTS:
@@ -203,6 +210,8 @@ class MPM_DRIVER:
             self.set_implicit(scene.implicit)
         if scene.dt_control is not None:
             self.set_dt_control(scene.dt_control)
+        if scene.reflection is not None:
+            self.set_reflection(scene.reflection)
         self.time = 0.0
         self.n = 0
 
@@ -352,6 +361,16 @@ class MPM_DRIVER:
         v = self._dev_view(X, V, Fc, Bc, valid=valid)
         self._check(self.L.mpm_get_particles(self.h, ctypes.byref(v)), "mpm_get_particles")
         return X, V, Fc, Bc, valid
+
+    # -- reflection boundary conditions -----------------------------------------
+    def set_reflection(self, reflection: Optional[S.Reflection]):
+        r = ReflectionDesc()
+        if reflection is not None:
+            r.enabled = 1
+            for k, t in enumerate(reflection.side_type):
+                r.side_type[k] = int(t)
+            r.friction, r.full_reflection = reflection.friction, 1 if reflection.full else 0
+        self._check(self.L.mpm_set_reflection(self.h, ctypes.byref(r)), "mpm_set_reflection")
 
     # -- adaptive substeps (Simulate_To_Frame) -------------------------------------
     def set_dt_control(self, control: S.DtControl):

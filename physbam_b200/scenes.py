@@ -143,6 +143,20 @@ class DtControl:
     cfl_sound: float = 0.9
 
 
+BC_FREE, BC_SLIP, BC_NOSLIP, BC_SEP = 0, 1, 2, 3
+
+
+@dataclasses.dataclass
+class Reflection:
+    """Reflection boundary conditions on the domain faces (MPM_EXAMPLE::reflection_bc,
+    side_bc_type per side -x +x -y +y -z +z; `MPM_DRIVER.cpp:307-446`), as
+    `STANDARD_TESTS_BASE::Add_Walls` sets them with -use_reflect (slip, separate or
+    no-slip walls; `full` is -use_reflect_friction, with `friction`)."""
+    side_type: Sequence[int] = (BC_SLIP, BC_SLIP, BC_NOSLIP, BC_FREE, BC_SLIP, BC_SLIP)
+    friction: float = 0.0
+    full: bool = False
+
+
 @dataclasses.dataclass
 class Scene:
     name: str
@@ -166,6 +180,7 @@ class Scene:
     plasticity: Optional[Plasticity] = None
     implicit: Optional[Implicit] = None
     dt_control: Optional[DtControl] = None     # set: nsteps counts frames of frame_dt
+    reflection: Optional[Reflection] = None
 
     @property
     def n(self) -> int:
@@ -444,6 +459,42 @@ def small_2d_adaptive(seed=53, G=16, nframes=3):
     return s
 
 
+def small_3d_reflect(seed=61, G=16, nsteps=20, dt=1e-4):
+    """A block in the domain's low corner thrown at the faces, with reflection
+    boundary conditions instead of wall objects: slip on x, no-slip floor, a free
+    top, separate on -z and slip on +z; particles cross the faces and are mirrored."""
+    rng = np.random.default_rng(seed)
+    dim, counts = 3, [G, G, G]
+    dmin, dmax = np.zeros(3), np.ones(3)
+    lo, hi = np.array([0.001, 0.002, 0.0015]), np.array([0.3, 0.3, 0.28])
+    X = _seed_cells(rng, dim, counts, dmin, 1.0 / G, lo, hi, 8, lambda P: np.all((P >= lo) & (P < hi), axis=1))
+    Ep = np.exp(rng.uniform(np.log(2e4), np.log(8e4), X.shape[0]))
+    V = np.tile(np.array([-8.0, -10.0, -6.0]), (X.shape[0], 1)) + 2.0 * np.cross(np.array([0.2, 1.0, 0.3]), X - 0.15)
+    s = _finish("small3dreflect", dim, counts, dmin, dmax, COROTATED, [0, -9.8, 0], dt, nsteps, [], X, V, Ep, 0.3,
+                1000.0, 8)
+    s.F = np.eye(3) + 0.05 * rng.standard_normal((s.n, 3, 3))
+    s.B = 0.3 * rng.standard_normal(s.B.shape) / G
+    s.reflection = Reflection(side_type=(BC_SLIP, BC_SLIP, BC_NOSLIP, BC_FREE, BC_SEP, BC_SLIP))
+    return s
+
+
+def small_2d_reflect(seed=63, G=16, nsteps=20, dt=1e-4, full=True):
+    """A 2D block against the low corner with frictional reflection (separate walls,
+    friction 0.4, -use_reflect_friction)."""
+    rng = np.random.default_rng(seed)
+    dim, counts = 2, [G, G]
+    dmin, dmax = np.zeros(2), np.ones(2)
+    lo, hi = np.array([0.001, 0.0015]), np.array([0.35, 0.3])
+    X = _seed_cells(rng, dim, counts, dmin, 1.0 / G, lo, hi, 4, lambda P: np.all((P >= lo) & (P < hi), axis=1))
+    Ep = np.exp(rng.uniform(np.log(1e4), np.log(5e4), X.shape[0]))
+    V = np.column_stack([np.full(X.shape[0], -8.0), -10.0 + 2.0 * (X[:, 0] - 0.2)])
+    s = _finish("small2dreflect", dim, counts, dmin, dmax, NEO_HOOKEAN, [0, -9.8], dt, nsteps, [], X, V, Ep, 0.3,
+                1000.0, 4)
+    s.F = np.eye(2) + 0.05 * rng.standard_normal((s.n, 2, 2))
+    s.reflection = Reflection(side_type=(BC_SEP, BC_SLIP, BC_SEP, BC_FREE), friction=0.4, full=full)
+    return s
+
+
 def small_sand_3d(seed=31, G=16, nsteps=20, dt=1e-4):
     """A small sand block (St. Venant-Kirchhoff Hencky + Drucker-Prager with Mast hardening)
     thrown against a sticky floor; a random initial F per particle, compressed by 3 % for
@@ -491,7 +542,7 @@ def snowballs_3d(seed=1234, G=128, ppc=8, E=1.4e5, nu=0.2, density=400.0, dt=5e-
 # --------------------------------------------------------------------------------------------
 # Scene file: read by the reference runner (oracle/ref_scene.cpp) and by the C oracle harness.
 # --------------------------------------------------------------------------------------------
-MAGIC = b"MPMSCN03"
+MAGIC = b"MPMSCN04"
 
 
 def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
@@ -502,9 +553,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         f.write(MAGIC)
         counts = list(s.counts) + [1] * (3 - d)
         pl = s.plasticity
-        im, dc = s.implicit, s.dt_control
-        f.write(struct.pack("<11i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
-                            1 if im else 0, 1 if dc else 0))
+        im, dc, rf = s.implicit, s.dt_control, s.reflection
+        f.write(struct.pack("<12i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
+                            1 if im else 0, 1 if dc else 0, 1 if rf else 0))
         f.write(struct.pack("<11d", *pad3(s.domain_min), *pad3(s.domain_max), *pad3(s.gravity), s.dt, 0.0))
         f.write(struct.pack("<%di" % len(dumps), *dumps))
         for o in s.objects:
@@ -518,6 +569,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         if dc:
             f.write(struct.pack("<8d", dc.frame_dt, dc.cfl, dc.min_dt, dc.max_dt, 1.0 if dc.strong_cfl else 0.0,
                                 dc.cfl_F, 1.0 if dc.sound_cfl else 0.0, dc.cfl_sound))
+        if rf:
+            sides = list(rf.side_type) + [BC_FREE] * (6 - len(rf.side_type))
+            f.write(struct.pack("<8d", *[float(x) for x in sides], rf.friction, 1.0 if rf.full else 0.0))
         f.write(struct.pack("<q", s.n))
         f.write(np.ascontiguousarray(s.X, np.float64).tobytes())
         f.write(np.ascontiguousarray(s.V, np.float64).tobytes())

@@ -39,6 +39,9 @@ CASES = {
     # Simulate_To_Frame with Compute_Dt and Reduce_Dt (steps are frames; substep counts kept)
     "small3d_adaptive": (lambda: S.small_3d_adaptive(), [0, 2], [2]),
     "small2d_adaptive": (lambda: S.small_2d_adaptive(), [0, 2], [2]),
+    # reflection boundary conditions on the domain faces (no wall objects)
+    "small3d_reflect": (lambda: S.small_3d_reflect(), [0, 1, 19], [0, 19]),
+    "small2d_reflect": (lambda: S.small_2d_reflect(), [0, 19], [0, 19]),
     # sand: ST_VENANT_KIRCHHOFF_HENCKY_STRAIN + MPM_DRUCKER_PRAGER (Fp, plastic_def, rho_F, sigma_Y, vc dumped)
     "smallsand3d_hencky": (lambda: S.small_sand_3d(), [0, 1, 19], [0, 19]),
     "smallsand2d_hencky": (lambda: S.small_sand_2d(), [0, 19], [19]),
@@ -71,6 +74,9 @@ def main(names=None):
         pl = scene.plasticity
         if pl is not None:
             arrays["plasticity"] = np.array(S.plastic_params(pl), np.float64)
+        rf = scene.reflection
+        if rf is not None:
+            arrays["reflection"] = np.array(list(rf.side_type) + [rf.friction, float(rf.full)], np.float64)
         dc = scene.dt_control
         if dc is not None:
             arrays["dt_control"] = np.array([dc.frame_dt, dc.cfl, dc.min_dt, dc.max_dt, float(dc.strong_cfl), dc.cfl_F,
@@ -103,6 +109,9 @@ def load(name):
                     z["volume"].copy(), z["mu"].copy(), z["lam"].copy())
     if "plasticity" in z:
         scene.plasticity = S.plastic_from_params(z["plasticity"])
+    if "reflection" in z:
+        r = z["reflection"]
+        scene.reflection = S.Reflection(tuple(int(x) for x in r[:-2]), float(r[-2]), bool(r[-1]))
     if "dt_control" in z:
         c = z["dt_control"]
         scene.dt_control = S.DtControl(float(c[0]), float(c[1]), float(c[2]), float(c[3]), bool(c[4]), float(c[5]),
