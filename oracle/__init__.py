@@ -228,9 +228,12 @@ def ref_available() -> bool:
     return os.path.exists(REF_SCENE)
 
 
-def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timing: bool = False, totals=None):
+def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timing: bool = False, totals=None,
+                  output: str = None, restart=None):
     """Run the reference's own driver on ``scene``; return {step: dump} (and timing JSON if asked).
 
+    ``output`` keeps the viewer directory the driver writes; ``restart=(dir, frame)``
+    starts from that frame's files (MPM_EXAMPLE::Read_Output_Files).
     With ``scene.dt_control`` the steps are frames of Simulate_To_Frame and the
     result is ``(dumps, {"frame_substeps": [...], "time": t})``.
     ``totals=(cfl, max_dt)`` returns instead ``(dumps, diagnostics)``: the
@@ -248,6 +251,10 @@ def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timin
             cmd.append("-time")
         if totals is not None:
             cmd += ["-totals", repr(float(totals[0])), repr(float(totals[1]))]
+        if output is not None:
+            cmd += ["-output", output]
+        if restart is not None:      # (viewer directory, frame): Read_Output_Files, then the substeps
+            cmd += ["-restart", restart[0], str(int(restart[1]))]
         out = subprocess.run(cmd, check=True, capture_output=True, text=True)
         res = S.read_dump(dp, scene.dim, scene.n, scene.counts, plastic=S.plastic_keys(scene.plasticity)) if dumps else {}
         if scene.dt_control is not None:   # frames: the substeps Simulate_To_Frame took per frame

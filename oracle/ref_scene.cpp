@@ -4,7 +4,8 @@
 // restatement in oracle/ and produces the golden fixtures); the product never
 // links or runs it.  Built by oracle/ref.mk against the reference's sources.
 //
-//   ref_scene <scene.bin> <dump.bin> [-threads T] [-float] [-time] [-totals CFL MAX_DT]
+//   ref_scene <scene.bin> <dump.bin> [-threads T] [-float] [-time] [-totals CFL MAX_DT] [-output DIR]
+//             [-restart DIR FRAME]
 //
 // The scene is set up through the reference's public API exactly as
 // Projects/mpm/STANDARD_TESTS_BASE.cpp does it: quadratic weights
@@ -222,6 +223,9 @@ template<class T> void wr(FILE* f, const T* p, size_t n) { fwrite(p, sizeof(T), 
 
 struct TOTALS_REQUEST { bool on = false; double cfl = 1, max_dt = 1; };
 
+std::string keep_output;   // -output DIR: the viewer directory the driver writes (kept)
+int restart_frame = 0;     // -restart DIR FRAME: start from that frame of DIR (Read_Output_Files)
+
 template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threads, bool report_time,
     const TOTALS_REQUEST& totals)
 {
@@ -230,8 +234,9 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
     const int d = TV::m;
     FILE_SCENE<TV> example(s, threads);
     char tmpl[] = "/tmp/ref_scene_XXXXXX";
-    std::string outdir = mkdtemp(tmpl);
+    std::string outdir = keep_output.empty() ? std::string(mkdtemp(tmpl)) : keep_output;
     example.viewer_dir.output_directory = outdir;
+    if(restart_frame) example.restart = restart_frame;
     MPM_DRIVER<TV> driver(example);
     driver.Initialize();
 
@@ -346,8 +351,10 @@ template<class TV> int Run(const SCENE_FILE& s, const char* dump_path, int threa
         for(size_t i = 0; i < step_seconds.size(); i++) printf("%s%.9g", i ? ", " : "", step_seconds[i]);
         printf("]}\n");
     }
-    std::string cmd = "rm -rf '" + outdir + "'";
-    if(system(cmd.c_str())) {}
+    if(keep_output.empty()) {
+        std::string cmd = "rm -rf '" + outdir + "'";
+        if(system(cmd.c_str())) {}
+    }
     return 0;
 }
 }
@@ -362,6 +369,8 @@ int main(int argc, char* argv[])
         if(!strcmp(argv[i], "-threads") && i + 1 < argc) threads = atoi(argv[++i]);
         else if(!strcmp(argv[i], "-float")) use_float = true;
         else if(!strcmp(argv[i], "-time")) report_time = true;
+        else if(!strcmp(argv[i], "-output") && i + 1 < argc) keep_output = argv[++i];
+        else if(!strcmp(argv[i], "-restart") && i + 2 < argc) { keep_output = argv[++i]; restart_frame = atoi(argv[++i]); }
         else if(!strcmp(argv[i], "-totals") && i + 2 < argc) {
             totals.on = true;
             totals.cfl = atof(argv[++i]);

@@ -306,6 +306,7 @@ class MPM_DRIVER:
     def set_scene_particles(self, scene: Optional[S.Scene] = None, dtype=np.float64):
         s = scene or self.scene
         self.set_particles(s.X, s.V, s.F, s.B, s.mass, s.volume, s.mu, s.lam, dtype=dtype)
+        self._attrs = {"mass": s.mass, "volume": s.volume, "mu": s.mu, "lam": s.lam}
 
     def get_particles(self, dtype=np.float64):
         d, n = self.dim, self.n
@@ -361,6 +362,48 @@ class MPM_DRIVER:
         v = self._dev_view(X, V, Fc, Bc, valid=valid)
         self._check(self.L.mpm_get_particles(self.h, ctypes.byref(v)), "mpm_get_particles")
         return X, V, Fc, Bc, valid
+
+    # -- output frames and restart (PhysBAM's viewer directory) ---------------------
+    def write_frame(self, directory: str, frame: int, use_doubles: bool = True):
+        """Write the particle state as the reference's Write_Output_Files does
+        (physbam_b200.io): <directory>/<frame>/mpm_particles.gz, restart_data.gz and
+        common/grid.gz, readable by the reference and by read_frame."""
+        from . import io
+        p = self.get_particles()
+        sc = self.scene
+        parts = {"X": p["X"], "V": p["V"], "F": p["F"], "B": p["B"], "valid": p["valid"],
+                 "mass": self._attr("mass"), "volume": self._attr("volume")}
+        if getattr(self, "plasticity", None) is not None:
+            st = self.get_plastic_state()
+            parts["mu"], parts["lambda"] = st["mu"], st["lam"]
+            for k, name in io.PLASTIC_NAMES.items():
+                if k in st:
+                    parts[name] = st[k]
+        else:
+            parts["mu"], parts["lambda"] = self._attr("mu"), self._attr("lam")
+        io.write_frame(directory, frame, self.time, parts, counts=sc.counts[:self.dim],
+                       domain_min=sc.domain_min[:self.dim], domain_max=sc.domain_max[:self.dim], use_doubles=use_doubles)
+
+    def read_frame(self, directory: str, frame: int):
+        """Restart from a frame (MPM_EXAMPLE::Read_Output_Files): the particles of
+        mpm_particles.gz (the plastic arrays too, where the file has them) and the time."""
+        from . import io
+        f = io.read_frame(directory, frame)
+        self.set_particles(f["X"], f["V"], f["F"], f["B"], f["mass"], f["volume"], f["mu"], f["lambda"],
+                           valid=f["valid"])
+        self._attrs = {"mass": f["mass"], "volume": f["volume"], "mu": f["mu"], "lam": f["lambda"]}
+        if getattr(self, "plasticity", None) is not None:
+            keys = {k: f[name] for k, name in io.PLASTIC_NAMES.items() if name in f and k in self._plastic_keys()}
+            if keys:
+                self.set_plastic_state(**keys)
+        self.time = f["time"]
+
+    def _attr(self, name):
+        """Per-particle constants as last set (mass, volume, mu, lam)."""
+        a = getattr(self, "_attrs", None)
+        if a is not None:
+            return a[name]
+        return getattr(self.scene, name)
 
     # -- reflection boundary conditions -----------------------------------------
     def set_reflection(self, reflection: Optional[S.Reflection]):
