@@ -541,9 +541,28 @@ def profile_case(args, D, S):
     """Small single-scene run for profilers: `--scene NAME --grid G` (no e2e, no CPU, no flush).
     Prints one JSON line with the per-kernel times; used to make the ncu summaries."""
     import torch
+    def spheres_implicit(**kw):
+        s = S.spheres_3d(dt=2e-3, **kw)
+        s.implicit = S.Implicit()
+        return s
     make = {"spheres3d": S.spheres_3d, "dam3d": S.dam_3d, "cube3d": S.cube_3d,
-            "snowballs3d": S.snowballs_3d, "sand3d": S.sand_3d}[args.scene]
+            "snowballs3d": S.snowballs_3d, "sand3d": S.sand_3d, "spheres3d_implicit": spheres_implicit}[args.scene]
     scene = make(G=args.grid) if args.grid else make()
+    if scene.implicit is not None:     # the plain path, FP64, from the contact phase on
+        drv = D.MPM_DRIVER(scene, precision=D.FP64, path=D.PATH_PLAIN)
+        drv.set_scene_particles(scene)
+        for _ in range(IMPLICIT_LEAD + args.warmup):
+            drv.Advance_One_Time_Step()
+        drv.synchronize()
+        drv.set_timing(True)
+        for _ in range(args.steps):
+            drv.Advance_One_Time_Step()
+        drv.synchronize()
+        kt = drv.get_timing()
+        drv.close()
+        print(json.dumps({"scene": args.scene, "particles": scene.n, "steps": args.steps,
+                          "kernel_ms_per_substep": {k: v[0] / max(args.steps, 1) for k, v in kt.items()}}), flush=True)
+        return 0
     drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
     if args.shape:
         drv.set_launch_shape(*[int(x) for x in args.shape.split(",")])
@@ -600,7 +619,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 path on the same workload")
     ap.add_argument("--no-implicit", action="store_true", help="skip the backward-Euler measurement")
     ap.add_argument("--no-snow", action="store_true", help="skip the snow and sand (plasticity) measurements")
-    ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d", "snowballs3d", "sand3d"],
+    ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d", "snowballs3d", "sand3d", "spheres3d_implicit"],
                     help="profiling run of one scene only")
     ap.add_argument("--grid", type=int, default=0, help="grid cells per side for --scene")
     ap.add_argument("--shape", default="", help="launch shape for --scene: P2G variant,G2P threads,CTA multiplier")

@@ -55,8 +55,8 @@ enum mpm_model { MPM_COROTATED_FIXED = 0, MPM_NEO_HOOKEAN = 1, MPM_STVK_HENCKY =
 /* MPM_COLLISION_OBJECT::COLLISION_TYPE (Hybrid_Methods/Collisions/MPM_COLLISION_OBJECT.h:21) */
 enum mpm_collision_type { MPM_STICK = 0, MPM_SLIP = 1, MPM_SEPARATE = 2 };
 
-/* implicit object behind a collision object: RANGE box or PLANE half-space */
-enum mpm_object_kind { MPM_BOX = 0, MPM_PLANE = 1 };
+/* implicit object behind a collision object: RANGE box, PLANE half-space or SPHERE */
+enum mpm_object_kind { MPM_BOX = 0, MPM_PLANE = 1, MPM_SPHERE = 2 };
 
 /* which kernels run the substep */
 enum mpm_path {
@@ -88,8 +88,9 @@ typedef struct {
 } mpm_model_desc;
 
 /* MPM_EXAMPLE::Add_Collision_Object(io, type, friction) for a static object.
- * MPM_BOX:   a = min corner, b = max corner (RANGE<TV>).
- * MPM_PLANE: a = unit normal, b = a point on the plane (PLANE<T>). */
+ * MPM_BOX:    a = min corner, b = max corner (RANGE<TV>).
+ * MPM_PLANE:  a = unit normal, b = a point on the plane (PLANE<T>).
+ * MPM_SPHERE: a = center, b[0] = radius (SPHERE<TV>; a circle in 2D). */
 typedef struct {
     int kind;
     int type;

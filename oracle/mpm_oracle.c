@@ -407,6 +407,11 @@ static void box_normal(int d, const oracle_object* o, const double* X, double* n
 static double obj_phi(int d, const oracle_object* o, const double* X)
 {
     if(o->kind == 0) return box_phi(d, o, X);
+    if(o->kind == 2) {   /* SPHERE::Signed_Distance, Geometry/Basic_Geometry/SPHERE.h:59-60 */
+        double r2 = 0;
+        for(int a = 0; a < d; a++) r2 += (X[a] - o->a[a]) * (X[a] - o->a[a]);
+        return sqrt(r2) - o->b[0];
+    }
     double s = 0;  /* PLANE::Signed_Distance, Geometry/Basic_Geometry/PLANE.h:62-63 */
     for(int a = 0; a < d; a++) s += o->a[a] * (X[a] - o->b[a]);
     return s;
@@ -414,6 +419,14 @@ static double obj_phi(int d, const oracle_object* o, const double* X)
 static void obj_normal(int d, const oracle_object* o, const double* X, double* n)
 {
     if(o->kind == 0) { box_normal(d, o, X, n); return; }
+    if(o->kind == 2) {   /* SPHERE::Normal: (X - center).Normalized() */
+        double mag = 0;
+        for(int a = 0; a < d; a++) { n[a] = X[a] - o->a[a]; mag += n[a] * n[a]; }
+        mag = sqrt(mag);
+        if(mag) { double s = 1 / mag; for(int a = 0; a < d; a++) n[a] *= s; }
+        else { for(int a = 0; a < d; a++) n[a] = a == 0; }
+        return;
+    }
     for(int a = 0; a < d; a++) n[a] = o->a[a];
 }
 

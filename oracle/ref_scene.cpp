@@ -21,6 +21,7 @@
 #include <Core/Matrices/MATRIX.h>
 #include <Core/Vectors/VECTOR.h>
 #include <Geometry/Basic_Geometry/PLANE.h>
+#include <Geometry/Basic_Geometry/SPHERE.h>
 #include <Geometry/Implicit_Objects/ANALYTIC_IMPLICIT_OBJECT.h>
 #include <Deformables/Constitutive_Models/COROTATED_FIXED.h>
 #include <Deformables/Constitutive_Models/NEO_HOOKEAN.h>
@@ -209,6 +210,7 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
             TV a, b;
             for(int k = 0; k < d; k++) { a(k) = (T)o.a[k]; b(k) = (T)o.b[k]; }
             if(o.kind == 0) this->Add_Collision_Object(RANGE<TV>(a, b), type, (T)o.friction);
+            else if(o.kind == 2) this->Add_Collision_Object(SPHERE<TV>(a, (T)o.b[0]), type, (T)o.friction);
             else Add_Plane(a, b, type, (T)o.friction);
         }
     }

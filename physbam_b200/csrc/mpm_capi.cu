@@ -243,7 +243,8 @@ int mpm_set_collision_objects(mpm_handle* h, const mpm_collision_object* objs, i
         return set_error(h, MPM_ERR_ARG, "full reflection is built for scenes without collision objects");
     for(int i = 0; i < count; i++) {
         const mpm_collision_object& o = objs[i];
-        if(o.kind != MPM_BOX && o.kind != MPM_PLANE) return set_error(h, MPM_ERR_ARG, "unknown object kind");
+        if(o.kind != MPM_BOX && o.kind != MPM_PLANE && o.kind != MPM_SPHERE) return set_error(h, MPM_ERR_ARG, "unknown object kind");
+        if(o.kind == MPM_SPHERE && !(o.b[0] > 0)) return set_error(h, MPM_ERR_ARG, "sphere radius must be positive");
         if(o.type < MPM_STICK || o.type > MPM_SEPARATE) return set_error(h, MPM_ERR_ARG, "unknown collision type");
         if(o.kind == MPM_BOX)
             for(int k = 0; k < h->sp.dim; k++)

@@ -2187,6 +2187,20 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* repor
     return rc;
 }
 
+int64_t sort_scratch_words(int64_t n) { return mpm_sort::scratch_words(n); }
+
+// Stable LSD radix sort of device keys on the handle's stream (the fast path's
+// sort), for the other paths: sorted keys and the permutation.
+int sort_keys_device(mpm_handle* h, const uint32_t* keys, int64_t n, int bits, uint32_t* sorted, uint32_t* perm,
+    uint32_t* alt_keys, uint32_t* alt_vals, uint32_t* scratch)
+{
+    MPM_CUDA(h, mpm_sort::prepare());
+    cudaError_t e = mpm_sort::radix_sort(keys, sorted, perm, alt_keys, alt_vals, n, bits, scratch, h->d_flags,
+                                         MPM_FLAG_TIMEOUT, h->sm_count * 4, h->stream);
+    if(e != cudaSuccess) return check_cuda(h, e, "radix_sort");
+    return MPM_OK;
+}
+
 int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm)
 {
     if(n < 0 || bits < 1 || bits > 32 || (n && (!keys || !sorted_keys || !perm))) return MPM_ERR_ARG;

@@ -13,10 +13,10 @@
 // runs the Newton / CG / line-search control flow, reading back one or two
 // reduced scalars per step (deterministic two-stage reductions in FP64).
 //
-// Collision objects are the static boxes and planes of the explicit path
-// (zero curvature, so the Hessian terms of Test_Add_Collision vanish).  A
-// node's collisions are kept per object, in object order (the reference
-// appends them per node in that order).
+// Collision objects are the static boxes, planes and spheres of the explicit
+// path; the curvature terms of the projection use the Hessian of the signed
+// distance at the tested position.  A node's collisions are kept per object,
+// in object order (the reference appends them per node in that order).
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -41,9 +41,34 @@ template<class T> struct ImpArgs {
     T *U, *FV, *sig, *dP;       // SVD of the current F: U, Fn V, singular values, stress derivative (9 + 3 + 3)
     double* pe;                 // per-particle potential energy
     uint8_t *cmask, *stuck;     // per node: collision objects (bit j), stuck flag
-    T* cdat;                    // per node and object: phi, n_dE, normal (2 + d)
+    T* cdat;                    // per node and object: phi, n_dE, normal, position, H g (2 + 3d)
     int nobj;
+    const uint32_t* order;      // particles sorted by cell (the passes visit them in this order)
 };
+
+// The t-th particle of a pass: neighbours in the grid run in neighbouring
+// threads, so the stencil gathers and the atomic scatters stay in cache.
+template<class T> __device__ __forceinline__ int64_t particle_at(const ImpArgs<T>& ia, int64_t t)
+{
+    return ia.order ? (int64_t)ia.order[t] : t;
+}
+
+// Sort key of a particle: the flat index of its stencil's first node; invalid
+// particles and stencils outside the grid go last.
+template<class T, int d> __global__ void k_imp_keys(ImpArgs<T> ia, uint32_t* keys)
+{
+    const PlainArgs<T>& a = ia.a;
+    for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t k = 0xffffffffu;
+        Stencil<T, d> s;
+        if(a.valid[p] && make_stencil<T, d>(a, a.X + p * d, s)) {
+            int64_t flat = 0;
+            for(int c = 0; c < d; c++) flat = flat * a.gs[c] + (s.base[c] + MPM_GHOST);
+            k = (uint32_t)flat;
+        }
+        keys[p] = k;
+    }
+}
 
 template<class T, int d> __device__ __forceinline__ bool node_valid(const ImpArgs<T>& ia, int64_t i) { return ia.a.gm[i] != 0; }
 
@@ -83,8 +108,10 @@ template<class T, int d> __global__ void k_imp_restore(ImpArgs<T> ia)
 template<class T, int d> __global__ void k_imp_update_F(ImpArgs<T> ia, const T* v)
 {
     const PlainArgs<T>& a = ia.a;
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if(p >= a.n || !a.valid[p]) return;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if(t >= a.n) return;
+    const int64_t p = particle_at(ia, t);
+    if(!a.valid[p]) return;
     Stencil<T, d> s;
     if(!make_stencil<T, d>(a, ia.X0 + p * d, s)) return;
     T Vp[3] = {0, 0, 0}, G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -121,8 +148,9 @@ template<class T, int d> __global__ void k_imp_update_F(ImpArgs<T> ia, const T* 
 template<class T, int d> __global__ void k_imp_precompute(ImpArgs<T> ia)
 {
     const PlainArgs<T>& a = ia.a;
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if(p >= a.n) return;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if(t >= a.n) return;
+    const int64_t p = particle_at(ia, t);
     if(!a.valid[p]) { ia.pe[p] = 0; return; }
     T F[9], U[9], V[9], S[3], P[3];
 #pragma unroll
@@ -169,8 +197,10 @@ template<class T, int d> __global__ void k_imp_precompute(ImpArgs<T> ia)
 template<class T, int d> __global__ void k_imp_forces(ImpArgs<T> ia, T* f)
 {
     const PlainArgs<T>& a = ia.a;
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if(p >= a.n || !a.valid[p]) return;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if(t >= a.n) return;
+    const int64_t p = particle_at(ia, t);
+    if(!a.valid[p]) return;
     Stencil<T, d> s;
     if(!make_stencil<T, d>(a, ia.X0 + p * d, s)) return;
     T A[9];
@@ -197,8 +227,10 @@ template<class T, int d> __global__ void k_imp_forces(ImpArgs<T> ia, T* f)
 template<class T, int d> __global__ void k_imp_hessian(ImpArgs<T> ia, const T* z, T* f)
 {
     const PlainArgs<T>& a = ia.a;
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if(p >= a.n || !a.valid[p]) return;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if(t >= a.n) return;
+    const int64_t p = particle_at(ia, t);
+    if(!a.valid[p]) return;
     Stencil<T, d> s;
     if(!make_stencil<T, d>(a, ia.X0 + p * d, s)) return;
     T W[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -316,10 +348,10 @@ template<class T, int d> __global__ void k_imp_adjust(ImpArgs<T> ia, T* dv)
             if(o.type != MPM_STICK && phi > (T)FLT_MAX) continue;
             T n[3];
             object_normal<T, d>(o, X, n);
-            T* cd = ia.cdat + (i * ia.nobj + j) * (2 + d);
+            T* cd = ia.cdat + (i * ia.nobj + j) * (2 + 3 * d);
             cd[0] = phi;
             cd[1] = 0;
-            for(int k = 0; k < d; k++) cd[2 + k] = n[k];
+            for(int k = 0; k < d; k++) { cd[2 + k] = n[k]; cd[2 + d + k] = X[k]; cd[2 + 2 * d + k] = 0; }
             mask |= (uint8_t)(1u << j);
             for(int k = 0; k < d; k++) { X[k] -= phi * n[k]; V[k] = (X[k] - X0[k]) / a.dt; }
             if(o.type == MPM_STICK) {
@@ -346,7 +378,7 @@ template<class T, int d> __global__ void k_imp_project(ImpArgs<T> ia, T* g, int 
             for(int k = 0; k < d; k++) g[i * d + k] = 0;
         for(int j = ia.nobj - 1; j >= 0; j--) {
             if(!(mask & (1u << j))) continue;
-            T* cd = ia.cdat + (i * ia.nobj + j) * (2 + d);
+            T* cd = ia.cdat + (i * ia.nobj + j) * (2 + 3 * d);
             T ndE = 0;
             for(int k = 0; k < d; k++) ndE += g[i * d + k] * cd[2 + k];
             cd[1] = ndE;
@@ -355,7 +387,16 @@ template<class T, int d> __global__ void k_imp_project(ImpArgs<T> ia, T* g, int 
                 mask &= (uint8_t)~(1u << j);
                 continue;
             }
-            for(int k = 0; k < d; k++) g[i * d + k] -= ndE * cd[2 + k];
+            // H_dE = H g; g -= n_dE n + phi H_dE
+            T H[9], gv[3];
+            object_hessian<T, d>(ia.a.sp.objs[j], cd + 2 + d, H);
+            for(int k = 0; k < d; k++) gv[k] = g[i * d + k];
+            for(int r = 0; r < d; r++) {
+                T hd = 0;
+                for(int c = 0; c < d; c++) hd += H[r + d * c] * gv[c];
+                cd[2 + 2 * d + r] = hd;
+            }
+            for(int k = 0; k < d; k++) g[i * d + k] -= ndE * cd[2 + k] + cd[0] * cd[2 + 2 * d + k];
         }
         ia.cmask[i] = mask;
     }
@@ -371,7 +412,7 @@ template<class T, int d> __global__ void k_imp_mult_pre(ImpArgs<T> ia, T* tmp, c
         const uint8_t mask = ia.cmask[i];
         for(int j = 0; j < ia.nobj; j++) {
             if(!(mask & (1u << j))) continue;
-            const T* n = ia.cdat + (i * ia.nobj + j) * (2 + d) + 2;
+            const T* n = ia.cdat + (i * ia.nobj + j) * (2 + 3 * d) + 2;
             T dn = 0;
             for(int k = 0; k < d; k++) dn += x[k] * n[k];
             for(int k = 0; k < d; k++) x[k] -= dn * n[k];
@@ -380,8 +421,10 @@ template<class T, int d> __global__ void k_imp_mult_pre(ImpArgs<T> ia, T* tmp, c
     }
 }
 
-// ... and after it: f = (dt^2/m) H tmp + tmp, projected the same way.
-template<class T, int d> __global__ void k_imp_mult_post(ImpArgs<T> ia, T* f, const T* tmp)
+// ... and after it: f = (dt^2/m) H tmp + tmp, with the stuck nodes zeroed and
+// per collision f -= n (n.f) + dt (Hc v n_dE + (n.v) H_dE + (H_dE.v) n), v the
+// unprojected input (the curvature terms of MPM_KRYLOV_SYSTEM::Multiply).
+template<class T, int d> __global__ void k_imp_mult_post(ImpArgs<T> ia, T* f, const T* tmp, const T* v)
 {
     NODE_LOOP(ia) {
         const T s = ia.a.dt * ia.a.dt / ia.a.gm[i];
@@ -392,10 +435,19 @@ template<class T, int d> __global__ void k_imp_mult_post(ImpArgs<T> ia, T* f, co
         const uint8_t mask = ia.cmask[i];
         for(int j = 0; j < ia.nobj; j++) {
             if(!(mask & (1u << j))) continue;
-            const T* n = ia.cdat + (i * ia.nobj + j) * (2 + d) + 2;
-            T dn = 0;
-            for(int k = 0; k < d; k++) dn += x[k] * n[k];
-            for(int k = 0; k < d; k++) x[k] -= dn * n[k];
+            const T* cd = ia.cdat + (i * ia.nobj + j) * (2 + 3 * d);
+            const T* n = cd + 2;
+            const T* hde = cd + 2 + 2 * d;
+            T H[9];
+            object_hessian<T, d>(ia.a.sp.objs[j], cd + 2 + d, H);
+            T dn = 0, nv = 0, hv = 0, Hv[3];
+            for(int k = 0; k < d; k++) { dn += x[k] * n[k]; nv += n[k] * v[i * d + k]; hv += hde[k] * v[i * d + k]; }
+            for(int r = 0; r < d; r++) {
+                Hv[r] = 0;
+                for(int c = 0; c < d; c++) Hv[r] += H[r + d * c] * v[i * d + c];
+            }
+            for(int k = 0; k < d; k++)
+                x[k] -= n[k] * dn + ia.a.dt * (Hv[k] * cd[1] + nv * hde[k] + hv * n[k]);
         }
         for(int k = 0; k < d; k++) f[i * d + k] = x[k];
     }
@@ -417,7 +469,7 @@ template<class T, int d> __global__ void k_imp_friction(ImpArgs<T> ia, const T* 
         const uint8_t mask = ia.cmask[i];
         for(int j = 0; j < ia.nobj; j++) {
             if(!(mask & (1u << j))) continue;
-            const T* n = ia.cdat + (i * ia.nobj + j) * (2 + d) + 2;
+            const T* n = ia.cdat + (i * ia.nobj + j) * (2 + 3 * d) + 2;
             T nf = 0, vn = 0;
             for(int k = 0; k < d; k++) { nf += n[k] * (tmp0[i * d + k] - tmp1[i * d + k]); vn += v[k] * n[k]; }
             T t[3], tm = 0;
@@ -505,14 +557,19 @@ __global__ void k_imp_max_final(const double* partial, int count, double* out)
     *out = r;
 }
 
+// one block per result slot; the partials (count == blockDim.x) summed by a
+// fixed tree, so the result does not depend on scheduling
 __global__ void k_imp_final(const double* partial, int count, int slots, double* out)
 {
-    // one thread per result slot, partials summed in block order
-    const int s = threadIdx.x;
-    if(s >= slots) return;
-    double acc = 0;
-    for(int b = 0; b < count; b++) acc += partial[s * count + b];
-    out[s] = acc;
+    __shared__ double sh[kRedThreads];
+    const int s = blockIdx.x;
+    sh[threadIdx.x] = threadIdx.x < count ? partial[s * count + threadIdx.x] : 0.0;
+    __syncthreads();
+    for(int st = kRedThreads / 2; st > 0; st >>= 1) {
+        if(threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+        __syncthreads();
+    }
+    if(threadIdx.x == 0) out[s] = sh[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -535,6 +592,8 @@ struct ImplicitState {
     double* partial = nullptr;     // 2 * kRedBlocks
     double* dout = nullptr;        // 2 results
     double* hout = nullptr;        // pinned copy
+    uint32_t *keys = nullptr, *sorted = nullptr, *perm = nullptr, *alt_k = nullptr, *alt_v = nullptr, *scratch = nullptr;
+    int key_bits = 1;
 };
 
 namespace {
@@ -558,6 +617,7 @@ template<class T, int d> struct Solver {
         ia.F0 = P; ia.X0 = P + n * d * d; ia.U = ia.X0 + n * d; ia.FV = ia.U + n * d * d;
         ia.sig = ia.FV + n * d * d; ia.dP = ia.sig + n * d;
         ia.pe = s.pe; ia.cmask = s.cmask; ia.stuck = s.stuck; ia.cdat = (T*)s.cdat; ia.nobj = h->sp.nobj;
+        ia.order = nullptr;
         for(int k = 0; k < V_COUNT; k++) v[k] = (T*)s.vec + (size_t)k * s.gn * d;
         pb = pblocks(s.n, 128);
         gb = gblocks(h, s.gn, 256);
@@ -580,7 +640,7 @@ template<class T, int d> struct Solver {
     {
         ImplicitState& s = *h->imp;
         k_imp_dot<T, d><<<kRedBlocks, kRedThreads, 0, st>>>(ia, x, y, s.partial);
-        k_imp_final<<<1, 32, 0, st>>>(s.partial, kRedBlocks, 1, s.dout);
+        k_imp_final<<<1, kRedThreads, 0, st>>>(s.partial, kRedBlocks, 1, s.dout);
         cudaMemcpyAsync(s.hout, s.dout, sizeof(double), cudaMemcpyDeviceToHost, st);
         cudaStreamSynchronize(st);
         check("implicit dot");
@@ -592,7 +652,7 @@ template<class T, int d> struct Solver {
         ImplicitState& s = *h->imp;
         k_imp_dot<T, d><<<kRedBlocks, kRedThreads, 0, st>>>(ia, x, x, s.partial);
         k_imp_sum_particles<T><<<kRedBlocks, kRedThreads, 0, st>>>(s.pe, s.n, s.partial + kRedBlocks);
-        k_imp_final<<<1, 32, 0, st>>>(s.partial, kRedBlocks, 2, s.dout);
+        k_imp_final<<<2, kRedThreads, 0, st>>>(s.partial, kRedBlocks, 2, s.dout);
         cudaMemcpyAsync(s.hout, s.dout, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
         cudaStreamSynchronize(st);
         check("implicit energy");
@@ -644,7 +704,7 @@ template<class T, int d> struct Solver {
         k_imp_mult_pre<T, d><<<gb, 256, 0, st>>>(ia, v[V_STMP], x);
         zero(out);
         k_imp_hessian<T, d><<<pb, 128, 0, st>>>(ia, v[V_STMP], out);
-        k_imp_mult_post<T, d><<<gb, 256, 0, st>>>(ia, out, v[V_STMP]);
+        k_imp_mult_post<T, d><<<gb, 256, 0, st>>>(ia, out, v[V_STMP], x);
     }
 
     // CONJUGATE_GRADIENT::Solve with relative tolerance and
@@ -796,7 +856,15 @@ template<class T, int d> struct Solver {
     int solve(double dt)
     {
         ImplicitState& s = *h->imp;
-        if(s.n) k_imp_save<T, d><<<pb, 128, 0, st>>>(ia);
+        if(s.n) {
+            // the particles in cell order for every pass of the solve (their weights
+            // are those of the step's start, so one sort serves the whole solve)
+            k_imp_keys<T, d><<<pb, 128, 0, st>>>(ia, s.keys);
+            check("implicit keys");
+            if((rc = sort_keys_device(h, s.keys, s.n, s.key_bits, s.sorted, s.perm, s.alt_k, s.alt_v, s.scratch))) return rc;
+            ia.order = s.perm;
+            k_imp_save<T, d><<<pb, 128, 0, st>>>(ia);
+        }
         for(int k = 0; k < V_COUNT; k++) zero(v[k]);
         if(ia.nobj) {
             cudaMemsetAsync(s.cmask, 0, s.gn, st);
@@ -849,10 +917,16 @@ template<class T> int ensure_state(mpm_handle* h)
     MPM_CUDA(h, cudaMalloc(&t.stuck, (size_t)t.gn));
     MPM_CUDA(h, cudaMemset(t.cmask, 0, (size_t)t.gn));
     MPM_CUDA(h, cudaMemset(t.stuck, 0, (size_t)t.gn));
-    if(t.nobj) MPM_CUDA(h, cudaMalloc(&t.cdat, (size_t)t.gn * t.nobj * (2 + d) * e));
+    if(t.nobj) MPM_CUDA(h, cudaMalloc(&t.cdat, (size_t)t.gn * t.nobj * (2 + 3 * d) * e));
     MPM_CUDA(h, cudaMalloc(&t.partial, 2 * kRedBlocks * sizeof(double)));
     MPM_CUDA(h, cudaMalloc(&t.dout, 2 * sizeof(double)));
     MPM_CUDA(h, cudaMallocHost(&t.hout, 2 * sizeof(double)));
+    uint32_t** sb[] = {&t.keys, &t.sorted, &t.perm, &t.alt_k, &t.alt_v};
+    for(uint32_t** p: sb) MPM_CUDA(h, cudaMalloc(p, (size_t)n * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&t.scratch, (size_t)sort_scratch_words(n) * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMemset(t.scratch, 0, (size_t)sort_scratch_words(n) * sizeof(uint32_t)));
+    t.key_bits = 1;
+    while((int64_t)((1ull << t.key_bits) - 1) < t.gn) t.key_bits++;
     return MPM_OK;
 }
 
@@ -912,6 +986,7 @@ void implicit_free(mpm_handle* h)
     ImplicitState& s = *h->imp;
     cudaFree(s.vec); cudaFree(s.part); cudaFree(s.pe); cudaFree(s.cmask); cudaFree(s.stuck); cudaFree(s.cdat);
     cudaFree(s.partial); cudaFree(s.dout);
+    cudaFree(s.keys); cudaFree(s.sorted); cudaFree(s.perm); cudaFree(s.alt_k); cudaFree(s.alt_v); cudaFree(s.scratch);
     if(s.hout) cudaFreeHost(s.hout);
     delete h->imp;
     h->imp = nullptr;

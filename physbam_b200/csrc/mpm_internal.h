@@ -183,6 +183,9 @@ int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_k
 int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, const mpm_collision_object* objs, int nobjs);
 int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* report, int report_len);
 int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm);
+int64_t sort_scratch_words(int64_t n);
+int sort_keys_device(mpm_handle* h, const uint32_t* keys, int64_t n, int bits, uint32_t* sorted, uint32_t* perm,
+    uint32_t* alt_keys, uint32_t* alt_vals, uint32_t* scratch);
 int fast_prepare_sort(mpm_handle* h);
 int fast_particle_totals(mpm_handle* h, mpm_totals* out);
 int fast_grid_totals(mpm_handle* h, mpm_totals* out);

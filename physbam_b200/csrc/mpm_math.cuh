@@ -549,6 +549,12 @@ struct DevObjectF {
 
 template<class T, int d, class O> __device__ T object_phi(const O& o, const T* X)
 {
+    if(o.kind == MPM_SPHERE) {   // SPHERE::Signed_Distance (Geometry/Basic_Geometry/SPHERE.h:59-60)
+        T r2 = 0;
+#pragma unroll
+        for(int a = 0; a < d; a++) r2 += (X[a] - (T)o.a[a]) * (X[a] - (T)o.a[a]);
+        return sqrt(r2) - (T)o.b[0];
+    }
     if(o.kind == MPM_PLANE) {
         T s = 0;
 #pragma unroll
@@ -575,6 +581,21 @@ template<class T, int d, class O> __device__ T object_phi(const O& o, const T* X
 
 template<class T, int d, class O> __device__ void object_normal(const O& o, const T* X, T* n)
 {
+    if(o.kind == MPM_SPHERE) {   // SPHERE::Normal: (X - center).Normalized()
+        T mag = 0;
+#pragma unroll
+        for(int a = 0; a < d; a++) { n[a] = X[a] - (T)o.a[a]; mag += n[a] * n[a]; }
+        mag = sqrt(mag);
+        if(mag != 0) {
+            const T s = (T)1 / mag;
+#pragma unroll
+            for(int a = 0; a < d; a++) n[a] *= s;
+        } else {
+#pragma unroll
+            for(int a = 0; a < d; a++) n[a] = a == 0 ? (T)1 : (T)0;
+        }
+        return;
+    }
     if(o.kind == MPM_PLANE) {
 #pragma unroll
         for(int a = 0; a < d; a++) n[a] = (T)o.a[a];
@@ -615,6 +636,48 @@ template<class T, int d, class O> __device__ void object_normal(const O& o, cons
 #pragma unroll
         for(int a = 0; a < d; a++) n[a] = a == 0 ? (T)1 : (T)0;
     }
+}
+
+// Hessian of the signed distance, H[a + d b] (the implicit solve's collision
+// curvature): zero for a plane and inside a box; outside a box
+// RANGE::Hessian (Core/Math_Tools/RANGE.cpp:67-81) (D - n n^T)/|n| over the
+// axes the point is beyond; SPHERE::Hessian (SPHERE.h:38-39) (I - z z^T)/|X - c|.
+template<class T, int d, class O> __device__ void object_hessian(const O& o, const T* X, T* H)
+{
+#pragma unroll
+    for(int e = 0; e < d * d; e++) H[e] = 0;
+    if(o.kind == MPM_PLANE) return;
+    T z[3], D[3], w = 0;
+    if(o.kind == MPM_SPHERE) {
+#pragma unroll
+        for(int a = 0; a < d; a++) { z[a] = X[a] - (T)o.a[a]; w += z[a] * z[a]; D[a] = 1; }
+    } else {
+        bool inside = true;
+#pragma unroll
+        for(int a = 0; a < d; a++) if(!(X[a] >= (T)o.a[a] && X[a] <= (T)o.b[a])) inside = false;
+        if(inside) return;
+#pragma unroll
+        for(int a = 0; a < d; a++) {
+            const T pmax = X[a] - (T)o.b[a], pmin = (T)o.a[a] - X[a];
+            const T phi = pmin > pmax ? pmin : pmax;
+            z[a] = 0; D[a] = 0;
+            if(phi > 0) { z[a] = pmax > pmin ? phi : -phi; D[a] = 1; }
+            w += z[a] * z[a];
+        }
+    }
+    w = sqrt(w);
+    if(w != 0) {
+        const T s = (T)1 / w;
+#pragma unroll
+        for(int a = 0; a < d; a++) z[a] *= s;
+    } else {
+#pragma unroll
+        for(int a = 0; a < d; a++) z[a] = a == 0 ? (T)1 : (T)0;
+    }
+#pragma unroll
+    for(int a = 0; a < d; a++)
+#pragma unroll
+        for(int b = 0; b < d; b++) H[a + d * b] = ((a == b ? D[a] : (T)0) - z[a] * z[b]) / w;
 }
 
 // Grid-node collision projection and Coulomb friction for one node.

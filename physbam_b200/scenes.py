@@ -40,6 +40,7 @@ SEPARATE = 2
 
 BOX = 0
 PLANE = 1
+SPHERE = 2          # a = center, b[0] = radius
 
 GHOST = 3
 
@@ -438,6 +439,27 @@ def small_2d_implicit(seed=43, G=16, nsteps=10, dt=1e-3):
     s = small_2d(seed=seed, G=G, nsteps=nsteps, dt=dt, model=NEO_HOOKEAN)
     s.name = "small2dimplicit"
     s.implicit = Implicit()
+    return s
+
+
+def small_3d_sphere(seed=71, G=16, nsteps=20, dt=1e-4, implicit=False):
+    """small_3d thrown at a spherical obstacle (separate, friction 0.3) as well as the walls."""
+    s = small_3d(seed=seed, G=G, nsteps=nsteps, dt=dt, friction=0.2, v=(3.0, -1.0, 1.5))
+    s.name = "small3dsphere"
+    s.objects = s.objects + [CollisionObject(SPHERE, SEPARATE, 0.3, [0.62, 0.3, 0.55], [0.12, 0, 0])]
+    if implicit:
+        s.name = "small3dsphereimplicit"
+        s.dt = 1e-3
+        s.nsteps = 8
+        s.implicit = Implicit()
+    return s
+
+
+def small_2d_sphere(seed=73, G=16, nsteps=20, dt=1e-4):
+    """small_2d with a sticky circle inside the block (its nodes are held at rest)."""
+    s = small_2d(seed=seed, G=G, nsteps=nsteps, dt=dt)
+    s.name = "small2dsphere"
+    s.objects = s.objects + [CollisionObject(SPHERE, STICK, 0.0, [0.45, 0.3], [0.08, 0])]
     return s
 
 

@@ -36,6 +36,10 @@ CASES = {
     # backward Euler (the reference's default solve), Newton tolerances as MPM_EXAMPLE's defaults
     "small3d_implicit": (lambda: S.small_3d_implicit(), [0, 1, 9], [0, 9]),
     "small2d_implicit": (lambda: S.small_2d_implicit(), [0, 9], [0, 9]),
+    # spherical collision objects (SPHERE): explicit (3D separate, 2D stick) and implicit
+    "small3d_sphere": (lambda: S.small_3d_sphere(), [0, 1, 19], [0, 19]),
+    "small2d_sphere": (lambda: S.small_2d_sphere(), [0, 19], [19]),
+    "small3d_sphere_implicit": (lambda: S.small_3d_sphere(implicit=True), [0, 7], [0, 7]),
     # Simulate_To_Frame with Compute_Dt and Reduce_Dt (steps are frames; substep counts kept)
     "small3d_adaptive": (lambda: S.small_3d_adaptive(), [0, 2], [2]),
     "small2d_adaptive": (lambda: S.small_2d_adaptive(), [0, 2], [2]),

@@ -40,7 +40,9 @@ TOL_FP64 = {"X": 1e-10, "V": 1e-7, "F": 1e-8, "B": 1e-6, "grid_m": 1e-12, "grid_
 # it), so the Wolfe search can end Newton anywhere inside the tolerance region
 # and the order of the atomic sums decides where: the state is bounded by the
 # Newton tolerance, not by rounding (the reference's float build behaves alike).
-TOL_FP32 = {"X": 1e-4, "V": 5e-2, "F": 1e-2, "B": 5e-2, "grid_m": 1e-5, "grid_v": 5e-2, "grid_vf": 5e-2}
+# The Newton tolerance (|g|_M < dt) allows velocity errors of a few 1e-2 at
+# light nodes, a few 1e-5 of position per 1e-3 step.
+TOL_FP32 = {"X": 1e-3, "V": 5e-2, "F": 1e-2, "B": 5e-2, "grid_m": 1e-5, "grid_v": 5e-2, "grid_vf": 5e-2}
 
 
 def run_implicit(name, precision, tol, grids=True):
