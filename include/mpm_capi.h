@@ -301,6 +301,27 @@ typedef struct {
 } mpm_reflection_desc;
 int mpm_set_reflection(mpm_handle* h, const mpm_reflection_desc* r);
 
+/* Penalty collision objects: one IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES per
+ * object (Deformables/Collisions_And_Interactions/
+ * IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES.cpp), added to the example's
+ * Lagrangian forces as STANDARD_TESTS_BASE::Add_Penalty_Collision_Object does
+ * (Projects/mpm/STANDARD_TESTS_BASE.cpp:555-563).  A particle whose signed
+ * distance phi to an object is at most `separation` (x = separation - phi)
+ * gets the force 3 stiffness x^2 n (n the object's normal at the particle;
+ * l.49-60, 82-85), scattered to the grid with its weights
+ * (MPM_DRIVER::Apply_Particle_Forces, MPM_DRIVER.cpp:933-945).  The implicit
+ * solve adds the energy stiffness x^3 at the particle's moved position and the
+ * Hessian 6 stiffness x n n^T - 3 stiffness x^2 Hess(phi)
+ * (MPM_EXAMPLE::Add_Forces / Add_Hessian_Times, MPM_EXAMPLE.cpp:139-177).
+ * Objects take mpm_collision_object's kind, a and b; `type` is not used and
+ * `friction` is the force's coefficient_of_friction, which the MPM substep does
+ * not apply.  The reference's scenes use stiffness 1e4 and separation 1e-4
+ * (STANDARD_TESTS_BASE.cpp:47-49).  count = 0 removes them.  Both paths (on
+ * the fast path as an impulse dt f added to the particle momentum in P2G); a
+ * batch takes none. */
+int mpm_set_penalty_objects(mpm_handle* h, const mpm_collision_object* objs, int count, double stiffness,
+                            double separation);
+
 /* ---- inspection ---------------------------------------------------------- */
 
 /* Grids of the last substep as doubles on the host, each (G+6)^d nodes (times

@@ -36,7 +36,8 @@ class _Obj(ctypes.Structure):
 class _Scene(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("counts", ctypes.c_int * 3), ("dmin", ctypes.c_double * 3),
                 ("dmax", ctypes.c_double * 3), ("model", ctypes.c_int), ("gravity", ctypes.c_double * 3),
-                ("nobj", ctypes.c_int), ("obj", _Obj * MAXOBJ)]
+                ("nobj", ctypes.c_int), ("obj", _Obj * MAXOBJ), ("npen", ctypes.c_int),
+                ("pen_stiffness", ctypes.c_double), ("pen_separation", ctypes.c_double), ("pen", _Obj * MAXOBJ)]
 
 
 def build(force: bool = False) -> str:
@@ -100,6 +101,15 @@ def _scene_struct(s) -> _Scene:
         c.obj[i].kind, c.obj[i].type, c.obj[i].friction = o.kind, o.type, o.friction
         for a in range(s.dim):
             c.obj[i].a[a], c.obj[i].b[a] = o.a[a], o.b[a]
+    pn = getattr(s, "penalty", None)
+    if pn is not None and pn.objects:
+        if len(pn.objects) > MAXOBJ:
+            raise ValueError("too many penalty objects")
+        c.npen, c.pen_stiffness, c.pen_separation = len(pn.objects), pn.stiffness, pn.separation
+        for i, o in enumerate(pn.objects):
+            c.pen[i].kind, c.pen[i].type, c.pen[i].friction = o.kind, o.type, o.friction
+            for a in range(s.dim):
+                c.pen[i].a[a], c.pen[i].b[a] = o.a[a], o.b[a]
     return c
 
 

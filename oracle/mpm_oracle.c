@@ -43,6 +43,9 @@ typedef struct {
     double gravity[3];
     int nobj;
     oracle_object obj[MAXOBJ];
+    int npen;            /* penalty collision objects (IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES) */
+    double pen_stiffness, pen_separation;
+    oracle_object pen[MAXOBJ];
 } oracle_scene;
 
 /* ------------------------------------------------------------------ */
@@ -430,6 +433,25 @@ static void obj_normal(int d, const oracle_object* o, const double* X, double* n
     for(int a = 0; a < d; a++) n[a] = o->a[a];
 }
 
+/* The force of the penalty collision objects on a particle at X, one
+ * IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES per object in order
+ * (Deformables/Collisions_And_Interactions/IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES.cpp:49-60,
+ * 82-85): where phi <= separation, x = separation - phi, a = k x^2,
+ * grad pe = -3 a n and F -= grad pe. */
+static void penalty_force(const oracle_scene* sc, const double* X, double* f)
+{
+    const int d = sc->dim;
+    for(int j = 0; j < sc->npen; j++) {
+        const oracle_object* o = sc->pen + j;
+        double phi = obj_phi(d, o, X);
+        if(phi > sc->pen_separation) continue;
+        double n[3];
+        obj_normal(d, o, X, n);
+        double x = sc->pen_separation - phi, a = sc->pen_stiffness * x * x;
+        for(int c = 0; c < d; c++) f[c] -= -3 * a * n[c];
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* the substep                                                          */
 /* ------------------------------------------------------------------ */
@@ -589,6 +611,18 @@ int oracle_substep(const oracle_scene* sc, long long n, double* X, double* V, do
     if(out_v0) memcpy(out_v0, gv0, sizeof(double) * gn * d);
 
     /* Apply_Forces, symplectic branch, MPM_DRIVER.cpp:959-1023 */
+    if(sc->npen) {   /* Apply_Particle_Forces, l.933-945: the penalty objects' particle forces, scattered */
+        for(long long k = 0; k < ns; k++) {
+            long long p = simulated[k];
+            double fp[3] = {0, 0, 0};
+            penalty_force(sc, X + p * d, fp);
+            int nn = stencil(sc, dX, W + p, gs, nodes);
+            for(int q = 0; q < nn; q++) {
+                long long i = nodes[q].idx;
+                for(int a = 0; a < d; a++) gf[i * d + a] += nodes[q].w * fp[a];
+            }
+        }
+    }
     for(long long k = 0; k < ns; k++) {       /* MPM_FINITE_ELEMENTS::Precompute */
         long long p = simulated[k];
         oracle_pft(d, sc->model, F + p * dd, mu[p], la[p], PFT + p * dd);

@@ -14,6 +14,7 @@
 // arrays (STANDARD_TESTS_BASE.cpp:372-404), MPM_PLASTICITY_CLAMP or
 // MPM_DRUCKER_PRAGER after G2P (l.409-486),
 // MPM_GRAVITY (l.354-358), collision objects through Add_Collision_Object,
+// penalty collision objects (IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES, l.555-563),
 // symplectic Euler or (scene flag) the backward-Euler Newton solve, APIC
 // (use_affine), flip=0, fixed dt.
 #include <Core/Log/LOG.h>
@@ -23,6 +24,7 @@
 #include <Geometry/Basic_Geometry/PLANE.h>
 #include <Geometry/Basic_Geometry/SPHERE.h>
 #include <Geometry/Implicit_Objects/ANALYTIC_IMPLICIT_OBJECT.h>
+#include <Deformables/Collisions_And_Interactions/IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES.h>
 #include <Deformables/Constitutive_Models/COROTATED_FIXED.h>
 #include <Deformables/Constitutive_Models/NEO_HOOKEAN.h>
 #include <Deformables/Constitutive_Models/ST_VENANT_KIRCHHOFF_HENCKY_STRAIN.h>
@@ -50,7 +52,8 @@ namespace {
 struct OBJ { int kind, type; double friction, a[3], b[3]; };
 struct SCENE_FILE
 {
-    int dim, counts[3], model, nsteps, nobj, ndump, plasticity, implicit, dt_control, reflection;
+    int dim, counts[3], model, nsteps, nobj, ndump, plasticity, implicit, dt_control, reflection, npen;
+    double pen_prm[2];   // penalty stiffness, separation
     double refl[8];   // side types (6), friction, full
     // frame_dt, cfl, min_dt, max_dt, strong_cfl, cfl_F, sound_cfl, cfl_sound
     double dtc[8];
@@ -60,7 +63,7 @@ struct SCENE_FILE
     double plastic[6];
     double dmin[3], dmax[3], gravity[3], dt, t0;
     std::vector<int> dumps;
-    std::vector<OBJ> objs;
+    std::vector<OBJ> objs, pen;
     long long n;
     std::vector<double> X, V, F, B, mass, volume, mu, lambda;
 };
@@ -76,10 +79,11 @@ SCENE_FILE Read_Scene(const char* path)
     if(!f) throw std::runtime_error("cannot open scene");
     char magic[8];
     rd(f, magic, 8);
-    if(memcmp(magic, "MPMSCN04", 8)) throw std::runtime_error("bad scene magic");
+    if(memcmp(magic, "MPMSCN05", 8)) throw std::runtime_error("bad scene magic");
     SCENE_FILE s;
-    int hdr[12];
-    rd(f, hdr, 12);
+    int hdr[13];
+    rd(f, hdr, 13);
+    s.npen = hdr[12];
     s.reflection = hdr[11];
     s.implicit = hdr[9];
     s.dt_control = hdr[10];
@@ -102,6 +106,14 @@ SCENE_FILE Read_Scene(const char* path)
     if(s.implicit) rd(f, s.implicit_prm, 4);
     if(s.dt_control) rd(f, s.dtc, 8);
     if(s.reflection) rd(f, s.refl, 8);
+    if(s.npen) {
+        rd(f, s.pen_prm, 2);
+        for(int i = 0; i < s.npen; i++) {
+            OBJ o;
+            rd(f, &o.kind, 1); rd(f, &o.type, 1); rd(f, &o.friction, 1); rd(f, o.a, 3); rd(f, o.b, 3);
+            s.pen.push_back(o);
+        }
+    }
     rd(f, &s.n, 1);
     size_t n = s.n, d = s.dim;
     s.X.resize(n * d); s.V.resize(n * d); s.F.resize(n * d * d); s.B.resize(n * d * d);
@@ -213,7 +225,25 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
             else if(o.kind == 2) this->Add_Collision_Object(SPHERE<TV>(a, (T)o.b[0]), type, (T)o.friction);
             else Add_Plane(a, b, type, (T)o.friction);
         }
+        // penalty collision objects as STANDARD_TESTS_BASE::Add_Penalty_Collision_Object
+        // adds them (Projects/mpm/STANDARD_TESTS_BASE.cpp:557-563): one force per object
+        for(const OBJ& o: s.pen) {
+            TV a, b;
+            for(int k = 0; k < d; k++) { a(k) = (T)o.a[k]; b(k) = (T)o.b[k]; }
+            IMPLICIT_OBJECT<TV>* io;
+            if(o.kind == 0) io = new ANALYTIC_IMPLICIT_OBJECT<RANGE<TV> >(RANGE<TV>(a, b));
+            else if(o.kind == 2) io = new ANALYTIC_IMPLICIT_OBJECT<SPHERE<TV> >(SPHERE<TV>(a, (T)o.b[0]));
+            else io = Plane_Object(a, b);
+            auto* pf = new IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES<TV>(particles, io, (T)s.pen_prm[0], (T)s.pen_prm[1], (T)1);
+            pf->coefficient_of_friction = (T)o.friction;
+            this->Add_Force(*pf);
+        }
     }
+
+    IMPLICIT_OBJECT<TV>* Plane_Object(const VECTOR<T, 3>& n, const VECTOR<T, 3>& x0)
+    {return new ANALYTIC_IMPLICIT_OBJECT<PLANE<T> >(PLANE<T>(n, x0));}
+    IMPLICIT_OBJECT<TV>* Plane_Object(const VECTOR<T, 2>&, const VECTOR<T, 2>&)
+    {throw std::runtime_error("plane objects are only wired for 3D in the runner");}
 
     void Add_Plane(const VECTOR<T, 3>& n, const VECTOR<T, 3>& x0, COLLISION_TYPE type, T friction)
     {this->Add_Collision_Object(PLANE<T>(n, x0), type, friction);}

@@ -219,6 +219,7 @@ int mpm_destroy(mpm_handle* h)
     implicit_free(h);
     plain_free(h);
     fast_free(h);
+    cudaFree(h->pen_f);
     cudaFree(h->d_flags);
     if(h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -495,6 +496,50 @@ int mpm_set_reflection(mpm_handle* h, const mpm_reflection_desc* r)
     h->reflect = *r;
     h->reflect.enabled = r->enabled ? 1 : 0;
     for(int k = 2 * h->sp.dim; k < 6; k++) h->reflect.side_type[k] = MPM_BC_FREE;
+    return MPM_OK;
+}
+
+int mpm_set_penalty_objects(mpm_handle* h, const mpm_collision_object* objs, int count, double stiffness,
+                            double separation)
+{
+    if(!h || count < 0 || count > MPM_MAX_OBJECTS || (count && !objs)) return MPM_ERR_ARG;
+    if(count) {
+        if(fast(h) && h->fast.batch) return set_error(h, MPM_ERR_ARG, "a batch takes no penalty objects");
+        if(!(stiffness >= 0) || !std::isfinite(stiffness) || !std::isfinite(separation))
+            return set_error(h, MPM_ERR_ARG, "penalty stiffness must be finite and >= 0, separation finite");
+    }
+    for(int i = 0; i < count; i++) {
+        const mpm_collision_object& o = objs[i];
+        if(o.kind != MPM_BOX && o.kind != MPM_PLANE && o.kind != MPM_SPHERE) return set_error(h, MPM_ERR_ARG, "unknown object kind");
+        if(o.kind == MPM_SPHERE && !(o.b[0] > 0)) return set_error(h, MPM_ERR_ARG, "sphere radius must be positive");
+        if(o.kind == MPM_BOX)
+            for(int k = 0; k < h->sp.dim; k++)
+                if(!(o.b[k] > o.a[k])) return set_error(h, MPM_ERR_ARG, "box with an empty side (RANGE::Signed_Distance)");
+    }
+    release_graph(h);
+    h->sp.npen = count;
+    h->sp.pen_stiffness = stiffness;
+    h->sp.pen_separation = separation;
+    for(int i = 0; i < count; i++) {
+        mpm::DevObject& d = h->sp.pen[i];
+        d.kind = objs[i].kind;
+        d.type = objs[i].type;
+        d.friction = objs[i].friction;
+        for(int k = 0; k < 3; k++) { d.a[k] = objs[i].a[k]; d.b[k] = objs[i].b[k]; }
+    }
+    if(fast(h) && count) {   // the fast path reads them from device memory, in float
+        mpm::DevObjectF tab[MPM_MAX_OBJECTS] = {};
+        for(int i = 0; i < count; i++) {
+            const mpm::DevObject& o = h->sp.pen[i];
+            tab[i].kind = o.kind;
+            tab[i].type = o.type;
+            tab[i].friction = (float)o.friction;
+            for(int k = 0; k < 3; k++) { tab[i].a[k] = (float)o.a[k]; tab[i].b[k] = (float)o.b[k]; }
+        }
+        if(!h->pen_f) MPM_CUDA(h, cudaMalloc(&h->pen_f, sizeof(tab)));
+        MPM_CUDA(h, cudaMemcpy(h->pen_f, tab, sizeof(tab), cudaMemcpyHostToDevice));
+        return fast_penalty_buffers(h);
+    }
     return MPM_OK;
 }
 

@@ -77,6 +77,11 @@ struct FastArgs {
     int pkind, nplas;     // plasticity kind; plastic floats per particle
     float prm[5];         // clamp: theta_c, theta_s, max_hardening, hardening_factor;
                           // Drucker-Prager: a0, a1, a3, a4, use_vc
+    const DevObjectF* pen;    // penalty collision objects (npen of them)
+    int npen;
+    float pen_k, pen_sep;     // their stiffness and separation
+    const float* vsrc;        // the velocities P2G reads (3 x npad): src's, or V + dt f / m with penalty objects
+    float* vkick;             // where k_penalty_kick writes V + dt f / m
 };
 
 __device__ __forceinline__ int64_t node_index(const SceneDev& sc, int qx, int qy, int qz)
@@ -420,7 +425,7 @@ __device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneD
     const uint32_t i = a.perm[j];
     float X[3], V[3], F[9], B[9];
 #pragma unroll
-    for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.src[(C_V + r) * a.npad + i]; }
+    for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.vsrc[r * a.npad + i]; }
 #pragma unroll
     for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; B[r] = a.src[(C_B + r) * a.npad + i]; }
     factors_from(a, sc, X, V, F, B, a.src_attr[i], j, P);   // attributes: mass, volume, mu, lambda
@@ -491,6 +496,24 @@ __device__ __forceinline__ void p2g_finish(const FastArgs& a, int* s_last)
     __threadfence();
     const uint32_t count = *(volatile uint32_t*)&a.counters[CNT_FALLBACK];
     for(uint32_t k = threadIdx.x; k < count; k += blockDim.x) p2g_fallback_force(a, k);
+}
+
+// Penalty collision objects (Apply_Particle_Forces, MPM_DRIVER.cpp:933-945):
+// per slot of the current buffer, V + dt f / m with f the objects' force at X
+// (penalty_particle in FP32).  P2G reads these velocities in place of V, so
+// the node accumulator of momentum plus impulse gains dt sum_p w_ip f_p, the
+// reference's scattered particle force times dt.
+__global__ void k_penalty_kick(FastArgs a)
+{
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        float X[3], f[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for(int r = 0; r < 3; r++) X[r] = a.src[(C_X + r) * a.npad + i];
+        penalty_particle<float, 3>(a.pen, a.npen, a.pen_k, a.pen_sep, X, f, (float*)nullptr);
+        const float s = a.dt / a.src_attr[i].x;
+#pragma unroll
+        for(int r = 0; r < 3; r++) a.vkick[r * a.npad + i] = fmaf(s, f[r], a.src[(C_V + r) * a.npad + i]);
+    }
 }
 
 // P2G variant 0: one thread per cell of the block.  A thread walks the
@@ -592,7 +615,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
             const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
             // this lane's two components: even lane (mass, x), odd lane (y, z)
             const int r0 = odd ? 1 : 0, r1 = odd ? 2 : 0;
-            float V0 = a.src[(C_V + r0) * a.npad + i], V1 = a.src[(C_V + r1) * a.npad + i];
+            float V0 = a.vsrc[r0 * a.npad + i], V1 = a.vsrc[r1 * a.npad + i];
             float B0[3], B1[3];
 #pragma unroll
             for(int c2 = 0; c2 < 3; c2++) {
@@ -1462,6 +1485,12 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.scenes = f.scenes; a.block_scene = f.block_scene; a.nb_scene = f.nb_scene; a.pbase = f.pbase;
     a.objs = f.objs;
     a.nscenes = f.nscenes;
+    a.pen = h->pen_f;
+    a.npen = h->pen_f && f.vkick ? h->sp.npen : 0;
+    a.pen_k = (float)h->sp.pen_stiffness;
+    a.pen_sep = (float)h->sp.pen_separation;
+    a.vkick = f.vkick;
+    a.vsrc = a.npen ? f.vkick : a.src + (size_t)C_V * a.npad;
     a.dt = (float)dt;
     a.flags = h->d_flags;
     const bool plastic = h->plastic.kind != MPM_PLASTICITY_NONE && f.plas[0];
@@ -1650,6 +1679,8 @@ int fast_alloc(mpm_handle* h, int64_t n)
         }
         uint32_t** ps[] = {&f.keys, &f.sorted_keys, &f.perm, &f.sort_keys_alt, &f.sort_vals_alt, &f.sort_scratch};
         for(uint32_t** p: ps) { cudaFree(*p); *p = nullptr; }
+        cudaFree(f.vkick);
+        f.vkick = nullptr;
         int64_t np = ((n ? n : 1) + 31) / 32 * 32;
         f.npad = np;
         for(int b = 0; b < 2; b++) {
@@ -1667,6 +1698,17 @@ int fast_alloc(mpm_handle* h, int64_t n)
         MPM_CUDA(h, mpm_sort::prepare());
         f.n = n;
     }
+    return fast_penalty_buffers(h);
+}
+
+// The side buffer of the penalty impulse, once there are penalty objects and particles.
+int fast_penalty_buffers(mpm_handle* h)
+{
+    FastState& f = h->fast;
+    if(h->sp.npen && f.npad && !f.vkick) {
+        f.generation++;   // make_args changes: graphs captured without the buffer are stale
+        MPM_CUDA(h, cudaMalloc(&f.vkick, 3 * f.npad * sizeof(float)));
+    }
     return MPM_OK;
 }
 
@@ -1680,7 +1722,7 @@ void fast_free(mpm_handle* h)
     void** ps[] = {(void**)&f.keys, (void**)&f.sorted_keys, (void**)&f.perm, (void**)&f.sort_keys_alt, (void**)&f.sort_vals_alt,
                    (void**)&f.sort_scratch, (void**)&f.bstart, (void**)&f.bend, (void**)&f.active, (void**)&f.nb_flag,
                    (void**)&f.nb_list, (void**)&f.counters, (void**)&f.acc, (void**)&f.vel, (void**)&f.scenes,
-                   (void**)&f.block_scene, (void**)&f.nb_scene, (void**)&f.pbase, (void**)&f.objs};
+                   (void**)&f.block_scene, (void**)&f.nb_scene, (void**)&f.pbase, (void**)&f.objs, (void**)&f.vkick};
     for(void** p: ps) { cudaFree(*p); *p = nullptr; }
     cudaFree(f.staging);
     f.staging = nullptr;
@@ -1967,6 +2009,10 @@ int fast_p2g(mpm_handle* h, double dt, double)
     if(rc) return rc;
     FastArgs a = make_args(h, dt);
     int slot = timer_begin(h, "fast_p2g");
+    if(a.npen) {
+        k_penalty_kick<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(a);
+        MPM_LAUNCHED(h, "k_penalty_kick");
+    }
     if(f.p2g_variant == 0) k_p2g_cells<<<occupancy_ctas(h, (const void*)k_p2g_cells, 64, f.cta_mult), 64, 0, h->stream>>>(a);
     else {
         if(f.p2g_variant == 1)

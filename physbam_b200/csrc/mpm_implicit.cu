@@ -42,6 +42,7 @@ template<class T> struct ImpArgs {
     double* pe;                 // per-particle potential energy
     uint8_t *cmask, *stuck;     // per node: collision objects (bit j), stuck flag
     T* cdat;                    // per node and object: phi, n_dE, normal, position, H g (2 + 3d)
+    T* pen;                     // per particle: penalty force (d) and Hessian (d x d) at the current X
     int nobj;
     const uint32_t* order;      // particles sorted by cell (the passes visit them in this order)
 };
@@ -151,7 +152,18 @@ template<class T, int d> __global__ void k_imp_precompute(ImpArgs<T> ia)
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if(t >= a.n) return;
     const int64_t p = particle_at(ia, t);
-    if(!a.valid[p]) { ia.pe[p] = 0; return; }
+    // IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES::Update_Position_Based_State
+    // runs over every particle, simulated or not (its energy counts them all).
+    double epen = 0;
+    if(a.sp.npen) {
+        T fp[3] = {0, 0, 0}, Hp[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        epen = (double)penalty_particle<T, d>(a.sp.pen, a.sp.npen, (T)a.sp.pen_stiffness, (T)a.sp.pen_separation,
+                                              a.X + p * d, fp, Hp);
+        T* q = ia.pen + p * (d + d * d);
+        for(int e = 0; e < d; e++) q[e] = fp[e];
+        for(int e = 0; e < d * d; e++) q[d + e] = Hp[e];
+    }
+    if(!a.valid[p]) { ia.pe[p] = epen; return; }
     T F[9], U[9], V[9], S[3], P[3];
 #pragma unroll
     for(int e = 0; e < d * d; e++) F[e] = a.F[p * d * d + e];
@@ -190,10 +202,11 @@ template<class T, int d> __global__ void k_imp_precompute(ImpArgs<T> ia)
     for(int e = 0; e < 3; e++) { ia.dP[p * 15 + 9 + e] = Bv[e]; ia.dP[p * 15 + 12 + e] = Cv[e]; }
     double e = (double)a.vol[p] * (double)energy_density<T, d>(a.sp.model, S, mu, la);
     for(int k = 0; k < d; k++) e -= (double)a.mass[p] * (double)a.X[p * d + k] * a.sp.gravity[k];
-    ia.pe[p] = e;
+    ia.pe[p] = e + epen;
 }
 
-// MPM_FINITE_ELEMENTS::Add_Forces (l.84-99) + MPM_GRAVITY::Add_Forces (l.62-68).
+// MPM_FINITE_ELEMENTS::Add_Forces (l.84-99) + MPM_GRAVITY::Add_Forces (l.62-68)
+// + the penalty forces of MPM_EXAMPLE::Add_Forces (MPM_EXAMPLE.cpp:139-153).
 template<class T, int d> __global__ void k_imp_forces(ImpArgs<T> ia, T* f)
 {
     const PlainArgs<T>& a = ia.a;
@@ -207,6 +220,9 @@ template<class T, int d> __global__ void k_imp_forces(ImpArgs<T> ia, T* f)
 #pragma unroll
     for(int e = 0; e < d * d; e++) A[e] = a.pft[p * d * d + e] * a.vol[p];
     const T mp = a.mass[p];
+    T fp[3] = {0, 0, 0};
+    if(a.sp.npen)
+        for(int e = 0; e < d; e++) fp[e] = ia.pen[p * (d + d * d) + e];
     const int nq = d == 3 ? 27 : 9;
     for(int q = 0; q < nq; q++) {
         int64_t i;
@@ -217,13 +233,15 @@ template<class T, int d> __global__ void k_imp_forces(ImpArgs<T> ia, T* f)
             T sum = 0;
 #pragma unroll
             for(int c = 0; c < d; c++) sum += A[r + d * c] * g[c];
-            atomicAdd(f + i * d + r, -sum + w * mp * (T)a.sp.gravity[r]);
+            atomicAdd(f + i * d + r, -sum + w * mp * (T)a.sp.gravity[r] + w * fp[r]);
         }
     }
 }
 
 // MPM_FINITE_ELEMENTS::Add_Hessian_Times (l.103-132): W = sum z_i grad w_i^T,
-// M = U dPhat(U^T W FV) FV^T vol, f_i += M grad w_i.
+// M = U dPhat(U^T W FV) FV^T vol, f_i += M grad w_i; with penalty objects also
+// MPM_EXAMPLE::Add_Hessian_Times' Lagrangian part (MPM_EXAMPLE.cpp:157-177):
+// z_p = sum w_i z_i, f_i += w_i H_p z_p.
 template<class T, int d> __global__ void k_imp_hessian(ImpArgs<T> ia, const T* z, T* f)
 {
     const PlainArgs<T>& a = ia.a;
@@ -233,16 +251,30 @@ template<class T, int d> __global__ void k_imp_hessian(ImpArgs<T> ia, const T* z
     if(!a.valid[p]) return;
     Stencil<T, d> s;
     if(!make_stencil<T, d>(a, ia.X0 + p * d, s)) return;
-    T W[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    T W[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, zp[3] = {0, 0, 0};
+    const bool pen = a.sp.npen != 0;
     const int nq = d == 3 ? 27 : 9;
     for(int q = 0; q < nq; q++) {
         int64_t i;
         T w, g[3], Z[3];
         node<T, d>(a, s, q, i, w, g, Z);
 #pragma unroll
-        for(int r = 0; r < d; r++)
+        for(int r = 0; r < d; r++) {
 #pragma unroll
             for(int c = 0; c < d; c++) W[r + d * c] += z[i * d + r] * g[c];
+            if(pen) zp[r] += w * z[i * d + r];
+        }
+    }
+    T Hz[3] = {0, 0, 0};
+    if(pen) {
+        const T* Hp = ia.pen + p * (d + d * d) + d;
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T sum = 0;
+#pragma unroll
+            for(int c = 0; c < d; c++) sum += Hp[r + d * c] * zp[c];
+            Hz[r] = sum;
+        }
     }
     const T* U = ia.U + p * d * d;
     const T* FV = ia.FV + p * d * d;
@@ -295,7 +327,7 @@ template<class T, int d> __global__ void k_imp_hessian(ImpArgs<T> ia, const T* z
             T sum = 0;
 #pragma unroll
             for(int c = 0; c < d; c++) sum += M[r + d * c] * g[c];
-            atomicAdd(f + i * d + r, sum);
+            atomicAdd(f + i * d + r, sum + w * Hz[r]);
         }
     }
 }
@@ -584,7 +616,7 @@ struct ImplicitState {
     int nobj = 0, d = 0;
     size_t esz = 0;
     void* vec = nullptr;           // V_COUNT node vectors of gn * d scalars
-    void* part = nullptr;          // F0, X0, U, FV, sig, dP
+    void* part = nullptr;          // F0, X0, U, FV, sig, dP, pen
     double* pe = nullptr;
     uint8_t* cmask = nullptr;
     uint8_t* stuck = nullptr;
@@ -615,7 +647,7 @@ template<class T, int d> struct Solver {
         const int64_t n = s.n ? s.n : 1;
         T* P = (T*)s.part;
         ia.F0 = P; ia.X0 = P + n * d * d; ia.U = ia.X0 + n * d; ia.FV = ia.U + n * d * d;
-        ia.sig = ia.FV + n * d * d; ia.dP = ia.sig + n * d;
+        ia.sig = ia.FV + n * d * d; ia.dP = ia.sig + n * d; ia.pen = ia.dP + n * 15;
         ia.pe = s.pe; ia.cmask = s.cmask; ia.stuck = s.stuck; ia.cdat = (T*)s.cdat; ia.nobj = h->sp.nobj;
         ia.order = nullptr;
         for(int k = 0; k < V_COUNT; k++) v[k] = (T*)s.vec + (size_t)k * s.gn * d;
@@ -911,7 +943,7 @@ template<class T> int ensure_state(mpm_handle* h)
     t.gn = ps.gn; t.n = ps.n; t.nobj = h->sp.nobj; t.d = d; t.esz = e;
     const int64_t n = t.n ? t.n : 1;
     MPM_CUDA(h, cudaMalloc(&t.vec, (size_t)V_COUNT * t.gn * d * e));
-    MPM_CUDA(h, cudaMalloc(&t.part, (size_t)n * (d * d * 3 + d * 2 + 15) * e));
+    MPM_CUDA(h, cudaMalloc(&t.part, (size_t)n * (d * d * 4 + d * 3 + 15) * e));
     MPM_CUDA(h, cudaMalloc(&t.pe, (size_t)n * sizeof(double)));
     MPM_CUDA(h, cudaMalloc(&t.cmask, (size_t)t.gn));
     MPM_CUDA(h, cudaMalloc(&t.stuck, (size_t)t.gn));

@@ -18,6 +18,9 @@ struct SceneParams {
     double gravity[3];
     int nobj;
     mpm::DevObject objs[MPM_MAX_OBJECTS];
+    int npen;                                   // penalty collision objects (plain path)
+    double pen_stiffness, pen_separation;
+    mpm::DevObject pen[MPM_MAX_OBJECTS];
 };
 
 // Reference-layout device arrays for the plain path (one thread per particle).
@@ -82,6 +85,7 @@ struct FastState {
     uint32_t* counters = nullptr;             // see FastCounter
     float4* acc = nullptr;                    // P2G accumulator: momentum+dt*force (xyz), mass (w)
     float4* vel = nullptr;                    // per node 2 x float4: vnew.xyz, vfric.x | vfric.yz, mass, 0
+    float* vkick = nullptr;                   // penalty objects on: 3 * npad floats, V + dt f / m per slot
     bool keys_ready = false;
     bool hist_ready = false;
     uint64_t generation = 0;   // bumped whenever device buffers are (re)allocated
@@ -129,6 +133,7 @@ struct mpm_handle {
     mpm_grid_desc grid{};
     mpm_model_desc model{};
     SceneParams sp{};
+    mpm::DevObjectF* pen_f = nullptr;   // penalty objects rounded to float (fast path), MPM_MAX_OBJECTS
     int64_t n = 0;
     bool have_particles = false;
     unsigned* d_flags = nullptr;
@@ -172,6 +177,7 @@ int plain_count_valid(mpm_handle* h, int64_t* c);
 // fast path (mpm_fast.cu)
 int fast_alloc(mpm_handle* h, int64_t n);
 void fast_free(mpm_handle* h);
+int fast_penalty_buffers(mpm_handle* h);
 int fast_set_particles(mpm_handle* h, const mpm_particles_view* v);
 int fast_get_particles(mpm_handle* h, mpm_particles_view* v);
 int fast_p2g(mpm_handle* h, double dt, double time);

@@ -680,6 +680,40 @@ template<class T, int d, class O> __device__ void object_hessian(const O& o, con
         for(int b = 0; b < d; b++) H[a + d * b] = ((a == b ? D[a] : (T)0) - z[a] * z[b]) / w;
 }
 
+// Penalty collision objects at one particle position, one
+// IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES per object, in object order
+// (Update_Position_Based_State_Particle,
+// Deformables/Collisions_And_Interactions/IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES.cpp:49-60):
+// where phi <= sep, x = sep - phi and a = k x^2, the energy a x, the force
+// -grad pe = 3 a n (Add_Velocity_Independent_Forces, l.82-85) added to f, and
+// the Hessian 6 k x n n^T - 3 a Hess(phi) added to H (when H is not null).
+// Returns the energy.
+template<class T, int d, class O> __device__ T penalty_particle(const O* objs, int nobj, T k, T sep, const T* X, T* f, T* H)
+{
+    T e = 0;
+    for(int j = 0; j < nobj; j++) {
+        const T phi = object_phi<T, d>(objs[j], X);
+        if(phi > sep) continue;
+        T n[3];
+        object_normal<T, d>(objs[j], X, n);
+        const T x = sep - phi, a = k * x * x;
+        e += a * x;
+        const T ga = (T)-3 * a;   // grad pe = -3 a n
+#pragma unroll
+        for(int r = 0; r < d; r++) f[r] -= ga * n[r];
+        if(H) {
+            T Hp[9];
+            object_hessian<T, d>(objs[j], X, Hp);
+            const T s = (T)6 * k * x, t = (T)3 * a;
+#pragma unroll
+            for(int c = 0; c < d; c++)
+#pragma unroll
+                for(int r = 0; r < d; r++) H[r + d * c] += s * (n[r] * n[c]) - t * Hp[r + d * c];
+        }
+    }
+    return e;
+}
+
 // Grid-node collision projection and Coulomb friction for one node.
 // MPM_OBJECTIVE::Test_Add_Collision / Adjust_For_Collision
 // (Hybrid_Methods/System/MPM_OBJECTIVE.cpp:150-225), MPM_DRIVER::Apply_Friction

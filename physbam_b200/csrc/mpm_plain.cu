@@ -90,8 +90,9 @@ template<class T, int d> __global__ void k_stress(PlainArgs<T> a)
     for(int e = 0; e < d * d; e++) a.pft[p * d * d + e] = PFT[e];
 }
 
-// MPM_FINITE_ELEMENTS::Add_Forces (MPM_FINITE_ELEMENTS.cpp:84-99) and
-// MPM_GRAVITY::Add_Forces (MPM_GRAVITY.cpp:62-68) in one pass.
+// MPM_FINITE_ELEMENTS::Add_Forces (MPM_FINITE_ELEMENTS.cpp:84-99),
+// MPM_GRAVITY::Add_Forces (MPM_GRAVITY.cpp:62-68) and the penalty collision
+// forces of Apply_Particle_Forces (MPM_DRIVER.cpp:933-945) in one pass.
 template<class T, int d> __global__ void k_forces(PlainArgs<T> a)
 {
     int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -102,6 +103,10 @@ template<class T, int d> __global__ void k_forces(PlainArgs<T> a)
 #pragma unroll
     for(int e = 0; e < d * d; e++) A[e] = a.pft[p * d * d + e] * a.vol[p];
     T mp = a.mass[p];
+    T fp[3] = {0, 0, 0};   // the particle's penalty force
+    if(a.sp.npen)
+        penalty_particle<T, d>(a.sp.pen, a.sp.npen, (T)a.sp.pen_stiffness, (T)a.sp.pen_separation, a.X + p * d, fp,
+                               (T*)nullptr);
     const int nq = d == 3 ? 27 : 9;
     for(int q = 0; q < nq; q++) {
         int64_t i;
@@ -113,7 +118,7 @@ template<class T, int d> __global__ void k_forces(PlainArgs<T> a)
             T sum = 0;
 #pragma unroll
             for(int c = 0; c < d; c++) sum += A[r + d * c] * g[c];
-            atomicAdd(a.gf + i * d + r, -sum + wm * (T)a.sp.gravity[r]);
+            atomicAdd(a.gf + i * d + r, -sum + wm * (T)a.sp.gravity[r] + w * fp[r]);
         }
     }
 }

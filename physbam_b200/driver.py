@@ -117,7 +117,7 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex",
            "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state", "mpm_set_implicit",
            "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt",
-           "mpm_set_reflection"]
+           "mpm_set_reflection", "mpm_set_penalty_objects"]
 
 _lib = None
 
@@ -168,6 +168,8 @@ def load_library(path: str = LIB_PATH):
                                      ctypes.POINTER(ctypes.c_int)]
     L.mpm_last_dt.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
     L.mpm_set_reflection.argtypes = [P, ctypes.POINTER(ReflectionDesc)]
+    L.mpm_set_penalty_objects.argtypes = [P, ctypes.POINTER(CollisionObject), ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_double]
     L.mpm_status_string.argtypes = [ctypes.c_int]
     L.mpm_status_string.restype = ctypes.c_char_p
     for f in EXPORTS:
@@ -212,6 +214,8 @@ class MPM_DRIVER:
             self.set_dt_control(scene.dt_control)
         if scene.reflection is not None:
             self.set_reflection(scene.reflection)
+        if scene.penalty is not None:
+            self.set_penalty(scene.penalty)
         self.time = 0.0
         self.n = 0
 
@@ -242,6 +246,18 @@ class MPM_DRIVER:
             for a in range(self.dim):
                 arr[i].a[a], arr[i].b[a] = o.a[a], o.b[a]
         self._check(self.L.mpm_set_collision_objects(self.h, arr, len(objects)), "mpm_set_collision_objects")
+
+    def set_penalty(self, penalty: Optional[S.Penalty]):
+        """Penalty collision objects (IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES, one per object);
+        None removes them."""
+        objects = penalty.objects if penalty is not None else []
+        arr = (CollisionObject * max(len(objects), 1))()
+        for i, o in enumerate(objects):
+            arr[i].kind, arr[i].type, arr[i].friction = o.kind, o.type, o.friction
+            for a in range(self.dim):
+                arr[i].a[a], arr[i].b[a] = o.a[a], o.b[a]
+        k, sep = (penalty.stiffness, penalty.separation) if penalty is not None else (0.0, 0.0)
+        self._check(self.L.mpm_set_penalty_objects(self.h, arr, len(objects), k, sep), "mpm_set_penalty_objects")
 
     def set_particles(self, X, V, F, B, mass, volume, mu, lam, valid=None, dtype=np.float64):
         """Arrays in the reference layout: X,V (n,d); F,B (n,d,d) row/col as numpy matrices."""
@@ -668,6 +684,8 @@ class MPM_BATCH(MPM_DRIVER):
         L.mpm_batch_create.restype = ctypes.c_int
         self.scenes = list(scenes_list)
         self.scene = self.scenes[0]
+        if any(s.penalty is not None for s in self.scenes):
+            raise ValueError("a batch takes no penalty collision objects")
         self.dim = 3
         self.precision, self.path = FP32, PATH_FAST
         descs = (SceneDesc * len(self.scenes))()

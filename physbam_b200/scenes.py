@@ -159,6 +159,21 @@ class Reflection:
 
 
 @dataclasses.dataclass
+class Penalty:
+    """Penalty collision objects: one IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES per object, as
+    `STANDARD_TESTS_BASE::Add_Penalty_Collision_Object` adds them with -use_penalty_collisions
+    (`Projects/mpm/STANDARD_TESTS_BASE.cpp:555-563`).  A particle within `separation` of an
+    object (phi <= separation, x = separation - phi) is pushed along the object's normal with
+    the force 3 stiffness x^2; the implicit solve adds its energy stiffness x^3 and Hessian.
+    Defaults as STANDARD_TESTS_BASE (stiffness 1e4, separation 1e-4).  The objects'
+    `type` is not used; `friction` is the force's coefficient_of_friction, which the MPM
+    substep does not apply."""
+    objects: List[CollisionObject]
+    stiffness: float = 1e4
+    separation: float = 1e-4
+
+
+@dataclasses.dataclass
 class Scene:
     name: str
     dim: int
@@ -182,6 +197,7 @@ class Scene:
     implicit: Optional[Implicit] = None
     dt_control: Optional[DtControl] = None     # set: nsteps counts frames of frame_dt
     reflection: Optional[Reflection] = None
+    penalty: Optional[Penalty] = None
 
     @property
     def n(self) -> int:
@@ -463,6 +479,34 @@ def small_2d_sphere(seed=73, G=16, nsteps=20, dt=1e-4):
     return s
 
 
+def small_3d_penalty(seed=81, G=16, nsteps=20, dt=1e-4, implicit=False):
+    """small_3d with penalty collision objects overlapping the block: a ball on its +x side,
+    a slab under its floor and a plane through its -z side (the walls stay as ordinary
+    collision objects).  Particles start up to 7 cm deep in the ball, so the penalty forces,
+    and in the implicit solve their Hessians with the ball's curvature, are far from zero."""
+    s = small_3d(seed=seed, G=G, nsteps=nsteps, dt=dt, friction=0.2, v=(1.0, -1.5, 0.5))
+    s.name = "small3dpenalty"
+    s.penalty = Penalty([CollisionObject(SPHERE, SLIP, 0.3, [0.62, 0.33, 0.52], [0.09, 0, 0]),
+                         CollisionObject(BOX, SLIP, 0.0, [-1.0, -1.0, -1.0], [2.0, 0.135, 2.0]),
+                         CollisionObject(PLANE, SLIP, 0.0, [0.0, 0.0, 1.0], [0.0, 0.0, 0.31])])
+    if implicit:
+        s.name = "small3dpenaltyimplicit"
+        s.dt = 1e-3
+        s.nsteps = 8
+        s.implicit = Implicit()
+    return s
+
+
+def small_2d_penalty(seed=83, G=16, nsteps=20, dt=1e-4):
+    """small_2d with a penalty circle on the block's +x side and a penalty slab under it,
+    with stiffness 2e4 and a wider separation (5e-3)."""
+    s = small_2d(seed=seed, G=G, nsteps=nsteps, dt=dt)
+    s.name = "small2dpenalty"
+    s.penalty = Penalty([CollisionObject(SPHERE, SLIP, 0.0, [0.7, 0.4], [0.1, 0]),
+                         CollisionObject(BOX, SLIP, 0.0, [-1.0, -1.0], [2.0, 0.215])], stiffness=2e4, separation=5e-3)
+    return s
+
+
 def small_3d_adaptive(seed=51, G=16, nframes=3):
     """A stiff small_3d (E 2e6..8e6) run frame by frame as Simulate_To_Frame does,
     with the strong and the sound-speed CFL on: the sound speed shortens most steps."""
@@ -564,7 +608,7 @@ def snowballs_3d(seed=1234, G=128, ppc=8, E=1.4e5, nu=0.2, density=400.0, dt=5e-
 # --------------------------------------------------------------------------------------------
 # Scene file: read by the reference runner (oracle/ref_scene.cpp) and by the C oracle harness.
 # --------------------------------------------------------------------------------------------
-MAGIC = b"MPMSCN04"
+MAGIC = b"MPMSCN05"
 
 
 def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
@@ -575,9 +619,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         f.write(MAGIC)
         counts = list(s.counts) + [1] * (3 - d)
         pl = s.plasticity
-        im, dc, rf = s.implicit, s.dt_control, s.reflection
-        f.write(struct.pack("<12i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
-                            1 if im else 0, 1 if dc else 0, 1 if rf else 0))
+        im, dc, rf, pn = s.implicit, s.dt_control, s.reflection, s.penalty
+        f.write(struct.pack("<13i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
+                            1 if im else 0, 1 if dc else 0, 1 if rf else 0, len(pn.objects) if pn else 0))
         f.write(struct.pack("<11d", *pad3(s.domain_min), *pad3(s.domain_max), *pad3(s.gravity), s.dt, 0.0))
         f.write(struct.pack("<%di" % len(dumps), *dumps))
         for o in s.objects:
@@ -594,6 +638,10 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         if rf:
             sides = list(rf.side_type) + [BC_FREE] * (6 - len(rf.side_type))
             f.write(struct.pack("<8d", *[float(x) for x in sides], rf.friction, 1.0 if rf.full else 0.0))
+        if pn and pn.objects:
+            f.write(struct.pack("<2d", pn.stiffness, pn.separation))
+            for o in pn.objects:
+                f.write(struct.pack("<2i7d", o.kind, o.type, o.friction, *pad3(o.a), *pad3(o.b)))
         f.write(struct.pack("<q", s.n))
         f.write(np.ascontiguousarray(s.X, np.float64).tobytes())
         f.write(np.ascontiguousarray(s.V, np.float64).tobytes())

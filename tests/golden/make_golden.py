@@ -49,6 +49,10 @@ CASES = {
     # sand: ST_VENANT_KIRCHHOFF_HENCKY_STRAIN + MPM_DRUCKER_PRAGER (Fp, plastic_def, rho_F, sigma_Y, vc dumped)
     "smallsand3d_hencky": (lambda: S.small_sand_3d(), [0, 1, 19], [0, 19]),
     "smallsand2d_hencky": (lambda: S.small_sand_2d(), [0, 19], [19]),
+    # penalty collision objects (IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES): explicit and implicit
+    "small3d_penalty": (lambda: S.small_3d_penalty(), [0, 1, 19], [0, 19]),
+    "small2d_penalty": (lambda: S.small_2d_penalty(), [0, 19], [0, 19]),
+    "small3d_penalty_implicit": (lambda: S.small_3d_penalty(implicit=True), [0, 7], [0, 7]),
 }
 
 
@@ -86,6 +90,14 @@ def main(names=None):
             arrays["dt_control"] = np.array([dc.frame_dt, dc.cfl, dc.min_dt, dc.max_dt, float(dc.strong_cfl), dc.cfl_F,
                                              float(dc.sound_cfl), dc.cfl_sound])
             arrays["frame_substeps"] = np.array(frames["frame_substeps"], np.int32)
+        pn = scene.penalty
+        if pn is not None:
+            arrays["penalty"] = np.array([pn.stiffness, pn.separation], np.float64)
+            arrays["pen_kind"] = np.array([o.kind for o in pn.objects], np.int32)
+            arrays["pen_type"] = np.array([o.type for o in pn.objects], np.int32)
+            arrays["pen_friction"] = np.array([o.friction for o in pn.objects])
+            arrays["pen_a"] = np.array([o.a for o in pn.objects]).reshape(-1, scene.dim)
+            arrays["pen_b"] = np.array([o.b for o in pn.objects]).reshape(-1, scene.dim)
         im = scene.implicit
         if im is not None:
             arrays["implicit"] = np.array([im.newton_tolerance, im.newton_iterations, im.solver_tolerance,
@@ -122,6 +134,10 @@ def load(name):
                                        bool(c[6]), float(c[7]))
         dumps_meta = {"frame_substeps": [int(x) for x in z["frame_substeps"]]}
         scene.frame_substeps = dumps_meta["frame_substeps"]
+    if "penalty" in z:
+        pobjs = [S.CollisionObject(int(k), int(t), float(f), list(a), list(b))
+                 for k, t, f, a, b in zip(z["pen_kind"], z["pen_type"], z["pen_friction"], z["pen_a"], z["pen_b"])]
+        scene.penalty = S.Penalty(pobjs, float(z["penalty"][0]), float(z["penalty"][1]))
     if "implicit" in z:
         im = z["implicit"]
         scene.implicit = S.Implicit(float(im[0]), int(im[1]), float(im[2]), int(im[3]))
