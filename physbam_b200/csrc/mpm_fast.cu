@@ -41,6 +41,14 @@ using namespace mpm;
 constexpr int BS = 4;                      // cells per particle-block edge
 constexpr int TE = BS + 2;                 // tile edge in nodes
 constexpr int TN = TE * TE * TE;           // 216 nodes per tile
+// P2G tile layout: node (x, y, z) of the 6^3 tile at x PSX + y PSY + z.  With
+// these strides the 32 cells of a warp-aligned half block (cell = lx << 4 |
+// ly << 2 | lz, lx in {0, 1} or {2, 3}) reach 32 distinct shared-memory banks
+// at every node offset (52 lx + 8 ly + lz is distinct mod 32), where the
+// dense 6-stride layout put up to four lanes on one bank.
+constexpr int PSY = 8, PSX = 52;
+constexpr int PTN = (TE - 1) * PSX + (TE - 1) * PSY + TE;   // 306 floats per quantity
+__host__ __device__ constexpr int ptile(int x, int y, int z) { return x * PSX + y * PSY + z; }
 constexpr uint32_t SENTINEL = 0xffffffffu;
 constexpr int NCOMP = 24;                  // x3 v3 F9 B9 floats per particle
 constexpr int C_X = 0, C_V = 3, C_F = 6, C_B = 15;
@@ -289,7 +297,7 @@ __device__ __forceinline__ int next_work(uint32_t* ctr, int* s_work)
 }
 
 struct P2GTile {
-    float m[TN], x[TN], y[TN], z[TN];
+    float m[PTN], x[PTN], y[PTN], z[PTN];
     uint32_t ccount[64], cstart[64];
     uint32_t maxc;
     SceneDev sc;
@@ -301,7 +309,7 @@ struct P2GTile {
 __device__ __forceinline__ void p2g_begin(const FastArgs& a, P2GTile& T, uint32_t b)
 {
     stage_scene(a, a.block_scene[b], &T.sc);
-    for(int t = threadIdx.x; t < TN; t += blockDim.x) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+    for(int t = threadIdx.x; t < PTN; t += blockDim.x) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
     if(threadIdx.x < 64) T.ccount[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t s = a.bstart[b], e = a.bend[b];
@@ -333,11 +341,10 @@ __device__ __forceinline__ void p2g_end(const FastArgs& a, P2GTile& T, uint32_t 
     int bx, by, bz;
     block_coords(sc, lb, bx, by, bz);
     for(int t = threadIdx.x; t < TN; t += blockDim.x) {
-        float mm = T.m[t];
-        if(mm != 0.f) {
-            int qx = 4 * bx + t / (TE * TE), qy = 4 * by + (t / TE) % TE, qz = 4 * bz + t % TE;
-            atomicAdd(&a.acc[node_index(sc, qx, qy, qz)], make_float4(T.x[t], T.y[t], T.z[t], mm));
-        }
+        const int tx = t / (TE * TE), ty = (t / TE) % TE, tz = t % TE, u = ptile(tx, ty, tz);
+        float mm = T.m[u];
+        if(mm != 0.f)
+            atomicAdd(&a.acc[node_index(sc, 4 * bx + tx, 4 * by + ty, 4 * bz + tz)], make_float4(T.x[u], T.y[u], T.z[u], mm));
     }
     if(threadIdx.x < 8) {
         int nx = bx + (threadIdx.x >> 2), ny = by + ((threadIdx.x >> 1) & 1), nz = bz + (threadIdx.x & 1);
@@ -543,14 +550,14 @@ __global__ void __launch_bounds__(64) k_p2g_cells(FastArgs a)
                     am[q] += m; ax[q] += px; ay[q] += py; az[q] += pz;
                 });
             }
-            const int t0 = (lx * TE + ly) * TE + lz;
+            const int t0 = ptile(lx, ly, lz);
 #pragma unroll
             for(int ii = 0; ii < 3; ii++)
 #pragma unroll
                 for(int jj = 0; jj < 3; jj++)
 #pragma unroll
                     for(int kk = 0; kk < 3; kk++) {
-                        const int q = (ii * 3 + jj) * 3 + kk, t = t0 + (ii * TE + jj) * TE + kk;
+                        const int q = (ii * 3 + jj) * 3 + kk, t = t0 + ptile(ii, jj, kk);
                         atomicAdd(&T.m[t], am[q]);
                         atomicAdd(&T.x[t], ax[q]);
                         atomicAdd(&T.y[t], ay[q]);
@@ -578,7 +585,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
     for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
         const uint32_t b = a.active[w];
         stage_scene(a, a.block_scene[b], &T.sc);
-        for(int t = threadIdx.x; t < TN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+        for(int t = threadIdx.x; t < PTN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
         __syncthreads();
         const SceneDev& sc = T.sc;
         const uint32_t s = a.bstart[b], e = a.bend[b];
@@ -594,10 +601,10 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
             const int c = (int)(a.sorted_keys[j] & 63u);
             if(c != cell) {
                 if(cell >= 0) {
-                    const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+                    const int t0 = ptile(cell >> 4, (cell >> 2) & 3, cell & 3);
 #pragma unroll
                     for(int q = 0; q < 27; q++) {
-                        const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+                        const int t = t0 + ptile(q / 9, (q / 3) % 3, q % 3);
                         atomicAdd(&out0[t], acc0[q]);
                         atomicAdd(&out1[t], acc1[q]);
                         acc0[q] = 0.f;
@@ -671,10 +678,10 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
                 }
         }
         if(cell >= 0) {
-            const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+            const int t0 = ptile(cell >> 4, (cell >> 2) & 3, cell & 3);
 #pragma unroll
             for(int q = 0; q < 27; q++) {
-                const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+                const int t = t0 + ptile(q / 9, (q / 3) % 3, q % 3);
                 atomicAdd(&out0[t], acc0[q]);
                 atomicAdd(&out1[t], acc1[q]);
             }
@@ -740,10 +747,10 @@ __device__ __forceinline__ void pair_accumulate(const float* w, const PairSlot& 
 
 __device__ __forceinline__ void pair_flush(int cell, float* out0, float* out1, float* acc0, float* acc1)
 {
-    const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+    const int t0 = ptile(cell >> 4, (cell >> 2) & 3, cell & 3);
 #pragma unroll
     for(int q = 0; q < 27; q++) {
-        const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+        const int t = t0 + ptile(q / 9, (q / 3) % 3, q % 3);
         atomicAdd(&out0[t], acc0[q]);
         atomicAdd(&out1[t], acc1[q]);
         acc0[q] = 0.f;
@@ -757,6 +764,22 @@ __device__ __forceinline__ void pair_flush(int cell, float* out0, float* out1, f
 // 27 node values of all four quantities go straight to the shared tile, so
 // the kernel needs few registers and keeps many warps in flight, at the price
 // of four shared atomics per node.
+
+// One particle of the interleaved variant: its 27 x 4 node values straight to the tile.
+__device__ __forceinline__ void interleaved_particle(const FastArgs& a, P2GTile& T, uint32_t j, uint32_t c)
+{
+    P2GFactors P;
+    particle_factors(a, T.sc, j, P);
+    const int t0 = ptile(c >> 4, (c >> 2) & 3, c & 3);
+    factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
+        const int t = t0 + ptile(ii, jj, kk);
+        atomicAdd(&T.m[t], m);
+        atomicAdd(&T.x[t], px);
+        atomicAdd(&T.y[t], py);
+        atomicAdd(&T.z[t], pz);
+    });
+}
+
 template<int THREADS> __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_p2g_interleaved(FastArgs a)
 {
     __shared__ P2GTile T;
@@ -767,17 +790,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
         const uint32_t s = a.bstart[b], slots = T.maxc * 64u;
         for(uint32_t q = threadIdx.x; q < slots; q += THREADS) {
             const uint32_t c = q & 63u, r = q >> 6;
-            if(r >= T.ccount[c]) continue;
-            P2GFactors P;
-            particle_factors(a, T.sc, s + T.cstart[c] + r, P);
-            const int t0 = ((c >> 4) * TE + ((c >> 2) & 3)) * TE + (c & 3);
-            factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
-                const int t = t0 + (ii * TE + jj) * TE + kk;
-                atomicAdd(&T.m[t], m);
-                atomicAdd(&T.x[t], px);
-                atomicAdd(&T.y[t], py);
-                atomicAdd(&T.z[t], pz);
-            });
+            if(r < T.ccount[c]) interleaved_particle(a, T, s + T.cstart[c] + r, c);
         }
         p2g_end(a, T, b - T.sc.block_base);
     }
@@ -799,7 +812,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
     for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
         const uint32_t b = a.active[w];
         stage_scene(a, a.block_scene[b], &T.sc);
-        for(int t = threadIdx.x; t < TN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+        for(int t = threadIdx.x; t < PTN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
         __syncthreads();
         const SceneDev& sc = T.sc;
         const uint32_t s = a.bstart[b], e = a.bend[b];
@@ -873,10 +886,10 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
             }
         }
         if(cell >= 0) {
-            const int t0 = ((cell >> 4) * TE + ((cell >> 2) & 3)) * TE + (cell & 3);
+            const int t0 = ptile(cell >> 4, (cell >> 2) & 3, cell & 3);
 #pragma unroll
             for(int q = 0; q < 27; q++) {
-                const int t = t0 + ((q / 9) * TE + (q / 3) % 3) * TE + q % 3;
+                const int t = t0 + ptile(q / 9, (q / 3) % 3, q % 3);
                 atomicAdd(&out0[t], acc0[q]);
                 atomicAdd(&out1[t], acc1[q]);
             }
