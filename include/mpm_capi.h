@@ -322,6 +322,30 @@ int mpm_set_reflection(mpm_handle* h, const mpm_reflection_desc* r);
 int mpm_set_penalty_objects(mpm_handle* h, const mpm_collision_object* objs, int count, double stiffness,
                             double separation);
 
+/* A moving collision object: MPM_COLLISION_OBJECT's func_frame and func_twist
+ * (Hybrid_Methods/Collisions/MPM_COLLISION_OBJECT.cpp:23-71).  The object's
+ * geometry (mpm_collision_object's a, b) is then given in its own frame: at a
+ * time its points Z sit at R Z + translation, R the rotation of the unit
+ * quaternion `rotation` (w, x, y, z) (ROTATION<VECTOR<T,3> >; in 2D
+ * (cos theta, sin theta, 0, 0), ROTATION<VECTOR<T,2> >), and a point X of the
+ * object moves with linear + angular x (X - translation) (TWIST; in 2D
+ * angular[0] is the spin).  The callback fills the state at `time` and returns
+ * 0 (non-zero: the substep fails with MPM_ERR_ARG).  Each substep from t to
+ * t + dt calls it at t and t + dt: MPM_OBJECTIVE::Test_Add_Collision
+ * (MPM_OBJECTIVE.cpp:150-181) tests a node's start against the frame at t,
+ * projects its end at t + dt, and holds a sticky node at the object's velocity
+ * there.  fn = NULL makes the object static again.  Substeps with moving
+ * objects run without the captured CUDA graph.  Both paths and the implicit
+ * solve; a batch takes none. */
+typedef struct {
+    double translation[3];
+    double rotation[4];
+    double linear[3];
+    double angular[3];
+} mpm_object_state;
+typedef int (*mpm_motion_fn)(void* user, int object, double time, mpm_object_state* state);
+int mpm_set_object_motion(mpm_handle* h, int object, mpm_motion_fn fn, void* user);
+
 /* ---- inspection ---------------------------------------------------------- */
 
 /* Grids of the last substep as doubles on the host, each (G+6)^d nodes (times

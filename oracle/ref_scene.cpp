@@ -15,11 +15,14 @@
 // MPM_DRUCKER_PRAGER after G2P (l.409-486),
 // MPM_GRAVITY (l.354-358), collision objects through Add_Collision_Object,
 // penalty collision objects (IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES, l.555-563),
+// moving collision objects (func_frame, func_twist of a constant twist),
 // symplectic Euler or (scene flag) the backward-Euler Newton solve, APIC
 // (use_affine), flip=0, fixed dt.
 #include <Core/Log/LOG.h>
 #include <Core/Math_Tools/RANGE.h>
+#include <Core/Matrices/FRAME.h>
 #include <Core/Matrices/MATRIX.h>
+#include <Core/Vectors/TWIST.h>
 #include <Core/Vectors/VECTOR.h>
 #include <Geometry/Basic_Geometry/PLANE.h>
 #include <Geometry/Basic_Geometry/SPHERE.h>
@@ -49,7 +52,7 @@
 using namespace PhysBAM;
 
 namespace {
-struct OBJ { int kind, type; double friction, a[3], b[3]; };
+struct OBJ { int kind, type; double friction, a[3], b[3]; int moving = 0; double c[3], v[3], w[3]; };
 struct SCENE_FILE
 {
     int dim, counts[3], model, nsteps, nobj, ndump, plasticity, implicit, dt_control, reflection, npen;
@@ -79,11 +82,12 @@ SCENE_FILE Read_Scene(const char* path)
     if(!f) throw std::runtime_error("cannot open scene");
     char magic[8];
     rd(f, magic, 8);
-    if(memcmp(magic, "MPMSCN05", 8)) throw std::runtime_error("bad scene magic");
+    if(memcmp(magic, "MPMSCN06", 8)) throw std::runtime_error("bad scene magic");
     SCENE_FILE s;
-    int hdr[13];
-    rd(f, hdr, 13);
+    int hdr[14];
+    rd(f, hdr, 14);
     s.npen = hdr[12];
+    const int nmoving = hdr[13];
     s.reflection = hdr[11];
     s.implicit = hdr[9];
     s.dt_control = hdr[10];
@@ -113,6 +117,14 @@ SCENE_FILE Read_Scene(const char* path)
             rd(f, &o.kind, 1); rd(f, &o.type, 1); rd(f, &o.friction, 1); rd(f, o.a, 3); rd(f, o.b, 3);
             s.pen.push_back(o);
         }
+    }
+    for(int i = 0; i < nmoving; i++) {   // object index, then its constant twist: center, linear, angular
+        int j;
+        rd(f, &j, 1);
+        if(j < 0 || j >= s.nobj) throw std::runtime_error("moving object index");
+        OBJ& o = s.objs[j];
+        o.moving = 1;
+        rd(f, o.c, 3); rd(f, o.v, 3); rd(f, o.w, 3);
     }
     rd(f, &s.n, 1);
     size_t n = s.n, d = s.dim;
@@ -221,9 +233,19 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
             COLLISION_TYPE type = o.type == 0 ? COLLISION_TYPE::stick : o.type == 1 ? COLLISION_TYPE::slip : COLLISION_TYPE::separate;
             TV a, b;
             for(int k = 0; k < d; k++) { a(k) = (T)o.a[k]; b(k) = (T)o.b[k]; }
-            if(o.kind == 0) this->Add_Collision_Object(RANGE<TV>(a, b), type, (T)o.friction);
-            else if(o.kind == 2) this->Add_Collision_Object(SPHERE<TV>(a, (T)o.b[0]), type, (T)o.friction);
-            else Add_Plane(a, b, type, (T)o.friction);
+            std::function<FRAME<TV>(T)> frame;
+            std::function<TWIST<TV>(T)> twist;
+            if(o.moving) {   // func_frame / func_twist of a constant twist, as the rotating scenes write them
+                TV c, v;
+                typename TV::SPIN w;
+                for(int k = 0; k < d; k++) { c(k) = (T)o.c[k]; v(k) = (T)o.v[k]; }
+                for(int k = 0; k < w.m; k++) w(k) = (T)o.w[k];
+                frame = [=](T time){return FRAME<TV>(c + v * time, ROTATION<TV>::From_Rotation_Vector(w * time));};
+                twist = [=](T){return TWIST<TV>(v, w);};
+            }
+            if(o.kind == 0) this->Add_Collision_Object(RANGE<TV>(a, b), type, (T)o.friction, frame, twist);
+            else if(o.kind == 2) this->Add_Collision_Object(SPHERE<TV>(a, (T)o.b[0]), type, (T)o.friction, frame, twist);
+            else Add_Plane(a, b, type, (T)o.friction, frame, twist);
         }
         // penalty collision objects as STANDARD_TESTS_BASE::Add_Penalty_Collision_Object
         // adds them (Projects/mpm/STANDARD_TESTS_BASE.cpp:557-563): one force per object
@@ -245,9 +267,11 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
     IMPLICIT_OBJECT<TV>* Plane_Object(const VECTOR<T, 2>&, const VECTOR<T, 2>&)
     {throw std::runtime_error("plane objects are only wired for 3D in the runner");}
 
-    void Add_Plane(const VECTOR<T, 3>& n, const VECTOR<T, 3>& x0, COLLISION_TYPE type, T friction)
-    {this->Add_Collision_Object(PLANE<T>(n, x0), type, friction);}
-    void Add_Plane(const VECTOR<T, 2>&, const VECTOR<T, 2>&, COLLISION_TYPE, T)
+    void Add_Plane(const VECTOR<T, 3>& n, const VECTOR<T, 3>& x0, COLLISION_TYPE type, T friction,
+        std::function<FRAME<TV>(T)> frame, std::function<TWIST<TV>(T)> twist)
+    {this->Add_Collision_Object(PLANE<T>(n, x0), type, friction, frame, twist);}
+    void Add_Plane(const VECTOR<T, 2>&, const VECTOR<T, 2>&, COLLISION_TYPE, T, std::function<FRAME<TV>(T)>,
+        std::function<TWIST<TV>(T)>)
     {throw std::runtime_error("plane objects are only wired for 3D in the runner");}
 };
 

@@ -96,6 +96,57 @@ static int release_graph(mpm_handle* h)
     return MPM_OK;
 }
 
+// ROTATION<TV>::Rotation_Matrix of a unit quaternion (w, x, y, z), or in 2D of
+// the unit complex number (cos, sin), column-major d x d.
+static void rotation_matrix(int d, const double* q, double* R)
+{
+    if(d == 2) {
+        double m = std::sqrt(q[0] * q[0] + q[1] * q[1]);
+        double c = m > 0 ? q[0] / m : 1, s = m > 0 ? q[1] / m : 0;
+        R[0] = c; R[1] = s; R[2] = -s; R[3] = c;
+        return;
+    }
+    double m = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    double w = 1, x = 0, y = 0, z = 0;
+    if(m > 0) { w = q[0] / m; x = q[1] / m; y = q[2] / m; z = q[3] / m; }
+    R[0] = 1 - 2 * (y * y + z * z); R[3] = 2 * (x * y - w * z);     R[6] = 2 * (x * z + w * y);
+    R[1] = 2 * (x * y + w * z);     R[4] = 1 - 2 * (x * x + z * z); R[7] = 2 * (y * z - w * x);
+    R[2] = 2 * (x * z - w * y);     R[5] = 2 * (y * z + w * x);     R[8] = 1 - 2 * (x * x + y * y);
+}
+
+// The moving objects' frames at time and time + dt and twists at time + dt,
+// from their callbacks, copied to the device in stream order (from host memory
+// the copy has staged before it returns, so the next substep may refill it).
+int update_motion(mpm_handle* h, double time, double dt)
+{
+    if(!h->moving) return MPM_OK;
+    const int d = h->sp.dim;
+    mpm::ObjMotion m[MPM_MAX_OBJECTS] = {};
+    mpm::ObjMotionF mf[MPM_MAX_OBJECTS] = {};
+    for(int j = 0; j < h->sp.nobj && j < MPM_MAX_OBJECTS; j++) {
+        if(!((h->moving >> j) & 1u)) continue;
+        mpm_object_state s0{}, s1{};
+        if(h->motion_fn[j](h->motion_user[j], j, time, &s0) || h->motion_fn[j](h->motion_user[j], j, time + dt, &s1))
+            return set_error(h, MPM_ERR_ARG, "an object motion callback failed");
+        rotation_matrix(d, s0.rotation, m[j].R0);
+        rotation_matrix(d, s1.rotation, m[j].R1);
+        for(int k = 0; k < 3; k++) {
+            m[j].x0[k] = s0.translation[k]; m[j].x1[k] = s1.translation[k];
+            m[j].v[k] = s1.linear[k]; m[j].w[k] = s1.angular[k];
+        }
+        for(int k = 0; k < 9; k++) { mf[j].R0[k] = (float)m[j].R0[k]; mf[j].R1[k] = (float)m[j].R1[k]; }
+        for(int k = 0; k < 3; k++) {
+            mf[j].x0[k] = (float)m[j].x0[k]; mf[j].x1[k] = (float)m[j].x1[k];
+            mf[j].v[k] = (float)m[j].v[k]; mf[j].w[k] = (float)m[j].w[k];
+        }
+    }
+    if(!h->motion_dev) MPM_CUDA(h, cudaMalloc(&h->motion_dev, sizeof(m)));
+    if(!h->motion_dev_f) MPM_CUDA(h, cudaMalloc(&h->motion_dev_f, sizeof(mf)));
+    MPM_CUDA(h, cudaMemcpyAsync(h->motion_dev, m, sizeof(m), cudaMemcpyHostToDevice, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(h->motion_dev_f, mf, sizeof(mf), cudaMemcpyHostToDevice, h->stream));
+    return MPM_OK;
+}
+
 // One substep: the three phases back to back.
 static bool reduces_dt(const mpm_handle* h) { return h->dt_control.strong_cfl || h->dt_control.sound_cfl; }
 
@@ -116,7 +167,7 @@ static int enqueue_substep(mpm_handle* h, double dt, double time)
 // path alternates its particle buffers, so it keeps one graph per parity.
 static int run_substep(mpm_handle* h, double dt, double time)
 {
-    if(h->timing || h->implicit.enabled || (!fast(h) && reduces_dt(h))) return enqueue_substep(h, dt, time);
+    if(h->timing || h->implicit.enabled || h->moving || (!fast(h) && reduces_dt(h))) return enqueue_substep(h, dt, time);
     const int par = fast(h) ? h->fast.cur : 0;
     cudaGraphExec_t& ge = h->graphs[par];
     if(!ge) {
@@ -220,6 +271,8 @@ int mpm_destroy(mpm_handle* h)
     plain_free(h);
     fast_free(h);
     cudaFree(h->pen_f);
+    cudaFree(h->motion_dev);
+    cudaFree(h->motion_dev_f);
     cudaFree(h->d_flags);
     if(h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -253,6 +306,8 @@ int mpm_set_collision_objects(mpm_handle* h, const mpm_collision_object* objs, i
     }
     if(fast(h) && h->fast.batch) return set_error(h, MPM_ERR_ARG, "a batch takes its objects at mpm_batch_create");
     release_graph(h);
+    h->moving = 0;   // a new object list starts static
+    for(int j = 0; j < MPM_MAX_OBJECTS; j++) { h->motion_fn[j] = nullptr; h->motion_user[j] = nullptr; }
     h->sp.nobj = count;
     for(int i = 0; i < count; i++) {
         mpm::DevObject& d = h->sp.objs[i];
@@ -318,6 +373,7 @@ int mpm_particle_to_grid(mpm_handle* h, double dt, double time)
 int mpm_apply_forces(mpm_handle* h, double dt, double time)
 {
     int rc = check_dt(h, dt);
+    if(!rc) rc = update_motion(h, time, dt);
     if(rc) return rc;
     if(fast(h)) return fast_forces(h, dt, time);
     return h->implicit.enabled ? plain_implicit_forces(h, dt, time) : plain_forces(h, dt, time);
@@ -540,6 +596,19 @@ int mpm_set_penalty_objects(mpm_handle* h, const mpm_collision_object* objs, int
         MPM_CUDA(h, cudaMemcpy(h->pen_f, tab, sizeof(tab), cudaMemcpyHostToDevice));
         return fast_penalty_buffers(h);
     }
+    return MPM_OK;
+}
+
+int mpm_set_object_motion(mpm_handle* h, int object, mpm_motion_fn fn, void* user)
+{
+    if(!h) return MPM_ERR_ARG;
+    if(object < 0 || object >= h->sp.nobj) return set_error(h, MPM_ERR_ARG, "no collision object with that index");
+    if(fast(h) && h->fast.batch) return set_error(h, MPM_ERR_ARG, "a batch takes no moving objects");
+    release_graph(h);
+    h->motion_fn[object] = fn;
+    h->motion_user[object] = fn ? user : nullptr;
+    if(fn) h->moving |= 1u << object;
+    else h->moving &= ~(1u << object);
     return MPM_OK;
 }
 

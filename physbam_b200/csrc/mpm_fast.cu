@@ -90,6 +90,8 @@ struct FastArgs {
     float pen_k, pen_sep;     // their stiffness and separation
     const float* vsrc;        // the velocities P2G reads (3 x npad): src's, or V + dt f / m with penalty objects
     float* vkick;             // where k_penalty_kick writes V + dt f / m
+    const ObjMotionF* motion; // moving collision objects (bit j of `moving`, single-scene handles)
+    unsigned moving;
 };
 
 __device__ __forceinline__ int64_t node_index(const SceneDev& sc, int qx, int qy, int qz)
@@ -954,7 +956,7 @@ __global__ void __launch_bounds__(256) k_grid(FastArgs a)
                                    sc.dmin[1] + ((float)(qy - MPM_GHOST) + 0.5f) * sc.dx[1],
                                    sc.dmin[2] + ((float)(qz - MPM_GHOST) + 0.5f) * sc.dx[2]};
                     float zero[3] = {0.f, 0.f, 0.f};
-                    collide_node<float, 3>(s_obj[grp], sc.nobj, X0, zero, V, a.dt, vn, vf);
+                    collide_node<float, 3>(s_obj[grp], sc.nobj, X0, zero, V, a.dt, vn, vf, a.motion, a.moving);
                 } else {
 #pragma unroll
                     for(int k = 0; k < 3; k++) vn[k] = vf[k] = V[k];
@@ -1503,6 +1505,8 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.pen_k = (float)h->sp.pen_stiffness;
     a.pen_sep = (float)h->sp.pen_separation;
     a.vkick = f.vkick;
+    a.motion = h->motion_dev_f;
+    a.moving = h->motion_dev_f ? h->moving : 0u;
     a.vsrc = a.npen ? f.vkick : a.src + (size_t)C_V * a.npad;
     a.dt = (float)dt;
     a.flags = h->d_flags;

@@ -43,6 +43,7 @@ template<class T> struct ImpArgs {
     uint8_t *cmask, *stuck;     // per node: collision objects (bit j), stuck flag
     T* cdat;                    // per node and object: phi, n_dE, normal, position, H g (2 + 3d)
     T* pen;                     // per particle: penalty force (d) and Hessian (d x d) at the current X
+    T* svel;                    // per node: the velocity of the sticky object holding it (stuck_velocity)
     int nobj;
     const uint32_t* order;      // particles sorted by cell (the passes visit them in this order)
 };
@@ -358,8 +359,9 @@ template<class T, int d> __global__ void k_imp_grad(ImpArgs<T> ia, T* g, const T
 
 // MPM_OBJECTIVE::Adjust_For_Collision (l.180-222) with Test_Add_Collision
 // (l.143-176), prune and stick on, objects in order: each test moves dv of
-// the node onto the object (or to rest for a sticky one) and records the
-// collision; an earlier object's projection feeds the next one's test.
+// the node onto the object (or to the object's velocity for a sticky one) and
+// records the collision; an earlier object's projection feeds the next one's
+// test.  A moving object is tested at its frames of the substep's start and end.
 template<class T, int d> __global__ void k_imp_adjust(ImpArgs<T> ia, T* dv)
 {
     NODE_LOOP(ia) {
@@ -372,14 +374,14 @@ template<class T, int d> __global__ void k_imp_adjust(ImpArgs<T> ia, T* dv)
             T V[3], X[3];
 #pragma unroll
             for(int k = 0; k < d; k++) { V[k] = a.gv0[i * d + k] + dv[i * d + k]; X[k] = X0[k] + a.dt * V[k]; }
-            const T phi0 = object_phi<T, d>(o, X0);
-            const T phi = object_phi<T, d>(o, X) - fmin(phi0, (T)0);
+            const T phi0 = phi_at<T, d>(o, a.motion, a.moving, j, false, X0);
+            const T phi = phi_at<T, d>(o, a.motion, a.moving, j, true, X) - fmin(phi0, (T)0);
             if(o.type == MPM_STICK && phi0 > 0) continue;
             if(o.type == MPM_SLIP && phi0 > 0) continue;
             if(o.type == MPM_SEPARATE && phi > (T)kCollisionThickness) continue;
             if(o.type != MPM_STICK && phi > (T)FLT_MAX) continue;
             T n[3];
-            object_normal<T, d>(o, X, n);
+            normal_at<T, d>(o, a.motion, a.moving, j, X, n);
             T* cd = ia.cdat + (i * ia.nobj + j) * (2 + 3 * d);
             cd[0] = phi;
             cd[1] = 0;
@@ -387,7 +389,8 @@ template<class T, int d> __global__ void k_imp_adjust(ImpArgs<T> ia, T* dv)
             mask |= (uint8_t)(1u << j);
             for(int k = 0; k < d; k++) { X[k] -= phi * n[k]; V[k] = (X[k] - X0[k]) / a.dt; }
             if(o.type == MPM_STICK) {
-                for(int k = 0; k < d; k++) V[k] = 0;   // static objects
+                velocity_at<T, d>(a.motion, a.moving, j, X, V);
+                for(int k = 0; k < d; k++) ia.svel[i * d + k] = V[k];
                 stuck = 1;
             }
             for(int k = 0; k < d; k++) dv[i * d + k] = V[k] - a.gv0[i * d + k];
@@ -421,7 +424,7 @@ template<class T, int d> __global__ void k_imp_project(ImpArgs<T> ia, T* g, int 
             }
             // H_dE = H g; g -= n_dE n + phi H_dE
             T H[9], gv[3];
-            object_hessian<T, d>(ia.a.sp.objs[j], cd + 2 + d, H);
+            hessian_at<T, d>(ia.a.sp.objs[j], ia.a.motion, ia.a.moving, j, cd + 2 + d, H);
             for(int k = 0; k < d; k++) gv[k] = g[i * d + k];
             for(int r = 0; r < d; r++) {
                 T hd = 0;
@@ -471,7 +474,7 @@ template<class T, int d> __global__ void k_imp_mult_post(ImpArgs<T> ia, T* f, co
             const T* n = cd + 2;
             const T* hde = cd + 2 + 2 * d;
             T H[9];
-            object_hessian<T, d>(ia.a.sp.objs[j], cd + 2 + d, H);
+            hessian_at<T, d>(ia.a.sp.objs[j], ia.a.motion, ia.a.moving, j, cd + 2 + d, H);
             T dn = 0, nv = 0, hv = 0, Hv[3];
             for(int k = 0; k < d; k++) { dn += x[k] * n[k]; nv += n[k] * v[i * d + k]; hv += hde[k] * v[i * d + k]; }
             for(int r = 0; r < d; r++) {
@@ -529,7 +532,7 @@ template<class T, int d> __global__ void k_imp_finish(ImpArgs<T> ia, const T* dv
         const PlainArgs<T>& a = ia.a;
         for(int k = 0; k < d; k++) {
             a.gv[i * d + k] = dv[i * d + k] + a.gv0[i * d + k];
-            a.gvf[i * d + k] = ia.stuck[i] ? (T)0 : vfs[i * d + k] + a.gv0[i * d + k];
+            a.gvf[i * d + k] = ia.stuck[i] ? ia.svel[i * d + k] : vfs[i * d + k] + a.gv0[i * d + k];
         }
     }
 }
@@ -607,7 +610,7 @@ __global__ void k_imp_final(const double* partial, int count, int slots, double*
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-enum { V_DV, V_GRAD, V_DX, V_TM, V_Q, V_S, V_R, V_TMP0, V_TMP1, V_TMP2, V_V1, V_STMP, V_VFS, V_COUNT };
+enum { V_DV, V_GRAD, V_DX, V_TM, V_Q, V_S, V_R, V_TMP0, V_TMP1, V_TMP2, V_V1, V_STMP, V_VFS, V_SVEL, V_COUNT };
 
 }  // namespace
 
@@ -651,6 +654,7 @@ template<class T, int d> struct Solver {
         ia.pe = s.pe; ia.cmask = s.cmask; ia.stuck = s.stuck; ia.cdat = (T*)s.cdat; ia.nobj = h->sp.nobj;
         ia.order = nullptr;
         for(int k = 0; k < V_COUNT; k++) v[k] = (T*)s.vec + (size_t)k * s.gn * d;
+        ia.svel = v[V_SVEL];
         pb = pblocks(s.n, 128);
         gb = gblocks(h, s.gn, 256);
     }

@@ -144,6 +144,12 @@ struct mpm_handle {
     mpm_dt_control dt_control{};     // Compute_Dt / Reduce_Dt controls
     mpm_reflection_desc reflect{};   // reflection boundary conditions (enabled 0: none)
     double last_dt = 0;              // step the last substep took (Reduce_Dt may shorten it)
+    // moving collision objects: host callbacks, and their frames for the current substep
+    mpm_motion_fn motion_fn[MPM_MAX_OBJECTS] = {};
+    void* motion_user[MPM_MAX_OBJECTS] = {};
+    unsigned moving = 0;                      // bit j: object j moves
+    mpm::ObjMotion* motion_dev = nullptr;     // MPM_MAX_OBJECTS, plain path and implicit solve
+    mpm::ObjMotionF* motion_dev_f = nullptr;  // the same in float, fast path
     mpm_implicit_stats imp_stats{};  // of the last implicit solve
     ImplicitState* imp = nullptr;
     // timing
@@ -158,6 +164,9 @@ struct mpm_handle {
     void* diff = nullptr;
     std::string last_error;
 };
+
+// frames and twists of the moving objects for the substep [time, time + dt] (mpm_capi.cu)
+int update_motion(mpm_handle* h, double time, double dt);
 
 // timing helpers (mpm_capi.cu)
 int timer_begin(mpm_handle* h, const char* name);

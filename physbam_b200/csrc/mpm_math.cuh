@@ -1,7 +1,7 @@
 // Device math for the explicit MPM substep: quadratic B-spline weights, the
-// 3x3 / 2x2 signed SVD, the two constitutive models, and the static collision
-// objects.  Templated on the scalar type so the FP64 path and the FP64
-// fallbacks inside the FP32 path share one implementation.
+// 3x3 / 2x2 signed SVD, the constitutive models, and the collision objects.
+// Templated on the scalar type so the FP64 path and the FP64 fallbacks inside
+// the FP32 path share one implementation.
 //
 // Matrices are column-major, a[i + d*j], the layout of PhysBAM's MATRIX<T,d>
 // (Core/Matrices/MATRIX_3X3.h:115-119).
@@ -680,6 +680,113 @@ template<class T, int d, class O> __device__ void object_hessian(const O& o, con
         for(int b = 0; b < d; b++) H[a + d * b] = ((a == b ? D[a] : (T)0) - z[a] * z[b]) / w;
 }
 
+// A moving collision object over one substep: MPM_COLLISION_OBJECT's
+// func_frame at the substep's start (R0, x0) and end (R1, x1) and func_twist
+// at its end (v, w) (Hybrid_Methods/Collisions/MPM_COLLISION_OBJECT.cpp:23-71).
+// The object's geometry is given in its own frame: a point Z of it sits at
+// R Z + x.  R is column-major d x d; in 2D w[0] is the spin.
+template<class S> struct ObjMotionT {
+    S R0[9], x0[3], R1[9], x1[3], v[3], w[3];
+};
+typedef ObjMotionT<double> ObjMotion;
+typedef ObjMotionT<float> ObjMotionF;
+
+// FRAME::Inverse_Times: Z = R^T (X - x), the frame at the substep's end when `end`.
+template<class T, int d, class S> __device__ __forceinline__ void to_local(const ObjMotionT<S>& m, bool end, const T* X, T* Z)
+{
+    const S* R = end ? m.R1 : m.R0;
+    const S* x = end ? m.x1 : m.x0;
+    T y[3];
+#pragma unroll
+    for(int a = 0; a < d; a++) y[a] = X[a] - (T)x[a];
+#pragma unroll
+    for(int c = 0; c < d; c++) {
+        T z = 0;
+#pragma unroll
+        for(int a = 0; a < d; a++) z += (T)R[a + d * c] * y[a];
+        Z[c] = z;
+    }
+}
+
+// MPM_COLLISION_OBJECT::Phi / Normal / Hessian (l.23-59) of object j at the
+// substep's start or end; `mo` null or bit j of `moving` clear: a static object.
+template<class T, int d, class O, class S> __device__ T phi_at(const O& o, const ObjMotionT<S>* mo, unsigned moving, int j,
+    bool end, const T* X)
+{
+    if(!mo || !((moving >> j) & 1u)) return object_phi<T, d>(o, X);
+    T Z[3];
+    to_local<T, d>(mo[j], end, X, Z);
+    return object_phi<T, d>(o, Z);
+}
+
+template<class T, int d, class O, class S> __device__ void normal_at(const O& o, const ObjMotionT<S>* mo, unsigned moving, int j,
+    const T* X, T* n)
+{
+    if(!mo || !((moving >> j) & 1u)) { object_normal<T, d>(o, X, n); return; }
+    T Z[3], nl[3];
+    to_local<T, d>(mo[j], true, X, Z);
+    object_normal<T, d>(o, Z, nl);
+    const S* R = mo[j].R1;
+#pragma unroll
+    for(int r = 0; r < d; r++) {
+        T s = 0;
+#pragma unroll
+        for(int c = 0; c < d; c++) s += (T)R[r + d * c] * nl[c];
+        n[r] = s;
+    }
+}
+
+// SYMMETRIC_MATRIX::Conjugate(R, H) = R H R^T for a moving object.
+template<class T, int d, class O, class S> __device__ void hessian_at(const O& o, const ObjMotionT<S>* mo, unsigned moving, int j,
+    const T* X, T* H)
+{
+    if(!mo || !((moving >> j) & 1u)) { object_hessian<T, d>(o, X, H); return; }
+    T Z[3], Hl[9], RH[9];
+    to_local<T, d>(mo[j], true, X, Z);
+    object_hessian<T, d>(o, Z, Hl);
+    const S* R = mo[j].R1;
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T s = 0;
+#pragma unroll
+            for(int k = 0; k < d; k++) s += (T)R[r + d * k] * Hl[k + d * c];
+            RH[r + d * c] = s;
+        }
+#pragma unroll
+    for(int c = 0; c < d; c++)
+#pragma unroll
+        for(int r = 0; r < d; r++) {
+            T s = 0;
+#pragma unroll
+            for(int k = 0; k < d; k++) s += RH[r + d * k] * (T)R[c + d * k];
+            H[r + d * c] = s;
+        }
+}
+
+// MPM_COLLISION_OBJECT::Velocity (l.63-71): v + w x (X - x1); zero when static.
+template<class T, int d, class S> __device__ void velocity_at(const ObjMotionT<S>* mo, unsigned moving, int j, const T* X, T* V)
+{
+    if(!mo || !((moving >> j) & 1u)) {
+#pragma unroll
+        for(int a = 0; a < d; a++) V[a] = 0;
+        return;
+    }
+    const ObjMotionT<S>& m = mo[j];
+    T r[3];
+#pragma unroll
+    for(int a = 0; a < d; a++) r[a] = X[a] - (T)m.x1[a];
+    if(d == 3) {
+        V[0] = (T)m.v[0] + ((T)m.w[1] * r[2] - (T)m.w[2] * r[1]);
+        V[1] = (T)m.v[1] + ((T)m.w[2] * r[0] - (T)m.w[0] * r[2]);
+        V[2] = (T)m.v[2] + ((T)m.w[0] * r[1] - (T)m.w[1] * r[0]);
+    } else {   // VECTOR<T,1>::Cross(VECTOR<T,2>): the spin times the perpendicular (-y, x)
+        V[0] = (T)m.v[0] + -(T)m.w[0] * r[1];
+        V[1] = (T)m.v[1] + (T)m.w[0] * r[0];
+    }
+}
+
 // Penalty collision objects at one particle position, one
 // IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES per object, in object order
 // (Update_Position_Based_State_Particle,
@@ -718,14 +825,17 @@ template<class T, int d, class O> __device__ T penalty_particle(const O* objs, i
 // MPM_OBJECTIVE::Test_Add_Collision / Adjust_For_Collision
 // (Hybrid_Methods/System/MPM_OBJECTIVE.cpp:150-225), MPM_DRIVER::Apply_Friction
 // (Hybrid_Methods/Examples_And_Drivers/MPM_DRIVER.cpp:1064-1094) and the final
-// assembly of Apply_Forces (l.1050-1056), for static objects (velocity 0).
+// assembly of Apply_Forces (l.1050-1056).  Objects are static, or move as
+// `mo` gives them (bit j of `moving`): the start test at the substep's start
+// frame, the projection at its end frame, a sticky node at the object's
+// velocity there.
 //
 // In: v0 (grid velocity after P2G), dv (dt/m f), node centre X0.
 // Out: vnew (velocity), vfric (velocity_friction_save).
-template<class T, int d, class O> __device__ void collide_node(const O* objs, int nobj, const T* X0,
-    const T* v0, T* dv, T dt, T* vnew, T* vfric)
+template<class T, int d, class O, class S = double> __device__ void collide_node(const O* objs, int nobj, const T* X0,
+    const T* v0, T* dv, T dt, T* vnew, T* vfric, const ObjMotionT<S>* mo = nullptr, unsigned moving = 0)
 {
-    T dvb[3], nrm[MPM_MAX_OBJECTS][3];
+    T dvb[3], nrm[MPM_MAX_OBJECTS][3], sv[3] = {0, 0, 0};
     int cobj[MPM_MAX_OBJECTS];
     int ncol = 0;
     bool stuck = false;
@@ -733,17 +843,17 @@ template<class T, int d, class O> __device__ void collide_node(const O* objs, in
     for(int a = 0; a < d; a++) dvb[a] = dv[a];
     for(int j = 0; j < nobj; j++) {
         const O& o = objs[j];
-        const T phi0 = object_phi<T, d>(o, X0);
+        const T phi0 = phi_at<T, d>(o, mo, moving, j, false, X0);
         // stick and slip test only nodes that start inside the object
         if((o.type == MPM_STICK || o.type == MPM_SLIP) && phi0 > 0) continue;
         T Vn[3], Xn[3];
 #pragma unroll
         for(int a = 0; a < d; a++) { Vn[a] = v0[a] + dv[a]; Xn[a] = X0[a] + dt * Vn[a]; }
-        T phi = object_phi<T, d>(o, Xn) - fmin(phi0, (T)0);
+        T phi = phi_at<T, d>(o, mo, moving, j, true, Xn) - fmin(phi0, (T)0);
         if(o.type == MPM_SEPARATE && phi > (T)1e-15) continue;
         if(o.type != MPM_STICK && phi > (T)FLT_MAX) continue;
         T n[3];
-        object_normal<T, d>(o, Xn, n);
+        normal_at<T, d>(o, mo, moving, j, Xn, n);
 #pragma unroll
         for(int a = 0; a < d; a++) nrm[ncol][a] = n[a];
         cobj[ncol] = j;
@@ -752,9 +862,10 @@ template<class T, int d, class O> __device__ void collide_node(const O* objs, in
         for(int a = 0; a < d; a++) Xn[a] -= phi * n[a];
 #pragma unroll
         for(int a = 0; a < d; a++) Vn[a] = (Xn[a] - X0[a]) / dt;
-        if(o.type == MPM_STICK) {
+        if(o.type == MPM_STICK) {   // at the object's velocity (stuck_velocity)
+            velocity_at<T, d>(mo, moving, j, Xn, Vn);
 #pragma unroll
-            for(int a = 0; a < d; a++) Vn[a] = 0;
+            for(int a = 0; a < d; a++) sv[a] = Vn[a];
             stuck = true;
         }
 #pragma unroll
@@ -802,7 +913,7 @@ template<class T, int d, class O> __device__ void collide_node(const O* objs, in
 #pragma unroll
     for(int a = 0; a < d; a++) {
         vnew[a] = dv[a] + v0[a];
-        vfric[a] = stuck ? (T)0 : gvf[a] + v0[a];
+        vfric[a] = stuck ? sv[a] : gvf[a] + v0[a];
     }
 }
 

@@ -141,7 +141,7 @@ template<class T, int d> __global__ void k_grid_update(PlainArgs<T> a)
             v0[k] = a.gv0[i * d + k];
             X0[k] = (T)a.sp.dmin[k] + ((T)idx[k] + (T).5) * (T)a.sp.dx[k];
         }
-        collide_node<T, d>(a.sp.objs, a.sp.nobj, X0, v0, dv, a.dt, vn, vf);
+        collide_node<T, d>(a.sp.objs, a.sp.nobj, X0, v0, dv, a.dt, vn, vf, a.motion, a.moving);
 #pragma unroll
         for(int k = 0; k < d; k++) { a.gv[i * d + k] = vn[k]; a.gvf[i * d + k] = vf[k]; }
     }

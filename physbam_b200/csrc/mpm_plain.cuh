@@ -21,6 +21,8 @@ template<class T> struct PlainArgs {
     int mark_left;
     int reflect;          // reflection boundary conditions on
     int side[6];          // their types per side (mpm_bc_type)
+    const ObjMotion* motion;   // moving collision objects (bit j of `moving`): their substep frames
+    unsigned moving;
 };
 
 template<class T, int d> struct Stencil {
@@ -89,6 +91,8 @@ template<class T> inline PlainArgs<T> args(mpm_handle* h, double dt)
     a.mark_left = h->plastic.kind != MPM_PLASTICITY_NONE;
     a.reflect = h->reflect.enabled;
     for(int k = 0; k < 6; k++) a.side[k] = h->reflect.enabled ? h->reflect.side_type[k] : MPM_BC_FREE;
+    a.motion = h->motion_dev;
+    a.moving = h->motion_dev ? h->moving : 0u;
     return a;
 }
 

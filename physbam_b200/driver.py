@@ -109,6 +109,14 @@ _PLASTIC_FIELDS = {"Fp": "Fp", "mu": "mu", "lam": "lambda_", "mu0": "mu0", "lam0
                    "pdef": "plastic_def", "rho_F": "rho_F", "cohesion": "cohesion", "vc": "vc"}
 
 
+class ObjectState(ctypes.Structure):
+    _fields_ = [("translation", ctypes.c_double * 3), ("rotation", ctypes.c_double * 4),
+                ("linear", ctypes.c_double * 3), ("angular", ctypes.c_double * 3)]
+
+
+MOTION_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ObjectState))
+
+
 EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_objects", "mpm_set_particles",
            "mpm_get_particles", "mpm_substep", "mpm_advance", "mpm_particle_to_grid", "mpm_apply_forces",
            "mpm_grid_to_particle", "mpm_synchronize", "mpm_get_grid", "mpm_count_valid", "mpm_set_timing",
@@ -117,7 +125,7 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex",
            "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state", "mpm_set_implicit",
            "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt",
-           "mpm_set_reflection", "mpm_set_penalty_objects"]
+           "mpm_set_reflection", "mpm_set_penalty_objects", "mpm_set_object_motion"]
 
 _lib = None
 
@@ -170,6 +178,7 @@ def load_library(path: str = LIB_PATH):
     L.mpm_set_reflection.argtypes = [P, ctypes.POINTER(ReflectionDesc)]
     L.mpm_set_penalty_objects.argtypes = [P, ctypes.POINTER(CollisionObject), ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double]
+    L.mpm_set_object_motion.argtypes = [P, ctypes.c_int, MOTION_FN, P]
     L.mpm_status_string.argtypes = [ctypes.c_int]
     L.mpm_status_string.restype = ctypes.c_char_p
     for f in EXPORTS:
@@ -246,6 +255,38 @@ class MPM_DRIVER:
             for a in range(self.dim):
                 arr[i].a[a], arr[i].b[a] = o.a[a], o.b[a]
         self._check(self.L.mpm_set_collision_objects(self.h, arr, len(objects)), "mpm_set_collision_objects")
+        self._motion_fns = {}
+        for j, o in enumerate(objects):
+            if getattr(o, "motion", None) is not None:
+                self.set_object_motion(j, o.motion)
+
+    def set_object_motion(self, j: int, motion):
+        """Make collision object j move (mpm_set_object_motion).  `motion` is an
+        S.Motion or any callable time -> (translation, quaternion (w, x, y, z) -- in 2D
+        (cos, sin, 0, 0) --, linear, angular); None makes it static."""
+        if motion is None:
+            self._motion_fns.pop(j, None)
+            self._check(self.L.mpm_set_object_motion(self.h, j, MOTION_FN(), None), "mpm_set_object_motion")
+            return
+        at = (lambda t: motion.state(self.dim, t)) if isinstance(motion, S.Motion) else motion
+
+        def fn(user, obj, time, state):
+            try:
+                tr, q, lin, ang = at(time)
+                st = state.contents
+                for k in range(3):
+                    st.translation[k] = tr[k] if k < len(tr) else 0.0
+                    st.linear[k] = lin[k] if k < len(lin) else 0.0
+                    st.angular[k] = ang[k] if k < len(ang) else 0.0
+                for k in range(4):
+                    st.rotation[k] = q[k]
+                return 0
+            except Exception:
+                return 1
+
+        cb = MOTION_FN(fn)
+        self._motion_fns[j] = cb   # the library holds the pointer: keep the callback alive
+        self._check(self.L.mpm_set_object_motion(self.h, j, cb, None), "mpm_set_object_motion")
 
     def set_penalty(self, penalty: Optional[S.Penalty]):
         """Penalty collision objects (IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES, one per object);
@@ -686,6 +727,8 @@ class MPM_BATCH(MPM_DRIVER):
         self.scene = self.scenes[0]
         if any(s.penalty is not None for s in self.scenes):
             raise ValueError("a batch takes no penalty collision objects")
+        if any(o.motion is not None for s in self.scenes for o in s.objects):
+            raise ValueError("a batch takes no moving collision objects")
         self.dim = 3
         self.precision, self.path = FP32, PATH_FAST
         descs = (SceneDesc * len(self.scenes))()

@@ -46,18 +46,48 @@ GHOST = 3
 
 
 @dataclasses.dataclass
+class Motion:
+    """A collision object moving with a constant twist: `func_frame(t)` =
+    FRAME(center + linear t, ROTATION::From_Rotation_Vector(angular t)) and
+    `func_twist(t)` = TWIST(linear, angular), the form of the reference's rotating
+    and translating objects (e.g. `Projects/mpm/STANDARD_TESTS_3D.cpp:1560-1561`).
+    The object's geometry is then given about the origin of its own frame.  In 2D
+    ``angular`` has one entry (the spin)."""
+    center: Sequence[float]
+    linear: Sequence[float]
+    angular: Sequence[float]
+
+    def state(self, dim, t):
+        """(translation, unit quaternion w, x, y, z -- in 2D (cos, sin, 0, 0) --, linear, angular) at t."""
+        tr = [float(self.center[k]) + float(self.linear[k]) * t for k in range(dim)]
+        if dim == 2:
+            th = float(self.angular[0]) * t
+            q = [np.cos(th), np.sin(th), 0.0, 0.0]
+        else:
+            r = np.asarray(self.angular[:3], float) * t
+            th = float(np.sqrt(r @ r))
+            if th > 0:
+                q = [np.cos(th / 2)] + list(np.sin(th / 2) / th * r)
+            else:
+                q = [1.0, 0.0, 0.0, 0.0]
+        return tr, q, list(self.linear[:dim]), list(self.angular[:3 if dim == 3 else 1])
+
+
+@dataclasses.dataclass
 class CollisionObject:
-    """A static collision object (`Hybrid_Methods/Collisions/MPM_COLLISION_OBJECT.h:13-37`).
+    """A collision object (`Hybrid_Methods/Collisions/MPM_COLLISION_OBJECT.h:13-37`).
 
     ``kind`` BOX: ``a`` = min corner, ``b`` = max corner (`Core/Math_Tools/RANGE.cpp:37-63`).
     ``kind`` PLANE: ``a`` = unit normal, ``b`` = a point on the plane
     (`Geometry/Basic_Geometry/PLANE.h:52-63`); inside is behind the normal.
+    ``motion`` (optional): the object moves, its geometry given in its own frame.
     """
     kind: int
     type: int
     friction: float
     a: Sequence[float]
     b: Sequence[float]
+    motion: Optional[Motion] = None
 
 
 PLASTICITY_NONE, PLASTICITY_CLAMP, PLASTICITY_DRUCKER_PRAGER = 0, 1, 2
@@ -507,6 +537,36 @@ def small_2d_penalty(seed=83, G=16, nsteps=20, dt=1e-4):
     return s
 
 
+def small_3d_moving(seed=91, G=16, nsteps=20, dt=1e-4, implicit=False):
+    """small_3d with two moving collision objects: a sticky paddle (a box in its own frame)
+    that starts inside the block's +x face and turns about y while it pushes in, and a
+    separating ball that comes down on the block's top (the walls stay static)."""
+    s = small_3d(seed=seed, G=G, nsteps=nsteps, dt=dt, friction=0.2, v=(0.5, -0.5, 0.25))
+    s.name = "small3dmoving"
+    s.objects = s.objects + [
+        CollisionObject(BOX, STICK, 0.0, [-0.04, -0.1, -0.12], [0.04, 0.1, 0.12],
+                        motion=Motion([0.62, 0.31, 0.5], [-4.0, 0.5, 0.0], [0.0, 6.0, 1.0])),
+        CollisionObject(SPHERE, SEPARATE, 0.3, [0.0, 0.0, 0.0], [0.08, 0, 0],
+                        motion=Motion([0.35, 0.56, 0.45], [0.5, -5.0, 0.0], [0.0, 0.0, 0.0]))]
+    if implicit:
+        s.name = "small3dmovingimplicit"
+        s.dt = 1e-3
+        s.nsteps = 8
+        s.implicit = Implicit()
+    return s
+
+
+def small_2d_moving(seed=93, G=16, nsteps=20, dt=1e-4):
+    """small_2d with a spinning sticky paddle inside the block's +x side and a slip box
+    sliding along its top with friction."""
+    s = small_2d(seed=seed, G=G, nsteps=nsteps, dt=dt)
+    s.name = "small2dmoving"
+    s.objects = s.objects + [
+        CollisionObject(BOX, STICK, 0.0, [-0.03, -0.1], [0.03, 0.1], motion=Motion([0.68, 0.38], [-3.0, 0.0], [8.0])),
+        CollisionObject(BOX, SLIP, 0.5, [-0.1, -0.03], [0.1, 0.03], motion=Motion([0.45, 0.57], [4.0, -2.0], [0.0]))]
+    return s
+
+
 def small_3d_adaptive(seed=51, G=16, nframes=3):
     """A stiff small_3d (E 2e6..8e6) run frame by frame as Simulate_To_Frame does,
     with the strong and the sound-speed CFL on: the sound speed shortens most steps."""
@@ -608,7 +668,7 @@ def snowballs_3d(seed=1234, G=128, ppc=8, E=1.4e5, nu=0.2, density=400.0, dt=5e-
 # --------------------------------------------------------------------------------------------
 # Scene file: read by the reference runner (oracle/ref_scene.cpp) and by the C oracle harness.
 # --------------------------------------------------------------------------------------------
-MAGIC = b"MPMSCN05"
+MAGIC = b"MPMSCN06"
 
 
 def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
@@ -620,8 +680,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         counts = list(s.counts) + [1] * (3 - d)
         pl = s.plasticity
         im, dc, rf, pn = s.implicit, s.dt_control, s.reflection, s.penalty
-        f.write(struct.pack("<13i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
-                            1 if im else 0, 1 if dc else 0, 1 if rf else 0, len(pn.objects) if pn else 0))
+        moving = [(j, o.motion) for j, o in enumerate(s.objects) if o.motion is not None]
+        f.write(struct.pack("<14i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
+                            1 if im else 0, 1 if dc else 0, 1 if rf else 0, len(pn.objects) if pn else 0, len(moving)))
         f.write(struct.pack("<11d", *pad3(s.domain_min), *pad3(s.domain_max), *pad3(s.gravity), s.dt, 0.0))
         f.write(struct.pack("<%di" % len(dumps), *dumps))
         for o in s.objects:
@@ -642,6 +703,8 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
             f.write(struct.pack("<2d", pn.stiffness, pn.separation))
             for o in pn.objects:
                 f.write(struct.pack("<2i7d", o.kind, o.type, o.friction, *pad3(o.a), *pad3(o.b)))
+        for j, m in moving:   # object index, center, linear, angular (2D: the spin first)
+            f.write(struct.pack("<i9d", j, *pad3(m.center), *pad3(m.linear), *pad3(m.angular)))
         f.write(struct.pack("<q", s.n))
         f.write(np.ascontiguousarray(s.X, np.float64).tobytes())
         f.write(np.ascontiguousarray(s.V, np.float64).tobytes())

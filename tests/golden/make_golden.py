@@ -53,6 +53,10 @@ CASES = {
     "small3d_penalty": (lambda: S.small_3d_penalty(), [0, 1, 19], [0, 19]),
     "small2d_penalty": (lambda: S.small_2d_penalty(), [0, 19], [0, 19]),
     "small3d_penalty_implicit": (lambda: S.small_3d_penalty(implicit=True), [0, 7], [0, 7]),
+    # moving collision objects (func_frame / func_twist): explicit 3D/2D and implicit 3D
+    "small3d_moving": (lambda: S.small_3d_moving(), [0, 1, 19], [0, 19]),
+    "small2d_moving": (lambda: S.small_2d_moving(), [0, 19], [0, 19]),
+    "small3d_moving_implicit": (lambda: S.small_3d_moving(implicit=True), [0, 7], [0, 7]),
 }
 
 
@@ -79,6 +83,10 @@ def main(names=None):
             obj_b=np.array([o.b for o in scene.objects]).reshape(-1, scene.dim),
             X=scene.X, V=scene.V, F=scene.F, B=scene.B, mass=scene.mass, volume=scene.volume,
             mu=scene.mu, lam=scene.lam, dumps=np.array(dumps))
+        if any(o.motion is not None for o in scene.objects):   # center, linear, angular (3 each, zero padded)
+            pad = lambda v: list(v) + [0.0] * (3 - len(v))
+            arrays["obj_motion"] = np.array([pad(o.motion.center) + pad(o.motion.linear) + pad(o.motion.angular)
+                                             if o.motion is not None else [np.nan] * 9 for o in scene.objects])
         pl = scene.plasticity
         if pl is not None:
             arrays["plasticity"] = np.array(S.plastic_params(pl), np.float64)
@@ -123,6 +131,10 @@ def load(name):
                     list(z["gravity"]), float(z["dt"]), int(z["nsteps"]), objs,
                     z["X"].copy(), z["V"].copy(), z["F"].copy(), z["B"].copy(), z["mass"].copy(),
                     z["volume"].copy(), z["mu"].copy(), z["lam"].copy())
+    if "obj_motion" in z:
+        for o, m in zip(objs, z["obj_motion"]):
+            if not np.isnan(m[0]):
+                o.motion = S.Motion(list(m[0:dim]), list(m[3:3 + dim]), list(m[6:9] if dim == 3 else m[6:7]))
     if "plasticity" in z:
         scene.plasticity = S.plastic_from_params(z["plasticity"])
     if "reflection" in z:
