@@ -121,6 +121,24 @@ class DruckerPrager:
     cohesion: float = 0.0
     use_vc: bool = True
 
+    @classmethod
+    def friction_angle(cls, phi_F: float, cohesion: float = 0.0, use_vc: bool = True) -> "DruckerPrager":
+        """A constant friction angle phi_F (degrees), no hardening: the reference's
+        Add_Drucker_Prager(E, nu, phi_F) (`Projects/mpm/STANDARD_TESTS_BASE.cpp:437-441`)."""
+        return cls(a0=phi_F, a1=0.0, a3=0.0, a4=0.0, cohesion=cohesion, use_vc=use_vc)
+
+    @classmethod
+    def mast_case(cls, case: int, use_vc: bool = True) -> "DruckerPrager":
+        """The hardening constants (a0, a1, a3, a4) of Mast et al.'s cases 0-9, as
+        Add_Drucker_Prager_Case selects them (`Projects/mpm/STANDARD_TESTS_BASE.cpp:445-464`)."""
+        a0, a1, a3, a4 = (float(x) for x in MAST_CASES[case])
+        return cls(a0=a0, a1=a1, a3=a3, a4=a4, use_vc=use_vc)
+
+
+# (a0, a1, a3, a4) per case of the sand hardening study the reference's scenes draw on
+MAST_CASES = ((35, 0, 0.2, 10), (35, 4, 0.29, 10), (35, 9, 0.3, 10), (35, 13, 0.27, 10), (35, 0, 0.2, 6.57),
+              (35, 0, 0.2, 3.33), (35, 0, 0.2, 0), (38.33, 0, 0.2, 13.33), (41.67, 0, 0.2, 16.67), (45, 0, 0.2, 20))
+
 
 def plastic_keys(pl) -> tuple:
     """Per-particle plastic state a dump / fixture carries for plasticity `pl`."""
@@ -652,7 +670,7 @@ def sand_3d(seed=1234, G=128, ppc=8, E=3.537e5, nu=0.3, density=2200.0, dt=5e-5,
     Hencky with Drucker-Prager (Mast et al. case 2 hardening: 35, 9, 0.3, 10)."""
     s = spheres_3d(seed=seed, G=G, ppc=ppc, E=E, nu=nu, density=density, dt=dt, nsteps=nsteps, model=HENCKY)
     s.name = "sand3d"
-    s.plasticity = DruckerPrager(a0=35.0, a1=9.0, a3=0.3, a4=10.0)
+    s.plasticity = DruckerPrager.mast_case(2)
     return s
 
 

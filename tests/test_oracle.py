@@ -164,3 +164,13 @@ def test_sand_fixtures_exercise_every_branch():
             assert (ref["vc"] != 0).mean() > 0.05, name
         assert ((ref["pdef"] > 0) & (ref["vc"] == 0)).mean() > 0.05, name
         assert scene.model == S.HENCKY
+
+
+def test_drucker_prager_parameter_forms():
+    """Add_Drucker_Prager_Case and the friction-angle form of Add_Drucker_Prager
+    (STANDARD_TESTS_BASE.cpp:437-464) map onto the hardening constants."""
+    assert S.DruckerPrager.mast_case(2) == S.DruckerPrager(a0=35.0, a1=9.0, a3=0.3, a4=10.0)
+    assert S.sand_3d(G=16).plasticity == S.DruckerPrager.mast_case(2)
+    assert len(S.MAST_CASES) == 10 and all(len(c) == 4 for c in S.MAST_CASES)
+    f = S.DruckerPrager.friction_angle(30.0, cohesion=5.0)
+    assert (f.a0, f.a1, f.a3, f.a4, f.cohesion) == (30.0, 0.0, 0.0, 0.0, 5.0)
