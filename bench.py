@@ -310,7 +310,7 @@ def our_arm(args):
     roof = roofline_of(ktimes, n, peak, peak_kind, WORKLOAD)
     total_k = sum(v[0] for v in ktimes.values())
 
-    large = batch = adjoint = plain = snow = sand = implicit = None
+    large = batch = adjoint = plain = snow = sand = implicit = extras = None
     if world == 1 and not args.no_plain:
         plain = measure_plain_fp64(args, D, S, stream, flush, substep_ms)
     if world == 1 and not args.no_snow:
@@ -320,6 +320,8 @@ def our_arm(args):
                                "sand3d-128^3-hencky-8ppc-druckerprager-fp32")
     if world == 1 and not args.no_implicit:
         implicit = measure_implicit(args, D, S, stream, flush)
+    if world == 1 and not args.no_extras:
+        extras = measure_collision_extras(args, D, S, stream, flush, substep_ms)
     if world == 1 and not args.no_large:
         large = measure_large(args, D, S, stream, flush, peak, peak_kind)
     if not args.no_batch:
@@ -352,6 +354,7 @@ def our_arm(args):
             "implicit": implicit,
             "snow": snow,
             "sand": sand,
+            "collision_extras": extras,
             "large_config": large,
             "batch_config": batch,
             "adjoint": adjoint,
@@ -451,6 +454,40 @@ def measure_plastic(args, D, S, stream, flush, peak, elastic_ms, scene, workload
                 "alg_bytes_per_particle": ALG_BYTES["g2p"] + extra},
             "autotune": tuned,
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
+
+
+def measure_collision_extras(args, D, S, stream, flush, elastic_ms):
+    """The headline scene on the fast path with (a) penalty collision objects: a
+    penalty slab under the balls and a penalty ball between them, so the
+    impulse pre-pass runs for every particle each substep; (b) moving collision
+    objects: a sticky paddle turning between the balls and a slip plate sliding
+    over them, whose frames the host evaluates and uploads every substep (such
+    substeps run eagerly, without the captured graph).  Their cost against the
+    elastic headline."""
+    out = {}
+    steps = max(5, min(args.steps, 20))
+    pen = S.spheres_3d()
+    pen.penalty = S.Penalty([S.CollisionObject(S.BOX, S.SLIP, 0.0, [-1, -1, -1], [2, 0.39, 2]),
+                             S.CollisionObject(S.SPHERE, S.SLIP, 0.0, [0.5, 0.5, 0.5], [0.05, 0, 0])])
+    mov = S.spheres_3d()
+    mov.objects = mov.objects + [
+        S.CollisionObject(S.BOX, S.STICK, 0.0, [-0.01, -0.15, -0.15], [0.01, 0.15, 0.15],
+                          motion=S.Motion([0.5, 0.5, 0.5], [0.0, 0.0, 0.0], [0.0, 3.0, 0.0])),
+        S.CollisionObject(S.BOX, S.SLIP, 0.3, [-0.2, -0.01, -0.2], [0.2, 0.01, 0.2],
+                          motion=S.Motion([0.5, 0.63, 0.5], [0.5, -1.0, 0.0], [0.0, 0.0, 0.0]))]
+    for key, scene, workload in (("penalty", pen, "spheres3d-128^3-neohookean-8ppc-fp32 + 2 penalty objects"),
+                                 ("moving", mov, "spheres3d-128^3-neohookean-8ppc-fp32 + 2 moving objects")):
+        drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+        drv.set_stream(stream.cuda_stream)
+        drv.set_scene_particles(scene)
+        drv.autotune(substeps=3, cold_l2=True)
+        ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
+        drv.close()
+        sub = ms / steps
+        out[key] = {"workload": workload, "particles": scene.n, "steps": steps, "ms_per_step": sub,
+                    "value": scene.n * steps / (ms / 1e3), "unit": METRIC, "over_elastic_headline": sub / elastic_ms,
+                    "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
+    return out
 
 
 def measure_implicit(args, D, S, stream, flush):
@@ -619,6 +656,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 path on the same workload")
     ap.add_argument("--no-implicit", action="store_true", help="skip the backward-Euler measurement")
     ap.add_argument("--no-snow", action="store_true", help="skip the snow and sand (plasticity) measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the penalty and moving-object measurements")
     ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d", "snowballs3d", "sand3d", "spheres3d_implicit"],
                     help="profiling run of one scene only")
     ap.add_argument("--grid", type=int, default=0, help="grid cells per side for --scene")

@@ -2025,11 +2025,13 @@ int fast_p2g(mpm_handle* h, double dt, double)
     int rc = fast_sort_ranges(h, dt, CNT_COUNT);
     if(rc) return rc;
     FastArgs a = make_args(h, dt);
-    int slot = timer_begin(h, "fast_p2g");
     if(a.npen) {
+        const int ps = timer_begin(h, "fast_penalty");
         k_penalty_kick<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(a);
+        timer_end(h, ps);
         MPM_LAUNCHED(h, "k_penalty_kick");
     }
+    int slot = timer_begin(h, "fast_p2g");
     if(f.p2g_variant == 0) k_p2g_cells<<<occupancy_ctas(h, (const void*)k_p2g_cells, 64, f.cta_mult), 64, 0, h->stream>>>(a);
     else {
         if(f.p2g_variant == 1)
