@@ -1,6 +1,6 @@
 """Benchmark of the explicit MPM substep on B200 (particle-substeps/s).
 
-Workload: the BASELINE 3D case -- two NEO_HOOKEAN spheres (r = 0.12, +-2 m/s)
+Workload: two colliding NEO_HOOKEAN spheres (r = 0.12, +-2 m/s)
 on a 128^3 grid, 8 particles per cell (242,664 particles), slip walls,
 gravity, dt = 5e-5.  One step = one substep over the whole scene.
 
@@ -543,7 +543,7 @@ def measure_implicit(args, D, S, stream, flush):
 
 
 def measure_adjoint(D, S):
-    """64^3 cube, 64 substeps, checkpoint every 8; FP32 forward and
+    """The differentiable cube: 64^3, 64 substeps, checkpoint every 8; FP32 forward and
     backward through the C ABI (device arrays), timed with CUDA events."""
     import torch
     scene = S.cube_3d()

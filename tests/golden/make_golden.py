@@ -27,7 +27,7 @@ CASES = {
     "small2d_neohookean": (lambda: S.small_2d(model=S.NEO_HOOKEAN, seed=5), [0, 19], [0]),
     "small3d_corotated": (lambda: S.small_3d(), [0, 1, 19], [0, 19]),
     "small3d_neohookean_friction": (lambda: S.small_3d(model=S.NEO_HOOKEAN, seed=9, friction=0.4), [0, 19], [0]),
-    # BASELINE 2D case, exactly: 64^2, block 0.25^2 at (0.5,0.6), 4 ppc, corotated, sticky ground, 100 substeps
+    # the 2D block case: 64^2, block 0.25^2 at (0.5,0.6), 4 ppc, corotated, sticky ground, 100 substeps
     "block2d_cfg": (lambda: S.block_2d(), [0, 9, 99], [0, 99]),
     # snow: MPM_PLASTICITY_CLAMP after every G2P (Fp, hardened mu and lambda dumped too)
     "smallsnow3d_corotated": (lambda: S.small_snow_3d(), [0, 19], [0, 19]),

@@ -1,7 +1,7 @@
 """GPU tests of the hand-written adjoint (mpm_diff_forward / mpm_diff_backward).
 
 Loss: squared distance of the final centre of mass to a seeded target (the
-BASELINE loss; the v0 checks use it) and the same for the half of the body
+rollout loss; the v0 checks use it) and the same for the half of the body
 that starts at x > 0.5 (it moves with the deformation, so the E checks use
 it -- the whole-body centre of mass does not depend on E at all).  The
 parameters are the initial velocity v0 (shared by all particles) and the
@@ -131,7 +131,7 @@ def test_checkpoint_interval_does_not_change_gradients(cuda_device):
 
 
 def test_adjoint_differentiable_config_fd(cuda_device):
-    """The BASELINE differentiable case: 64^3, side-0.3 cube at 8 ppc, E log-uniform in
+    """The differentiable cube: 64^3, side-0.3 cube at 8 ppc, E log-uniform in
     [5e3, 5e4], v0 = (1, .5, 0), 64 substeps of 1e-4, checkpoint every 8."""
     scene = S.cube_3d()
     check_case(scene, 64, 8, check_E=False)

@@ -3,7 +3,7 @@
 * FP64 plain path vs the reference's own FP64 dumps (tests/golden), node for node.
 * FP32 fast path vs the same dumps, at FP32 tolerances stated per quantity.
 * Radix sort and the fast path's cell keys bit-exact against a CPU stable sort.
-* Full-size BASELINE 3D case (two spheres, 128^3, 200 substeps): FP32 fast path
+* Full-size two-sphere case (128^3, 200 substeps): FP32 fast path
   within 1e-4 relative position error of the FP64 plain path.
 * Edge cases: empty particle set, particles leaving the domain, NaN input,
   particles outside the grid.
@@ -190,7 +190,7 @@ def test_fast_cell_keys_and_sort_bit_exact(cuda_device):
 
 
 def test_fast_vs_plain_fp64_full_size_spheres(cuda_device):
-    """The BASELINE 3D case as stated (128^3, two spheres, NEO_HOOKEAN, 200 substeps):
+    """The full-size two-sphere case (128^3, NEO_HOOKEAN, 200 substeps):
     FP32 fast path within 1e-4 relative position error of the FP64 plain path."""
     scene = S.spheres_3d()
     out = {}
