@@ -346,6 +346,15 @@ typedef struct {
 typedef int (*mpm_motion_fn)(void* user, int object, double time, mpm_object_state* state);
 int mpm_set_object_motion(mpm_handle* h, int object, mpm_motion_fn fn, void* user);
 
+/* A constitutive model per particle (mpm_model values, n bytes in the caller's
+ * particle order): the reference's several MPM_FINITE_ELEMENTS forces, each
+ * over its affected_particles with its own model (MPM_FINITE_ELEMENTS.cpp:
+ * 47-132; Projects/mpm/STANDARD_TESTS_BASE.cpp:373-404).  models = NULL: every
+ * particle takes the handle's model again.  Call after mpm_set_particles; a
+ * new particle count drops the per-particle models.  Plain path (explicit and
+ * implicit). */
+int mpm_set_particle_models(mpm_handle* h, const uint8_t* models, int64_t n);
+
 /* ---- inspection ---------------------------------------------------------- */
 
 /* Grids of the last substep as doubles on the host, each (G+6)^d nodes (times

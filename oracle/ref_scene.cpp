@@ -69,6 +69,7 @@ struct SCENE_FILE
     std::vector<OBJ> objs, pen;
     long long n;
     std::vector<double> X, V, F, B, mass, volume, mu, lambda;
+    std::vector<unsigned char> models;   // per-particle constitutive model (empty: `model` for all)
 };
 
 template<class T> void rd(FILE* f, T* p, size_t n)
@@ -82,10 +83,10 @@ SCENE_FILE Read_Scene(const char* path)
     if(!f) throw std::runtime_error("cannot open scene");
     char magic[8];
     rd(f, magic, 8);
-    if(memcmp(magic, "MPMSCN06", 8)) throw std::runtime_error("bad scene magic");
+    if(memcmp(magic, "MPMSCN07", 8)) throw std::runtime_error("bad scene magic");
     SCENE_FILE s;
-    int hdr[14];
-    rd(f, hdr, 14);
+    int hdr[15];
+    rd(f, hdr, 15);
     s.npen = hdr[12];
     const int nmoving = hdr[13];
     s.reflection = hdr[11];
@@ -133,6 +134,7 @@ SCENE_FILE Read_Scene(const char* path)
     rd(f, s.X.data(), n * d); rd(f, s.V.data(), n * d);
     rd(f, s.F.data(), n * d * d); rd(f, s.B.data(), n * d * d);
     rd(f, s.mass.data(), n); rd(f, s.volume.data(), n); rd(f, s.mu.data(), n); rd(f, s.lambda.data(), n);
+    if(hdr[14]) { s.models.resize(n); rd(f, s.models.data(), n); }
     fclose(f);
     return s;
 }
@@ -221,11 +223,17 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
             dp->Initialize_Particles(0, (T)s.plastic[4]);
             this->plasticity_models.Append(dp);
         }
-        ISOTROPIC_CONSTITUTIVE_MODEL<T, TV::m>* model;
-        if(s.model == 0) model = new COROTATED_FIXED<T, TV::m>((T)1, (T).3);
-        else if(s.model == 1) model = new NEO_HOOKEAN<T, TV::m>((T)1, (T).3);
-        else model = new ST_VENANT_KIRCHHOFF_HENCKY_STRAIN<T, TV::m>((T)1, (T).3);
-        this->Add_Force(*new MPM_FINITE_ELEMENTS<TV>(force_helper, *model, gather_scatter, 0));
+        auto make_model = [](int m) -> ISOTROPIC_CONSTITUTIVE_MODEL<T, TV::m>* {
+            if(m == 0) return new COROTATED_FIXED<T, TV::m>((T)1, (T).3);
+            if(m == 1) return new NEO_HOOKEAN<T, TV::m>((T)1, (T).3);
+            return new ST_VENANT_KIRCHHOFF_HENCKY_STRAIN<T, TV::m>((T)1, (T).3);};
+        if(s.models.empty()) this->Add_Force(*new MPM_FINITE_ELEMENTS<TV>(force_helper, *make_model(s.model), gather_scatter, 0));
+        else   // one force per model over its particles, as the scenes pass affected_particles
+            for(int m = 0; m < 3; m++) {
+                ARRAY<int> affected;
+                for(int p = 0; p < (int)s.models.size(); p++) if(s.models[p] == m) affected.Append(p);
+                if(affected.m) this->Add_Force(*new MPM_FINITE_ELEMENTS<TV>(force_helper, *make_model(m), gather_scatter, &affected));
+            }
         TV g;
         for(int a = 0; a < d; a++) g(a) = (T)s.gravity[a];
         this->Add_Force(*new MPM_GRAVITY<TV>(force_helper, g, gather_scatter, 0));

@@ -435,6 +435,7 @@ int diff_forward(mpm_handle* h, double dt, int nsteps, int every)
         return set_error(h, MPM_ERR_ARG, "the adjoint runs on the 3D plain path");
     if(h->sp.nobj || h->sp.npen) return set_error(h, MPM_ERR_ARG, "the adjoint does not differentiate collision objects");
     if(h->plastic.kind) return set_error(h, MPM_ERR_ARG, "the adjoint does not differentiate plasticity");
+    if(h->plain.pmodel) return set_error(h, MPM_ERR_ARG, "the adjoint takes one constitutive model");
     if(h->implicit.enabled) return set_error(h, MPM_ERR_ARG, "the adjoint differentiates the explicit substep");
     if(h->sp.model == MPM_STVK_HENCKY) return set_error(h, MPM_ERR_ARG, "the adjoint covers COROTATED_FIXED and NEO_HOOKEAN");
     if(nsteps < 1 || every < 1) return set_error(h, MPM_ERR_ARG, "nsteps and checkpoint interval must be >= 1");

@@ -612,6 +612,29 @@ int mpm_set_object_motion(mpm_handle* h, int object, mpm_motion_fn fn, void* use
     return MPM_OK;
 }
 
+int mpm_set_particle_models(mpm_handle* h, const uint8_t* models, int64_t n)
+{
+    if(!h) return MPM_ERR_ARG;
+    if(fast(h)) return set_error(h, MPM_ERR_ARG, "per-particle models run on the plain path");
+    PlainState& s = h->plain;
+    if(!models) {
+        release_graph(h);
+        MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+        cudaFree(s.pmodel);
+        s.pmodel = nullptr;
+        return MPM_OK;
+    }
+    if(!h->have_particles || n != s.n) return set_error(h, MPM_ERR_ARG, "one model per particle, after mpm_set_particles");
+    for(int64_t p = 0; p < n; p++)
+        if(models[p] != MPM_COROTATED_FIXED && models[p] != MPM_NEO_HOOKEAN && models[p] != MPM_STVK_HENCKY)
+            return set_error(h, MPM_ERR_ARG, "unknown constitutive model");
+    release_graph(h);
+    if(!s.pmodel) MPM_CUDA(h, cudaMalloc(&s.pmodel, (size_t)(n ? n : 1)));
+    MPM_CUDA(h, cudaMemcpyAsync(s.pmodel, models, (size_t)n, cudaMemcpyHostToDevice, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));   // the caller may free its array on return
+    return MPM_OK;
+}
+
 int mpm_set_dt_control(mpm_handle* h, const mpm_dt_control* c)
 {
     if(!h || !c) return MPM_ERR_ARG;

@@ -173,7 +173,8 @@ template<class T, int d> __global__ void k_imp_precompute(ImpArgs<T> ia)
     else svd2<T>(F, U, S, V);
     if(!ok) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
     const T mu = a.mu[p], la = a.lam[p];
-    phat<T, d>(a.sp.model, S, mu, la, P);
+    const int model = model_of(a, p);
+    phat<T, d>(model, S, mu, la, P);
     const T* F0 = ia.F0 + p * d * d;
     T FV[9];
 #pragma unroll
@@ -196,12 +197,12 @@ template<class T, int d> __global__ void k_imp_precompute(ImpArgs<T> ia)
             a.pft[p * d * d + r + d * c] = sum;
         }
     T H[9], Bv[3], Cv[3];
-    stress_derivative<T, d>(a.sp.model, S, mu, la, H, Bv, Cv);
+    stress_derivative<T, d>(model, S, mu, la, H, Bv, Cv);
     for(int e = 0; e < d * d; e++) { ia.U[p * d * d + e] = U[e]; ia.FV[p * d * d + e] = FV[e]; }
     for(int e = 0; e < d; e++) ia.sig[p * d + e] = S[e];
     for(int e = 0; e < 9; e++) ia.dP[p * 15 + e] = H[e];
     for(int e = 0; e < 3; e++) { ia.dP[p * 15 + 9 + e] = Bv[e]; ia.dP[p * 15 + 12 + e] = Cv[e]; }
-    double e = (double)a.vol[p] * (double)energy_density<T, d>(a.sp.model, S, mu, la);
+    double e = (double)a.vol[p] * (double)energy_density<T, d>(model, S, mu, la);
     for(int k = 0; k < d; k++) e -= (double)a.mass[p] * (double)a.X[p * d + k] * a.sp.gravity[k];
     ia.pe[p] = e + epen;
 }

@@ -32,6 +32,7 @@ struct PlainState {
     void *gm = nullptr, *gmv = nullptr, *gv0 = nullptr, *gf = nullptr, *gv = nullptr, *gvf = nullptr;
     void *Fp = nullptr, *mu0 = nullptr, *lam0 = nullptr;   // plastic state (plasticity on): clamp
     void *pdef = nullptr, *rhoF = nullptr, *sigY = nullptr, *vc = nullptr;   // Drucker-Prager
+    uint8_t* pmodel = nullptr;   // per-particle constitutive model (null: the handle's model)
 };
 
 // One scene of a batch, as the fast-path kernels see it.

@@ -85,7 +85,7 @@ template<class T, int d> __global__ void k_stress(PlainArgs<T> a)
     T F[9], PFT[9];
 #pragma unroll
     for(int e = 0; e < d * d; e++) F[e] = a.F[p * d * d + e];
-    if(!pft_svd<T, d>(a.sp.model, F, a.mu[p], a.lam[p], PFT)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
+    if(!pft_svd<T, d>(model_of(a, p), F, a.mu[p], a.lam[p], PFT)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
 #pragma unroll
     for(int e = 0; e < d * d; e++) a.pft[p * d * d + e] = PFT[e];
 }
@@ -570,7 +570,7 @@ template<class T, int d> __global__ void k_sound_speed(PlainArgs<T> a, double* p
         for(int e = 0; e < d * d; e++) F[e] = a.F[p * d * d + e];
         if(d == 3) svd3<T>(F, U, S, V);
         else svd2<T>(F, U, S, V);
-        stress_derivative<T, d>(a.sp.model, S, a.mu[p], a.lam[p], H, Bv, Cv);
+        stress_derivative<T, d>(model_of(a, p), S, a.mu[p], a.lam[p], H, Bv, Cv);
         smax = fmax(smax, (double)sound_speed<T, d>(S, H, Bv, a.mass[p] / a.vol[p]));
     }
     const double r = block_reduce(smax, false);
@@ -783,6 +783,7 @@ int plain_alloc(mpm_handle* h, int64_t n)
                        &s.pdef, &s.rhoF, &s.sigY, &s.vc};
         for(void** p: pa) { cudaFree(*p); *p = nullptr; }
         cudaFree(s.valid); s.valid = nullptr;
+        cudaFree(s.pmodel); s.pmodel = nullptr;
         int64_t m = n ? n : 1;
         MPM_CUDA(h, cudaMalloc(&s.X, m * d * e));
         MPM_CUDA(h, cudaMalloc(&s.V, m * d * e));
@@ -803,7 +804,7 @@ void plain_free(mpm_handle* h)
 {
     PlainState& s = h->plain;
     void* ps[] = {s.X, s.V, s.F, s.B, s.mass, s.vol, s.mu, s.lam, s.pft, s.valid, s.gm, s.gmv, s.gv0, s.gf, s.gv, s.gvf,
-                  s.Fp, s.mu0, s.lam0, s.pdef, s.rhoF, s.sigY, s.vc};
+                  s.Fp, s.mu0, s.lam0, s.pdef, s.rhoF, s.sigY, s.vc, s.pmodel};
     for(void* p: ps) cudaFree(p);
     s = PlainState();
 }

@@ -23,7 +23,14 @@ template<class T> struct PlainArgs {
     int side[6];          // their types per side (mpm_bc_type)
     const ObjMotion* motion;   // moving collision objects (bit j of `moving`): their substep frames
     unsigned moving;
+    const uint8_t* pmodel;     // per-particle constitutive model, or null (sp.model for all)
 };
+
+// The constitutive model of particle p: its own, or the handle's.
+template<class T> __device__ __forceinline__ int model_of(const PlainArgs<T>& a, int64_t p)
+{
+    return a.pmodel ? (int)a.pmodel[p] : a.sp.model;
+}
 
 template<class T, int d> struct Stencil {
     Axis<T> ax[3];
@@ -91,6 +98,7 @@ template<class T> inline PlainArgs<T> args(mpm_handle* h, double dt)
     a.mark_left = h->plastic.kind != MPM_PLASTICITY_NONE;
     a.reflect = h->reflect.enabled;
     for(int k = 0; k < 6; k++) a.side[k] = h->reflect.enabled ? h->reflect.side_type[k] : MPM_BC_FREE;
+    a.pmodel = s.pmodel;
     a.motion = h->motion_dev;
     a.moving = h->motion_dev ? h->moving : 0u;
     return a;

@@ -125,7 +125,7 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex",
            "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state", "mpm_set_implicit",
            "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt",
-           "mpm_set_reflection", "mpm_set_penalty_objects", "mpm_set_object_motion"]
+           "mpm_set_reflection", "mpm_set_penalty_objects", "mpm_set_object_motion", "mpm_set_particle_models"]
 
 _lib = None
 
@@ -179,6 +179,7 @@ def load_library(path: str = LIB_PATH):
     L.mpm_set_penalty_objects.argtypes = [P, ctypes.POINTER(CollisionObject), ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double]
     L.mpm_set_object_motion.argtypes = [P, ctypes.c_int, MOTION_FN, P]
+    L.mpm_set_particle_models.argtypes = [P, P, ctypes.c_int64]
     L.mpm_status_string.argtypes = [ctypes.c_int]
     L.mpm_status_string.restype = ctypes.c_char_p
     for f in EXPORTS:
@@ -364,6 +365,17 @@ class MPM_DRIVER:
         s = scene or self.scene
         self.set_particles(s.X, s.V, s.F, s.B, s.mass, s.volume, s.mu, s.lam, dtype=dtype)
         self._attrs = {"mass": s.mass, "volume": s.volume, "mu": s.mu, "lam": s.lam}
+        if getattr(s, "models", None) is not None:
+            self.set_particle_models(s.models)
+
+    def set_particle_models(self, models: Optional[np.ndarray]):
+        """A constitutive model per particle (mpm_set_particle_models); None: the scene's."""
+        if models is None:
+            self._check(self.L.mpm_set_particle_models(self.h, None, 0), "mpm_set_particle_models")
+            return
+        m = np.ascontiguousarray(models, np.uint8)
+        self._check(self.L.mpm_set_particle_models(self.h, m.ctypes.data_as(ctypes.c_void_p), m.shape[0]),
+                    "mpm_set_particle_models")
 
     def get_particles(self, dtype=np.float64):
         d, n = self.dim, self.n

@@ -246,6 +246,7 @@ class Scene:
     dt_control: Optional[DtControl] = None     # set: nsteps counts frames of frame_dt
     reflection: Optional[Reflection] = None
     penalty: Optional[Penalty] = None
+    models: Optional[np.ndarray] = None        # per-particle constitutive model (None: `model` for all)
 
     @property
     def n(self) -> int:
@@ -265,7 +266,8 @@ class Scene:
         return dataclasses.replace(
             self, X=self.X[idx].copy(), V=self.V[idx].copy(), F=self.F[idx].copy(),
             B=self.B[idx].copy(), mass=self.mass[idx].copy(), volume=self.volume[idx].copy(),
-            mu=self.mu[idx].copy(), lam=self.lam[idx].copy(), objects=list(self.objects))
+            mu=self.mu[idx].copy(), lam=self.lam[idx].copy(), objects=list(self.objects),
+            models=None if self.models is None else self.models[idx].copy())
 
 
 def lame(E, nu):
@@ -585,6 +587,20 @@ def small_2d_moving(seed=93, G=16, nsteps=20, dt=1e-4):
     return s
 
 
+def small_3d_mixed(seed=101, G=16, nsteps=20, dt=1e-4, implicit=False):
+    """small_3d with two materials: COROTATED_FIXED for x < 0.4, NEO_HOOKEAN beyond (the
+    reference's several MPM_FINITE_ELEMENTS forces over particle subsets)."""
+    s = small_3d(seed=seed, G=G, nsteps=nsteps, dt=dt, friction=0.2, E=(2e4, 2e5))
+    s.name = "small3dmixed"
+    s.models = np.where(s.X[:, 0] < 0.4, COROTATED, NEO_HOOKEAN).astype(np.uint8)
+    if implicit:
+        s.name = "small3dmixedimplicit"
+        s.dt = 1e-3
+        s.nsteps = 8
+        s.implicit = Implicit()
+    return s
+
+
 def small_3d_adaptive(seed=51, G=16, nframes=3):
     """A stiff small_3d (E 2e6..8e6) run frame by frame as Simulate_To_Frame does,
     with the strong and the sound-speed CFL on: the sound speed shortens most steps."""
@@ -686,7 +702,7 @@ def snowballs_3d(seed=1234, G=128, ppc=8, E=1.4e5, nu=0.2, density=400.0, dt=5e-
 # --------------------------------------------------------------------------------------------
 # Scene file: read by the reference runner (oracle/ref_scene.cpp) and by the C oracle harness.
 # --------------------------------------------------------------------------------------------
-MAGIC = b"MPMSCN06"
+MAGIC = b"MPMSCN07"
 
 
 def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
@@ -699,8 +715,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         pl = s.plasticity
         im, dc, rf, pn = s.implicit, s.dt_control, s.reflection, s.penalty
         moving = [(j, o.motion) for j, o in enumerate(s.objects) if o.motion is not None]
-        f.write(struct.pack("<14i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
-                            1 if im else 0, 1 if dc else 0, 1 if rf else 0, len(pn.objects) if pn else 0, len(moving)))
+        f.write(struct.pack("<15i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
+                            1 if im else 0, 1 if dc else 0, 1 if rf else 0, len(pn.objects) if pn else 0, len(moving),
+                            1 if s.models is not None else 0))
         f.write(struct.pack("<11d", *pad3(s.domain_min), *pad3(s.domain_max), *pad3(s.gravity), s.dt, 0.0))
         f.write(struct.pack("<%di" % len(dumps), *dumps))
         for o in s.objects:
@@ -731,6 +748,8 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         f.write(np.ascontiguousarray(np.swapaxes(s.B, 1, 2), np.float64).tobytes())
         for a in (s.mass, s.volume, s.mu, s.lam):
             f.write(np.ascontiguousarray(a, np.float64).tobytes())
+        if s.models is not None:
+            f.write(np.ascontiguousarray(s.models, np.uint8).tobytes())
 
 
 def read_dump(path, dim, n, counts, plastic=()):

@@ -57,6 +57,9 @@ CASES = {
     "small3d_moving": (lambda: S.small_3d_moving(), [0, 1, 19], [0, 19]),
     "small2d_moving": (lambda: S.small_2d_moving(), [0, 19], [0, 19]),
     "small3d_moving_implicit": (lambda: S.small_3d_moving(implicit=True), [0, 7], [0, 7]),
+    # two materials: one MPM_FINITE_ELEMENTS force per model over its particles
+    "small3d_mixed": (lambda: S.small_3d_mixed(), [0, 19], [0, 19]),
+    "small3d_mixed_implicit": (lambda: S.small_3d_mixed(implicit=True), [0, 7], [0, 7]),
 }
 
 
@@ -87,6 +90,8 @@ def main(names=None):
             pad = lambda v: list(v) + [0.0] * (3 - len(v))
             arrays["obj_motion"] = np.array([pad(o.motion.center) + pad(o.motion.linear) + pad(o.motion.angular)
                                              if o.motion is not None else [np.nan] * 9 for o in scene.objects])
+        if scene.models is not None:
+            arrays["models"] = np.asarray(scene.models, np.uint8)
         pl = scene.plasticity
         if pl is not None:
             arrays["plasticity"] = np.array(S.plastic_params(pl), np.float64)
@@ -135,6 +140,8 @@ def load(name):
         for o, m in zip(objs, z["obj_motion"]):
             if not np.isnan(m[0]):
                 o.motion = S.Motion(list(m[0:dim]), list(m[3:3 + dim]), list(m[6:9] if dim == 3 else m[6:7]))
+    if "models" in z:
+        scene.models = z["models"].copy()
     if "plasticity" in z:
         scene.plasticity = S.plastic_from_params(z["plasticity"])
     if "reflection" in z:

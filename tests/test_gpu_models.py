@@ -1,0 +1,64 @@
+"""GPU tests of per-particle constitutive models (mpm_set_particle_models).
+
+Parity with the reference's own dumps of a two-material scene (one
+MPM_FINITE_ELEMENTS force per model over its particles) runs with the other
+fixtures: test_gpu_parity.py (explicit, plain FP64) and test_gpu_implicit.py
+(backward Euler).  Here: the argument checks, and that a per-particle array
+naming the handle's model everywhere reproduces the single-model run.
+"""
+import numpy as np
+import pytest
+
+from physbam_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+
+def D():
+    from physbam_b200 import driver
+    return driver
+
+
+def rel(a, b, floor=1e-300):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b))) / max(float(np.max(np.abs(b))), floor)
+
+
+def test_model_arguments(cuda_device):
+    s = S.small_3d(nsteps=1)
+    drv = D().MPM_DRIVER(s, precision=D().FP64, path=D().PATH_PLAIN)
+    with pytest.raises(D().MPMError):
+        drv.set_particle_models(np.zeros(s.n, np.uint8))          # before the particles
+    drv.set_scene_particles(s)
+    with pytest.raises(D().MPMError):
+        drv.set_particle_models(np.zeros(s.n - 1, np.uint8))      # one per particle
+    with pytest.raises(D().MPMError):
+        drv.set_particle_models(np.full(s.n, 7, np.uint8))        # unknown model
+    drv.set_particle_models(np.ones(s.n, np.uint8))
+    drv.set_particle_models(None)
+    drv.close()
+    fast = D().MPM_DRIVER(s, precision=D().FP32, path=D().PATH_FAST)
+    fast.set_scene_particles(s)
+    with pytest.raises(D().MPMError):
+        fast.set_particle_models(np.zeros(s.n, np.uint8))
+    fast.close()
+
+
+@pytest.mark.parametrize("implicit", [False, True])
+def test_uniform_models_equal_the_handle_model(cuda_device, implicit):
+    s = S.small_3d(model=S.NEO_HOOKEAN, nsteps=5)
+    if implicit:
+        s.implicit, s.dt = S.Implicit(), 1e-3
+    out = []
+    for models in (None, np.full(s.n, S.NEO_HOOKEAN, np.uint8)):
+        e = s.copy()
+        e.models = models
+        drv = D().MPM_DRIVER(e, precision=D().FP64, path=D().PATH_PLAIN)
+        drv.set_scene_particles(e)
+        for _ in range(5):
+            drv.Advance_One_Time_Step()
+        out.append(drv.get_particles())
+        drv.close()
+    tol = 2e-9 if implicit else 1e-13
+    for k in ("X", "V", "F"):
+        assert rel(out[1][k], out[0][k], 1.0) < tol, k

@@ -103,3 +103,23 @@ def test_fast_matches_plain(cuda_device):
     assert rel(fast["X"], ref["X"], 1.0) < 2e-6
     assert rel(fast["V"], ref["V"], vmax) < 2e-3
     assert rel(fast["F"], ref["F"], 1.0) < 1e-4
+
+
+def test_fast_penalty_survives_a_new_particle_count(cuda_device):
+    """The fast path's impulse buffer is rebuilt with the particle buffers: a
+    second, smaller particle set on the same handle still feels the objects."""
+    s = S.small_3d_penalty(nsteps=10)
+    sub = s.subset(np.arange(0, s.n, 2))
+    drv = D().MPM_DRIVER(s, precision=D().FP32, path=D().PATH_FAST)
+    drv.set_scene_particles(s)
+    drv.advance(3)
+    drv.set_scene_particles(sub)                 # new count: every particle buffer is reallocated
+    drv.time = 0.0
+    for _ in range(10):
+        drv.Advance_One_Time_Step()
+    got = drv.get_particles()
+    drv.close()
+    ref = run(sub, "plain", 10)
+    vmax = float(np.abs(ref["V"]).max())
+    assert rel(got["X"], ref["X"], 1.0) < 2e-6
+    assert rel(got["V"], ref["V"], vmax) < 2e-3
