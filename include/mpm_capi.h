@@ -355,6 +355,15 @@ int mpm_set_object_motion(mpm_handle* h, int object, mpm_motion_fn fn, void* use
  * implicit). */
 int mpm_set_particle_models(mpm_handle* h, const uint8_t* models, int64_t n);
 
+/* The particles the plasticity model acts on (n bytes, non-zero: plastic), the
+ * model's affected_particles (MPM_PLASTICITY_MODEL::Update_Particles over its
+ * gather_scatter's particles, MPM_PLASTICITY_MODEL.cpp:35-49; Initialize_
+ * Particles over the same, MPM_DRUCKER_PRAGER.cpp:43-60), e.g. the sand of a
+ * sand-and-water scene.  The others keep Fp = I and a zero Drucker-Prager state.
+ * mask = NULL: every particle.  Call after mpm_set_particles; it restarts the
+ * plastic state.  Plain path. */
+int mpm_set_plastic_particles(mpm_handle* h, const uint8_t* mask, int64_t n);
+
 /* ---- inspection ---------------------------------------------------------- */
 
 /* Grids of the last substep as doubles on the host, each (G+6)^d nodes (times

@@ -70,6 +70,7 @@ struct SCENE_FILE
     long long n;
     std::vector<double> X, V, F, B, mass, volume, mu, lambda;
     std::vector<unsigned char> models;   // per-particle constitutive model (empty: `model` for all)
+    std::vector<unsigned char> plastic_mask;   // the plasticity's particles (empty: all)
 };
 
 template<class T> void rd(FILE* f, T* p, size_t n)
@@ -83,10 +84,10 @@ SCENE_FILE Read_Scene(const char* path)
     if(!f) throw std::runtime_error("cannot open scene");
     char magic[8];
     rd(f, magic, 8);
-    if(memcmp(magic, "MPMSCN07", 8)) throw std::runtime_error("bad scene magic");
+    if(memcmp(magic, "MPMSCN08", 8)) throw std::runtime_error("bad scene magic");
     SCENE_FILE s;
-    int hdr[15];
-    rd(f, hdr, 15);
+    int hdr[16];
+    rd(f, hdr, 16);
     s.npen = hdr[12];
     const int nmoving = hdr[13];
     s.reflection = hdr[11];
@@ -135,6 +136,7 @@ SCENE_FILE Read_Scene(const char* path)
     rd(f, s.F.data(), n * d * d); rd(f, s.B.data(), n * d * d);
     rd(f, s.mass.data(), n); rd(f, s.volume.data(), n); rd(f, s.mu.data(), n); rd(f, s.lambda.data(), n);
     if(hdr[14]) { s.models.resize(n); rd(f, s.models.data(), n); }
+    if(hdr[15]) { s.plastic_mask.resize(n); rd(f, s.plastic_mask.data(), n); }
     fclose(f);
     return s;
 }
@@ -213,14 +215,25 @@ template<class TV> struct FILE_SCENE: public MPM_EXAMPLE<TV>
                 particles.lambda0(p) = particles.lambda(p);
             }
         }
+        // a plasticity over a particle subset runs on its own gather_scatter of those particles, as
+        // Add_Drucker_Prager hands it the subset force's (STANDARD_TESTS_BASE.cpp:409-433)
+        GATHER_SCATTER<TV>* pgs = &gather_scatter;
+        ARRAY<int> plastic;
+        if(!s.plastic_mask.empty()) {
+            for(int p = 0; p < (int)s.plastic_mask.size(); p++) if(s.plastic_mask[p]) plastic.Append(p);
+            pgs = new GATHER_SCATTER<TV>(grid, *new ARRAY<int>(plastic));
+            pgs->weights = gather_scatter.weights;
+            pgs->threads = gather_scatter.threads;
+            pgs->Prepare_Scatter(particles);
+        }
         if(s.plasticity == 1)
-            this->plasticity_models.Append(new MPM_PLASTICITY_CLAMP<TV>(particles, &gather_scatter, (T)s.plastic[0],
+            this->plasticity_models.Append(new MPM_PLASTICITY_CLAMP<TV>(particles, pgs, (T)s.plastic[0],
                 (T)s.plastic[1], (T)s.plastic[2], (T)s.plastic[3]));
         if(s.plasticity == 2) {   // as STANDARD_TESTS_BASE::Add_Drucker_Prager (explicit)
-            dp = new MPM_DRUCKER_PRAGER<TV>(particles, &gather_scatter, (T)s.plastic[0], (T)s.plastic[1],
+            dp = new MPM_DRUCKER_PRAGER<TV>(particles, pgs, (T)s.plastic[0], (T)s.plastic[1],
                 (T)s.plastic[2], (T)s.plastic[3]);
             dp->use_vc = s.plastic[5] != 0;
-            dp->Initialize_Particles(0, (T)s.plastic[4]);
+            dp->Initialize_Particles(s.plastic_mask.empty() ? 0 : &plastic, (T)s.plastic[4]);
             this->plasticity_models.Append(dp);
         }
         auto make_model = [](int m) -> ISOTROPIC_CONSTITUTIVE_MODEL<T, TV::m>* {

@@ -635,6 +635,25 @@ int mpm_set_particle_models(mpm_handle* h, const uint8_t* models, int64_t n)
     return MPM_OK;
 }
 
+int mpm_set_plastic_particles(mpm_handle* h, const uint8_t* mask, int64_t n)
+{
+    if(!h) return MPM_ERR_ARG;
+    if(fast(h)) return set_error(h, MPM_ERR_ARG, "plastic particle subsets run on the plain path");
+    PlainState& s = h->plain;
+    if(mask && (!h->have_particles || n != s.n)) return set_error(h, MPM_ERR_ARG, "one flag per particle, after mpm_set_particles");
+    release_graph(h);
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    if(!mask) {
+        cudaFree(s.pmask);
+        s.pmask = nullptr;
+    } else {
+        if(!s.pmask) MPM_CUDA(h, cudaMalloc(&s.pmask, (size_t)(n ? n : 1)));
+        MPM_CUDA(h, cudaMemcpy(s.pmask, mask, (size_t)n, cudaMemcpyHostToDevice));
+    }
+    if(h->plastic.kind != MPM_PLASTICITY_NONE && h->have_particles) return plain_plastic_init(h);
+    return MPM_OK;
+}
+
 int mpm_set_dt_control(mpm_handle* h, const mpm_dt_control* c)
 {
     if(!h || !c) return MPM_ERR_ARG;

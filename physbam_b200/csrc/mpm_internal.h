@@ -33,6 +33,7 @@ struct PlainState {
     void *Fp = nullptr, *mu0 = nullptr, *lam0 = nullptr;   // plastic state (plasticity on): clamp
     void *pdef = nullptr, *rhoF = nullptr, *sigY = nullptr, *vc = nullptr;   // Drucker-Prager
     uint8_t* pmodel = nullptr;   // per-particle constitutive model (null: the handle's model)
+    uint8_t* pmask = nullptr;    // particles the plasticity acts on (null: all)
 };
 
 // One scene of a batch, as the fast-path kernels see it.

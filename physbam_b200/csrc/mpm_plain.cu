@@ -660,6 +660,7 @@ template<class T, int d> __global__ void k_plastic_clamp(PlainArgs<T> a, T* Fp, 
     for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
         if(!a.valid[p]) continue;
         if(a.valid[p] == 2) a.valid[p] = 0;   // left the domain in this G2P: updated once more
+        if(a.pmask && !a.pmask[p]) continue;
         T F[d * d], P[d * d];
 #pragma unroll
         for(int k = 0; k < d * d; k++) { F[k] = a.F[p * d * d + k]; P[k] = Fp[p * d * d + k]; }
@@ -681,6 +682,7 @@ template<class T, int d> __global__ void k_plastic_dp(PlainArgs<T> a, T* Fp, T* 
     for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
         if(!a.valid[p]) continue;
         if(a.valid[p] == 2) a.valid[p] = 0;
+        if(a.pmask && !a.pmask[p]) continue;
         T F[d * d], P[d * d], st[4] = {q[p], rhoF[p], sigY[p], vc[p]};
 #pragma unroll
         for(int k = 0; k < d * d; k++) { F[k] = a.F[p * d * d + k]; P[k] = Fp[p * d * d + k]; }
@@ -696,15 +698,18 @@ template<class T, int d> __global__ void k_plastic_dp(PlainArgs<T> a, T* Fp, T* 
 }
 
 // Drucker-Prager start (MPM_DRUCKER_PRAGER::Initialize_Particles): Fp = I,
-// plastic_def = vc = 0, sigma_Y = cohesion, rho_F at zero plastic deformation.
-template<class T, int d> __global__ void k_dp_init(int64_t n, T* Fp, T* q, T* rhoF, T* sigY, T* vc, T cohesion, Vec5<T> prm)
+// plastic_def = vc = 0, sigma_Y = cohesion, rho_F at zero plastic deformation;
+// particles outside `mask` keep the arrays' zero state.
+template<class T, int d> __global__ void k_dp_init(int64_t n, T* Fp, T* q, T* rhoF, T* sigY, T* vc, T cohesion, Vec5<T> prm,
+    const uint8_t* mask)
 {
     for(int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
         for(int k = 0; k < d * d; k++) Fp[p * d * d + k] = k % (d + 1) == 0 ? (T)1 : (T)0;
         T qq = 0, r = 0;
-        dp_hardening<T>(qq, r, (T)0, prm.v);
-        q[p] = qq; rhoF[p] = r; sigY[p] = cohesion; vc[p] = 0;
+        const bool on = !mask || mask[p];
+        if(on) dp_hardening<T>(qq, r, (T)0, prm.v);
+        q[p] = qq; rhoF[p] = r; sigY[p] = on ? cohesion : (T)0; vc[p] = 0;
     }
 }
 
@@ -784,6 +789,7 @@ int plain_alloc(mpm_handle* h, int64_t n)
         for(void** p: pa) { cudaFree(*p); *p = nullptr; }
         cudaFree(s.valid); s.valid = nullptr;
         cudaFree(s.pmodel); s.pmodel = nullptr;
+        cudaFree(s.pmask); s.pmask = nullptr;
         int64_t m = n ? n : 1;
         MPM_CUDA(h, cudaMalloc(&s.X, m * d * e));
         MPM_CUDA(h, cudaMalloc(&s.V, m * d * e));
@@ -804,7 +810,7 @@ void plain_free(mpm_handle* h)
 {
     PlainState& s = h->plain;
     void* ps[] = {s.X, s.V, s.F, s.B, s.mass, s.vol, s.mu, s.lam, s.pft, s.valid, s.gm, s.gmv, s.gv0, s.gf, s.gv, s.gvf,
-                  s.Fp, s.mu0, s.lam0, s.pdef, s.rhoF, s.sigY, s.vc, s.pmodel};
+                  s.Fp, s.mu0, s.lam0, s.pdef, s.rhoF, s.sigY, s.vc, s.pmodel, s.pmask};
     for(void* p: ps) cudaFree(p);
     s = PlainState();
 }
@@ -903,12 +909,12 @@ int plain_plastic_init(mpm_handle* h)
         const double c = h->plastic.cohesion;
         if(e == 8) {
             const Vec5<double> prm = dp_params<double>(h->plastic);
-            if(d == 3) k_dp_init<double, 3><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.pdef, (double*)s.rhoF, (double*)s.sigY, (double*)s.vc, c, prm);
-            else k_dp_init<double, 2><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.pdef, (double*)s.rhoF, (double*)s.sigY, (double*)s.vc, c, prm);
+            if(d == 3) k_dp_init<double, 3><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.pdef, (double*)s.rhoF, (double*)s.sigY, (double*)s.vc, c, prm, s.pmask);
+            else k_dp_init<double, 2><<<b, 256, 0, h->stream>>>(s.n, (double*)s.Fp, (double*)s.pdef, (double*)s.rhoF, (double*)s.sigY, (double*)s.vc, c, prm, s.pmask);
         } else {
             const Vec5<float> prm = dp_params<float>(h->plastic);
-            if(d == 3) k_dp_init<float, 3><<<b, 256, 0, h->stream>>>(s.n, (float*)s.Fp, (float*)s.pdef, (float*)s.rhoF, (float*)s.sigY, (float*)s.vc, (float)c, prm);
-            else k_dp_init<float, 2><<<b, 256, 0, h->stream>>>(s.n, (float*)s.Fp, (float*)s.pdef, (float*)s.rhoF, (float*)s.sigY, (float*)s.vc, (float)c, prm);
+            if(d == 3) k_dp_init<float, 3><<<b, 256, 0, h->stream>>>(s.n, (float*)s.Fp, (float*)s.pdef, (float*)s.rhoF, (float*)s.sigY, (float*)s.vc, (float)c, prm, s.pmask);
+            else k_dp_init<float, 2><<<b, 256, 0, h->stream>>>(s.n, (float*)s.Fp, (float*)s.pdef, (float*)s.rhoF, (float*)s.sigY, (float*)s.vc, (float)c, prm, s.pmask);
         }
         MPM_LAUNCHED(h, "k_dp_init");
         return MPM_OK;

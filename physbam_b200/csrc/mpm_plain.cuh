@@ -24,6 +24,7 @@ template<class T> struct PlainArgs {
     const ObjMotion* motion;   // moving collision objects (bit j of `moving`): their substep frames
     unsigned moving;
     const uint8_t* pmodel;     // per-particle constitutive model, or null (sp.model for all)
+    const uint8_t* pmask;      // particles the plasticity acts on, or null (all)
 };
 
 // The constitutive model of particle p: its own, or the handle's.
@@ -99,6 +100,7 @@ template<class T> inline PlainArgs<T> args(mpm_handle* h, double dt)
     a.reflect = h->reflect.enabled;
     for(int k = 0; k < 6; k++) a.side[k] = h->reflect.enabled ? h->reflect.side_type[k] : MPM_BC_FREE;
     a.pmodel = s.pmodel;
+    a.pmask = s.pmask;
     a.motion = h->motion_dev;
     a.moving = h->motion_dev ? h->moving : 0u;
     return a;

@@ -125,7 +125,8 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex",
            "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state", "mpm_set_implicit",
            "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt",
-           "mpm_set_reflection", "mpm_set_penalty_objects", "mpm_set_object_motion", "mpm_set_particle_models"]
+           "mpm_set_reflection", "mpm_set_penalty_objects", "mpm_set_object_motion", "mpm_set_particle_models",
+           "mpm_set_plastic_particles"]
 
 _lib = None
 
@@ -180,6 +181,7 @@ def load_library(path: str = LIB_PATH):
                                           ctypes.c_double]
     L.mpm_set_object_motion.argtypes = [P, ctypes.c_int, MOTION_FN, P]
     L.mpm_set_particle_models.argtypes = [P, P, ctypes.c_int64]
+    L.mpm_set_plastic_particles.argtypes = [P, P, ctypes.c_int64]
     L.mpm_status_string.argtypes = [ctypes.c_int]
     L.mpm_status_string.restype = ctypes.c_char_p
     for f in EXPORTS:
@@ -367,6 +369,18 @@ class MPM_DRIVER:
         self._attrs = {"mass": s.mass, "volume": s.volume, "mu": s.mu, "lam": s.lam}
         if getattr(s, "models", None) is not None:
             self.set_particle_models(s.models)
+        if getattr(s, "plastic_mask", None) is not None:
+            self.set_plastic_particles(s.plastic_mask)
+
+    def set_plastic_particles(self, mask: Optional[np.ndarray]):
+        """The particles the plasticity acts on (mpm_set_plastic_particles); None: all.
+        Restarts the plastic state."""
+        if mask is None:
+            self._check(self.L.mpm_set_plastic_particles(self.h, None, 0), "mpm_set_plastic_particles")
+            return
+        m = np.ascontiguousarray(mask, np.uint8)
+        self._check(self.L.mpm_set_plastic_particles(self.h, m.ctypes.data_as(ctypes.c_void_p), m.shape[0]),
+                    "mpm_set_plastic_particles")
 
     def set_particle_models(self, models: Optional[np.ndarray]):
         """A constitutive model per particle (mpm_set_particle_models); None: the scene's."""

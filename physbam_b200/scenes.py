@@ -247,6 +247,7 @@ class Scene:
     reflection: Optional[Reflection] = None
     penalty: Optional[Penalty] = None
     models: Optional[np.ndarray] = None        # per-particle constitutive model (None: `model` for all)
+    plastic_mask: Optional[np.ndarray] = None  # the particles the plasticity acts on (None: all)
 
     @property
     def n(self) -> int:
@@ -267,7 +268,8 @@ class Scene:
             self, X=self.X[idx].copy(), V=self.V[idx].copy(), F=self.F[idx].copy(),
             B=self.B[idx].copy(), mass=self.mass[idx].copy(), volume=self.volume[idx].copy(),
             mu=self.mu[idx].copy(), lam=self.lam[idx].copy(), objects=list(self.objects),
-            models=None if self.models is None else self.models[idx].copy())
+            models=None if self.models is None else self.models[idx].copy(),
+            plastic_mask=None if self.plastic_mask is None else self.plastic_mask[idx].copy())
 
 
 def lame(E, nu):
@@ -601,6 +603,18 @@ def small_3d_mixed(seed=101, G=16, nsteps=20, dt=1e-4, implicit=False):
     return s
 
 
+def small_sand_water_3d(seed=111, G=16, nsteps=20, dt=1e-4):
+    """A sand block (Hencky + Drucker-Prager, x >= 0.4) beside an elastic one (COROTATED_FIXED,
+    no plasticity): two MPM_FINITE_ELEMENTS forces over particle subsets and the plasticity over
+    the sand alone, the structure of the reference's sand-and-water scenes."""
+    s = small_sand_3d(seed=seed, G=G, nsteps=nsteps, dt=dt)
+    s.name = "smallsandwater3d"
+    sand = s.X[:, 0] >= 0.4
+    s.models = np.where(sand, HENCKY, COROTATED).astype(np.uint8)
+    s.plastic_mask = sand.astype(np.uint8)
+    return s
+
+
 def small_3d_adaptive(seed=51, G=16, nframes=3):
     """A stiff small_3d (E 2e6..8e6) run frame by frame as Simulate_To_Frame does,
     with the strong and the sound-speed CFL on: the sound speed shortens most steps."""
@@ -702,7 +716,7 @@ def snowballs_3d(seed=1234, G=128, ppc=8, E=1.4e5, nu=0.2, density=400.0, dt=5e-
 # --------------------------------------------------------------------------------------------
 # Scene file: read by the reference runner (oracle/ref_scene.cpp) and by the C oracle harness.
 # --------------------------------------------------------------------------------------------
-MAGIC = b"MPMSCN07"
+MAGIC = b"MPMSCN08"
 
 
 def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
@@ -715,9 +729,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
         pl = s.plasticity
         im, dc, rf, pn = s.implicit, s.dt_control, s.reflection, s.penalty
         moving = [(j, o.motion) for j, o in enumerate(s.objects) if o.motion is not None]
-        f.write(struct.pack("<15i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
+        f.write(struct.pack("<16i", d, *counts, s.model, s.nsteps, len(s.objects), len(dumps), pl.kind if pl else 0,
                             1 if im else 0, 1 if dc else 0, 1 if rf else 0, len(pn.objects) if pn else 0, len(moving),
-                            1 if s.models is not None else 0))
+                            1 if s.models is not None else 0, 1 if s.plastic_mask is not None else 0))
         f.write(struct.pack("<11d", *pad3(s.domain_min), *pad3(s.domain_max), *pad3(s.gravity), s.dt, 0.0))
         f.write(struct.pack("<%di" % len(dumps), *dumps))
         for o in s.objects:
@@ -750,6 +764,8 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
             f.write(np.ascontiguousarray(a, np.float64).tobytes())
         if s.models is not None:
             f.write(np.ascontiguousarray(s.models, np.uint8).tobytes())
+        if s.plastic_mask is not None:
+            f.write(np.ascontiguousarray(s.plastic_mask, np.uint8).tobytes())
 
 
 def read_dump(path, dim, n, counts, plastic=()):

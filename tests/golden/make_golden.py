@@ -60,6 +60,8 @@ CASES = {
     # two materials: one MPM_FINITE_ELEMENTS force per model over its particles
     "small3d_mixed": (lambda: S.small_3d_mixed(), [0, 19], [0, 19]),
     "small3d_mixed_implicit": (lambda: S.small_3d_mixed(implicit=True), [0, 7], [0, 7]),
+    # sand beside an elastic body: the plasticity over the sand's particles alone
+    "smallsandwater3d_mixed": (lambda: S.small_sand_water_3d(), [0, 1, 19], [0, 19]),
 }
 
 
@@ -92,6 +94,8 @@ def main(names=None):
                                              if o.motion is not None else [np.nan] * 9 for o in scene.objects])
         if scene.models is not None:
             arrays["models"] = np.asarray(scene.models, np.uint8)
+        if scene.plastic_mask is not None:
+            arrays["plastic_mask"] = np.asarray(scene.plastic_mask, np.uint8)
         pl = scene.plasticity
         if pl is not None:
             arrays["plasticity"] = np.array(S.plastic_params(pl), np.float64)
@@ -142,6 +146,8 @@ def load(name):
                 o.motion = S.Motion(list(m[0:dim]), list(m[3:3 + dim]), list(m[6:9] if dim == 3 else m[6:7]))
     if "models" in z:
         scene.models = z["models"].copy()
+    if "plastic_mask" in z:
+        scene.plastic_mask = z["plastic_mask"].copy()
     if "plasticity" in z:
         scene.plasticity = S.plastic_from_params(z["plasticity"])
     if "reflection" in z:

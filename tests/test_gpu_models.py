@@ -62,3 +62,40 @@ def test_uniform_models_equal_the_handle_model(cuda_device, implicit):
     tol = 2e-9 if implicit else 1e-13
     for k in ("X", "V", "F"):
         assert rel(out[1][k], out[0][k], 1.0) < tol, k
+
+
+def test_plastic_particles(cuda_device):
+    """mpm_set_plastic_particles: argument checks; a mask naming every particle
+    reproduces the plasticity over all; the particles outside it keep Fp = I."""
+    s = S.small_sand_3d(nsteps=5)
+    out = []
+    for mask in (None, np.ones(s.n, np.uint8)):
+        e = s.copy()
+        e.plastic_mask = mask
+        drv = D().MPM_DRIVER(e, precision=D().FP64, path=D().PATH_PLAIN)
+        drv.set_scene_particles(e)
+        for _ in range(5):
+            drv.Advance_One_Time_Step()
+        out.append(drv.get_particles())
+        out[-1].update(drv.get_plastic_state())
+        drv.close()
+    for k in ("X", "F", "Fp", "pdef"):
+        assert rel(out[1][k], out[0][k], 1.0) < 1e-13, k
+    drv = D().MPM_DRIVER(s, precision=D().FP64, path=D().PATH_PLAIN)
+    drv.set_scene_particles(s)
+    with pytest.raises(D().MPMError):
+        drv.set_plastic_particles(np.ones(s.n + 1, np.uint8))
+    half = (np.arange(s.n) % 2).astype(np.uint8)
+    drv.set_plastic_particles(half)
+    for _ in range(5):
+        drv.Advance_One_Time_Step()
+    st = drv.get_plastic_state()
+    drv.close()
+    off = half == 0
+    np.testing.assert_array_equal(st["Fp"][off], np.broadcast_to(np.eye(3), (int(off.sum()), 3, 3)))
+    assert np.all(st["pdef"][off] == 0) and np.all(st["rho_F"][off] == 0)
+    fast = D().MPM_DRIVER(s, precision=D().FP32, path=D().PATH_FAST)
+    fast.set_scene_particles(s)
+    with pytest.raises(D().MPMError):
+        fast.set_plastic_particles(half)
+    fast.close()
