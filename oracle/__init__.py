@@ -30,14 +30,17 @@ MAXOBJ = 32
 
 class _Obj(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("type", ctypes.c_int), ("friction", ctypes.c_double),
-                ("a", ctypes.c_double * 3), ("b", ctypes.c_double * 3)]
+                ("a", ctypes.c_double * 3), ("b", ctypes.c_double * 3), ("moving", ctypes.c_int),
+                ("R0", ctypes.c_double * 9), ("x0", ctypes.c_double * 3), ("R1", ctypes.c_double * 9),
+                ("x1", ctypes.c_double * 3), ("v", ctypes.c_double * 3), ("w", ctypes.c_double * 3)]
 
 
 class _Scene(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("counts", ctypes.c_int * 3), ("dmin", ctypes.c_double * 3),
                 ("dmax", ctypes.c_double * 3), ("model", ctypes.c_int), ("gravity", ctypes.c_double * 3),
                 ("nobj", ctypes.c_int), ("obj", _Obj * MAXOBJ), ("npen", ctypes.c_int),
-                ("pen_stiffness", ctypes.c_double), ("pen_separation", ctypes.c_double), ("pen", _Obj * MAXOBJ)]
+                ("pen_stiffness", ctypes.c_double), ("pen_separation", ctypes.c_double), ("pen", _Obj * MAXOBJ),
+                ("models", ctypes.POINTER(ctypes.c_ubyte))]
 
 
 def build(force: bool = False) -> str:
@@ -85,7 +88,21 @@ def lib():
     return _lib
 
 
-def _scene_struct(s) -> _Scene:
+def _rotation(dim, q):
+    """ROTATION<TV>::Rotation_Matrix of a unit quaternion (w, x, y, z), in 2D of (cos, sin),
+    column-major."""
+    if dim == 2:
+        m = np.hypot(q[0], q[1])
+        c, s = (q[0] / m, q[1] / m) if m > 0 else (1.0, 0.0)
+        return [c, s, -s, c]
+    m = float(np.sqrt(sum(x * x for x in q[:4])))
+    w, x, y, z = (q[0] / m, q[1] / m, q[2] / m, q[3] / m) if m > 0 else (1.0, 0.0, 0.0, 0.0)
+    return [1 - 2 * (y * y + z * z), 2 * (x * y + w * z), 2 * (x * z - w * y),
+            2 * (x * y - w * z), 1 - 2 * (x * x + z * z), 2 * (y * z + w * x),
+            2 * (x * z + w * y), 2 * (y * z - w * x), 1 - 2 * (x * x + y * y)]
+
+
+def _scene_struct(s, time: float = 0.0) -> _Scene:
     c = _Scene()
     c.dim = s.dim
     for a in range(3):
@@ -101,6 +118,23 @@ def _scene_struct(s) -> _Scene:
         c.obj[i].kind, c.obj[i].type, c.obj[i].friction = o.kind, o.type, o.friction
         for a in range(s.dim):
             c.obj[i].a[a], c.obj[i].b[a] = o.a[a], o.b[a]
+        m = getattr(o, "motion", None)
+        if m is not None:   # the frames at the substep's start and end, the twist at its end
+            t0, q0, _, _ = m.state(s.dim, time)
+            t1, q1, lin, ang = m.state(s.dim, time + s.dt)
+            c.obj[i].moving = 1
+            for k, val in enumerate(_rotation(s.dim, q0)):
+                c.obj[i].R0[k] = val
+            for k, val in enumerate(_rotation(s.dim, q1)):
+                c.obj[i].R1[k] = val
+            for k in range(s.dim):
+                c.obj[i].x0[k], c.obj[i].x1[k], c.obj[i].v[k] = t0[k], t1[k], lin[k]
+            for k in range(len(ang)):
+                c.obj[i].w[k] = ang[k]
+    models = getattr(s, "models", None)
+    if models is not None:
+        c._models = np.ascontiguousarray(models, np.uint8)   # kept alive with the struct
+        c.models = c._models.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte))
     pn = getattr(s, "penalty", None)
     if pn is not None and pn.objects:
         if len(pn.objects) > MAXOBJ:
@@ -143,6 +177,11 @@ class State:
             self.pdef, self.rho_F, self.cohesion, self.vc = (np.zeros(n) for _ in range(4))
             lib().oracle_dp_init(n, _ptr(self.pdef), _ptr(self.rho_F), _ptr(self.cohesion), _ptr(self.vc),
                                  pl.cohesion, _ptr(self._dp_prm()))
+            mask = getattr(scene, "plastic_mask", None)
+            if mask is not None:   # over the model's affected particles only; the rest keep zeros
+                off = np.asarray(mask) == 0
+                for a in (self.pdef, self.rho_F, self.cohesion, self.vc):
+                    a[off] = 0.0
 
     def _dp_prm(self):
         pl = self.scene.plasticity
@@ -167,6 +206,9 @@ class State:
         if pl is None:
             return
         sim = np.ascontiguousarray(simulated, np.uint8)
+        mask = getattr(self.scene, "plastic_mask", None)
+        if mask is not None:   # the plasticity's own particles (its gather_scatter's)
+            sim = np.ascontiguousarray(sim & (np.asarray(mask) != 0), np.uint8)
         if pl.kind == 2:
             lib().oracle_plastic_dp(self.scene.dim, self.scene.n, _ptr(self.F), _ptr(self.Fp), _ptr(self.mu),
                                     _ptr(self.lam), _ptr(self.pdef), _ptr(self.rho_F), _ptr(self.cohesion),
@@ -190,7 +232,7 @@ class State:
 def substep(state: State, want_grid: bool = False):
     s = state.scene
     L = lib()
-    sc = _scene_struct(s)
+    sc = _scene_struct(s, state.time)
     gn = int(np.prod([c + 6 for c in s.counts[:s.dim]]))
     grids = None
     args = [None] * 4
@@ -214,8 +256,8 @@ def substep(state: State, want_grid: bool = False):
 
 def run(state: State, nsteps: int):
     s = state.scene
-    if s.plasticity is not None:
-        for _ in range(nsteps):
+    if s.plasticity is not None or any(getattr(o, "motion", None) is not None for o in s.objects):
+        for _ in range(nsteps):   # per-substep work on the host: plasticity, object frames
             substep(state)
         return
     sc = _scene_struct(s)

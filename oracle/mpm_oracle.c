@@ -29,10 +29,14 @@
 #define MAXOBJ 32
 
 typedef struct {
-    int kind;            /* 0 = RANGE box, 1 = PLANE */
+    int kind;            /* 0 = RANGE box, 1 = PLANE, 2 = SPHERE */
     int type;            /* 0 = stick, 1 = slip, 2 = separate */
     double friction;
-    double a[3], b[3];   /* box: min, max corners;  plane: unit normal, point */
+    double a[3], b[3];   /* box: min, max corners;  plane: unit normal, point;  sphere: center, radius */
+    /* a moving object (func_frame / func_twist, MPM_COLLISION_OBJECT.cpp:23-71): its frame at the
+       substep's start (R0, x0) and end (R1, x1), R column-major d x d, and its twist at the end */
+    int moving;
+    double R0[9], x0[3], R1[9], x1[3], v[3], w[3];
 } oracle_object;
 
 typedef struct {
@@ -46,6 +50,7 @@ typedef struct {
     int npen;            /* penalty collision objects (IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES) */
     double pen_stiffness, pen_separation;
     oracle_object pen[MAXOBJ];
+    const unsigned char* models;   /* per-particle model (one MPM_FINITE_ELEMENTS per model), or NULL */
 } oracle_scene;
 
 /* ------------------------------------------------------------------ */
@@ -433,6 +438,52 @@ static void obj_normal(int d, const oracle_object* o, const double* X, double* n
     for(int a = 0; a < d; a++) n[a] = o->a[a];
 }
 
+/* MPM_COLLISION_OBJECT::Phi / Normal / Velocity (MPM_COLLISION_OBJECT.cpp:23-71):
+ * a moving object is evaluated in its own frame, Z = R^T (X - x). */
+static void obj_local(int d, const oracle_object* o, int end, const double* X, double* Z)
+{
+    const double* R = end ? o->R1 : o->R0;
+    const double* x = end ? o->x1 : o->x0;
+    for(int c = 0; c < d; c++) {
+        double z = 0;
+        for(int a = 0; a < d; a++) z += R[a + d * c] * (X[a] - x[a]);
+        Z[c] = z;
+    }
+}
+static double obj_phi_at(int d, const oracle_object* o, int end, const double* X)
+{
+    if(!o->moving) return obj_phi(d, o, X);
+    double Z[3];
+    obj_local(d, o, end, X, Z);
+    return obj_phi(d, o, Z);
+}
+static void obj_normal_at(int d, const oracle_object* o, const double* X, double* n)
+{
+    if(!o->moving) { obj_normal(d, o, X, n); return; }
+    double Z[3], nl[3];
+    obj_local(d, o, 1, X, Z);
+    obj_normal(d, o, Z, nl);
+    for(int r = 0; r < d; r++) {
+        double s = 0;
+        for(int c = 0; c < d; c++) s += o->R1[r + d * c] * nl[c];
+        n[r] = s;
+    }
+}
+static void obj_velocity_at(int d, const oracle_object* o, const double* X, double* V)
+{
+    double r[3];
+    if(!o->moving) { for(int a = 0; a < d; a++) V[a] = 0; return; }
+    for(int a = 0; a < d; a++) r[a] = X[a] - o->x1[a];
+    if(d == 3) {
+        V[0] = o->v[0] + (o->w[1] * r[2] - o->w[2] * r[1]);
+        V[1] = o->v[1] + (o->w[2] * r[0] - o->w[0] * r[2]);
+        V[2] = o->v[2] + (o->w[0] * r[1] - o->w[1] * r[0]);
+    } else {
+        V[0] = o->v[0] + -o->w[0] * r[1];
+        V[1] = o->v[1] + o->w[0] * r[0];
+    }
+}
+
 /* The force of the penalty collision objects on a particle at X, one
  * IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES per object in order
  * (Deformables/Collisions_And_Interactions/IMPLICIT_OBJECT_COLLISION_PENALTY_FORCES.cpp:49-60,
@@ -561,7 +612,8 @@ int oracle_substep(const oracle_scene* sc, long long n, double* X, double* V, do
     int* cobj = malloc(sizeof(int) * gn * (sc->nobj ? sc->nobj : 1));
     double* cn = malloc(sizeof(double) * gn * (sc->nobj ? sc->nobj : 1) * 3);
     unsigned char* stuck = calloc(gn, 1);
-    if(!gm || !gv || !gv0 || !gf || !gvf || !dvb || !v1 || !coll || !simulated || !W || !PFT || !ncol || !cobj || !cn || !stuck) {
+    double* sv = calloc(gn * d, sizeof(double));      /* stuck_velocity */
+    if(!sv || !gm || !gv || !gv0 || !gf || !gvf || !dvb || !v1 || !coll || !simulated || !W || !PFT || !ncol || !cobj || !cn || !stuck) {
         rc = -2; goto done;
     }
     node_t nodes[27];
@@ -625,7 +677,7 @@ int oracle_substep(const oracle_scene* sc, long long n, double* X, double* V, do
     }
     for(long long k = 0; k < ns; k++) {       /* MPM_FINITE_ELEMENTS::Precompute */
         long long p = simulated[k];
-        oracle_pft(d, sc->model, F + p * dd, mu[p], la[p], PFT + p * dd);
+        oracle_pft(d, sc->models ? sc->models[p] : sc->model, F + p * dd, mu[p], la[p], PFT + p * dd);
     }
     for(long long k = 0; k < ns; k++) {       /* MPM_FINITE_ELEMENTS::Add_Forces, l.84-99 */
         long long p = simulated[k];
@@ -666,19 +718,23 @@ int oracle_substep(const oracle_scene* sc, long long n, double* X, double* V, do
             const oracle_object* o = sc->obj + j;
             double Vn[3], Xn[3], nrm[3];
             for(int a = 0; a < d; a++) { Vn[a] = gv0[i * d + a] + dv[a]; Xn[a] = X0[a] + dt * Vn[a]; }
-            double phi0 = obj_phi(d, o, X0);
-            double phi = obj_phi(d, o, Xn) - fmin(phi0, 0.);
+            double phi0 = obj_phi_at(d, o, 0, X0);
+            double phi = obj_phi_at(d, o, 1, Xn) - fmin(phi0, 0.);
             if(o->type == 0 && phi0 > 0) continue;
             if(o->type == 1 && phi0 > 0) continue;
             if(o->type == 2 && phi > 1e-15) continue;
             if(o->type != 0 && phi > FLT_MAX) continue;
-            obj_normal(d, o, Xn, nrm);
+            obj_normal_at(d, o, Xn, nrm);
             int c = ncol[i]++;
             cobj[i * sc->nobj + c] = j;
             for(int a = 0; a < d; a++) cn[(i * sc->nobj + c) * 3 + a] = nrm[a];
             for(int a = 0; a < d; a++) Xn[a] -= phi * nrm[a];
             for(int a = 0; a < d; a++) Vn[a] = (Xn[a] - X0[a]) / dt;
-            if(o->type == 0) { for(int a = 0; a < d; a++) Vn[a] = 0; stuck[i] = 1; }
+            if(o->type == 0) {   /* at the object's velocity (stuck_velocity) */
+                obj_velocity_at(d, o, Xn, Vn);
+                for(int a = 0; a < d; a++) sv[i * d + a] = Vn[a];
+                stuck[i] = 1;
+            }
             for(int a = 0; a < d; a++) dv[a] = Vn[a] - gv0[i * d + a];
         }
         (void)t1;
@@ -718,7 +774,7 @@ int oracle_substep(const oracle_scene* sc, long long n, double* X, double* V, do
             gv[i * d + a] = gf[i * d + a] + gv0[i * d + a];
             gvf[i * d + a] += gv0[i * d + a];
         }
-        if(stuck[i]) for(int a = 0; a < d; a++) gvf[i * d + a] = 0;
+        if(stuck[i]) for(int a = 0; a < d; a++) gvf[i * d + a] = sv[i * d + a];
     }
     if(out_v) memcpy(out_v, gv, sizeof(double) * gn * d);
     if(out_vf) memcpy(out_vf, gvf, sizeof(double) * gn * d);
@@ -776,7 +832,7 @@ int oracle_substep(const oracle_scene* sc, long long n, double* X, double* V, do
     }
 done:
     free(gm); free(gv); free(gv0); free(gf); free(gvf); free(dvb); free(v1); free(coll);
-    free(simulated); free(W); free(PFT); free(ncol); free(cobj); free(cn); free(stuck);
+    free(simulated); free(W); free(PFT); free(ncol); free(cobj); free(cn); free(stuck); free(sv);
     return rc;
 }
 

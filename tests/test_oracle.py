@@ -33,10 +33,11 @@ def floors(scene, ref):
             "pdef": 1e-300, "rho_F": 1e-300, "cohesion": 1.0, "vc": 1e-300}
 
 
-# the backward-Euler, adaptive-frame, reflection and moving-object cases pin
-# the GPU path directly against the reference's dumps; the C restatement covers
-# the symplectic-Euler substep with static collision objects
-EXPLICIT = sorted(n for n in CASES if not any(k in n for k in ("implicit", "adaptive", "reflect", "moving", "mixed")))
+# the backward-Euler, adaptive-frame and reflection cases pin the GPU path
+# directly against the reference's dumps; the C restatement covers the
+# symplectic-Euler substep with its collision objects (static, moving and
+# penalty), several materials and plasticity (also over a particle subset)
+EXPLICIT = sorted(n for n in CASES if not any(k in n for k in ("implicit", "adaptive", "reflect")))
 
 
 @pytest.mark.parametrize("name", EXPLICIT)
