@@ -351,8 +351,8 @@ int mpm_set_object_motion(mpm_handle* h, int object, mpm_motion_fn fn, void* use
  * over its affected_particles with its own model (MPM_FINITE_ELEMENTS.cpp:
  * 47-132; Projects/mpm/STANDARD_TESTS_BASE.cpp:373-404).  models = NULL: every
  * particle takes the handle's model again.  Call after mpm_set_particles; a
- * new particle count drops the per-particle models.  Plain path (explicit and
- * implicit). */
+ * new particle count drops the per-particle models.  Both paths (the implicit
+ * solve included); a batch takes one model per scene. */
 int mpm_set_particle_models(mpm_handle* h, const uint8_t* models, int64_t n);
 
 /* The particles the plasticity model acts on (n bytes, non-zero: plastic), the
@@ -361,7 +361,7 @@ int mpm_set_particle_models(mpm_handle* h, const uint8_t* models, int64_t n);
  * Particles over the same, MPM_DRUCKER_PRAGER.cpp:43-60), e.g. the sand of a
  * sand-and-water scene.  The others keep Fp = I and a zero Drucker-Prager state.
  * mask = NULL: every particle.  Call after mpm_set_particles; it restarts the
- * plastic state.  Plain path. */
+ * plastic state.  Both paths; a batch takes one plasticity for all. */
 int mpm_set_plastic_particles(mpm_handle* h, const uint8_t* mask, int64_t n);
 
 /* ---- inspection ---------------------------------------------------------- */

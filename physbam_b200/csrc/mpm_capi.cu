@@ -612,45 +612,45 @@ int mpm_set_object_motion(mpm_handle* h, int object, mpm_motion_fn fn, void* use
     return MPM_OK;
 }
 
+// A per-particle byte array (caller order) on the device: the plain path's
+// particles are in caller order, the fast path looks it up by caller index.
+static int set_particle_bytes(mpm_handle* h, uint8_t*& dst, const uint8_t* src, int64_t n)
+{
+    release_graph(h);
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    if(!src) {
+        cudaFree(dst);
+        dst = nullptr;
+        return MPM_OK;
+    }
+    if(!dst) MPM_CUDA(h, cudaMalloc(&dst, (size_t)(n ? n : 1)));
+    MPM_CUDA(h, cudaMemcpy(dst, src, (size_t)n, cudaMemcpyHostToDevice));
+    return MPM_OK;
+}
+
 int mpm_set_particle_models(mpm_handle* h, const uint8_t* models, int64_t n)
 {
     if(!h) return MPM_ERR_ARG;
-    if(fast(h)) return set_error(h, MPM_ERR_ARG, "per-particle models run on the plain path");
-    PlainState& s = h->plain;
-    if(!models) {
-        release_graph(h);
-        MPM_CUDA(h, cudaStreamSynchronize(h->stream));
-        cudaFree(s.pmodel);
-        s.pmodel = nullptr;
-        return MPM_OK;
+    if(fast(h) && h->fast.batch) return set_error(h, MPM_ERR_ARG, "a batch takes one model per scene");
+    const int64_t count = fast(h) ? h->fast.n : h->plain.n;
+    if(models) {
+        if(!h->have_particles || n != count) return set_error(h, MPM_ERR_ARG, "one model per particle, after mpm_set_particles");
+        for(int64_t p = 0; p < n; p++)
+            if(models[p] != MPM_COROTATED_FIXED && models[p] != MPM_NEO_HOOKEAN && models[p] != MPM_STVK_HENCKY)
+                return set_error(h, MPM_ERR_ARG, "unknown constitutive model");
     }
-    if(!h->have_particles || n != s.n) return set_error(h, MPM_ERR_ARG, "one model per particle, after mpm_set_particles");
-    for(int64_t p = 0; p < n; p++)
-        if(models[p] != MPM_COROTATED_FIXED && models[p] != MPM_NEO_HOOKEAN && models[p] != MPM_STVK_HENCKY)
-            return set_error(h, MPM_ERR_ARG, "unknown constitutive model");
-    release_graph(h);
-    if(!s.pmodel) MPM_CUDA(h, cudaMalloc(&s.pmodel, (size_t)(n ? n : 1)));
-    MPM_CUDA(h, cudaMemcpyAsync(s.pmodel, models, (size_t)n, cudaMemcpyHostToDevice, h->stream));
-    MPM_CUDA(h, cudaStreamSynchronize(h->stream));   // the caller may free its array on return
-    return MPM_OK;
+    return set_particle_bytes(h, fast(h) ? h->fast.pmodel : h->plain.pmodel, models, n);
 }
 
 int mpm_set_plastic_particles(mpm_handle* h, const uint8_t* mask, int64_t n)
 {
     if(!h) return MPM_ERR_ARG;
-    if(fast(h)) return set_error(h, MPM_ERR_ARG, "plastic particle subsets run on the plain path");
-    PlainState& s = h->plain;
-    if(mask && (!h->have_particles || n != s.n)) return set_error(h, MPM_ERR_ARG, "one flag per particle, after mpm_set_particles");
-    release_graph(h);
-    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
-    if(!mask) {
-        cudaFree(s.pmask);
-        s.pmask = nullptr;
-    } else {
-        if(!s.pmask) MPM_CUDA(h, cudaMalloc(&s.pmask, (size_t)(n ? n : 1)));
-        MPM_CUDA(h, cudaMemcpy(s.pmask, mask, (size_t)n, cudaMemcpyHostToDevice));
-    }
-    if(h->plastic.kind != MPM_PLASTICITY_NONE && h->have_particles) return plain_plastic_init(h);
+    if(fast(h) && h->fast.batch) return set_error(h, MPM_ERR_ARG, "a batch takes one plasticity for all particles");
+    const int64_t count = fast(h) ? h->fast.n : h->plain.n;
+    if(mask && (!h->have_particles || n != count)) return set_error(h, MPM_ERR_ARG, "one flag per particle, after mpm_set_particles");
+    int rc = set_particle_bytes(h, fast(h) ? h->fast.pmask : h->plain.pmask, mask, n);
+    if(rc) return rc;
+    if(h->plastic.kind != MPM_PLASTICITY_NONE && h->have_particles) return fast(h) ? fast_plastic_init(h) : plain_plastic_init(h);
     return MPM_OK;
 }
 

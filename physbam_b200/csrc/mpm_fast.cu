@@ -92,7 +92,15 @@ struct FastArgs {
     float* vkick;             // where k_penalty_kick writes V + dt f / m
     const ObjMotionF* motion; // moving collision objects (bit j of `moving`, single-scene handles)
     unsigned moving;
+    const uint8_t* pmodel;    // constitutive model per caller particle index, or null (the scene's)
+    const uint8_t* pmask;     // plasticity on, per caller particle index, or null (all)
 };
+
+// The constitutive model of the particle in slot i of the current buffer.
+__device__ __forceinline__ int slot_model(const FastArgs& a, const SceneDev& sc, uint32_t i)
+{
+    return a.pmodel ? (int)a.pmodel[a.src_pid[i]] : sc.model;
+}
 
 __device__ __forceinline__ int64_t node_index(const SceneDev& sc, int qx, int qy, int qz)
 {
@@ -394,10 +402,10 @@ struct P2GFactors {
 // Factors from a particle state held in registers (X, V, F, B, attributes);
 // `j` is the sorted position recorded if the stress needs the FP64 route.
 __device__ __forceinline__ void factors_from(const FastArgs& a, const SceneDev& sc, const float* X, const float* V,
-    const float* F, const float* B, const float4 at, uint32_t j, P2GFactors& P)
+    const float* F, const float* B, const float4 at, uint32_t j, P2GFactors& P, int model)
 {
     float S[9];
-    if(!stress_fast(sc.model, F, at.z, at.w, S)) {
+    if(!stress_fast(model, F, at.z, at.w, S)) {
         a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
 #pragma unroll
         for(int r = 0; r < 9; r++) S[r] = 0.f;
@@ -437,7 +445,7 @@ __device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneD
     for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.vsrc[r * a.npad + i]; }
 #pragma unroll
     for(int r = 0; r < 9; r++) { F[r] = a.src[(C_F + r) * a.npad + i]; B[r] = a.src[(C_B + r) * a.npad + i]; }
-    factors_from(a, sc, X, V, F, B, a.src_attr[i], j, P);   // attributes: mass, volume, mu, lambda
+    factors_from(a, sc, X, V, F, B, a.src_attr[i], j, P, slot_model(a, sc, i));   // attributes: mass, volume, mu, lambda
 }
 
 // The 27 node values of one particle: f(ii, jj, kk, mass, px, py, pz).
@@ -475,7 +483,7 @@ __device__ __noinline__ void p2g_fallback_force(const FastArgs& a, uint32_t k)
 #pragma unroll
     for(int r = 0; r < 9; r++) F[r] = a.src[(C_F + r) * a.npad + i];
     const float4 at = a.src_attr[i];
-    if(!stress_fp64(sc.model, F, at.z, at.w, S)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
+    if(!stress_fp64(slot_model(a, sc, i), F, at.z, at.w, S)) atomicOr(a.flags, MPM_FLAG_NOT_CONVERGED);
     const float sv = a.dt * at.y;
     const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
     const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
@@ -632,7 +640,7 @@ template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) 
                 B1[c2] = a.src[(C_B + r1 + 3 * c2) * a.npad + i];
             }
             float S[9];
-            if(!stress_fast(sc.model, F, at.z, at.w, S)) {
+            if(!stress_fast(slot_model(a, sc, i), F, at.z, at.w, S)) {
                 // the FP64 SVD route runs in p2g_finish, which adds this
                 // particle's force; here it contributes mass and momentum only
                 if(!odd) a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
@@ -1278,10 +1286,11 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
         for(int k = 0; k < 9; k++) Fp[k] = a.psrc[k * a.npad + i];
 #pragma unroll
         for(int k = 0; k < (PK == 1 ? 2 : 4); k++) st[k] = a.psrc[(9 + k) * a.npad + i];
+        const bool on = !a.pmask || a.pmask[pid];   // the plasticity's own particles
         if(PK == 1)   // st = mu0, lambda0
-            svd = finite && !clamp_inactive(Fn, a.prm) && plastic_eig(Fn, Fp, at, st[0], st[1], a.prm) < 0;
+            svd = on && finite && !clamp_inactive(Fn, a.prm) && plastic_eig(Fn, Fp, at, st[0], st[1], a.prm) < 0;
         else
-            svd = finite && plastic_dp_eig(Fn, Fp, at.z, at.w, st, a.prm) < 0;
+            svd = on && finite && plastic_dp_eig(Fn, Fp, at.z, at.w, st, a.prm) < 0;
 #pragma unroll
         for(int k = 0; k < 9; k++) a.pdst[k * a.npad + j] = Fp[k];
 #pragma unroll
@@ -1401,17 +1410,20 @@ __global__ void k_plastic_init(int64_t n, int64_t npad, float* P, const float4* 
 
 // Drucker-Prager start (MPM_DRUCKER_PRAGER::Initialize_Particles): Fp = I,
 // plastic_def = vc = 0, sigma_Y = cohesion, rho_F at zero plastic deformation.
-__global__ void k_dp_init(int64_t n, int64_t npad, float* P, float cohesion, float a0, float a1, float a3, float a4)
+// Particles outside `mask` (by caller index `pid`) keep the arrays' zero state.
+__global__ void k_dp_init(int64_t n, int64_t npad, float* P, float cohesion, float a0, float a1, float a3, float a4,
+    const int* pid, const uint8_t* mask)
 {
     const float prm[5] = {a0, a1, a3, a4, 0.f};
     float q = 0.f, rho = 0.f;
     dp_hardening<float>(q, rho, 0.f, prm);
     for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const bool on = !mask || mask[pid[j]];
 #pragma unroll
         for(int k = 0; k < 9; k++) P[k * npad + j] = k % 4 == 0 ? 1.f : 0.f;
-        P[9 * npad + j] = q;
-        P[10 * npad + j] = rho;
-        P[11 * npad + j] = cohesion;
+        P[9 * npad + j] = on ? q : 0.f;
+        P[10 * npad + j] = on ? rho : 0.f;
+        P[11 * npad + j] = on ? cohesion : 0.f;
         P[12 * npad + j] = 0.f;
     }
 }
@@ -1505,6 +1517,8 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.pen_k = (float)h->sp.pen_stiffness;
     a.pen_sep = (float)h->sp.pen_separation;
     a.vkick = f.vkick;
+    a.pmodel = f.pmodel;
+    a.pmask = f.pmask;
     a.motion = h->motion_dev_f;
     a.moving = h->motion_dev_f ? h->moving : 0u;
     a.vsrc = a.npen ? f.vkick : a.src + (size_t)C_V * a.npad;
@@ -1698,6 +1712,8 @@ int fast_alloc(mpm_handle* h, int64_t n)
         for(uint32_t** p: ps) { cudaFree(*p); *p = nullptr; }
         cudaFree(f.vkick);
         f.vkick = nullptr;
+        cudaFree(f.pmodel); cudaFree(f.pmask);   // per caller index: a new count drops them
+        f.pmodel = nullptr; f.pmask = nullptr;
         int64_t np = ((n ? n : 1) + 31) / 32 * 32;
         f.npad = np;
         for(int b = 0; b < 2; b++) {
@@ -1739,7 +1755,8 @@ void fast_free(mpm_handle* h)
     void** ps[] = {(void**)&f.keys, (void**)&f.sorted_keys, (void**)&f.perm, (void**)&f.sort_keys_alt, (void**)&f.sort_vals_alt,
                    (void**)&f.sort_scratch, (void**)&f.bstart, (void**)&f.bend, (void**)&f.active, (void**)&f.nb_flag,
                    (void**)&f.nb_list, (void**)&f.counters, (void**)&f.acc, (void**)&f.vel, (void**)&f.scenes,
-                   (void**)&f.block_scene, (void**)&f.nb_scene, (void**)&f.pbase, (void**)&f.objs, (void**)&f.vkick};
+                   (void**)&f.block_scene, (void**)&f.nb_scene, (void**)&f.pbase, (void**)&f.objs, (void**)&f.vkick,
+                   (void**)&f.pmodel, (void**)&f.pmask};
     for(void** p: ps) { cudaFree(*p); *p = nullptr; }
     cudaFree(f.staging);
     f.staging = nullptr;
@@ -1840,7 +1857,7 @@ int fast_plastic_init(mpm_handle* h)
     const mpm_plasticity_desc& pl = h->plastic;
     if(pl.kind == MPM_PLASTICITY_DRUCKER_PRAGER) {
         k_dp_init<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(f.n, f.npad, f.plas[f.cur], (float)pl.cohesion,
-            (float)pl.dp_a0, (float)pl.dp_a1, (float)pl.dp_a3, (float)pl.dp_a4);
+            (float)pl.dp_a0, (float)pl.dp_a1, (float)pl.dp_a3, (float)pl.dp_a4, f.pid[f.cur], f.pmask);
         MPM_LAUNCHED(h, "k_dp_init");
         return MPM_OK;
     }

@@ -88,6 +88,8 @@ struct FastState {
     float4* acc = nullptr;                    // P2G accumulator: momentum+dt*force (xyz), mass (w)
     float4* vel = nullptr;                    // per node 2 x float4: vnew.xyz, vfric.x | vfric.yz, mass, 0
     float* vkick = nullptr;                   // penalty objects on: 3 * npad floats, V + dt f / m per slot
+    uint8_t* pmodel = nullptr;                // constitutive model per caller particle index (null: the scene's)
+    uint8_t* pmask = nullptr;                 // plasticity on per caller particle index (null: all)
     bool keys_ready = false;
     bool hist_ready = false;
     uint64_t generation = 0;   // bumped whenever device buffers are (re)allocated

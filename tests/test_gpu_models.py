@@ -1,10 +1,13 @@
 """GPU tests of per-particle constitutive models (mpm_set_particle_models).
 
 Parity with the reference's own dumps of a two-material scene (one
-MPM_FINITE_ELEMENTS force per model over its particles) runs with the other
-fixtures: test_gpu_parity.py (explicit, plain FP64) and test_gpu_implicit.py
-(backward Euler).  Here: the argument checks, and that a per-particle array
-naming the handle's model everywhere reproduces the single-model run.
+MPM_FINITE_ELEMENTS force per model over its particles) and of sand beside an
+elastic body (the plasticity over the sand alone) runs with the other
+fixtures: test_gpu_parity.py (explicit: plain FP64, fast FP32 in every launch
+shape), test_gpu_plasticity.py and test_gpu_implicit.py (backward Euler).
+Here: the argument checks, that a per-particle array naming the handle's model
+everywhere reproduces the single-model run, and the particles outside the
+plastic subset.
 """
 import numpy as np
 import pytest
@@ -40,8 +43,28 @@ def test_model_arguments(cuda_device):
     fast = D().MPM_DRIVER(s, precision=D().FP32, path=D().PATH_FAST)
     fast.set_scene_particles(s)
     with pytest.raises(D().MPMError):
-        fast.set_particle_models(np.zeros(s.n, np.uint8))
+        fast.set_particle_models(np.zeros(s.n + 1, np.uint8))
+    fast.set_particle_models(np.zeros(s.n, np.uint8))
     fast.close()
+
+
+@pytest.mark.parametrize("path", ["plain", "fast"])
+def test_uniform_models_equal_the_scene_model(cuda_device, path):
+    s = S.small_3d(model=S.NEO_HOOKEAN, nsteps=5)
+    p, prec = (D().PATH_PLAIN, D().FP64) if path == "plain" else (D().PATH_FAST, D().FP32)
+    out = []
+    for models in (None, np.full(s.n, S.NEO_HOOKEAN, np.uint8)):
+        e = s.copy()
+        e.models = models
+        drv = D().MPM_DRIVER(e, precision=prec, path=p)
+        drv.set_scene_particles(e)
+        for _ in range(5):
+            drv.Advance_One_Time_Step()
+        out.append(drv.get_particles())
+        drv.close()
+    tol = 1e-13 if path == "plain" else 1e-6
+    for k in ("X", "V", "F"):
+        assert rel(out[1][k], out[0][k], 1.0) < tol, k
 
 
 @pytest.mark.parametrize("implicit", [False, True])
@@ -96,6 +119,11 @@ def test_plastic_particles(cuda_device):
     assert np.all(st["pdef"][off] == 0) and np.all(st["rho_F"][off] == 0)
     fast = D().MPM_DRIVER(s, precision=D().FP32, path=D().PATH_FAST)
     fast.set_scene_particles(s)
-    with pytest.raises(D().MPMError):
-        fast.set_plastic_particles(half)
+    fast.set_plastic_particles(half)
+    for _ in range(5):
+        fast.Advance_One_Time_Step()
+    st = fast.get_plastic_state()
     fast.close()
+    np.testing.assert_array_equal(st["Fp"][off], np.broadcast_to(np.eye(3), (int(off.sum()), 3, 3)))
+    assert np.all(st["pdef"][off] == 0) and np.all(st["rho_F"][off] == 0)
+    assert np.abs(st["Fp"][~off] - np.eye(3)).max() > 1e-4   # the sand half did yield

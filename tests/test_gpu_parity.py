@@ -77,8 +77,8 @@ def run_case(name, precision, path, tol, shape=None):
 # fixed-step symplectic-Euler cases (the implicit and adaptive-frame fixtures
 # have their own tests)
 FIXED = sorted(n for n in CASES if "implicit" not in n and "adaptive" not in n)
-# the fast path has no reflection boundary conditions nor per-particle models
-FAST = sorted(n for n in FIXED if n.startswith("small3d") and "reflect" not in n and "mixed" not in n)
+# the fast path has no reflection boundary conditions
+FAST = sorted(n for n in FIXED if n.startswith("small3d") and "reflect" not in n)
 
 
 @pytest.mark.parametrize("name", FIXED)

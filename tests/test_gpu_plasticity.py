@@ -45,8 +45,10 @@ TOL_FP64 = {"X": 1e-12, "V": 1e-9, "F": 1e-10, "B": 1e-8, "Fp": 1e-10, "mu": 1e-
 # FP32 after 20 substeps; the hardening exp(10 (1 - det Fp)) turns an FP32
 # error of det Fp into ten times that in mu and lambda; the Drucker-Prager
 # state is a sum of FP32 logarithms of the singular values.
+# vc accumulates the log of the volume change over every yielding step (relative to its
+# largest value); beside a stiff elastic body the FP32 sums reach 1.1e-4 after 20 steps.
 TOL_FP32 = {"X": 2e-6, "V": 2e-3, "F": 1e-4, "B": 2e-3, "Fp": 1e-4, "mu": 1e-3, "lam": 1e-3,
-            "pdef": 1e-4, "rho_F": 1e-5, "cohesion": 1e-6, "vc": 1e-4}
+            "pdef": 1e-4, "rho_F": 1e-5, "cohesion": 1e-6, "vc": 3e-4}
 
 
 def run_snow(name, precision, path, tol, shape=None):
@@ -84,7 +86,7 @@ SHAPES = [(0, 128, 1), (2, 64, 2), (3, 256, 1)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "p2g%d-g2p%d-x%d" % s)
-@pytest.mark.parametrize("name", [n for n in SNOW + SAND if "3d" in n and "mixed" not in n])
+@pytest.mark.parametrize("name", [n for n in SNOW + SAND if "3d" in n])
 def test_fast_fp32_plastic_matches_reference(cuda_device, name, shape):
     run_snow(name, D().FP32, D().PATH_FAST, TOL_FP32, shape)
 
