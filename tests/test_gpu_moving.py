@@ -81,9 +81,14 @@ def test_identity_motion_equals_static(cuda_device, path, implicit):
     moved.objects = [S.CollisionObject(o.kind, o.type, o.friction, o.a, o.b, motion=S.Motion([0, 0, 0], [0, 0, 0], [0, 0, 0]))
                      for o in s.objects]
     a, b = run(s, path, 5), run(moved, path, 5)
-    tol = (1e-9 if implicit else 1e-13) if path == "plain" else 1e-6
+    # implicit: two runs of the same solve may take different Newton paths (the order of
+    # the atomic sums), within the bounds of the implicit parity tests
+    if implicit:
+        tol = {"X": 2e-9, "V": 1e-6, "F": 1e-7}
+    else:
+        tol = dict.fromkeys(("X", "V", "F"), 1e-13 if path == "plain" else 1e-6)
     for k in ("X", "V", "F"):
-        assert rel(b[k], a[k], 1.0) < tol, k
+        assert rel(b[k], a[k], 1.0) < tol[k], k
 
 
 def test_sticky_nodes_follow_the_object(cuda_device):
