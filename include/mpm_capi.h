@@ -334,9 +334,11 @@ int mpm_set_penalty_objects(mpm_handle* h, const mpm_collision_object* objs, int
  * t + dt calls it at t and t + dt: MPM_OBJECTIVE::Test_Add_Collision
  * (MPM_OBJECTIVE.cpp:150-181) tests a node's start against the frame at t,
  * projects its end at t + dt, and holds a sticky node at the object's velocity
- * there.  fn = NULL makes the object static again.  Substeps with moving
- * objects run without the captured CUDA graph.  Both paths and the implicit
- * solve; a batch takes none. */
+ * there.  fn = NULL makes the object static again.  mpm_substep with moving
+ * objects runs eagerly; mpm_advance over several substeps evaluates every
+ * substep's frames first and replays its CUDA graph, whose first kernel takes
+ * the next substep's frames.  Both paths and the implicit solve; a batch takes
+ * none. */
 typedef struct {
     double translation[3];
     double rotation[4];

@@ -114,15 +114,10 @@ static void rotation_matrix(int d, const double* q, double* R)
     R[2] = 2 * (x * z - w * y);     R[5] = 2 * (y * z + w * x);     R[8] = 1 - 2 * (x * x + y * y);
 }
 
-// The moving objects' frames at time and time + dt and twists at time + dt,
-// from their callbacks, copied to the device in stream order (from host memory
-// the copy has staged before it returns, so the next substep may refill it).
-int update_motion(mpm_handle* h, double time, double dt)
+// The frames of one substep from the objects' callbacks (double and float).
+static int eval_motion(mpm_handle* h, double time, double dt, mpm::ObjMotion* m, mpm::ObjMotionF* mf)
 {
-    if(!h->moving) return MPM_OK;
     const int d = h->sp.dim;
-    mpm::ObjMotion m[MPM_MAX_OBJECTS] = {};
-    mpm::ObjMotionF mf[MPM_MAX_OBJECTS] = {};
     for(int j = 0; j < h->sp.nobj && j < MPM_MAX_OBJECTS; j++) {
         if(!((h->moving >> j) & 1u)) continue;
         mpm_object_state s0{}, s1{};
@@ -140,6 +135,71 @@ int update_motion(mpm_handle* h, double time, double dt)
             mf[j].v[k] = (float)m[j].v[k]; mf[j].w[k] = (float)m[j].w[k];
         }
     }
+    return MPM_OK;
+}
+
+// Copy slot *slot of the tables into the substep's frames and step the slot.
+__global__ void k_motion_pick(const mpm::ObjMotion* tab, const mpm::ObjMotionF* tabf, unsigned* slot, int cap,
+    mpm::ObjMotion* out, mpm::ObjMotionF* outf)
+{
+    const unsigned s = *slot < (unsigned)cap ? *slot : (unsigned)cap - 1u;
+    const int nd = (int)(sizeof(mpm::ObjMotion) * MPM_MAX_OBJECTS / sizeof(double));
+    const int nf = (int)(sizeof(mpm::ObjMotionF) * MPM_MAX_OBJECTS / sizeof(float));
+    const double* src = (const double*)(tab + (size_t)s * MPM_MAX_OBJECTS);
+    const float* srcf = (const float*)(tabf + (size_t)s * MPM_MAX_OBJECTS);
+    for(int k = threadIdx.x; k < nd; k += blockDim.x) ((double*)out)[k] = src[k];
+    for(int k = threadIdx.x; k < nf; k += blockDim.x) ((float*)outf)[k] = srcf[k];
+    __syncthreads();
+    if(threadIdx.x == 0) *slot = s + 1u;
+}
+
+// The frames of the substeps of one mpm_advance, before its graph replays.
+static int fill_motion_table(mpm_handle* h, double dt, double time, int nsteps)
+{
+    const size_t one = sizeof(mpm::ObjMotion) * MPM_MAX_OBJECTS, onef = sizeof(mpm::ObjMotionF) * MPM_MAX_OBJECTS;
+    if(nsteps > h->motion_cap) {   // the replayed graphs hold the table pointers
+        release_graph(h);
+        MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+        cudaFree(h->motion_table); cudaFree(h->motion_table_f);
+        h->motion_table = nullptr; h->motion_table_f = nullptr; h->motion_cap = 0;
+        MPM_CUDA(h, cudaMalloc(&h->motion_table, one * nsteps));
+        MPM_CUDA(h, cudaMalloc(&h->motion_table_f, onef * nsteps));
+        h->motion_cap = nsteps;
+    }
+    if(!h->motion_slot) MPM_CUDA(h, cudaMalloc(&h->motion_slot, sizeof(unsigned)));
+    if(!h->motion_dev) MPM_CUDA(h, cudaMalloc(&h->motion_dev, one));
+    if(!h->motion_dev_f) MPM_CUDA(h, cudaMalloc(&h->motion_dev_f, onef));
+    std::vector<mpm::ObjMotion> m((size_t)nsteps * MPM_MAX_OBJECTS);
+    std::vector<mpm::ObjMotionF> mf((size_t)nsteps * MPM_MAX_OBJECTS);
+    for(int s = 0; s < nsteps; s++) {
+        int rc = eval_motion(h, time + s * dt, dt, &m[(size_t)s * MPM_MAX_OBJECTS], &mf[(size_t)s * MPM_MAX_OBJECTS]);
+        if(rc) return rc;
+    }
+    // in stream order after the earlier replays that read the tables; a copy from
+    // pageable memory has staged it before it returns
+    MPM_CUDA(h, cudaMemcpyAsync(h->motion_table, m.data(), one * nsteps, cudaMemcpyHostToDevice, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(h->motion_table_f, mf.data(), onef * nsteps, cudaMemcpyHostToDevice, h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(h->motion_slot, 0, sizeof(unsigned), h->stream));
+    return MPM_OK;
+}
+
+// The moving objects' frames at time and time + dt and twists at time + dt,
+// from their callbacks, copied to the device in stream order (from host memory
+// the copy has staged before it returns, so the next substep may refill it);
+// inside mpm_advance the next slot of the prepared tables instead.
+int update_motion(mpm_handle* h, double time, double dt)
+{
+    if(!h->moving) return MPM_OK;
+    if(h->motion_from_table) {
+        k_motion_pick<<<1, 256, 0, h->stream>>>(h->motion_table, h->motion_table_f, h->motion_slot, h->motion_cap,
+                                                h->motion_dev, h->motion_dev_f);
+        MPM_LAUNCHED(h, "k_motion_pick");
+        return MPM_OK;
+    }
+    mpm::ObjMotion m[MPM_MAX_OBJECTS] = {};
+    mpm::ObjMotionF mf[MPM_MAX_OBJECTS] = {};
+    int rc = eval_motion(h, time, dt, m, mf);
+    if(rc) return rc;
     if(!h->motion_dev) MPM_CUDA(h, cudaMalloc(&h->motion_dev, sizeof(m)));
     if(!h->motion_dev_f) MPM_CUDA(h, cudaMalloc(&h->motion_dev_f, sizeof(mf)));
     MPM_CUDA(h, cudaMemcpyAsync(h->motion_dev, m, sizeof(m), cudaMemcpyHostToDevice, h->stream));
@@ -167,7 +227,8 @@ static int enqueue_substep(mpm_handle* h, double dt, double time)
 // path alternates its particle buffers, so it keeps one graph per parity.
 static int run_substep(mpm_handle* h, double dt, double time)
 {
-    if(h->timing || h->implicit.enabled || h->moving || (!fast(h) && reduces_dt(h))) return enqueue_substep(h, dt, time);
+    if(h->timing || h->implicit.enabled || (h->moving && !h->motion_from_table) || (!fast(h) && reduces_dt(h)))
+        return enqueue_substep(h, dt, time);
     const int par = fast(h) ? h->fast.cur : 0;
     cudaGraphExec_t& ge = h->graphs[par];
     if(!ge) {
@@ -273,6 +334,9 @@ int mpm_destroy(mpm_handle* h)
     cudaFree(h->pen_f);
     cudaFree(h->motion_dev);
     cudaFree(h->motion_dev_f);
+    cudaFree(h->motion_table);
+    cudaFree(h->motion_table_f);
+    cudaFree(h->motion_slot);
     cudaFree(h->d_flags);
     if(h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -400,9 +464,13 @@ int mpm_advance(mpm_handle* h, double dt, double time, int nsteps)
     if(nsteps < 0) return set_error(h, MPM_ERR_ARG, "nsteps < 0");
     if(h->graph_dt != dt) release_graph(h);
     if(fast(h) && nsteps && (rc = fast_prepare_sort(h))) return rc;
-    for(int s = 0; s < nsteps; s++)
-        if((rc = run_substep(h, dt, time + s * dt))) return rc;
-    return MPM_OK;
+    // moving objects: their frames go into tables first, so the substeps can replay a graph
+    const bool table = h->moving && nsteps > 1 && !h->timing && !h->implicit.enabled && !(!fast(h) && reduces_dt(h));
+    if(table && (rc = fill_motion_table(h, dt, time, nsteps))) return rc;
+    h->motion_from_table = table;
+    for(int s = 0; s < nsteps && !rc; s++) rc = run_substep(h, dt, time + s * dt);
+    h->motion_from_table = false;
+    return rc;
 }
 
 int mpm_synchronize(mpm_handle* h)

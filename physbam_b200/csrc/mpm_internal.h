@@ -154,6 +154,13 @@ struct mpm_handle {
     unsigned moving = 0;                      // bit j: object j moves
     mpm::ObjMotion* motion_dev = nullptr;     // MPM_MAX_OBJECTS, plain path and implicit solve
     mpm::ObjMotionF* motion_dev_f = nullptr;  // the same in float, fast path
+    // mpm_advance over moving objects: the frames of every substep, filled before the
+    // graph replays; each replay's first kernel copies the next slot into motion_dev
+    mpm::ObjMotion* motion_table = nullptr;
+    mpm::ObjMotionF* motion_table_f = nullptr;
+    unsigned* motion_slot = nullptr;          // device counter of the slot to take next
+    int motion_cap = 0;                       // substeps the tables hold
+    bool motion_from_table = false;
     mpm_implicit_stats imp_stats{};  // of the last implicit solve
     ImplicitState* imp = nullptr;
     // timing
