@@ -461,9 +461,9 @@ def measure_collision_extras(args, D, S, stream, flush, elastic_ms):
     penalty slab under the balls and a penalty ball between them, so the
     impulse pre-pass runs for every particle each substep; (b) moving collision
     objects: a sticky paddle turning between the balls and a slip plate sliding
-    over them, whose frames the host evaluates and uploads every substep (such
-    substeps run eagerly, without the captured graph).  Their cost against the
-    elastic headline."""
+    over them, whose frames the host evaluates and uploads every substep (timed
+    one substep per call, each runs eagerly; mpm_advance over several substeps
+    would replay a graph).  Their cost against the elastic headline."""
     out = {}
     steps = max(5, min(args.steps, 20))
     pen = S.spheres_3d()
