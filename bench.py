@@ -44,6 +44,12 @@ SNOW_LEAD_SUBSTEPS = 600                                # plastic legs: substeps
 GRID_BYTES_PER_NODE = 48                                # grid update: read 16, write 32
 
 
+def chosen(report):
+    """The autotuner's full report goes to stderr; the JSON line keeps the chosen shape."""
+    print("autotune: " + report, file=sys.stderr, flush=True)
+    return report.split("chosen", 1)[-1].strip() if "chosen" in report else report
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -263,7 +269,7 @@ def our_arm(args):
     stream = torch.cuda.Stream()
     drv.set_stream(stream.cuda_stream)
     drv.set_scene_particles(scene)
-    tuned = drv.autotune(substeps=5, cold_l2=True)   # the timed substeps below run with the L2 flushed
+    tuned = chosen(drv.autotune(substeps=5, cold_l2=True))   # the timed substeps below run with the L2 flushed
     shape = drv.get_launch_shape()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -327,7 +333,10 @@ def our_arm(args):
     if not args.no_batch:
         batch = measure_batch(args, D, S, stream, flush, peak, dist)
     if world == 1 and not args.no_adjoint:
-        adjoint = measure_adjoint(D, S)
+        adjoint = measure_adjoint(D, S, stream)
+    par = None
+    if rank == 0 and world == 1 and not args.no_parity:
+        par = measure_parity(args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -335,6 +344,13 @@ def our_arm(args):
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": substep_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
+            # the precision and adjoint targets, short and early in the line
+            "fp32_over_plain_fp64": plain["fast_fp32_speedup"] if plain else None,
+            "cfg2_pos_rel_err": par["spheres3d-128"]["X"] if par and "spheres3d-128" in par else None,
+            "cfg2_pos_rel_err_vs_plain_fp64": plain["pos_rel_err_vs_fast_fp32"] if plain else None,
+            "bwd_over_fwd_plain": adjoint["bwd_over_fwd_plain"] if adjoint else None,
+            "bwd_over_fwd_fast": adjoint["bwd_over_fwd_fast"] if adjoint else None,
+            "parity": par,
             "data": "synthetic (seeded jittered-in-cell seeding, numpy PCG64 seed 1234)",
             "config": {"workload": WORKLOAD, "particles": n, "grid": "128^3", "dt": scene.dt,
                        "l2": "flushed before every timed substep (512 MB write)",
@@ -383,7 +399,7 @@ def measure_batch(args, D, S, stream, flush, peak, dist=None):
     drv = D.MPM_BATCH(scenes)
     drv.set_stream(stream.cuda_stream)
     drv.set_scene_particles(dtype=np.float32)
-    report = drv.autotune(substeps=3, cold_l2=True)
+    report = chosen(drv.autotune(substeps=3, cold_l2=True))
     steps = max(5, min(args.steps, 20))
     ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3, dist)
     drv.close()
@@ -411,8 +427,19 @@ def measure_plain_fp64(args, D, S, stream, flush, fast_ms):
     ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
     drv.close()
     sub = ms / steps
+    # precision beside the speed-up: both paths over the scene's 200 substeps
+    finals = []
+    for prec, path in ((D.FP64, D.PATH_PLAIN), (D.FP32, D.PATH_FAST)):
+        d = D.MPM_DRIVER(scene, precision=prec, path=path)
+        d.set_stream(stream.cuda_stream)
+        d.set_scene_particles(scene)
+        d.advance(scene.nsteps)
+        finals.append(d.get_particles()["X"])
+        d.close()
+    err = float(np.linalg.norm(finals[1] - finals[0]) / np.linalg.norm(finals[0]))
     return {"workload": WORKLOAD.replace("fp32", "fp64-plain"), "steps": steps, "ms_per_step": sub,
             "value": scene.n * steps / (ms / 1e3), "unit": METRIC, "fast_fp32_speedup": sub / fast_ms,
+            "pos_rel_err_vs_fast_fp32": err,
             "kernel_ms_per_substep": {k: v[0] / max(v[1], 1) for k, v in ktimes.items()}}
 
 
@@ -429,7 +456,7 @@ def measure_plastic(args, D, S, stream, flush, peak, elastic_ms, scene, workload
     # timed mid-collision: the balls touch after ~300 substeps, and from then on
     # the clamp acts and hardens (before, the SVD is skipped for every particle)
     drv.advance(SNOW_LEAD_SUBSTEPS)
-    tuned = drv.autotune(substeps=3, cold_l2=True)
+    tuned = chosen(drv.autotune(substeps=3, cold_l2=True))
     steps = max(5, min(args.steps, 20))
     ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
     plastic = drv.get_plastic_state(np.float32)
@@ -480,7 +507,7 @@ def measure_collision_extras(args, D, S, stream, flush, elastic_ms):
         drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
         drv.set_stream(stream.cuda_stream)
         drv.set_scene_particles(scene)
-        drv.autotune(substeps=3, cold_l2=True)
+        chosen(drv.autotune(substeps=3, cold_l2=True))
         ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
         drv.close()
         sub = ms / steps
@@ -542,36 +569,73 @@ def measure_implicit(args, D, S, stream, flush):
     return out
 
 
-def measure_adjoint(D, S):
-    """The differentiable cube: 64^3, 64 substeps, checkpoint every 8; FP32 forward and
-    backward through the C ABI (device arrays), timed with CUDA events."""
+def measure_adjoint(D, S, stream):
+    """The differentiable cube: 64^3, 64 substeps, checkpoint every 8.  The FP32
+    rollout with checkpoints (mpm_diff_forward, plain path) and its adjoint
+    (mpm_diff_backward) through the C ABI on device arrays, beside the fast FP32
+    forward of the same 64 substeps (mpm_advance); each timed with CUDA events on
+    the library's stream, best of 3 after one warm-up."""
     import torch
     scene = S.cube_3d()
     n = scene.n
     drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_PLAIN)
+    drv.set_stream(stream.cuda_stream)
     t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float32, device="cuda")
     X, V = t(scene.X), t(scene.V)
     Fc = t(np.swapaxes(scene.F, 1, 2).reshape(n, 9))
     Bc = t(np.swapaxes(scene.B, 1, 2).reshape(n, 9))
     m, vol, mu, lam = t(scene.mass), t(scene.volume), t(scene.mu), t(scene.lam)
     g = [torch.ones_like(X) * 1e-3, torch.zeros_like(V), torch.zeros_like(Fc), torch.zeros_like(Bc)]
-    fwd, bwd = [], []
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    fwd, bwd, fast = [], [], []
     for it in range(4):
         drv.set_particles_device(X, V, Fc, Bc, m, vol, mu, lam)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        drv.diff_forward(64, 8)
-        t1 = time.perf_counter()
-        drv.diff_backward(*g)
-        t2 = time.perf_counter()
+        f = timed(lambda: drv.diff_forward(64, 8))
+        b = timed(lambda: drv.diff_backward(*g))
         if it:
-            fwd.append(t1 - t0)
-            bwd.append(t2 - t1)
+            fwd.append(f)
+            bwd.append(b)
     drv.close()
-    f, b = min(fwd), min(bwd)
+    fd = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+    fd.set_stream(stream.cuda_stream)
+    for it in range(4):
+        fd.set_scene_particles(scene)
+        torch.cuda.synchronize()
+        ms = timed(lambda: fd.advance(64))
+        if it:
+            fast.append(ms)
+    fd.close()
+    f, b, ff = min(fwd), min(bwd), min(fast)
     return {"workload": "cube3d-64^3-corotated-8ppc, 64 substeps, checkpoint every 8, fp32", "particles": n,
-            "fwd_ms": f * 1e3, "bwd_ms": b * 1e3, "bwd_over_fwd": b / f,
-            "timing": "host wall clock around synchronous C-ABI calls, best of 3"}
+            "fwd_plain_ms": f, "bwd_ms": b, "fwd_fast_ms": ff, "bwd_over_fwd_plain": b / f,
+            "bwd_over_fwd_fast": b / ff,
+            "timing": "CUDA events on the library's stream around each C-ABI call, best of 3 after a warm-up"}
+
+
+def measure_parity(args):
+    """Per-quantity relative L2 error of the FP32 fast path against the reference's
+    own FP64 build (oracle/_ref, all host threads) after the last substep: the two
+    spheres (200 substeps), the 64^3 dam break (100), the cube (64) and eleven
+    scenes of the 256-scene batch run in one batch handle.  Outside every timed
+    region; the checker, not a measurement of speed."""
+    import oracle
+    from oracle import parity
+    if not oracle.ref_available():
+        return None
+    table = {}
+    for name in sorted(parity.SINGLE):
+        table[name] = parity.single_table(name)
+    table.update(parity.batch_table())
+    return parity.compact(table)
 
 
 def profile_case(args, D, S):
@@ -627,7 +691,7 @@ def measure_large(args, D, S, stream, flush, peak, peak_kind):
     drv.set_stream(stream.cuda_stream)
     drv.set_scene_particles(scene, dtype=np.float32)
     del scene.F, scene.B
-    tuned = drv.autotune(substeps=2, cold_l2=True)
+    tuned = chosen(drv.autotune(substeps=2, cold_l2=True))
     steps = max(5, min(args.steps, 20))
     ms, ktimes, _ = measure_substeps(drv, stream, flush, steps, 3)
     drv.close()
@@ -657,6 +721,7 @@ def main():
     ap.add_argument("--no-implicit", action="store_true", help="skip the backward-Euler measurement")
     ap.add_argument("--no-snow", action="store_true", help="skip the snow and sand (plasticity) measurements")
     ap.add_argument("--no-extras", action="store_true", help="skip the penalty and moving-object measurements")
+    ap.add_argument("--no-parity", action="store_true", help="skip the FP32-vs-reference-FP64 error table")
     ap.add_argument("--scene", choices=["spheres3d", "dam3d", "cube3d", "snowballs3d", "sand3d", "spheres3d_implicit"],
                     help="profiling run of one scene only")
     ap.add_argument("--grid", type=int, default=0, help="grid cells per side for --scene")

@@ -433,6 +433,12 @@ typedef struct {
 int mpm_batch_create(const mpm_scene_desc* scenes, int count, const mpm_collision_object* objects, int object_count,
                      mpm_handle** out);
 
+/* mpm_get_grid for scene `scene` of a batch (or scene 0 of any fast-path
+ * handle): the scene's ghosted grid, (G+6)^3 nodes, of the last substep, as
+ * that scene's MPM_EXAMPLE would hold it (mass, velocity after the forces,
+ * friction velocity; any pointer may be NULL). */
+int mpm_batch_get_grid(mpm_handle* h, int scene, double* mass, double* v, double* vfric);
+
 /* Time the fast path's launch shapes (P2G work split, G2P block size, number of
  * persistent CTAs) for `substeps` substeps each on the handle's own particles
  * and keep the fastest; the particle state is left unchanged.  `report` (may be
@@ -488,20 +494,22 @@ int mpm_diff_backward(mpm_handle* h, const mpm_particles_view* grad_final, mpm_p
 int mpm_radix_sort_u32(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm);
 
 /* The same sort for callers that cannot allocate device memory at the time
- * they sort: work recorded into a CUDA graph by stream capture, hosts that
- * give the library a fixed memory budget up front, and loops that cannot
- * absorb cudaMalloc/cudaFree and the device synchronisation they bring.
+ * they sort: hosts that give the library a fixed memory budget up front and
+ * forbid growth afterwards, and loops that cannot absorb cudaMalloc/cudaFree
+ * and the device-wide synchronisation cudaFree brings.
  * There is no counterpart in the reference (it sorts on the CPU).
  * keys, sorted_keys and perm are DEVICE arrays of n entries on the current
- * device (keys must not alias an output); the work runs on `stream`
- * (cudaStream_t, NULL = legacy default stream) and the call returns when it
- * is done.  It allocates nothing: its temporaries live in one fixed array
- * compiled into the library (about 2.6 MB, held on every device that loads
- * the library until exit), so n is limited to MPM_NOALLOC_MAX_KEYS; larger n
- * returns MPM_ERR_ARG (use mpm_radix_sort_u32).  The first call on a device
- * looks up that array's address and zeroes it (a synchronous cudaMemset):
- * make that first call before any stream capture.  All calls on a device
- * share the array, so calls that overlap on the GPU race; serialise them. */
+ * device; keys must not alias an output and the two outputs must not alias
+ * each other (MPM_ERR_ARG).  The work runs on `stream` (cudaStream_t, NULL =
+ * legacy default stream) and the call blocks until it is done: it reads back
+ * the sort's timeout flag and returns MPM_ERR_TIMEOUT if a bounded wait gave up.
+ * It allocates nothing: its temporaries live in one fixed array compiled into
+ * the library (about 2.6 MB, held on every device that loads the library until
+ * exit), so n is limited to MPM_NOALLOC_MAX_KEYS; larger n returns MPM_ERR_ARG
+ * (use mpm_radix_sort_u32).  The first call on a device looks up that array's
+ * address and zeroes it (a synchronous cudaMemset): make that first call before
+ * any stream capture.  All calls on a device share the array, so calls that
+ * overlap on the GPU race; serialise them. */
 #define MPM_NOALLOC_MAX_KEYS 262144
 int mpm_radix_sort_u32_noalloc(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm,
                                void* stream);
@@ -510,6 +518,20 @@ int mpm_radix_sort_u32_noalloc(const uint32_t* keys, int64_t n, int bits, uint32
  * and slot permutation of the last sort (host arrays of n entries, NULL-able).
  * Key = (particle block << 6) | cell in block; 0xffffffff = invalid particle. */
 int mpm_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm);
+
+/* Test hooks for the device-side failure paths (no reference counterpart; the
+ * reference's asserts throw, Core/Log/DEBUG_UTILITIES.cpp:95-103):
+ * mpm_debug_sort_stall runs one radix pass over the host keys whose first tile
+ * never runs, so the other tiles' bounded look-back gives up after spin_limit
+ * polls (<= 2^22); returns MPM_ERR_TIMEOUT when it did (2 to 2^21/1024 tiles of
+ * 1024 keys).  mpm_debug_set_sort_epoch seeds the epoch word of a fast-path
+ * handle's sort scratch (sorts across the wrap of its 30-bit field).
+ * mpm_debug_set_svd_iterations bounds the FP64 3x3 SVD's QR sweeps on the
+ * current device (default 64); a particle whose SVD does not converge within
+ * the bound sets MPM_ERR_NOT_CONVERGED. */
+int mpm_debug_sort_stall(const uint32_t* keys, int64_t n, int bits, uint32_t spin_limit);
+int mpm_debug_set_sort_epoch(mpm_handle* h, uint32_t epoch);
+int mpm_debug_set_svd_iterations(int max_it);
 
 /* Human-readable text of the last error on this handle / of a status code. */
 int mpm_last_error(mpm_handle* h, char* buf, int len);

@@ -52,9 +52,20 @@ def build(force: bool = False) -> str:
     return LIB
 
 
-def build_ref(ref_root: str = "/root/reference", jobs: int = os.cpu_count() or 8) -> bool:
+def reference_root():
+    """The PhysBAM checkout: $PHYSBAM_REFERENCE, else a directory named
+    ``reference`` beside this repository; None when neither holds Public_Library."""
+    cands = [os.environ.get("PHYSBAM_REFERENCE"), os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")]
+    for c in cands:
+        if c and os.path.isdir(os.path.join(c, "Public_Library")):
+            return c
+    return None
+
+
+def build_ref(ref_root: str = None, jobs: int = os.cpu_count() or 8) -> bool:
     """Compile the reference's MPM path from its sources (minutes on first run)."""
-    if not os.path.isdir(ref_root):
+    ref_root = ref_root or reference_root()
+    if not ref_root or not os.path.isdir(ref_root):
         return os.path.exists(REF_SCENE)
     subprocess.check_call(["make", "-f", os.path.join(HERE, "ref.mk"), "-j%d" % jobs, "REF=" + ref_root,
                            "OUT=" + REF_DIR], cwd=os.path.dirname(HERE))

@@ -2,12 +2,13 @@
 # into oracle/_ref/ so that tests can pin the CPU restatement against it.
 # Test infrastructure only: nothing in the product links or loads this.
 #
-#   make -f oracle/ref.mk -j8 REF=/root/reference
+#   make -f oracle/ref.mk -j8 REF=<PhysBAM checkout>
 #
 # Only the library layers the explicit MPM driver links against are compiled.
 # Four sources are skipped: they need boost or cblas, which are absent, or do
 # not compile with g++ 13 (a pointer comparison); none is on the MPM path.
-REF ?= /root/reference
+REF ?= $(PHYSBAM_REFERENCE)
+$(if $(REF),,$(error set REF (or PHYSBAM_REFERENCE) to the PhysBAM checkout))
 OUT ?= $(dir $(lastword $(MAKEFILE_LIST)))_ref
 PL  := $(REF)/Public_Library
 LAYERS := Core Tools Grid_Tools Grid_PDE Geometry Rigids Deformables Solids Hybrid_Methods

@@ -615,3 +615,6 @@ int diff_backward(mpm_handle* h, const mpm_particles_view* gout, mpm_particles_v
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
 }
+
+// This module's copy of the SVD sweep bound (mpm_debug_set_svd_iterations).
+MPM_SVD_LIMIT_SETTER(svd_limit_adjoint)

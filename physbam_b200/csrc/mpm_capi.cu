@@ -485,7 +485,16 @@ int mpm_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf)
 {
     if(!h) return MPM_ERR_ARG;
     if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
-    return fast(h) ? fast_get_grid(h, m, v0, v, vf) : plain_get_grid(h, m, v0, v, vf);
+    if(fast(h) && h->fast.nscenes != 1) return set_error(h, MPM_ERR_ARG, "a batch returns its grids per scene: mpm_batch_get_grid");
+    return fast(h) ? fast_get_grid(h, 0, m, v0, v, vf) : plain_get_grid(h, m, v0, v, vf);
+}
+
+int mpm_batch_get_grid(mpm_handle* h, int scene, double* m, double* v, double* vf)
+{
+    if(!h) return MPM_ERR_ARG;
+    if(!fast(h)) return set_error(h, MPM_ERR_ARG, "grids per scene belong to fast-path handles");
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    return fast_get_grid(h, scene, m, nullptr, v, vf);
 }
 
 int mpm_count_valid(mpm_handle* h, int64_t* count)
@@ -580,6 +589,28 @@ int mpm_diff_backward(mpm_handle* h, const mpm_particles_view* grad_final, mpm_p
 int mpm_radix_sort_u32(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_keys, uint32_t* perm)
 {
     return radix_sort_host(keys, n, bits, sorted_keys, perm);
+}
+
+int mpm_debug_sort_stall(const uint32_t* keys, int64_t n, int bits, uint32_t spin_limit)
+{
+    return debug_sort_stall(keys, n, bits, spin_limit);
+}
+
+int mpm_debug_set_sort_epoch(mpm_handle* h, uint32_t epoch)
+{
+    if(!h) return MPM_ERR_ARG;
+    if(!fast(h)) return set_error(h, MPM_ERR_ARG, "the sort scratch exists on the fast path only");
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    return debug_set_sort_epoch(h, epoch);
+}
+
+int mpm_debug_set_svd_iterations(int max_it)
+{
+    if(max_it < 0 || max_it > 1000000) return MPM_ERR_ARG;
+    cudaError_t (*set[])(int) = {svd_limit_plain, svd_limit_adjoint, svd_limit_implicit, svd_limit_fast, svd_limit_capi};
+    for(auto f: set)
+        if(f(max_it) != cudaSuccess) return MPM_ERR_CUDA;
+    return MPM_OK;
 }
 
 int mpm_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm)
@@ -902,3 +933,6 @@ int mpm_get_timing(mpm_handle* h, char* names, int names_len, double* ms, int64_
 }
 
 }  // extern "C"
+
+// This module's copy of the SVD sweep bound (mpm_debug_set_svd_iterations).
+MPM_SVD_LIMIT_SETTER(svd_limit_capi)

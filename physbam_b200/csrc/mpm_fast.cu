@@ -1465,11 +1465,14 @@ template<class T> __global__ void k_plastic_in(int64_t n, int64_t npad, float* P
     }
 }
 
-// Grids of scene 0 in the reference's ghosted layout (single-scene handles).
-__global__ void k_grid_out(FastArgs a, const uint32_t* list, uint32_t count, double* m, double* v, double* vf, int G0, int G1, int G2)
+// Grids of scene `s` in the reference's ghosted layout: the node blocks of the
+// last substep's list that belong to the scene.
+__global__ void k_grid_out(FastArgs a, const uint32_t* list, uint32_t count, int s, double* m, double* v, double* vf,
+    int G0, int G1, int G2)
 {
-    const SceneDev& sc = a.scenes[0];
+    const SceneDev& sc = a.scenes[s];
     for(uint32_t w = blockIdx.x; w < count; w += gridDim.x) {
+        if(a.nb_scene[list[w]] != s) continue;
         uint32_t nb = list[w] - sc.nb_base;
         int nz = nb % sc.NN[2], r = nb / sc.NN[2], ny = r % sc.NN[1], nx = r / sc.NN[1];
         int t = threadIdx.x;
@@ -2104,14 +2107,14 @@ int fast_g2p(mpm_handle* h, double dt, double)
     return MPM_OK;
 }
 
-int fast_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf)
+int fast_get_grid(mpm_handle* h, int scene, double* m, double* v0, double* v, double* vf)
 {
     FastState& f = h->fast;
     if(v0) return set_error(h, MPM_ERR_ARG, "velocity after P2G is not kept on the fast path");
-    if(f.nscenes != 1) return set_error(h, MPM_ERR_ARG, "grids are returned for single-scene handles");
+    if(scene < 0 || scene >= f.nscenes) return set_error(h, MPM_ERR_ARG, "scene index");
     int G[3];
     int64_t gn = 1;
-    for(int k = 0; k < 3; k++) { G[k] = h->sp.counts[k] + 2 * MPM_GHOST; gn *= G[k]; }
+    for(int k = 0; k < 3; k++) { G[k] = f.scenes_h[scene].counts[k] + 2 * MPM_GHOST; gn *= G[k]; }
     uint32_t count = 0;
     MPM_CUDA(h, cudaMemcpyAsync(&count, f.counters + CNT_NODE_BLOCKS, sizeof(count), cudaMemcpyDeviceToHost, h->stream));
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -2121,7 +2124,7 @@ int fast_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf)
     if(vf) { MPM_CUDA(h, cudaMallocAsync((void**)&dvf, gn * 24, h->stream)); MPM_CUDA(h, cudaMemsetAsync(dvf, 0, gn * 24, h->stream)); }
     FastArgs a = make_args(h, 0.0);
     if(count) {
-        k_grid_out<<<count < 65535u ? count : 65535u, 64, 0, h->stream>>>(a, f.nb_list, count, dm, dv, dvf, G[0], G[1], G[2]);
+        k_grid_out<<<count < 65535u ? count : 65535u, 64, 0, h->stream>>>(a, f.nb_list, count, scene, dm, dv, dvf, G[0], G[1], G[2]);
         MPM_LAUNCHED(h, "k_grid_out");
     }
     if(m) { MPM_CUDA(h, cudaMemcpyAsync(m, dm, gn * 8, cudaMemcpyDeviceToHost, h->stream)); MPM_CUDA(h, cudaFreeAsync(dm, h->stream)); }
@@ -2320,17 +2323,65 @@ int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_
     return rc;
 }
 
+// A sort pass whose first tile never runs: the pass's ticket counter starts at
+// 1 and one CTA fewer than the tiles is launched, so every tile's look-back
+// reaches tile 0, which never publishes, and gives up after `spin_limit` polls.
+// Every output position stays inside [0, n): a tile that gave up misses tile
+// 0's counts, which only lowers its positions.  Test hook for the timeout path.
+int debug_sort_stall(const uint32_t* keys, int64_t n, int bits, uint32_t spin_limit)
+{
+    const int64_t tiles = mpm_sort::tiles_for(n, mpm_sort::kSmallTile);
+    if(!keys || bits < 1 || bits > 32 || tiles < 2 || n > mpm_sort::kSmallSortMax || spin_limit > (1u << 22))
+        return MPM_ERR_ARG;
+    cudaStream_t st;
+    if(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return MPM_ERR_CUDA;
+    uint32_t *k = nullptr, *ko = nullptr, *vo = nullptr, *scratch = nullptr;
+    unsigned* flags = nullptr;
+    const size_t b = n * sizeof(uint32_t), sw = mpm_sort::scratch_words(n) * sizeof(uint32_t);
+    int rc = MPM_OK;
+    if(cudaMalloc(&k, b) || cudaMalloc(&ko, b) || cudaMalloc(&vo, b) || cudaMalloc(&scratch, sw) ||
+       cudaMalloc(&flags, sizeof(unsigned))) rc = MPM_ERR_NOMEM;
+    if(!rc && (cudaMemsetAsync(scratch, 0, sw, st) || cudaMemsetAsync(flags, 0, sizeof(unsigned), st) ||
+               mpm_sort::prepare() || cudaMemcpyAsync(k, keys, b, cudaMemcpyHostToDevice, st))) rc = MPM_ERR_CUDA;
+    if(!rc) {
+        mpm_sort::k_upfront_hist<<<1, mpm_sort::kThreads, 0, st>>>(k, n, bits, scratch);   // epoch 1, tickets 0
+        const uint32_t one = 1;
+        cudaMemcpyAsync(scratch + mpm_sort::kTicketOff, &one, sizeof one, cudaMemcpyHostToDevice, st);
+        mpm_sort::k_onesweep<mpm_sort::kSmallItems><<<(unsigned)(tiles - 1), mpm_sort::kThreads,
+            mpm_sort::pass_smem<mpm_sort::kSmallItems>(), st>>>(k, nullptr, ko, vo, n, bits, 0, tiles, scratch, flags,
+                                                                MPM_FLAG_TIMEOUT, spin_limit);
+        unsigned fl = 0;
+        cudaMemcpyAsync(&fl, flags, sizeof fl, cudaMemcpyDeviceToHost, st);
+        if(cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = MPM_ERR_CUDA;
+        else if(fl & MPM_FLAG_TIMEOUT) rc = MPM_ERR_TIMEOUT;
+    }
+    cudaFree(k); cudaFree(ko); cudaFree(vo); cudaFree(scratch); cudaFree(flags);
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+// Seed the epoch word of the handle's sort scratch (test hook: sorts across
+// the 2^30 wrap of the status words' epoch field).
+int debug_set_sort_epoch(mpm_handle* h, uint32_t epoch)
+{
+    FastState& f = h->fast;
+    if(!f.sort_scratch) return set_error(h, MPM_ERR_STATE, "no sort scratch");
+    MPM_CUDA(h, cudaMemcpyAsync(f.sort_scratch + mpm_sort::kEpochOff, &epoch, sizeof epoch, cudaMemcpyHostToDevice, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Radix sort without any allocation.
 //
-// Some callers cannot allocate device memory when they need to sort: code
-// recorded into a CUDA graph by stream capture (an allocation would either be
-// illegal there or become part of the graph), hosts that give this library a
-// fixed memory budget up front and forbid growth afterwards, and loops with
-// latency limits that cannot absorb cudaMalloc / cudaFree and the device-wide
-// synchronisation cudaFree implies.  mpm_radix_sort_u32_noalloc serves them:
-// the caller passes device arrays for the keys and both outputs, and every
-// temporary the sort needs lives in one fixed array compiled into this file.
+// Some callers cannot allocate device memory when they need to sort: hosts
+// that give this library a fixed memory budget up front and forbid growth
+// afterwards, and loops with latency limits that cannot absorb cudaMalloc /
+// cudaFree and the device-wide synchronisation cudaFree implies.
+// mpm_radix_sort_u32_noalloc serves them: the caller passes device arrays for
+// the keys and both outputs, and every temporary the sort needs lives in one
+// fixed array compiled into this file.  The call blocks until the sort is
+// done (it reads back the timeout flag of the sort's bounded waits).
 //
 // The array is a file-scope __device__ variable, so every GPU that loads the
 // library holds it (about 2.6 MB) until the process exits, whether or not the
@@ -2378,7 +2429,7 @@ extern "C" int mpm_radix_sort_u32_noalloc(const uint32_t* keys, int64_t n, int b
     if(n < 0 || bits < 1 || bits > 32) return MPM_ERR_ARG;
     if(n > kNoAllocMaxKeys) return MPM_ERR_ARG;     // beyond the fixed scratch: use mpm_radix_sort_u32
     if(n == 0) return MPM_OK;
-    if(!keys || !sorted_keys || !perm || keys == sorted_keys || keys == perm) return MPM_ERR_ARG;
+    if(!keys || !sorted_keys || !perm || keys == sorted_keys || keys == perm || sorted_keys == perm) return MPM_ERR_ARG;
     int dev = 0;
     if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return MPM_ERR_CUDA;
     uint32_t* base = nullptr;
@@ -2538,3 +2589,6 @@ int fast_grid_totals(mpm_handle* h, mpm_totals* out)
     cudaFreeAsync(d, h->stream);
     return rc;
 }
+
+// This module's copy of the SVD sweep bound (mpm_debug_set_svd_iterations).
+MPM_SVD_LIMIT_SETTER(svd_limit_fast)

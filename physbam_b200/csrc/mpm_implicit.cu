@@ -1033,3 +1033,6 @@ int plain_implicit_forces(mpm_handle* h, double dt, double)
 {
     return h->model.precision == MPM_FP64 ? implicit_t<double>(h, dt) : implicit_t<float>(h, dt);
 }
+
+// This module's copy of the SVD sweep bound (mpm_debug_set_svd_iterations).
+MPM_SVD_LIMIT_SETTER(svd_limit_implicit)

@@ -203,7 +203,15 @@ int fast_get_particles(mpm_handle* h, mpm_particles_view* v);
 int fast_p2g(mpm_handle* h, double dt, double time);
 int fast_forces(mpm_handle* h, double dt, double time);
 int fast_g2p(mpm_handle* h, double dt, double time);
-int fast_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf);
+int fast_get_grid(mpm_handle* h, int scene, double* m, double* v0, double* v, double* vf);
+// Each compiled module's copy of the SVD sweep bound (mpm_math.cuh, g_svd_max_it).
+cudaError_t svd_limit_plain(int v);
+cudaError_t svd_limit_adjoint(int v);
+cudaError_t svd_limit_implicit(int v);
+cudaError_t svd_limit_fast(int v);
+cudaError_t svd_limit_capi(int v);
+int debug_sort_stall(const uint32_t* keys, int64_t n, int bits, uint32_t spin_limit);
+int debug_set_sort_epoch(mpm_handle* h, uint32_t epoch);
 int fast_count_valid(mpm_handle* h, int64_t* c);
 int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_keys, uint32_t* perm);
 int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, const mpm_collision_object* objs, int nobjs);

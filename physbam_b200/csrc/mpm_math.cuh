@@ -225,10 +225,19 @@ template<class T> __device__ bool lazy_sort(T* U, T* B, T* V, int i, int j)
     return true;
 }
 
+// The bound on svd3's sweeps (the reference iterates without bound; a bounded
+// loop keeps the GPU safe).  One device variable per compiled module, set on
+// the current device through mpm_debug_set_svd_iterations, a test hook that
+// makes the non-convergence flag reachable.
+static __device__ int g_svd_max_it = 64;
+#define MPM_SVD_LIMIT_SETTER(name) \
+    cudaError_t name(int v) { return cudaMemcpyToSymbol(mpm::g_svd_max_it, &v, sizeof v); }
+
 // Returns false when the iteration did not converge within max_it sweeps
-// (the reference iterates without bound; a bounded loop keeps the GPU safe).
-template<class T> __device__ bool svd3(const T* F, T* U, T* D, T* V, int max_it = 64)
+// (g_svd_max_it when max_it < 0).
+template<class T> __device__ bool svd3(const T* F, T* U, T* D, T* V, int max_it = -1)
 {
+    if(max_it < 0) max_it = g_svd_max_it;
     T B[9];
 #pragma unroll
     for(int i = 0; i < 9; i++) { B[i] = F[i]; U[i] = V[i] = (i % 4 == 0) ? (T)1 : (T)0; }

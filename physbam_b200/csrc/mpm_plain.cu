@@ -1168,3 +1168,6 @@ static int plain_totals(mpm_handle* h, bool grid, mpm_totals* out)
 
 int plain_particle_totals(mpm_handle* h, mpm_totals* out) { return plain_totals(h, false, out); }
 int plain_grid_totals(mpm_handle* h, mpm_totals* out) { return plain_totals(h, true, out); }
+
+// This module's copy of the SVD sweep bound (mpm_debug_set_svd_iterations).
+MPM_SVD_LIMIT_SETTER(svd_limit_plain)

@@ -42,6 +42,9 @@ constexpr int kRadix = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxPasses = 4;
 constexpr uint32_t kSpinLimit = 1u << 22;
+// Status words keep the epoch in their top 30 bits; the epoch counter itself
+// is a 32-bit word, so it is compared modulo 2^30 on both sides.
+constexpr uint32_t kEpochMask = (1u << 30) - 1u;
 
 constexpr uint64_t kFlagAggregate = 1;
 constexpr uint64_t kFlagInclusive = 2;
@@ -199,7 +202,7 @@ template<int ITEMS> struct PassSmem {
 template<int ITEMS>
 __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int bits, int pass, int64_t tiles,
-    uint32_t* __restrict__ scratch, unsigned* __restrict__ err_flags, unsigned timeout_flag)
+    uint32_t* __restrict__ scratch, unsigned* __restrict__ err_flags, unsigned timeout_flag, uint32_t spin_limit)
 {
     constexpr int kItems = ITEMS, kTile = kThreads * ITEMS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -211,7 +214,7 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
     if(threadIdx.x == 0) S.tile = atomicAdd(&scratch[kTicketOff + pass], 1u);
     __syncthreads();
     const uint32_t tile = S.tile;
-    const uint64_t epoch = scratch[kEpochOff];
+    const uint64_t epoch = scratch[kEpochOff] & kEpochMask;
     uint64_t* status = reinterpret_cast<uint64_t*>(scratch + kStatusOff) + (int64_t)pass * tiles * kRadix;
 
     const int64_t base = (int64_t)tile * kTile;
@@ -282,7 +285,7 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const uint32_t* __restric
                 if(flag == kFlagInclusive) { done = true; stop = true; }
             }
             if(done) break;
-            if(adv == 0 && ++spins > kSpinLimit) { atomicOr(err_flags, timeout_flag); break; }
+            if(adv == 0 && ++spins > spin_limit) { atomicOr(err_flags, timeout_flag); break; }
             j -= adv;
         }
         mine.store((epoch << 34) | (kFlagInclusive << 32) | (excl + tot), cuda::memory_order_relaxed);
@@ -358,10 +361,10 @@ inline cudaError_t radix_sort(const uint32_t* keys, uint32_t* keys_out, uint32_t
         uint32_t* vo = last_to_out ? vals_out : vals_alt;
         if(small)
             k_onesweep<kSmallItems><<<(unsigned)tiles, kThreads, pass_smem<kSmallItems>(), st>>>(
-                kin, vin, ko, vo, n, bits, p, tiles, scratch, err_flags, timeout_flag);
+                kin, vin, ko, vo, n, bits, p, tiles, scratch, err_flags, timeout_flag, kSpinLimit);
         else
             k_onesweep<kItems><<<(unsigned)tiles, kThreads, pass_smem<kItems>(), st>>>(
-                kin, vin, ko, vo, n, bits, p, tiles, scratch, err_flags, timeout_flag);
+                kin, vin, ko, vo, n, bits, p, tiles, scratch, err_flags, timeout_flag, kSpinLimit);
         kin = ko;
         vin = vo;
     }

@@ -126,7 +126,8 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state", "mpm_set_implicit",
            "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt",
            "mpm_set_reflection", "mpm_set_penalty_objects", "mpm_set_object_motion", "mpm_set_particle_models",
-           "mpm_set_plastic_particles"]
+           "mpm_set_plastic_particles", "mpm_batch_get_grid", "mpm_debug_sort_stall", "mpm_debug_set_sort_epoch",
+           "mpm_debug_set_svd_iterations"]
 
 _lib = None
 
@@ -152,6 +153,10 @@ def load_library(path: str = LIB_PATH):
     L.mpm_advance.argtypes = [P, ctypes.c_double, ctypes.c_double, ctypes.c_int]
     L.mpm_synchronize.argtypes = [P]
     L.mpm_get_grid.argtypes = [P, P, P, P, P]
+    L.mpm_batch_get_grid.argtypes = [P, ctypes.c_int, P, P, P]
+    L.mpm_debug_sort_stall.argtypes = [P, ctypes.c_int64, ctypes.c_int, ctypes.c_uint32]
+    L.mpm_debug_set_sort_epoch.argtypes = [P, ctypes.c_uint32]
+    L.mpm_debug_set_svd_iterations.argtypes = [ctypes.c_int]
     L.mpm_count_valid.argtypes = [P, ctypes.POINTER(ctypes.c_int64)]
     L.mpm_set_timing.argtypes = [P, ctypes.c_int]
     L.mpm_get_timing.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -796,5 +801,14 @@ class MPM_BATCH(MPM_DRIVER):
 
     def split(self, arrays):
         return [{k: v[self.offsets[i]:self.offsets[i + 1]] for k, v in arrays.items()} for i in range(len(self.scenes))]
+
+    def get_scene_grid(self, i):
+        """Scene i's ghosted grid of the last substep (mpm_batch_get_grid): mass, velocity, friction velocity."""
+        s = self.scenes[i]
+        shape = tuple(c + 2 * S.GHOST for c in s.counts[:3])
+        gn = int(np.prod(shape))
+        m, v, vf = np.zeros(gn), np.zeros(gn * 3), np.zeros(gn * 3)
+        self._check(self.L.mpm_batch_get_grid(self.h, int(i), _ptr(m), _ptr(v), _ptr(vf)), "mpm_batch_get_grid")
+        return {"grid_m": m.reshape(shape), "grid_v": v.reshape(shape + (3,)), "grid_vf": vf.reshape(shape + (3,))}
 
 

@@ -1,10 +1,13 @@
 """GPU tests of the batched path (mpm_batch_create): many independent scenes,
-different grid sizes and models, advanced by one persistent launch per phase.
-Each scene of the batch must evolve exactly as it does alone (FP32 tolerance:
-atomic summation order is the only difference)."""
+different grid sizes and models, advanced together.  Each scene of the batch
+is checked against the FP64 oracle (oracle/mpm_oracle.c, itself pinned to the
+reference's dumps) run on that scene alone, at the FP32 path's tolerances; the
+full-size batch scenes are pinned to the reference's own build in
+test_gpu_baseline_parity.py."""
 import numpy as np
 import pytest
 
+import oracle
 from physbam_b200 import scenes as S
 
 pytestmark = pytest.mark.gpu
@@ -31,15 +34,13 @@ def test_batch_matches_individual_scenes(cuda_device):
     got = batch.split(batch.get_particles())
     batch.close()
     for s, g in zip(scenes, got):
-        drv = D.MPM_DRIVER(s)
-        drv.set_scene_particles(s)
-        drv.advance(nsteps)
-        ref = drv.get_particles()
-        drv.close()
-        np.testing.assert_array_equal(g["valid"], ref["valid"])
-        ex = np.max(np.abs(g["X"] - ref["X"]))
-        ef = np.max(np.abs(g["F"] - ref["F"]))
-        assert ex < 1e-6 and ef < 1e-4, (s.name, s.counts, ex, ef)
+        st = oracle.State(s)
+        oracle.run(st, nsteps)
+        np.testing.assert_array_equal(g["valid"], st.valid.astype(bool))
+        ex = np.max(np.abs(g["X"] - st.X))
+        ef = np.max(np.abs(g["F"] - st.F_rowmajor()))
+        ev = np.max(np.abs(g["V"] - st.V)) / max(np.max(np.abs(st.V)), 1e-12)
+        assert ex < 2e-6 and ef < 1e-4 and ev < 2e-3, (s.name, s.counts, ex, ef, ev)
 
 
 @pytest.mark.parametrize("cold", [False, True])

@@ -121,21 +121,28 @@ def test_fast_matches_plain(cuda_device):
 
 @pytest.mark.parametrize("path", ["plain", "fast"])
 def test_advance_with_moving_objects(cuda_device, path):
-    """mpm_advance over moving objects (run eagerly, a frame per substep) gives
-    the substep-by-substep result."""
-    s = S.small_3d_moving(nsteps=12)
+    """mpm_advance over moving objects (every substep's frames evaluated into a
+    device table first, then the captured graph replayed, its first kernel taking
+    the next table slot) gives the substep-by-substep result: one advance of 12,
+    and advance(5) then advance(12) (a second replay, whose slot counter the table
+    upload resets, then a longer table: regrow, new capture) against 17 eager
+    substeps."""
+    s = S.small_3d_moving(nsteps=17)
     p, prec = PATHS[path]()
-    out = []
-    for batched in (False, True):
-        drv = D().MPM_DRIVER(s, precision=prec, path=p)
-        drv.set_scene_particles(s)
-        if batched:
-            drv.advance(12)
-        else:
-            for _ in range(12):
-                drv.Advance_One_Time_Step()
-        out.append(drv.get_particles())
-        drv.close()
     tol = 1e-12 if path == "plain" else 1e-5
-    for k in ("X", "V", "F"):
-        assert rel(out[1][k], out[0][k], 1.0) < tol, k
+    for plan in ([12], [5, 12]):
+        total = sum(plan)
+        out = []
+        for batched in (False, True):
+            drv = D().MPM_DRIVER(s, precision=prec, path=p)
+            drv.set_scene_particles(s)
+            if batched:
+                for k in plan:
+                    drv.advance(k)
+            else:
+                for _ in range(total):
+                    drv.Advance_One_Time_Step()
+            out.append(drv.get_particles())
+            drv.close()
+        for k in ("X", "V", "F"):
+            assert rel(out[1][k], out[0][k], 1.0) < tol, (plan, k)
