@@ -841,9 +841,48 @@ template<class T, int d, class O> __device__ T penalty_particle(const O* objs, i
 //
 // In: v0 (grid velocity after P2G), dv (dt/m f), node centre X0.
 // Out: vnew (velocity), vfric (velocity_friction_save).
+//
+// FP32 state: the reference's projection moves the node to X = X0 + dt V,
+// projects X and takes V = (X - X0) / dt, which in FP32 keeps only a few bits
+// of V once |dt V| is far below |X0| (dt 2e-5 and |X0| ~ 1 quantise V to
+// ~3e-3 m/s).  So with T = float, a node that may touch an object during the
+// substep is collided in FP64 (the same formulas, exact inputs promoted);
+// a static object whose signed distance at the node exceeds dt |V| plus the
+// FP32 rounding of that distance is out of reach, as the FP64 test decides
+// too (signed distances are 1-Lipschitz), and a node out of every object's
+// reach keeps V.
 template<class T, int d, class O, class S = double> __device__ void collide_node(const O* objs, int nobj, const T* X0,
     const T* v0, T* dv, T dt, T* vnew, T* vfric, const ObjMotionT<S>* mo = nullptr, unsigned moving = 0)
 {
+    if constexpr(sizeof(T) == 4) {
+        T speed = 0, xmax = 1;
+#pragma unroll
+        for(int a = 0; a < d; a++) {
+            const T va = v0[a] + dv[a];
+            speed += va * va;
+            xmax = fmaxf(xmax, fabsf(X0[a]));
+        }
+        const T step = dt * sqrtf(speed);
+        bool near = false;
+        for(int j = 0; j < nobj && !near; j++) {
+            T scale = xmax;
+#pragma unroll
+            for(int a = 0; a < 3; a++) scale = fmaxf(scale, fmaxf(fabsf((T)objs[j].a[a]), fabsf((T)objs[j].b[a])));
+            near = (mo && ((moving >> j) & 1u)) || !(object_phi<T, d>(objs[j], X0) > step + (T)64 * FLT_EPSILON * scale);
+        }
+        if(!near) {
+#pragma unroll
+            for(int a = 0; a < d; a++) vnew[a] = vfric[a] = v0[a] + dv[a];
+            return;
+        }
+        double X0d[3] = {0, 0, 0}, v0d[3] = {0, 0, 0}, dvd[3] = {0, 0, 0}, vnd[3], vfd[3];
+#pragma unroll
+        for(int a = 0; a < d; a++) { X0d[a] = X0[a]; v0d[a] = v0[a]; dvd[a] = dv[a]; }
+        collide_node<double, d, O, S>(objs, nobj, X0d, v0d, dvd, (double)dt, vnd, vfd, mo, moving);
+#pragma unroll
+        for(int a = 0; a < d; a++) { dv[a] = (T)dvd[a]; vnew[a] = (T)vnd[a]; vfric[a] = (T)vfd[a]; }
+        return;
+    }
     T dvb[3], nrm[MPM_MAX_OBJECTS][3], sv[3] = {0, 0, 0};
     int cobj[MPM_MAX_OBJECTS];
     int ncol = 0;

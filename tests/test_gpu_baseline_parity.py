@@ -13,7 +13,9 @@ V, F over the particles, of the node masses and of the node momenta after the
 grid update (mass x velocity) over the ghosted grid.
 
 Bounds: positions 1e-4 (the precision target of the FP32 path); the others are
-set a few times above what the FP32 path measures, so a regression shows.
+set a few times above what the FP32 path measures (V, F up to 1.2e-5; node
+mass and momentum up to 1e-4, which is the particles' position error carried
+through the weights' slope 1/dx), so a regression shows.
 """
 import json
 import os
@@ -27,7 +29,7 @@ from oracle import parity
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not oracle.ref_available(), reason="the reference build oracle/_ref is absent")]
 
-BOUNDS = {"X": 1e-4, "V": 1e-2, "F": 1e-4, "grid_m": 1e-4, "grid_mv": 1e-2}
+BOUNDS = {"X": 1e-4, "V": 1e-4, "F": 1e-4, "grid_m": 3e-4, "grid_mv": 3e-4}
 
 
 def _record(name, table):
