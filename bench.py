@@ -175,15 +175,9 @@ def cpu_baseline_sample(scene, seconds_budget=20.0):
 
 
 def kernels_per_substep(scene, p2g_variant=0):
-    """Our kernels launched per fast-path substep: the digit histograms, one
-    single-pass kernel per radix digit, ranges (+ invalid tail), p2g, grid, g2p."""
-    blocks = 1
-    for c in scene.counts:
-        blocks *= (c + 4 + 3) // 4
-    bits = 6
-    while (1 << bits) <= blocks * 64:
-        bits += 1
-    return (bits + 7) // 8 + 5
+    """Our kernels launched per fast-path substep: the block scan (k_bins), the
+    routing of the slots (k_route), P2G, the grid update and G2P."""
+    return 5
 
 
 def read_traffic(kernel, workload=WORKLOAD):

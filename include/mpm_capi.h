@@ -375,6 +375,18 @@ int mpm_set_plastic_particles(mpm_handle* h, const uint8_t* mask, int64_t n);
  * Any pointer may be NULL. */
 int mpm_get_grid(mpm_handle* h, double* mass, double* v0, double* v, double* vfric);
 
+/* Extra node forces for the next grid update: the Add_Forces of a force this
+ * library does not model (PARTICLE_GRID_FORCES::Add_Forces,
+ * Hybrid_Methods/Forces/PARTICLE_GRID_FORCES.h:17-36; MPM_EXAMPLE::Add_Forces
+ * sums every force's, MPM_EXAMPLE.cpp:115-153), evaluated by the caller.
+ * `force` holds d values per node of the ghosted grid ((G+6)^d nodes, last
+ * index fastest: the layout of MPM_EXAMPLE's ARRAY<TV,TV_INT>), float or
+ * double (dtype), host or device pointer (on_device).  Call between
+ * mpm_particle_to_grid and mpm_apply_forces; that grid update adds the force
+ * at every node with mass (dv = dt f / m), dt being the step it takes.  Calls
+ * add up.  Single-scene handles, explicit substep. */
+int mpm_add_grid_forces(mpm_handle* h, double dt, const void* force, int dtype, int on_device);
+
 /* Number of valid particles (MPM_EXAMPLE::simulated_particles.m). */
 int mpm_count_valid(mpm_handle* h, int64_t* count);
 
@@ -453,13 +465,14 @@ int mpm_autotune_ex(mpm_handle* h, double dt, int substeps, int flags, char* rep
 
 /* The fast path's launch shape, as mpm_autotune chooses it (no reference
  * counterpart: the reference's OpenMP loops have no launch configuration).
- * p2g_variant: MPM_P2G_CELLS (one thread per cell), MPM_P2G_INTERLEAVED (one
- * thread per particle), MPM_P2G_PAIRS (two threads per range of particles,
- * splitting the node quantities), MPM_P2G_PAIRX (as PAIRS, the two threads
- * also splitting the per-particle work);
+ * p2g_variant: MPM_P2G_GROUPS128 / MPM_P2G_GROUPS256 (groups of 4 lanes
+ * accumulating a cell's node values in registers, 128 or 256 threads, work
+ * items of up to 512 / 1024 particles of a block), MPM_P2G_FIXED128 /
+ * MPM_P2G_FIXED256 (one thread per particle into a fixed-point shared tile,
+ * work items of up to 128 / 256 particles); G2P takes the same work items;
  * g2p_threads: 64, 128 or 256 per CTA; cta_mult: 1 or 2 times the resident
  * CTAs per SM. */
-enum { MPM_P2G_CELLS = 0, MPM_P2G_INTERLEAVED = 1, MPM_P2G_PAIRS = 2, MPM_P2G_PAIRX = 3 };
+enum { MPM_P2G_GROUPS128 = 0, MPM_P2G_GROUPS256 = 1, MPM_P2G_FIXED128 = 2, MPM_P2G_FIXED256 = 3 };
 int mpm_set_launch_shape(mpm_handle* h, int p2g_variant, int g2p_threads, int cta_mult);
 int mpm_get_launch_shape(mpm_handle* h, int* p2g_variant, int* g2p_threads, int* cta_mult);
 

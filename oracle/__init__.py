@@ -291,6 +291,39 @@ def ref_available() -> bool:
     return os.path.exists(REF_SCENE)
 
 
+REF_B200 = os.path.join(REF_DIR, "ref_b200")
+
+
+def b200_binding_available() -> bool:
+    return os.path.exists(REF_B200)
+
+
+def run_b200_binding(scene, use_float: bool = True, per_substep: bool = False):
+    """Run ``scene`` through the reference-side binding (``oracle/ref_b200``: the
+    reference's MPM_EXAMPLE set up from the scene file, its substeps run on the GPU
+    by include/mpm_physbam.hpp).  Returns (state dict with X, V, F, B as (n,3,3)
+    row-major matrices and valid, the runner's JSON report)."""
+    import json
+    from physbam_b200 import scenes as S
+    tmp = tempfile.mkdtemp(prefix="mpmb200_")
+    try:
+        sp, dp = os.path.join(tmp, "scene.bin"), os.path.join(tmp, "dump.bin")
+        S.write_scene(sp, scene, [])
+        cmd = [REF_B200, sp, dp] + (["-float"] if use_float else []) + (["-substeps"] if per_substep else [])
+        out = subprocess.run(cmd, check=True, capture_output=True, text=True)
+        report = json.loads(out.stdout.strip().splitlines()[-1])
+        with open(dp, "rb") as f:
+            n = int(np.frombuffer(f.read(4), np.int32)[0])
+            X = np.frombuffer(f.read(8 * n * 3), np.float64).reshape(n, 3)
+            V = np.frombuffer(f.read(8 * n * 3), np.float64).reshape(n, 3)
+            F = np.swapaxes(np.frombuffer(f.read(8 * n * 9), np.float64).reshape(n, 3, 3), 1, 2)
+            B = np.swapaxes(np.frombuffer(f.read(8 * n * 9), np.float64).reshape(n, 3, 3), 1, 2)
+            valid = np.frombuffer(f.read(n), np.uint8).astype(bool)
+        return {"X": X, "V": V, "F": F, "B": B, "valid": valid}, report
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def run_reference(scene, dumps, threads: int = 1, use_float: bool = False, timing: bool = False, totals=None,
                   output: str = None, restart=None):
     """Run the reference's own driver on ``scene``; return {step: dump} (and timing JSON if asked).

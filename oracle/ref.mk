@@ -22,7 +22,10 @@ CXX := g++
 CXXFLAGS := -std=gnu++14 -O2 -fPIC -fopenmp -DUSE_OPENMP -DNDEBUG -fno-math-errno \
             -fno-signed-zeros -include limits -include functional -fpermissive -w -I$(PL)
 
-all: $(OUT)/libphysbam_ref.so $(OUT)/ref_scene
+HERE := $(dir $(lastword $(MAKEFILE_LIST)))
+MPM_LIB := $(HERE)../physbam_b200/libphysbam_mpm.so
+
+all: $(OUT)/libphysbam_ref.so $(OUT)/ref_scene $(OUT)/ref_b200
 
 $(OUT)/obj/%.o: $(PL)/%.cpp
 	@mkdir -p $(dir $@)
@@ -31,7 +34,12 @@ $(OUT)/obj/%.o: $(PL)/%.cpp
 $(OUT)/libphysbam_ref.so: $(OBJS)
 	$(CXX) -shared -fopenmp -o $@ $^ -lz
 
-$(OUT)/ref_scene: $(dir $(lastword $(MAKEFILE_LIST)))ref_scene.cpp $(OUT)/libphysbam_ref.so
+$(OUT)/ref_scene: $(HERE)ref_scene.cpp $(HERE)ref_scene.h $(OUT)/libphysbam_ref.so
 	$(CXX) $(CXXFLAGS) -o $@ $< -L$(OUT) -lphysbam_ref -Wl,-rpath,'$$ORIGIN' -Wl,--allow-shlib-undefined -lz
+
+# the reference-side binding (include/mpm_physbam.hpp) driving MPM_EXAMPLE scenes on the GPU
+$(OUT)/ref_b200: $(HERE)ref_b200.cpp $(HERE)ref_scene.h $(HERE)../include/mpm_physbam.hpp $(OUT)/libphysbam_ref.so $(MPM_LIB)
+	$(CXX) $(CXXFLAGS) -I$(HERE)../include -o $@ $< -L$(OUT) -lphysbam_ref -L$(dir $(MPM_LIB)) -lphysbam_mpm \
+	    -Wl,-rpath,'$$ORIGIN' -Wl,-rpath,'$$ORIGIN/../../physbam_b200' -Wl,--allow-shlib-undefined -lz
 
 .PHONY: all

@@ -1,5 +1,5 @@
-// Reverse-mode derivative of the explicit substep (3D, no collision objects),
-// written by hand for the plain path's data layout.
+// Reverse-mode derivative of the explicit substep (3D; static frictionless
+// collision objects), written by hand for the plain path's data layout.
 //
 // The reference has no reverse mode; its linearisations of the same maps are
 // MPM_FINITE_ELEMENTS::Add_Hessian_Times (Hybrid_Methods/Forces/
@@ -11,11 +11,18 @@
 // 144-167) and NEO_HOOKEAN (NEO_HOOKEAN.cpp:162ff); it is the Hessian of the
 // energy density, a symmetric operator, so it is its own transpose.
 //
-// Substep (no collisions, v_fric = v_new):
+// Substep (v_fric = v_new without friction):
 //   m_i = sum w m_p,   p_i = sum w m_p (V + B D (Z_i - X)) - dt vol S g,   S = P(F) F^T
-//   v_i = p_i / m_i + dt gravity
+//   u_i = p_i / m_i + dt gravity,   v_i = C_i(u_i)   (collision projection)
 //   V' = sum w v_i,  G = sum v_i g^T,  B' = sum w v_i (Z_i - X)^T,  F' = (I + dt G) F,  X' = X + dt V'
 // with w = w_ip(X), g = dw_ip/dX, Hw = d^2 w_ip / dX^2, D = 4/dx^2.
+// C_i applies the node's collisions in object order (MPM_OBJECTIVE::
+// Test_Add_Collision, System/MPM_OBJECTIVE.cpp:150-183): a slip or
+// separating object moves the node's end point X = X0 + dt u onto its surface,
+// u <- u - (phi / dt) n, phi = Phi(X) - min(Phi(X0), 0), n = grad Phi(X), whose
+// derivative is I - n n^T - phi Hess Phi(X) (symmetric); a sticking static
+// object sets u = 0.  Which objects act is held fixed (the projection is
+// differentiated where it acts), as for any piecewise-smooth map.
 // Adjoint per substep, last to first:
 //   adj_g2p  (per particle; the adjoint of the gather is a scatter to the grid)
 //   adj_grid (per node)
@@ -43,7 +50,8 @@ template<class T> struct AdjArgs {
     const uint8_t* valid;
     const T *mass, *vol, *mu, *lam;
     const T* pft;                   // P F^T of the substep
-    const T *gm, *gv;               // grid mass, velocity after the forces
+    const T *gm, *gv;               // grid mass, velocity after the forces (v_new)
+    const T* gu;                    // grid velocity before the collision projection (u)
     const T *aX1, *aV1, *aB1, *aF1; // adjoints of the substep's outputs
     T *aX0, *aV0, *aB0, *aF0;       // adjoints of its inputs
     T *amu, *alam;                  // accumulated over substeps
@@ -178,19 +186,78 @@ template<class T> __global__ void k_adj_g2p(AdjArgs<T> a)
     for(int k = 0; k < 9; k++) a.aF0[9 * p + k] = Fb[k];
 }
 
+// The adjoint of a node's collision projection C(u): replay the projections
+// to find which objects act and their normals, then apply the transposed
+// (symmetric) derivatives in reverse object order to vb.
+template<class T> __device__ void adj_collide(const AdjArgs<T>& a, int64_t i, const T* u, T* vb)
+{
+    int64_t r = i;
+    int idx[3];
+    for(int k = 2; k >= 0; k--) { idx[k] = (int)(r % a.gs[k]) - MPM_GHOST; r /= a.gs[k]; }
+    T X0[3], v[3], J[MPM_MAX_OBJECTS][6];   // per acting object: symmetric derivative (xx yy zz xy xz yz)
+    bool stick[MPM_MAX_OBJECTS];
+    int ncol = 0;
+    for(int k = 0; k < 3; k++) { X0[k] = (T)a.sp.dmin[k] + ((T)idx[k] + (T).5) * (T)a.sp.dx[k]; v[k] = u[k]; }
+    for(int j = 0; j < a.sp.nobj; j++) {
+        const DevObject& o = a.sp.objs[j];
+        const T phi0 = object_phi<T, 3>(o, X0);
+        if((o.type == MPM_STICK || o.type == MPM_SLIP) && phi0 > 0) continue;
+        T X[3];
+        for(int k = 0; k < 3; k++) X[k] = X0[k] + a.dt * v[k];
+        const T phi = object_phi<T, 3>(o, X) - fmin(phi0, (T)0);
+        if(o.type == MPM_SEPARATE && phi > (T)1e-15) continue;
+        if(o.type != MPM_STICK && phi > (T)FLT_MAX) continue;
+        T n[3], H[9];
+        object_normal<T, 3>(o, X, n);
+        object_hessian<T, 3>(o, X, H);
+        J[ncol][0] = 1 - n[0] * n[0] - phi * H[0];
+        J[ncol][1] = 1 - n[1] * n[1] - phi * H[4];
+        J[ncol][2] = 1 - n[2] * n[2] - phi * H[8];
+        J[ncol][3] = -n[0] * n[1] - phi * H[1];
+        J[ncol][4] = -n[0] * n[2] - phi * H[2];
+        J[ncol][5] = -n[1] * n[2] - phi * H[5];
+        stick[ncol] = o.type == MPM_STICK;
+        ncol++;
+        for(int k = 0; k < 3; k++) v[k] -= phi * n[k] / a.dt;
+        if(o.type == MPM_STICK)
+            for(int k = 0; k < 3; k++) v[k] = 0;   // a static object's velocity
+    }
+    for(int c = ncol - 1; c >= 0; c--) {
+        if(stick[c]) { vb[0] = vb[1] = vb[2] = 0; continue; }
+        const T* M = J[c];
+        const T x = M[0] * vb[0] + M[3] * vb[1] + M[4] * vb[2];
+        const T y = M[3] * vb[0] + M[1] * vb[1] + M[5] * vb[2];
+        const T z = M[4] * vb[0] + M[5] * vb[1] + M[2] * vb[2];
+        vb[0] = x; vb[1] = y; vb[2] = z;
+    }
+}
+
 template<class T> __global__ void k_adj_grid(AdjArgs<T> a)
 {
     for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.gn; i += (int64_t)gridDim.x * blockDim.x) {
         T m = a.gm[i];
         if(m == 0) { a.gma[i] = 0; continue; }
+        T vb[3] = {a.ga[3 * i], a.ga[3 * i + 1], a.ga[3 * i + 2]};
+        const T* u = a.gu + 3 * i;
+        if(a.sp.nobj) adj_collide<T>(a, i, u, vb);
         T im = (T)1 / m, s = 0;
 #pragma unroll
         for(int k = 0; k < 3; k++) {
-            T vb = a.ga[3 * i + k];
-            s += vb * (a.gv[3 * i + k] - a.dt * (T)a.sp.gravity[k]);
-            a.ga[3 * i + k] = vb * im;
+            s += vb[k] * (u[k] - a.dt * (T)a.sp.gravity[k]);
+            a.ga[3 * i + k] = vb[k] * im;
         }
         a.gma[i] = -s * im;
+    }
+}
+
+// The grid velocity before the collision projection, as the grid update forms
+// it: u = v0 + (dt / m) f.
+template<class T> __global__ void k_grid_u(const T* gv0, const T* gf, const T* gm, T dt, int64_t gn, T* u)
+{
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < gn; i += (int64_t)gridDim.x * blockDim.x) {
+        const T m = gm[i];
+        const T s = m != 0 ? dt / m : (T)0;
+        for(int k = 0; k < 3; k++) u[3 * i + k] = gv0[3 * i + k] + s * gf[3 * i + k];
     }
 }
 
@@ -383,7 +450,7 @@ struct DiffTape {
     uint8_t* ckpt_valid = nullptr;
     void* seg = nullptr;             // every states
     uint8_t* seg_valid = nullptr;
-    void *seg_gm = nullptr, *seg_gv = nullptr, *seg_pft = nullptr;
+    void *seg_gm = nullptr, *seg_gv = nullptr, *seg_gu = nullptr, *seg_pft = nullptr;
     void* final_state = nullptr;
     uint8_t* final_valid = nullptr;
     void *adj[2] = {nullptr, nullptr};   // X V F B adjoints, double-buffered
@@ -404,7 +471,7 @@ void diff_free(mpm_handle* h)
 {
     DiffTape* t = tape(h);
     if(!t) return;
-    void* ps[] = {t->ckpt, t->ckpt_valid, t->seg, t->seg_valid, t->seg_gm, t->seg_gv, t->seg_pft, t->final_state,
+    void* ps[] = {t->ckpt, t->ckpt_valid, t->seg, t->seg_valid, t->seg_gm, t->seg_gv, t->seg_gu, t->seg_pft, t->final_state,
                   t->final_valid, t->adj[0], t->adj[1], t->amu, t->alam, t->ga, t->gma};
     for(void* p: ps) cudaFree(p);
     delete t;
@@ -433,7 +500,12 @@ int diff_forward(mpm_handle* h, double dt, int nsteps, int every)
 {
     if(h->model.path != MPM_PATH_PLAIN || h->sp.dim != 3)
         return set_error(h, MPM_ERR_ARG, "the adjoint runs on the 3D plain path");
-    if(h->sp.nobj || h->sp.npen) return set_error(h, MPM_ERR_ARG, "the adjoint does not differentiate collision objects");
+    if(h->sp.npen) return set_error(h, MPM_ERR_ARG, "the adjoint does not differentiate penalty collision objects");
+    if(h->moving) return set_error(h, MPM_ERR_ARG, "the adjoint differentiates static collision objects");
+    for(int j = 0; j < h->sp.nobj; j++)
+        if(h->sp.objs[j].friction != 0)
+            return set_error(h, MPM_ERR_ARG, "the adjoint differentiates frictionless collision objects");
+    if(h->reflect.enabled) return set_error(h, MPM_ERR_ARG, "the adjoint does not differentiate reflection boundaries");
     if(h->plastic.kind) return set_error(h, MPM_ERR_ARG, "the adjoint does not differentiate plasticity");
     if(h->plain.pmodel) return set_error(h, MPM_ERR_ARG, "the adjoint takes one constitutive model");
     if(h->implicit.enabled) return set_error(h, MPM_ERR_ARG, "the adjoint differentiates the explicit substep");
@@ -490,6 +562,7 @@ template<class T> static int backward_t(mpm_handle* h, const void* gX, const voi
         MPM_CUDA(h, cudaMalloc(&t->seg_valid, every * n + 1));
         MPM_CUDA(h, cudaMalloc(&t->seg_gm, every * gn * e));
         MPM_CUDA(h, cudaMalloc(&t->seg_gv, every * gn * 3 * e));
+        MPM_CUDA(h, cudaMalloc(&t->seg_gu, every * gn * 3 * e));
         MPM_CUDA(h, cudaMalloc(&t->seg_pft, every * 9 * n * e + 1));
         for(int k = 0; k < 2; k++) MPM_CUDA(h, cudaMalloc(&t->adj[k], st + 1));
         MPM_CUDA(h, cudaMalloc(&t->amu, n * e + 1));
@@ -519,6 +592,9 @@ template<class T> static int backward_t(mpm_handle* h, const void* gX, const voi
             if((rc = plain_forces(h, t->dt, 0))) return rc;
             MPM_CUDA(h, cudaMemcpyAsync((T*)t->seg_gm + j * gn, s.gm, gn * e, cudaMemcpyDeviceToDevice, h->stream));
             MPM_CUDA(h, cudaMemcpyAsync((T*)t->seg_gv + j * gn * 3, s.gv, gn * 3 * e, cudaMemcpyDeviceToDevice, h->stream));
+            k_grid_u<T><<<blocks_for(h, gn, 256, true), 256, 0, h->stream>>>((const T*)s.gv0, (const T*)s.gf, (const T*)s.gm,
+                                                                           (T)t->dt, gn, (T*)t->seg_gu + j * gn * 3);
+            MPM_LAUNCHED(h, "k_grid_u");
             MPM_CUDA(h, cudaMemcpyAsync((T*)t->seg_pft + j * 9 * n, s.pft, 9 * n * e, cudaMemcpyDeviceToDevice, h->stream));
             if(k + 1 < k1 && (rc = plain_g2p(h, t->dt, 0))) return rc;
         }
@@ -535,6 +611,7 @@ template<class T> static int backward_t(mpm_handle* h, const void* gX, const voi
             a.pft = (const T*)t->seg_pft + j * 9 * n;
             a.gm = (const T*)t->seg_gm + j * gn;
             a.gv = (const T*)t->seg_gv + j * gn * 3;
+            a.gu = (const T*)t->seg_gu + j * gn * 3;
             a.aX1 = a1; a.aV1 = a1 + 3 * n; a.aF1 = a1 + 6 * n; a.aB1 = a1 + 15 * n;
             a.aX0 = a0; a.aV0 = a0 + 3 * n; a.aF0 = a0 + 6 * n; a.aB0 = a0 + 15 * n;
             a.amu = (T*)t->amu; a.alam = (T*)t->alam;

@@ -83,6 +83,7 @@ static int read_flags(mpm_handle* h)
     if(f & MPM_FLAG_DOMAIN) return set_error(h, MPM_ERR_DOMAIN, "particle stencil outside the ghosted grid");
     if(f & MPM_FLAG_TIMEOUT) return set_error(h, MPM_ERR_TIMEOUT, "device wait gave up");
     if(f & MPM_FLAG_NOT_CONVERGED) return set_error(h, MPM_ERR_NOT_CONVERGED, "SVD did not converge");
+    if(f & MPM_FLAG_ORDER) return set_error(h, MPM_ERR_CUDA, "particle order out of step with its block counts");
     return MPM_OK;
 }
 
@@ -229,6 +230,9 @@ static int run_substep(mpm_handle* h, double dt, double time)
 {
     if(h->timing || h->implicit.enabled || (h->moving && !h->motion_from_table) || (!fast(h) && reduces_dt(h)))
         return enqueue_substep(h, dt, time);
+    // the fast path's full sort after new particles runs eagerly, never in a graph
+    int prc = fast(h) ? fast_prepare(h) : MPM_OK;
+    if(prc) return prc;
     const int par = fast(h) ? h->fast.cur : 0;
     cudaGraphExec_t& ge = h->graphs[par];
     if(!ge) {
@@ -463,7 +467,7 @@ int mpm_advance(mpm_handle* h, double dt, double time, int nsteps)
     if(rc) return rc;
     if(nsteps < 0) return set_error(h, MPM_ERR_ARG, "nsteps < 0");
     if(h->graph_dt != dt) release_graph(h);
-    if(fast(h) && nsteps && (rc = fast_prepare_sort(h))) return rc;
+    if(fast(h) && nsteps && (rc = fast_prepare(h))) return rc;
     // moving objects: their frames go into tables first, so the substeps can replay a graph
     const bool table = h->moving && nsteps > 1 && !h->timing && !h->implicit.enabled && !(!fast(h) && reduces_dt(h));
     if(table && (rc = fill_motion_table(h, dt, time, nsteps))) return rc;
@@ -487,6 +491,17 @@ int mpm_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf)
     if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
     if(fast(h) && h->fast.nscenes != 1) return set_error(h, MPM_ERR_ARG, "a batch returns its grids per scene: mpm_batch_get_grid");
     return fast(h) ? fast_get_grid(h, 0, m, v0, v, vf) : plain_get_grid(h, m, v0, v, vf);
+}
+
+int mpm_add_grid_forces(mpm_handle* h, double dt, const void* force, int dtype, int on_device)
+{
+    if(!h || !force) return MPM_ERR_ARG;
+    if(!(dt > 0) || !std::isfinite(dt)) return set_error(h, MPM_ERR_ARG, "dt must be positive");
+    if(dtype != MPM_FP32 && dtype != MPM_FP64) return set_error(h, MPM_ERR_ARG, "dtype");
+    if(!h->have_particles) return set_error(h, MPM_ERR_STATE, "no particles set");
+    if(h->implicit.enabled) return set_error(h, MPM_ERR_ARG, "extra node forces enter the explicit substep");
+    if(fast(h) && h->fast.nscenes != 1) return set_error(h, MPM_ERR_ARG, "extra node forces take single-scene handles");
+    return fast(h) ? fast_add_forces(h, dt, force, dtype, on_device != 0) : plain_add_forces(h, force, dtype, on_device != 0);
 }
 
 int mpm_batch_get_grid(mpm_handle* h, int scene, double* m, double* v, double* vf)
@@ -548,7 +563,7 @@ int mpm_set_launch_shape(mpm_handle* h, int p2g_variant, int g2p_threads, int ct
 {
     if(!h) return MPM_ERR_ARG;
     if(!fast(h)) return set_error(h, MPM_ERR_ARG, "launch shapes belong to the fast path");
-    if(p2g_variant < MPM_P2G_CELLS || p2g_variant > MPM_P2G_PAIRX) return set_error(h, MPM_ERR_ARG, "unknown P2G variant");
+    if(p2g_variant < MPM_P2G_GROUPS128 || p2g_variant > MPM_P2G_FIXED256) return set_error(h, MPM_ERR_ARG, "unknown P2G variant");
     if(g2p_threads != 64 && g2p_threads != 128 && g2p_threads != 256) return set_error(h, MPM_ERR_ARG, "G2P threads: 64, 128 or 256");
     if(cta_mult != 1 && cta_mult != 2) return set_error(h, MPM_ERR_ARG, "CTA multiplier: 1 or 2");
     release_graph(h);

@@ -1,29 +1,33 @@
-// Fast path: the explicit MPM substep in FP32 with cell-sorted particles, for
+// Fast path: the explicit MPM substep in FP32 with block-sorted particles, for
 // one scene or a batch of independent scenes (a single scene is a batch of one).
 //
 // Per substep (MPM_DRIVER::Advance_One_Time_Step, MPM_DRIVER.cpp:141-157), each
-// phase is ONE persistent launch over the blocks of all scenes:
-//   sort     particle keys (global block of 4^3 cells, cell in block) are
-//            radix-sorted; the previous G2P wrote them, so particles are already
-//            nearly in order and the permutation is local.
-//   ranges   sorted keys -> [start, end) per particle block, list of active
-//            blocks, number of valid particles (invalid ones carry the
-//            sentinel key and sort to the tail).
-//   p2g      one CTA per active block: B-spline weights, the stress P(F) F^T
-//            (fused; MPM_FINITE_ELEMENTS::Precompute, .cpp:47-67), APIC momentum
-//            plus dt * force into a 6^3-node shared tile, flushed with one
-//            float4 atomic per touched node (Particle_To_Grid l.245-306 with
-//            MPM_FINITE_ELEMENTS::Add_Forces and MPM_GRAVITY::Add_Forces folded
-//            in).  The CTA marks the node blocks its tile covers.
-//   grid     one CTA per marked node block: v = (mv + dt f)/m + dt g, collision
-//            projection and friction (Apply_Forces l.959-1060); clears the
-//            accumulator for the next substep.
-//   g2p      one CTA per active block: stage the tile of (v, v_fric), gather,
-//            update F, X, V and the APIC B (Grid_To_Particle l.450-515), write
-//            the particle to its sorted slot in the other buffer with its next key.
-// Scenes differ in grid size, domain, model and collision objects; blocks and
-// node blocks of all scenes share one numbering, and a CTA looks up the scene
-// of the block it works on.
+// phase is ONE launch over the blocks of all scenes:
+//   bins     the substep's order from the previous one: per particle block
+//            (4^3 cells) its count from the neighbour blocks' move counts the
+//            last G2P kept, a scan into block ranges, the work items (parts of
+//            a block's particles) and where each group of moved particles lands.
+//   route    every particle slot to its place in that order (a stable sort by
+//            block; invalid particles go to the tail).
+//   p2g      one CTA per part: B-spline weights, the stress P(F) F^T (fused;
+//            MPM_FINITE_ELEMENTS::Precompute, .cpp:47-67), APIC momentum plus
+//            dt * force into a 6^3-node shared fixed-point tile, flushed with
+//            one float4 atomic per touched node (Particle_To_Grid l.245-306 with
+//            MPM_FINITE_ELEMENTS::Add_Forces folded in).  It marks the node
+//            blocks its tile covers.
+//   grid     one thread per node of the marked node blocks: v = (mv + dt f)/m
+//            + dt g, collision projection and friction (Apply_Forces
+//            l.959-1060); clears the accumulator for the next substep.
+//   g2p      one CTA per part: stage the tile of (v, v_fric), gather, update F,
+//            X, V and the APIC B (Grid_To_Particle l.450-515), write the
+//            particle to its slot in the other buffer with its next key, and
+//            count where the part's particles move (the next bins' input).
+// After new particles (or a restore) a full radix sort of the keys orders the
+// slots once (fast_prepare).  Scenes differ in grid size, domain, model and
+// collision objects; blocks and node blocks of all scenes share one
+// numbering, and a CTA looks up the scene of the block it works on.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -55,6 +59,15 @@ constexpr int C_X = 0, C_V = 3, C_F = 6, C_B = 15;
 constexpr int NPLAS = 13;                  // plastic state floats per particle: Fp0..8, then
                                            // mu0, lambda0 (clamp) or plastic_def, rho_F, sigma_Y, vc
 
+// Move directions of a particle between two substeps' orders: the 27
+// neighbour blocks (dx, dy, dz in -1..1, index (dx+1) 9 + (dy+1) 3 + dz+1),
+// then farther than a neighbour, then invalidated.
+constexpr int NDIR = 29;
+constexpr int DIR_STAY = 13, DIR_FAR = 27, DIR_INVALID = 28;
+constexpr int SCAN_TILE = 256;             // allocation unit of the block scan's status words (>= its tiles)
+// Largest work item (particles of one block) of each P2G launch shape.
+constexpr int kPartSize[4] = {512, 1024, 128, 256};
+
 struct FastArgs {
     int64_t n, npad;
     const float* src;
@@ -63,13 +76,22 @@ struct FastArgs {
     float* dst;
     float4* dst_attr;
     int* dst_pid;
-    const uint32_t* perm;
-    const uint32_t* sorted_keys;
-    uint32_t* keys_next;
-    uint32_t *bstart, *bend, *active, *nb_flag, *nb_list, *counters;
+    uint32_t* perm;
+    uint32_t* sorted_keys;
+    const uint32_t* keys_cur;   // cell keys of the current buffer's slots
+    uint32_t* keys_next;        // cell keys of the other buffer's slots (G2P writes them)
+    // this substep's order: block ranges, active blocks, work items, counters
+    uint32_t *bstart, *bend, *active, *ctr;
+    uint4* chunks;
+    // the previous substep's order (routing input)
+    const uint32_t *obstart, *obend, *oactive, *octr;
+    uint32_t *dcount, *doff, *far_in, *farpos, *bcount, *scan;
+    int64_t nblk;               // particle blocks of all scenes
+    int part;                   // P2G work-item size (particles)
+    uint32_t chunk_cap;         // capacity of the work-item lists
+    uint32_t *nb_flag, *nb_list;
     uint32_t* fallback;   // sorted positions whose stress takes the FP64 route (P2G)
-    uint32_t* sort_scratch;   // digit histograms of the next sort live at its start
-    int key_bits;
+    const CUtensorMap* tmaps;   // per scene: its grid of 8-float nodes as a 4D tensor (G2P tiles)
     float4* acc;
     float4* vel;
     const SceneDev* scenes;
@@ -248,7 +270,7 @@ __device__ __noinline__ bool stress_fp64(int model, const float* Ff, float mu, f
 }
 
 // ---------------------------------------------------------------------------
-__global__ void k_init_keys(FastArgs a, const uint8_t* valid_by_slot)
+__global__ void k_init_keys(FastArgs a, const uint8_t* valid_by_slot, uint32_t* out)
 {
     for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
         // scene of particle i: pbase[s] <= i < pbase[s + 1] (particles arrive in scene order)
@@ -260,108 +282,349 @@ __global__ void k_init_keys(FastArgs a, const uint8_t* valid_by_slot)
         float X[3] = {a.src[(C_X + 0) * a.npad + i], a.src[(C_X + 1) * a.npad + i], a.src[(C_X + 2) * a.npad + i]};
         uint32_t k = valid_by_slot[i] ? cell_key(a.scenes[lo], X) : SENTINEL;
         if(valid_by_slot[i] && k == SENTINEL) atomicOr(a.flags, MPM_FLAG_DOMAIN);
-        a.keys_next[i] = k;
+        out[i] = k;
     }
 }
 
-// Block ranges of the sorted keys and the list of active blocks.  Invalid
-// particles (sentinel keys, sorted last) keep their last state: they are
-// copied to their sorted slot here, as G2P does for the valid ones.
-__global__ void k_ranges(FastArgs a)
+// ---------------------------------------------------------------------------
+// The substep's particle order, built from the previous one.
+//
+// The previous G2P wrote every particle's new cell key to its slot and
+// counted, per block it processed, how many of its particles moved to each
+// neighbour block (dcount[d][block], d the move direction) and how many left
+// the domain (d = DIR_INVALID); a particle that moved farther than a
+// neighbour block adds one arrival to its new block (far_in).  Slots are
+// grouped by their previous block, in block order.  A stable sort by block
+// key is then: new block b holds the particles that came from block
+// b - delta(d) with direction d, group after group in the order of those
+// previous blocks (each group in slot order), then its far arrivals; all valid particles come first, in block order, then the
+// particles the last G2P invalidated (in slot order), then those invalid
+// before.  k_bins scans the per-block counts into block ranges (one pass of
+// decoupled look-back over tiles of blocks) and hands out the work items;
+// k_route moves every slot to its place.  This takes the place of a radix
+// sort of the keys every substep: the order equals a stable sort by block key
+// whenever no particle crossed more than one block (4 cells) in the substep;
+// far arrivals go to the end of their block in arrival order.  The
+// reference's analogue is the binning of GATHER_SCATTER::Prepare_Scatter
+// (Hybrid_Methods/Iterators/GATHER_SCATTER.cpp:33-87).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int dir_dx(int d) { return d / 9 - 1; }
+__device__ __forceinline__ int dir_dy(int d) { return (d / 3) % 3 - 1; }
+__device__ __forceinline__ int dir_dz(int d) { return d % 3 - 1; }
+
+// Direction of a move from block (ox, oy, oz) to block (nx, ny, nz) of a scene.
+__device__ __forceinline__ int move_dir(int ox, int oy, int oz, int nx, int ny, int nz)
 {
-    // the sort has read its histograms: G2P builds the next ones
-    if(blockIdx.x == 0) mpm_sort::hist_reset(a.sort_scratch);
-    for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < a.n; j += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t k = a.sorted_keys[j];
-        uint32_t kp = j ? a.sorted_keys[j - 1] : SENTINEL;
-        if(k == SENTINEL) {
-            if(j == 0 || kp != SENTINEL) a.counters[CNT_ACTIVE_PARTICLES] = (uint32_t)j;
-            const uint32_t i = a.perm[j];
+    const int dx = nx - ox, dy = ny - oy, dz = nz - oz;
+    if(dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) return DIR_FAR;
+    return (dx + 1) * 9 + (dy + 1) * 3 + dz + 1;
+}
+
+// Direction of the particle with new cell key `key`, previously in block `b`
+// (local coordinates bx, by, bz) of scene sc.
+__device__ __forceinline__ int key_dir(const SceneDev& sc, uint32_t b, int bx, int by, int bz, uint32_t key)
+{
+    if(key == SENTINEL) return DIR_INVALID;
+    const uint32_t nb = key >> 6;
+    if(nb == b) return DIR_STAY;
+    int nx, ny, nz;
+    block_coords(sc, nb - sc.block_base, nx, ny, nz);
+    return move_dir(bx, by, bz, nx, ny, nz);
+}
+
+// Decoupled look-back of one running count by one warp: publish the tile's
+// aggregate, add the predecessors' aggregates until an inclusive prefix, then
+// publish the inclusive prefix; returns the exclusive prefix (every lane).
+// Status word: epoch (30 bits) | flag (2 bits: 1 aggregate, 2 inclusive) |
+// value (32 bits).  The wait is bounded: past the limit the tile sets the
+// timeout flag and goes on with what it has summed.
+__device__ uint32_t warp_lookback(uint64_t* status, int64_t tile, uint32_t agg, uint64_t epoch, unsigned* flags)
+{
+    using ref = cuda::atomic_ref<uint64_t, cuda::thread_scope_device>;
+    const int lane = threadIdx.x & 31;
+    if(tile == 0) {
+        if(lane == 0) ref(status[0]).store((epoch << 34) | (2ull << 32) | agg, cuda::memory_order_relaxed);
+        return 0;
+    }
+    if(lane == 0) ref(status[tile]).store((epoch << 34) | (1ull << 32) | agg, cuda::memory_order_relaxed);
+    uint32_t excl = 0, spins = 0;
+    int64_t j = tile - 1;
+    for(;;) {
+        const int64_t t = j - lane;
+        uint64_t w = (epoch << 34) | (2ull << 32);          // before tile 0: an inclusive zero
+        if(t >= 0) w = ref(status[t]).load(cuda::memory_order_relaxed);
+        const uint32_t fl = (w >> 34) == epoch ? (uint32_t)(w >> 32) & 3u : 0u;
+        const unsigned pending = __ballot_sync(0xffffffffu, fl == 0);
+        const unsigned incl = __ballot_sync(0xffffffffu, fl == 2);
+        const int np = pending ? __ffs(pending) - 1 : 32;
+        const int ni = incl ? __ffs(incl) - 1 : 32;
+        const int take = ni < np ? ni + 1 : np;             // lanes 0 .. take - 1 count
+        uint32_t v = lane < take ? (uint32_t)w : 0u;
+#pragma unroll
+        for(int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        if(ni < np) break;
+        j -= np;
+        if(np == 0 && ++spins > mpm_sort::kSpinLimit) {
+            if(lane == 0) atomicOr(flags, MPM_FLAG_TIMEOUT);
+            break;
+        }
+    }
+    if(lane == 0) ref(status[tile]).store((epoch << 34) | (2ull << 32) | (excl + agg), cuda::memory_order_relaxed);
+    return excl;
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for(int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if(lane >= o) x += y;
+    }
+    return x;
+}
+
+// Tiles of BIN_TILE blocks of all scenes in ticket order, BIN_PER consecutive
+// blocks per thread: each block's particle count (arrivals the last G2P
+// counted), the exclusive prefix over all blocks (block ranges), the active
+// blocks and the work items (parts of at most a.part particles); for an
+// active block the offsets at which each (previous block, direction) group
+// of its particles lands.  Consumed counts are zeroed for the next G2P.
+constexpr int BIN_THREADS = 256, BIN_PER = 4, BIN_TILE = BIN_THREADS * BIN_PER;
+
+__global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
+{
+    constexpr int NW = BIN_THREADS / 32;
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp[NW][4];
+    __shared__ uint32_t s_pre[4];         // prefixes of the tile: count, invalid (look-back); parts, active (bases)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(threadIdx.x == 0) s_tile = atomicAdd(&a.ctr[CNT_BIN_TICKET], 1u);
+    __syncthreads();
+    const int64_t tile = s_tile, ntiles = (a.nblk + BIN_TILE - 1) / BIN_TILE;
+    const int64_t b0 = tile * BIN_TILE + threadIdx.x * BIN_PER;
+    const uint64_t epoch = a.scan[0] & mpm_sort::kEpochMask;
+    uint64_t* status = reinterpret_cast<uint64_t*>(a.scan + 2);
+    uint32_t cnt[BIN_PER], inv[BIN_PER], v[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for(int u = 0; u < BIN_PER; u++) {
+        const int64_t b = b0 + u;
+        cnt[u] = b < a.nblk ? a.bcount[b] : 0u;
+        inv[u] = b < a.nblk ? a.dcount[DIR_INVALID * a.nblk + b] : 0u;
+        v[0] += cnt[u];
+        v[1] += inv[u];
+        v[2] += cnt[u] ? (cnt[u] + a.part - 1) / a.part : 0u;
+        v[3] += cnt[u] ? 1u : 0u;
+    }
+    uint32_t x[4];
+#pragma unroll
+    for(int q = 0; q < 4; q++) {
+        x[q] = warp_incl_scan(v[q]);
+        if(lane == 31) s_warp[warp][q] = x[q];
+    }
+    __syncthreads();
+    if(warp == 0) {
+#pragma unroll
+        for(int q = 0; q < 4; q++) {
+            const uint32_t t = lane < NW ? s_warp[lane][q] : 0u;
+            const uint32_t ti = warp_incl_scan(t);
+            if(lane < NW) s_warp[lane][q] = ti - t;                  // exclusive warp offset
+            const uint32_t tot = __shfl_sync(0xffffffffu, ti, NW - 1);
+            if(lane == 0) s_pre[q] = tot;                            // tile total, for now
+        }
+    }
+    __syncthreads();
+    uint32_t tot[4];
+#pragma unroll
+    for(int q = 0; q < 4; q++) tot[q] = s_pre[q];
+    __syncthreads();
+    if(warp == 0) {
+        const uint32_t p = warp_lookback(status, tile, tot[0], epoch, a.flags);
+        if(lane == 0) s_pre[0] = p;
+    } else if(warp == 1) {
+        const uint32_t p = warp_lookback(status + ntiles, tile, tot[1], epoch, a.flags);
+        if(lane == 0) s_pre[1] = p;
+    } else if(threadIdx.x == 64) {
+        s_pre[2] = tot[2] ? atomicAdd(&a.ctr[CNT_CHUNKS], tot[2]) : 0u;
+        s_pre[3] = tot[3] ? atomicAdd(&a.ctr[CNT_ACTIVE_BLOCKS], tot[3]) : 0u;
+    }
+    __syncthreads();
+    if(tile == ntiles - 1 && threadIdx.x == 0) {
+        a.ctr[CNT_ACTIVE_PARTICLES] = s_pre[0] + tot[0];
+        a.ctr[CNT_NEW_INVALID] = s_pre[1] + tot[1];
+    }
+    uint32_t ex[4];
+#pragma unroll
+    for(int q = 0; q < 4; q++) ex[q] = s_pre[q] + s_warp[warp][q] + x[q] - v[q];
+    for(int u = 0; u < BIN_PER; u++) {
+        const int64_t b = b0 + u;
+        if(inv[u]) {
+            a.doff[DIR_INVALID * a.nblk + b] = ex[1];
+            a.dcount[DIR_INVALID * a.nblk + b] = 0u;
+            ex[1] += inv[u];
+        }
+        if(!cnt[u]) continue;
+        const uint32_t start = ex[0], parts = (cnt[u] + a.part - 1) / a.part;
+        ex[0] += cnt[u];
+        a.bstart[b] = start;
+        a.bend[b] = start + cnt[u];
+        a.bcount[b] = 0u;
+        a.active[ex[3]++] = (uint32_t)b;
+        for(uint32_t k = 0; k < parts; k++, ex[2]++)
+            if(ex[2] < a.chunk_cap) a.chunks[ex[2]] = make_uint4((uint32_t)b, k, parts, 0u);
+        // the groups of arrivals, in the order of their previous block (slot order):
+        // block b - delta(d) grows as d falls
+        const SceneDev& sc = a.scenes[a.block_scene[b]];
+        int bx, by, bz;
+        block_coords(sc, (uint32_t)(b - sc.block_base), bx, by, bz);
+        uint32_t src[27], cin[27];
+#pragma unroll
+        for(int d = 0; d < 27; d++) {
+            const int ox = bx - dir_dx(d), oy = by - dir_dy(d), oz = bz - dir_dz(d);
+            const bool in = ox >= 0 && oy >= 0 && oz >= 0 && ox < sc.NB[0] && oy < sc.NB[1] && oz < sc.NB[2];
+            src[d] = in ? sc.block_base + ((uint32_t)ox * sc.NB[1] + oy) * sc.NB[2] + oz : SENTINEL;
+        }
+#pragma unroll
+        for(int d = 0; d < 27; d++) cin[d] = src[d] != SENTINEL ? a.dcount[d * a.nblk + src[d]] : 0u;
+        uint32_t run = start;
+#pragma unroll
+        for(int d = 26; d >= 0; d--) {
+            if(cin[d]) {
+                a.doff[d * a.nblk + src[d]] = run;
+                run += cin[d];
+                a.dcount[d * a.nblk + src[d]] = 0u;
+            }
+        }
+        if(run != start + cnt[u]) {     // far arrivals fill the rest of the block
+            a.farpos[b] = run;
+            a.far_in[b] = 0u;
+        }
+    }
+}
+
+// Slot j of the current buffer to slot `dest` of the other (state, attributes,
+// caller index, plastic state) with key `key`.
+__device__ __forceinline__ void copy_slot(const FastArgs& a, uint32_t j, uint32_t dest, uint32_t key)
+{
 #pragma unroll 4
-            for(int c = 0; c < NCOMP; c++) a.dst[c * a.npad + j] = a.src[c * a.npad + i];
-            a.dst_attr[j] = a.src_attr[i];
-            a.dst_pid[j] = a.src_pid[i];
-            if(a.psrc)
-                for(int c = 0; c < a.nplas; c++) a.pdst[c * a.npad + j] = a.psrc[c * a.npad + i];
-            a.keys_next[j] = SENTINEL;
+    for(int c = 0; c < NCOMP; c++) a.dst[c * a.npad + dest] = a.src[c * a.npad + j];
+    a.dst_attr[dest] = a.src_attr[j];
+    a.dst_pid[dest] = a.src_pid[j];
+    if(a.psrc)
+        for(int c = 0; c < a.nplas; c++) a.pdst[c * a.npad + dest] = a.psrc[c * a.npad + j];
+    a.keys_next[dest] = key;
+}
+
+// Every slot of the current buffer to its place in the new order (perm[dest]
+// = slot, sorted key).  Valid particles keep their state in place (P2G and
+// G2P read it through perm); invalid ones are copied to their tail slot of
+// the other buffer, which G2P does not write.  One CTA per previous block at
+// a time; ranks within (block, direction) follow slot order.
+__global__ void __launch_bounds__(256) k_route(FastArgs a)
+{
+    constexpr int W = 8;
+    __shared__ uint32_t s_wc[W][32];      // particles per warp and direction, this round
+    __shared__ uint32_t s_run[32];        // particles per direction, earlier rounds
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nold = a.octr[CNT_ACTIVE_BLOCKS], nvalid_old = a.octr[CNT_ACTIVE_PARTICLES];
+    const uint32_t nvalid = a.ctr[CNT_ACTIVE_PARTICLES], ninv = a.ctr[CNT_NEW_INVALID];
+    (&s_wc[0][0])[threadIdx.x] = 0u;
+    for(uint32_t w = blockIdx.x; w < nold; w += gridDim.x) {
+        const uint32_t o = a.oactive[w];
+        const SceneDev& sc = a.scenes[a.block_scene[o]];
+        int ox, oy, oz;
+        block_coords(sc, o - sc.block_base, ox, oy, oz);
+        const uint32_t s = a.obstart[o], e = a.obend[o];
+        if(threadIdx.x < 32) s_run[threadIdx.x] = 0u;
+        __syncthreads();
+        for(uint32_t base = s; base < e; base += 256) {
+            const uint32_t j = base + threadIdx.x;
+            const bool ok = j < e;
+            const uint32_t key = ok ? a.keys_cur[j] : SENTINEL;
+            const int d = ok ? key_dir(sc, o, ox, oy, oz, key) : 31;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const uint32_t intra = __popc(peers & ((1u << lane) - 1u));
+            if(ok && (__ffs(peers) - 1) == lane) s_wc[warp][d] = __popc(peers);
+            __syncthreads();
+            if(ok) {
+                uint32_t rank = s_run[d] + intra;
+                for(int w2 = 0; w2 < warp; w2++) rank += s_wc[w2][d];
+                uint32_t dest;
+                if(d < 27) dest = a.doff[d * a.nblk + o] + rank;
+                else if(d == DIR_FAR) {
+                    dest = atomicAdd(&a.farpos[key >> 6], 1u);
+                    atomicAdd(&a.ctr[CNT_FAR], 1u);
+                } else dest = nvalid + a.doff[DIR_INVALID * a.nblk + o] + rank;
+                if(dest < a.n) {
+                    if(d == DIR_INVALID) copy_slot(a, j, dest, SENTINEL);
+                    a.perm[dest] = j;
+                    a.sorted_keys[dest] = key;
+                } else atomicOr(a.flags, MPM_FLAG_ORDER);   // counts out of step: report, write nothing
+            }
+            __syncthreads();
+            if(threadIdx.x < 32) {
+                uint32_t t = 0;
+#pragma unroll
+                for(int w2 = 0; w2 < W; w2++) {
+                    t += s_wc[w2][threadIdx.x];
+                    s_wc[w2][threadIdx.x] = 0u;
+                }
+                s_run[threadIdx.x] += t;
+            }
+            __syncthreads();
+        }
+    }
+    // the particles invalid before the last G2P follow, in slot order
+    for(int64_t j = nvalid_old + blockIdx.x * 256ll + threadIdx.x; j < a.n; j += (int64_t)gridDim.x * 256) {
+        const uint32_t dest = (uint32_t)(nvalid + ninv + (j - nvalid_old));
+        if(dest >= a.n) {
+            atomicOr(a.flags, MPM_FLAG_ORDER);
+            break;
+        }
+        copy_slot(a, (uint32_t)j, dest, SENTINEL);
+        a.perm[dest] = (uint32_t)j;
+        a.sorted_keys[dest] = SENTINEL;
+    }
+    if(blockIdx.x == 0 && threadIdx.x == 0) a.scan[0] += 1u;   // the next block scan's epoch
+}
+
+// After a full radix sort of the current slots' keys (particles just set, or
+// the autotuner's restore): the particles are copied to the other buffer in
+// sorted order, and that order is recorded as the previous substep's (block
+// ranges and active blocks into the given set, every particle counted as
+// staying in its block), so the next substep's routing is the identity.
+__global__ void k_prepare(FastArgs a, uint32_t* pbstart, uint32_t* pbend, uint32_t* pactive, uint32_t* pctr)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t end = (a.n + 31) & ~(int64_t)31;      // whole warps stay in the loop
+    for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < end; j += (int64_t)gridDim.x * blockDim.x) {
+        const bool in = j < a.n;
+        const uint32_t k = in ? a.sorted_keys[j] : SENTINEL;
+        if(in) copy_slot(a, a.perm[j], (uint32_t)j, k);
+        const bool valid = k != SENTINEL;
+        const uint32_t b = k >> 6;
+        const unsigned peers = __match_any_sync(0xffffffffu, valid ? b : 0xffffffffu);
+        if(valid && (__ffs(peers) - 1) == lane) {
+            atomicAdd(&a.dcount[DIR_STAY * a.nblk + b], (uint32_t)__popc(peers));
+            atomicAdd(&a.bcount[b], (uint32_t)__popc(peers));
+        }
+        if(!in) continue;
+        const uint32_t kp = j ? a.sorted_keys[j - 1] : SENTINEL;
+        if(!valid) {
+            if(j == 0 || kp != SENTINEL) pctr[CNT_ACTIVE_PARTICLES] = (uint32_t)j;
             continue;
         }
-        uint32_t b = k >> 6;
         if(j == 0 || (kp >> 6) != b) {
-            a.bstart[b] = (uint32_t)j;
-            a.active[atomicAdd(&a.counters[CNT_ACTIVE_BLOCKS], 1u)] = b;
+            pbstart[b] = (uint32_t)j;
+            pactive[atomicAdd(&pctr[CNT_ACTIVE_BLOCKS], 1u)] = b;
         }
-        uint32_t kn = j + 1 < a.n ? a.sorted_keys[j + 1] : SENTINEL;
-        if(kn == SENTINEL || (kn >> 6) != b) a.bend[b] = (uint32_t)(j + 1);
-        if(j + 1 == a.n) a.counters[CNT_ACTIVE_PARTICLES] = (uint32_t)a.n;
+        const uint32_t kn = j + 1 < a.n ? a.sorted_keys[j + 1] : SENTINEL;
+        if(kn == SENTINEL || (kn >> 6) != b) pbend[b] = (uint32_t)(j + 1);
+        if(j + 1 == a.n) pctr[CNT_ACTIVE_PARTICLES] = (uint32_t)a.n;
     }
 }
 
-
-__device__ __forceinline__ int next_work(uint32_t* ctr, int* s_work)
-{
-    __syncthreads();
-    if(threadIdx.x == 0) *s_work = (int)atomicAdd(ctr, 1u);
-    __syncthreads();
-    return *s_work;
-}
-
-struct P2GTile {
-    float m[PTN], x[PTN], y[PTN], z[PTN];
-    uint32_t ccount[64], cstart[64];
-    uint32_t maxc;
-    SceneDev sc;
-    int work;
-};
-
-// Block set-up shared by both P2G variants: stage the scene, zero the tile,
-// count the block's particles per cell (they arrive sorted by cell) and scan.
-__device__ __forceinline__ void p2g_begin(const FastArgs& a, P2GTile& T, uint32_t b)
-{
-    stage_scene(a, a.block_scene[b], &T.sc);
-    for(int t = threadIdx.x; t < PTN; t += blockDim.x) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
-    if(threadIdx.x < 64) T.ccount[threadIdx.x] = 0;
-    __syncthreads();
-    const uint32_t s = a.bstart[b], e = a.bend[b];
-    for(uint32_t j = s + threadIdx.x; j < e; j += blockDim.x) atomicAdd(&T.ccount[a.sorted_keys[j] & 63u], 1u);
-    __syncthreads();
-    if(threadIdx.x < 32) {
-        const int c = threadIdx.x;
-        uint32_t c0 = T.ccount[2 * c], c1 = T.ccount[2 * c + 1];
-        uint32_t sum = c0 + c1, x = sum, mx = c0 > c1 ? c0 : c1;
-#pragma unroll
-        for(int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if(c >= o) x += y;
-            mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        }
-        T.cstart[2 * c] = x - sum;
-        T.cstart[2 * c + 1] = x - sum + c0;
-        if(c == 0) T.maxc = mx;
-    }
-    __syncthreads();
-}
-
-// Flush the tile with one float4 atomic per touched node and mark the 8 node
-// blocks the tile covers for the grid update.
-__device__ __forceinline__ void p2g_end(const FastArgs& a, P2GTile& T, uint32_t lb)
-{
-    __syncthreads();
-    const SceneDev& sc = T.sc;
-    int bx, by, bz;
-    block_coords(sc, lb, bx, by, bz);
-    for(int t = threadIdx.x; t < TN; t += blockDim.x) {
-        const int tx = t / (TE * TE), ty = (t / TE) % TE, tz = t % TE, u = ptile(tx, ty, tz);
-        float mm = T.m[u];
-        if(mm != 0.f)
-            atomicAdd(&a.acc[node_index(sc, 4 * bx + tx, 4 * by + ty, 4 * bz + tz)], make_float4(T.x[u], T.y[u], T.z[u], mm));
-    }
-    if(threadIdx.x < 8) {
-        int nx = bx + (threadIdx.x >> 2), ny = by + ((threadIdx.x >> 1) & 1), nz = bz + (threadIdx.x & 1);
-        uint32_t nb = sc.nb_base + ((uint32_t)nx * sc.NN[1] + ny) * sc.NN[2] + nz;
-        if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.counters[CNT_NODE_BLOCKS], 1u)] = nb;
-    }
-}
 
 // Every node quantity of a particle has the separable form (w = wx wy wz at
 // node (i, j, k))
@@ -406,7 +669,7 @@ __device__ __forceinline__ void factors_from(const FastArgs& a, const SceneDev& 
 {
     float S[9];
     if(!stress_fast(model, F, at.z, at.w, S)) {
-        a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
+        a.fallback[atomicAdd(&a.ctr[CNT_FALLBACK], 1u)] = j;
 #pragma unroll
         for(int r = 0; r < 9; r++) S[r] = 0.f;
     }
@@ -506,12 +769,12 @@ __device__ __forceinline__ void p2g_finish(const FastArgs& a, int* s_last)
     __syncthreads();
     if(threadIdx.x == 0) {
         __threadfence();
-        *s_last = atomicAdd(&a.counters[CNT_P2G_DONE], 1u) == gridDim.x - 1;
+        *s_last = atomicAdd(&a.ctr[CNT_P2G_DONE], 1u) == gridDim.x - 1;
     }
     __syncthreads();
     if(!*s_last) return;
     __threadfence();
-    const uint32_t count = *(volatile uint32_t*)&a.counters[CNT_FALLBACK];
+    const uint32_t count = *(volatile uint32_t*)&a.ctr[CNT_FALLBACK];
     for(uint32_t k = threadIdx.x; k < count; k += blockDim.x) p2g_fallback_force(a, k);
 }
 
@@ -533,395 +796,396 @@ __global__ void k_penalty_kick(FastArgs a)
     }
 }
 
-// P2G variant 0: one thread per cell of the block.  A thread walks the
-// particles of its cell (they share the 27 nodes), accumulates the node values
-// in registers, and adds them to the shared tile once per cell: 8x fewer
-// shared atomics than one per particle, and the 64 lanes of a block hit 64
-// different node addresses for any given node offset.
-__global__ void __launch_bounds__(64) k_p2g_cells(FastArgs a)
-{
-    __shared__ P2GTile T;
-    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    const int c = threadIdx.x;   // cell in block: (lx << 4) | (ly << 2) | lz
-    const int lx = c >> 4, ly = (c >> 2) & 3, lz = c & 3;
-    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
-        const uint32_t b = a.active[w];
-        p2g_begin(a, T, b);
-        const uint32_t cnt = T.ccount[c], beg = a.bstart[b] + T.cstart[c];
-        if(cnt) {
-            float am[27], ax[27], ay[27], az[27];
-#pragma unroll
-            for(int q = 0; q < 27; q++) { am[q] = 0; ax[q] = 0; ay[q] = 0; az[q] = 0; }
-            for(uint32_t k = 0; k < cnt; k++) {
-                P2GFactors P;
-                particle_factors(a, T.sc, beg + k, P);
-                factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
-                    const int q = (ii * 3 + jj) * 3 + kk;
-                    am[q] += m; ax[q] += px; ay[q] += py; az[q] += pz;
-                });
-            }
-            const int t0 = ptile(lx, ly, lz);
-#pragma unroll
-            for(int ii = 0; ii < 3; ii++)
-#pragma unroll
-                for(int jj = 0; jj < 3; jj++)
-#pragma unroll
-                    for(int kk = 0; kk < 3; kk++) {
-                        const int q = (ii * 3 + jj) * 3 + kk, t = t0 + ptile(ii, jj, kk);
-                        atomicAdd(&T.m[t], am[q]);
-                        atomicAdd(&T.x[t], ax[q]);
-                        atomicAdd(&T.y[t], ay[q]);
-                        atomicAdd(&T.z[t], az[q]);
-                    }
-        }
-        p2g_end(a, T, b - T.sc.block_base);
-    }
-    p2g_finish(a, &T.work);
-}
-
-// P2G variant 2: two lanes per contiguous range of the block's sorted
-// particles.  The ranges split the block evenly (no lane idles on a sparse
-// cell), and the two lanes of a pair split the four node quantities: the even
-// lane accumulates mass and x momentum, the odd lane y and z momentum, so each
-// holds 54 accumulators instead of 108 and twice as many warps fit on an SM.
-// Accumulators go to the shared tile whenever the range moves to a new cell.
-template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_p2g_pairs(FastArgs a)
-{
-    __shared__ P2GTile T;
-    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    const bool odd = threadIdx.x & 1;
-    const int pair = threadIdx.x >> 1;
-    constexpr int kPairs = THREADS / 2;
-    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
-        const uint32_t b = a.active[w];
-        stage_scene(a, a.block_scene[b], &T.sc);
-        for(int t = threadIdx.x; t < PTN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
-        __syncthreads();
-        const SceneDev& sc = T.sc;
-        const uint32_t s = a.bstart[b], e = a.bend[b];
-        const uint32_t per = (e - s + kPairs - 1) / kPairs;
-        const uint32_t j0 = s + pair * per, j1 = min(j0 + per, e);
-        float* const out0 = odd ? T.y : T.m;
-        float* const out1 = odd ? T.z : T.x;
-        float acc0[27], acc1[27];
-#pragma unroll
-        for(int q = 0; q < 27; q++) { acc0[q] = 0.f; acc1[q] = 0.f; }
-        int cell = -1;
-        for(uint32_t j = j0; j < j1; j++) {
-            const int c = (int)(a.sorted_keys[j] & 63u);
-            if(c != cell) {
-                if(cell >= 0) {
-                    const int t0 = ptile(cell >> 4, (cell >> 2) & 3, cell & 3);
-#pragma unroll
-                    for(int q = 0; q < 27; q++) {
-                        const int t = t0 + ptile(q / 9, (q / 3) % 3, q % 3);
-                        atomicAdd(&out0[t], acc0[q]);
-                        atomicAdd(&out1[t], acc1[q]);
-                        acc0[q] = 0.f;
-                        acc1[q] = 0.f;
-                    }
-                }
-                cell = c;
-            }
-            const uint32_t i = a.perm[j];
-            float X[3], F[9];
-#pragma unroll
-            for(int r = 0; r < 3; r++) X[r] = a.src[(C_X + r) * a.npad + i];
-#pragma unroll
-            for(int r = 0; r < 9; r++) F[r] = a.src[(C_F + r) * a.npad + i];
-            const float4 at = a.src_attr[i];   // mass, volume, mu, lambda
-            // this lane's two components: even lane (mass, x), odd lane (y, z)
-            const int r0 = odd ? 1 : 0, r1 = odd ? 2 : 0;
-            float V0 = a.vsrc[r0 * a.npad + i], V1 = a.vsrc[r1 * a.npad + i];
-            float B0[3], B1[3];
-#pragma unroll
-            for(int c2 = 0; c2 < 3; c2++) {
-                B0[c2] = a.src[(C_B + r0 + 3 * c2) * a.npad + i];
-                B1[c2] = a.src[(C_B + r1 + 3 * c2) * a.npad + i];
-            }
-            float S[9];
-            if(!stress_fast(slot_model(a, sc, i), F, at.z, at.w, S)) {
-                // the FP64 SVD route runs in p2g_finish, which adds this
-                // particle's force; here it contributes mass and momentum only
-                if(!odd) a.fallback[atomicAdd(&a.counters[CNT_FALLBACK], 1u)] = j;
-#pragma unroll
-                for(int r = 0; r < 9; r++) S[r] = 0.f;
-            }
-            const float sv = a.dt * at.y, m = at.x;
-            const Axis<float> wx = spline_axis<float>(X[0], sc.dmin[0], sc.dx[0], sc.inv[0]);
-            const Axis<float> wy = spline_axis<float>(X[1], sc.dmin[1], sc.dx[1], sc.inv[1]);
-            const Axis<float> wz = spline_axis<float>(X[2], sc.dmin[2], sc.dx[2], sc.inv[2]);
-            float dX[3][3];
-#pragma unroll
-            for(int o = 0; o < 3; o++) {
-                dX[0][o] = sc.dmin[0] + ((float)(wx.base + o) + 0.5f) * sc.dx[0] - X[0];
-                dX[1][o] = sc.dmin[1] + ((float)(wy.base + o) + 0.5f) * sc.dx[1] - X[1];
-                dX[2][o] = sc.dmin[2] + ((float)(wz.base + o) + 0.5f) * sc.dx[2] - X[2];
-            }
-            const float Dm[3] = {4.f * sc.inv[0] * sc.inv[0] * m, 4.f * sc.inv[1] * sc.inv[1] * m,
-                                 4.f * sc.inv[2] * sc.inv[2] * m};
-            float mBD0[3], mBD1[3], S0[3], S1[3];
-#pragma unroll
-            for(int c2 = 0; c2 < 3; c2++) {
-                // slot 0 of the even lane is the mass: V = 1, B = 0, PF^T = 0
-                mBD0[c2] = odd ? B0[c2] * Dm[c2] : 0.f;
-                mBD1[c2] = B1[c2] * Dm[c2];
-                S0[c2] = odd ? S[1 + 3 * c2] * sv : 0.f;
-                S1[c2] = (odd ? S[2 + 3 * c2] : S[3 * c2]) * sv;
-            }
-            PairSlot q0, q1;
-            pair_slot(wx, wy, wz, dX, odd ? m * V0 : m, mBD0, S0, q0);
-            pair_slot(wx, wy, wz, dX, m * V1, mBD1, S1, q1);
-#pragma unroll
-            for(int ii = 0; ii < 3; ii++)
-#pragma unroll
-                for(int jj = 0; jj < 3; jj++) {
-                    const float wxy = wx.w[ii] * wy.w[jj];
-                    const float A0 = fmaf(q0.Hx[ii], wy.w[jj], wx.w[ii] * q0.Hy[jj]);
-                    const float A1 = fmaf(q1.Hx[ii], wy.w[jj], wx.w[ii] * q1.Hy[jj]);
-#pragma unroll
-                    for(int kk = 0; kk < 3; kk++) {
-                        const int q = (ii * 3 + jj) * 3 + kk;
-                        acc0[q] = fmaf(A0, wz.w[kk], fmaf(wxy, q0.Hz[kk], acc0[q]));
-                        acc1[q] = fmaf(A1, wz.w[kk], fmaf(wxy, q1.Hz[kk], acc1[q]));
-                    }
-                }
-        }
-        if(cell >= 0) {
-            const int t0 = ptile(cell >> 4, (cell >> 2) & 3, cell & 3);
-#pragma unroll
-            for(int q = 0; q < 27; q++) {
-                const int t = t0 + ptile(q / 9, (q / 3) % 3, q % 3);
-                atomicAdd(&out0[t], acc0[q]);
-                atomicAdd(&out1[t], acc1[q]);
-            }
-        }
-        p2g_end(a, T, b - sc.block_base);
-    }
-    p2g_finish(a, &T.work);
-}
-
-// P2G variant 3: as variant 2 (two lanes per range, the even lane holding
-// mass and x momentum, the odd lane y and z), but the lanes share the
-// per-particle work: the even lane prepares particle j, the odd lane particle
-// j + 1 (stress, weights and the separable factors of all four quantities),
-// and each sends its partner the weights and the factors of the partner's two
-// quantities through a shuffle.
-struct PairPrep {
-    float w[9];            // wx[3], wy[3], wz[3]
-    PairSlot keep0, keep1, send0, send1;
-    int cell;
+// ---------------------------------------------------------------------------
+// P2G (MPM_DRIVER::Particle_To_Grid, MPM_DRIVER.cpp:245-306, with
+// MPM_FINITE_ELEMENTS::Add_Forces, MPM_FINITE_ELEMENTS.cpp:84-99, folded in as
+// dt f): one work item is part k of a block, the particles bstart + k,
+// bstart + k + parts, ... (a strided part samples every cell of the block),
+// one thread per particle.
+//
+// The part's node values are summed in a shared tile of fixed-point
+// integers: shared-memory integer adds are single instructions, where float
+// adds to shared memory are compare-and-swap loops, and integer sums do not
+// depend on their order.  Each quantity (mass, momentum x, y, z) has its own
+// power-of-two scale, chosen after every particle of the part has bounded its
+// largest node value: the bounds' sum B maps to at most 2^30, so no node sum
+// can overflow.  A contribution goes in as its nearest integer plus its
+// rounding residual in units of 2^-22 (a second 32-bit sum: at most 512
+// residuals of at most 2^21), so a node keeps B 2^-53 absolutely: nodes that
+// only the edges of a few stencils reach, with masses many orders below the
+// part's, still get float-like relative precision.  The tile goes out as
+// floats (hi + lo 2^-22 combined in FP64) with one float4 atomic per touched node.
+//
+// Lanes must hit different nodes in each shared add, so the part's particles
+// are first binned by cell and handed out round by round (round r: the
+// (r+1)-th particle of every cell that has one), cells in index order.
+// ---------------------------------------------------------------------------
+template<int T> struct P2GSmem {
+    int q[4][PTN];                        // fixed-point tile: mass, momentum x, y, z (units of 1 / scale)
+    int ql[4][PTN];                       // the rounding residuals, units of 2^-22 / scale
+    uint32_t ccount[64];                  // particles per cell of the part
+    uint32_t rsize[T];                    // particles in round r
+    uint32_t roff[T];                     // first list position of round r
+    unsigned long long rmask[T];          // cells with more than r particles
+    uint32_t list[T];                     // the part's sorted positions, round by round
+    float bound[4];
+    float scale[4];
+    int maxc;
+    int scene;
+    uint4 work;
+    SceneDev sc;
 };
 
-__device__ __forceinline__ void pair_prep(const FastArgs& a, const SceneDev& sc, uint32_t j, bool odd, PairPrep& P)
+// Largest |node value| of a particle over its 27 nodes, per quantity.
+__device__ __forceinline__ void factor_bounds(const P2GFactors& P, float* bnd)
 {
-    P.cell = (int)(a.sorted_keys[j] & 63u);
-    P2GFactors G;
-    particle_factors(a, sc, j, G);
+    const float mx = fmaxf(P.w[0], fmaxf(P.w[1], P.w[2]));
+    const float my = fmaxf(P.w[3], fmaxf(P.w[4], P.w[5]));
+    const float mz = fmaxf(P.w[6], fmaxf(P.w[7], P.w[8]));
+    bnd[0] = fmaxf(P.mwx[0], fmaxf(P.mwx[1], P.mwx[2])) * my * mz;
 #pragma unroll
-    for(int k = 0; k < 9; k++) P.w[k] = G.w[k];
-    PairSlot qm;
+    for(int r = 0; r < 3; r++) {
+        const PairSlot& s = P.q[r];
+        const float hx = fmaxf(fabsf(s.Hx[0]), fmaxf(fabsf(s.Hx[1]), fabsf(s.Hx[2])));
+        const float hy = fmaxf(fabsf(s.Hy[0]), fmaxf(fabsf(s.Hy[1]), fabsf(s.Hy[2])));
+        const float hz = fmaxf(fabsf(s.Hz[0]), fmaxf(fabsf(s.Hz[1]), fabsf(s.Hz[2])));
+        bnd[1 + r] = hx * my * mz + mx * hy * mz + mx * my * hz;
+    }
+}
+
+template<int T> __global__ void __launch_bounds__(T, 1024 / T) k_p2g(FastArgs a)
+{
+    constexpr int NW = T / 32;
+    __shared__ P2GSmem<T> S;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nwork = min(a.ctr[CNT_CHUNKS], a.chunk_cap);
+    if(threadIdx.x == 0) S.scene = -1;
+    for(;;) {
+        __syncthreads();
+        if(threadIdx.x == 0) {
+            const uint32_t w = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+            S.work = w < nwork ? a.chunks[w] : make_uint4(SENTINEL, 0u, 0u, 0u);
+            S.maxc = 0;
+        }
+        for(int t = threadIdx.x; t < 4 * PTN; t += T) { (&S.q[0][0])[t] = 0; (&S.ql[0][0])[t] = 0; }
+        if(threadIdx.x < 64) S.ccount[threadIdx.x] = 0u;
+        if(threadIdx.x < 4) S.bound[threadIdx.x] = 0.f;
+        __syncthreads();
+        const uint4 wk = S.work;
+        if(wk.x == SENTINEL) break;
+        const uint32_t b = wk.x, part = wk.y, parts = wk.z;
+        const int sid = a.block_scene[b];
+        if(sid != S.scene) stage_scene(a, sid, &S.sc);
+        const uint32_t s = a.bstart[b], e = a.bend[b];
+        const uint32_t cnt = e - s > part ? min((e - s - part + parts - 1) / parts, (uint32_t)T) : 0u;
+        // bin the part's particles by cell
+        const bool mine = threadIdx.x < cnt;
+        uint32_t j = 0, cell = 0, r = 0;
+        if(mine) {
+            j = s + part + threadIdx.x * parts;
+            cell = a.sorted_keys[j] & 63u;
+            r = atomicAdd(&S.ccount[cell], 1u);
+        }
+        __syncthreads();
+        if(threadIdx.x == 0) S.scene = sid;
+        if(threadIdx.x < 64) {
+            uint32_t c = S.ccount[threadIdx.x];
 #pragma unroll
-    for(int o = 0; o < 3; o++) { qm.Hx[o] = G.mwx[o]; qm.Hy[o] = 0.f; qm.Hz[o] = 0.f; }
-    const PairSlot* q = G.q;
-    // even lane keeps (mass, x) and sends (y, z); odd lane the other way round
+            for(int o = 16; o; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
+            if(lane == 0) atomicMax(&S.maxc, (int)c);
+        }
+        __syncthreads();
+        const int maxc = S.maxc;
+        for(int rr = warp; rr < maxc; rr += NW) {
+            const unsigned lo = __ballot_sync(0xffffffffu, S.ccount[lane] > (uint32_t)rr);
+            const unsigned hi = __ballot_sync(0xffffffffu, S.ccount[lane + 32] > (uint32_t)rr);
+            if(lane == 0) {
+                S.rmask[rr] = lo | ((unsigned long long)hi << 32);
+                S.rsize[rr] = __popc(lo) + __popc(hi);
+            }
+        }
+        __syncthreads();
+        if(warp == 0) {   // exclusive scan of the round sizes
+            uint32_t carry = 0;
+            for(int r0 = 0; r0 < maxc; r0 += 32) {
+                const uint32_t x = r0 + lane < maxc ? S.rsize[r0 + lane] : 0u;
+                const uint32_t xi = warp_incl_scan(x);
+                if(r0 + lane < maxc) S.roff[r0 + lane] = carry + xi - x;
+                carry += __shfl_sync(0xffffffffu, xi, 31);
+            }
+        }
+        __syncthreads();
+        if(mine) S.list[S.roff[r] + __popcll(S.rmask[r] & ((1ull << cell) - 1ull))] = j;
+        __syncthreads();
+        // this thread's particle: factors and the bound of its node values
+        P2GFactors P;
+        float bnd[4] = {0.f, 0.f, 0.f, 0.f};
+        int pc = 0;
+        if(mine) {
+            const uint32_t jj = S.list[threadIdx.x];
+            pc = (int)(a.sorted_keys[jj] & 63u);
+            particle_factors(a, S.sc, jj, P);
+            factor_bounds(P, bnd);
+        }
+#pragma unroll
+        for(int q = 0; q < 4; q++) {
+            float v = bnd[q];
+#pragma unroll
+            for(int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if(lane == 0 && v != 0.f) atomicAdd(&S.bound[q], v);
+        }
+        __syncthreads();
+        if(threadIdx.x < 4) {
+            const float B = S.bound[threadIdx.x];
+            float sc = 0.f;
+            if(!isfinite(B)) atomicOr(a.flags, MPM_FLAG_NAN);
+            else if(B > 0.f) {
+                int ex;
+                frexpf(B, &ex);                      // B < 2^ex
+                sc = ldexpf(1.f, 30 - max(ex, -90));
+            }
+            S.scale[threadIdx.x] = sc;
+        }
+        __syncthreads();
+        if(mine) {
+            const float s0 = S.scale[0], s1 = S.scale[1], s2 = S.scale[2], s3 = S.scale[3];
+            const int t0 = ptile(pc >> 4, (pc >> 2) & 3, pc & 3);
+            // nearest integer and the residual's 2^-22 units: y - rint(y) is exact in float
+            auto add = [&](int q, int t, float y) {
+                const float h = rintf(y);
+                atomicAdd(&S.q[q][t], (int)h);
+                atomicAdd(&S.ql[q][t], __float2int_rn((y - h) * 4194304.f));
+            };
+            factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
+                const int t = t0 + ptile(ii, jj, kk);
+                add(0, t, m * s0);
+                add(1, t, px * s1);
+                add(2, t, py * s2);
+                add(3, t, pz * s3);
+            });
+        }
+        __syncthreads();
+        // out: one float4 atomic per touched node, and the node blocks for the grid update
+        const SceneDev& sc = S.sc;
+        int bx, by, bz;
+        block_coords(sc, b - sc.block_base, bx, by, bz);
+        double inv[4];
+#pragma unroll
+        for(int q = 0; q < 4; q++) inv[q] = S.scale[q] > 0.f ? 1.0 / S.scale[q] : 0.0;
+        for(int t = threadIdx.x; t < TN; t += T) {
+            const int tx = t / (TE * TE), ty = (t / TE) % TE, tz = t % TE, u = ptile(tx, ty, tz);
+            float v[4];
+            bool any = false;
+#pragma unroll
+            for(int q = 0; q < 4; q++) {
+                const int hi = S.q[q][u], lo = S.ql[q][u];
+                any |= (hi | lo) != 0;
+                v[q] = (float)(((double)hi + (double)lo * 2.384185791015625e-07) * inv[q]);
+            }
+            if(any)
+                atomicAdd(&a.acc[node_index(sc, 4 * bx + tx, 4 * by + ty, 4 * bz + tz)], make_float4(v[1], v[2], v[3], v[0]));
+        }
+        if(threadIdx.x < 8) {
+            const int nx = bx + (threadIdx.x >> 2), ny = by + ((threadIdx.x >> 1) & 1), nz = bz + (threadIdx.x & 1);
+            const uint32_t nb = sc.nb_base + ((uint32_t)nx * sc.NN[1] + ny) * sc.NN[2] + nz;
+            if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.ctr[CNT_NODE_BLOCKS], 1u)] = nb;
+        }
+    }
+    p2g_finish(a, &S.maxc);
+}
+
+// ---------------------------------------------------------------------------
+// P2G by lane groups: a work item is a contiguous part of a block (at most
+// 4 T particles for T threads), binned by cell in shared memory; groups of 4
+// lanes walk balanced ranges of the cell-sorted part.  Per round each lane of
+// a group prepares one particle (stress, weights, the separable factors of
+// all four node quantities); in four rotating sub-steps lane k takes from the
+// group's lane (k + p) mod 4 that particle's weights and the factors of
+// quantity k (mass, momentum x, y, z) and adds its 27 node values into 27
+// registers.  A lane writes its registers to the shared float tile only when
+// its particles move to another cell, so a cell of ~8 particles costs 27
+// shared atomics per quantity instead of 27 per particle; the tile goes out
+// with one float4 atomic per touched node.
+// ---------------------------------------------------------------------------
+template<int T> struct P2GGroupSmem {
+    float q[4][PTN];                      // node sums: mass, momentum + dt force x, y, z
+    uint32_t ccount[64], cstart[64];
+    uint32_t list[4 * T];                 // the part's sorted positions, cell by cell
+    uint8_t lcell[4 * T];
+    int scene;
+    uint4 work;
+};
+
+// The 9 separable factors of quantity `qn` (0 mass, 1-3 momentum) of P.
+__device__ __forceinline__ void quantity_factors(const P2GFactors& P, int qn, float* h)
+{
 #pragma unroll
     for(int o = 0; o < 3; o++) {
-        P.keep0.Hx[o] = odd ? q[1].Hx[o] : qm.Hx[o]; P.send0.Hx[o] = odd ? qm.Hx[o] : q[1].Hx[o];
-        P.keep0.Hy[o] = odd ? q[1].Hy[o] : 0.f;      P.send0.Hy[o] = odd ? 0.f : q[1].Hy[o];
-        P.keep0.Hz[o] = odd ? q[1].Hz[o] : 0.f;      P.send0.Hz[o] = odd ? 0.f : q[1].Hz[o];
-        P.keep1.Hx[o] = odd ? q[2].Hx[o] : q[0].Hx[o]; P.send1.Hx[o] = odd ? q[0].Hx[o] : q[2].Hx[o];
-        P.keep1.Hy[o] = odd ? q[2].Hy[o] : q[0].Hy[o]; P.send1.Hy[o] = odd ? q[0].Hy[o] : q[2].Hy[o];
-        P.keep1.Hz[o] = odd ? q[2].Hz[o] : q[0].Hz[o]; P.send1.Hz[o] = odd ? q[0].Hz[o] : q[2].Hz[o];
+        const float m = P.mwx[o];
+        const float x0 = P.q[0].Hx[o], x1 = P.q[1].Hx[o], x2 = P.q[2].Hx[o];
+        const float y0 = P.q[0].Hy[o], y1 = P.q[1].Hy[o], y2 = P.q[2].Hy[o];
+        const float z0 = P.q[0].Hz[o], z1 = P.q[1].Hz[o], z2 = P.q[2].Hz[o];
+        h[o] = qn == 0 ? m : (qn == 1 ? x0 : (qn == 2 ? x1 : x2));
+        h[3 + o] = qn == 0 ? 0.f : (qn == 1 ? y0 : (qn == 2 ? y1 : y2));
+        h[6 + o] = qn == 0 ? 0.f : (qn == 1 ? z0 : (qn == 2 ? z1 : z2));
     }
 }
 
-
-__device__ __forceinline__ void pair_accumulate(const float* w, const PairSlot& q0, const PairSlot& q1, float* acc0, float* acc1)
+template<int T> __global__ void __launch_bounds__(T, 512 / T) k_p2g_groups(FastArgs a)
 {
-#pragma unroll
-    for(int ii = 0; ii < 3; ii++)
-#pragma unroll
-        for(int jj = 0; jj < 3; jj++) {
-            const float wxy = w[ii] * w[3 + jj];
-            const float A0 = fmaf(q0.Hx[ii], w[3 + jj], w[ii] * q0.Hy[jj]);
-            const float A1 = fmaf(q1.Hx[ii], w[3 + jj], w[ii] * q1.Hy[jj]);
-#pragma unroll
-            for(int kk = 0; kk < 3; kk++) {
-                const int q = (ii * 3 + jj) * 3 + kk;
-                acc0[q] = fmaf(A0, w[6 + kk], fmaf(wxy, q0.Hz[kk], acc0[q]));
-                acc1[q] = fmaf(A1, w[6 + kk], fmaf(wxy, q1.Hz[kk], acc1[q]));
-            }
-        }
-}
-
-__device__ __forceinline__ void pair_flush(int cell, float* out0, float* out1, float* acc0, float* acc1)
-{
-    const int t0 = ptile(cell >> 4, (cell >> 2) & 3, cell & 3);
-#pragma unroll
-    for(int q = 0; q < 27; q++) {
-        const int t = t0 + ptile(q / 9, (q / 3) % 3, q % 3);
-        atomicAdd(&out0[t], acc0[q]);
-        atomicAdd(&out1[t], acc1[q]);
-        acc0[q] = 0.f;
-        acc1[q] = 0.f;
-    }
-}
-
-// P2G variant 1: one thread per particle, handed out round-robin over the
-// cells of the block (lane c of a round takes that cell's next particle), so
-// the lanes of one shared atomic hit different nodes.  No accumulators: the
-// 27 node values of all four quantities go straight to the shared tile, so
-// the kernel needs few registers and keeps many warps in flight, at the price
-// of four shared atomics per node.
-
-// One particle of the interleaved variant: its 27 x 4 node values straight to the tile.
-__device__ __forceinline__ void interleaved_particle(const FastArgs& a, P2GTile& T, uint32_t j, uint32_t c)
-{
-    P2GFactors P;
-    particle_factors(a, T.sc, j, P);
-    const int t0 = ptile(c >> 4, (c >> 2) & 3, c & 3);
-    factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
-        const int t = t0 + ptile(ii, jj, kk);
-        atomicAdd(&T.m[t], m);
-        atomicAdd(&T.x[t], px);
-        atomicAdd(&T.y[t], py);
-        atomicAdd(&T.z[t], pz);
-    });
-}
-
-template<int THREADS> __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_p2g_interleaved(FastArgs a)
-{
-    __shared__ P2GTile T;
-    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
-        const uint32_t b = a.active[w];
-        p2g_begin(a, T, b);
-        const uint32_t s = a.bstart[b], slots = T.maxc * 64u;
-        for(uint32_t q = threadIdx.x; q < slots; q += THREADS) {
-            const uint32_t c = q & 63u, r = q >> 6;
-            if(r < T.ccount[c]) interleaved_particle(a, T, s + T.cstart[c] + r, c);
-        }
-        p2g_end(a, T, b - T.sc.block_base);
-    }
-    p2g_finish(a, &T.work);
-}
-
-// Swap with the other lane of the pair.  Only the pair takes part: pairs of
-// one warp may run different trip counts.
-__device__ __forceinline__ unsigned pair_mask() { return 3u << ((threadIdx.x & 31) & ~1u); }
-__device__ __forceinline__ float shfl1(float v) { return __shfl_xor_sync(pair_mask(), v, 1); }
-
-template<int THREADS> __global__ void __launch_bounds__(THREADS, 512 / THREADS) k_p2g_pairx(FastArgs a)
-{
-    __shared__ P2GTile T;
-    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    const bool odd = threadIdx.x & 1;
-    const int pair = threadIdx.x >> 1;
-    constexpr int kPairs = THREADS / 2;
-    for(int w = next_work(&a.counters[CNT_P2G_WORK], &T.work); w < (int)nblocks; w = next_work(&a.counters[CNT_P2G_WORK], &T.work)) {
-        const uint32_t b = a.active[w];
-        stage_scene(a, a.block_scene[b], &T.sc);
-        for(int t = threadIdx.x; t < PTN; t += THREADS) { T.m[t] = 0; T.x[t] = 0; T.y[t] = 0; T.z[t] = 0; }
+    constexpr int G = T / 4;              // lane groups
+    __shared__ P2GGroupSmem<T> S;
+    __shared__ SceneDev s_sc;
+    const int lane = threadIdx.x & 31, k = threadIdx.x & 3, g = threadIdx.x >> 2;
+    const unsigned gmask = 0xfu << (lane & ~3);
+    const uint32_t nwork = min(a.ctr[CNT_CHUNKS], a.chunk_cap);
+    if(threadIdx.x == 0) S.scene = -1;
+    for(;;) {
         __syncthreads();
-        const SceneDev& sc = T.sc;
-        const uint32_t s = a.bstart[b], e = a.bend[b];
-        // ranges of an even length, so both lanes of a pair always have a particle but the last
-        const uint32_t per = ((e - s + kPairs - 1) / kPairs + 1) & ~1u;
-        const uint32_t j0 = s + pair * per, j1 = min(j0 + per, e);
-        float* const out0 = odd ? T.y : T.m;
-        float* const out1 = odd ? T.z : T.x;
-        float acc0[27], acc1[27];
+        if(threadIdx.x == 0) {
+            const uint32_t w = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+            S.work = w < nwork ? a.chunks[w] : make_uint4(SENTINEL, 0u, 0u, 0u);
+        }
+        for(int t = threadIdx.x; t < 4 * PTN; t += T) (&S.q[0][0])[t] = 0.f;
+        if(threadIdx.x < 64) S.ccount[threadIdx.x] = 0u;
+        __syncthreads();
+        const uint4 wk = S.work;
+        if(wk.x == SENTINEL) break;
+        const uint32_t b = wk.x, part = wk.y, parts = wk.z;
+        const int sid = a.block_scene[b];
+        if(sid != S.scene) stage_scene(a, sid, &s_sc);
+        const uint32_t s = a.bstart[b], c = a.bend[b] - s;
+        const uint32_t j0 = s + (uint32_t)((uint64_t)c * part / parts);
+        const uint32_t cnt = min((uint32_t)((uint64_t)c * (part + 1) / parts) + s - j0, (uint32_t)(4 * T));
+        // bin by cell: up to 4 particles per thread
+        uint32_t cl[4], rk[4];
 #pragma unroll
-        for(int q = 0; q < 27; q++) { acc0[q] = 0.f; acc1[q] = 0.f; }
-        int cell = -1;
-        // the pair's lanes run the same trip count: j0 and j1 are shared
-        for(uint32_t j = j0; j < j1; j += 2) {
-            const bool have1 = j + 1 < j1;
-            PairPrep P;
-            const bool mine = !odd || have1;
-            if(mine) pair_prep(a, sc, j + (odd ? 1u : 0u), odd, P);
-            else {
+        for(int u = 0; u < 4; u++) {
+            const uint32_t i = threadIdx.x + u * T;
+            cl[u] = i < cnt ? a.sorted_keys[j0 + i] & 63u : 0u;
+            rk[u] = i < cnt ? atomicAdd(&S.ccount[cl[u]], 1u) : 0u;
+        }
+        __syncthreads();
+        if(threadIdx.x == 0) S.scene = sid;
+        if(threadIdx.x < 32) {   // exclusive scan of the 64 cell counts
+            const uint32_t c0 = S.ccount[2 * lane], c1 = S.ccount[2 * lane + 1];
+            const uint32_t x = warp_incl_scan(c0 + c1);
+            S.cstart[2 * lane] = x - c0 - c1;
+            S.cstart[2 * lane + 1] = x - c1;
+        }
+        __syncthreads();
 #pragma unroll
-                for(int k = 0; k < 9; k++) P.w[k] = 0.f;
-                P.cell = -1;
-            }
-            // swap: partner's cell, weights and the factors of my quantities
-            PairPrep R;
-            R.cell = __shfl_xor_sync(pair_mask(), P.cell, 1);
-#pragma unroll
-            for(int k = 0; k < 9; k++) R.w[k] = shfl1(P.w[k]);
-#pragma unroll
-            for(int o = 0; o < 3; o++) {
-                R.keep0.Hx[o] = shfl1(P.send0.Hx[o]); R.keep0.Hy[o] = shfl1(P.send0.Hy[o]); R.keep0.Hz[o] = shfl1(P.send0.Hz[o]);
-                R.keep1.Hx[o] = shfl1(P.send1.Hx[o]); R.keep1.Hy[o] = shfl1(P.send1.Hy[o]); R.keep1.Hz[o] = shfl1(P.send1.Hz[o]);
-            }
-            // particle j first (the even lane's), then j + 1 (the odd lane's)
-            const int c_first = odd ? R.cell : P.cell, c_second = odd ? P.cell : R.cell;
-            {
-                if(c_first != cell) {
-                    if(cell >= 0) pair_flush(cell, out0, out1, acc0, acc1);
-                    cell = c_first;
-                }
-                float wf[9];
-#pragma unroll
-                for(int k = 0; k < 9; k++) wf[k] = odd ? R.w[k] : P.w[k];
-                PairSlot f0, f1;
-#pragma unroll
-                for(int o = 0; o < 3; o++) {
-                    f0.Hx[o] = odd ? R.keep0.Hx[o] : P.keep0.Hx[o]; f0.Hy[o] = odd ? R.keep0.Hy[o] : P.keep0.Hy[o];
-                    f0.Hz[o] = odd ? R.keep0.Hz[o] : P.keep0.Hz[o];
-                    f1.Hx[o] = odd ? R.keep1.Hx[o] : P.keep1.Hx[o]; f1.Hy[o] = odd ? R.keep1.Hy[o] : P.keep1.Hy[o];
-                    f1.Hz[o] = odd ? R.keep1.Hz[o] : P.keep1.Hz[o];
-                }
-                pair_accumulate(wf, f0, f1, acc0, acc1);
-            }
-            if(have1) {
-                if(c_second != cell) {
-                    pair_flush(cell, out0, out1, acc0, acc1);
-                    cell = c_second;
-                }
-                float ws[9];
-#pragma unroll
-                for(int k = 0; k < 9; k++) ws[k] = odd ? P.w[k] : R.w[k];
-                PairSlot g0, g1;
-#pragma unroll
-                for(int o = 0; o < 3; o++) {
-                    g0.Hx[o] = odd ? P.keep0.Hx[o] : R.keep0.Hx[o]; g0.Hy[o] = odd ? P.keep0.Hy[o] : R.keep0.Hy[o];
-                    g0.Hz[o] = odd ? P.keep0.Hz[o] : R.keep0.Hz[o];
-                    g1.Hx[o] = odd ? P.keep1.Hx[o] : R.keep1.Hx[o]; g1.Hy[o] = odd ? P.keep1.Hy[o] : R.keep1.Hy[o];
-                    g1.Hz[o] = odd ? P.keep1.Hz[o] : R.keep1.Hz[o];
-                }
-                pair_accumulate(ws, g0, g1, acc0, acc1);
+        for(int u = 0; u < 4; u++) {
+            const uint32_t i = threadIdx.x + u * T;
+            if(i < cnt) {
+                const uint32_t pos = S.cstart[cl[u]] + rk[u];
+                S.list[pos] = j0 + i;
+                S.lcell[pos] = (uint8_t)cl[u];
             }
         }
-        if(cell >= 0) {
+        __syncthreads();
+        // this group's balanced range of the cell-sorted part
+        const uint32_t r0 = (uint32_t)((uint64_t)cnt * g / G), r1 = (uint32_t)((uint64_t)cnt * (g + 1) / G);
+        const SceneDev& sc = s_sc;
+        float acc[27];
+#pragma unroll
+        for(int q = 0; q < 27; q++) acc[q] = 0.f;
+        int cell = -1;
+        float* const tq = S.q[k];
+        auto flush = [&]() {
             const int t0 = ptile(cell >> 4, (cell >> 2) & 3, cell & 3);
 #pragma unroll
             for(int q = 0; q < 27; q++) {
-                const int t = t0 + ptile(q / 9, (q / 3) % 3, q % 3);
-                atomicAdd(&out0[t], acc0[q]);
-                atomicAdd(&out1[t], acc1[q]);
+                atomicAdd(&tq[t0 + ptile(q / 9, (q / 3) % 3, q % 3)], acc[q]);
+                acc[q] = 0.f;
+            }
+        };
+        for(uint32_t rb = r0; rb < r1; rb += 4) {   // a round: one particle per lane of the group
+            const uint32_t mine = rb + k;
+            P2GFactors P;
+            int pc = -1;
+            if(mine < r1) {
+                pc = S.lcell[mine];
+                particle_factors(a, sc, S.list[mine], P);
+            } else {
+#pragma unroll
+                for(int e = 0; e < 9; e++) P.w[e] = 0.f;
+#pragma unroll
+                for(int o = 0; o < 3; o++) {
+                    P.mwx[o] = 0.f;
+#pragma unroll
+                    for(int r = 0; r < 3; r++) P.q[r].Hx[o] = P.q[r].Hy[o] = P.q[r].Hz[o] = 0.f;
+                }
+            }
+#pragma unroll
+            for(int p = 0; p < 4; p++) {
+                // lane k reads lane (k + p) mod 4, which sends the factors of quantity (its index - p) mod 4
+                const int src = (lane & ~3) | ((k + p) & 3);
+                float h[9];
+                quantity_factors(P, (k - p) & 3, h);
+                float w[9], f[9];
+#pragma unroll
+                for(int e = 0; e < 9; e++) {
+                    w[e] = __shfl_sync(gmask, P.w[e], src);
+                    f[e] = __shfl_sync(gmask, h[e], src);
+                }
+                const int rc = __shfl_sync(gmask, pc, src);
+                if(rc < 0) continue;                  // past the group's range
+                if(rc != cell) {
+                    if(cell >= 0) flush();
+                    cell = rc;
+                }
+                // node (i, j, l): Hx[i] wy[j] wz[l] + wx[i] Hy[j] wz[l] + wx[i] wy[j] Hz[l]
+#pragma unroll
+                for(int ii = 0; ii < 3; ii++)
+#pragma unroll
+                    for(int jj = 0; jj < 3; jj++) {
+                        const float wxy = w[ii] * w[3 + jj];
+                        const float A = fmaf(f[ii], w[3 + jj], w[ii] * f[3 + jj]);
+#pragma unroll
+                        for(int ll = 0; ll < 3; ll++) {
+                            const int q = (ii * 3 + jj) * 3 + ll;
+                            acc[q] = fmaf(A, w[6 + ll], fmaf(wxy, f[6 + ll], acc[q]));
+                        }
+                    }
             }
         }
-        p2g_end(a, T, b - sc.block_base);
+        if(cell >= 0) flush();
+        __syncthreads();
+        // out: one float4 atomic per touched node, and the node blocks for the grid update
+        int bx, by, bz;
+        block_coords(sc, b - sc.block_base, bx, by, bz);
+        for(int t = threadIdx.x; t < TN; t += T) {
+            const int tx = t / (TE * TE), ty = (t / TE) % TE, tz = t % TE, u = ptile(tx, ty, tz);
+            const float m = S.q[0][u];
+            if(m != 0.f)
+                atomicAdd(&a.acc[node_index(sc, 4 * bx + tx, 4 * by + ty, 4 * bz + tz)],
+                          make_float4(S.q[1][u], S.q[2][u], S.q[3][u], m));
+        }
+        if(threadIdx.x < 8) {
+            const int nx = bx + (threadIdx.x >> 2), ny = by + ((threadIdx.x >> 1) & 1), nz = bz + (threadIdx.x & 1);
+            const uint32_t nb = sc.nb_base + ((uint32_t)nx * sc.NN[1] + ny) * sc.NN[2] + nz;
+            if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.ctr[CNT_NODE_BLOCKS], 1u)] = nb;
+        }
     }
-    p2g_finish(a, &T.work);
+    __shared__ int s_last;
+    p2g_finish(a, &s_last);
 }
 
 // One thread per node of the listed node blocks (4^3 nodes each, 64
 // consecutive threads), grid-stride with CTA-uniform trip counts.  Each group
 // of 64 threads (one node block) copies its scene record and collision
-// objects, rounded to float, into shared memory before use; a one-scene
-// handle does that once per CTA.
+// objects into shared memory before use; a one-scene handle does that once
+// per CTA.  Nodes within reach of an object are collided in FP64
+// (collide_node).
 __global__ void __launch_bounds__(256) k_grid(FastArgs a)
 {
     constexpr int kGroups = 4;   // node blocks per CTA pass
     __shared__ SceneDev s_sc[kGroups];
-    __shared__ DevObjectF s_obj[kGroups][MPM_MAX_OBJECTS];
+    __shared__ DevObject s_obj[kGroups][MPM_MAX_OBJECTS];
     __shared__ int s_scene[kGroups];
     const int grp = threadIdx.x >> 6, t = threadIdx.x & 63;
-    const uint64_t total = (uint64_t)a.counters[CNT_NODE_BLOCKS] * 64u;
+    const uint64_t total = (uint64_t)a.ctr[CNT_NODE_BLOCKS] * 64u;
     const uint64_t stride = (uint64_t)gridDim.x * 256u;
     if(threadIdx.x < kGroups) s_scene[threadIdx.x] = -1;
     __syncthreads();
@@ -935,15 +1199,7 @@ __global__ void __launch_bounds__(256) k_grid(FastArgs a)
             constexpr int words = (int)(sizeof(SceneDev) / 4);
             if(t < words) ((uint32_t*)&s_sc[grp])[t] = ((const uint32_t*)(a.scenes + scene))[t];
             const SceneDev& gs = a.scenes[scene];
-            if(t < gs.nobj) {
-                const DevObject& o = a.objs[gs.obj_begin + t];
-                DevObjectF& f = s_obj[grp][t];
-                f.kind = o.kind;
-                f.type = o.type;
-                f.friction = (float)o.friction;
-#pragma unroll
-                for(int k = 0; k < 3; k++) { f.a[k] = (float)o.a[k]; f.b[k] = (float)o.b[k]; }
-            }
+            if(t < gs.nobj) s_obj[grp][t] = a.objs[gs.obj_begin + t];
         }
         __syncthreads();
         if(t == 0 && live) s_scene[grp] = scene;
@@ -982,7 +1238,7 @@ __global__ void __launch_bounds__(256) k_grid(FastArgs a)
 }
 
 // G2P, one thread per particle in sorted order (coalesced).  The tile of
-// (v_new, v_fric) is staged in shared memory; the sums over the 27 nodes are
+// (v_new, v_fric) is copied to shared memory by TMA; the sums over the 27 nodes are
 // taken separably (z first, then y, then x), so each node costs two 16-byte
 // shared loads and twelve FMAs:
 //   V' = sum w vn,  G = sum vn g^T,  Vf = sum w vf,  Bv = sum w vf (Z - X)^T.
@@ -991,22 +1247,6 @@ __global__ void __launch_bounds__(256) k_grid(FastArgs a)
 // is non-zero only where the grid update changed v_fric against v_new (nodes
 // that met a collision object), so it is summed only for tiles holding such
 // nodes.
-// Stage the 6^3 tile of (v_new, v_fric, mass) of a particle block; true when
-// some node's friction velocity differs from its velocity (collided nodes).
-__device__ __forceinline__ bool g2p_stage(const FastArgs& a, const SceneDev& sc, float4* tv, int ox, int oy, int oz, int threads)
-{
-    int differs = 0;
-    for(int t = threadIdx.x; t < TN; t += threads) {
-        int qx = ox + t / (TE * TE), qy = oy + (t / TE) % TE, qz = oz + t % TE;
-        int64_t q = node_index(sc, qx, qy, qz);
-        float4 p0 = a.vel[2 * q], p1 = a.vel[2 * q + 1];
-        tv[2 * t] = p0;
-        tv[2 * t + 1] = p1;
-        differs |= (p0.w != p0.x) | (p1.x != p0.y) | (p1.y != p0.z);
-    }
-    return __syncthreads_or(differs) != 0;
-}
-
 // G2P of the particle at sorted position j against the staged tile `tv`
 // (origin node (ox, oy, oz)): writes its new state to slot j of the other
 // buffer and its next key; also returns it in `out`.
@@ -1315,52 +1555,165 @@ __device__ __forceinline__ void g2p_particle(const FastArgs& a, const SceneDev& 
     out.ok = ok;
 }
 
+// ---------------------------------------------------------------------------
+// G2P tiles by TMA.  Every scene's grid of (v_new, v_fric, mass) nodes, 8
+// floats each, is described by a 4D tensor map {8 floats, z, y, x} over this
+// GPU's own grid allocation (fast_setup_scenes encodes one per scene); a
+// work item's 6^3-node tile is one cp.async.bulk.tensor copy into shared
+// memory, completing on an mbarrier.  The copy of the next work item's tile
+// is issued before the current item is computed (two tile buffers), so its
+// latency hides behind the current particles' gather and arithmetic.
+// ---------------------------------------------------------------------------
+constexpr uint32_t TILE_BYTES = TN * 32;   // 6^3 nodes x 8 floats
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Make barrier initialisation visible to the asynchronous (TMA) proxy.
+__device__ __forceinline__ void fence_async_shared()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return done != 0;
+}
+
+// Bounded wait for phase `parity` of `bar`; false when it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    for(uint32_t spin = 0; spin < mpm_sort::kSpinLimit; spin++)
+        if(mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// One tile: box {8, 6, 6, 6} at node (ox, oy, oz) of the scene's map, into `dst`
+// (128-byte aligned shared memory), completing `bar`'s current phase.
+__device__ __forceinline__ void tma_tile(float4* dst, const CUtensorMap* map, uint64_t* bar, int ox, int oy, int oz)
+{
+    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%3, %4, %5, %6}], [%2];"
+                 :: "r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(0), "r"(oz), "r"(oy), "r"(ox)
+                 : "memory");
+}
+
+// Thread 0: take the next work item and start its tile copy into `dst`.
+__device__ __forceinline__ uint4 g2p_take(const FastArgs& a, uint32_t nwork, float4* dst, uint64_t* bar)
+{
+    const uint32_t w = atomicAdd(&a.ctr[CNT_G2P_WORK], 1u);
+    if(w >= nwork) return make_uint4(SENTINEL, 0u, 0u, 0u);
+    const uint4 wk = a.chunks[w];
+    const int sid = a.block_scene[wk.x];
+    const SceneDev& sc = a.scenes[sid];
+    int bx, by, bz;
+    block_coords(sc, wk.x - sc.block_base, bx, by, bz);
+    fence_async_shared();   // the CTA's reads of this buffer come before the copy's writes
+    mbar_expect_tx(bar, TILE_BYTES);
+    tma_tile(dst, a.tmaps + sid, bar, 4 * bx, 4 * by, 4 * bz);
+    return wk;
+}
+
 template<int THREADS, int PK> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
 {
-    __shared__ float4 tv[2 * TN];
-    __shared__ int s_work;
+    __shared__ alignas(128) float4 tv[2][2 * TN];
+    __shared__ alignas(8) uint64_t s_bar[2];
+    __shared__ uint4 s_work[2];
+    __shared__ int s_scene;
     __shared__ SceneDev s_sc;
-    // digit histograms of the keys this CTA writes (for the next sort)
-    __shared__ uint32_t s_hist[mpm_sort::kMaxPasses][mpm_sort::kRadix];
-    __shared__ uint32_t s_stay;
-    for(int i = threadIdx.x; i < mpm_sort::kMaxPasses * mpm_sort::kRadix; i += THREADS) (&s_hist[0][0])[i] = 0;
-    // invalid particles, copied to the tail by k_ranges, keep sentinel keys
-    if(blockIdx.x == 0 && threadIdx.x == 0)
-        mpm_sort::hist_add_sentinels(a.sort_scratch, (uint32_t)(a.n - a.counters[CNT_ACTIVE_PARTICLES]), a.key_bits);
-    const uint32_t nblocks = a.counters[CNT_ACTIVE_BLOCKS];
-    for(int w = next_work(&a.counters[CNT_G2P_WORK], &s_work); w < (int)nblocks; w = next_work(&a.counters[CNT_G2P_WORK], &s_work)) {
-        const uint32_t b = a.active[w];
-        stage_scene(a, a.block_scene[b], &s_sc);
-        __syncthreads();
+    // where this part's particles go next substep: per direction (k_bins, k_route)
+    __shared__ uint32_t s_dc[32];
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwork = min(a.ctr[CNT_CHUNKS], a.chunk_cap);
+    if(threadIdx.x < 32) s_dc[threadIdx.x] = 0u;
+    if(threadIdx.x == 0) {
+        s_scene = -1;
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        fence_async_shared();
+        s_work[0] = g2p_take(a, nwork, tv[0], &s_bar[0]);
+    }
+    __syncthreads();
+    uint32_t issued = 1u;               // bit b: a copy into buffer b is in flight (thread 0's view)
+    bool failed = false;
+    for(int k = 0;; k++) {
+        const int buf = k & 1;
+        const uint4 wk = s_work[buf];
+        if(wk.x == SENTINEL) break;
+        if(threadIdx.x == 0) {          // the next item's tile copy, overlapping this item
+            s_work[buf ^ 1] = g2p_take(a, nwork, tv[buf ^ 1], &s_bar[buf ^ 1]);
+            issued = (issued & ~(1u << buf)) | (s_work[buf ^ 1].x != SENTINEL ? 1u << (buf ^ 1) : 0u);
+        }
+        const uint32_t b = wk.x, part = wk.y, parts = wk.z;
+        const int sid = a.block_scene[b];
+        if(sid != s_scene) {
+            stage_scene(a, sid, &s_sc);
+            __syncthreads();
+            if(threadIdx.x == 0) s_scene = sid;
+        }
         const SceneDev& sc = s_sc;
         int bx, by, bz;
         block_coords(sc, b - sc.block_base, bx, by, bz);
         const int ox = 4 * bx, oy = 4 * by, oz = 4 * bz;
-        if(threadIdx.x == 0) s_stay = 0;
-        const bool anti = g2p_stage(a, sc, tv, ox, oy, oz, THREADS);
-        const uint32_t s = a.bstart[b], e = a.bend[b];
-        uint32_t stay = 0;
-        for(uint32_t j = s + threadIdx.x; j < e; j += THREADS) {
-            G2PState o;
-            g2p_particle<PK>(a, sc, tv, anti, ox, oy, oz, j, o);
-            // most particles stay in their block: their keys differ from the
-            // block's only in the lowest digit, counted per particle; the
-            // block's higher digits are counted once below
-            if((o.key >> 6) == b) {
-                mpm_sort::hist_add_low(s_hist, o.key, a.key_bits);
-                stay++;
-            } else {
-                mpm_sort::hist_add(s_hist, o.key, a.key_bits);
-            }
+        // the tile: wait for its copy, then note nodes whose friction velocity differs
+        const bool arrived = mbar_wait(&s_bar[buf], (uint32_t)(k >> 1) & 1u);
+        int differs = 0;
+        const float4* t4 = tv[buf];
+        for(int t = threadIdx.x; t < TN; t += THREADS) {
+            const float4 p0 = t4[2 * t], p1 = t4[2 * t + 1];
+            differs |= (p0.w != p0.x) | (p1.x != p0.y) | (p1.y != p0.z);
         }
-        if(stay) atomicAdd(&s_stay, stay);
+        if(__syncthreads_or(!arrived)) {
+            failed = true;
+            break;
+        }
+        const bool anti = __syncthreads_or(differs) != 0;
+        // a contiguous part of the block (coalesced slots)
+        const uint32_t s = a.bstart[b], c = a.bend[b] - s;
+        const uint32_t j0 = s + (uint32_t)((uint64_t)c * part / parts), j1 = s + (uint32_t)((uint64_t)c * (part + 1) / parts);
+        for(uint32_t j = j0 + threadIdx.x; j < j1; j += THREADS) {
+            G2PState o;
+            g2p_particle<PK>(a, sc, t4, anti, ox, oy, oz, j, o);
+            const int d = key_dir(sc, b, bx, by, bz, o.key);
+            if(d == DIR_FAR) {
+                atomicAdd(&a.far_in[o.key >> 6], 1u);
+                atomicAdd(&a.bcount[o.key >> 6], 1u);
+            }
+            const unsigned act = __activemask();
+            const unsigned peers = __match_any_sync(act, d);
+            if((__ffs(peers) - 1) == lane) atomicAdd(&s_dc[d], (uint32_t)__popc(peers));
+        }
         __syncthreads();
-        if(threadIdx.x == 0 && s_stay) mpm_sort::hist_add_high(s_hist, b << 6, s_stay, a.key_bits);
+        if(threadIdx.x < NDIR) {
+            const int d = threadIdx.x;
+            const uint32_t c2 = s_dc[d];
+            if(c2 && d != DIR_FAR) {
+                atomicAdd(&a.dcount[d * a.nblk + b], c2);
+                if(d < 27)   // the neighbour block it moved to: block + delta(d)
+                    atomicAdd(&a.bcount[b + ((dir_dx(d) * sc.NB[1]) + dir_dy(d)) * sc.NB[2] + dir_dz(d)], c2);
+            }
+            s_dc[d] = 0u;
+        }
     }
-    __syncthreads();
-    for(int i = threadIdx.x; i < mpm_sort::kMaxPasses * mpm_sort::kRadix; i += THREADS) {
-        const uint32_t c = (&s_hist[0][0])[i];
-        if(c) atomicAdd(&a.sort_scratch[i], c);
+    if(threadIdx.x == 0) {
+        if(failed) atomicOr(a.flags, MPM_FLAG_TIMEOUT);
+        // copies still in flight land before the CTA's shared memory goes away
+        for(int bb = 0; bb < 2; bb++)
+            if(failed && ((issued >> bb) & 1u)) mbar_wait(&s_bar[bb], 0u), mbar_wait(&s_bar[bb], 1u);
     }
 }
 
@@ -1505,13 +1858,21 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.dst = f.soa[o]; a.dst_attr = f.attr[o]; a.dst_pid = f.pid[o];
     a.perm = f.perm;
     a.sorted_keys = f.sorted_keys;
-    a.keys_next = f.keys;
-    a.bstart = f.bstart; a.bend = f.bend; a.active = f.active;
-    a.nb_flag = f.nb_flag; a.nb_list = f.nb_list; a.counters = f.counters;
+    a.keys_cur = f.keys[c];
+    a.keys_next = f.keys[o];
+    // this substep's order is set c, the previous substep's set o
+    a.bstart = f.bstart[c]; a.bend = f.bend[c]; a.active = f.active[c]; a.chunks = f.chunks[c];
+    a.ctr = f.counters ? f.counters + CNT_COUNT * c : nullptr;
+    a.obstart = f.bstart[o]; a.obend = f.bend[o]; a.oactive = f.active[o];
+    a.octr = f.counters ? f.counters + CNT_COUNT * o : nullptr;
+    a.dcount = f.dcount; a.doff = f.doff; a.far_in = f.far_in; a.farpos = f.farpos; a.bcount = f.bcount; a.scan = f.scan;
+    a.nblk = f.total_blocks;
+    a.part = kPartSize[f.route_variant];
+    a.chunk_cap = (uint32_t)f.chunk_cap;
+    a.nb_flag = f.nb_flag; a.nb_list = f.nb_list;
     a.acc = f.acc; a.vel = f.vel;
-    a.fallback = f.sort_keys_alt;   // the sort's ping-pong buffer is free until the next sort
-    a.sort_scratch = f.sort_scratch;
-    a.key_bits = f.key_bits;
+    a.fallback = f.sort_keys_alt;   // the full sort's ping-pong buffer is free during substeps
+    a.tmaps = (const CUtensorMap*)f.tmaps;
     a.scenes = f.scenes; a.block_scene = f.block_scene; a.nb_scene = f.nb_scene; a.pbase = f.pbase;
     a.objs = f.objs;
     a.nscenes = f.nscenes;
@@ -1550,9 +1911,11 @@ int grid_stride_blocks(mpm_handle* h, int64_t n, int t)
     return (int)(b < 1 ? 1 : b);
 }
 
-// Launch shapes the autotuner chooses among.
+// Launch shapes the autotuner chooses among.  P2G: lane groups with 128 or
+// 256 threads (work items of up to 512 / 1024 particles), or the fixed-point
+// tile with 128 or 256 threads (one particle per thread).
 const int kG2PThreads[] = {64, 128, 256};
-const char* const kP2GNames[] = {"cells", "interleaved", "pairs", "pairx"};
+const char* const kP2GNames[] = {"groups128", "groups256", "fixed128", "fixed256"};
 
 int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult)
 {
@@ -1566,6 +1929,8 @@ int occupancy_ctas(mpm_handle* h, const void* fn, int threads, int mult)
 // ---------------------------------------------------------------------------
 // Scenes: block / node-block / grid numbering of the whole batch.
 // ---------------------------------------------------------------------------
+static int encode_tile_maps(mpm_handle* h);
+
 int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, const mpm_collision_object* objs, int nobjs)
 {
     h->fast.generation++;
@@ -1656,14 +2021,66 @@ int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, con
     MPM_CUDA(h, cudaMalloc(&f.vel, nodes * 2 * sizeof(float4)));
     MPM_CUDA(h, cudaMemset(f.acc, 0, nodes * sizeof(float4)));
     MPM_CUDA(h, cudaMemset(f.vel, 0, nodes * 2 * sizeof(float4)));
-    MPM_CUDA(h, cudaMalloc(&f.bstart, blocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMalloc(&f.bend, blocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMalloc(&f.active, blocks * sizeof(uint32_t)));
+    for(int k = 0; k < 2; k++) {
+        MPM_CUDA(h, cudaMalloc(&f.bstart[k], blocks * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.bend[k], blocks * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.active[k], blocks * sizeof(uint32_t)));
+    }
     MPM_CUDA(h, cudaMalloc(&f.nb_flag, nblocks * sizeof(uint32_t)));
     MPM_CUDA(h, cudaMalloc(&f.nb_list, nblocks * sizeof(uint32_t)));
     MPM_CUDA(h, cudaMemset(f.nb_flag, 0, nblocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMalloc(&f.counters, CNT_COUNT * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMemset(f.counters, 0, CNT_COUNT * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.counters, 2 * CNT_COUNT * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMemset(f.counters, 0, 2 * CNT_COUNT * sizeof(uint32_t)));
+    // routing between substeps: direction counts and offsets, far arrivals,
+    // the block scan's epoch word and look-back status words (two chains)
+    MPM_CUDA(h, cudaMalloc(&f.dcount, (size_t)NDIR * blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.doff, (size_t)NDIR * blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.far_in, blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.farpos, blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.bcount, blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMemset(f.bcount, 0, blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMemset(f.dcount, 0, (size_t)NDIR * blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMemset(f.far_in, 0, blocks * sizeof(uint32_t)));
+    const int64_t tiles = (blocks + SCAN_TILE - 1) / SCAN_TILE;
+    MPM_CUDA(h, cudaMalloc(&f.scan, (2 + 4 * tiles) * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMemset(f.scan, 0, (2 + 4 * tiles) * sizeof(uint32_t)));
+    f.order_ready = false;
+    f.sorted_now = false;
+    return encode_tile_maps(h);
+}
+
+// G2P's tile copies: per scene, its slice of the node grid (GA[0] x GA[1] x
+// GA[2] nodes, z fastest, 8 floats = 32 bytes per node: v_new, v_fric, mass)
+// as a 4D tensor {8, z, y, x} with a box of {8, 6, 6, 6}.  The driver's
+// encoder is looked up through the runtime, so the library does not link
+// libcuda directly.
+static int encode_tile_maps(mpm_handle* h)
+{
+    FastState& f = h->fast;
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if(!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        if(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+           q != cudaDriverEntryPointSuccess || !fn)
+            return set_error(h, MPM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    std::vector<CUtensorMap> maps(f.nscenes);
+    for(int s = 0; s < f.nscenes; s++) {
+        const SceneDev& c = f.scenes_h[s];
+        const cuuint64_t dim[4] = {8, (cuuint64_t)c.GA[2], (cuuint64_t)c.GA[1], (cuuint64_t)c.GA[0]};
+        const cuuint64_t stride[3] = {32, 32ull * c.GA[2], 32ull * c.GA[2] * c.GA[1]};
+        const cuuint32_t box[4] = {8, TE, TE, TE}, estride[4] = {1, 1, 1, 1};
+        CUresult r = encode(&maps[s], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void*)(f.vel + 2 * c.node_base), dim, stride, box,
+                            estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if(r != CUDA_SUCCESS) return set_error(h, MPM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    }
+    cudaFree(f.tmaps);
+    f.tmaps = nullptr;
+    MPM_CUDA(h, cudaMalloc(&f.tmaps, maps.size() * sizeof(CUtensorMap)));
+    MPM_CUDA(h, cudaMemcpy(f.tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
     return MPM_OK;
 }
 
@@ -1711,8 +2128,10 @@ int fast_alloc(mpm_handle* h, int64_t n)
             cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); cudaFree(f.plas[b]);
             f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; f.plas[b] = nullptr;
         }
-        uint32_t** ps[] = {&f.keys, &f.sorted_keys, &f.perm, &f.sort_keys_alt, &f.sort_vals_alt, &f.sort_scratch};
+        uint32_t** ps[] = {&f.keys[0], &f.keys[1], &f.sorted_keys, &f.perm, &f.sort_keys_alt, &f.sort_vals_alt,
+                           &f.sort_scratch};
         for(uint32_t** p: ps) { cudaFree(*p); *p = nullptr; }
+        for(int k = 0; k < 2; k++) { cudaFree(f.chunks[k]); f.chunks[k] = nullptr; }
         cudaFree(f.vkick);
         f.vkick = nullptr;
         cudaFree(f.pmodel); cudaFree(f.pmask);   // per caller index: a new count drops them
@@ -1724,7 +2143,10 @@ int fast_alloc(mpm_handle* h, int64_t n)
             MPM_CUDA(h, cudaMalloc(&f.attr[b], np * sizeof(float4)));
             MPM_CUDA(h, cudaMalloc(&f.pid[b], np * sizeof(int)));
         }
-        MPM_CUDA(h, cudaMalloc(&f.keys, np * sizeof(uint32_t)));
+        for(int k = 0; k < 2; k++) MPM_CUDA(h, cudaMalloc(&f.keys[k], np * sizeof(uint32_t)));
+        // work items: a block's particles in parts of at least 64
+        f.chunk_cap = np / 64 + std::min<int64_t>(np, f.total_blocks) + 1;
+        for(int k = 0; k < 2; k++) MPM_CUDA(h, cudaMalloc(&f.chunks[k], f.chunk_cap * sizeof(uint4)));
         MPM_CUDA(h, cudaMalloc(&f.sorted_keys, np * sizeof(uint32_t)));
         MPM_CUDA(h, cudaMalloc(&f.perm, np * sizeof(uint32_t)));
         MPM_CUDA(h, cudaMalloc(&f.sort_keys_alt, np * sizeof(uint32_t)));
@@ -1733,6 +2155,8 @@ int fast_alloc(mpm_handle* h, int64_t n)
         MPM_CUDA(h, cudaMemsetAsync(f.sort_scratch, 0, mpm_sort::scratch_words(np) * sizeof(uint32_t), h->stream));
         MPM_CUDA(h, mpm_sort::prepare());
         f.n = n;
+        f.order_ready = false;
+        f.sorted_now = false;
     }
     return fast_penalty_buffers(h);
 }
@@ -1755,12 +2179,17 @@ void fast_free(mpm_handle* h)
         cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); cudaFree(f.plas[b]);
         f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; f.plas[b] = nullptr;
     }
-    void** ps[] = {(void**)&f.keys, (void**)&f.sorted_keys, (void**)&f.perm, (void**)&f.sort_keys_alt, (void**)&f.sort_vals_alt,
-                   (void**)&f.sort_scratch, (void**)&f.bstart, (void**)&f.bend, (void**)&f.active, (void**)&f.nb_flag,
+    void** ps[] = {(void**)&f.keys[0], (void**)&f.keys[1], (void**)&f.sorted_keys, (void**)&f.perm,
+                   (void**)&f.sort_keys_alt, (void**)&f.sort_vals_alt, (void**)&f.sort_scratch, (void**)&f.bstart[0],
+                   (void**)&f.bend[0], (void**)&f.active[0], (void**)&f.chunks[0], (void**)&f.bstart[1],
+                   (void**)&f.bend[1], (void**)&f.active[1], (void**)&f.chunks[1], (void**)&f.nb_flag,
                    (void**)&f.nb_list, (void**)&f.counters, (void**)&f.acc, (void**)&f.vel, (void**)&f.scenes,
                    (void**)&f.block_scene, (void**)&f.nb_scene, (void**)&f.pbase, (void**)&f.objs, (void**)&f.vkick,
-                   (void**)&f.pmodel, (void**)&f.pmask};
+                   (void**)&f.pmodel, (void**)&f.pmask, (void**)&f.dcount, (void**)&f.doff, (void**)&f.far_in,
+                   (void**)&f.farpos, (void**)&f.scan, (void**)&f.tmaps, (void**)&f.bcount};
     for(void** p: ps) { cudaFree(*p); *p = nullptr; }
+    f.order_ready = false;
+    f.sorted_now = false;
     cudaFree(f.staging);
     f.staging = nullptr;
     f.staging_bytes = 0;
@@ -1799,7 +2228,8 @@ int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
     }
     f.cur = 0;
     f.keys_ready = n == 0;
-    f.hist_ready = false;
+    f.order_ready = false;
+    f.sorted_now = false;
     if(!n) return MPM_OK;
     // stage caller arrays on the device if needed
     bool dev = v->on_device != 0;
@@ -1841,7 +2271,7 @@ int fast_set_particles(mpm_handle* h, const mpm_particles_view* v)
             (const float*)dptr[3], (const float*)dptr[4], (const float*)dptr[5], (const float*)dptr[6], (const float*)dptr[7], dvalid, valid_slot);
     MPM_LAUNCHED(h, "k_scatter_in");
     a = make_args(h, 0.0);
-    k_init_keys<<<blocks, 256, 0, h->stream>>>(a, valid_slot);
+    k_init_keys<<<blocks, 256, 0, h->stream>>>(a, valid_slot, f.keys[f.cur]);
     MPM_LAUNCHED(h, "k_init_keys");
 
     f.keys_ready = true;
@@ -1984,8 +2414,8 @@ int fast_get_particles(mpm_handle* h, mpm_particles_view* v)
     if(v->valid) dvalid = dev ? v->valid : stage + (size_t)n * 24 * e;
     FastArgs a = make_args(h, 0.0);
     int blocks = grid_stride_blocks(h, n, 256);
-    if(e == 8) k_gather_out<double><<<blocks, 256, 0, h->stream>>>(a, f.keys, (double*)dptr[0], (double*)dptr[1], (double*)dptr[2], (double*)dptr[3], dvalid);
-    else k_gather_out<float><<<blocks, 256, 0, h->stream>>>(a, f.keys, (float*)dptr[0], (float*)dptr[1], (float*)dptr[2], (float*)dptr[3], dvalid);
+    if(e == 8) k_gather_out<double><<<blocks, 256, 0, h->stream>>>(a, f.keys[f.cur], (double*)dptr[0], (double*)dptr[1], (double*)dptr[2], (double*)dptr[3], dvalid);
+    else k_gather_out<float><<<blocks, 256, 0, h->stream>>>(a, f.keys[f.cur], (float*)dptr[0], (float*)dptr[1], (float*)dptr[2], (float*)dptr[3], dvalid);
     MPM_LAUNCHED(h, "k_gather_out");
     if(!dev) {
         for(int i = 0; i < 4; i++) {
@@ -1998,43 +2428,65 @@ int fast_get_particles(mpm_handle* h, mpm_particles_view* v)
     return MPM_OK;
 }
 
-// sort + ranges + tail copy + P2G (with fused stress and gravity)
-// Sort the keys, then block ranges and the active list; the first `cleared`
-// words of `counters` are zeroed before the ranges kernel counts into them.
-static int fast_sort_ranges(mpm_handle* h, double dt, int cleared)
+// The order of the current slots when no G2P produced it (particles just
+// set, or the autotuner's restore): a radix sort of the slots' cell keys,
+// then the particles are copied to the other buffer in sorted order and that
+// order is recorded as a previous substep's (k_prepare).  Runs eagerly, never
+// inside a captured substep.
+int fast_prepare(mpm_handle* h)
 {
     FastState& f = h->fast;
+    if(f.order_ready || !f.keys_ready || !f.n) return MPM_OK;
     const int64_t n = f.n;
-    int slot = timer_begin(h, "fast_sort");
-    // sort the slot keys (f.keys, left intact for get_particles) into sorted_keys / perm;
-    // the histograms come from the G2P that wrote the keys, else they are counted here
-    cudaError_t e = mpm_sort::radix_sort(f.keys, f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, n, f.key_bits,
-                                         f.sort_scratch, h->d_flags, MPM_FLAG_TIMEOUT, h->sm_count * 4, h->stream,
-                                         true, f.hist_ready);
+    const int c = f.cur;
+    int slot = timer_begin(h, "fast_full_sort");
+    cudaError_t e = mpm_sort::radix_sort(f.keys[c], f.sorted_keys, f.perm, f.sort_keys_alt, f.sort_vals_alt, n, f.key_bits,
+                                         f.sort_scratch, h->d_flags, MPM_FLAG_TIMEOUT, h->sm_count * 4, h->stream);
     if(e != cudaSuccess) return check_cuda(h, e, "radix_sort");
-    f.hist_ready = false;
     timer_end(h, slot);
-    FastArgs a = make_args(h, dt);
-    slot = timer_begin(h, "fast_ranges");
-    MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, cleared * sizeof(uint32_t), h->stream));
-    k_ranges<<<grid_stride_blocks(h, n, 256), 256, 0, h->stream>>>(a);
-    MPM_LAUNCHED(h, "k_ranges");
-    timer_end(h, slot);
+    MPM_CUDA(h, cudaMemsetAsync(f.dcount, 0, (size_t)NDIR * f.total_blocks * sizeof(uint32_t), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(f.far_in, 0, f.total_blocks * sizeof(uint32_t), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(f.bcount, 0, f.total_blocks * sizeof(uint32_t), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(f.counters + CNT_COUNT * c, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
+    FastArgs a = make_args(h, 0.0);
+    k_prepare<<<grid_stride_blocks(h, n, 256), 256, 0, h->stream>>>(a, f.bstart[c], f.bend[c], f.active[c],
+                                                                    f.counters + CNT_COUNT * c);
+    MPM_LAUNCHED(h, "k_prepare");
+    f.cur = 1 - c;       // the sorted copy is the current buffer; set c describes it
+    f.order_ready = true;
+    f.sorted_now = false;
     return MPM_OK;
 }
 
-// Count the digit histograms of the current keys (after mpm_set_particles or
-// the autotuner's restore), so that a captured substep never has to.
-int fast_prepare_sort(mpm_handle* h)
+// This substep's order from the previous one: block scan (ranges, routing
+// offsets, work items) and routing of every slot.
+static int fast_route(mpm_handle* h)
 {
     FastState& f = h->fast;
-    if(f.hist_ready || !f.keys_ready || !f.n) return MPM_OK;
-    MPM_CUDA(h, cudaMemsetAsync(f.sort_scratch, 0, mpm_sort::kHistWords * sizeof(uint32_t), h->stream));
-    const int hb = std::min((int)((f.n + 1023) / 1024), h->sm_count * 4);
-    mpm_sort::k_upfront_hist<<<std::max(hb, 1), mpm_sort::kThreads, 0, h->stream>>>(f.keys, f.n, f.key_bits, f.sort_scratch);
-    MPM_LAUNCHED(h, "k_upfront_hist");
-    f.hist_ready = true;
+    const int c = f.cur;
+    int slot = timer_begin(h, "fast_bins");
+    MPM_CUDA(h, cudaMemsetAsync(f.counters + CNT_COUNT * c, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
+    FastArgs a = make_args(h, 0.0);
+    const int64_t tiles = (f.total_blocks + BIN_TILE - 1) / BIN_TILE;
+    k_bins<<<(unsigned)tiles, BIN_THREADS, 0, h->stream>>>(a);
+    MPM_LAUNCHED(h, "k_bins");
+    timer_end(h, slot);
+    slot = timer_begin(h, "fast_route");
+    k_route<<<h->sm_count * 8, 256, 0, h->stream>>>(a);
+    MPM_LAUNCHED(h, "k_route");
+    timer_end(h, slot);
+    f.sorted_now = true;
     return MPM_OK;
+}
+
+template<int T> static void launch_p2g(mpm_handle* h, const FastArgs& a)
+{
+    k_p2g<T><<<occupancy_ctas(h, (const void*)k_p2g<T>, T, h->fast.cta_mult), T, 0, h->stream>>>(a);
+}
+
+template<int T> static void launch_p2g_groups(mpm_handle* h, const FastArgs& a)
+{
+    k_p2g_groups<T><<<occupancy_ctas(h, (const void*)k_p2g_groups<T>, T, h->fast.cta_mult), T, 0, h->stream>>>(a);
 }
 
 int fast_p2g(mpm_handle* h, double dt, double)
@@ -2042,8 +2494,13 @@ int fast_p2g(mpm_handle* h, double dt, double)
     FastState& f = h->fast;
     if(!f.keys_ready) return set_error(h, MPM_ERR_STATE, "particles not set");
     if(!f.n) return MPM_OK;
-    int rc = fast_sort_ranges(h, dt, CNT_COUNT);
+    int rc = fast_prepare(h);
     if(rc) return rc;
+    const bool repeat = f.sorted_now;
+    if(!repeat) {
+        f.route_variant = f.p2g_variant;   // the work items' size; a repeated P2G keeps it
+        if((rc = fast_route(h))) return rc;
+    }
     FastArgs a = make_args(h, dt);
     if(a.npen) {
         const int ps = timer_begin(h, "fast_penalty");
@@ -2051,16 +2508,16 @@ int fast_p2g(mpm_handle* h, double dt, double)
         timer_end(h, ps);
         MPM_LAUNCHED(h, "k_penalty_kick");
     }
+    if(repeat) {   // P2G again before a G2P (the phase entry points): its work tickets restart
+        MPM_CUDA(h, cudaMemsetAsync(a.ctr + CNT_P2G_WORK, 0, sizeof(uint32_t), h->stream));
+        MPM_CUDA(h, cudaMemsetAsync(a.ctr + CNT_FALLBACK, 0, 2 * sizeof(uint32_t), h->stream));
+    }
     int slot = timer_begin(h, "fast_p2g");
-    if(f.p2g_variant == 0) k_p2g_cells<<<occupancy_ctas(h, (const void*)k_p2g_cells, 64, f.cta_mult), 64, 0, h->stream>>>(a);
-    else {
-        if(f.p2g_variant == 1)
-            k_p2g_interleaved<128><<<occupancy_ctas(h, (const void*)k_p2g_interleaved<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
-        else if(f.p2g_variant == 2)
-            k_p2g_pairs<128><<<occupancy_ctas(h, (const void*)k_p2g_pairs<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
-        else
-            k_p2g_pairx<128><<<occupancy_ctas(h, (const void*)k_p2g_pairx<128>, 128, f.cta_mult), 128, 0, h->stream>>>(a);
-        MPM_LAUNCHED(h, "k_p2g_pairs");
+    switch(f.route_variant) {
+        case MPM_P2G_GROUPS256: launch_p2g_groups<256>(h, a); break;
+        case MPM_P2G_FIXED128: launch_p2g<128>(h, a); break;
+        case MPM_P2G_FIXED256: launch_p2g<256>(h, a); break;
+        default: launch_p2g_groups<128>(h, a); break;
     }
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_p2g");
@@ -2072,7 +2529,9 @@ int fast_forces(mpm_handle* h, double dt, double)
 {
     FastState& f = h->fast;
     if(!f.n) return MPM_OK;
+    if(!f.sorted_now) return set_error(h, MPM_ERR_STATE, "grid update before P2G");
     FastArgs a = make_args(h, dt);
+    f.grid_set = f.cur;
     int slot = timer_begin(h, "fast_grid");
     k_grid<<<h->sm_count * 8, 256, 0, h->stream>>>(a);
     f.grid_dirty = false;
@@ -2095,6 +2554,7 @@ int fast_g2p(mpm_handle* h, double dt, double)
 {
     FastState& f = h->fast;
     if(!f.n) return MPM_OK;
+    if(!f.sorted_now) return set_error(h, MPM_ERR_STATE, "G2P before P2G");
     FastArgs a = make_args(h, dt);
     int slot = timer_begin(h, "fast_g2p");
     if(!a.psrc) launch_g2p<0>(h, a);
@@ -2103,7 +2563,58 @@ int fast_g2p(mpm_handle* h, double dt, double)
     timer_end(h, slot);
     MPM_LAUNCHED(h, "k_g2p");
     f.cur = 1 - f.cur;
-    f.hist_ready = true;
+    f.sorted_now = false;
+    f.order_ready = true;
+    return MPM_OK;
+}
+
+namespace {
+// Extra node forces (the caller's, in the reference's ghosted layout) into the
+// P2G accumulator of the listed node blocks: momentum + dt f where the node
+// has mass, which the grid update then turns into dv = dt f / m.
+template<class S> __global__ void k_add_forces(FastArgs a, const S* f, float dt, int G0, int G1, int G2)
+{
+    const SceneDev& sc = a.scenes[0];
+    const uint64_t total = (uint64_t)a.ctr[CNT_NODE_BLOCKS] * 64u;
+    for(uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total; g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t nb = a.nb_list[g >> 6] - sc.nb_base;
+        const int t = (int)(g & 63u);
+        const int nz = nb % sc.NN[2], r = nb / sc.NN[2], ny = r % sc.NN[1], nx = r / sc.NN[1];
+        const int qx = 4 * nx + (t >> 4), qy = 4 * ny + ((t >> 2) & 3), qz = 4 * nz + (t & 3);
+        if(qx >= G0 || qy >= G1 || qz >= G2) continue;
+        const int64_t q = node_index(sc, qx, qy, qz);
+        float4 c = a.acc[q];
+        if(c.w == 0.f) continue;
+        const int64_t o = 3 * (((int64_t)qx * G1 + qy) * G2 + qz);
+        c.x += dt * (float)f[o];
+        c.y += dt * (float)f[o + 1];
+        c.z += dt * (float)f[o + 2];
+        a.acc[q] = c;
+    }
+}
+}  // namespace
+
+int fast_add_forces(mpm_handle* h, double dt, const void* f, int dtype, bool on_device)
+{
+    FastState& f_ = h->fast;
+    if(!f_.n) return MPM_OK;
+    if(!f_.sorted_now || !f_.grid_dirty) return set_error(h, MPM_ERR_STATE, "extra node forces go between P2G and the grid update");
+    int G[3];
+    int64_t gn = 1;
+    for(int k = 0; k < 3; k++) { G[k] = h->sp.counts[k] + 2 * MPM_GHOST; gn *= G[k]; }
+    const size_t e = dtype == MPM_FP64 ? 8 : 4;
+    const void* src = f;
+    void* stage = nullptr;
+    if(!on_device) {
+        MPM_CUDA(h, cudaMallocAsync(&stage, gn * 3 * e, h->stream));
+        MPM_CUDA(h, cudaMemcpyAsync(stage, f, gn * 3 * e, cudaMemcpyHostToDevice, h->stream));
+        src = stage;
+    }
+    FastArgs a = make_args(h, dt);
+    if(e == 8) k_add_forces<double><<<h->sm_count * 8, 256, 0, h->stream>>>(a, (const double*)src, (float)dt, G[0], G[1], G[2]);
+    else k_add_forces<float><<<h->sm_count * 8, 256, 0, h->stream>>>(a, (const float*)src, (float)dt, G[0], G[1], G[2]);
+    MPM_LAUNCHED(h, "k_add_forces");
+    if(stage) MPM_CUDA(h, cudaFreeAsync(stage, h->stream));
     return MPM_OK;
 }
 
@@ -2116,7 +2627,8 @@ int fast_get_grid(mpm_handle* h, int scene, double* m, double* v0, double* v, do
     int64_t gn = 1;
     for(int k = 0; k < 3; k++) { G[k] = f.scenes_h[scene].counts[k] + 2 * MPM_GHOST; gn *= G[k]; }
     uint32_t count = 0;
-    MPM_CUDA(h, cudaMemcpyAsync(&count, f.counters + CNT_NODE_BLOCKS, sizeof(count), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(&count, f.counters + CNT_COUNT * f.grid_set + CNT_NODE_BLOCKS, sizeof(count),
+                                cudaMemcpyDeviceToHost, h->stream));
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     double *dm = nullptr, *dv = nullptr, *dvf = nullptr;
     if(m) { MPM_CUDA(h, cudaMallocAsync((void**)&dm, gn * 8, h->stream)); MPM_CUDA(h, cudaMemsetAsync(dm, 0, gn * 8, h->stream)); }
@@ -2141,7 +2653,7 @@ int fast_count_valid(mpm_handle* h, int64_t* c)
     MPM_CUDA(h, cudaMallocAsync(&d, sizeof(*d), h->stream));
     MPM_CUDA(h, cudaMemsetAsync(d, 0, sizeof(*d), h->stream));
     if(f.n) {
-        k_count_keys<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(f.keys, f.n, d);
+        k_count_keys<<<grid_stride_blocks(h, f.n, 256), 256, 0, h->stream>>>(f.keys[f.cur], f.n, d);
         MPM_LAUNCHED(h, "k_count_keys");
     }
     unsigned long long r = 0;
@@ -2156,7 +2668,7 @@ int fast_debug_sort_state(mpm_handle* h, uint32_t* slot_keys, uint32_t* sorted_k
 {
     FastState& f = h->fast;
     size_t bytes = f.n * sizeof(uint32_t);
-    if(slot_keys) MPM_CUDA(h, cudaMemcpyAsync(slot_keys, f.keys, bytes, cudaMemcpyDeviceToHost, h->stream));
+    if(slot_keys) MPM_CUDA(h, cudaMemcpyAsync(slot_keys, f.keys[f.cur], bytes, cudaMemcpyDeviceToHost, h->stream));
     if(sorted_keys) MPM_CUDA(h, cudaMemcpyAsync(sorted_keys, f.sorted_keys, bytes, cudaMemcpyDeviceToHost, h->stream));
     if(perm) MPM_CUDA(h, cudaMemcpyAsync(perm, f.perm, bytes, cudaMemcpyDeviceToHost, h->stream));
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -2198,7 +2710,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* repor
     MPM_CUDA(h, cudaMemcpyAsync(save_soa, f.soa[cur0], NCOMP * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
     MPM_CUDA(h, cudaMemcpyAsync(save_attr, f.attr[cur0], np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream));
     MPM_CUDA(h, cudaMemcpyAsync(save_pid, f.pid[cur0], np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
-    MPM_CUDA(h, cudaMemcpyAsync(save_keys, f.keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(save_keys, f.keys[cur0], np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
     float* save_plas = nullptr;
     const bool plastic = h->plastic.kind && f.plas[0];
     if(plastic) {
@@ -2213,7 +2725,7 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* repor
     const bool timing = h->timing;
     h->timing = false;
     int rc = MPM_OK;
-    for(int variant = 0; variant <= MPM_P2G_PAIRX && !rc; variant++)
+    for(int variant = 0; variant <= MPM_P2G_FIXED256 && !rc; variant++)
         for(int ti = 0; ti < 3 && !rc; ti++)
             for(int mult = 1; mult <= 2 && !rc; mult++) {
                 f.p2g_variant = variant;
@@ -2224,9 +2736,10 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* repor
                 cudaMemcpyAsync(f.soa[cur0], save_soa, NCOMP * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
                 cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
-                cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
+                cudaMemcpyAsync(f.keys[cur0], save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
                 if(plastic) cudaMemcpyAsync(f.plas[cur0], save_plas, NPLAS * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
-                f.hist_ready = false;
+                f.order_ready = false;
+                f.sorted_now = false;
                 if((rc = fast_p2g(h, dt, 0)) || (rc = fast_forces(h, dt, 0)) || (rc = fast_g2p(h, dt, 0))) break;
                 for(int s = 0; s < substeps && !rc; s++) {
                     if(cold) cudaMemsetAsync(scrub, s & 0xff, scrub_bytes, h->stream);
@@ -2257,9 +2770,10 @@ int fast_autotune(mpm_handle* h, double dt, int substeps, int flags, char* repor
     cudaMemcpyAsync(f.soa[cur0], save_soa, NCOMP * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(f.attr[cur0], save_attr, np * sizeof(float4), cudaMemcpyDeviceToDevice, h->stream);
     cudaMemcpyAsync(f.pid[cur0], save_pid, np * sizeof(int), cudaMemcpyDeviceToDevice, h->stream);
-    cudaMemcpyAsync(f.keys, save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(f.keys[cur0], save_keys, np * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream);
     if(plastic) cudaMemcpyAsync(f.plas[cur0], save_plas, NPLAS * np * sizeof(float), cudaMemcpyDeviceToDevice, h->stream);
-    f.hist_ready = false;
+    f.order_ready = false;
+    f.sorted_now = false;
     cudaStreamSynchronize(h->stream);
     cudaFree(save_soa); cudaFree(save_attr); cudaFree(save_pid); cudaFree(save_keys); cudaFree(save_plas);
     for(int k = 0; k < substeps; k++) { cudaEventDestroy(e0[k]); cudaEventDestroy(e1[k]); }
@@ -2360,13 +2874,14 @@ int debug_sort_stall(const uint32_t* keys, int64_t n, int bits, uint32_t spin_li
     return rc;
 }
 
-// Seed the epoch word of the handle's sort scratch (test hook: sorts across
-// the 2^30 wrap of the status words' epoch field).
+// Seed the epoch words of the handle's radix-sort scratch and block scan (test
+// hook: sorts and scans across the 2^30 wrap of the status words' epoch field).
 int debug_set_sort_epoch(mpm_handle* h, uint32_t epoch)
 {
     FastState& f = h->fast;
-    if(!f.sort_scratch) return set_error(h, MPM_ERR_STATE, "no sort scratch");
+    if(!f.sort_scratch || !f.scan) return set_error(h, MPM_ERR_STATE, "no sort scratch");
     MPM_CUDA(h, cudaMemcpyAsync(f.sort_scratch + mpm_sort::kEpochOff, &epoch, sizeof epoch, cudaMemcpyHostToDevice, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(f.scan, &epoch, sizeof epoch, cudaMemcpyHostToDevice, h->stream));
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     return MPM_OK;
 }
@@ -2473,7 +2988,7 @@ __global__ void k_particle_totals(FastArgs a, double* acc, unsigned long long* m
 {
     double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, vmax = 0, amax = 0;
     for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t key = a.keys_next[i];
+        uint32_t key = a.keys_cur[i];
         if(key == SENTINEL) continue;
         const SceneDev& sc = a.scenes[a.block_scene[key >> 6]];
         double X[3], V[3], B[9];
@@ -2574,7 +3089,8 @@ int fast_grid_totals(mpm_handle* h, mpm_totals* out)
 {
     FastState& f = h->fast;
     uint32_t count = 0;
-    MPM_CUDA(h, cudaMemcpyAsync(&count, f.counters + CNT_NODE_BLOCKS, sizeof(count), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync(&count, f.counters + CNT_COUNT * f.grid_set + CNT_NODE_BLOCKS, sizeof(count),
+                                cudaMemcpyDeviceToHost, h->stream));
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     double* d = nullptr;
     MPM_CUDA(h, cudaMallocAsync((void**)&d, 16 * sizeof(double), h->stream));

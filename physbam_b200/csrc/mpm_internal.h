@@ -73,25 +73,41 @@ struct FastState {
     int* pid[2] = {nullptr, nullptr};         // caller's particle index
     float* plas[2] = {nullptr, nullptr};      // plasticity on: 13 * npad floats: Fp0..8, then mu0, lambda0
                                               // (clamp) or plastic_def, rho_F, sigma_Y, vc (Drucker-Prager)
-    uint32_t* keys = nullptr;                 // keys of the current buffer's slots
+    uint32_t* keys[2] = {nullptr, nullptr};   // cell keys of each buffer's slots
     uint32_t* sorted_keys = nullptr;
     uint32_t* perm = nullptr;                 // sorted position -> slot in the current buffer
     uint32_t* sort_keys_alt = nullptr;
     uint32_t* sort_vals_alt = nullptr;
     uint32_t* sort_scratch = nullptr;         // histograms, tickets, epoch, look-back status words
-    uint32_t* bstart = nullptr;               // per particle block
-    uint32_t* bend = nullptr;
-    uint32_t* active = nullptr;               // active particle blocks
+    // the particle blocks of a substep's sorted order, one set per buffer parity
+    // (the next substep's routing reads the previous set)
+    uint32_t* bstart[2] = {nullptr, nullptr}; // per particle block
+    uint32_t* bend[2] = {nullptr, nullptr};
+    uint32_t* active[2] = {nullptr, nullptr}; // active particle blocks
+    uint4* chunks[2] = {nullptr, nullptr};    // work items: (block, part, parts, 0)
+    int64_t chunk_cap = 0;
+    // routing from one substep's order to the next (mpm_fast.cu, k_bins / k_route):
+    // per (block, direction) counts written by G2P and their offsets, arrivals
+    // from farther than a neighbour block, look-back status of the block scan
+    uint32_t* dcount = nullptr;               // NDIR x total_blocks
+    uint32_t* doff = nullptr;                 // NDIR x total_blocks
+    uint32_t* far_in = nullptr;               // total_blocks
+    uint32_t* farpos = nullptr;               // total_blocks
+    uint32_t* bcount = nullptr;               // total_blocks: particles arriving in each block (near and far)
+    uint32_t* scan = nullptr;                 // epoch word, then 2 x tiles uint64 status words
+    void* tmaps = nullptr;                    // per scene: CUtensorMap of its node grid (G2P tiles by TMA)
+    bool order_ready = false;                 // the previous set + dcount describe the current slots
+    bool sorted_now = false;                  // this substep's order is built (P2G may repeat)
     uint32_t* nb_flag = nullptr;              // node-block touched this substep
     uint32_t* nb_list = nullptr;              // touched node blocks
-    uint32_t* counters = nullptr;             // see FastCounter
+    uint32_t* counters = nullptr;             // 2 x 16 words, one set per parity: see FastCounter
+    int grid_set = 0;                         // counter set of the last grid update (its node blocks)
     float4* acc = nullptr;                    // P2G accumulator: momentum+dt*force (xyz), mass (w)
     float4* vel = nullptr;                    // per node 2 x float4: vnew.xyz, vfric.x | vfric.yz, mass, 0
     float* vkick = nullptr;                   // penalty objects on: 3 * npad floats, V + dt f / m per slot
     uint8_t* pmodel = nullptr;                // constitutive model per caller particle index (null: the scene's)
     uint8_t* pmask = nullptr;                 // plasticity on per caller particle index (null: all)
     bool keys_ready = false;
-    bool hist_ready = false;
     uint64_t generation = 0;   // bumped whenever device buffers are (re)allocated
     int64_t grid_nodes = 0;
     uint32_t grid_node_blocks = 0;
@@ -99,21 +115,27 @@ struct FastState {
     void* staging = nullptr;   // device copies of host particle arrays (set / get)
     size_t staging_bytes = 0;   // sort_scratch holds the digit histograms of `keys` (built by G2P)
     // launch shapes (mpm_autotune)
-    int p2g_variant = 0;                      // 0: thread per cell, 1: thread per particle, cells interleaved
+    int p2g_variant = 0;                      // P2G launch shape (MPM_P2G_*)
+    int route_variant = 0;                    // the shape whose work-item size the current order has
     int g2p_threads = 128;
     int cta_mult = 1;
 };
 
+// One set of per-substep counters (two sets, one per buffer parity).
 enum FastCounter {
     CNT_ACTIVE_BLOCKS = 0,
-    CNT_ACTIVE_PARTICLES = 1,
+    CNT_ACTIVE_PARTICLES = 1,      // valid particles of the substep's order
     CNT_P2G_WORK = 2,
     CNT_G2P_WORK = 3,
     CNT_NODE_BLOCKS = 4,
     CNT_GRID_WORK = 5,
     CNT_FALLBACK = 6,
     CNT_P2G_DONE = 7,
-    CNT_COUNT = 8
+    CNT_CHUNKS = 8,                // work items in the set's chunk list
+    CNT_NEW_INVALID = 9,           // particles the last G2P invalidated
+    CNT_BIN_TICKET = 10,           // tile tickets of the block scan
+    CNT_FAR = 11,                  // particles that moved past a neighbour block
+    CNT_COUNT = 16
 };
 
 struct ImplicitState;   // mpm_implicit.cu
@@ -193,6 +215,8 @@ int plain_forces(mpm_handle* h, double dt, double time);
 int plain_g2p(mpm_handle* h, double dt, double time);
 int plain_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf);
 int plain_count_valid(mpm_handle* h, int64_t* c);
+int plain_add_forces(mpm_handle* h, const void* f, int dtype, bool on_device);
+int fast_add_forces(mpm_handle* h, double dt, const void* f, int dtype, bool on_device);
 
 // fast path (mpm_fast.cu)
 int fast_alloc(mpm_handle* h, int64_t n);
@@ -220,7 +244,7 @@ int radix_sort_host(const uint32_t* keys, int64_t n, int bits, uint32_t* sorted_
 int64_t sort_scratch_words(int64_t n);
 int sort_keys_device(mpm_handle* h, const uint32_t* keys, int64_t n, int bits, uint32_t* sorted, uint32_t* perm,
     uint32_t* alt_keys, uint32_t* alt_vals, uint32_t* scratch);
-int fast_prepare_sort(mpm_handle* h);
+int fast_prepare(mpm_handle* h);
 int fast_particle_totals(mpm_handle* h, mpm_totals* out);
 int fast_grid_totals(mpm_handle* h, mpm_totals* out);
 int plain_particle_totals(mpm_handle* h, mpm_totals* out);

@@ -1027,6 +1027,42 @@ int plain_get_grid(mpm_handle* h, double* m, double* v0, double* v, double* vf)
     return MPM_OK;
 }
 
+namespace {
+// Extra node forces into the grid force array of the current substep (after
+// P2G cleared it and before the grid update reads it).
+template<class T, class S> __global__ void k_add_forces(T* gf, const S* f, int64_t count)
+{
+    for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        gf[i] += (T)f[i];
+}
+}  // namespace
+
+int plain_add_forces(mpm_handle* h, const void* f, int dtype, bool on_device)
+{
+    PlainState& s = h->plain;
+    const int64_t count = s.gn * h->sp.dim;
+    const size_t e = dtype == MPM_FP64 ? 8 : 4;
+    if(!count) return MPM_OK;
+    const void* src = f;
+    void* stage = nullptr;
+    if(!on_device) {
+        MPM_CUDA(h, cudaMallocAsync(&stage, count * e, h->stream));
+        MPM_CUDA(h, cudaMemcpyAsync(stage, f, count * e, cudaMemcpyHostToDevice, h->stream));
+        src = stage;
+    }
+    const int blocks = gblocks(h, count, 256);
+    if(h->model.precision == MPM_FP64) {
+        if(e == 8) k_add_forces<double, double><<<blocks, 256, 0, h->stream>>>((double*)s.gf, (const double*)src, count);
+        else k_add_forces<double, float><<<blocks, 256, 0, h->stream>>>((double*)s.gf, (const float*)src, count);
+    } else {
+        if(e == 8) k_add_forces<float, double><<<blocks, 256, 0, h->stream>>>((float*)s.gf, (const double*)src, count);
+        else k_add_forces<float, float><<<blocks, 256, 0, h->stream>>>((float*)s.gf, (const float*)src, count);
+    }
+    MPM_LAUNCHED(h, "k_add_forces");
+    if(stage) MPM_CUDA(h, cudaFreeAsync(stage, h->stream));
+    return MPM_OK;
+}
+
 int plain_count_valid(mpm_handle* h, int64_t* c)
 {
     unsigned long long* d = nullptr;

@@ -9,3 +9,4 @@
 #define MPM_FLAG_DOMAIN 2u
 #define MPM_FLAG_NOT_CONVERGED 4u
 #define MPM_FLAG_TIMEOUT 8u
+#define MPM_FLAG_ORDER 16u       // the fast path's per-block counts were out of step (nothing written)

@@ -127,7 +127,7 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt",
            "mpm_set_reflection", "mpm_set_penalty_objects", "mpm_set_object_motion", "mpm_set_particle_models",
            "mpm_set_plastic_particles", "mpm_batch_get_grid", "mpm_debug_sort_stall", "mpm_debug_set_sort_epoch",
-           "mpm_debug_set_svd_iterations"]
+           "mpm_debug_set_svd_iterations", "mpm_add_grid_forces"]
 
 _lib = None
 
@@ -157,6 +157,7 @@ def load_library(path: str = LIB_PATH):
     L.mpm_debug_sort_stall.argtypes = [P, ctypes.c_int64, ctypes.c_int, ctypes.c_uint32]
     L.mpm_debug_set_sort_epoch.argtypes = [P, ctypes.c_uint32]
     L.mpm_debug_set_svd_iterations.argtypes = [ctypes.c_int]
+    L.mpm_add_grid_forces.argtypes = [P, ctypes.c_double, P, ctypes.c_int, ctypes.c_int]
     L.mpm_count_valid.argtypes = [P, ctypes.POINTER(ctypes.c_int64)]
     L.mpm_set_timing.argtypes = [P, ctypes.c_int]
     L.mpm_get_timing.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -627,8 +628,29 @@ class MPM_DRIVER:
     # -- the substep (MPM_DRIVER.cpp:141-157) --------------------------------
     def Advance_One_Time_Step(self, dt: Optional[float] = None):
         dt = self.scene.dt if dt is None else dt
+        if getattr(self.scene, "node_force", None) is not None:   # the caller's force between the phases
+            self.Particle_To_Grid(dt)
+            self.add_grid_forces(self._node_force_array(), dt)
+            self.Apply_Forces(dt)
+            self.Grid_To_Particle(dt)
+            return
         self._check(self.L.mpm_substep(self.h, dt, self.time), "mpm_substep")
         self.time += dt
+
+    def _node_force_array(self):
+        shape = tuple(c + 2 * S.GHOST for c in self.scene.counts[:self.dim])
+        f = np.empty(shape + (self.dim,))
+        f[...] = np.asarray(self.scene.node_force, np.float64)[:self.dim]
+        return f
+
+    def add_grid_forces(self, force: np.ndarray, dt: Optional[float] = None):
+        """Extra node forces (ghosted grid, d per node) for the next grid update (mpm_add_grid_forces)."""
+        dt = self.scene.dt if dt is None else dt
+        f = np.ascontiguousarray(force, np.float64)
+        shape = tuple(c + 2 * S.GHOST for c in self.scene.counts[:self.dim]) + (self.dim,)
+        if f.shape != shape:
+            raise ValueError("node forces must have shape %s" % (shape,))
+        self._check(self.L.mpm_add_grid_forces(self.h, dt, _ptr(f), FP64, 0), "mpm_add_grid_forces")
 
     def Particle_To_Grid(self, dt=None):
         self._check(self.L.mpm_particle_to_grid(self.h, self.scene.dt if dt is None else dt, self.time), "p2g")
@@ -644,6 +666,10 @@ class MPM_DRIVER:
     def advance(self, nsteps: int, dt: Optional[float] = None):
         """Fixed-dt substep loop (Simulate_To_Frame with min_dt = max_dt), CUDA-graph replay."""
         dt = self.scene.dt if dt is None else dt
+        if getattr(self.scene, "node_force", None) is not None:
+            for _ in range(nsteps):
+                self.Advance_One_Time_Step(dt)
+            return
         self._check(self.L.mpm_advance(self.h, dt, self.time, nsteps), "mpm_advance")
         self.time += nsteps * dt
 

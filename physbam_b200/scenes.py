@@ -248,6 +248,9 @@ class Scene:
     penalty: Optional[Penalty] = None
     models: Optional[np.ndarray] = None        # per-particle constitutive model (None: `model` for all)
     plastic_mask: Optional[np.ndarray] = None  # the particles the plasticity acts on (None: all)
+    # a force the library does not model, added by the caller between P2G and the grid
+    # update (mpm_add_grid_forces): this vector at every node with mass
+    node_force: Optional[Sequence[float]] = None
 
     @property
     def n(self) -> int:
@@ -559,6 +562,14 @@ def small_2d_penalty(seed=83, G=16, nsteps=20, dt=1e-4):
     return s
 
 
+def small_3d_node_force(seed=121, G=16, nsteps=20, dt=1e-4, force=(0.05, 0.1, -0.025)):
+    """The small 3D scene with a constant extra force at every node with mass (a force the
+    library does not model, handed in through mpm_add_grid_forces)."""
+    s = small_3d(seed=seed, G=G, nsteps=nsteps, dt=dt)
+    s.node_force = list(force)
+    return s
+
+
 def small_3d_moving(seed=91, G=16, nsteps=20, dt=1e-4, implicit=False):
     """small_3d with two moving collision objects: a sticky paddle (a box in its own frame)
     that starts inside the block's +x face and turns about y while it pushes in, and a
@@ -766,6 +777,9 @@ def write_scene(path, s: Scene, dumps: Optional[Sequence[int]] = None):
             f.write(np.ascontiguousarray(s.models, np.uint8).tobytes())
         if s.plastic_mask is not None:
             f.write(np.ascontiguousarray(s.plastic_mask, np.uint8).tobytes())
+        if s.node_force is not None:   # optional trailer: a constant force at every node with mass
+            f.write(b"XNF1")
+            f.write(struct.pack("<3d", *pad3(s.node_force)))
 
 
 def read_dump(path, dim, n, counts, plastic=()):

@@ -62,6 +62,9 @@ CASES = {
     "small3d_mixed_implicit": (lambda: S.small_3d_mixed(implicit=True), [0, 7], [0, 7]),
     # sand beside an elastic body: the plasticity over the sand's particles alone
     "smallsandwater3d_mixed": (lambda: S.small_sand_water_3d(), [0, 1, 19], [0, 19]),
+    # a force the library does not model (a constant vector at every node with mass), which
+    # the GPU path receives from the caller through mpm_add_grid_forces
+    "small3d_node_force": (lambda: S.small_3d_node_force(), [0, 1, 19], [0, 19]),
 }
 
 
@@ -115,6 +118,8 @@ def main(names=None):
             arrays["pen_friction"] = np.array([o.friction for o in pn.objects])
             arrays["pen_a"] = np.array([o.a for o in pn.objects]).reshape(-1, scene.dim)
             arrays["pen_b"] = np.array([o.b for o in pn.objects]).reshape(-1, scene.dim)
+        if scene.node_force is not None:
+            arrays["node_force"] = np.array(scene.node_force, np.float64)
         im = scene.implicit
         if im is not None:
             arrays["implicit"] = np.array([im.newton_tolerance, im.newton_iterations, im.solver_tolerance,
@@ -163,6 +168,8 @@ def load(name):
         pobjs = [S.CollisionObject(int(k), int(t), float(f), list(a), list(b))
                  for k, t, f, a, b in zip(z["pen_kind"], z["pen_type"], z["pen_friction"], z["pen_a"], z["pen_b"])]
         scene.penalty = S.Penalty(pobjs, float(z["penalty"][0]), float(z["penalty"][1]))
+    if "node_force" in z:
+        scene.node_force = [float(x) for x in z["node_force"]]
     if "implicit" in z:
         im = z["implicit"]
         scene.implicit = S.Implicit(float(im[0]), int(im[1]), float(im[2]), int(im[3]))

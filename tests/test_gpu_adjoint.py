@@ -148,3 +148,36 @@ def test_adjoint_differentiable_config_deformed_fd(cuda_device):
     """Same size and schedule, body pre-stressed and spinning so the E gradient is non-zero."""
     scene = deformed(S.cube_3d())
     check_case(scene, 64, 8)
+
+
+def with_objects(scene):
+    """The body meets static, frictionless collision objects during the rollout: a
+    slip plane ahead of it in x (nodes beyond it are projected onto it), a
+    separating sphere under its bottom face (curved: the projection's derivative
+    has the curvature term) and a sticking box along its low-y face (nodes stop)."""
+    s = scene.copy()
+    s.target = scene.target
+    if hasattr(scene, "vfield"):
+        s.vfield = scene.vfield
+    s.objects = [S.CollisionObject(S.PLANE, S.SLIP, 0.0, [-1.0, 0.0, 0.0], [0.66, 0.5, 0.5]),
+                 S.CollisionObject(S.SPHERE, S.SEPARATE, 0.0, [0.5, 0.5, 0.25], [0.12, 0.0, 0.0]),
+                 S.CollisionObject(S.BOX, S.STICK, 0.0, [-1.0, -1.0, -1.0], [2.0, 0.36, 2.0])]
+    return s
+
+
+def test_adjoint_with_collision_objects_fd(cuda_device):
+    """The projection of MPM_OBJECTIVE::Test_Add_Collision (System/MPM_OBJECTIVE.cpp:150-183),
+    transposed: gradients with a slip plane, a separating sphere and a sticking box."""
+    scene = with_objects(deformed(S.cube_3d(G=16, nsteps=12)))
+    check_case(scene, 12, 4)
+
+
+def test_adjoint_differentiable_config_with_walls_fd(cuda_device):
+    """The differentiable cube at full size (64^3, 64 substeps, checkpoint every 8) with the
+    slip walls Add_Walls builds and a slip plane the cube runs into."""
+    scene = S.cube_3d()
+    s = scene.copy()
+    s.target = scene.target
+    s.objects = S.walls(3, s.counts, s.domain_min, s.domain_max, 63, S.SLIP, 0.0, 0.05) + [
+        S.CollisionObject(S.PLANE, S.SLIP, 0.0, [-1.0, 0.0, 0.0], [0.653, 0.5, 0.5])]
+    check_case(s, 64, 8, check_E=False)

@@ -5,8 +5,8 @@ the same process keeps sorting and simulating correctly.
 * The radix sort's decoupled look-back waits on a predecessor tile that never
   publishes (its ticket is taken before the pass starts): the bounded wait
   gives up and the call returns MPM_ERR_TIMEOUT.
-* The sort's status words carry a 30-bit epoch: sorts across its wrap stay
-  bit-exact against a CPU stable sort.
+* The look-back status words of the radix sort and of the block scan carry a
+  30-bit epoch: sorts across its wrap stay bit-exact against a CPU stable sort.
 * The FP64 SVD (the reference's unbounded implicit-shift QR,
   Core/Matrices/MATRIX_3X3.cpp:202-236) gets a one-sweep bound: the substep
   reports MPM_ERR_NOT_CONVERGED.
@@ -51,7 +51,7 @@ def test_sort_across_epoch_wrap(cuda_device):
             drv.set_scene_particles(scene)     # a full sort of freshly uploaded keys next
         drv.Particle_To_Grid()
         keys, sk, perm = drv.sort_state()
-        ref = np.argsort(keys, kind="stable").astype(np.uint32)
+        ref = np.argsort(keys >> 6, kind="stable").astype(np.uint32)
         np.testing.assert_array_equal(perm, ref, err_msg="sort %d" % it)
         np.testing.assert_array_equal(sk, keys[ref])
         drv.Apply_Forces()

@@ -33,11 +33,11 @@ def floors(scene, ref):
             "pdef": 1e-300, "rho_F": 1e-300, "cohesion": 1.0, "vc": 1e-300}
 
 
-# the backward-Euler, adaptive-frame and reflection cases pin the GPU path
-# directly against the reference's dumps; the C restatement covers the
+# the backward-Euler, adaptive-frame, reflection and caller-force cases pin the
+# GPU path directly against the reference's dumps; the C restatement covers the
 # symplectic-Euler substep with its collision objects (static, moving and
 # penalty), several materials and plasticity (also over a particle subset)
-EXPLICIT = sorted(n for n in CASES if not any(k in n for k in ("implicit", "adaptive", "reflect")))
+EXPLICIT = sorted(n for n in CASES if not any(k in n for k in ("implicit", "adaptive", "reflect", "node_force")))
 
 
 @pytest.mark.parametrize("name", EXPLICIT)
