@@ -399,6 +399,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp[NW][4];
     __shared__ uint32_t s_pre[4];         // prefixes of the tile: count, invalid (look-back); parts, active (bases)
+    __shared__ uint2 s_act[BIN_TILE];     // the tile's active blocks: block, first sorted position
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if(threadIdx.x == 0) s_tile = atomicAdd(&a.ctr[CNT_BIN_TICKET], 1u);
     __syncthreads();
@@ -457,6 +458,9 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
     uint32_t ex[4];
 #pragma unroll
     for(int q = 0; q < 4; q++) ex[q] = s_pre[q] + s_warp[warp][q] + x[q] - v[q];
+    // ranges, work items and the active list; the tile's active blocks go to
+    // shared memory so that their neighbour loads spread over all threads
+    const uint32_t act0 = s_pre[3];   // the tile's first active-list slot
     for(int u = 0; u < BIN_PER; u++) {
         const int64_t b = b0 + u;
         if(inv[u]) {
@@ -470,9 +474,14 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
         a.bstart[b] = start;
         a.bend[b] = start + cnt[u];
         a.bcount[b] = 0u;
+        s_act[ex[3] - act0] = make_uint2((uint32_t)b, start);
         a.active[ex[3]++] = (uint32_t)b;
         for(uint32_t k = 0; k < parts; k++, ex[2]++)
             if(ex[2] < a.chunk_cap) a.chunks[ex[2]] = make_uint4((uint32_t)b, k, parts, 0u);
+    }
+    __syncthreads();
+    for(uint32_t i = threadIdx.x; i < tot[3]; i += BIN_THREADS) {
+        const uint32_t b = s_act[i].x, start = s_act[i].y;
         // the groups of arrivals, in the order of their previous block (slot order):
         // block b - delta(d) grows as d falls
         const SceneDev& sc = a.scenes[a.block_scene[b]];
@@ -496,7 +505,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
                 a.dcount[d * a.nblk + src[d]] = 0u;
             }
         }
-        if(run != start + cnt[u]) {     // far arrivals fill the rest of the block
+        if(run != a.bend[b]) {          // far arrivals fill the rest of the block
             a.farpos[b] = run;
             a.far_in[b] = 0u;
         }
@@ -804,17 +813,18 @@ __global__ void k_penalty_kick(FastArgs a)
 // one thread per particle.
 //
 // The part's node values are summed in a shared tile of fixed-point
-// integers: shared-memory integer adds are single instructions, where float
-// adds to shared memory are compare-and-swap loops, and integer sums do not
-// depend on their order.  Each quantity (mass, momentum x, y, z) has its own
-// power-of-two scale, chosen after every particle of the part has bounded its
-// largest node value: the bounds' sum B maps to at most 2^30, so no node sum
-// can overflow.  A contribution goes in as its nearest integer plus its
-// rounding residual in units of 2^-22 (a second 32-bit sum: at most 512
-// residuals of at most 2^21), so a node keeps B 2^-53 absolutely: nodes that
-// only the edges of a few stencils reach, with masses many orders below the
-// part's, still get float-like relative precision.  The tile goes out as
-// floats (hi + lo 2^-22 combined in FP64) with one float4 atomic per touched node.
+// integers: shared-memory integer adds run at three times the rate of float
+// adds to shared memory, and integer sums do not depend on their order.  Each
+// quantity (mass, momentum x, y, z) has its own power-of-two scale, chosen
+// after every particle of the part has bounded its largest node value: the
+// bounds' sum B maps below 2^21, so no node sum can overflow.  A contribution
+// goes in as its nearest integer plus its rounding residual in units of 2^-23
+// (a second 32-bit sum: at most 256 residuals of at most 2^22), both formed by
+// float adds rather than conversion instructions, so a node keeps B 2^-45
+// absolutely: nodes that only the edges of a few stencils reach, with masses
+// many orders below the part's, keep their velocities to FP32 accuracy.  The
+// tile goes out as floats (hi + lo 2^-23 combined in FP64) with one float4
+// atomic per touched node.
 //
 // Lanes must hit different nodes in each shared add, so the part's particles
 // are first binned by cell and handed out round by round (round r: the
@@ -853,10 +863,54 @@ __device__ __forceinline__ void factor_bounds(const P2GFactors& P, float* bnd)
     }
 }
 
-template<int T> __global__ void __launch_bounds__(T, 1024 / T) k_p2g(FastArgs a)
+// The factors of a particle in shared memory, one array of T per value (so the
+// thread that reads slot t reads consecutive words).
+constexpr int NFAC = 39;   // w[9], mass factor m wx[3], momentum Hx, Hy, Hz of x, y, z
+
+constexpr float kRoundMagic = 12582912.f;       // 1.5 2^23
+constexpr int kRoundMagicBits = 0x4B400000;     // its bit pattern
+
+__device__ __forceinline__ void store_factors(float* FS, int T, int pos, const P2GFactors& P)
+{
+#pragma unroll
+    for(int e = 0; e < 9; e++) FS[e * T + pos] = P.w[e];
+#pragma unroll
+    for(int o = 0; o < 3; o++) FS[(9 + o) * T + pos] = P.mwx[o];
+#pragma unroll
+    for(int r = 0; r < 3; r++)
+#pragma unroll
+        for(int o = 0; o < 3; o++) {
+            FS[(12 + 9 * r + o) * T + pos] = P.q[r].Hx[o];
+            FS[(15 + 9 * r + o) * T + pos] = P.q[r].Hy[o];
+            FS[(18 + 9 * r + o) * T + pos] = P.q[r].Hz[o];
+        }
+}
+
+__device__ __forceinline__ void load_factors(const float* FS, int T, int pos, P2GFactors& P)
+{
+#pragma unroll
+    for(int e = 0; e < 9; e++) P.w[e] = FS[e * T + pos];
+#pragma unroll
+    for(int o = 0; o < 3; o++) P.mwx[o] = FS[(9 + o) * T + pos];
+#pragma unroll
+    for(int r = 0; r < 3; r++)
+#pragma unroll
+        for(int o = 0; o < 3; o++) {
+            P.q[r].Hx[o] = FS[(12 + 9 * r + o) * T + pos];
+            P.q[r].Hy[o] = FS[(15 + 9 * r + o) * T + pos];
+            P.q[r].Hz[o] = FS[(18 + 9 * r + o) * T + pos];
+        }
+}
+
+// Each thread first prepares the particle its own slot of the part holds
+// (loads through perm stay close to consecutive), then the factors move
+// through shared memory to the thread of the particle's place in the
+// round-by-round cell order, which adds them to the tile.
+template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
 {
     constexpr int NW = T / 32;
     __shared__ P2GSmem<T> S;
+    extern __shared__ __align__(16) float FS[];    // NFAC x T factors, in place order
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t nwork = min(a.ctr[CNT_CHUNKS], a.chunk_cap);
     if(threadIdx.x == 0) S.scene = -1;
@@ -878,16 +932,29 @@ template<int T> __global__ void __launch_bounds__(T, 1024 / T) k_p2g(FastArgs a)
         if(sid != S.scene) stage_scene(a, sid, &S.sc);
         const uint32_t s = a.bstart[b], e = a.bend[b];
         const uint32_t cnt = e - s > part ? min((e - s - part + parts - 1) / parts, (uint32_t)T) : 0u;
-        // bin the part's particles by cell
+        // this thread's slot of the (strided) part: cell, rank in its cell, factors, bounds
         const bool mine = threadIdx.x < cnt;
-        uint32_t j = 0, cell = 0, r = 0;
+        uint32_t cell = 0, r = 0;
+        float bnd[4] = {0.f, 0.f, 0.f, 0.f};
+        P2GFactors P;
         if(mine) {
-            j = s + part + threadIdx.x * parts;
+            const uint32_t j = s + part + threadIdx.x * parts;
             cell = a.sorted_keys[j] & 63u;
             r = atomicAdd(&S.ccount[cell], 1u);
         }
         __syncthreads();
         if(threadIdx.x == 0) S.scene = sid;
+        if(mine) {
+            particle_factors(a, S.sc, s + part + threadIdx.x * parts, P);
+            factor_bounds(P, bnd);
+        }
+#pragma unroll
+        for(int q = 0; q < 4; q++) {
+            float v = bnd[q];
+#pragma unroll
+            for(int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if(lane == 0 && v != 0.f) atomicAdd(&S.bound[q], v);
+        }
         if(threadIdx.x < 64) {
             uint32_t c = S.ccount[threadIdx.x];
 #pragma unroll
@@ -904,6 +971,18 @@ template<int T> __global__ void __launch_bounds__(T, 1024 / T) k_p2g(FastArgs a)
                 S.rsize[rr] = __popc(lo) + __popc(hi);
             }
         }
+        if(threadIdx.x >= T - 4) {   // the scale of each quantity
+            const int q = threadIdx.x - (T - 4);
+            const float B = S.bound[q];
+            float sc = 0.f;
+            if(!isfinite(B)) atomicOr(a.flags, MPM_FLAG_NAN);
+            else if(B > 0.f) {
+                int ex;
+                frexpf(B, &ex);                      // B < 2^ex
+                sc = ldexpf(1.f, 21 - max(ex, -90));
+            }
+            S.scale[q] = sc;
+        }
         __syncthreads();
         if(warp == 0) {   // exclusive scan of the round sizes
             uint32_t carry = 0;
@@ -915,46 +994,27 @@ template<int T> __global__ void __launch_bounds__(T, 1024 / T) k_p2g(FastArgs a)
             }
         }
         __syncthreads();
-        if(mine) S.list[S.roff[r] + __popcll(S.rmask[r] & ((1ull << cell) - 1ull))] = j;
-        __syncthreads();
-        // this thread's particle: factors and the bound of its node values
-        P2GFactors P;
-        float bnd[4] = {0.f, 0.f, 0.f, 0.f};
-        int pc = 0;
         if(mine) {
-            const uint32_t jj = S.list[threadIdx.x];
-            pc = (int)(a.sorted_keys[jj] & 63u);
-            particle_factors(a, S.sc, jj, P);
-            factor_bounds(P, bnd);
-        }
-#pragma unroll
-        for(int q = 0; q < 4; q++) {
-            float v = bnd[q];
-#pragma unroll
-            for(int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if(lane == 0 && v != 0.f) atomicAdd(&S.bound[q], v);
+            const int pos = (int)(S.roff[r] + __popcll(S.rmask[r] & ((1ull << cell) - 1ull)));
+            store_factors(FS, T, pos, P);
+            S.list[pos] = cell;
         }
         __syncthreads();
-        if(threadIdx.x < 4) {
-            const float B = S.bound[threadIdx.x];
-            float sc = 0.f;
-            if(!isfinite(B)) atomicOr(a.flags, MPM_FLAG_NAN);
-            else if(B > 0.f) {
-                int ex;
-                frexpf(B, &ex);                      // B < 2^ex
-                sc = ldexpf(1.f, 30 - max(ex, -90));
-            }
-            S.scale[threadIdx.x] = sc;
-        }
-        __syncthreads();
-        if(mine) {
+        if(mine) {   // the particle at place threadIdx.x of the round-by-round order
+            load_factors(FS, T, threadIdx.x, P);
+            const int pc = (int)S.list[threadIdx.x];
             const float s0 = S.scale[0], s1 = S.scale[1], s2 = S.scale[2], s3 = S.scale[3];
             const int t0 = ptile(pc >> 4, (pc >> 2) & 3, pc & 3);
-            // nearest integer and the residual's 2^-22 units: y - rint(y) is exact in float
+            // y = rint(y) + residual, both as integers without a conversion
+            // instruction: for |x| <= 2^22, x + 1.5 2^23 rounds x to an integer
+            // held in the low mantissa bits (|y| < 2^21 by the scale; the
+            // residual, |y - rint(y)| <= 1/2, goes in units of 2^-23, and
+            // y - rint(y) is exact in float)
             auto add = [&](int q, int t, float y) {
-                const float h = rintf(y);
-                atomicAdd(&S.q[q][t], (int)h);
-                atomicAdd(&S.ql[q][t], __float2int_rn((y - h) * 4194304.f));
+                const float m1 = y + kRoundMagic;
+                const float r = y - (m1 - kRoundMagic);
+                atomicAdd(&S.q[q][t], __float_as_int(m1) - kRoundMagicBits);
+                atomicAdd(&S.ql[q][t], __float_as_int(fmaf(r, 8388608.f, kRoundMagic)) - kRoundMagicBits);
             };
             factor_nodes(P, [&](int ii, int jj, int kk, float m, float px, float py, float pz) {
                 const int t = t0 + ptile(ii, jj, kk);
@@ -980,7 +1040,7 @@ template<int T> __global__ void __launch_bounds__(T, 1024 / T) k_p2g(FastArgs a)
             for(int q = 0; q < 4; q++) {
                 const int hi = S.q[q][u], lo = S.ql[q][u];
                 any |= (hi | lo) != 0;
-                v[q] = (float)(((double)hi + (double)lo * 2.384185791015625e-07) * inv[q]);
+                v[q] = (float)(((double)hi + (double)lo * 1.1920928955078125e-07) * inv[q]);
             }
             if(any)
                 atomicAdd(&a.acc[node_index(sc, 4 * bx + tx, 4 * by + ty, 4 * bz + tz)], make_float4(v[1], v[2], v[3], v[0]));
@@ -2481,7 +2541,15 @@ static int fast_route(mpm_handle* h)
 
 template<int T> static void launch_p2g(mpm_handle* h, const FastArgs& a)
 {
-    k_p2g<T><<<occupancy_ctas(h, (const void*)k_p2g<T>, T, h->fast.cta_mult), T, 0, h->stream>>>(a);
+    const int smem = NFAC * T * (int)sizeof(float);
+    static bool attr = false;
+    if(!attr) {
+        cudaFuncSetAttribute((const void*)k_p2g<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_p2g<T>, T, smem);
+    k_p2g<T><<<h->sm_count * (occ > 0 ? occ : 1) * h->fast.cta_mult, T, smem, h->stream>>>(a);
 }
 
 template<int T> static void launch_p2g_groups(mpm_handle* h, const FastArgs& a)
