@@ -193,6 +193,14 @@ def read_traffic(kernel, workload=WORKLOAD):
     return None
 
 
+def hold_gpu(ms=1.0):
+    """A bounded spin kernel on the current stream: the host queues the next
+    substep's launches and events while it runs, so that the per-kernel event
+    times measure the kernels back to back rather than the host's launch gaps."""
+    import torch
+    torch.cuda._sleep(int(ms * 2e6))
+
+
 def measure_substeps(drv, stream, flush, steps, warmup, dist=None, clock_index=None):
     """Warm up, take per-kernel shares from an eager event-timed pass, then time
     `steps` graph-replayed substeps, each bracketed by CUDA events on the
@@ -205,6 +213,7 @@ def measure_substeps(drv, stream, flush, steps, warmup, dist=None, clock_index=N
     for _ in range(4):
         with torch.cuda.stream(stream):
             flush.fill_(1.0)
+            hold_gpu()
         drv.Advance_One_Time_Step()
     drv.synchronize()
     ktimes = drv.get_timing()
@@ -663,6 +672,8 @@ def profile_case(args, D, S):
                           "kernel_ms_per_substep": {k: v[0] / max(args.steps, 1) for k, v in kt.items()}}), flush=True)
         return 0
     drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+    stream = torch.cuda.Stream()
+    drv.set_stream(stream.cuda_stream)
     if args.shape:
         drv.set_launch_shape(*[int(x) for x in args.shape.split(",")])
     drv.set_scene_particles(scene, dtype=np.float32)
@@ -672,6 +683,8 @@ def profile_case(args, D, S):
     drv.synchronize()
     drv.set_timing(True)
     for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            hold_gpu()
         drv.Advance_One_Time_Step()
     drv.synchronize()
     kt = drv.get_timing()

@@ -64,6 +64,11 @@ constexpr int NPLAS = 13;                  // plastic state floats per particle:
 // then farther than a neighbour, then invalidated.
 constexpr int NDIR = 29;
 constexpr int DIR_STAY = 13, DIR_FAR = 27, DIR_INVALID = 28;
+// Row of a block in the arrival counts (dcount) and offsets (doff): one
+// 128-byte line, entries 0..26 the arrivals from each neighbour direction,
+// 27 the arrivals from farther away, 28 (offsets only) the first tail slot of
+// the particles the block lost out of the domain.
+constexpr int ROW = 32;
 constexpr int SCAN_TILE = 256;             // allocation unit of the block scan's status words (>= its tiles)
 // Largest work item (particles of one block) of each P2G launch shape.
 constexpr int kPartSize[4] = {512, 1024, 128, 256};
@@ -85,7 +90,8 @@ struct FastArgs {
     uint4* chunks;
     // the previous substep's order (routing input)
     const uint32_t *obstart, *obend, *oactive, *octr;
-    uint32_t *dcount, *doff, *far_in, *farpos, *bcount, *scan;
+    uint32_t *dcount, *doff, *scan;
+    unsigned long long* bcount;
     int64_t nblk;               // particle blocks of all scenes
     int part;                   // P2G work-item size (particles)
     uint32_t chunk_cap;         // capacity of the work-item lists
@@ -290,18 +296,19 @@ __global__ void k_init_keys(FastArgs a, const uint8_t* valid_by_slot, uint32_t* 
 // The substep's particle order, built from the previous one.
 //
 // The previous G2P wrote every particle's new cell key to its slot and
-// counted, per block it processed, how many of its particles moved to each
-// neighbour block (dcount[d][block], d the move direction) and how many left
-// the domain (d = DIR_INVALID); a particle that moved farther than a
-// neighbour block adds one arrival to its new block (far_in).  Slots are
-// grouped by their previous block, in block order.  A stable sort by block
-// key is then: new block b holds the particles that came from block
-// b - delta(d) with direction d, group after group in the order of those
-// previous blocks (each group in slot order), then its far arrivals; all valid particles come first, in block order, then the
-// particles the last G2P invalidated (in slot order), then those invalid
-// before.  k_bins scans the per-block counts into block ranges (one pass of
-// decoupled look-back over tiles of blocks) and hands out the work items;
-// k_route moves every slot to its place.  This takes the place of a radix
+// counted, in the row of each block, how many particles arrived from each
+// neighbour block (dcount[block][d], d the move direction, d = DIR_FAR for
+// arrivals from farther away), and per block the particles it received and
+// the particles it lost out of the domain (bcount).  Slots are grouped by
+// their previous block, in block order.  A stable sort by block key is then:
+// new block b holds the particles that came from block b - delta(d) with
+// direction d, group after group in the order of those previous blocks (each
+// group in slot order), then its far arrivals; all valid particles come
+// first, in block order, then the particles the last G2P invalidated (in slot
+// order), then those invalid before.  k_bins scans the per-block counts into
+// block ranges (one pass of decoupled look-back over tiles of blocks), turns
+// each block's row of counts into the row of its groups' offsets and hands out
+// the work items; k_route moves every slot to its place.  This takes the place of a radix
 // sort of the keys every substep: the order equals a stable sort by block key
 // whenever no particle crossed more than one block (4 cells) in the substep;
 // far arrivals go to the end of their block in arrival order.  The
@@ -335,9 +342,13 @@ __device__ __forceinline__ int key_dir(const SceneDev& sc, uint32_t b, int bx, i
 // Decoupled look-back of one running count by one warp: publish the tile's
 // aggregate, add the predecessors' aggregates until an inclusive prefix, then
 // publish the inclusive prefix; returns the exclusive prefix (every lane).
-// Status word: epoch (30 bits) | flag (2 bits: 1 aggregate, 2 inclusive) |
-// value (32 bits).  The wait is bounded: past the limit the tile sets the
-// timeout flag and goes on with what it has summed.
+// Each round reads a window of 32 predecessors.  Status word of tile t at
+// status[t * STATUS_STRIDE], one per 32-byte sector (the polling of all tiles
+// then spreads over many L2 lines): epoch (30 bits) | flag (2 bits: 1
+// aggregate, 2 inclusive) | value (32 bits).  The wait is bounded: past the
+// limit the tile sets the timeout flag and goes on with what it has summed.
+constexpr int STATUS_STRIDE = 4;
+
 __device__ uint32_t warp_lookback(uint64_t* status, int64_t tile, uint32_t agg, uint64_t epoch, unsigned* flags)
 {
     using ref = cuda::atomic_ref<uint64_t, cuda::thread_scope_device>;
@@ -346,13 +357,13 @@ __device__ uint32_t warp_lookback(uint64_t* status, int64_t tile, uint32_t agg, 
         if(lane == 0) ref(status[0]).store((epoch << 34) | (2ull << 32) | agg, cuda::memory_order_relaxed);
         return 0;
     }
-    if(lane == 0) ref(status[tile]).store((epoch << 34) | (1ull << 32) | agg, cuda::memory_order_relaxed);
+    if(lane == 0) ref(status[tile * STATUS_STRIDE]).store((epoch << 34) | (1ull << 32) | agg, cuda::memory_order_relaxed);
     uint32_t excl = 0, spins = 0;
     int64_t j = tile - 1;
     for(;;) {
         const int64_t t = j - lane;
         uint64_t w = (epoch << 34) | (2ull << 32);          // before tile 0: an inclusive zero
-        if(t >= 0) w = ref(status[t]).load(cuda::memory_order_relaxed);
+        if(t >= 0) w = ref(status[t * STATUS_STRIDE]).load(cuda::memory_order_relaxed);
         const uint32_t fl = (w >> 34) == epoch ? (uint32_t)(w >> 32) & 3u : 0u;
         const unsigned pending = __ballot_sync(0xffffffffu, fl == 0);
         const unsigned incl = __ballot_sync(0xffffffffu, fl == 2);
@@ -370,7 +381,7 @@ __device__ uint32_t warp_lookback(uint64_t* status, int64_t tile, uint32_t agg, 
             break;
         }
     }
-    if(lane == 0) ref(status[tile]).store((epoch << 34) | (2ull << 32) | (excl + agg), cuda::memory_order_relaxed);
+    if(lane == 0) ref(status[tile * STATUS_STRIDE]).store((epoch << 34) | (2ull << 32) | (excl + agg), cuda::memory_order_relaxed);
     return excl;
 }
 
@@ -385,34 +396,33 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x)
     return x;
 }
 
-// Tiles of BIN_TILE blocks of all scenes in ticket order, BIN_PER consecutive
-// blocks per thread: each block's particle count (arrivals the last G2P
-// counted), the exclusive prefix over all blocks (block ranges), the active
-// blocks and the work items (parts of at most a.part particles); for an
-// active block the offsets at which each (previous block, direction) group
-// of its particles lands.  Consumed counts are zeroed for the next G2P.
-constexpr int BIN_THREADS = 256, BIN_PER = 4, BIN_TILE = BIN_THREADS * BIN_PER;
+// Tiles of BIN_TILE blocks of all scenes, one per CTA in launch order (a
+// tile waits only on tiles of lower index, whose CTAs start first), BIN_PER
+// consecutive blocks per thread: each block's arrivals and departures out of
+// the domain, the exclusive prefix over all blocks (block ranges, tail slots
+// of the departed), the active blocks and the work items (parts of at most
+// a.part particles); for an active block its row of group offsets, from its
+// row of arrival counts (loaded while the tile looks back, so that no tile
+// publishes its aggregate late).  Consumed counts are zeroed for the next G2P.
+constexpr int BIN_THREADS = 512, BIN_PER = 2, BIN_TILE = BIN_THREADS * BIN_PER;
 
 __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
 {
     constexpr int NW = BIN_THREADS / 32;
-    __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp[NW][4];
     __shared__ uint32_t s_pre[4];         // prefixes of the tile: count, invalid (look-back); parts, active (bases)
-    __shared__ uint2 s_act[BIN_TILE];     // the tile's active blocks: block, first sorted position
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if(threadIdx.x == 0) s_tile = atomicAdd(&a.ctr[CNT_BIN_TICKET], 1u);
-    __syncthreads();
-    const int64_t tile = s_tile, ntiles = (a.nblk + BIN_TILE - 1) / BIN_TILE;
+    const int64_t tile = blockIdx.x, ntiles = (a.nblk + BIN_TILE - 1) / BIN_TILE;
     const int64_t b0 = tile * BIN_TILE + threadIdx.x * BIN_PER;
     const uint64_t epoch = a.scan[0] & mpm_sort::kEpochMask;
-    uint64_t* status = reinterpret_cast<uint64_t*>(a.scan + 2);
+    uint64_t* status = reinterpret_cast<uint64_t*>(a.scan + 8);
     uint32_t cnt[BIN_PER], inv[BIN_PER], v[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
     for(int u = 0; u < BIN_PER; u++) {
         const int64_t b = b0 + u;
-        cnt[u] = b < a.nblk ? a.bcount[b] : 0u;
-        inv[u] = b < a.nblk ? a.dcount[DIR_INVALID * a.nblk + b] : 0u;
+        const unsigned long long c = b < a.nblk ? a.bcount[b] : 0ull;
+        cnt[u] = (uint32_t)c;
+        inv[u] = (uint32_t)(c >> 32);
         v[0] += cnt[u];
         v[1] += inv[u];
         v[2] += cnt[u] ? (cnt[u] + a.part - 1) / a.part : 0u;
@@ -444,12 +454,36 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
         const uint32_t p = warp_lookback(status, tile, tot[0], epoch, a.flags);
         if(lane == 0) s_pre[0] = p;
     } else if(warp == 1) {
-        const uint32_t p = warp_lookback(status + ntiles, tile, tot[1], epoch, a.flags);
+        const uint32_t p = warp_lookback(status + ntiles * STATUS_STRIDE, tile, tot[1], epoch, a.flags);
         if(lane == 0) s_pre[1] = p;
     } else if(threadIdx.x == 64) {
         s_pre[2] = tot[2] ? atomicAdd(&a.ctr[CNT_CHUNKS], tot[2]) : 0u;
         s_pre[3] = tot[3] ? atomicAdd(&a.ctr[CNT_ACTIVE_BLOCKS], tot[3]) : 0u;
     }
+    // the arrival rows of the active blocks, as offsets within the block: the
+    // groups in the order of their previous blocks (direction falling), then the far arrivals
+    uint32_t rel[BIN_PER][28];
+    bool consistent = true;
+#pragma unroll
+    for(int u = 0; u < BIN_PER; u++) {
+        if(!cnt[u]) continue;
+        const uint4* row = reinterpret_cast<const uint4*>(a.dcount + (size_t)(b0 + u) * ROW);
+#pragma unroll
+        for(int k = 0; k < 7; k++) {
+            const uint4 r4 = row[k];
+            rel[u][4 * k] = r4.x; rel[u][4 * k + 1] = r4.y; rel[u][4 * k + 2] = r4.z; rel[u][4 * k + 3] = r4.w;
+        }
+        uint32_t run = 0;
+#pragma unroll
+        for(int d = 26; d >= 0; d--) {
+            const uint32_t c = rel[u][d];
+            rel[u][d] = run;
+            run += c;
+        }
+        consistent &= run + rel[u][DIR_FAR] == cnt[u];
+        rel[u][DIR_FAR] = run;
+    }
+    if(!consistent) atomicOr(a.flags, MPM_FLAG_ORDER);   // counts out of step: report
     __syncthreads();
     if(tile == ntiles - 1 && threadIdx.x == 0) {
         a.ctr[CNT_ACTIVE_PARTICLES] = s_pre[0] + tot[0];
@@ -458,57 +492,34 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
     uint32_t ex[4];
 #pragma unroll
     for(int q = 0; q < 4; q++) ex[q] = s_pre[q] + s_warp[warp][q] + x[q] - v[q];
-    // ranges, work items and the active list; the tile's active blocks go to
-    // shared memory so that their neighbour loads spread over all threads
-    const uint32_t act0 = s_pre[3];   // the tile's first active-list slot
+    // ranges, offset rows, work items and the active list
+#pragma unroll
     for(int u = 0; u < BIN_PER; u++) {
         const int64_t b = b0 + u;
-        if(inv[u]) {
-            a.doff[DIR_INVALID * a.nblk + b] = ex[1];
-            a.dcount[DIR_INVALID * a.nblk + b] = 0u;
+        if(!cnt[u] && !inv[u]) continue;
+        a.bcount[b] = 0ull;
+        if(!cnt[u]) {
+            a.doff[(size_t)b * ROW + DIR_INVALID] = ex[1];
             ex[1] += inv[u];
+            continue;
         }
-        if(!cnt[u]) continue;
         const uint32_t start = ex[0], parts = (cnt[u] + a.part - 1) / a.part;
         ex[0] += cnt[u];
         a.bstart[b] = start;
         a.bend[b] = start + cnt[u];
-        a.bcount[b] = 0u;
-        s_act[ex[3] - act0] = make_uint2((uint32_t)b, start);
+        uint4* orow = reinterpret_cast<uint4*>(a.doff + (size_t)b * ROW);
+        uint4* crow = reinterpret_cast<uint4*>(a.dcount + (size_t)b * ROW);
+#pragma unroll
+        for(int k = 0; k < 7; k++) {
+            orow[k] = make_uint4(start + rel[u][4 * k], start + rel[u][4 * k + 1], start + rel[u][4 * k + 2],
+                                 start + rel[u][4 * k + 3]);
+            crow[k] = make_uint4(0u, 0u, 0u, 0u);
+        }
+        orow[7] = make_uint4(ex[1], 0u, 0u, 0u);   // DIR_INVALID: the departed's first tail slot
+        ex[1] += inv[u];
         a.active[ex[3]++] = (uint32_t)b;
         for(uint32_t k = 0; k < parts; k++, ex[2]++)
             if(ex[2] < a.chunk_cap) a.chunks[ex[2]] = make_uint4((uint32_t)b, k, parts, 0u);
-    }
-    __syncthreads();
-    for(uint32_t i = threadIdx.x; i < tot[3]; i += BIN_THREADS) {
-        const uint32_t b = s_act[i].x, start = s_act[i].y;
-        // the groups of arrivals, in the order of their previous block (slot order):
-        // block b - delta(d) grows as d falls
-        const SceneDev& sc = a.scenes[a.block_scene[b]];
-        int bx, by, bz;
-        block_coords(sc, (uint32_t)(b - sc.block_base), bx, by, bz);
-        uint32_t src[27], cin[27];
-#pragma unroll
-        for(int d = 0; d < 27; d++) {
-            const int ox = bx - dir_dx(d), oy = by - dir_dy(d), oz = bz - dir_dz(d);
-            const bool in = ox >= 0 && oy >= 0 && oz >= 0 && ox < sc.NB[0] && oy < sc.NB[1] && oz < sc.NB[2];
-            src[d] = in ? sc.block_base + ((uint32_t)ox * sc.NB[1] + oy) * sc.NB[2] + oz : SENTINEL;
-        }
-#pragma unroll
-        for(int d = 0; d < 27; d++) cin[d] = src[d] != SENTINEL ? a.dcount[d * a.nblk + src[d]] : 0u;
-        uint32_t run = start;
-#pragma unroll
-        for(int d = 26; d >= 0; d--) {
-            if(cin[d]) {
-                a.doff[d * a.nblk + src[d]] = run;
-                run += cin[d];
-                a.dcount[d * a.nblk + src[d]] = 0u;
-            }
-        }
-        if(run != a.bend[b]) {          // far arrivals fill the rest of the block
-            a.farpos[b] = run;
-            a.far_in[b] = 0u;
-        }
     }
 }
 
@@ -560,11 +571,11 @@ __global__ void __launch_bounds__(256) k_route(FastArgs a)
                 uint32_t rank = s_run[d] + intra;
                 for(int w2 = 0; w2 < warp; w2++) rank += s_wc[w2][d];
                 uint32_t dest;
-                if(d < 27) dest = a.doff[d * a.nblk + o] + rank;
+                if(d < 27) dest = a.doff[(size_t)(key >> 6) * ROW + d] + rank;
                 else if(d == DIR_FAR) {
-                    dest = atomicAdd(&a.farpos[key >> 6], 1u);
+                    dest = atomicAdd(&a.doff[(size_t)(key >> 6) * ROW + DIR_FAR], 1u);
                     atomicAdd(&a.ctr[CNT_FAR], 1u);
-                } else dest = nvalid + a.doff[DIR_INVALID * a.nblk + o] + rank;
+                } else dest = nvalid + a.doff[(size_t)o * ROW + DIR_INVALID] + rank;
                 if(dest < a.n) {
                     if(d == DIR_INVALID) copy_slot(a, j, dest, SENTINEL);
                     a.perm[dest] = j;
@@ -615,8 +626,8 @@ __global__ void k_prepare(FastArgs a, uint32_t* pbstart, uint32_t* pbend, uint32
         const uint32_t b = k >> 6;
         const unsigned peers = __match_any_sync(0xffffffffu, valid ? b : 0xffffffffu);
         if(valid && (__ffs(peers) - 1) == lane) {
-            atomicAdd(&a.dcount[DIR_STAY * a.nblk + b], (uint32_t)__popc(peers));
-            atomicAdd(&a.bcount[b], (uint32_t)__popc(peers));
+            atomicAdd(&a.dcount[(size_t)b * ROW + DIR_STAY], (uint32_t)__popc(peers));
+            atomicAdd(&a.bcount[b], (unsigned long long)__popc(peers));
         }
         if(!in) continue;
         const uint32_t kp = j ? a.sorted_keys[j - 1] : SENTINEL;
@@ -1750,8 +1761,8 @@ template<int THREADS, int PK> __global__ void __launch_bounds__(THREADS) k_g2p(F
             g2p_particle<PK>(a, sc, t4, anti, ox, oy, oz, j, o);
             const int d = key_dir(sc, b, bx, by, bz, o.key);
             if(d == DIR_FAR) {
-                atomicAdd(&a.far_in[o.key >> 6], 1u);
-                atomicAdd(&a.bcount[o.key >> 6], 1u);
+                atomicAdd(&a.dcount[(size_t)(o.key >> 6) * ROW + DIR_FAR], 1u);
+                atomicAdd(&a.bcount[o.key >> 6], 1ull);
             }
             const unsigned act = __activemask();
             const unsigned peers = __match_any_sync(act, d);
@@ -1761,10 +1772,11 @@ template<int THREADS, int PK> __global__ void __launch_bounds__(THREADS) k_g2p(F
         if(threadIdx.x < NDIR) {
             const int d = threadIdx.x;
             const uint32_t c2 = s_dc[d];
-            if(c2 && d != DIR_FAR) {
-                atomicAdd(&a.dcount[d * a.nblk + b], c2);
-                if(d < 27)   // the neighbour block it moved to: block + delta(d)
-                    atomicAdd(&a.bcount[b + ((dir_dx(d) * sc.NB[1]) + dir_dy(d)) * sc.NB[2] + dir_dz(d)], c2);
+            if(c2 && d == DIR_INVALID) atomicAdd(&a.bcount[b], (unsigned long long)c2 << 32);
+            else if(c2 && d != DIR_FAR) {   // the neighbour block they moved to: block + delta(d)
+                const uint32_t nb = b + ((dir_dx(d) * sc.NB[1]) + dir_dy(d)) * sc.NB[2] + dir_dz(d);
+                atomicAdd(&a.dcount[(size_t)nb * ROW + d], c2);
+                atomicAdd(&a.bcount[nb], (unsigned long long)c2);
             }
             s_dc[d] = 0u;
         }
@@ -1925,7 +1937,7 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.ctr = f.counters ? f.counters + CNT_COUNT * c : nullptr;
     a.obstart = f.bstart[o]; a.obend = f.bend[o]; a.oactive = f.active[o];
     a.octr = f.counters ? f.counters + CNT_COUNT * o : nullptr;
-    a.dcount = f.dcount; a.doff = f.doff; a.far_in = f.far_in; a.farpos = f.farpos; a.bcount = f.bcount; a.scan = f.scan;
+    a.dcount = f.dcount; a.doff = f.doff; a.bcount = f.bcount; a.scan = f.scan;
     a.nblk = f.total_blocks;
     a.part = kPartSize[f.route_variant];
     a.chunk_cap = (uint32_t)f.chunk_cap;
@@ -2093,17 +2105,14 @@ int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, con
     MPM_CUDA(h, cudaMemset(f.counters, 0, 2 * CNT_COUNT * sizeof(uint32_t)));
     // routing between substeps: direction counts and offsets, far arrivals,
     // the block scan's epoch word and look-back status words (two chains)
-    MPM_CUDA(h, cudaMalloc(&f.dcount, (size_t)NDIR * blocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMalloc(&f.doff, (size_t)NDIR * blocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMalloc(&f.far_in, blocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMalloc(&f.farpos, blocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMalloc(&f.bcount, blocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMemset(f.bcount, 0, blocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMemset(f.dcount, 0, (size_t)NDIR * blocks * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMemset(f.far_in, 0, blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.dcount, (size_t)ROW * blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.doff, (size_t)ROW * blocks * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.bcount, blocks * sizeof(unsigned long long)));
+    MPM_CUDA(h, cudaMemset(f.bcount, 0, blocks * sizeof(unsigned long long)));
+    MPM_CUDA(h, cudaMemset(f.dcount, 0, (size_t)ROW * blocks * sizeof(uint32_t)));
     const int64_t tiles = (blocks + SCAN_TILE - 1) / SCAN_TILE;
-    MPM_CUDA(h, cudaMalloc(&f.scan, (2 + 4 * tiles) * sizeof(uint32_t)));
-    MPM_CUDA(h, cudaMemset(f.scan, 0, (2 + 4 * tiles) * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMalloc(&f.scan, (8 + 4 * STATUS_STRIDE * tiles) * sizeof(uint32_t)));
+    MPM_CUDA(h, cudaMemset(f.scan, 0, (8 + 4 * STATUS_STRIDE * tiles) * sizeof(uint32_t)));
     f.order_ready = false;
     f.sorted_now = false;
     return encode_tile_maps(h);
@@ -2245,8 +2254,8 @@ void fast_free(mpm_handle* h)
                    (void**)&f.bend[1], (void**)&f.active[1], (void**)&f.chunks[1], (void**)&f.nb_flag,
                    (void**)&f.nb_list, (void**)&f.counters, (void**)&f.acc, (void**)&f.vel, (void**)&f.scenes,
                    (void**)&f.block_scene, (void**)&f.nb_scene, (void**)&f.pbase, (void**)&f.objs, (void**)&f.vkick,
-                   (void**)&f.pmodel, (void**)&f.pmask, (void**)&f.dcount, (void**)&f.doff, (void**)&f.far_in,
-                   (void**)&f.farpos, (void**)&f.scan, (void**)&f.tmaps, (void**)&f.bcount};
+                   (void**)&f.pmodel, (void**)&f.pmask, (void**)&f.dcount, (void**)&f.doff,
+                   (void**)&f.scan, (void**)&f.tmaps, (void**)&f.bcount};
     for(void** p: ps) { cudaFree(*p); *p = nullptr; }
     f.order_ready = false;
     f.sorted_now = false;
@@ -2504,9 +2513,8 @@ int fast_prepare(mpm_handle* h)
                                          f.sort_scratch, h->d_flags, MPM_FLAG_TIMEOUT, h->sm_count * 4, h->stream);
     if(e != cudaSuccess) return check_cuda(h, e, "radix_sort");
     timer_end(h, slot);
-    MPM_CUDA(h, cudaMemsetAsync(f.dcount, 0, (size_t)NDIR * f.total_blocks * sizeof(uint32_t), h->stream));
-    MPM_CUDA(h, cudaMemsetAsync(f.far_in, 0, f.total_blocks * sizeof(uint32_t), h->stream));
-    MPM_CUDA(h, cudaMemsetAsync(f.bcount, 0, f.total_blocks * sizeof(uint32_t), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(f.dcount, 0, (size_t)ROW * f.total_blocks * sizeof(uint32_t), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(f.bcount, 0, f.total_blocks * sizeof(unsigned long long), h->stream));
     MPM_CUDA(h, cudaMemsetAsync(f.counters + CNT_COUNT * c, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
     FastArgs a = make_args(h, 0.0);
     k_prepare<<<grid_stride_blocks(h, n, 256), 256, 0, h->stream>>>(a, f.bstart[c], f.bend[c], f.active[c],

@@ -87,14 +87,13 @@ struct FastState {
     uint4* chunks[2] = {nullptr, nullptr};    // work items: (block, part, parts, 0)
     int64_t chunk_cap = 0;
     // routing from one substep's order to the next (mpm_fast.cu, k_bins / k_route):
-    // per (block, direction) counts written by G2P and their offsets, arrivals
-    // from farther than a neighbour block, look-back status of the block scan
-    uint32_t* dcount = nullptr;               // NDIR x total_blocks
-    uint32_t* doff = nullptr;                 // NDIR x total_blocks
-    uint32_t* far_in = nullptr;               // total_blocks
-    uint32_t* farpos = nullptr;               // total_blocks
-    uint32_t* bcount = nullptr;               // total_blocks: particles arriving in each block (near and far)
-    uint32_t* scan = nullptr;                 // epoch word, then 2 x tiles uint64 status words
+    // per block a row of arrival counts by direction (G2P) and the row of their
+    // sorted offsets, per block its arrivals and departures out of the domain,
+    // look-back status of the block scan
+    uint32_t* dcount = nullptr;               // total_blocks x 32
+    uint32_t* doff = nullptr;                 // total_blocks x 32
+    unsigned long long* bcount = nullptr;     // total_blocks: arrivals (low word), invalidated (high word)
+    uint32_t* scan = nullptr;                 // epoch word, then the look-back status words (two chains)
     void* tmaps = nullptr;                    // per scene: CUtensorMap of its node grid (G2P tiles by TMA)
     bool order_ready = false;                 // the previous set + dcount describe the current slots
     bool sorted_now = false;                  // this substep's order is built (P2G may repeat)
@@ -133,7 +132,7 @@ enum FastCounter {
     CNT_P2G_DONE = 7,
     CNT_CHUNKS = 8,                // work items in the set's chunk list
     CNT_NEW_INVALID = 9,           // particles the last G2P invalidated
-    CNT_BIN_TICKET = 10,           // tile tickets of the block scan
+    CNT_SPARE = 10,                // (unused)
     CNT_FAR = 11,                  // particles that moved past a neighbour block
     CNT_COUNT = 16
 };
