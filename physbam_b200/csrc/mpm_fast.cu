@@ -64,10 +64,12 @@ constexpr int NPLAS = 13;                  // plastic state floats per particle:
 // then farther than a neighbour, then invalidated.
 constexpr int NDIR = 29;
 constexpr int DIR_STAY = 13, DIR_FAR = 27, DIR_INVALID = 28;
-// Row of a block in the arrival counts (dcount) and offsets (doff): one
-// 128-byte line, entries 0..26 the arrivals from each neighbour direction,
-// 27 the arrivals from farther away, 28 (offsets only) the first tail slot of
-// the particles the block lost out of the domain.
+// Row of a block in the arrival counts (dcount): one 128-byte line, entries
+// 0..26 the arrivals from each neighbour direction, 27 the arrivals from
+// farther away.  Row of a block in the offsets (doff): entries 0..26 the first
+// sorted position of the group of its particles that moved in direction d,
+// 27 the next sorted position of an arrival from farther away, 28 the first
+// tail slot of the particles it lost out of the domain.
 constexpr int ROW = 32;
 constexpr int SCAN_TILE = 256;             // allocation unit of the block scan's status words (>= its tiles)
 // Largest work item (particles of one block) of each P2G launch shape.
@@ -85,11 +87,15 @@ struct FastArgs {
     uint32_t* sorted_keys;
     const uint32_t* keys_cur;   // cell keys of the current buffer's slots
     uint32_t* keys_next;        // cell keys of the other buffer's slots (G2P writes them)
+    const uint8_t* dir_cur;     // move directions of the current buffer's slots
+    uint8_t* dir_next;          // move directions of the other buffer's slots (G2P writes them)
     // this substep's order: block ranges, active blocks, work items, counters
-    uint32_t *bstart, *bend, *active, *ctr;
+    uint32_t *bstart, *bend, *ctr;
+    uint4* active;              // active blocks: (block, start, count or SENTINEL, scene)
     uint4* chunks;
     // the previous substep's order (routing input)
-    const uint32_t *obstart, *obend, *oactive, *octr;
+    const uint32_t *obstart, *obend, *octr;
+    const uint4* oactive;
     uint32_t *dcount, *doff, *scan;
     unsigned long long* bcount;
     int64_t nblk;               // particle blocks of all scenes
@@ -396,6 +402,35 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x)
     return x;
 }
 
+// Work items (P2G and G2P): part k of the `parts` parts of a block, two uint4
+// each, (block, k, parts, scene) and (block start, block count, 0, 0), so that
+// a kernel needs no other load to begin an item.  CTAs take items by ticket
+// (an atomic counter: CTAs that finish early take more) ahead of need: P2G
+// holds the next item's descriptor in flight and the ticket after it, so
+// neither round trip falls between two items.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
+                 :: "r"((uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+}
+
+// Thread 0: start the copy of item w's descriptor into dst[0..1] (nothing past the last item).
+__device__ __forceinline__ void work_prefetch(const FastArgs& a, uint32_t w, uint32_t nwork, uint4* dst)
+{
+    if(w < nwork) {
+        cp_async16(dst, a.chunks + 2 * (size_t)w);
+        cp_async16(dst + 1, a.chunks + 2 * (size_t)w + 1);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Thread 0: wait for the copy; past the last item dst holds the end mark.
+__device__ __forceinline__ void work_arrive(uint32_t w, uint32_t nwork, uint4* dst)
+{
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    if(w >= nwork) dst[0] = make_uint4(SENTINEL, 0u, 0u, 0u);
+}
+
 // Tiles of BIN_TILE blocks of all scenes, one per CTA in launch order (a
 // tile waits only on tiles of lower index, whose CTAs start first), BIN_PER
 // consecutive blocks per thread: each block's arrivals and departures out of
@@ -416,11 +451,12 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
     const int64_t b0 = tile * BIN_TILE + threadIdx.x * BIN_PER;
     const uint64_t epoch = a.scan[0] & mpm_sort::kEpochMask;
     uint64_t* status = reinterpret_cast<uint64_t*>(a.scan + 8);
-    uint32_t cnt[BIN_PER], inv[BIN_PER], v[4] = {0u, 0u, 0u, 0u};
+    uint32_t cnt[BIN_PER], inv[BIN_PER], sid[BIN_PER], v[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
     for(int u = 0; u < BIN_PER; u++) {
         const int64_t b = b0 + u;
         const unsigned long long c = b < a.nblk ? a.bcount[b] : 0ull;
+        sid[u] = b < a.nblk ? a.block_scene[b] : 0u;
         cnt[u] = (uint32_t)c;
         inv[u] = (uint32_t)(c >> 32);
         v[0] += cnt[u];
@@ -462,8 +498,10 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
     }
     // the arrival rows of the active blocks, as offsets within the block: the
     // groups in the order of their previous blocks (direction falling), then the far arrivals
-    uint32_t rel[BIN_PER][28];
+    uint32_t rel[BIN_PER][28], nz[BIN_PER];
     bool consistent = true;
+#pragma unroll
+    for(int u = 0; u < BIN_PER; u++) nz[u] = 0u;
 #pragma unroll
     for(int u = 0; u < BIN_PER; u++) {
         if(!cnt[u]) continue;
@@ -479,6 +517,7 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
             const uint32_t c = rel[u][d];
             rel[u][d] = run;
             run += c;
+            nz[u] |= (c ? 1u : 0u) << d;
         }
         consistent &= run + rel[u][DIR_FAR] == cnt[u];
         rel[u][DIR_FAR] = run;
@@ -507,19 +546,25 @@ __global__ void __launch_bounds__(BIN_THREADS) k_bins(FastArgs a)
         ex[0] += cnt[u];
         a.bstart[b] = start;
         a.bend[b] = start + cnt[u];
-        uint4* orow = reinterpret_cast<uint4*>(a.doff + (size_t)b * ROW);
+        // each group's offset into the row of the block it came from (b - delta(d), entry d)
+        const SceneDev& sc = a.scenes[sid[u]];
+        const int64_t sy = sc.NB[2], sx = (int64_t)sc.NB[1] * sc.NB[2];
+#pragma unroll
+        for(int d = 0; d < 27; d++)
+            if((nz[u] >> d) & 1u)
+                a.doff[(size_t)(b - dir_dx(d) * sx - dir_dy(d) * sy - dir_dz(d)) * ROW + d] = start + rel[u][d];
+        a.doff[(size_t)b * ROW + DIR_FAR] = start + rel[u][DIR_FAR];
+        if(inv[u]) a.doff[(size_t)b * ROW + DIR_INVALID] = ex[1];   // the departed's first tail slot
+        ex[1] += inv[u];
         uint4* crow = reinterpret_cast<uint4*>(a.dcount + (size_t)b * ROW);
 #pragma unroll
-        for(int k = 0; k < 7; k++) {
-            orow[k] = make_uint4(start + rel[u][4 * k], start + rel[u][4 * k + 1], start + rel[u][4 * k + 2],
-                                 start + rel[u][4 * k + 3]);
-            crow[k] = make_uint4(0u, 0u, 0u, 0u);
-        }
-        orow[7] = make_uint4(ex[1], 0u, 0u, 0u);   // DIR_INVALID: the departed's first tail slot
-        ex[1] += inv[u];
-        a.active[ex[3]++] = (uint32_t)b;
+        for(int k = 0; k < 7; k++) crow[k] = make_uint4(0u, 0u, 0u, 0u);
+        a.active[ex[3]++] = make_uint4((uint32_t)b, start, cnt[u], sid[u]);
         for(uint32_t k = 0; k < parts; k++, ex[2]++)
-            if(ex[2] < a.chunk_cap) a.chunks[ex[2]] = make_uint4((uint32_t)b, k, parts, 0u);
+            if(ex[2] < a.chunk_cap) {
+                a.chunks[2 * (size_t)ex[2]] = make_uint4((uint32_t)b, k, parts, sid[u]);
+                a.chunks[2 * (size_t)ex[2] + 1] = make_uint4(start, cnt[u], 0u, 0u);
+            }
     }
 }
 
@@ -539,60 +584,94 @@ __device__ __forceinline__ void copy_slot(const FastArgs& a, uint32_t j, uint32_
 // Every slot of the current buffer to its place in the new order (perm[dest]
 // = slot, sorted key).  Valid particles keep their state in place (P2G and
 // G2P read it through perm); invalid ones are copied to their tail slot of
-// the other buffer, which G2P does not write.  One CTA per previous block at
-// a time; ranks within (block, direction) follow slot order.
+// the other buffer, which G2P does not write.
+//
+// A group of G warps per previous block, G (1, 2, 4 or 8) as large as keeps
+// every block in flight at once: many blocks per SM when there are many, many
+// warps per block when there are few.  Per batch, warp k of the group takes
+// RW rounds of 32 consecutive slots (keys and the move directions G2P
+// recorded, loaded together) after those of warps 0..k-1, counts each round's
+// directions into its rows of shared memory and turns them into ranks; the
+// group then offsets each warp's ranks by the counts of the warps before it
+// and by the direction's next destination (first: entry d of the block's
+// offset row, which k_bins wrote), so that ranks follow slot order.  The
+// group synchronises on its own named barrier, never the whole CTA.
 __global__ void __launch_bounds__(256) k_route(FastArgs a)
 {
-    constexpr int W = 8;
-    __shared__ uint32_t s_wc[W][32];      // particles per warp and direction, this round
-    __shared__ uint32_t s_run[32];        // particles per direction, earlier rounds
+    constexpr int W = 8, RW = 4, CS = 33;       // warps per CTA, rounds per warp and batch, padded row
+    __shared__ uint32_t s_cnt[W * RW][CS];      // per warp and round: count per direction, then rank
+    __shared__ uint32_t s_tot[W][32];           // per warp: its batch's count per direction
+    __shared__ uint32_t s_next[W][32];          // per group (its last warp): next destination per direction
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
     const uint32_t nold = a.octr[CNT_ACTIVE_BLOCKS], nvalid_old = a.octr[CNT_ACTIVE_PARTICLES];
     const uint32_t nvalid = a.ctr[CNT_ACTIVE_PARTICLES], ninv = a.ctr[CNT_NEW_INVALID];
-    (&s_wc[0][0])[threadIdx.x] = 0u;
-    for(uint32_t w = blockIdx.x; w < nold; w += gridDim.x) {
-        const uint32_t o = a.oactive[w];
-        const SceneDev& sc = a.scenes[a.block_scene[o]];
-        int ox, oy, oz;
-        block_coords(sc, o - sc.block_base, ox, oy, oz);
-        const uint32_t s = a.obstart[o], e = a.obend[o];
-        if(threadIdx.x < 32) s_run[threadIdx.x] = 0u;
-        __syncthreads();
-        for(uint32_t base = s; base < e; base += 256) {
-            const uint32_t j = base + threadIdx.x;
-            const bool ok = j < e;
-            const uint32_t key = ok ? a.keys_cur[j] : SENTINEL;
-            const int d = ok ? key_dir(sc, o, ox, oy, oz, key) : 31;
-            const unsigned peers = __match_any_sync(0xffffffffu, d);
-            const uint32_t intra = __popc(peers & ((1u << lane) - 1u));
-            if(ok && (__ffs(peers) - 1) == lane) s_wc[warp][d] = __popc(peers);
-            __syncthreads();
-            if(ok) {
-                uint32_t rank = s_run[d] + intra;
-                for(int w2 = 0; w2 < warp; w2++) rank += s_wc[w2][d];
+    int G = 1;
+    while(G < W && (uint64_t)nold * (uint64_t)(2 * G) <= (uint64_t)gridDim.x * W) G *= 2;
+    const int gw = warp % G, g0 = warp - gw, last = g0 + G - 1;
+    const uint32_t groups = gridDim.x * (uint32_t)(W / G);
+    auto gsync = [&]() {
+        if(G == 1) __syncwarp();
+        else asm volatile("bar.sync %0, %1;" :: "r"(1 + warp / G), "r"(32 * G) : "memory");
+    };
+    for(uint32_t w = blockIdx.x * (uint32_t)(W / G) + (uint32_t)(warp / G); w < nold; w += groups) {
+        const uint4 od = a.oactive[w];
+        const uint32_t o = od.x, s = od.y, e = od.z != SENTINEL ? od.y + od.z : a.obend[o];
+        if(warp == last) {   // lane d: the first destination of direction d (other entries are not read)
+            const uint32_t first = a.doff[(size_t)o * ROW + lane];
+            s_next[g0][lane] = lane == DIR_INVALID ? nvalid + first : first;
+        }
+        for(uint32_t jb = s; jb < e; jb += (uint32_t)(32 * RW * G)) {
+            const uint32_t jw = jb + (uint32_t)(32 * RW * gw);
+            uint32_t key[RW], intra[RW];
+            int dr[RW];
+#pragma unroll
+            for(int r = 0; r < RW; r++) {
+                const uint32_t j = jw + 32 * r + lane;
+                key[r] = j < e ? a.keys_cur[j] : SENTINEL;
+                dr[r] = j < e ? a.dir_cur[j] : 31;
+                s_cnt[warp * RW + r][lane] = 0u;
+            }
+            __syncwarp();
+#pragma unroll
+            for(int r = 0; r < RW; r++) {
+                const unsigned peers = __match_any_sync(0xffffffffu, dr[r]);
+                intra[r] = __popc(peers & below);
+                if(dr[r] != 31 && (__ffs(peers) - 1) == lane) s_cnt[warp * RW + r][dr[r]] = __popc(peers);
+            }
+            __syncwarp();
+            uint32_t run = 0;                    // lane d: this warp's ranks of direction d
+#pragma unroll
+            for(int r = 0; r < RW; r++) {
+                const uint32_t c = s_cnt[warp * RW + r][lane];
+                s_cnt[warp * RW + r][lane] = run;
+                run += c;
+            }
+            s_tot[warp][lane] = run;
+            gsync();
+            uint32_t base = s_next[g0][lane];
+            for(int k = g0; k < warp; k++) base += s_tot[k][lane];
+#pragma unroll
+            for(int r = 0; r < RW; r++) s_cnt[warp * RW + r][lane] += base;
+            __syncwarp();
+#pragma unroll
+            for(int r = 0; r < RW; r++) {
+                const int d = dr[r];
+                if(d == 31) continue;
+                const uint32_t j = jw + 32 * r + lane;
                 uint32_t dest;
-                if(d < 27) dest = a.doff[(size_t)(key >> 6) * ROW + d] + rank;
-                else if(d == DIR_FAR) {
-                    dest = atomicAdd(&a.doff[(size_t)(key >> 6) * ROW + DIR_FAR], 1u);
+                if(d == DIR_FAR) {
+                    dest = atomicAdd(&a.doff[(size_t)(key[r] >> 6) * ROW + DIR_FAR], 1u);
                     atomicAdd(&a.ctr[CNT_FAR], 1u);
-                } else dest = nvalid + a.doff[(size_t)o * ROW + DIR_INVALID] + rank;
+                } else dest = s_cnt[warp * RW + r][d] + intra[r];
                 if(dest < a.n) {
                     if(d == DIR_INVALID) copy_slot(a, j, dest, SENTINEL);
                     a.perm[dest] = j;
-                    a.sorted_keys[dest] = key;
+                    a.sorted_keys[dest] = key[r];
                 } else atomicOr(a.flags, MPM_FLAG_ORDER);   // counts out of step: report, write nothing
             }
-            __syncthreads();
-            if(threadIdx.x < 32) {
-                uint32_t t = 0;
-#pragma unroll
-                for(int w2 = 0; w2 < W; w2++) {
-                    t += s_wc[w2][threadIdx.x];
-                    s_wc[w2][threadIdx.x] = 0u;
-                }
-                s_run[threadIdx.x] += t;
-            }
-            __syncthreads();
+            gsync();
+            if(warp == last) s_next[g0][lane] = base + run;
         }
     }
     // the particles invalid before the last G2P follow, in slot order
@@ -614,14 +693,17 @@ __global__ void __launch_bounds__(256) k_route(FastArgs a)
 // sorted order, and that order is recorded as the previous substep's (block
 // ranges and active blocks into the given set, every particle counted as
 // staying in its block), so the next substep's routing is the identity.
-__global__ void k_prepare(FastArgs a, uint32_t* pbstart, uint32_t* pbend, uint32_t* pactive, uint32_t* pctr)
+__global__ void k_prepare(FastArgs a, uint32_t* pbstart, uint32_t* pbend, uint4* pactive, uint32_t* pctr)
 {
     const int lane = threadIdx.x & 31;
     const int64_t end = (a.n + 31) & ~(int64_t)31;      // whole warps stay in the loop
     for(int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < end; j += (int64_t)gridDim.x * blockDim.x) {
         const bool in = j < a.n;
         const uint32_t k = in ? a.sorted_keys[j] : SENTINEL;
-        if(in) copy_slot(a, a.perm[j], (uint32_t)j, k);
+        if(in) {
+            copy_slot(a, a.perm[j], (uint32_t)j, k);
+            a.dir_next[j] = k != SENTINEL ? (uint8_t)DIR_STAY : (uint8_t)DIR_INVALID;
+        }
         const bool valid = k != SENTINEL;
         const uint32_t b = k >> 6;
         const unsigned peers = __match_any_sync(0xffffffffu, valid ? b : 0xffffffffu);
@@ -637,7 +719,7 @@ __global__ void k_prepare(FastArgs a, uint32_t* pbstart, uint32_t* pbend, uint32
         }
         if(j == 0 || (kp >> 6) != b) {
             pbstart[b] = (uint32_t)j;
-            pactive[atomicAdd(&pctr[CNT_ACTIVE_BLOCKS], 1u)] = b;
+            pactive[atomicAdd(&pctr[CNT_ACTIVE_BLOCKS], 1u)] = make_uint4(b, (uint32_t)j, SENTINEL, a.block_scene[b]);
         }
         const uint32_t kn = j + 1 < a.n ? a.sorted_keys[j + 1] : SENTINEL;
         if(kn == SENTINEL || (kn >> 6) != b) pbend[b] = (uint32_t)(j + 1);
@@ -853,7 +935,7 @@ template<int T> struct P2GSmem {
     float scale[4];
     int maxc;
     int scene;
-    uint4 work;
+    uint4 work[2][2];                     // this item's descriptor and the next one's
     SceneDev sc;
 };
 
@@ -924,24 +1006,32 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
     extern __shared__ __align__(16) float FS[];    // NFAC x T factors, in place order
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t nwork = min(a.ctr[CNT_CHUNKS], a.chunk_cap);
-    if(threadIdx.x == 0) S.scene = -1;
-    for(;;) {
+    uint32_t w = 0, wnext = 0;            // thread 0: this item's ticket, the next one's
+    if(threadIdx.x == 0) {
+        S.scene = -1;
+        w = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+        work_prefetch(a, w, nwork, S.work[0]);
+        wnext = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+    }
+    for(int cur = 0;; cur ^= 1) {
         __syncthreads();
         if(threadIdx.x == 0) {
-            const uint32_t w = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
-            S.work = w < nwork ? a.chunks[w] : make_uint4(SENTINEL, 0u, 0u, 0u);
+            work_arrive(w, nwork, S.work[cur]);
+            work_prefetch(a, wnext, nwork, S.work[cur ^ 1]);
+            w = wnext;
+            wnext = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
             S.maxc = 0;
         }
         for(int t = threadIdx.x; t < 4 * PTN; t += T) { (&S.q[0][0])[t] = 0; (&S.ql[0][0])[t] = 0; }
         if(threadIdx.x < 64) S.ccount[threadIdx.x] = 0u;
         if(threadIdx.x < 4) S.bound[threadIdx.x] = 0.f;
         __syncthreads();
-        const uint4 wk = S.work;
+        const uint4 wk = S.work[cur][0], wr = S.work[cur][1];
         if(wk.x == SENTINEL) break;
         const uint32_t b = wk.x, part = wk.y, parts = wk.z;
-        const int sid = a.block_scene[b];
+        const int sid = (int)wk.w;
         if(sid != S.scene) stage_scene(a, sid, &S.sc);
-        const uint32_t s = a.bstart[b], e = a.bend[b];
+        const uint32_t s = wr.x, e = wr.x + wr.y;
         const uint32_t cnt = e - s > part ? min((e - s - part + parts - 1) / parts, (uint32_t)T) : 0u;
         // this thread's slot of the (strided) part: cell, rank in its cell, factors, bounds
         const bool mine = threadIdx.x < cnt;
@@ -955,6 +1045,16 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
         }
         __syncthreads();
         if(threadIdx.x == 0) S.scene = sid;
+        // the block's 8 node blocks for the grid update: flags exchanged now,
+        // first touches listed after the flush (the round trip overlaps the item)
+        uint32_t nb = 0, nb_prev = 1;
+        if(threadIdx.x >= T - 8) {
+            const int o = threadIdx.x - (T - 8);
+            int bx, by, bz;
+            block_coords(S.sc, b - S.sc.block_base, bx, by, bz);
+            nb = S.sc.nb_base + ((uint32_t)(bx + (o >> 2)) * S.sc.NN[1] + by + ((o >> 1) & 1)) * S.sc.NN[2] + bz + (o & 1);
+            nb_prev = atomicExch(&a.nb_flag[nb], 1u);
+        }
         if(mine) {
             particle_factors(a, S.sc, s + part + threadIdx.x * parts, P);
             factor_bounds(P, bnd);
@@ -1056,11 +1156,7 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
             if(any)
                 atomicAdd(&a.acc[node_index(sc, 4 * bx + tx, 4 * by + ty, 4 * bz + tz)], make_float4(v[1], v[2], v[3], v[0]));
         }
-        if(threadIdx.x < 8) {
-            const int nx = bx + (threadIdx.x >> 2), ny = by + ((threadIdx.x >> 1) & 1), nz = bz + (threadIdx.x & 1);
-            const uint32_t nb = sc.nb_base + ((uint32_t)nx * sc.NN[1] + ny) * sc.NN[2] + nz;
-            if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.ctr[CNT_NODE_BLOCKS], 1u)] = nb;
-        }
+        if(nb_prev == 0u) a.nb_list[atomicAdd(&a.ctr[CNT_NODE_BLOCKS], 1u)] = nb;
     }
     p2g_finish(a, &S.maxc);
 }
@@ -1084,7 +1180,7 @@ template<int T> struct P2GGroupSmem {
     uint32_t list[4 * T];                 // the part's sorted positions, cell by cell
     uint8_t lcell[4 * T];
     int scene;
-    uint4 work;
+    uint4 work[2][2];                     // this item's descriptor and the next one's
 };
 
 // The 9 separable factors of quantity `qn` (0 mass, 1-3 momentum) of P.
@@ -1110,22 +1206,30 @@ template<int T> __global__ void __launch_bounds__(T, 512 / T) k_p2g_groups(FastA
     const int lane = threadIdx.x & 31, k = threadIdx.x & 3, g = threadIdx.x >> 2;
     const unsigned gmask = 0xfu << (lane & ~3);
     const uint32_t nwork = min(a.ctr[CNT_CHUNKS], a.chunk_cap);
-    if(threadIdx.x == 0) S.scene = -1;
-    for(;;) {
+    uint32_t w = 0, wnext = 0;            // thread 0: this item's ticket, the next one's
+    if(threadIdx.x == 0) {
+        S.scene = -1;
+        w = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+        work_prefetch(a, w, nwork, S.work[0]);
+        wnext = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+    }
+    for(int cur = 0;; cur ^= 1) {
         __syncthreads();
         if(threadIdx.x == 0) {
-            const uint32_t w = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
-            S.work = w < nwork ? a.chunks[w] : make_uint4(SENTINEL, 0u, 0u, 0u);
+            work_arrive(w, nwork, S.work[cur]);
+            work_prefetch(a, wnext, nwork, S.work[cur ^ 1]);
+            w = wnext;
+            wnext = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
         }
         for(int t = threadIdx.x; t < 4 * PTN; t += T) (&S.q[0][0])[t] = 0.f;
         if(threadIdx.x < 64) S.ccount[threadIdx.x] = 0u;
         __syncthreads();
-        const uint4 wk = S.work;
+        const uint4 wk = S.work[cur][0], wr = S.work[cur][1];
         if(wk.x == SENTINEL) break;
         const uint32_t b = wk.x, part = wk.y, parts = wk.z;
-        const int sid = a.block_scene[b];
+        const int sid = (int)wk.w;
         if(sid != S.scene) stage_scene(a, sid, &s_sc);
-        const uint32_t s = a.bstart[b], c = a.bend[b] - s;
+        const uint32_t s = wr.x, c = wr.y;
         const uint32_t j0 = s + (uint32_t)((uint64_t)c * part / parts);
         const uint32_t cnt = min((uint32_t)((uint64_t)c * (part + 1) / parts) + s - j0, (uint32_t)(4 * T));
         // bin by cell: up to 4 particles per thread
@@ -1138,6 +1242,16 @@ template<int T> __global__ void __launch_bounds__(T, 512 / T) k_p2g_groups(FastA
         }
         __syncthreads();
         if(threadIdx.x == 0) S.scene = sid;
+        // the block's 8 node blocks for the grid update: flags exchanged now,
+        // first touches listed after the flush (the round trip overlaps the item)
+        uint32_t nb = 0, nb_prev = 1;
+        if(threadIdx.x >= T - 8) {
+            const int o = threadIdx.x - (T - 8);
+            int bx, by, bz;
+            block_coords(s_sc, b - s_sc.block_base, bx, by, bz);
+            nb = s_sc.nb_base + ((uint32_t)(bx + (o >> 2)) * s_sc.NN[1] + by + ((o >> 1) & 1)) * s_sc.NN[2] + bz + (o & 1);
+            nb_prev = atomicExch(&a.nb_flag[nb], 1u);
+        }
         if(threadIdx.x < 32) {   // exclusive scan of the 64 cell counts
             const uint32_t c0 = S.ccount[2 * lane], c1 = S.ccount[2 * lane + 1];
             const uint32_t x = warp_incl_scan(c0 + c1);
@@ -1233,11 +1347,7 @@ template<int T> __global__ void __launch_bounds__(T, 512 / T) k_p2g_groups(FastA
                 atomicAdd(&a.acc[node_index(sc, 4 * bx + tx, 4 * by + ty, 4 * bz + tz)],
                           make_float4(S.q[1][u], S.q[2][u], S.q[3][u], m));
         }
-        if(threadIdx.x < 8) {
-            const int nx = bx + (threadIdx.x >> 2), ny = by + ((threadIdx.x >> 1) & 1), nz = bz + (threadIdx.x & 1);
-            const uint32_t nb = sc.nb_base + ((uint32_t)nx * sc.NN[1] + ny) * sc.NN[2] + nz;
-            if(atomicExch(&a.nb_flag[nb], 1u) == 0u) a.nb_list[atomicAdd(&a.ctr[CNT_NODE_BLOCKS], 1u)] = nb;
-        }
+        if(nb_prev == 0u) a.nb_list[atomicAdd(&a.ctr[CNT_NODE_BLOCKS], 1u)] = nb;
     }
     __shared__ int s_last;
     p2g_finish(a, &s_last);
@@ -1683,27 +1793,32 @@ __device__ __forceinline__ void tma_tile(float4* dst, const CUtensorMap* map, ui
                  : "memory");
 }
 
-// Thread 0: take the next work item and start its tile copy into `dst`.
-__device__ __forceinline__ uint4 g2p_take(const FastArgs& a, uint32_t nwork, float4* dst, uint64_t* bar)
+// Thread 0: the next work item's descriptor into work[0..1] and its tile copy
+// into `dst` started; returns whether there is such an item.
+__device__ __forceinline__ bool g2p_take(const FastArgs& a, uint32_t nwork, uint4* work, float4* dst, uint64_t* bar)
 {
     const uint32_t w = atomicAdd(&a.ctr[CNT_G2P_WORK], 1u);
-    if(w >= nwork) return make_uint4(SENTINEL, 0u, 0u, 0u);
-    const uint4 wk = a.chunks[w];
-    const int sid = a.block_scene[wk.x];
-    const SceneDev& sc = a.scenes[sid];
+    if(w >= nwork) {
+        work[0] = make_uint4(SENTINEL, 0u, 0u, 0u);
+        return false;
+    }
+    const uint4 wk = a.chunks[2 * (size_t)w], wr = a.chunks[2 * (size_t)w + 1];
+    const SceneDev& sc = a.scenes[wk.w];
     int bx, by, bz;
     block_coords(sc, wk.x - sc.block_base, bx, by, bz);
     fence_async_shared();   // the CTA's reads of this buffer come before the copy's writes
     mbar_expect_tx(bar, TILE_BYTES);
-    tma_tile(dst, a.tmaps + sid, bar, 4 * bx, 4 * by, 4 * bz);
-    return wk;
+    tma_tile(dst, a.tmaps + wk.w, bar, 4 * bx, 4 * by, 4 * bz);
+    work[0] = wk;
+    work[1] = wr;
+    return true;
 }
 
 template<int THREADS, int PK> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
 {
     __shared__ alignas(128) float4 tv[2][2 * TN];
     __shared__ alignas(8) uint64_t s_bar[2];
-    __shared__ uint4 s_work[2];
+    __shared__ uint4 s_work[2][2];
     __shared__ int s_scene;
     __shared__ SceneDev s_sc;
     // where this part's particles go next substep: per direction (k_bins, k_route)
@@ -1716,21 +1831,21 @@ template<int THREADS, int PK> __global__ void __launch_bounds__(THREADS) k_g2p(F
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
         fence_async_shared();
-        s_work[0] = g2p_take(a, nwork, tv[0], &s_bar[0]);
+        g2p_take(a, nwork, s_work[0], tv[0], &s_bar[0]);
     }
     __syncthreads();
     uint32_t issued = 1u;               // bit b: a copy into buffer b is in flight (thread 0's view)
     bool failed = false;
     for(int k = 0;; k++) {
         const int buf = k & 1;
-        const uint4 wk = s_work[buf];
+        const uint4 wk = s_work[buf][0], wr = s_work[buf][1];
         if(wk.x == SENTINEL) break;
         if(threadIdx.x == 0) {          // the next item's tile copy, overlapping this item
-            s_work[buf ^ 1] = g2p_take(a, nwork, tv[buf ^ 1], &s_bar[buf ^ 1]);
-            issued = (issued & ~(1u << buf)) | (s_work[buf ^ 1].x != SENTINEL ? 1u << (buf ^ 1) : 0u);
+            const bool more = g2p_take(a, nwork, s_work[buf ^ 1], tv[buf ^ 1], &s_bar[buf ^ 1]);
+            issued = (issued & ~(1u << buf)) | (more ? 1u << (buf ^ 1) : 0u);
         }
         const uint32_t b = wk.x, part = wk.y, parts = wk.z;
-        const int sid = a.block_scene[b];
+        const int sid = (int)wk.w;
         if(sid != s_scene) {
             stage_scene(a, sid, &s_sc);
             __syncthreads();
@@ -1754,12 +1869,13 @@ template<int THREADS, int PK> __global__ void __launch_bounds__(THREADS) k_g2p(F
         }
         const bool anti = __syncthreads_or(differs) != 0;
         // a contiguous part of the block (coalesced slots)
-        const uint32_t s = a.bstart[b], c = a.bend[b] - s;
+        const uint32_t s = wr.x, c = wr.y;
         const uint32_t j0 = s + (uint32_t)((uint64_t)c * part / parts), j1 = s + (uint32_t)((uint64_t)c * (part + 1) / parts);
         for(uint32_t j = j0 + threadIdx.x; j < j1; j += THREADS) {
             G2PState o;
             g2p_particle<PK>(a, sc, t4, anti, ox, oy, oz, j, o);
             const int d = key_dir(sc, b, bx, by, bz, o.key);
+            a.dir_next[j] = (uint8_t)d;
             if(d == DIR_FAR) {
                 atomicAdd(&a.dcount[(size_t)(o.key >> 6) * ROW + DIR_FAR], 1u);
                 atomicAdd(&a.bcount[o.key >> 6], 1ull);
@@ -1932,6 +2048,8 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.sorted_keys = f.sorted_keys;
     a.keys_cur = f.keys[c];
     a.keys_next = f.keys[o];
+    a.dir_cur = f.dirs[c];
+    a.dir_next = f.dirs[o];
     // this substep's order is set c, the previous substep's set o
     a.bstart = f.bstart[c]; a.bend = f.bend[c]; a.active = f.active[c]; a.chunks = f.chunks[c];
     a.ctr = f.counters ? f.counters + CNT_COUNT * c : nullptr;
@@ -2096,7 +2214,7 @@ int fast_setup_scenes(mpm_handle* h, const mpm_scene_desc* descs, int count, con
     for(int k = 0; k < 2; k++) {
         MPM_CUDA(h, cudaMalloc(&f.bstart[k], blocks * sizeof(uint32_t)));
         MPM_CUDA(h, cudaMalloc(&f.bend[k], blocks * sizeof(uint32_t)));
-        MPM_CUDA(h, cudaMalloc(&f.active[k], blocks * sizeof(uint32_t)));
+        MPM_CUDA(h, cudaMalloc(&f.active[k], blocks * sizeof(uint4)));
     }
     MPM_CUDA(h, cudaMalloc(&f.nb_flag, nblocks * sizeof(uint32_t)));
     MPM_CUDA(h, cudaMalloc(&f.nb_list, nblocks * sizeof(uint32_t)));
@@ -2200,7 +2318,10 @@ int fast_alloc(mpm_handle* h, int64_t n)
         uint32_t** ps[] = {&f.keys[0], &f.keys[1], &f.sorted_keys, &f.perm, &f.sort_keys_alt, &f.sort_vals_alt,
                            &f.sort_scratch};
         for(uint32_t** p: ps) { cudaFree(*p); *p = nullptr; }
-        for(int k = 0; k < 2; k++) { cudaFree(f.chunks[k]); f.chunks[k] = nullptr; }
+        for(int k = 0; k < 2; k++) {
+            cudaFree(f.chunks[k]); f.chunks[k] = nullptr;
+            cudaFree(f.dirs[k]); f.dirs[k] = nullptr;
+        }
         cudaFree(f.vkick);
         f.vkick = nullptr;
         cudaFree(f.pmodel); cudaFree(f.pmask);   // per caller index: a new count drops them
@@ -2212,10 +2333,13 @@ int fast_alloc(mpm_handle* h, int64_t n)
             MPM_CUDA(h, cudaMalloc(&f.attr[b], np * sizeof(float4)));
             MPM_CUDA(h, cudaMalloc(&f.pid[b], np * sizeof(int)));
         }
-        for(int k = 0; k < 2; k++) MPM_CUDA(h, cudaMalloc(&f.keys[k], np * sizeof(uint32_t)));
+        for(int k = 0; k < 2; k++) {
+            MPM_CUDA(h, cudaMalloc(&f.keys[k], np * sizeof(uint32_t)));
+            MPM_CUDA(h, cudaMalloc(&f.dirs[k], np * sizeof(uint8_t)));
+        }
         // work items: a block's particles in parts of at least 64
         f.chunk_cap = np / 64 + std::min<int64_t>(np, f.total_blocks) + 1;
-        for(int k = 0; k < 2; k++) MPM_CUDA(h, cudaMalloc(&f.chunks[k], f.chunk_cap * sizeof(uint4)));
+        for(int k = 0; k < 2; k++) MPM_CUDA(h, cudaMalloc(&f.chunks[k], 2 * f.chunk_cap * sizeof(uint4)));
         MPM_CUDA(h, cudaMalloc(&f.sorted_keys, np * sizeof(uint32_t)));
         MPM_CUDA(h, cudaMalloc(&f.perm, np * sizeof(uint32_t)));
         MPM_CUDA(h, cudaMalloc(&f.sort_keys_alt, np * sizeof(uint32_t)));
@@ -2248,7 +2372,8 @@ void fast_free(mpm_handle* h)
         cudaFree(f.soa[b]); cudaFree(f.attr[b]); cudaFree(f.pid[b]); cudaFree(f.plas[b]);
         f.soa[b] = nullptr; f.attr[b] = nullptr; f.pid[b] = nullptr; f.plas[b] = nullptr;
     }
-    void** ps[] = {(void**)&f.keys[0], (void**)&f.keys[1], (void**)&f.sorted_keys, (void**)&f.perm,
+    void** ps[] = {(void**)&f.keys[0], (void**)&f.keys[1], (void**)&f.dirs[0], (void**)&f.dirs[1],
+                   (void**)&f.sorted_keys, (void**)&f.perm,
                    (void**)&f.sort_keys_alt, (void**)&f.sort_vals_alt, (void**)&f.sort_scratch, (void**)&f.bstart[0],
                    (void**)&f.bend[0], (void**)&f.active[0], (void**)&f.chunks[0], (void**)&f.bstart[1],
                    (void**)&f.bend[1], (void**)&f.active[1], (void**)&f.chunks[1], (void**)&f.nb_flag,
@@ -2540,7 +2665,7 @@ static int fast_route(mpm_handle* h)
     MPM_LAUNCHED(h, "k_bins");
     timer_end(h, slot);
     slot = timer_begin(h, "fast_route");
-    k_route<<<h->sm_count * 8, 256, 0, h->stream>>>(a);
+    k_route<<<occupancy_ctas(h, (const void*)k_route, 256, 1), 256, 0, h->stream>>>(a);   // resident CTAs only
     MPM_LAUNCHED(h, "k_route");
     timer_end(h, slot);
     f.sorted_now = true;

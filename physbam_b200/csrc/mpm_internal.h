@@ -74,6 +74,7 @@ struct FastState {
     float* plas[2] = {nullptr, nullptr};      // plasticity on: 13 * npad floats: Fp0..8, then mu0, lambda0
                                               // (clamp) or plastic_def, rho_F, sigma_Y, vc (Drucker-Prager)
     uint32_t* keys[2] = {nullptr, nullptr};   // cell keys of each buffer's slots
+    uint8_t* dirs[2] = {nullptr, nullptr};    // each slot's move direction from its previous block (G2P)
     uint32_t* sorted_keys = nullptr;
     uint32_t* perm = nullptr;                 // sorted position -> slot in the current buffer
     uint32_t* sort_keys_alt = nullptr;
@@ -83,8 +84,8 @@ struct FastState {
     // (the next substep's routing reads the previous set)
     uint32_t* bstart[2] = {nullptr, nullptr}; // per particle block
     uint32_t* bend[2] = {nullptr, nullptr};
-    uint32_t* active[2] = {nullptr, nullptr}; // active particle blocks
-    uint4* chunks[2] = {nullptr, nullptr};    // work items: (block, part, parts, 0)
+    uint4* active[2] = {nullptr, nullptr};    // active particle blocks: (block, start, count, scene)
+    uint4* chunks[2] = {nullptr, nullptr};    // work items, two uint4 each: (block, part, parts, scene), (block start, block count, 0, 0)
     int64_t chunk_cap = 0;
     // routing from one substep's order to the next (mpm_fast.cu, k_bins / k_route):
     // per block a row of arrival counts by direction (G2P) and the row of their
