@@ -299,6 +299,7 @@ def our_arm(args):
     h2d = n * 4 * (3 + 3 + 9 + 9 + 4)
     d2h = n * (4 * (3 + 3 + 9 + 9) + 1)
     e2e_drv = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
+    e2e_drv.set_launch_shape(*shape)   # the autotuner's choice above (mpm_set_launch_shape)
     e2e_drv.set_particles_native(hX, hV, hF, hB, hm, hvol, hmu, hla)
     e2e_drv.advance(2)
     e2e_drv.get_particles_native(oX, oV, oF, oB, ovalid)

@@ -471,7 +471,7 @@ int mpm_autotune_ex(mpm_handle* h, double dt, int substeps, int flags, char* rep
  * MPM_P2G_FIXED256 (one thread per particle into a fixed-point shared tile,
  * work items of up to 128 / 256 particles); G2P takes the same work items;
  * g2p_threads: 64, 128 or 256 per CTA; cta_mult: 1 or 2 times the resident
- * CTAs per SM. */
+ * CTAs per SM.  A new handle starts with MPM_P2G_FIXED256, 128, 1. */
 enum { MPM_P2G_GROUPS128 = 0, MPM_P2G_GROUPS256 = 1, MPM_P2G_FIXED128 = 2, MPM_P2G_FIXED256 = 3 };
 int mpm_set_launch_shape(mpm_handle* h, int p2g_variant, int g2p_threads, int cta_mult);
 int mpm_get_launch_shape(mpm_handle* h, int* p2g_variant, int* g2p_threads, int* cta_mult);

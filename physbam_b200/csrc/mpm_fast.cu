@@ -406,8 +406,9 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x)
 // each, (block, k, parts, scene) and (block start, block count, 0, 0), so that
 // a kernel needs no other load to begin an item.  CTAs take items by ticket
 // (an atomic counter: CTAs that finish early take more) ahead of need: P2G
-// holds the next item's descriptor in flight and the ticket after it, so
-// neither round trip falls between two items.
+// starts on the item of its CTA index, then holds the next item's descriptor
+// in flight and the ticket after it, so neither round trip falls between two
+// items.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
 {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
@@ -1006,12 +1007,14 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
     extern __shared__ __align__(16) float FS[];    // NFAC x T factors, in place order
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t nwork = min(a.ctr[CNT_CHUNKS], a.chunk_cap);
-    uint32_t w = 0, wnext = 0;            // thread 0: this item's ticket, the next one's
+    // thread 0: this item and the next; the first item by CTA index (every CTA
+    // starts on one), later ones by ticket
+    uint32_t w = 0, wnext = 0;
     if(threadIdx.x == 0) {
         S.scene = -1;
-        w = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+        w = blockIdx.x;
         work_prefetch(a, w, nwork, S.work[0]);
-        wnext = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+        wnext = gridDim.x + atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
     }
     for(int cur = 0;; cur ^= 1) {
         __syncthreads();
@@ -1019,7 +1022,7 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
             work_arrive(w, nwork, S.work[cur]);
             work_prefetch(a, wnext, nwork, S.work[cur ^ 1]);
             w = wnext;
-            wnext = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+            wnext = gridDim.x + atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
             S.maxc = 0;
         }
         for(int t = threadIdx.x; t < 4 * PTN; t += T) { (&S.q[0][0])[t] = 0; (&S.ql[0][0])[t] = 0; }
@@ -1206,12 +1209,14 @@ template<int T> __global__ void __launch_bounds__(T, 512 / T) k_p2g_groups(FastA
     const int lane = threadIdx.x & 31, k = threadIdx.x & 3, g = threadIdx.x >> 2;
     const unsigned gmask = 0xfu << (lane & ~3);
     const uint32_t nwork = min(a.ctr[CNT_CHUNKS], a.chunk_cap);
-    uint32_t w = 0, wnext = 0;            // thread 0: this item's ticket, the next one's
+    // thread 0: this item and the next; the first item by CTA index (every CTA
+    // starts on one), later ones by ticket
+    uint32_t w = 0, wnext = 0;
     if(threadIdx.x == 0) {
         S.scene = -1;
-        w = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+        w = blockIdx.x;
         work_prefetch(a, w, nwork, S.work[0]);
-        wnext = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+        wnext = gridDim.x + atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
     }
     for(int cur = 0;; cur ^= 1) {
         __syncthreads();
@@ -1219,7 +1224,7 @@ template<int T> __global__ void __launch_bounds__(T, 512 / T) k_p2g_groups(FastA
             work_arrive(w, nwork, S.work[cur]);
             work_prefetch(a, wnext, nwork, S.work[cur ^ 1]);
             w = wnext;
-            wnext = atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
+            wnext = gridDim.x + atomicAdd(&a.ctr[CNT_P2G_WORK], 1u);
         }
         for(int t = threadIdx.x; t < 4 * PTN; t += T) (&S.q[0][0])[t] = 0.f;
         if(threadIdx.x < 64) S.ccount[threadIdx.x] = 0u;

@@ -115,8 +115,8 @@ struct FastState {
     void* staging = nullptr;   // device copies of host particle arrays (set / get)
     size_t staging_bytes = 0;   // sort_scratch holds the digit histograms of `keys` (built by G2P)
     // launch shapes (mpm_autotune)
-    int p2g_variant = 0;                      // P2G launch shape (MPM_P2G_*)
-    int route_variant = 0;                    // the shape whose work-item size the current order has
+    int p2g_variant = MPM_P2G_FIXED256;       // P2G launch shape (MPM_P2G_*)
+    int route_variant = MPM_P2G_FIXED256;     // the shape whose work-item size the current order has
     int g2p_threads = 128;
     int cta_mult = 1;
 };
