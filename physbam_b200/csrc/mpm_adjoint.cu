@@ -448,7 +448,8 @@ struct DiffTape {
     size_t esz = 0;
     void* ckpt = nullptr;            // (nsteps/every + 1) states
     uint8_t* ckpt_valid = nullptr;
-    void* seg = nullptr;             // every states
+    bool full = false;               // every substep recorded by the forward (no recompute)
+    void* seg = nullptr;             // every (or, full, nsteps) states
     uint8_t* seg_valid = nullptr;
     void *seg_gm = nullptr, *seg_gv = nullptr, *seg_gu = nullptr, *seg_pft = nullptr;
     void* final_state = nullptr;
@@ -496,6 +497,45 @@ static int state_copy(mpm_handle* h, void* dst, uint8_t* dvalid, bool to_tape)
     return MPM_OK;
 }
 
+// One substep of the rollout with its intermediates into tape slot j: the
+// state before it, the node masses and velocities after the forces, the grid
+// update's velocity map (k_grid_u) and P F^T; `advance`: the G2P that ends it.
+template<class T> static int record_substep(mpm_handle* h, DiffTape* t, int j, bool advance)
+{
+    PlainState& s = h->plain;
+    const int64_t n = t->n, gn = t->gn;
+    const size_t e = sizeof(T), st = 24 * n * e;
+    int rc;
+    if((rc = state_copy(h, (char*)t->seg + j * st, t->seg_valid + j * n, true))) return rc;
+    if((rc = plain_p2g(h, t->dt, 0))) return rc;
+    if((rc = plain_forces(h, t->dt, 0))) return rc;
+    MPM_CUDA(h, cudaMemcpyAsync((T*)t->seg_gm + j * gn, s.gm, gn * e, cudaMemcpyDeviceToDevice, h->stream));
+    MPM_CUDA(h, cudaMemcpyAsync((T*)t->seg_gv + j * gn * 3, s.gv, gn * 3 * e, cudaMemcpyDeviceToDevice, h->stream));
+    k_grid_u<T><<<blocks_for(h, gn, 256, true), 256, 0, h->stream>>>((const T*)s.gv0, (const T*)s.gf, (const T*)s.gm,
+                                                                   (T)t->dt, gn, (T*)t->seg_gu + j * gn * 3);
+    MPM_LAUNCHED(h, "k_grid_u");
+    MPM_CUDA(h, cudaMemcpyAsync((T*)t->seg_pft + j * 9 * n, s.pft, 9 * n * e, cudaMemcpyDeviceToDevice, h->stream));
+    if(advance && (rc = plain_g2p(h, t->dt, 0))) return rc;
+    return MPM_OK;
+}
+
+// Tape slots for `slots` substeps (the segment buffers the backward reads).
+static int alloc_segments(mpm_handle* h, DiffTape* t, int slots)
+{
+    const int64_t n = t->n, gn = t->gn;
+    const size_t e = t->esz, st = 24 * n * e;
+    MPM_CUDA(h, cudaMalloc(&t->seg, slots * st + 1));
+    MPM_CUDA(h, cudaMalloc(&t->seg_valid, slots * n + 1));
+    MPM_CUDA(h, cudaMalloc(&t->seg_gm, slots * gn * e));
+    MPM_CUDA(h, cudaMalloc(&t->seg_gv, slots * gn * 3 * e));
+    MPM_CUDA(h, cudaMalloc(&t->seg_gu, slots * gn * 3 * e));
+    MPM_CUDA(h, cudaMalloc(&t->seg_pft, slots * 9 * n * e + 1));
+    return MPM_OK;
+}
+
+// Bytes of the tape slots of one substep.
+static size_t slot_bytes(int64_t n, int64_t gn, size_t e) { return (24 * n + 9 * n) * e + n + 7 * gn * e; }
+
 int diff_forward(mpm_handle* h, double dt, int nsteps, int every)
 {
     if(h->model.path != MPM_PATH_PLAIN || h->sp.dim != 3)
@@ -522,6 +562,15 @@ int diff_forward(mpm_handle* h, double dt, int nsteps, int every)
         h->diff = t;
         t->n = s.n; t->gn = s.gn; t->nsteps = nsteps; t->every = every;
         t->esz = esz;
+        // every substep's intermediates kept when they take at most a quarter of
+        // the free device memory: the backward then recomputes nothing
+        size_t free_b = 0, total_b = 0;
+        if(cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+        t->full = nsteps > every && (double)slot_bytes(s.n, s.gn, esz) * nsteps <= 0.25 * (double)free_b;
+        if(t->full) {
+            int arc = alloc_segments(h, t, nsteps);
+            if(arc) return arc;
+        }
     }
     t->recorded = false;
     t->dt = dt;
@@ -535,6 +584,11 @@ int diff_forward(mpm_handle* h, double dt, int nsteps, int every)
     }
     int rc;
     for(int k = 0; k < nsteps; k++) {
+        if(t->full) {
+            rc = esz == 8 ? record_substep<double>(h, t, k, true) : record_substep<float>(h, t, k, true);
+            if(rc) return rc;
+            continue;
+        }
         if(k % every == 0) {
             int c = k / every;
             if((rc = state_copy(h, (char*)t->ckpt + c * st, t->ckpt_valid + c * s.n, true))) return rc;
@@ -558,12 +612,10 @@ template<class T> static int backward_t(mpm_handle* h, const void* gX, const voi
     const size_t st = 24 * n * e;
     const int every = t->every;
     if(!t->seg) {
-        MPM_CUDA(h, cudaMalloc(&t->seg, every * st + 1));
-        MPM_CUDA(h, cudaMalloc(&t->seg_valid, every * n + 1));
-        MPM_CUDA(h, cudaMalloc(&t->seg_gm, every * gn * e));
-        MPM_CUDA(h, cudaMalloc(&t->seg_gv, every * gn * 3 * e));
-        MPM_CUDA(h, cudaMalloc(&t->seg_gu, every * gn * 3 * e));
-        MPM_CUDA(h, cudaMalloc(&t->seg_pft, every * 9 * n * e + 1));
+        int arc = alloc_segments(h, t, every);
+        if(arc) return arc;
+    }
+    if(!t->adj[0]) {
         for(int k = 0; k < 2; k++) MPM_CUDA(h, cudaMalloc(&t->adj[k], st + 1));
         MPM_CUDA(h, cudaMalloc(&t->amu, n * e + 1));
         MPM_CUDA(h, cudaMalloc(&t->alam, n * e + 1));
@@ -580,23 +632,17 @@ template<class T> static int backward_t(mpm_handle* h, const void* gX, const voi
     MPM_CUDA(h, cudaMemsetAsync(t->amu, 0, n * e, h->stream));
     MPM_CUDA(h, cudaMemsetAsync(t->alam, 0, n * e, h->stream));
     const int tb = 128;
-    int nck = (t->nsteps + every - 1) / every;
+    // a full tape is one segment, recorded by the forward; otherwise each
+    // checkpoint's segment is recomputed from it, keeping what the adjoint needs
+    const int nck = t->full ? 1 : (t->nsteps + every - 1) / every;
+    const int span = t->full ? t->nsteps : every;
     int rc;
     for(int c = nck - 1; c >= 0; c--) {
-        int k0 = c * every, k1 = k0 + every < t->nsteps ? k0 + every : t->nsteps;
-        if((rc = state_copy(h, (char*)t->ckpt + c * st, t->ckpt_valid + c * n, false))) return rc;
-        for(int k = k0; k < k1; k++) {   // recompute the segment, keeping what the adjoint needs
-            int j = k - k0;
-            if((rc = state_copy(h, (char*)t->seg + j * st, t->seg_valid + j * n, true))) return rc;
-            if((rc = plain_p2g(h, t->dt, 0))) return rc;
-            if((rc = plain_forces(h, t->dt, 0))) return rc;
-            MPM_CUDA(h, cudaMemcpyAsync((T*)t->seg_gm + j * gn, s.gm, gn * e, cudaMemcpyDeviceToDevice, h->stream));
-            MPM_CUDA(h, cudaMemcpyAsync((T*)t->seg_gv + j * gn * 3, s.gv, gn * 3 * e, cudaMemcpyDeviceToDevice, h->stream));
-            k_grid_u<T><<<blocks_for(h, gn, 256, true), 256, 0, h->stream>>>((const T*)s.gv0, (const T*)s.gf, (const T*)s.gm,
-                                                                           (T)t->dt, gn, (T*)t->seg_gu + j * gn * 3);
-            MPM_LAUNCHED(h, "k_grid_u");
-            MPM_CUDA(h, cudaMemcpyAsync((T*)t->seg_pft + j * 9 * n, s.pft, 9 * n * e, cudaMemcpyDeviceToDevice, h->stream));
-            if(k + 1 < k1 && (rc = plain_g2p(h, t->dt, 0))) return rc;
+        int k0 = c * span, k1 = k0 + span < t->nsteps ? k0 + span : t->nsteps;
+        if(!t->full) {
+            if((rc = state_copy(h, (char*)t->ckpt + c * st, t->ckpt_valid + c * n, false))) return rc;
+            for(int k = k0; k < k1; k++)
+                if((rc = record_substep<T>(h, t, k - k0, k + 1 < k1))) return rc;
         }
         for(int k = k1 - 1; k >= k0; k--) {
             int j = k - k0;
