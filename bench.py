@@ -582,7 +582,9 @@ def measure_adjoint(D, S, stream):
     rollout with checkpoints (mpm_diff_forward, plain path) and its adjoint
     (mpm_diff_backward) through the C ABI on device arrays, beside the fast FP32
     forward of the same 64 substeps (mpm_advance); each timed with CUDA events on
-    the library's stream, best of 3 after one warm-up."""
+    the library's stream, best of 3 after one warm-up.  Twice: with the default
+    tape budget (the forward keeps every substep, the backward recomputes
+    nothing) and with checkpoints only (each segment recomputed)."""
     import torch
     scene = S.cube_3d()
     n = scene.n
@@ -604,14 +606,16 @@ def measure_adjoint(D, S, stream):
         torch.cuda.synchronize()
         return a.elapsed_time(b)
 
-    fwd, bwd, fast = [], [], []
-    for it in range(4):
-        drv.set_particles_device(X, V, Fc, Bc, m, vol, mu, lam)
-        f = timed(lambda: drv.diff_forward(64, 8))
-        b = timed(lambda: drv.diff_backward(*g))
-        if it:
-            fwd.append(f)
-            bwd.append(b)
+    fwd, bwd, fwd_ck, bwd_ck, fast = [], [], [], [], []
+    for budget, fl, bl in ((-1, fwd, bwd), (0, fwd_ck, bwd_ck)):   # every substep kept; checkpoints only
+        drv.set_diff_tape_budget(budget)
+        for it in range(4):
+            drv.set_particles_device(X, V, Fc, Bc, m, vol, mu, lam)
+            f = timed(lambda: drv.diff_forward(64, 8))
+            b = timed(lambda: drv.diff_backward(*g))
+            if it:
+                fl.append(f)
+                bl.append(b)
     drv.close()
     fd = D.MPM_DRIVER(scene, precision=D.FP32, path=D.PATH_FAST)
     fd.set_stream(stream.cuda_stream)
@@ -622,10 +626,13 @@ def measure_adjoint(D, S, stream):
         if it:
             fast.append(ms)
     fd.close()
-    f, b, ff = min(fwd), min(bwd), min(fast)
+    f, b, ff, fc, bc = min(fwd), min(bwd), min(fast), min(fwd_ck), min(bwd_ck)
     return {"workload": "cube3d-64^3-corotated-8ppc, 64 substeps, checkpoint every 8, fp32", "particles": n,
             "fwd_plain_ms": f, "bwd_ms": b, "fwd_fast_ms": ff, "bwd_over_fwd_plain": b / f,
             "bwd_over_fwd_fast": b / ff,
+            "checkpoints_only": {"fwd_plain_ms": fc, "bwd_ms": bc, "bwd_over_fwd_plain": bc / fc,
+                                 "bwd_over_fwd_fast": bc / ff,
+                                 "note": "mpm_set_diff_tape_budget(0): the backward recomputes each segment"},
             "timing": "CUDA events on the library's stream around each C-ABI call, best of 3 after a warm-up"}
 
 

@@ -479,8 +479,10 @@ int mpm_get_launch_shape(mpm_handle* h, int* p2g_variant, int* g2p_threads, int*
 /* ---- differentiation ------------------------------------------------------ */
 
 /* Records a differentiable rollout: nsteps explicit substeps from the current
- * particles, keeping the particle state every checkpoint_every substeps.
- * MPM_PATH_PLAIN, 3D, no collision objects.  The reference has no reverse
+ * particles, keeping the particle state every checkpoint_every substeps, and,
+ * when the tape budget allows (mpm_set_diff_tape_budget), every substep's
+ * intermediates.  MPM_PATH_PLAIN, 3D, static frictionless boxes, planes and
+ * spheres, one constitutive model.  The reference has no reverse
  * mode; this is the forward whose transposed linearisation mpm_diff_backward
  * applies (the reference's linearisations of the same maps are
  * MPM_FINITE_ELEMENTS::Add_Hessian_Times, Hybrid_Methods/Forces/
@@ -492,10 +494,20 @@ int mpm_diff_forward(mpm_handle* h, double dt, int nsteps, int checkpoint_every)
 /* Reverse pass of the last mpm_diff_forward: given dL/d(final X, V, F, B) in
  * grad_final, writes dL/d(initial X, V, F, B) to grad_initial and dL/dmu,
  * dL/dlambda (n each) to grad_mu / grad_lambda.  Segments between checkpoints
- * are recomputed.  Views carry only X, V, F, B; dtype must equal the path's
- * precision; on_device selects device or host pointers. */
+ * are recomputed unless the forward kept every substep.  Views carry only X,
+ * V, F, B; dtype must equal the path's precision; on_device selects device or
+ * host pointers. */
 int mpm_diff_backward(mpm_handle* h, const mpm_particles_view* grad_final, mpm_particles_view* grad_initial,
                       void* grad_mu, void* grad_lambda);
+
+/* Device memory the next mpm_diff_forward may spend on keeping every substep's
+ * intermediates (state, node masses and velocities, the grid update's map,
+ * P F^T), so that the backward recomputes nothing: bytes < 0 (the default)
+ * allows up to a quarter of the free device memory, 0 keeps checkpoints only
+ * (every segment recomputed by the backward, memory bounded by the checkpoint
+ * interval), bytes > 0 caps it.  No reference counterpart (the reference has
+ * no reverse mode). */
+int mpm_set_diff_tape_budget(mpm_handle* h, int64_t bytes);
 
 /* ---- sorting ------------------------------------------------------------- */
 

@@ -36,6 +36,8 @@
 #include <cstring>
 #include <vector>
 
+#include <algorithm>
+
 #include "mpm_internal.h"
 
 namespace {
@@ -554,19 +556,22 @@ int diff_forward(mpm_handle* h, double dt, int nsteps, int every)
     PlainState& s = h->plain;
     const size_t esz = h->model.precision == MPM_FP64 ? 8 : 4;
     DiffTape* t = tape(h);
+    // every substep's intermediates kept when the tape budget allows (by default
+    // a quarter of the free device memory): the backward then recomputes nothing
+    size_t free_b = 0, total_b = 0;
+    if(cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+    const double budget = h->diff_budget < 0 ? 0.25 * (double)free_b : std::min((double)h->diff_budget, 0.9 * (double)free_b);
+    const bool want_full = nsteps > every && (double)slot_bytes(s.n, s.gn, esz) * nsteps <= budget;
     // a tape of the same shape is reused as it is (no allocation)
-    const bool reuse = t && t->n == s.n && t->gn == s.gn && t->nsteps == nsteps && t->every == every && t->esz == esz;
+    const bool reuse = t && t->n == s.n && t->gn == s.gn && t->nsteps == nsteps && t->every == every && t->esz == esz &&
+                       t->full == want_full;
     if(!reuse) {
         diff_free(h);
         t = new DiffTape();
         h->diff = t;
         t->n = s.n; t->gn = s.gn; t->nsteps = nsteps; t->every = every;
         t->esz = esz;
-        // every substep's intermediates kept when they take at most a quarter of
-        // the free device memory: the backward then recomputes nothing
-        size_t free_b = 0, total_b = 0;
-        if(cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
-        t->full = nsteps > every && (double)slot_bytes(s.n, s.gn, esz) * nsteps <= 0.25 * (double)free_b;
+        t->full = want_full;
         if(t->full) {
             int arc = alloc_segments(h, t, nsteps);
             if(arc) return arc;

@@ -583,6 +583,13 @@ int mpm_get_launch_shape(mpm_handle* h, int* p2g_variant, int* g2p_threads, int*
     return MPM_OK;
 }
 
+int mpm_set_diff_tape_budget(mpm_handle* h, int64_t bytes)
+{
+    if(!h) return MPM_ERR_ARG;
+    h->diff_budget = bytes;
+    return MPM_OK;
+}
+
 int mpm_diff_forward(mpm_handle* h, double dt, int nsteps, int checkpoint_every)
 {
     int rc = check_dt(h, dt);

@@ -195,6 +195,7 @@ struct mpm_handle {
     double graph_dt = 0;
     // checkpoints of the last mpm_diff_forward (mpm_adjoint.cu)
     void* diff = nullptr;
+    int64_t diff_budget = -1;                 // mpm_set_diff_tape_budget
     std::string last_error;
 };
 

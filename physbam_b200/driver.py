@@ -121,7 +121,7 @@ EXPORTS = ["mpm_create", "mpm_destroy", "mpm_set_stream", "mpm_set_collision_obj
            "mpm_get_particles", "mpm_substep", "mpm_advance", "mpm_particle_to_grid", "mpm_apply_forces",
            "mpm_grid_to_particle", "mpm_synchronize", "mpm_get_grid", "mpm_count_valid", "mpm_set_timing",
            "mpm_get_timing", "mpm_last_error", "mpm_status_string", "mpm_radix_sort_u32", "mpm_debug_sort_state",
-           "mpm_diff_forward", "mpm_diff_backward", "mpm_batch_create", "mpm_autotune", "mpm_particle_totals",
+           "mpm_diff_forward", "mpm_diff_backward", "mpm_set_diff_tape_budget", "mpm_batch_create", "mpm_autotune", "mpm_particle_totals",
            "mpm_grid_totals", "mpm_compute_dt", "mpm_set_launch_shape", "mpm_get_launch_shape", "mpm_autotune_ex",
            "mpm_set_plasticity", "mpm_get_plastic_state", "mpm_set_plastic_state", "mpm_set_implicit",
            "mpm_get_implicit_stats", "mpm_set_dt_control", "mpm_simulate_frame", "mpm_last_dt",
@@ -163,6 +163,7 @@ def load_library(path: str = LIB_PATH):
     L.mpm_get_timing.argtypes = [P, ctypes.c_char_p, ctypes.c_int, P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.mpm_last_error.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
     L.mpm_diff_forward.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    L.mpm_set_diff_tape_budget.argtypes = [P, ctypes.c_int64]
     L.mpm_diff_backward.argtypes = [P, ctypes.POINTER(ParticlesView), ctypes.POINTER(ParticlesView), P, P]
     L.mpm_radix_sort_u32.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P]
     L.mpm_autotune.argtypes = [P, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
@@ -605,6 +606,11 @@ class MPM_DRIVER:
         self._check(self.L.mpm_set_plastic_state(self.h, ctypes.byref(v)), "mpm_set_plastic_state")
 
     # -- differentiation -------------------------------------------------------
+    def set_diff_tape_budget(self, nbytes):
+        """Memory the next diff_forward may keep for a backward without recomputation
+        (< 0: a quarter of the free device memory, 0: checkpoints only)."""
+        self._check(self.L.mpm_set_diff_tape_budget(self.h, int(nbytes)), "mpm_set_diff_tape_budget")
+
     def diff_forward(self, nsteps, checkpoint_every=8, dt=None):
         dt = self.scene.dt if dt is None else dt
         self._check(self.L.mpm_diff_forward(self.h, dt, nsteps, checkpoint_every), "mpm_diff_forward")

@@ -130,6 +130,23 @@ def test_checkpoint_interval_does_not_change_gradients(cuda_device):
         np.testing.assert_allclose(r[2], res[0][2], rtol=1e-10, atol=1e-12 * np.abs(res[0][2]).max())
 
 
+def test_tape_budget_does_not_change_gradients(cuda_device):
+    """A backward from every substep kept by the forward (the default budget) and
+    one that recomputes each segment from its checkpoint (budget 0) agree."""
+    from physbam_b200 import driver as D
+    scene = deformed(S.cube_3d(G=16, nsteps=12))
+    v0 = np.asarray(scene.V[0], float)
+    E = scene.mu * 2 * (1 + 0.3)
+    res = []
+    for budget in (-1, 0):
+        drv, dt, t = setup(scene, D.FP64)
+        drv.set_diff_tape_budget(budget)
+        res.append(loss_fn(drv, scene, t, dt, v0, E, 12, 4, True, part=True))
+        drv.close()
+    np.testing.assert_allclose(res[1][1], res[0][1], rtol=1e-12)
+    np.testing.assert_allclose(res[1][2], res[0][2], rtol=1e-10, atol=1e-12 * np.abs(res[0][2]).max())
+
+
 def test_adjoint_differentiable_config_fd(cuda_device):
     """The differentiable cube: 64^3, side-0.3 cube at 8 ppc, E log-uniform in
     [5e3, 5e4], v0 = (1, .5, 0), 64 substeps of 1e-4, checkpoint every 8."""
