@@ -96,6 +96,7 @@ struct FastArgs {
     // the previous substep's order (routing input)
     const uint32_t *obstart, *obend, *octr;
     const uint4* oactive;
+    uint32_t* nctr;             // the next substep's counters (the same storage as octr; G2P clears it)
     uint32_t *dcount, *doff, *scan;
     unsigned long long* bcount;
     int64_t nblk;               // particle blocks of all scenes
@@ -1821,6 +1822,9 @@ __device__ __forceinline__ bool g2p_take(const FastArgs& a, uint32_t nwork, uint
 
 template<int THREADS, int PK> __global__ void __launch_bounds__(THREADS) k_g2p(FastArgs a)
 {
+    // the previous order's counters are read by nothing after the routing: they
+    // become the next substep's, cleared here (no memset node between substeps)
+    if(blockIdx.x == 0 && threadIdx.x < CNT_COUNT) a.nctr[threadIdx.x] = 0u;
     __shared__ alignas(128) float4 tv[2][2 * TN];
     __shared__ alignas(8) uint64_t s_bar[2];
     __shared__ uint4 s_work[2][2];
@@ -2060,6 +2064,7 @@ FastArgs make_args(mpm_handle* h, double dt)
     a.ctr = f.counters ? f.counters + CNT_COUNT * c : nullptr;
     a.obstart = f.bstart[o]; a.obend = f.bend[o]; a.oactive = f.active[o];
     a.octr = f.counters ? f.counters + CNT_COUNT * o : nullptr;
+    a.nctr = f.counters ? f.counters + CNT_COUNT * o : nullptr;
     a.dcount = f.dcount; a.doff = f.doff; a.bcount = f.bcount; a.scan = f.scan;
     a.nblk = f.total_blocks;
     a.part = kPartSize[f.route_variant];
@@ -2645,7 +2650,7 @@ int fast_prepare(mpm_handle* h)
     timer_end(h, slot);
     MPM_CUDA(h, cudaMemsetAsync(f.dcount, 0, (size_t)ROW * f.total_blocks * sizeof(uint32_t), h->stream));
     MPM_CUDA(h, cudaMemsetAsync(f.bcount, 0, f.total_blocks * sizeof(unsigned long long), h->stream));
-    MPM_CUDA(h, cudaMemsetAsync(f.counters + CNT_COUNT * c, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
+    MPM_CUDA(h, cudaMemsetAsync(f.counters, 0, 2 * CNT_COUNT * sizeof(uint32_t), h->stream));   // both sets
     FastArgs a = make_args(h, 0.0);
     k_prepare<<<grid_stride_blocks(h, n, 256), 256, 0, h->stream>>>(a, f.bstart[c], f.bend[c], f.active[c],
                                                                     f.counters + CNT_COUNT * c);
@@ -2661,10 +2666,8 @@ int fast_prepare(mpm_handle* h)
 static int fast_route(mpm_handle* h)
 {
     FastState& f = h->fast;
-    const int c = f.cur;
     int slot = timer_begin(h, "fast_bins");
-    MPM_CUDA(h, cudaMemsetAsync(f.counters + CNT_COUNT * c, 0, CNT_COUNT * sizeof(uint32_t), h->stream));
-    FastArgs a = make_args(h, 0.0);
+    FastArgs a = make_args(h, 0.0);   // a.ctr: cleared by the last G2P or by fast_prepare
     const int64_t tiles = (f.total_blocks + BIN_TILE - 1) / BIN_TILE;
     k_bins<<<(unsigned)tiles, BIN_THREADS, 0, h->stream>>>(a);
     MPM_LAUNCHED(h, "k_bins");
