@@ -804,9 +804,9 @@ __device__ __forceinline__ void factors_from(const FastArgs& a, const SceneDev& 
     }
 }
 
-__device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneDev& sc, uint32_t j, P2GFactors& P)
+// i = perm[j], the slot of sorted position j (callers load it early).
+__device__ __forceinline__ void particle_factors(const FastArgs& a, const SceneDev& sc, uint32_t j, uint32_t i, P2GFactors& P)
 {
-    const uint32_t i = a.perm[j];
     float X[3], V[3], F[9], B[9];
 #pragma unroll
     for(int r = 0; r < 3; r++) { X[r] = a.src[(C_X + r) * a.npad + i]; V[r] = a.vsrc[r * a.npad + i]; }
@@ -1042,9 +1042,11 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
         uint32_t cell = 0, r = 0;
         float bnd[4] = {0.f, 0.f, 0.f, 0.f};
         P2GFactors P;
-        if(mine) {
+        uint32_t slot = 0;
+        if(mine) {   // the slot with the key: one round trip before the particle loads, not two
             const uint32_t j = s + part + threadIdx.x * parts;
             cell = a.sorted_keys[j] & 63u;
+            slot = a.perm[j];
             r = atomicAdd(&S.ccount[cell], 1u);
         }
         __syncthreads();
@@ -1060,7 +1062,7 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
             nb_prev = atomicExch(&a.nb_flag[nb], 1u);
         }
         if(mine) {
-            particle_factors(a, S.sc, s + part + threadIdx.x * parts, P);
+            particle_factors(a, S.sc, s + part + threadIdx.x * parts, slot, P);
             factor_bounds(P, bnd);
         }
 #pragma unroll
@@ -1297,7 +1299,7 @@ template<int T> __global__ void __launch_bounds__(T, 512 / T) k_p2g_groups(FastA
             int pc = -1;
             if(mine < r1) {
                 pc = S.lcell[mine];
-                particle_factors(a, sc, S.list[mine], P);
+                particle_factors(a, sc, S.list[mine], a.perm[S.list[mine]], P);
             } else {
 #pragma unroll
                 for(int e = 0; e < 9; e++) P.w[e] = 0.f;

@@ -233,6 +233,35 @@ def test_graph_advance_matches_eager(cuda_device):
         assert rel(res[1][k], res[0][k], 1.0) < 1e-6
 
 
+@pytest.mark.parametrize("path", ["fast", "plain"])
+def test_timed_substeps_match_untimed(cuda_device, path):
+    """With per-kernel timing on, the substeps run eagerly with events around
+    each kernel: the state equals the untimed (graph-replayed) run's, and every
+    kernel of the substep is timed once per substep."""
+    scene = S.small_3d(nsteps=6)
+    p = D().PATH_FAST if path == "fast" else D().PATH_PLAIN
+    prec = D().FP32 if path == "fast" else D().FP64
+    res, timers = [], None
+    for timed in (False, True):
+        drv = D().MPM_DRIVER(scene, precision=prec, path=p)
+        drv.set_scene_particles(scene)
+        drv.advance(2)
+        drv.set_timing(timed)
+        for _ in range(4):
+            drv.Advance_One_Time_Step()
+        drv.synchronize()
+        if timed:
+            timers = drv.get_timing()
+        res.append(drv.get_particles())
+        drv.close()
+    for k in ("X", "V", "F"):
+        assert rel(res[1][k], res[0][k], 1.0) < 1e-6, k
+    names = ("fast_bins", "fast_route", "fast_p2g", "fast_grid", "fast_g2p") if path == "fast" else \
+        ("plain_p2g", "plain_g2p")
+    for name in names:
+        assert name in timers and timers[name][1] == 4 and timers[name][0] > 0, (name, timers.get(name))
+
+
 def test_empty_and_leaving_particles(cuda_device):
     scene = S.small_3d(with_walls=False)
     for path, prec in ((D().PATH_FAST, D().FP32), (D().PATH_PLAIN, D().FP64)):
