@@ -4,12 +4,13 @@
 // Per substep (MPM_DRIVER::Advance_One_Time_Step, MPM_DRIVER.cpp:141-157), each
 // phase is ONE launch over the blocks of all scenes:
 //   bins     the substep's order from the previous one: per particle block
-//            (4^3 cells) its count from the neighbour blocks' move counts the
-//            last G2P kept, a scan into block ranges, the work items (parts of
-//            a block's particles) and where each group of moved particles lands.
+//            (4^3 cells) its arrivals, counted by the last G2P in the block's
+//            row by direction, a scan into block ranges, the work items (parts
+//            of a block's particles) and where each group of moved particles
+//            lands.
 //   route    every particle slot to its place in that order (a stable sort by
 //            block; invalid particles go to the tail).
-//   p2g      one CTA per part: B-spline weights, the stress P(F) F^T (fused;
+//   p2g      persistent CTAs over the work items: B-spline weights, the stress P(F) F^T (fused;
 //            MPM_FINITE_ELEMENTS::Precompute, .cpp:47-67), APIC momentum plus
 //            dt * force into a 6^3-node shared fixed-point tile, flushed with
 //            one float4 atomic per touched node (Particle_To_Grid l.245-306 with
@@ -18,7 +19,8 @@
 //   grid     one thread per node of the marked node blocks: v = (mv + dt f)/m
 //            + dt g, collision projection and friction (Apply_Forces
 //            l.959-1060); clears the accumulator for the next substep.
-//   g2p      one CTA per part: stage the tile of (v, v_fric), gather, update F,
+//   g2p      persistent CTAs over the work items: the tile of (v, v_fric) by TMA
+//            (the next item's copy in flight), gather, update F,
 //            X, V and the APIC B (Grid_To_Particle l.450-515), write the
 //            particle to its slot in the other buffer with its next key, and
 //            count where the part's particles move (the next bins' input).

@@ -113,7 +113,7 @@ struct FastState {
     uint32_t grid_node_blocks = 0;
     bool grid_dirty = false;   // the accumulator holds a P2G that no grid update consumed
     void* staging = nullptr;   // device copies of host particle arrays (set / get)
-    size_t staging_bytes = 0;   // sort_scratch holds the digit histograms of `keys` (built by G2P)
+    size_t staging_bytes = 0;   // size of `staging`
     // launch shapes (mpm_autotune)
     int p2g_variant = MPM_P2G_FIXED256;       // P2G launch shape (MPM_P2G_*)
     int route_variant = MPM_P2G_FIXED256;     // the shape whose work-item size the current order has
