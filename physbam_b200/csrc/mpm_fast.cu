@@ -1065,6 +1065,21 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
             nb = S.sc.nb_base + ((uint32_t)(bx + (o >> 2)) * S.sc.NN[1] + by + ((o >> 1) & 1)) * S.sc.NN[2] + bz + (o & 1);
             nb_prev = atomicExch(&a.nb_flag[nb], 1u);
         }
+        // the part's rounds: every warp reduces the 64 cell counts itself (no
+        // barrier) and writes the masks of its rounds
+        const uint32_t cc0 = S.ccount[lane], cc1 = S.ccount[lane + 32];
+        uint32_t mc = max(cc0, cc1);
+#pragma unroll
+        for(int o = 16; o; o >>= 1) mc = max(mc, __shfl_xor_sync(0xffffffffu, mc, o));
+        const int maxc = (int)mc;
+        for(int rr = warp; rr < maxc; rr += NW) {
+            const unsigned lo = __ballot_sync(0xffffffffu, cc0 > (uint32_t)rr);
+            const unsigned hi = __ballot_sync(0xffffffffu, cc1 > (uint32_t)rr);
+            if(lane == 0) {
+                S.rmask[rr] = lo | ((unsigned long long)hi << 32);
+                S.rsize[rr] = __popc(lo) + __popc(hi);
+            }
+        }
         if(mine) {
             particle_factors(a, S.sc, s + part + threadIdx.x * parts, slot, P);
             factor_bounds(P, bnd);
@@ -1076,22 +1091,7 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
             for(int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             if(lane == 0 && v != 0.f) atomicAdd(&S.bound[q], v);
         }
-        if(threadIdx.x < 64) {
-            uint32_t c = S.ccount[threadIdx.x];
-#pragma unroll
-            for(int o = 16; o; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
-            if(lane == 0) atomicMax(&S.maxc, (int)c);
-        }
         __syncthreads();
-        const int maxc = S.maxc;
-        for(int rr = warp; rr < maxc; rr += NW) {
-            const unsigned lo = __ballot_sync(0xffffffffu, S.ccount[lane] > (uint32_t)rr);
-            const unsigned hi = __ballot_sync(0xffffffffu, S.ccount[lane + 32] > (uint32_t)rr);
-            if(lane == 0) {
-                S.rmask[rr] = lo | ((unsigned long long)hi << 32);
-                S.rsize[rr] = __popc(lo) + __popc(hi);
-            }
-        }
         if(threadIdx.x >= T - 4) {   // the scale of each quantity
             const int q = threadIdx.x - (T - 4);
             const float B = S.bound[q];
@@ -1104,7 +1104,6 @@ template<int T> __global__ void __launch_bounds__(T, 768 / T) k_p2g(FastArgs a)
             }
             S.scale[q] = sc;
         }
-        __syncthreads();
         if(warp == 0) {   // exclusive scan of the round sizes
             uint32_t carry = 0;
             for(int r0 = 0; r0 < maxc; r0 += 32) {
